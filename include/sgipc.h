@@ -1,0 +1,238 @@
+/*
+ * sgipc.h — C ABI of the B200-native per-Newton-iteration linear system of StiffGIPC.
+ *
+ * The reference has no C ABI; its C++ class interfaces are the API this header
+ * replaces.  Every entry point below names the reference interface it stands in for.
+ *
+ * Conventions (all entry points):
+ *   - return an SgipcStatus; nothing aborts or exits the process;
+ *   - array arguments marked [dev] are caller-owned device pointers, [host] host ones;
+ *   - `stream` is a cudaStream_t passed as void* (0 = legacy default stream); all work
+ *     is stream-ordered and no entry point synchronises the device unless it returns a
+ *     host-side scalar (documented per call);
+ *   - one host thread per context, as the reference uses one host thread per GIPC
+ *     object (StiffGIPC/gl_main.cu:100-108);
+ *   - vectors of 3D points are packed double3 (x0,y0,z0,x1,...), 3x3 blocks are row-major.
+ */
+#ifndef SGIPC_H_
+#define SGIPC_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum SgipcStatus {
+    SGIPC_OK            = 0,
+    SGIPC_CUDA_ERROR    = 1,  /* a CUDA runtime call or kernel launch failed */
+    SGIPC_NOT_CONVERGED = 2,  /* PCG hit its iteration cap (reference: 0.3*dof, pcg_solver.cu:168) */
+    SGIPC_BREAKDOWN     = 3,  /* p^T A p <= 0 or a non-finite scalar inside PCG */
+    SGIPC_BAD_INPUT     = 4,  /* null pointer, negative count, index out of range, NaN input */
+    SGIPC_CAPACITY      = 5,  /* more pairs/blocks than the context was created for */
+    SGIPC_NOT_READY     = 6   /* a call whose prerequisite (assemble, mas_build) has not run */
+} SgipcStatus;
+
+typedef enum SgipcPrecision {
+    SGIPC_FP64  = 0,  /* FP64 matrix, vectors and MAS domain inverses ("plain FP64 MAS-PCG") */
+    SGIPC_MIXED = 1,  /* FP32 matrix copy, FP32 MAS and inner PCG; FP64 residual refinement */
+    SGIPC_REF   = 2   /* the reference's shipping mix: FP64 matrix/PCG, FP32 MAS inverses */
+} SgipcPrecision;
+
+typedef enum SgipcCriterion {
+    SGIPC_CRIT_RZ   = 0,  /* |r.z| <= tol * r0.z0, checked before the update (pcg_solver.cu:232) */
+    SGIPC_CRIT_TRUE = 1   /* ||b - A x||_2 <= tol * ||b||_2 */
+} SgipcCriterion;
+
+/* Static topology, given once at context creation [host].  Mirrors what
+ * StiffGIPC's init reads: the tet/triangle/hinge connectivity (device_TetraData,
+ * StiffGIPC/device_fem_data.cuh:17-78) and the MAS neighbour CSR + part maps
+ * (MASPreconditioner::initPreconditioner_Neighbor, StiffGIPC/MASPreconditioner.cu:2264). */
+typedef struct SgipcTopology {
+    int32_t         vertex_num;
+    int32_t         tet_num;
+    int32_t         tri_num;
+    int32_t         tri_edge_num;
+    int32_t         soft_num;
+    const uint32_t* tetrahedras;          /* uint4[tet_num] */
+    const uint32_t* triangles;            /* uint3[tri_num] */
+    const uint32_t* tri_edges;            /* uint2[tri_edge_num] */
+    const int32_t*  tri_edge_adj_vertex;  /* int2[tri_edge_num], -1 = boundary hinge */
+    const uint32_t* targetIndex;          /* uint32[soft_num] */
+    /* MAS partition: positions padded to a multiple of 16 (partId_map_real = -1 on padding) */
+    int32_t         part_map_size;
+    const int32_t*  partId_map_real;      /* int[part_map_size] */
+    const int32_t*  real_map_partId;      /* int[vertex_num] */
+    const uint32_t* neighborStart;        /* uint[vertex_num + 1] (CSR; the reference keeps start+num) */
+    const uint32_t* neighborList;         /* uint[neighborStart[vertex_num]] */
+    /* capacities of the per-Newton contact inputs */
+    int32_t         max_pairs;
+    int32_t         max_ground;
+    int32_t         max_fric_pairs;
+    int32_t         max_fric_ground;
+    int32_t         max_rhs;              /* right-hand sides batched in one adjoint solve (>= 1) */
+} SgipcTopology;
+
+/* Per-Newton FEM state [dev]; field names follow device_TetraData. */
+typedef struct SgipcFemData {
+    const double*   vertexes;             /* double3[V]  current iterate x */
+    const double*   o_vertexes;           /* double3[V]  start-of-step positions (friction) */
+    const double*   rest_vertexes;        /* double3[V]  rest positions (mollifier eps) */
+    const double*   xTilta;               /* double3[V]  inertial target */
+    const double*   masses;               /* double[V] */
+    const int32_t*  BoundaryType;         /* int[V], 0 = free */
+    const double*   DmInverses;           /* Matrix3x3d[T] row-major */
+    const double*   volum;                /* double[T] */
+    const double*   lengthRate;           /* double[T]  4*mu/3 */
+    const double*   volumeRate;           /* double[T]  lambda + 5*mu/6 */
+    const double*   triDmInverses;        /* Matrix2x2d[F] row-major */
+    const double*   area;                 /* double[F]  area * thickness */
+    const double*   quad_bending_Q;       /* Matrix4d[Eh] (column-major, as Eigen stores it) */
+    const double*   targetVert;           /* double3[soft_num] */
+} SgipcFemData;
+
+/* Contact inputs of one Newton iteration [dev].  Encodings as produced by the
+ * reference's LBVH queries (StiffGIPC/mlbvh.cu:560-1059). */
+typedef struct SgipcContacts {
+    const int32_t*  pairs;                /* int4[pair_num] */
+    int32_t         pair_num;
+    const uint32_t* ground_pairs;         /* uint[ground_num] vertex ids near the ground */
+    int32_t         ground_num;
+    /* lagged friction set-up (_calFrictionLastH_DistAndTan, StiffGIPC/GIPC.cu:8388) */
+    const int32_t*  fric_pairs;           /* int4[fric_num] */
+    const double*   fric_lambda;          /* double[fric_num] lagged normal force */
+    const double*   fric_coord;           /* double2[fric_num] closest-point coordinates */
+    const double*   fric_basis;           /* Matrix3x2d[fric_num] row-major tangent basis */
+    int32_t         fric_num;
+    const uint32_t* fric_gd_pairs;        /* uint[fric_gd_num] */
+    const double*   fric_gd_lambda;       /* double[fric_gd_num] */
+    int32_t         fric_gd_num;
+} SgipcContacts;
+
+/* Scalars of the Newton system (the GIPC members read by computeGradientAndHessian). */
+typedef struct SgipcParams {
+    double dt;               /* IPC_dt */
+    double dHat;             /* squared barrier distance (GIPC.cu:8602) */
+    double kappa;            /* barrier stiffness */
+    double fDhat;            /* friction d-hat, squared (GIPC.cu:8603); eps_f^2 = fDhat*dt^2 */
+    double frictionRate;     /* mu for pair friction */
+    double gd_frictionRate;  /* mu for ground friction */
+    double ground_offset;    /* plane n.x = offset, n = +y (GIPC.cu:8541-8549) */
+    double stretchStiff;     /* cloth membrane */
+    double shearStiff;
+    double strainRate;
+    double bendStiff;
+    double motionRate;       /* soft constraint stiffness */
+    double softRate;         /* soft constraint rate (squared inside) */
+} SgipcParams;
+
+typedef struct SgipcSolveStats {
+    int32_t iterations;          /* PCG iterations (inner iterations summed in MIXED mode) */
+    int32_t refinements;         /* outer refinement steps (MIXED) */
+    double  rz0;                 /* r0.z0 */
+    double  rz;                  /* final r.z */
+    double  rel_residual;        /* ||b - A x|| / ||b|| recomputed in FP64 */
+    int32_t status;              /* SgipcStatus of the solve */
+} SgipcSolveStats;
+
+typedef struct SgipcCtx SgipcCtx;
+
+/* ---- context ------------------------------------------------------------------------ */
+
+/* Builds the static symmetric-upper BSR pattern of the FEM topology (tets, triangles,
+ * hinges, mass diagonal), the element -> slot maps and the MAS level-0 tables, and
+ * allocates every workspace.  Replaces GIPC::init's triplet buffers (GIPC.cu:8593-8640),
+ * MASPreconditioner::initPreconditioner_Neighbor/_Matrix (MASPreconditioner.cu:2264-2330)
+ * and PCGSolver's vectors (pcg_solver.cu:158-172).  Synchronises the device. */
+SgipcStatus sgipc_create(const SgipcTopology* topo, int device, SgipcCtx** out);
+SgipcStatus sgipc_destroy(SgipcCtx* ctx);
+const char* sgipc_status_string(SgipcStatus s);
+/* Last CUDA error text recorded on the context (empty if none). */
+const char* sgipc_last_error(const SgipcCtx* ctx);
+
+/* ---- assembly (GIPC::computeGradientAndHessian, StiffGIPC/GIPC.cu:10110-10344) -------- */
+
+/* Full assembly: kinetic gradient, barrier, friction, ground, soft constraints, stable
+ * Neo-Hookean tets, cloth membrane, quadratic bending, Dirichlet zeroing and the mass
+ * diagonal, written straight into the context's BSR (static part) and contact BCOO
+ * (dynamic part), plus the right-hand side b = fb + shape_grads with Dirichlet rows
+ * zeroed (FEMLinearSubsystem::assemble, fem_linear_subsystem.cu:56-84).  Stream-ordered. */
+SgipcStatus sgipc_assemble(SgipcCtx* ctx, const SgipcFemData* fem, const SgipcContacts* con,
+                           const SgipcParams* prm, void* stream);
+
+/* GIPC::calBarrierGradientAndHessian (GIPC.cu:9112): barrier gradient added into
+ * grad [dev double3[V]] and barrier blocks written into the contact BCOO. */
+SgipcStatus sgipc_barrier_grad_hess(SgipcCtx* ctx, const SgipcFemData* fem,
+                                    const SgipcContacts* con, const SgipcParams* prm,
+                                    double* grad, void* stream);
+/* GIPC::calFrictionGradient + calFrictionHessian (GIPC.cu:9164-9217). */
+SgipcStatus sgipc_friction_grad_hess(SgipcCtx* ctx, const SgipcFemData* fem,
+                                     const SgipcContacts* con, const SgipcParams* prm,
+                                     double* grad, void* stream);
+/* femEnergy.cu:1719 _calculate_fem_gradient_hessian: SNK gradient added into grad and
+ * element blocks gathered into the static BSR values. */
+SgipcStatus sgipc_fem_grad_hess(SgipcCtx* ctx, const SgipcFemData* fem, const SgipcParams* prm,
+                                double* grad, void* stream);
+
+/* Copy the assembled upper block matrix out as merged, sorted BCOO (static + contact,
+ * duplicates summed) [host arrays of capacity cap blocks].  Synchronises.  For parity
+ * tests and checkpoints: the layout of GIPCTripletMatrix after Converter::convert. */
+SgipcStatus sgipc_export_bcoo(SgipcCtx* ctx, int32_t cap, int32_t* rows, int32_t* cols,
+                              double* vals, int32_t* count);
+/* Right-hand side b [dev double[3n]] of the last assembly. */
+SgipcStatus sgipc_get_rhs(SgipcCtx* ctx, double* b, void* stream);
+
+/* ---- operators --------------------------------------------------------------------- */
+
+/* y = A x with the assembled symmetric matrix (Spmv::warp_reduce_sym_spmv, spmv.cu:8). */
+SgipcStatus sgipc_spmv(SgipcCtx* ctx, const double* x, double* y, void* stream);
+
+/* MASPreconditioner::setPreconditioner_bcoo (MASPreconditioner.cu:2180): per-Newton
+ * hierarchy with contact connectivity, domain matrices and their inverses. */
+SgipcStatus sgipc_mas_build(SgipcCtx* ctx, const SgipcContacts* con, SgipcPrecision prec,
+                            void* stream);
+/* MASPreconditioner::preconditioning (MASPreconditioner.cu:2221): z = M^-1 r. */
+SgipcStatus sgipc_mas_apply(SgipcCtx* ctx, const double* r, double* z, void* stream);
+/* Host copy of the level structure: levels, per-level node counts, total clusters. */
+SgipcStatus sgipc_mas_info(SgipcCtx* ctx, int32_t* levelnum, int32_t* level_counts /*[8]*/,
+                           int32_t* total_clusters);
+/* Host copy of the per-vertex coarse node table (global cluster index of each vertex at
+ * levels 1..levelnum-1, int[V*(levelnum-1)]) for hierarchy parity tests. */
+SgipcStatus sgipc_mas_export_tables(SgipcCtx* ctx, int32_t* table);
+
+/* ---- solve ------------------------------------------------------------------------- */
+
+/* PCGSolver::pcg (pcg_solver.cu:174-267) on the assembled system: x [dev] = A^-1 b.
+ * max_iter <= 0 selects the reference cap 0.3*dof.  Fills stats [host]; synchronises. */
+SgipcStatus sgipc_pcg_solve(SgipcCtx* ctx, SgipcPrecision prec, SgipcCriterion crit,
+                            double tol, int32_t max_iter, const double* b, double* x,
+                            SgipcSolveStats* stats, void* stream);
+
+/* Batched PCG on nrhs right-hand sides sharing A and M (b, x: [dev] nrhs x 3n, rhs-major). */
+SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* ctx, SgipcPrecision prec, SgipcCriterion crit,
+                                    double tol, int32_t max_iter, int32_t nrhs,
+                                    const double* b, double* x, SgipcSolveStats* stats,
+                                    void* stream);
+
+/* GIPC::calculateMovingDirection (GIPC.cu:10581-10592): MAS build + PCG on the
+ * assembled system, move_dir [dev double3[V]] = dx.  Synchronises (returns stats). */
+SgipcStatus sgipc_solve(SgipcCtx* ctx, const SgipcContacts* con, SgipcPrecision prec,
+                        SgipcCriterion crit, double tol, int32_t max_iter, double* move_dir,
+                        SgipcSolveStats* stats, void* stream);
+
+/* ---- adjoint (new; no counterpart in the reference) --------------------------------- */
+
+/* Parameter derivatives of the gradient g(x; E, v0) at the assembled state, contracted
+ * with nrhs adjoint vectors lambda [dev nrhs x 3V]:
+ *   dLdE  [dev nrhs x T]  = -lambda^T dg/dE_t   (stable Neo-Hookean, per tet)
+ *   dLdv0 [dev nrhs x 3V] = +dt * m_i * lambda_i (g_kin = M(x - x_prev - dt v0 - dt^2 g))
+ * poisson: Poisson ratio used to split E into (lengthRate, volumeRate). */
+SgipcStatus sgipc_adjoint_param_grads(SgipcCtx* ctx, const SgipcFemData* fem,
+                                      const SgipcParams* prm, double poisson, int32_t nrhs,
+                                      const double* lambda, double* dLdE, double* dLdv0,
+                                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SGIPC_H_ */

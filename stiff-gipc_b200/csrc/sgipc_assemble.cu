@@ -1,0 +1,812 @@
+// sgipc_assemble.cu — gradient and Hessian assembly of one Newton iteration.
+//
+// Follows GIPC::computeGradientAndHessian (StiffGIPC/GIPC.cu:10110-10344):
+//   kinetic gradient M(x - x~)                          GIPC.cu:6339
+//   IPC barrier, RANK 2, Gauss-Newton Hessian            GIPC.cu:3106-4945
+//   lagged smoothed friction (pairs and ground)          GIPC.cu:1357-1800, 5047-5270
+//   ground barrier, soft constraints                     GIPC.cu:6363-6514
+//   stable Neo-Hookean tets with the analytic projection femEnergy.cu:1593-1857
+//   Dirichlet zeroing, mass diagonal                     GIPC.cu:10295-10336
+//   b = fb + shape_grads, Dirichlet rows zeroed          fem_linear_subsystem.cu:56-84
+//
+// Layout on the GPU (all FP64):
+//   * static part: element kernels write oriented 3x3 blocks into per-element slots
+//     (eblk) and per-vertex gradient rows (egrad); gather kernels sum them into the BSR
+//     values and shape_grads through CSR lists built at context creation;
+//   * dynamic part: every contact pair writes its upper blocks under a (row,col) key; one
+//     radix sort plus a segmented sum gives the unique contact blocks, kept row-sorted
+//     together with a transposed index list so that SpMV needs no atomics.
+#include <cub/cub.cuh>
+
+#include "sgipc_internal.cuh"
+
+using namespace sgipc;
+
+namespace {
+
+constexpr unsigned long long kBadKey = ~0ull;
+
+// ------------------------------------------------------------------------------------------
+// kinetic gradient, reset of the contact gradient
+// ------------------------------------------------------------------------------------------
+__global__ void k_kinetic(int nv, const double* __restrict__ x, const double* __restrict__ xt,
+                          const double* __restrict__ m, double* __restrict__ shape_grads, double* __restrict__ fb) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * nv) return;
+    shape_grads[i] = m[i / 3] * (x[i] - xt[i]);
+    fb[i] = 0.0;
+}
+
+// ------------------------------------------------------------------------------------------
+// stable Neo-Hookean tet (USE_SNK1): PK1 femEnergy.cu:432-459, eigensystem 1593-1717
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_snk(int nt, const uint32_t* __restrict__ tets, const double* __restrict__ x,
+                                             const double* __restrict__ dminv, const double* __restrict__ vol,
+                                             const double* __restrict__ lr, const double* __restrict__ vr, double dt2,
+                                             double* __restrict__ eblk, double* __restrict__ egrad) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    uint4 tv = reinterpret_cast<const uint4*>(tets)[t];
+    const uint32_t vid[4] = {tv.x, tv.y, tv.z, tv.w};
+    d3 X0 = ld3(x, tv.x), X1 = ld3(x, tv.y), X2 = ld3(x, tv.z), X3 = ld3(x, tv.w);
+    double Di[3][3];
+#pragma unroll
+    for (int k = 0; k < 9; k++) Di[k / 3][k % 3] = dminv[9 * (size_t)t + k];
+    const double mu = lr[t], lam = vr[t], sc = dt2 * vol[t];
+    d3 e1 = X1 - X0, e2 = X2 - X0, e3 = X3 - X0;
+    double F[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        double a = comp(e1, i), b = comp(e2, i), c = comp(e3, i);
+#pragma unroll
+        for (int j = 0; j < 3; j++) F[i][j] = a * Di[0][j] + b * Di[1][j] + c * Di[2][j];
+    }
+    d3 f0 = mk(F[0][0], F[1][0], F[2][0]), f1 = mk(F[0][1], F[1][1], F[2][1]), f2 = mk(F[0][2], F[1][2], F[2][2]);
+    d3 g0 = cross(f1, f2), g1 = cross(f2, f0), g2 = cross(f0, f1);
+    const double J = dot(f0, g0);
+    const double ev = lam * (J - 1.0) - mu;  // evScale of the twist/flip pairs
+    // P = mu F + (lam (J - 1) - mu) cof(F); gradient rows G = P Dm^-T
+    d3 P0 = mu * f0 + ev * g0, P1 = mu * f1 + ev * g1, P2 = mu * f2 + ev * g2;
+    d3 gr[4];
+#pragma unroll
+    for (int k = 0; k < 3; k++) gr[k + 1] = sc * (Di[k][0] * P0 + Di[k][1] * P1 + Di[k][2] * P2);
+    gr[0] = -(gr[1] + gr[2] + gr[3]);
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        double* o = egrad + 3 * (4 * (size_t)t + a);
+        o[0] = gr[a].x;
+        o[1] = gr[a].y;
+        o[2] = gr[a].z;
+    }
+    // analytic eigensystem of d2Psi/dF2 (Smith et al., "Analytic eigensystems for isotropic
+    // distortion energies"): twist/flip pairs per axis plus a 3x3 scaling block
+    double U[3][3], S[3], V[3][3];
+    svd3_rv(F, U, S, V);
+    double c1[3], c2[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double lt = fmax(mu + ev * S[k], 0.0), lf = fmax(mu - ev * S[k], 0.0);
+        c1[k] = 0.5 * (lt + lf);
+        c2[k] = 0.5 * (lf - lt);
+    }
+    double A[3][3], Q[3][3];
+    const double es = lam * (2.0 * J - 1.0) - mu;
+    A[0][0] = mu + lam * S[1] * S[1] * S[2] * S[2];
+    A[1][1] = mu + lam * S[0] * S[0] * S[2] * S[2];
+    A[2][2] = mu + lam * S[0] * S[0] * S[1] * S[1];
+    A[0][1] = A[1][0] = es * S[2];
+    A[0][2] = A[2][0] = es * S[1];
+    A[1][2] = A[2][1] = es * S[0];
+    sym_eig3(A, Q);
+    double Sp[3][3];
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            double s = 0;
+#pragma unroll
+            for (int m = 0; m < 3; m++) s += fmax(A[m][m], 0.0) * Q[p][m] * Q[q][m];
+            Sp[p][q] = s;
+        }
+    // d_a = V^T D(a,:)^T with D the rows of dF/dx
+    double d[4][3];
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double v = V[j][p];
+            s1 += v * Di[0][j];
+            s2 += v * Di[1][j];
+            s3 += v * Di[2][j];
+        }
+        s0 = -(s1 + s2 + s3);
+        d[0][p] = s0;
+        d[1][p] = s1;
+        d[2][p] = s2;
+        d[3][p] = s3;
+    }
+    const int pa[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
+    const int pb[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+    const int ax_i[3] = {1, 0, 0}, ax_j[3] = {2, 2, 1};
+#pragma unroll 1
+    for (int k = 0; k < 10; k++) {
+        const int a = pa[k], b = pb[k];
+        double K[3][3];
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) K[p][q] = Sp[p][q] * d[a][p] * d[b][q];
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            const int i = ax_i[m], j = ax_j[m];
+            K[j][j] += c1[m] * d[a][i] * d[b][i];
+            K[i][i] += c1[m] * d[a][j] * d[b][j];
+            K[j][i] += c2[m] * d[a][i] * d[b][j];
+            K[i][j] += c2[m] * d[a][j] * d[b][i];
+        }
+        // H = sc * U K U^T, written transposed when the element's vertex order is reversed
+        double UK[3][3];
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) UK[p][q] = U[p][0] * K[0][q] + U[p][1] * K[1][q] + U[p][2] * K[2][q];
+        const bool tr = vid[a] > vid[b];
+        double* o = eblk + 9 * (10 * (size_t)t + k);
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                double h = sc * (UK[p][0] * U[q][0] + UK[p][1] * U[q][1] + UK[p][2] * U[q][2]);
+                o[tr ? (3 * q + p) : (3 * p + q)] = h;
+            }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// static gathers
+// ------------------------------------------------------------------------------------------
+__global__ void k_gather_blocks(int nnz, const int* __restrict__ cptr, const int* __restrict__ contrib,
+                                const double* __restrict__ eblk, const int* __restrict__ slot_row,
+                                const int* __restrict__ col, const int32_t* __restrict__ btype,
+                                const double* __restrict__ mass, double* __restrict__ v64, float* __restrict__ v32) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 9LL * nnz) return;
+    int s = (int)(tid / 9), q = (int)(tid % 9);
+    int r = slot_row[s], c = col[s];
+    double acc = 0.0;
+    if (btype[r] == 0 && btype[c] == 0)
+        for (int k = cptr[s]; k < cptr[s + 1]; k++) acc += eblk[9 * (size_t)contrib[k] + q];
+    if (r == c && (q == 0 || q == 4 || q == 8)) acc += mass[r];
+    v64[tid] = acc;
+    v32[tid] = (float)acc;
+}
+
+__global__ void k_gather_grad(int nv, const int* __restrict__ vptr, const int* __restrict__ vinc,
+                              const double* __restrict__ egrad, double* __restrict__ shape_grads) {
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 3 * nv) return;
+    int v = tid / 3, q = tid % 3;
+    double acc = 0.0;
+    for (int k = vptr[v]; k < vptr[v + 1]; k++) acc += egrad[3 * (size_t)vinc[k] + q];
+    shape_grads[tid] += acc;
+}
+
+__global__ void k_rhs(int nv, const double* __restrict__ fb, const double* __restrict__ sg,
+                      const int32_t* __restrict__ btype, double* __restrict__ b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * nv) return;
+    b[i] = btype[i / 3] != 0 ? 0.0 : fb[i] + sg[i];
+}
+
+// ------------------------------------------------------------------------------------------
+// contact blocks
+// ------------------------------------------------------------------------------------------
+struct BlockSink {
+    unsigned long long* key;
+    int* idx;
+    double* val;
+    const int32_t* btype;
+    int bits;
+    int nv;
+    int* flag;  // set to 1 when a pair names a vertex outside [0, nv)
+};
+
+__device__ __forceinline__ bool ids_ok(const BlockSink& bs, const int* v, int n) {
+    for (int a = 0; a < n; a++)
+        if (v[a] < 0 || v[a] >= bs.nv) {
+            atomicOr(bs.flag, 1);
+            return false;
+        }
+    return true;
+}
+
+// store up to 10 upper blocks of an nv-vertex pair: H_ab = sum_t coef_t u_t,a w_t,b^T
+// expressed through a callback producing the 3x3 block for local (a,b)
+template <class BlockFn>
+__device__ __forceinline__ void emit_pair_blocks(const BlockSink& bs, int base, int nvp, const int* vid, BlockFn fn) {
+    int k = 0;
+#pragma unroll 1
+    for (int a = 0; a < 4; a++)
+#pragma unroll 1
+        for (int b = a; b < 4; b++, k++) {
+            int slot = base + k;
+            bs.idx[slot] = slot;
+            if (a >= nvp || b >= nvp) {
+                bs.key[slot] = kBadKey;
+                continue;
+            }
+            int r = vid[a], c = vid[b];
+            bool tr = r > c;
+            int rr = tr ? c : r, cc = tr ? r : c;
+            bs.key[slot] = ((unsigned long long)rr << bs.bits) | (unsigned long long)cc;
+            double H[3][3];
+            fn(a, b, H);
+            bool dir = bs.btype[r] != 0 || bs.btype[c] != 0;
+            double* o = bs.val + 9 * (size_t)slot;
+#pragma unroll
+            for (int p = 0; p < 3; p++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) o[3 * p + q] = dir ? 0.0 : (tr ? H[q][p] : H[p][q]);
+        }
+}
+
+__device__ __forceinline__ void emit_diag_block(const BlockSink& bs, int slot, int v, const double H[3][3]) {
+    bs.idx[slot] = slot;
+    bs.key[slot] = ((unsigned long long)v << bs.bits) | (unsigned long long)v;
+    bool dir = bs.btype[v] != 0;
+    double* o = bs.val + 9 * (size_t)slot;
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+        for (int q = 0; q < 3; q++) o[3 * p + q] = dir ? 0.0 : H[p][q];
+}
+
+__device__ __forceinline__ void add_grad(double* fb, int v, d3 g) {
+    atomicAdd(fb + 3 * v, g.x);
+    atomicAdd(fb + 3 * v + 1, g.y);
+    atomicAdd(fb + 3 * v + 2, g.z);
+}
+
+// Decoded barrier pair: kind 0 PP, 1 PE, 2 PT, 3 EE, 4 mollified EE, 5 mollified PE,
+// 6 mollified PP (encoding of StiffGIPC/mlbvh.cu:560-1059, decoded as GIPC.cu:3131-4945)
+__device__ __forceinline__ int decode_pair(int4 e, int* v, int& nvp) {
+    if (e.x >= 0) {
+        v[0] = e.x; v[1] = e.y; v[2] = e.z;
+        if (e.w >= 0) { v[3] = e.w; nvp = 4; return 3; }
+        v[3] = -e.w - 1; nvp = 4; return 4;
+    }
+    v[0] = -e.x - 1;
+    if (e.z < 0) {
+        if (e.y < 0) { v[1] = -e.y - 1; v[2] = -e.z - 1; v[3] = -e.w - 1; nvp = 4; return 6; }
+        v[1] = e.y; v[2] = v[3] = 0; nvp = 2; return 0;
+    }
+    if (e.w < 0) {
+        if (e.y < 0) { v[1] = -e.y - 1; v[2] = e.z; v[3] = -e.w - 1; nvp = 4; return 5; }
+        v[1] = e.y; v[2] = e.z; v[3] = 0; nvp = 3; return 1;
+    }
+    v[1] = e.y; v[2] = e.z; v[3] = e.w; nvp = 4; return 2;
+}
+
+// squared distance and its gradient (hand-derived, see the derivation in each branch)
+__device__ __forceinline__ double dist2_grad(int kind, const d3* X, d3* g) {
+    if (kind == 0 || kind == 6) {  // |a - b|^2
+        d3 d = X[0] - X[1];
+        g[0] = 2.0 * d;
+        g[1] = -2.0 * d;
+        g[2] = g[3] = mk(0, 0, 0);
+        return sq(d);
+    }
+    if (kind == 1 || kind == 5) {  // |(e0-p) x (e1-p)|^2 / |e1-e0|^2
+        d3 p = X[0], e0 = X[1], e1 = X[2];
+        d3 c = cross(e0 - p, e1 - p), e = e1 - e0;
+        double L = sq(e), C = sq(c);
+        d3 gp = 2.0 * cross(c, e), ge0 = 2.0 * cross(e1 - p, c), ge1 = 2.0 * cross(c, e0 - p);
+        double iL = 1.0 / L, r = C * iL * iL;
+        g[0] = iL * gp;
+        g[1] = iL * ge0 + (2.0 * r) * e;
+        g[2] = iL * ge1 - (2.0 * r) * e;
+        g[3] = mk(0, 0, 0);
+        return C * iL;
+    }
+    if (kind == 2) {  // s^2 / |n|^2, n = (t1-t0) x (t2-t0), s = (p - t0).n
+        d3 p = X[0], t0 = X[1], t1 = X[2], t2 = X[3];
+        d3 e1 = t1 - t0, e2 = t2 - t0, w = p - t0;
+        d3 n = cross(e1, e2);
+        double s = dot(w, n), N = sq(n), iN = 1.0 / N;
+        d3 sp = n, s0 = cross(e1 - e2, w) - n, s1 = cross(e2, w), s2 = cross(w, e1);
+        d3 N0 = 2.0 * cross(e1 - e2, n), N1 = 2.0 * cross(e2, n), N2 = 2.0 * cross(n, e1);
+        double a = 2.0 * s * iN, b = s * s * iN * iN;
+        g[0] = a * sp;
+        g[1] = a * s0 - b * N0;
+        g[2] = a * s1 - b * N1;
+        g[3] = a * s2 - b * N2;
+        return s * s * iN;
+    }
+    // EE: s^2/|n|^2, n = (a1-a0) x (b1-b0), s = (b0 - a0).n
+    d3 a0 = X[0], a1 = X[1], b0 = X[2], b1 = X[3];
+    d3 u = a1 - a0, v = b1 - b0, w = b0 - a0;
+    d3 n = cross(u, v);
+    double s = dot(w, n), N = sq(n), iN = 1.0 / N;
+    d3 vw = cross(v, w), wu = cross(w, u), vn = cross(v, n), nu = cross(n, u);
+    double a = 2.0 * s * iN, b = s * s * iN * iN;
+    g[0] = a * (-1.0 * n - vw) + (2.0 * b) * vn;
+    g[1] = a * vw - (2.0 * b) * vn;
+    g[2] = a * (n - wu) + (2.0 * b) * nu;
+    g[3] = a * wu - (2.0 * b) * nu;
+    return s * s * iN;
+}
+
+// B(I) = c (I-1)^2 ln(I)^2 and its first two derivatives in I
+__device__ __forceinline__ void barrier_s(double I, double c, double& B, double& dB, double& d2B) {
+    double L = log(I), t = I - 1.0;
+    B = c * t * t * L * L;
+    dB = c * (2.0 * t * L * L + 2.0 * t * t * L / I);
+    d2B = c * (2.0 * L * L + 8.0 * t * L / I + 2.0 * t * t * (1.0 - L) / (I * I));
+}
+
+__global__ void __launch_bounds__(128) k_barrier(int np, const int4* __restrict__ pairs, const double* __restrict__ x,
+                                                 const double* __restrict__ rest, double dhat, double kappa,
+                                                 double* __restrict__ fb, BlockSink bs, int base) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    int v[4], nvp;
+    int kind = decode_pair(pairs[p], v, nvp);
+    if (!ids_ok(bs, v, nvp)) {
+        emit_pair_blocks(bs, base + 10 * p, 0, v, [&](int, int, double H[3][3]) {});
+        return;
+    }
+    d3 X[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) X[a] = a < nvp ? ld3(x, v[a]) : mk(0, 0, 0);
+    d3 gd2[4];
+    double d2 = dist2_grad(kind, X, gd2);
+    const double sdh = sqrt(dhat), dist = sqrt(d2);
+    const double I = d2 / dhat, f = sqrt(I);
+    d3 gf[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) gf[a] = (1.0 / (2.0 * dist * sdh)) * gd2[a];
+    if (kind <= 3) {
+        double B, dB, d2B;
+        barrier_s(I, kappa * dhat * dhat, B, dB, d2B);
+        double dBdf = 2.0 * f * dB;
+        double Ic = d2 < 1e-6 * dhat ? 1e-6 : I;  // gassThreshold clamp (GIPC.cu:3258-3272)
+        double Bc, dBc, d2Bc;
+        barrier_s(Ic, kappa * dhat * dhat, Bc, dBc, d2Bc);
+        double lam0 = 4.0 * Ic * d2Bc + 2.0 * dBc;
+        for (int a = 0; a < nvp; a++) add_grad(fb, v[a], dBdf * gf[a]);
+        emit_pair_blocks(bs, base + 10 * p, nvp, v, [&](int a, int b, double H[3][3]) {
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) H[i][j] = lam0 * comp(gf[a], i) * comp(gf[b], j);
+        });
+        return;
+    }
+    // mollified pairs: b = kappa e(c^2) Bt(I), c = |edge0 x edge1|
+    int ea0, ea1, eb0, eb1;
+    if (kind == 4) { ea0 = 0; ea1 = 1; eb0 = 2; eb1 = 3; }
+    else if (kind == 6) { ea0 = 0; ea1 = 2; eb0 = 1; eb1 = 3; }
+    else { ea0 = 0; ea1 = 3; eb0 = 1; eb1 = 2; }
+    d3 u = X[ea1] - X[ea0], w = X[eb1] - X[eb0];
+    d3 n = cross(u, w);
+    double I1 = sq(n);
+    if (I1 == 0.0) {
+        emit_pair_blocks(bs, base + 10 * p, 0, v, [&](int, int, double H[3][3]) {});
+        return;
+    }
+    double c = sqrt(I1);
+    d3 gc[4];
+    {
+        d3 wn = cross(w, n), nu = cross(n, u);
+        double k = 1.0 / (2.0 * c);
+        gc[ea0] = (-2.0 * k) * wn;
+        gc[ea1] = (2.0 * k) * wn;
+        gc[eb0] = (-2.0 * k) * nu;
+        gc[eb1] = (2.0 * k) * nu;
+    }
+    d3 r0 = ld3(rest, v[ea0]), r1 = ld3(rest, v[ea1]), r2 = ld3(rest, v[eb0]), r3 = ld3(rest, v[eb1]);
+    double ex = 1e-3 * sq(r0 - r1) * sq(r2 - r3);  // _compute_epx, mlbvh.cu:264
+    double em = -I1 * I1 / (ex * ex) + 2.0 * I1 / ex;
+    double dem = -2.0 * I1 / (ex * ex) + 2.0 / ex;
+    double B, dB, d2B;
+    barrier_s(I, dhat * dhat, B, dB, d2B);
+    double dbdc = kappa * dem * 2.0 * c * B, dbdf = kappa * em * dB * 2.0 * f;
+    for (int a = 0; a < 4; a++) add_grad(fb, v[a], dbdc * gc[a] + dbdf * gf[a]);
+    double M00 = kappa * B * (-4.0 * (3.0 * I1 - ex) / (ex * ex));
+    double M11 = kappa * em * (4.0 * I * d2B + 2.0 * dB);
+    double M01 = kappa * dem * 2.0 * c * dB * 2.0 * f;
+    make_pd2(M00, M01, M11);
+    emit_pair_blocks(bs, base + 10 * p, 4, v, [&](int a, int b, double H[3][3]) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                H[i][j] = M00 * comp(gc[a], i) * comp(gc[b], j) +
+                          M01 * (comp(gc[a], i) * comp(gf[b], j) + comp(gf[a], i) * comp(gc[b], j)) +
+                          M11 * comp(gf[a], i) * comp(gf[b], j);
+    });
+}
+
+// friction pairs (FrictionUtils.cuh, GIPC.cu:1439-1800 and 5087-5270), C1 static clamping
+__global__ void __launch_bounds__(128) k_friction(int np, const int4* __restrict__ pairs, const double* __restrict__ x,
+                                                  const double* __restrict__ x0, const double* __restrict__ lam,
+                                                  const double* __restrict__ coord, const double* __restrict__ basis,
+                                                  double mu, double eps2, double* __restrict__ fb, BlockSink bs,
+                                                  int base) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    int4 e = pairs[p];
+    int v[4] = {0, 0, 0, 0}, nvp = 0;
+    double cf[4] = {0, 0, 0, 0};
+    double g1 = coord[2 * p], g2 = coord[2 * p + 1];
+    if (e.x >= 0) {
+        if (e.w >= 0) {
+            v[0] = e.x; v[1] = e.y; v[2] = e.z; v[3] = e.w; nvp = 4;
+            cf[0] = 1.0 - g1; cf[1] = g1; cf[2] = g2 - 1.0; cf[3] = -g2;
+        }
+    } else if (e.y >= 0) {
+        v[0] = -e.x - 1;
+        if (e.z < 0) { v[1] = e.y; nvp = 2; cf[0] = 1.0; cf[1] = -1.0; }
+        else if (e.w < 0) { v[1] = e.y; v[2] = e.z; nvp = 3; cf[0] = 1.0; cf[1] = g1 - 1.0; cf[2] = -g1; }
+        else { v[1] = e.y; v[2] = e.z; v[3] = e.w; nvp = 4; cf[0] = 1.0; cf[1] = -1.0 + g1 + g2; cf[2] = -g1; cf[3] = -g2; }
+    }
+    if (nvp == 0 || !ids_ok(bs, v, nvp)) {
+        emit_pair_blocks(bs, base + 10 * p, 0, v, [&](int, int, double H[3][3]) {});
+        return;
+    }
+    const double* Tb = basis + 6 * (size_t)p;  // 3x2 row-major
+    d3 t0 = mk(Tb[0], Tb[2], Tb[4]), t1 = mk(Tb[1], Tb[3], Tb[5]);
+    d3 rel = mk(0, 0, 0);
+    for (int a = 0; a < nvp; a++) rel = rel + cf[a] * (ld3(x, v[a]) - ld3(x0, v[a]));
+    double u0 = dot(t0, rel), u1 = dot(t1, rel);
+    double un2 = u0 * u0 + u1 * u1, un = sqrt(un2), eps = sqrt(eps2);
+    double f1d, M00, M01, M11;
+    if (un2 > eps2) {
+        f1d = 1.0 / un;
+        double k = 1.0 / (un2 * un);
+        M00 = f1d - k * u0 * u0; M01 = -k * u0 * u1; M11 = f1d - k * u1 * u1;
+    } else {
+        f1d = (-un + 2.0 * eps) / (eps * eps);
+        double f2 = 2.0 * (eps - un) / (eps * eps);
+        if (f2 != f1d && un2 != 0.0) {
+            double k = (f1d - f2) / un2;
+            M00 = f1d - k * u0 * u0; M01 = -k * u0 * u1; M11 = f1d - k * u1 * u1;
+        } else {
+            M00 = M11 = f1d; M01 = 0.0;
+        }
+    }
+    make_pd2(M00, M01, M11);
+    const double s = mu * lam[p];
+    d3 gt = (s * f1d) * (u0 * t0 + u1 * t1);
+    for (int a = 0; a < nvp; a++) add_grad(fb, v[a], cf[a] * gt);
+    // W = basis M basis^T
+    double W[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double ti0 = comp(t0, i), ti1 = comp(t1, i), tj0 = comp(t0, j), tj1 = comp(t1, j);
+            W[i][j] = s * (ti0 * (M00 * tj0 + M01 * tj1) + ti1 * (M01 * tj0 + M11 * tj1));
+        }
+    emit_pair_blocks(bs, base + 10 * p, nvp, v, [&](int a, int b, double H[3][3]) {
+        double k = cf[a] * cf[b];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) H[i][j] = k * W[i][j];
+    });
+}
+
+// ground barrier (GIPC.cu:6463-6514), plane y = offset
+__global__ void k_ground(int ng, const uint32_t* __restrict__ gp, const double* __restrict__ x, double offset,
+                         double dhat, double kappa, double* __restrict__ fb, BlockSink bs, int base) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ng) return;
+    int v = gp[p];
+    if (!ids_ok(bs, &v, 1)) {
+        bs.idx[base + p] = base + p;
+        bs.key[base + p] = kBadKey;
+        return;
+    }
+    double dist = x[3 * v + 1] - offset, d2 = dist * dist, t = d2 - dhat;
+    double gb = t * log(d2 / dhat) * -2.0 - (t * t) / d2;
+    double hb = (log(d2 / dhat) * -2.0 - t * 4.0 / d2) + 1.0 / (d2 * d2) * (t * t);
+    atomicAdd(fb + 3 * v + 1, kappa * gb * 2.0 * dist);
+    double H[3][3] = {{0, 0, 0}, {0, kappa * (4.0 * hb * d2 + 2.0 * gb), 0}, {0, 0, 0}};
+    emit_diag_block(bs, base + p, v, H);
+}
+
+// ground friction (GIPC.cu:1357-1437, 5047-5085), normal +y
+__global__ void k_fric_ground(int ng, const uint32_t* __restrict__ gp, const double* __restrict__ x,
+                              const double* __restrict__ x0, const double* __restrict__ lam, double mu, double eps2,
+                              double* __restrict__ fb, BlockSink bs, int base) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ng) return;
+    int v = gp[p];
+    if (!ids_ok(bs, &v, 1)) {
+        bs.idx[base + p] = base + p;
+        bs.key[base + p] = kBadKey;
+        return;
+    }
+    double vx = x[3 * v] - x0[3 * v], vz = x[3 * v + 2] - x0[3 * v + 2];
+    double m2 = vx * vx + vz * vz, s = mu * lam[p], eps = sqrt(eps2);
+    double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (m2 > eps2) {
+        double m = sqrt(m2), k = s / (m2 * m);
+        atomicAdd(fb + 3 * v, s * vx / m);
+        atomicAdd(fb + 3 * v + 2, s * vz / m);
+        double a = s / m - k * vx * vx, b = -k * vx * vz, c = s / m - k * vz * vz;
+        make_pd2(a, b, c);
+        H[0][0] = a; H[0][2] = b; H[2][0] = b; H[2][2] = c;
+    } else {
+        atomicAdd(fb + 3 * v, s * vx / eps);
+        atomicAdd(fb + 3 * v + 2, s * vz / eps);
+        H[0][0] = s / eps;
+        H[2][2] = s / eps;
+    }
+    emit_diag_block(bs, base + p, v, H);
+}
+
+// soft constraints (GIPC.cu:6363-6407)
+__global__ void k_soft(int ns, const uint32_t* __restrict__ idx, const double* __restrict__ x,
+                       const double* __restrict__ target, double k, double* __restrict__ sg, BlockSink bs, int base) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ns) return;
+    int v = idx[p];
+    for (int q = 0; q < 3; q++) atomicAdd(sg + 3 * v + q, k * (x[3 * v + q] - target[3 * p + q]));
+    double H[3][3] = {{k, 0, 0}, {0, k, 0}, {0, 0, k}};
+    emit_diag_block(bs, base + p, v, H);
+}
+
+// ---- contact block merge ------------------------------------------------------------------
+__global__ void k_head_flags(int m, const unsigned long long* __restrict__ ks, int* __restrict__ flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > m) return;
+    if (i == m) { flag[i] = 0; return; }
+    unsigned long long k = ks[i];
+    flag[i] = (k != kBadKey && (i == 0 || ks[i - 1] != k)) ? 1 : 0;
+}
+
+__global__ void k_reduce_unique(int m, const unsigned long long* __restrict__ ks, const int* __restrict__ is,
+                                const int* __restrict__ uid, const double* __restrict__ cval, int bits,
+                                int* __restrict__ uc_row, int* __restrict__ uc_col, double* __restrict__ u64,
+                                float* __restrict__ u32, int* __restrict__ nuc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) nuc[0] = uid[m];
+    if (i >= m) return;
+    unsigned long long k = ks[i];
+    if (k == kBadKey || (i > 0 && ks[i - 1] == k)) return;
+    int u = uid[i];
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = i; j < m && ks[j] == k; j++) {
+        const double* v = cval + 9 * (size_t)is[j];
+#pragma unroll
+        for (int q = 0; q < 9; q++) acc[q] += v[q];
+    }
+    unsigned long long mask = (1ull << bits) - 1ull;
+    uc_row[u] = (int)(k >> bits);
+    uc_col[u] = (int)(k & mask);
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        u64[9 * (size_t)u + q] = acc[q];
+        u32[9 * (size_t)u + q] = (float)acc[q];
+    }
+}
+
+__global__ void k_lower_keys(int m, const int* __restrict__ nuc, const int* __restrict__ uc_row,
+                             const int* __restrict__ uc_col, int bits, unsigned long long* __restrict__ lk,
+                             int* __restrict__ li) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= m) return;
+    li[u] = u;
+    if (u < nuc[0] && uc_row[u] != uc_col[u])
+        lk[u] = ((unsigned long long)uc_col[u] << bits) | (unsigned long long)uc_row[u];
+    else
+        lk[u] = kBadKey;
+}
+
+// row pointers: first index whose row field >= i (binary search over sorted keys / rows)
+__global__ void k_row_ptr_rows(int n, const int* __restrict__ nuc, const int* __restrict__ rows, int* __restrict__ ptr) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    int lo = 0, hi = nuc[0];
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (rows[mid] < i) lo = mid + 1; else hi = mid;
+    }
+    ptr[i] = lo;
+}
+
+__global__ void k_row_ptr_keys(int n, int m, const unsigned long long* __restrict__ ks, int bits, int* __restrict__ ptr) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    unsigned long long target = (unsigned long long)i << bits;
+    int lo = 0, hi = m;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (ks[mid] < target) lo = mid + 1; else hi = mid;
+    }
+    ptr[i] = lo;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+static SgipcStatus check_inputs(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k, const SgipcParams* p) {
+    if (!c || !f || !p) return SGIPC_BAD_INPUT;
+    if (!f->vertexes || !f->xTilta || !f->masses || !f->BoundaryType) return SGIPC_BAD_INPUT;
+    if (c->nt && (!f->DmInverses || !f->volum || !f->lengthRate || !f->volumeRate)) return SGIPC_BAD_INPUT;
+    if (c->nsoft && !f->targetVert) return SGIPC_BAD_INPUT;
+    if (!(p->dt > 0.0) || !(p->dHat > 0.0) || !(p->kappa >= 0.0)) return SGIPC_BAD_INPUT;
+    if (k) {
+        if (k->pair_num < 0 || k->ground_num < 0 || k->fric_num < 0 || k->fric_gd_num < 0) return SGIPC_BAD_INPUT;
+        if (k->pair_num > c->max_pairs || k->ground_num > c->max_ground || k->fric_num > c->max_fric ||
+            k->fric_gd_num > c->max_fric_gd) {
+            snprintf(c->err, sizeof(c->err), "contact counts exceed the context capacity");
+            return SGIPC_CAPACITY;
+        }
+        if ((k->pair_num && (!k->pairs || !f->rest_vertexes)) || (k->ground_num && !k->ground_pairs) ||
+            (k->fric_num && (!k->fric_pairs || !k->fric_lambda || !k->fric_coord || !k->fric_basis || !f->o_vertexes)) ||
+            (k->fric_gd_num && (!k->fric_gd_pairs || !k->fric_gd_lambda || !f->o_vertexes)))
+            return SGIPC_BAD_INPUT;
+    }
+    return SGIPC_OK;
+}
+
+static BlockSink sink(SgipcCtx* c, const SgipcFemData* f) {
+    BlockSink bs;
+    bs.key = c->ckey;
+    bs.idx = c->cidx;
+    bs.val = c->cval;
+    bs.btype = f->BoundaryType;
+    bs.bits = c->key_bits;
+    bs.nv = c->nv;
+    bs.flag = c->dflag;
+    return bs;
+}
+
+// launch the contact kernels; returns the number of contact block slots used
+static int launch_contacts(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k, const SgipcParams* p,
+                           double* grad, cudaStream_t s) {
+    BlockSink bs = sink(c, f);
+    int base = 0;
+    if (k && k->pair_num > 0) {
+        k_barrier<<<nblk(k->pair_num, 128), 128, 0, s>>>(k->pair_num, (const int4*)k->pairs, f->vertexes,
+                                                          f->rest_vertexes, p->dHat, p->kappa, grad, bs, base);
+        base += 10 * k->pair_num;
+    }
+    const double eps2 = p->fDhat * p->dt * p->dt;
+    if (k && k->fric_num > 0 && p->frictionRate > 0.0) {
+        k_friction<<<nblk(k->fric_num, 128), 128, 0, s>>>(k->fric_num, (const int4*)k->fric_pairs, f->vertexes,
+                                                           f->o_vertexes, k->fric_lambda, k->fric_coord, k->fric_basis,
+                                                           p->frictionRate, eps2, grad, bs, base);
+        base += 10 * k->fric_num;
+    }
+    if (k && k->ground_num > 0) {
+        k_ground<<<nblk(k->ground_num), SGIPC_BLOCK, 0, s>>>(k->ground_num, k->ground_pairs, f->vertexes,
+                                                              p->ground_offset, p->dHat, p->kappa, grad, bs, base);
+        base += k->ground_num;
+    }
+    if (k && k->fric_gd_num > 0 && p->gd_frictionRate > 0.0) {
+        k_fric_ground<<<nblk(k->fric_gd_num), SGIPC_BLOCK, 0, s>>>(k->fric_gd_num, k->fric_gd_pairs, f->vertexes,
+                                                                    f->o_vertexes, k->fric_gd_lambda,
+                                                                    p->gd_frictionRate, eps2, grad, bs, base);
+        base += k->fric_gd_num;
+    }
+    return base;
+}
+
+static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
+    if (m == 0) {
+        SG_CHECK(c, cudaMemsetAsync(c->nuc, 0, sizeof(int), s));
+        SG_CHECK(c, cudaMemsetAsync(c->cu_ptr, 0, sizeof(int) * (c->n + 1), s));
+        SG_CHECK(c, cudaMemsetAsync(c->cl_ptr, 0, sizeof(int) * (c->n + 1), s));
+        return SGIPC_OK;
+    }
+    const int endbit = 2 * c->key_bits;
+    size_t tb = c->cub_tmp_bytes;
+    SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->ckey, c->ckey_s, c->cidx, c->cidx_s, m, 0, endbit, s));
+    k_head_flags<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cflag);
+    tb = c->cub_tmp_bytes;
+    SG_CHECK(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp, tb, c->cflag, c->cflag, m + 1, s));
+    k_reduce_unique<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cidx_s, c->cflag, c->cval, c->key_bits, c->uc_row,
+                                                    c->uc_col, c->uc64, c->uc32, c->nuc);
+    k_row_ptr_rows<<<nblk(c->n + 1), SGIPC_BLOCK, 0, s>>>(c->n, c->nuc, c->uc_row, c->cu_ptr);
+    k_lower_keys<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->nuc, c->uc_row, c->uc_col, c->key_bits, c->lkey, c->lidx);
+    tb = c->cub_tmp_bytes;
+    SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->lkey, c->lkey_s, c->lidx, c->cl_idx, m, 0, endbit, s));
+    k_row_ptr_keys<<<nblk(c->n + 1), SGIPC_BLOCK, 0, s>>>(c->n, m, c->lkey_s, c->key_bits, c->cl_ptr);
+    SG_LAUNCH_CHECK(c, "contact merge");
+    return SGIPC_OK;
+}
+
+static SgipcStatus launch_fem(SgipcCtx* c, const SgipcFemData* f, const SgipcParams* p, cudaStream_t s) {
+    if (c->nt > 0) {
+        k_snk<<<nblk(c->nt, 128), 128, 0, s>>>(c->nt, c->tets, f->vertexes, f->DmInverses, f->volum, f->lengthRate,
+                                               f->volumeRate, p->dt * p->dt, c->eblk, c->egrad);
+    }
+    SG_LAUNCH_CHECK(c, "fem element kernels");
+    return SGIPC_OK;
+}
+
+static SgipcStatus gather_static(SgipcCtx* c, const SgipcFemData* f, cudaStream_t s) {
+    k_gather_blocks<<<nblk(9LL * c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->contrib_ptr, c->contrib, c->eblk, c->slot_row,
+                                                                c->col, f->BoundaryType, f->masses, c->val64, c->val32);
+    if (c->n_egrad > 0)
+        k_gather_grad<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, c->vinc_ptr, c->vinc, c->egrad, c->shape_grads);
+    SG_LAUNCH_CHECK(c, "static gather");
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k,
+                                      const SgipcParams* p, void* stream) {
+    SgipcStatus st = check_inputs(c, f, k, p);
+    if (st != SGIPC_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    SG_CHECK(c, cudaSetDevice(c->device));
+    c->btype = f->BoundaryType;
+    k_kinetic<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, f->vertexes, f->xTilta, f->masses, c->shape_grads, c->fb);
+    int m = launch_contacts(c, f, k, p, c->fb, s);
+    if (c->nsoft > 0) {
+        BlockSink bs = sink(c, f);
+        k_soft<<<nblk(c->nsoft), SGIPC_BLOCK, 0, s>>>(c->nsoft, c->soft_idx, f->vertexes, f->targetVert,
+                                                      p->motionRate * p->softRate * p->softRate, c->shape_grads, bs, m);
+        m += c->nsoft;
+    }
+    SG_LAUNCH_CHECK(c, "contact kernels");
+    if ((st = launch_fem(c, f, p, s)) != SGIPC_OK) return st;
+    if ((st = gather_static(c, f, s)) != SGIPC_OK) return st;
+    if ((st = merge_contacts(c, m, s)) != SGIPC_OK) return st;
+    k_rhs<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, c->fb, c->shape_grads, f->BoundaryType, c->b);
+    SG_LAUNCH_CHECK(c, "rhs");
+    c->assembled = 1;
+    c->mas.built = 0;
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_barrier_grad_hess(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k,
+                                               const SgipcParams* p, double* grad, void* stream) {
+    SgipcStatus st = check_inputs(c, f, k, p);
+    if (st != SGIPC_OK) return st;
+    if (!grad || !k) return SGIPC_BAD_INPUT;
+    cudaStream_t s = (cudaStream_t)stream;
+    SgipcContacts only = *k;
+    only.fric_num = 0;
+    only.ground_num = 0;
+    only.fric_gd_num = 0;
+    int m = launch_contacts(c, f, &only, p, grad, s);
+    SG_LAUNCH_CHECK(c, "barrier");
+    return merge_contacts(c, m, s);
+}
+
+extern "C" SgipcStatus sgipc_friction_grad_hess(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k,
+                                                const SgipcParams* p, double* grad, void* stream) {
+    SgipcStatus st = check_inputs(c, f, k, p);
+    if (st != SGIPC_OK) return st;
+    if (!grad || !k) return SGIPC_BAD_INPUT;
+    cudaStream_t s = (cudaStream_t)stream;
+    SgipcContacts only = *k;
+    only.pair_num = 0;
+    only.ground_num = 0;
+    int m = launch_contacts(c, f, &only, p, grad, s);
+    SG_LAUNCH_CHECK(c, "friction");
+    return merge_contacts(c, m, s);
+}
+
+extern "C" SgipcStatus sgipc_fem_grad_hess(SgipcCtx* c, const SgipcFemData* f, const SgipcParams* p, double* grad,
+                                           void* stream) {
+    SgipcStatus st = check_inputs(c, f, nullptr, p);
+    if (st != SGIPC_OK) return st;
+    if (!grad) return SGIPC_BAD_INPUT;
+    cudaStream_t s = (cudaStream_t)stream;
+    if ((st = launch_fem(c, f, p, s)) != SGIPC_OK) return st;
+    if ((st = gather_static(c, f, s)) != SGIPC_OK) return st;
+    // gather_static added the element gradient into shape_grads; hand it to the caller
+    if (c->n_egrad > 0)
+        k_gather_grad<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, c->vinc_ptr, c->vinc, c->egrad, grad);
+    SG_LAUNCH_CHECK(c, "fem gradient");
+    return SGIPC_OK;
+}

@@ -1,0 +1,342 @@
+// sgipc_ctx.cu — context creation: the static symmetric-upper BSR pattern, element ->
+// slot gather lists and every workspace.
+//
+// Replaces, at init time, what StiffGIPC re-derives every Newton iteration: the triplet
+// buffers sized in GIPC::init (GIPC.cu:8593-8640) and the per-iteration radix sort /
+// segmented reduce of Converter::convert (linear_system/utils/converter.cu:23-196).  The
+// FEM connectivity never changes, so its block pattern is computed once here; element
+// kernels then write straight into per-element block slots that a gather sums into the
+// BSR values, deterministically and without atomics.
+#include <algorithm>
+#include <cub/cub.cuh>
+#include <numeric>
+#include <vector>
+
+#include "sgipc_internal.cuh"
+
+using namespace sgipc;
+
+namespace {
+
+template <class T>
+SgipcStatus dalloc(SgipcCtx* c, T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc");
+    return SGIPC_OK;
+}
+
+template <class T>
+SgipcStatus upload(SgipcCtx* c, T** p, const std::vector<T>& h) {
+    SgipcStatus s = dalloc(c, p, h.size());
+    if (s != SGIPC_OK) return s;
+    if (!h.empty()) SG_CHECK(c, cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return SGIPC_OK;
+}
+
+#define SG_TRY(x)                          \
+    do {                                   \
+        SgipcStatus s_ = (x);              \
+        if (s_ != SGIPC_OK) return s_;     \
+    } while (0)
+
+// local upper block pairs of a 4-vertex element, in the reference's write order
+// (femEnergy.cu:1840-1856)
+const int kPair4[10][2] = {{0, 0}, {0, 1}, {0, 2}, {0, 3}, {1, 1}, {1, 2}, {1, 3}, {2, 2}, {2, 3}, {3, 3}};
+const int kPair3[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+
+}  // namespace
+
+static SgipcStatus build_static(SgipcCtx* c, const SgipcTopology* t) {
+    const int nv = t->vertex_num;
+    // element block keys: tets (10), triangles (6), hinges (10)
+    std::vector<std::pair<int, int>> eb;  // (min, max) per element block, in element order
+    eb.reserve((size_t)t->tet_num * 10 + (size_t)t->tri_num * 6 + (size_t)t->tri_edge_num * 10);
+    std::vector<int> egv;                 // vertex of each element gradient row
+    egv.reserve((size_t)t->tet_num * 4 + (size_t)t->tri_num * 3 + (size_t)t->tri_edge_num * 4);
+    for (int e = 0; e < t->tet_num; e++) {
+        const uint32_t* v = t->tetrahedras + 4 * e;
+        for (int k = 0; k < 10; k++) {
+            int a = v[kPair4[k][0]], b = v[kPair4[k][1]];
+            eb.push_back({std::min(a, b), std::max(a, b)});
+        }
+        for (int a = 0; a < 4; a++) egv.push_back(v[a]);
+    }
+    for (int e = 0; e < t->tri_num; e++) {
+        const uint32_t* v = t->triangles + 3 * e;
+        for (int k = 0; k < 6; k++) {
+            int a = v[kPair3[k][0]], b = v[kPair3[k][1]];
+            eb.push_back({std::min(a, b), std::max(a, b)});
+        }
+        for (int a = 0; a < 3; a++) egv.push_back(v[a]);
+    }
+    for (int e = 0; e < t->tri_edge_num; e++) {
+        int v[4] = {(int)t->tri_edges[2 * e], (int)t->tri_edges[2 * e + 1], t->tri_edge_adj_vertex[2 * e],
+                    t->tri_edge_adj_vertex[2 * e + 1]};
+        bool boundary = v[2] < 0 || v[3] < 0;
+        for (int k = 0; k < 10; k++) {
+            int a = v[kPair4[k][0]], b = v[kPair4[k][1]];
+            if (boundary) a = b = v[0];  // boundary hinges contribute zero blocks (femEnergy.cu:2640-2660)
+            eb.push_back({std::min(a, b), std::max(a, b)});
+        }
+        for (int a = 0; a < 4; a++) egv.push_back(boundary ? v[0] : v[a]);
+    }
+    for (auto& p : eb)
+        if (p.first < 0 || p.second >= nv) {
+            snprintf(c->err, sizeof(c->err), "element vertex index out of range");
+            return SGIPC_BAD_INPUT;
+        }
+    // pattern: element blocks + the full diagonal (mass)
+    std::vector<uint64_t> keys;
+    keys.reserve(eb.size() + nv);
+    for (auto& p : eb) keys.push_back(((uint64_t)p.first << 32) | (uint32_t)p.second);
+    for (int i = 0; i < nv; i++) keys.push_back(((uint64_t)i << 32) | (uint32_t)i);
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    const int n = c->n, nnz = (int)keys.size();
+    c->nnz = nnz;
+    std::vector<int> row_ptr(n + 1, 0), col(nnz), slot_row(nnz), diag(n, -1);
+    for (int s = 0; s < nnz; s++) {
+        int r = (int)(keys[s] >> 32), cc = (int)(keys[s] & 0xffffffffu);
+        row_ptr[r + 1]++;
+        col[s] = cc;
+        slot_row[s] = r;
+        if (r == cc) diag[r] = s;
+    }
+    for (int i = 0; i < n; i++) row_ptr[i + 1] += row_ptr[i];
+    // lower lists: slot (r, c) with r < c appears transposed in row c
+    std::vector<int> low_ptr(n + 1, 0);
+    for (int s = 0; s < nnz; s++)
+        if (slot_row[s] != col[s]) low_ptr[col[s] + 1]++;
+    for (int i = 0; i < n; i++) low_ptr[i + 1] += low_ptr[i];
+    std::vector<int> low_slot(std::max(low_ptr[n], 1)), fill(low_ptr.begin(), low_ptr.end() - 1);
+    for (int s = 0; s < nnz; s++)
+        if (slot_row[s] != col[s]) low_slot[fill[col[s]]++] = s;
+    // element block -> slot, then gather CSR by slot
+    c->n_eblk = (int)eb.size();
+    std::vector<int> eslot(eb.size());
+    for (size_t e = 0; e < eb.size(); e++) {
+        uint64_t k = ((uint64_t)eb[e].first << 32) | (uint32_t)eb[e].second;
+        eslot[e] = (int)(std::lower_bound(keys.begin(), keys.end(), k) - keys.begin());
+    }
+    std::vector<int> cptr(nnz + 1, 0);
+    for (int s : eslot) cptr[s + 1]++;
+    for (int s = 0; s < nnz; s++) cptr[s + 1] += cptr[s];
+    std::vector<int> contrib(std::max((size_t)1, eb.size())), cf(cptr.begin(), cptr.end() - 1);
+    for (size_t e = 0; e < eb.size(); e++) contrib[cf[eslot[e]]++] = (int)e;
+    // element gradient rows -> vertex gather CSR
+    c->n_egrad = (int)egv.size();
+    std::vector<int> vptr(nv + 1, 0);
+    for (int v : egv) vptr[v + 1]++;
+    for (int i = 0; i < nv; i++) vptr[i + 1] += vptr[i];
+    std::vector<int> vinc(std::max((size_t)1, egv.size())), vf(vptr.begin(), vptr.end() - 1);
+    for (size_t e = 0; e < egv.size(); e++) vinc[vf[egv[e]]++] = (int)e;
+
+    SG_TRY(upload(c, &c->row_ptr, row_ptr));
+    SG_TRY(upload(c, &c->col, col));
+    SG_TRY(upload(c, &c->slot_row, slot_row));
+    SG_TRY(upload(c, &c->diag_slot, diag));
+    SG_TRY(upload(c, &c->low_ptr, low_ptr));
+    SG_TRY(upload(c, &c->low_slot, low_slot));
+    SG_TRY(upload(c, &c->contrib_ptr, cptr));
+    SG_TRY(upload(c, &c->contrib, contrib));
+    SG_TRY(upload(c, &c->vinc_ptr, vptr));
+    SG_TRY(upload(c, &c->vinc, vinc));
+    SG_TRY(dalloc(c, &c->val64, (size_t)nnz * 9));
+    SG_TRY(dalloc(c, &c->val32, (size_t)nnz * 9));
+    SG_TRY(dalloc(c, &c->eblk, (size_t)c->n_eblk * 9));
+    SG_TRY(dalloc(c, &c->egrad, (size_t)c->n_egrad * 3));
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx** out) {
+    if (!t || !out) return SGIPC_BAD_INPUT;
+    *out = nullptr;
+    if (t->vertex_num <= 0 || t->tet_num < 0 || t->tri_num < 0 || t->tri_edge_num < 0 || t->soft_num < 0 ||
+        t->max_pairs < 0 || t->max_ground < 0 || t->max_fric_pairs < 0 || t->max_fric_ground < 0)
+        return SGIPC_BAD_INPUT;
+    if ((t->tet_num && !t->tetrahedras) || (t->tri_num && !t->triangles) ||
+        (t->tri_edge_num && (!t->tri_edges || !t->tri_edge_adj_vertex)) || !t->partId_map_real ||
+        !t->real_map_partId || !t->neighborStart || (t->soft_num && !t->targetIndex))
+        return SGIPC_BAD_INPUT;
+    if (t->part_map_size < t->vertex_num || t->part_map_size % SGIPC_BANK) return SGIPC_BAD_INPUT;
+    SgipcCtx* c = new SgipcCtx();
+    memset(c, 0, sizeof(SgipcCtx));
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        return SGIPC_CUDA_ERROR;
+    }
+    c->nv = t->vertex_num;
+    c->nt = t->tet_num;
+    c->nf = t->tri_num;
+    c->nh = t->tri_edge_num;
+    c->nsoft = t->soft_num;
+    c->n = t->vertex_num;
+    c->max_pairs = t->max_pairs;
+    c->max_ground = t->max_ground;
+    c->max_fric = t->max_fric_pairs;
+    c->max_fric_gd = t->max_fric_ground;
+    c->max_rhs = t->max_rhs < 1 ? 1 : t->max_rhs;
+    SgipcStatus st = build_static(c, t);
+    auto fail = [&](SgipcStatus s) {
+        sgipc_destroy(c);
+        return s;
+    };
+    if (st != SGIPC_OK) return fail(st);
+    // topology copies
+    std::vector<uint32_t> tets(t->tetrahedras, t->tetrahedras + 4 * (size_t)t->tet_num);
+    std::vector<uint32_t> tris(t->triangles ? t->triangles : nullptr,
+                               t->triangles ? t->triangles + 3 * (size_t)t->tri_num : nullptr);
+    std::vector<uint32_t> hin(t->tri_edges ? t->tri_edges : nullptr,
+                              t->tri_edges ? t->tri_edges + 2 * (size_t)t->tri_edge_num : nullptr);
+    std::vector<int32_t> hadj(t->tri_edge_adj_vertex ? t->tri_edge_adj_vertex : nullptr,
+                              t->tri_edge_adj_vertex ? t->tri_edge_adj_vertex + 2 * (size_t)t->tri_edge_num : nullptr);
+    std::vector<uint32_t> soft(t->targetIndex ? t->targetIndex : nullptr,
+                               t->targetIndex ? t->targetIndex + t->soft_num : nullptr);
+    for (uint32_t s : soft)
+        if ((int)s >= c->nv) return fail(SGIPC_BAD_INPUT);
+    if ((st = upload(c, &c->tets, tets)) != SGIPC_OK) return fail(st);
+    if ((st = upload(c, &c->tris, tris)) != SGIPC_OK) return fail(st);
+    if ((st = upload(c, &c->hinges, hin)) != SGIPC_OK) return fail(st);
+    if ((st = upload(c, &c->hinge_adj, hadj)) != SGIPC_OK) return fail(st);
+    if ((st = upload(c, &c->soft_idx, soft)) != SGIPC_OK) return fail(st);
+    const int n = c->n;
+    if ((st = dalloc(c, &c->shape_grads, 3 * (size_t)c->nv)) != SGIPC_OK) return fail(st);
+    if ((st = dalloc(c, &c->fb, 3 * (size_t)c->nv)) != SGIPC_OK) return fail(st);
+    if ((st = dalloc(c, &c->b, 3 * (size_t)n)) != SGIPC_OK) return fail(st);
+    // contact block capacity: 10 upper blocks per barrier pair and per friction pair,
+    // one per ground barrier / ground friction / soft constraint
+    long long cap = 10LL * c->max_pairs + 10LL * c->max_fric + c->max_ground + c->max_fric_gd + c->nsoft + 1;
+    if (cap > (1LL << 30)) return fail(SGIPC_CAPACITY);
+    c->cap_cblk = (int)cap;
+    if ((st = dalloc(c, &c->ckey, cap)) || (st = dalloc(c, &c->ckey_s, cap)) || (st = dalloc(c, &c->cidx, cap)) ||
+        (st = dalloc(c, &c->cidx_s, cap)) || (st = dalloc(c, &c->cval, cap * 9)) ||
+        (st = dalloc(c, &c->cflag, cap + 1)) || (st = dalloc(c, &c->nuc, 4)) || (st = dalloc(c, &c->uc_row, cap)) ||
+        (st = dalloc(c, &c->uc_col, cap)) || (st = dalloc(c, &c->uc64, cap * 9)) ||
+        (st = dalloc(c, &c->uc32, cap * 9)) || (st = dalloc(c, &c->cu_ptr, n + 1)) ||
+        (st = dalloc(c, &c->cl_ptr, n + 1)) || (st = dalloc(c, &c->cl_idx, cap)) || (st = dalloc(c, &c->lkey, cap)) ||
+        (st = dalloc(c, &c->lkey_s, cap)) || (st = dalloc(c, &c->lidx, cap)) || (st = dalloc(c, &c->dflag, 4)))
+        return fail(st);
+    SG_CHECK(c, cudaMemset(c->dflag, 0, 4 * sizeof(int)));
+    // contact block keys are (row << bits) | col with row, col < 2^bits - 1, so that the
+    // all-ones key of an unused slot sorts after every real block
+    int bits = 1;
+    while ((1LL << bits) < (long long)n + 2) bits++;
+    c->key_bits = bits;
+    // CUB temporary storage: radix sort of cap pairs and an exclusive scan of cap ints
+    size_t b1 = 0, b2 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b1, c->ckey, c->ckey_s, c->cidx, c->cidx_s, (int)cap, 0, 64);
+    cub::DeviceScan::ExclusiveSum(nullptr, b2, c->cflag, c->cflag, (int)cap + 1);
+    c->cub_tmp_bytes = std::max(b1, b2) + 256;
+    if ((st = dalloc(c, (char**)&c->cub_tmp, c->cub_tmp_bytes)) != SGIPC_OK) return fail(st);
+    SG_CHECK(c, cudaMemset(c->nuc, 0, 4 * sizeof(int)));
+    if ((st = mas_create(c, t)) != SGIPC_OK) return fail(st);
+    if ((st = pcg_create(c)) != SGIPC_OK) return fail(st);
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail(cuda_fail(c, e, "cudaDeviceSynchronize"));
+    *out = c;
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
+    if (!c) return SGIPC_OK;
+    cudaSetDevice(c->device);
+    pcg_destroy(c);
+    mas_destroy(c);
+    void* ptrs[] = {c->row_ptr, c->col, c->slot_row, c->diag_slot, c->low_ptr, c->low_slot, c->val64, c->val32,
+                    c->eblk, c->contrib_ptr, c->contrib, c->egrad, c->vinc_ptr, c->vinc, c->tets, c->tris,
+                    c->hinges, c->hinge_adj, c->soft_idx, c->shape_grads, c->fb, c->b, c->ckey, c->ckey_s,
+                    c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,
+                    c->cu_ptr, c->cl_ptr, c->cl_idx, c->lkey, c->lkey_s, c->lidx, c->cub_tmp, c->dflag};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete c;
+    return SGIPC_OK;
+}
+
+extern "C" const char* sgipc_status_string(SgipcStatus s) {
+    switch (s) {
+        case SGIPC_OK: return "ok";
+        case SGIPC_CUDA_ERROR: return "cuda error";
+        case SGIPC_NOT_CONVERGED: return "not converged";
+        case SGIPC_BREAKDOWN: return "pcg breakdown";
+        case SGIPC_BAD_INPUT: return "bad input";
+        case SGIPC_CAPACITY: return "capacity exceeded";
+        case SGIPC_NOT_READY: return "not ready";
+    }
+    return "unknown";
+}
+
+extern "C" const char* sgipc_last_error(const SgipcCtx* c) { return c ? c->err : ""; }
+
+extern "C" SgipcStatus sgipc_get_rhs(SgipcCtx* c, double* b, void* stream) {
+    if (!c || !b) return SGIPC_BAD_INPUT;
+    if (!c->assembled) return SGIPC_NOT_READY;
+    SG_CHECK(c, cudaMemcpyAsync(b, c->b, 3 * sizeof(double) * c->n, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    return SGIPC_OK;
+}
+
+namespace sgipc {
+SgipcStatus check_device_flag(SgipcCtx* c, cudaStream_t s) {
+    int h = 0;
+    SG_CHECK(c, cudaMemcpyAsync(&h, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    if (h) {
+        SG_CHECK(c, cudaMemsetAsync(c->dflag, 0, sizeof(int), s));
+        snprintf(c->err, sizeof(c->err), "a contact pair names a vertex outside [0, vertex_num); it was skipped");
+        return SGIPC_BAD_INPUT;
+    }
+    return SGIPC_OK;
+}
+}  // namespace sgipc
+
+extern "C" SgipcStatus sgipc_export_bcoo(SgipcCtx* c, int32_t cap, int32_t* rows, int32_t* cols, double* vals,
+                                         int32_t* count) {
+    if (!c || !count) return SGIPC_BAD_INPUT;
+    if (!c->assembled) return SGIPC_NOT_READY;
+    SG_CHECK(c, cudaDeviceSynchronize());
+    {
+        SgipcStatus fs = check_device_flag(c, 0);
+        if (fs != SGIPC_OK) return fs;
+    }
+    int nuc = 0;
+    SG_CHECK(c, cudaMemcpy(&nuc, c->nuc, sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> sr(c->nnz), sc(c->nnz), ur(nuc), ucc(nuc);
+    std::vector<double> sv((size_t)c->nnz * 9), uv((size_t)nuc * 9);
+    SG_CHECK(c, cudaMemcpy(sr.data(), c->slot_row, sizeof(int) * c->nnz, cudaMemcpyDeviceToHost));
+    SG_CHECK(c, cudaMemcpy(sc.data(), c->col, sizeof(int) * c->nnz, cudaMemcpyDeviceToHost));
+    SG_CHECK(c, cudaMemcpy(sv.data(), c->val64, sizeof(double) * 9 * c->nnz, cudaMemcpyDeviceToHost));
+    if (nuc) {
+        SG_CHECK(c, cudaMemcpy(ur.data(), c->uc_row, sizeof(int) * nuc, cudaMemcpyDeviceToHost));
+        SG_CHECK(c, cudaMemcpy(ucc.data(), c->uc_col, sizeof(int) * nuc, cudaMemcpyDeviceToHost));
+        SG_CHECK(c, cudaMemcpy(uv.data(), c->uc64, sizeof(double) * 9 * nuc, cudaMemcpyDeviceToHost));
+    }
+    // merge the two sorted lists, summing equal keys
+    int i = 0, j = 0, k = 0;
+    auto key = [](int r, int cc) { return ((uint64_t)r << 32) | (uint32_t)cc; };
+    while (i < c->nnz || j < nuc) {
+        uint64_t ki = i < c->nnz ? key(sr[i], sc[i]) : ~0ull;
+        uint64_t kj = j < nuc ? key(ur[j], ucc[j]) : ~0ull;
+        uint64_t kk = std::min(ki, kj);
+        double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (ki == kk) {
+            for (int q = 0; q < 9; q++) acc[q] += sv[(size_t)9 * i + q];
+            i++;
+        }
+        if (kj == kk) {
+            for (int q = 0; q < 9; q++) acc[q] += uv[(size_t)9 * j + q];
+            j++;
+        }
+        if (rows && k < cap) {
+            rows[k] = (int)(kk >> 32);
+            cols[k] = (int)(kk & 0xffffffffu);
+            for (int q = 0; q < 9; q++) vals[(size_t)9 * k + q] = acc[q];
+        }
+        k++;
+    }
+    *count = k;
+    return (rows && k > cap) ? SGIPC_CAPACITY : SGIPC_OK;
+}

@@ -1,0 +1,193 @@
+// sgipc_internal.cuh — context layout shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/sgipc.h"
+#include "sgipc_math.cuh"
+
+#define SGIPC_BANK 16
+#define SGIPC_MAX_LEVELS 6
+#define SGIPC_BLOCK 256
+
+namespace sgipc {
+
+// Device-resident PCG scalars (no host round trip per iteration).
+struct PcgScalars {
+    double rz;        // r.z of the current iterate (reference: rz)
+    double rz_next;   // r.z after the latest preconditioner apply (rz_new)
+    double rz0;
+    double pAp;
+    double alpha;
+    double tol;
+    double bnorm2;    // ||b||^2 (true-residual criterion)
+    double rr;        // ||r||^2 of the current iterate
+    int32_t iter;     // SpMVs performed
+    int32_t max_iter;
+    int32_t state;    // 0 running, 1 stop after this update, 2 stopped
+    int32_t status;   // SgipcStatus
+    int32_t crit;     // SgipcCriterion
+    int32_t bodies;   // iteration bodies executed (hard bound on the graph's while loop)
+};
+
+// One precision's PCG workspace (T = double or float) for up to `nrhs` right-hand sides.
+struct PcgWork {
+    void* x;
+    void* r;
+    void* z;
+    void* p;
+    void* Ap;
+    PcgScalars* sc;          // [nrhs]
+    double* partial;         // reduction partials [nrhs][max_blocks]
+    unsigned int* ticket;    // last-block counters [nrhs * 4]
+    cudaGraphExec_t exec;    // captured iteration loop
+    bool cond_graph;         // true: while-node graph (whole loop in one launch)
+    long long captured_key;  // precision/rhs tag and domain count the graph was captured for
+};
+
+struct MasWork {
+    int npos;                // level-0 positions (padded to 16)
+    int levelnum;
+    int total_cap;           // cluster capacity = levelnum * npos
+    int* part_map;           // [npos] position -> vertex or -1
+    int* real_map;           // [nv]
+    int* nbr_ptr;            // [nv+1] mesh neighbour CSR
+    int* nbr;                // [nnz]
+    int* table;              // [nv * levelnum] global cluster per level (level 0 = position)
+    int* node;               // [nv] node id at the level being built
+    uint32_t* mask;          // [npos] bank-local connectivity
+    int* comp_rank;          // [npos] new local id of the component a node belongs to
+    int* bank_cnt;           // [npos/16 + 1]
+    int* bank_off;           // [npos/16 + 1]
+    int* info;               // device: [0..7] level starts, [8..15] level counts, [16] total
+    int h_info[17];          // host copy after build
+    double* dom64;           // [total_cap/16][48*48] FP64 domain matrices / inverses
+    float* dom32;            // [total_cap/16][48*48] FP32 inverses
+    double* R64;             // [total_cap*3]
+    double* Z64;
+    float* R32;
+    float* Z32;
+    void* scan_tmp;
+    size_t scan_tmp_bytes;
+    int built;               // 0 none, else SgipcPrecision+1 of the stored inverses
+};
+
+}  // namespace sgipc
+
+struct SgipcCtx {
+    int device;
+    int nv, nt, nf, nh, nsoft;
+    int n;                    // block rows
+    int max_pairs, max_ground, max_fric, max_fric_gd, max_rhs;
+    char err[512];
+
+    // ---- static symmetric-upper BSR ---------------------------------------------------
+    int nnz;                  // static blocks (upper incl. diagonal)
+    int* row_ptr;             // [n+1]
+    int* col;                 // [nnz]
+    int* slot_row;            // [nnz]
+    int* diag_slot;           // [n]
+    int* low_ptr;             // [n+1] lower (transposed) entries per row
+    int* low_slot;            // [nnz - n]
+    double* val64;            // [nnz*9]
+    float* val32;             // [nnz*9]
+    // element blocks and their gather lists
+    int n_eblk;               // 10 per tet, 6 per triangle, 10 per hinge
+    double* eblk;             // [n_eblk*9] oriented element blocks
+    int* contrib_ptr;         // [nnz+1]
+    int* contrib;             // [n_eblk] element block ids sorted by slot
+    int n_egrad;              // 4 per tet, 3 per triangle, 4 per hinge
+    double* egrad;            // [n_egrad*3]
+    int* vinc_ptr;            // [nv+1]
+    int* vinc;                // [n_egrad] element gradient rows per vertex
+    // topology
+    uint32_t* tets;           // [nt*4]
+    uint32_t* tris;           // [nf*3]
+    uint32_t* hinges;         // [nh*2]
+    int32_t* hinge_adj;       // [nh*2]
+    uint32_t* soft_idx;       // [nsoft]
+    // gradients and right-hand side
+    double* shape_grads;      // [3nv]
+    double* fb;               // [3nv]
+    double* b;                // [3n]
+    const int32_t* btype;     // last assembly's BoundaryType (caller-owned, device)
+
+    // ---- dynamic contact blocks -------------------------------------------------------
+    int cap_cblk;
+    unsigned long long* ckey;     // [cap]
+    unsigned long long* ckey_s;   // sorted
+    int* cidx;                    // [cap]
+    int* cidx_s;
+    double* cval;                 // [cap*9]
+    int* cflag;                   // [cap+1] segment heads -> unique ids
+    int* nuc;                     // device: number of unique contact blocks
+    int* uc_row;                  // [cap]
+    int* uc_col;
+    double* uc64;                 // [cap*9]
+    float* uc32;
+    int* cu_ptr;                  // [n+1] unique contact blocks by row (upper)
+    int* cl_ptr;                  // [n+1] transposed entries by row
+    int* cl_idx;                  // [cap]
+    unsigned long long* lkey;     // [cap]
+    unsigned long long* lkey_s;
+    int* lidx;
+    void* cub_tmp;
+    size_t cub_tmp_bytes;
+    int key_bits;
+    int assembled;
+    int* dflag;                   // device: input errors found by kernels (bit 0: pair index)
+
+    // ---- MAS and PCG ------------------------------------------------------------------
+    sgipc::MasWork mas;
+    sgipc::PcgWork pcg64;
+    sgipc::PcgWork pcg32;
+    double* tmp64;            // [3n * max_rhs] scratch vectors
+    double* tmp64b;
+    double* dot_partial;      // reduction scratch
+    unsigned int* dot_ticket;
+    double* dot_out;          // [16]
+    double* h_pinned;         // host pinned scalars
+    cudaStream_t cap_stream;  // capture stream
+    int max_blocks;           // reduction grid cap
+};
+
+namespace sgipc {
+
+inline SgipcStatus cuda_fail(SgipcCtx* c, cudaError_t e, const char* what) {
+    if (c) snprintf(c->err, sizeof(c->err), "%s: %s", what, cudaGetErrorString(e));
+    return SGIPC_CUDA_ERROR;
+}
+
+#define SG_CHECK(ctx, call)                                          \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return sgipc::cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+#define SG_LAUNCH_CHECK(ctx, name)                                   \
+    do {                                                             \
+        cudaError_t e_ = cudaGetLastError();                         \
+        if (e_ != cudaSuccess) return sgipc::cuda_fail(ctx, e_, name); \
+    } while (0)
+
+inline int nblk(long long n, int b = SGIPC_BLOCK) { return (int)((n + b - 1) / b); }
+
+// ---- cross-unit entry points ------------------------------------------------------------
+SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t);
+void mas_destroy(SgipcCtx* c);
+SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, cudaStream_t s);
+// z = M^-1 r for T in {double, float}; r, z are [3n] vectors of T (rz accumulated into
+// out_dot[0] when out_dot != nullptr, using r . z with r in T precision).
+template <class T>
+SgipcStatus mas_apply_t(SgipcCtx* c, const T* r, T* z, int fp32_inv, cudaStream_t s);
+SgipcStatus pcg_create(SgipcCtx* c);
+void pcg_destroy(SgipcCtx* c);
+template <class T>
+SgipcStatus spmv_t(SgipcCtx* c, const T* x, T* y, cudaStream_t s);
+SgipcStatus dot64(SgipcCtx* c, const double* a, const double* b, int n, double* out_dev, cudaStream_t s);
+// BAD_INPUT if a kernel flagged an invalid input since the last check (synchronises)
+SgipcStatus check_device_flag(SgipcCtx* c, cudaStream_t s);
+
+}  // namespace sgipc

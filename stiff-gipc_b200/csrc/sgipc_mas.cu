@@ -1,0 +1,451 @@
+// sgipc_mas.cu — multilevel additive Schwarz (MAS) preconditioner.
+//
+// Semantics of StiffGIPC's MASPreconditioner (MASPreconditioner.cu:29-2262):
+//   level 0   : the partition positions; a domain is a bank of 16 consecutive positions;
+//   level l+1 : the connected components, inside each level-l bank, of the graph made of
+//               mesh edges (StiffGIPC/load_mesh.cpp:934-1040) and of every vertex pair of
+//               every contact pair (_buildCollisionConnection_new, :1132); components are
+//               numbered bank by bank, by their lowest lane (_buildLevel1_new, _prefixSumLx);
+//   levels    : computeNumLevels (:1724-1743), at most 6;
+//   matrices  : the bank-diagonal 48x48 blocks of P_l^T A P_l over the FEM block rows
+//               (PrepareHessian_bcoo, :1816-2093), a zero diagonal entry replaced by 1 and
+//               inverted by Gauss-Jordan without pivoting (__inverse6_P96x96, :630-726);
+//   apply     : z = sum_l P_l A_l^-1 P_l^T r (__buildMultiLevelR_optimized_new,
+//               _schwarzLocalXSym6, __collectFinalZ_new, :729-1027).
+// The B200 version keeps every level's bookkeeping on the device (no per-level host
+// copy), builds the per-level masks with one thread per vertex / per contact pair and
+// resolves a bank's components with one thread per bank.
+#include <cub/cub.cuh>
+#include <vector>
+
+#include "sgipc_internal.cuh"
+
+using namespace sgipc;
+
+namespace {
+
+__device__ __forceinline__ void mask_edge(uint32_t* mask, int a, int b) {
+    if (a != b && (a >> 4) == (b >> 4)) atomicOr(mask + a, 1u << (b & 15));
+}
+
+__global__ void k_init_level0(int nv, const int* __restrict__ real_map, int L, int* __restrict__ node,
+                              int* __restrict__ table, int* __restrict__ info, int npos) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v == 0) {
+        info[0] = 0;     // start of level 0
+        info[8] = npos;  // count of level 0 (positions, padding included)
+    }
+    if (v >= nv) return;
+    int p = real_map[v];
+    node[v] = p;
+    table[(size_t)v * L] = p;
+}
+
+__global__ void k_mask_edges(int nv, const int* __restrict__ ptr, const int* __restrict__ nbr,
+                             const int* __restrict__ node, uint32_t* __restrict__ mask) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    int a = node[v];
+    for (int k = ptr[v]; k < ptr[v + 1]; k++) mask_edge(mask, a, node[nbr[k]]);
+}
+
+__global__ void k_mask_pairs(int np, const int4* __restrict__ pairs, int nv, const int* __restrict__ node,
+                             uint32_t* __restrict__ mask) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    int4 e = pairs[p];
+    int v[4], n = 0;
+    if (e.x >= 0) {
+        v[0] = e.x; v[1] = e.y; v[2] = e.z; v[3] = e.w < 0 ? -e.w - 1 : e.w; n = 4;
+    } else {
+        v[0] = -e.x - 1;
+        if (e.z < 0) {
+            if (e.y < 0) { v[1] = -e.y - 1; v[2] = -e.z - 1; v[3] = -e.w - 1; n = 4; }
+            else { v[1] = e.y; n = 2; }
+        } else if (e.w < 0) {
+            if (e.y < 0) { v[1] = -e.y - 1; v[2] = e.z; v[3] = -e.w - 1; n = 4; }
+            else { v[1] = e.y; v[2] = e.z; n = 3; }
+        } else { v[1] = e.y; v[2] = e.z; v[3] = e.w; n = 4; }
+    }
+    int a[4];
+    for (int i = 0; i < n; i++) a[i] = (v[i] >= 0 && v[i] < nv) ? node[v[i]] : -1;
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++)
+            if (a[i] >= 0 && a[j] >= 0) {
+                mask_edge(mask, a[i], a[j]);
+                mask_edge(mask, a[j], a[i]);
+            }
+}
+
+// One thread per bank: components by repeated OR closure, numbered by lowest lane.
+__global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, int level,
+                                  const uint32_t* __restrict__ mask, int* __restrict__ rank,
+                                  int* __restrict__ bank_cnt) {
+    int bk = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bk > nbank_cap) return;
+    const int count = info[8 + level];
+    const int nbank = (count + 15) >> 4;
+    if (bk >= nbank) {
+        bank_cnt[bk] = 0;
+        return;
+    }
+    const int lo = bk << 4, hi = min(count, lo + 16);
+    uint32_t comp[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) comp[i] = (lo + i < hi) ? (mask[lo + i] | (1u << i)) : (1u << i);
+    for (int it = 0; it < 16; it++) {
+        bool changed = false;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            uint32_t m = comp[i], acc = m;
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+                if (m & (1u << j)) acc |= comp[j];
+            if (acc != m) {
+                comp[i] = acc;
+                changed = true;
+            }
+        }
+        if (!changed) break;
+    }
+    // leaders: lowest lane of their component; rank = number of leaders below
+    uint32_t leaders = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+        if (lo + i < hi && (__ffs(comp[i]) - 1) == i) leaders |= 1u << i;
+    for (int i = 0; i < hi - lo; i++) {
+        int lead = __ffs(comp[i]) - 1;
+        rank[lo + i] = __popc(leaders & ((1u << lead) - 1u));
+    }
+    bank_cnt[bk] = __popc(leaders);
+}
+
+__global__ void k_assign(int nv, int L, int level, const int* __restrict__ bank_off, const int* __restrict__ rank,
+                         int* __restrict__ node, int* __restrict__ table, int* __restrict__ info) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int count = info[8 + level];
+    const int start_next = info[level] + ((count + 15) & ~15);
+    if (v == 0) {
+        int nbank = (count + 15) >> 4;
+        info[level + 1] = start_next;
+        info[8 + level + 1] = bank_off[nbank];
+        if (level + 2 == L) info[16] = start_next + ((bank_off[nbank] + 15) & ~15);
+    }
+    if (v >= nv) return;
+    int a = node[v];
+    int nn = bank_off[a >> 4] + rank[a];
+    node[v] = nn;
+    table[(size_t)v * L + level + 1] = start_next + nn;
+}
+
+// scatter one 3x3 block B at (r,c) (and B^T at (c,r)) into every level whose bank holds both
+__device__ __forceinline__ void scatter_block(double* dom, const int* __restrict__ table, int L, int r, int c,
+                                              const double* B) {
+    for (int l = 0; l < L; l++) {
+        int ga = table[(size_t)r * L + l], gb = table[(size_t)c * L + l];
+        if ((ga >> 4) != (gb >> 4)) continue;
+        double* D = dom + (size_t)(ga >> 4) * 2304;
+        int ra = 3 * (ga & 15), cb = 3 * (gb & 15);
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                double v = B[3 * i + j];
+                if (v == 0.0) continue;
+                atomicAdd(D + (ra + i) * 48 + cb + j, v);
+                if (r != c) atomicAdd(D + (cb + j) * 48 + ra + i, v);
+            }
+    }
+}
+
+__global__ void k_scatter_static(int nnz, const int* __restrict__ slot_row, const int* __restrict__ col,
+                                 const double* __restrict__ val, const int* __restrict__ table, int L,
+                                 double* __restrict__ dom) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nnz) return;
+    double B[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) B[q] = val[9 * (size_t)s + q];
+    scatter_block(dom, table, L, slot_row[s], col[s], B);
+}
+
+__global__ void k_scatter_contact(int cap, const int* __restrict__ nuc, const int* __restrict__ ur,
+                                  const int* __restrict__ uc, const double* __restrict__ val,
+                                  const int* __restrict__ table, int L, double* __restrict__ dom) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= cap || u >= nuc[0]) return;
+    double B[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) B[q] = val[9 * (size_t)u + q];
+    scatter_block(dom, table, L, ur[u], uc[u], B);
+}
+
+// In-place Gauss-Jordan inversion of one 48x48 domain per CTA (FP64 in shared memory).
+__global__ void __launch_bounds__(256) k_invert(int ndom, double* __restrict__ dom, float* __restrict__ dom32,
+                                                int write64, int write32) {
+    __shared__ double A[48][49];
+    __shared__ double colk[48];
+    const int d = blockIdx.x;
+    if (d >= ndom) return;
+    double* D = dom + (size_t)d * 2304;
+    for (int e = threadIdx.x; e < 2304; e += blockDim.x) A[e / 48][e % 48] = D[e];
+    __syncthreads();
+    if (threadIdx.x < 48 && A[threadIdx.x][threadIdx.x] == 0.0) A[threadIdx.x][threadIdx.x] = 1.0;
+    __syncthreads();
+    for (int k = 0; k < 48; k++) {
+        const double piv = A[k][k];
+        if (threadIdx.x < 48) colk[threadIdx.x] = A[threadIdx.x][k];
+        __syncthreads();
+        if (threadIdx.x < 48) {
+            const int j = threadIdx.x;
+            A[k][j] = (j == k) ? 1.0 / piv : A[k][j] / piv;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 2304; e += blockDim.x) {
+            const int i = e / 48, j = e % 48;
+            if (i == k) continue;
+            const double f = colk[i];
+            A[i][j] = (j == k) ? -f * A[k][k] : A[i][j] - f * A[k][j];
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < 2304; e += blockDim.x) {
+        const double v = A[e / 48][e % 48];
+        if (write64) D[e] = v;
+        if (write32) dom32[(size_t)d * 2304 + e] = (float)v;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// apply kernels (also used by the fused PCG kernels through the templates below)
+// ------------------------------------------------------------------------------------------
+namespace sgipc {
+
+template <class T, class M>
+__global__ void k_restrict(int nv, const T* __restrict__ r, const int* __restrict__ table, int L, M* __restrict__ R) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    const int* tv = table + (size_t)v * L;
+    M x = (M)r[3 * v], y = (M)r[3 * v + 1], z = (M)r[3 * v + 2];
+    int p = tv[0];
+    R[3 * p] = x;
+    R[3 * p + 1] = y;
+    R[3 * p + 2] = z;
+    for (int l = 1; l < L; l++) {
+        int g = tv[l];
+        atomicAdd(R + 3 * g, x);
+        atomicAdd(R + 3 * g + 1, y);
+        atomicAdd(R + 3 * g + 2, z);
+    }
+}
+
+// Z_d = A_d^-1 R_d, four domains per 192-thread CTA
+template <class M>
+__global__ void __launch_bounds__(192) k_domain_mv(const int* __restrict__ info, const M* __restrict__ inv,
+                                                   const M* __restrict__ R, M* __restrict__ Z) {
+    __shared__ M sR[4][48];
+    const int ndom = info[16] >> 4;
+    const int ld = threadIdx.x / 48, i = threadIdx.x % 48;
+    const int d = blockIdx.x * 4 + ld;
+    if (d < ndom) sR[ld][i] = R[48 * (size_t)d + i];
+    __syncthreads();
+    if (d >= ndom) return;
+    const M* Ad = inv + (size_t)d * 2304;
+    M acc = 0;
+#pragma unroll 8
+    for (int j = 0; j < 48; j++) acc += Ad[j * 48 + i] * sR[ld][j];
+    Z[48 * (size_t)d + i] = acc;
+}
+
+template <class T, class M>
+__global__ void k_prolong(int nv, const int* __restrict__ table, int L, const M* __restrict__ Z, T* __restrict__ z,
+                          M* __restrict__ R, const int* __restrict__ info, int npos) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    // clear the coarse part of R for the next restriction
+    const int total = info[16];
+    for (int k = npos * 3 + v; k < total * 3; k += gridDim.x * blockDim.x) R[k] = 0;
+    if (v >= nv) return;
+    const int* tv = table + (size_t)v * L;
+    M x = 0, y = 0, w = 0;
+    for (int l = 0; l < L; l++) {
+        int g = tv[l];
+        x += Z[3 * g];
+        y += Z[3 * g + 1];
+        w += Z[3 * g + 2];
+    }
+    z[3 * v] = (T)x;
+    z[3 * v + 1] = (T)y;
+    z[3 * v + 2] = (T)w;
+}
+
+template <class T>
+SgipcStatus mas_apply_t(SgipcCtx* c, const T* r, T* z, int fp32_inv, cudaStream_t s) {
+    MasWork& m = c->mas;
+    if (!m.built) return SGIPC_NOT_READY;
+    const int L = m.levelnum;
+    const int ndom = m.h_info[16] / 16;
+    if (fp32_inv) {
+        k_restrict<T, float><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, r, m.table, L, m.R32);
+        k_domain_mv<float><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom32, m.R32, m.Z32);
+        k_prolong<T, float><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, m.table, L, m.Z32, z, m.R32, m.info, m.npos);
+    } else {
+        k_restrict<T, double><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, r, m.table, L, m.R64);
+        k_domain_mv<double><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom64, m.R64, m.Z64);
+        k_prolong<T, double><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, m.table, L, m.Z64, z, m.R64, m.info, m.npos);
+    }
+    SG_LAUNCH_CHECK(c, "mas apply");
+    return SGIPC_OK;
+}
+
+template SgipcStatus mas_apply_t<double>(SgipcCtx*, const double*, double*, int, cudaStream_t);
+template SgipcStatus mas_apply_t<float>(SgipcCtx*, const float*, float*, int, cudaStream_t);
+
+static int num_levels(int nodes) {
+    int nLevel = 1;
+    int levelSz = (nodes + 15) / 16 * 16;
+    while (levelSz > 16) {
+        levelSz /= 16;
+        nLevel++;
+        levelSz = (levelSz + 15) / 16 * 16;
+    }
+    nLevel = nLevel + 1;
+    return nLevel > SGIPC_MAX_LEVELS ? SGIPC_MAX_LEVELS : nLevel;
+}
+
+SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
+    MasWork& m = c->mas;
+    m.npos = t->part_map_size;
+    m.levelnum = num_levels(m.npos > c->nv ? m.npos : c->nv);
+    m.total_cap = m.levelnum * m.npos;
+    const int nv = c->nv;
+    std::vector<int> pm(t->partId_map_real, t->partId_map_real + m.npos);
+    std::vector<int> rm(t->real_map_partId, t->real_map_partId + nv);
+    for (int i = 0; i < m.npos; i++)
+        if (pm[i] >= nv) return SGIPC_BAD_INPUT;
+    for (int v = 0; v < nv; v++)
+        if (rm[v] < 0 || rm[v] >= m.npos || pm[rm[v]] != v) return SGIPC_BAD_INPUT;
+    std::vector<int> ptr(nv + 1), nb(t->neighborStart[nv]);
+    for (int i = 0; i <= nv; i++) ptr[i] = (int)t->neighborStart[i];
+    for (size_t k = 0; k < nb.size(); k++) {
+        nb[k] = (int)t->neighborList[k];
+        if (nb[k] < 0 || nb[k] >= nv) return SGIPC_BAD_INPUT;
+    }
+    const size_t ndom_cap = (size_t)m.total_cap / 16;
+    const size_t rhs = (size_t)c->max_rhs;
+    auto A = [&](void** p, size_t bytes) -> bool { return cudaMalloc(p, bytes ? bytes : 4) == cudaSuccess; };
+    if (!A((void**)&m.part_map, sizeof(int) * m.npos) || !A((void**)&m.real_map, sizeof(int) * nv) ||
+        !A((void**)&m.nbr_ptr, sizeof(int) * (nv + 1)) || !A((void**)&m.nbr, sizeof(int) * nb.size()) ||
+        !A((void**)&m.table, sizeof(int) * (size_t)nv * m.levelnum) || !A((void**)&m.node, sizeof(int) * nv) ||
+        !A((void**)&m.mask, sizeof(uint32_t) * m.npos) || !A((void**)&m.comp_rank, sizeof(int) * m.npos) ||
+        !A((void**)&m.bank_cnt, sizeof(int) * (m.npos / 16 + 2)) ||
+        !A((void**)&m.bank_off, sizeof(int) * (m.npos / 16 + 2)) || !A((void**)&m.info, sizeof(int) * 32) ||
+        !A((void**)&m.dom64, sizeof(double) * ndom_cap * 2304) || !A((void**)&m.dom32, sizeof(float) * ndom_cap * 2304) ||
+        !A((void**)&m.R64, sizeof(double) * 3 * m.total_cap * rhs) ||
+        !A((void**)&m.Z64, sizeof(double) * 3 * m.total_cap * rhs) ||
+        !A((void**)&m.R32, sizeof(float) * 3 * m.total_cap * rhs) ||
+        !A((void**)&m.Z32, sizeof(float) * 3 * m.total_cap * rhs)) {
+        snprintf(c->err, sizeof(c->err), "MAS workspace allocation failed");
+        return SGIPC_CUDA_ERROR;
+    }
+    SG_CHECK(c, cudaMemcpy(m.part_map, pm.data(), sizeof(int) * m.npos, cudaMemcpyHostToDevice));
+    SG_CHECK(c, cudaMemcpy(m.real_map, rm.data(), sizeof(int) * nv, cudaMemcpyHostToDevice));
+    SG_CHECK(c, cudaMemcpy(m.nbr_ptr, ptr.data(), sizeof(int) * (nv + 1), cudaMemcpyHostToDevice));
+    if (!nb.empty()) SG_CHECK(c, cudaMemcpy(m.nbr, nb.data(), sizeof(int) * nb.size(), cudaMemcpyHostToDevice));
+    SG_CHECK(c, cudaMemset(m.R64, 0, sizeof(double) * 3 * m.total_cap * rhs));
+    SG_CHECK(c, cudaMemset(m.R32, 0, sizeof(float) * 3 * m.total_cap * rhs));
+    SG_CHECK(c, cudaMemset(m.info, 0, sizeof(int) * 32));
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, m.bank_cnt, m.bank_off, m.npos / 16 + 2);
+    m.scan_tmp_bytes = tb + 256;
+    SG_CHECK(c, cudaMalloc(&m.scan_tmp, m.scan_tmp_bytes));
+    return SGIPC_OK;
+}
+
+void mas_destroy(SgipcCtx* c) {
+    MasWork& m = c->mas;
+    void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.table, m.node, m.mask, m.comp_rank, m.bank_cnt,
+                    m.bank_off, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32, m.scan_tmp};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}
+
+SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, cudaStream_t s) {
+    MasWork& m = c->mas;
+    if (!c->assembled) return SGIPC_NOT_READY;
+    const int nv = c->nv, L = m.levelnum;
+    const int nbank_cap = m.npos / 16 + 1;
+    k_init_level0<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, m.real_map, L, m.node, m.table, m.info, m.npos);
+    for (int l = 0; l + 1 < L; l++) {
+        SG_CHECK(c, cudaMemsetAsync(m.mask, 0, sizeof(uint32_t) * m.npos, s));
+        k_mask_edges<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, m.nbr_ptr, m.nbr, m.node, m.mask);
+        if (con && con->pair_num > 0)
+            k_mask_pairs<<<nblk(con->pair_num), SGIPC_BLOCK, 0, s>>>(con->pair_num, (const int4*)con->pairs, nv,
+                                                                     m.node, m.mask);
+        k_bank_components<<<nblk(nbank_cap + 1, 128), 128, 0, s>>>(nbank_cap, m.info, l, m.mask, m.comp_rank,
+                                                                   m.bank_cnt);
+        size_t tb = m.scan_tmp_bytes;
+        SG_CHECK(c, cub::DeviceScan::ExclusiveSum(m.scan_tmp, tb, m.bank_cnt, m.bank_off, nbank_cap + 1, s));
+        k_assign<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, L, l, m.bank_off, m.comp_rank, m.node, m.table, m.info);
+    }
+    if (L == 1) {
+        int h[17] = {0};
+        h[8] = m.npos;
+        h[16] = m.npos;
+        SG_CHECK(c, cudaMemcpyAsync(m.info, h, sizeof(h), cudaMemcpyHostToDevice, s));
+    }
+    SG_LAUNCH_CHECK(c, "mas hierarchy");
+    SG_CHECK(c, cudaMemcpyAsync(m.h_info, m.info, sizeof(int) * 17, cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    const int total = m.h_info[16];
+    if (total > m.total_cap || total <= 0) {
+        snprintf(c->err, sizeof(c->err), "MAS cluster count %d exceeds capacity %d", total, m.total_cap);
+        return SGIPC_CAPACITY;
+    }
+    const int ndom = total / 16;
+    SG_CHECK(c, cudaMemsetAsync(m.dom64, 0, sizeof(double) * 2304 * (size_t)ndom, s));
+    k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L, m.dom64);
+    k_scatter_contact<<<nblk(c->cap_cblk), SGIPC_BLOCK, 0, s>>>(c->cap_cblk, c->nuc, c->uc_row, c->uc_col, c->uc64,
+                                                               m.table, L, m.dom64);
+    const int w64 = prec == SGIPC_FP64 ? 1 : 0, w32 = prec == SGIPC_FP64 ? 0 : 1;
+    k_invert<<<ndom, 256, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
+    SG_LAUNCH_CHECK(c, "mas matrices");
+    m.built = (int)prec + 1;
+    return SGIPC_OK;
+}
+
+}  // namespace sgipc
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+extern "C" SgipcStatus sgipc_mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, void* stream) {
+    if (!c) return SGIPC_BAD_INPUT;
+    if (con && con->pair_num > 0 && !con->pairs) return SGIPC_BAD_INPUT;
+    SG_CHECK(c, cudaSetDevice(c->device));
+    return mas_build(c, con, prec, (cudaStream_t)stream);
+}
+
+extern "C" SgipcStatus sgipc_mas_apply(SgipcCtx* c, const double* r, double* z, void* stream) {
+    if (!c || !r || !z) return SGIPC_BAD_INPUT;
+    return mas_apply_t<double>(c, r, z, c->mas.built == SGIPC_FP64 + 1 ? 0 : 1, (cudaStream_t)stream);
+}
+
+extern "C" SgipcStatus sgipc_mas_info(SgipcCtx* c, int32_t* levelnum, int32_t* level_counts, int32_t* total) {
+    if (!c) return SGIPC_BAD_INPUT;
+    if (!c->mas.built) return SGIPC_NOT_READY;
+    if (levelnum) *levelnum = c->mas.levelnum;
+    if (level_counts)
+        for (int l = 0; l < c->mas.levelnum; l++) level_counts[l] = c->mas.h_info[8 + l];
+    if (total) *total = c->mas.h_info[16];
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_mas_export_tables(SgipcCtx* c, int32_t* table) {
+    if (!c || !table) return SGIPC_BAD_INPUT;
+    if (!c->mas.built) return SGIPC_NOT_READY;
+    SG_CHECK(c, cudaDeviceSynchronize());
+    SG_CHECK(c, cudaMemcpy(table, c->mas.table, sizeof(int) * (size_t)c->nv * c->mas.levelnum, cudaMemcpyDeviceToHost));
+    return SGIPC_OK;
+}

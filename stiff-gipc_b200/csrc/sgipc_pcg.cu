@@ -1,0 +1,917 @@
+// sgipc_pcg.cu — symmetric BSR SpMV and MAS-preconditioned conjugate gradients.
+//
+// Algorithm of PCGSolver::pcg (StiffGIPC/linear_system/solver/pcg_solver.cu:174-267):
+//   r = b, z = M r, p = z, rz0 = rz = r.z
+//   for k = 1 .. max_iter-1:
+//     Ap = A p; alpha = rz / p.Ap; x += alpha p; r -= alpha Ap
+//     if |rz| <= tol * rz0: break          (tested on the rz from before the update)
+//     z = M r; rz_new = r.z; p = z + (rz_new / rz) p; rz = rz_new
+// The reference does each dot with a two-pass reduction and a blocking cudaMemcpy (two
+// host round trips per iteration).  Here every scalar stays in device memory: each
+// reduction finishes in the kernel's last CTA, a per-solve `state` word lets kernels of a
+// finished solve return at once, and the whole loop is one CUDA graph whose while-node
+// condition is set by the last kernel of the iteration body — one launch per solve.
+//
+// Kernels of one iteration (T = vector type, M = MAS type, NR = right-hand sides):
+//   K1 spmv_dot    Ap = A p over the static BSR (upper + transposed lists) and the unique
+//                  contact blocks, fused with p.Ap; last CTA: alpha, stop test, iteration cap
+//   K2 update      x += alpha p, r -= alpha Ap, MAS restriction of r (level 0 + coarse)
+//   K3 domain_mv   Z = A_d^-1 R for every 16-node domain (all NR columns per read of A_d^-1)
+//   K4 prolong_dot z = sum_l Z, r.z; last CTA: rz_next
+//   K5 p_update    p = z + beta p; sets the graph's loop condition
+#include <cub/cub.cuh>
+#include <vector>
+
+#include "sgipc_internal.cuh"
+
+using namespace sgipc;
+
+namespace sgipc {
+
+template <class T>
+struct MatView {
+    const T* val;      // static block values
+    const T* uc;       // unique contact block values
+};
+
+struct Topo {
+    int n;
+    const int* row_ptr;
+    const int* col;
+    const int* slot_row;
+    const int* low_ptr;
+    const int* low_slot;
+    const int* cu_ptr;
+    const int* cl_ptr;
+    const int* cl_idx;
+    const int* uc_row;
+    const int* uc_col;
+};
+
+struct MasView {
+    const int* table;
+    int L;
+    int npos;
+    const int* info;
+};
+
+inline Topo topo_of(SgipcCtx* c) {
+    Topo t;
+    t.n = c->n;
+    t.row_ptr = c->row_ptr;
+    t.col = c->col;
+    t.slot_row = c->slot_row;
+    t.low_ptr = c->low_ptr;
+    t.low_slot = c->low_slot;
+    t.cu_ptr = c->cu_ptr;
+    t.cl_ptr = c->cl_ptr;
+    t.cl_idx = c->cl_idx;
+    t.uc_row = c->uc_row;
+    t.uc_col = c->uc_col;
+    return t;
+}
+
+// ---- block reduction helpers ---------------------------------------------------------------
+template <int NR>
+__device__ __forceinline__ void block_sum(double (&v)[NR], double* smem /*[NR*8]*/) {
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[r] += __shfl_down_sync(0xffffffffu, v[r], o);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+        for (int r = 0; r < NR; r++) smem[r * 8 + w] = v[r];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            double s = 0;
+            for (int k = 0; k < nw; k++) s += smem[r * 8 + k];
+            v[r] = s;
+        }
+    }
+}
+
+// Publishes this CTA's partial sums; returns true in every thread of the last CTA to
+// arrive, after which out[r] holds the deterministic (CTA-order) total.
+template <int NR>
+__device__ __forceinline__ bool grid_sum(double (&v)[NR], double* partial, unsigned int* ticket, double* out,
+                                         double* smem) {
+    block_sum<NR>(v, smem);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) partial[r * gridDim.x + blockIdx.x] = v[r];
+        __threadfence();
+        unsigned int t = atomicAdd(ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        acc[r] = 0;
+        for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x)
+            acc[r] += ((volatile double*)partial)[r * gridDim.x + k];
+    }
+    block_sum<NR>(acc, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) out[r] = acc[r];
+        *ticket = 0;
+    }
+    __syncthreads();
+    return true;
+}
+
+// ---- SpMV core ------------------------------------------------------------------------------
+template <class T, int NR>
+__device__ __forceinline__ void block_mv(const T* __restrict__ B, const T* __restrict__ x, int j, bool transpose,
+                                         T (&acc)[NR][3]) {
+    T b[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) b[q] = B[q];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        T x0 = x[(3 * j) * NR + r], x1 = x[(3 * j + 1) * NR + r], x2 = x[(3 * j + 2) * NR + r];
+        if (!transpose) {
+            acc[r][0] += b[0] * x0 + b[1] * x1 + b[2] * x2;
+            acc[r][1] += b[3] * x0 + b[4] * x1 + b[5] * x2;
+            acc[r][2] += b[6] * x0 + b[7] * x1 + b[8] * x2;
+        } else {
+            acc[r][0] += b[0] * x0 + b[3] * x1 + b[6] * x2;
+            acc[r][1] += b[1] * x0 + b[4] * x1 + b[7] * x2;
+            acc[r][2] += b[2] * x0 + b[5] * x1 + b[8] * x2;
+        }
+    }
+}
+
+template <class T, int NR>
+__device__ __forceinline__ void row_mv(const Topo& tp, const MatView<T>& A, const T* __restrict__ x, int i,
+                                       T (&acc)[NR][3]) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r][0] = acc[r][1] = acc[r][2] = 0;
+    for (int s = tp.row_ptr[i]; s < tp.row_ptr[i + 1]; s++) block_mv<T, NR>(A.val + 9 * (size_t)s, x, tp.col[s], false, acc);
+    for (int k = tp.low_ptr[i]; k < tp.low_ptr[i + 1]; k++) {
+        int s = tp.low_slot[k];
+        block_mv<T, NR>(A.val + 9 * (size_t)s, x, tp.slot_row[s], true, acc);
+    }
+    for (int u = tp.cu_ptr[i]; u < tp.cu_ptr[i + 1]; u++) block_mv<T, NR>(A.uc + 9 * (size_t)u, x, tp.uc_col[u], false, acc);
+    for (int k = tp.cl_ptr[i]; k < tp.cl_ptr[i + 1]; k++) {
+        int u = tp.cl_idx[k];
+        block_mv<T, NR>(A.uc + 9 * (size_t)u, x, tp.uc_row[u], true, acc);
+    }
+}
+
+template <class T>
+__global__ void k_spmv(Topo tp, MatView<T> A, const T* __restrict__ x, T* __restrict__ y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= tp.n) return;
+    T acc[1][3];
+    row_mv<T, 1>(tp, A, x, i, acc);
+    y[3 * i] = acc[0][0];
+    y[3 * i + 1] = acc[0][1];
+    y[3 * i + 2] = acc[0][2];
+}
+
+// ---- PCG kernels ----------------------------------------------------------------------------
+template <class T, int NR>
+struct PcgPtrs {
+    T* x;
+    T* r;
+    T* z;
+    T* p;
+    T* Ap;
+    PcgScalars* sc;
+    double* partial;
+    unsigned int* ticket;
+};
+
+template <class T, int NR>
+__global__ void __launch_bounds__(256) k_pcg_spmv_dot(Topo tp, MatView<T> A, PcgPtrs<T, NR> P) {
+    __shared__ double smem[NR * 8];
+    __shared__ int st_run[NR];
+    if (threadIdx.x < NR) st_run[threadIdx.x] = P.sc[threadIdx.x].state == 0;
+    __syncthreads();
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < NR; r++) any |= st_run[r] != 0;
+    if (!any) return;  // uniform across the grid: state only changes in the last CTA below
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double part[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) part[r] = 0.0;
+    if (i < tp.n) {
+        T acc[NR][3];
+        row_mv<T, NR>(tp, A, P.p, i, acc);
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                P.Ap[(3 * i + q) * NR + r] = acc[r][q];
+                part[r] += (double)P.p[(3 * i + q) * NR + r] * (double)acc[r][q];
+            }
+    }
+    double tot[NR];
+    if (grid_sum<NR>(part, P.partial, P.ticket, tot, smem) && threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            PcgScalars& s = P.sc[r];
+            if (!st_run[r]) continue;
+            s.rz = s.rz_next;
+            s.pAp = tot[r];
+            s.iter += 1;
+            if (!(tot[r] > 0.0) || !isfinite(tot[r]) || !isfinite(s.rz)) {
+                s.state = 2;
+                s.status = SGIPC_BREAKDOWN;
+                continue;
+            }
+            s.alpha = s.rz / tot[r];
+            if (s.crit == SGIPC_CRIT_RZ && fabs(s.rz) <= s.tol * s.rz0) s.state = 1;
+        }
+    }
+}
+
+template <class T, class M, int NR>
+__global__ void __launch_bounds__(256) k_pcg_update(int nv, PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R) {
+    __shared__ double smem[NR * 8];
+    __shared__ int st[NR];
+    __shared__ double alpha[NR];
+    if (threadIdx.x < NR) {
+        st[threadIdx.x] = P.sc[threadIdx.x].state;
+        alpha[threadIdx.x] = P.sc[threadIdx.x].alpha;
+    }
+    __syncthreads();
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < NR; r++) any |= st[r] < 2;
+    if (!any) return;
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    double part[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) part[r] = 0.0;
+    if (v < nv) {
+        const int* tv = mv.table + (size_t)v * mv.L;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            if (st[r] == 2) continue;
+            T a = (T)alpha[r];
+            T rv[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const size_t k = (size_t)(3 * v + q) * NR + r;
+                P.x[k] += a * P.p[k];
+                rv[q] = P.r[k] - a * P.Ap[k];
+                P.r[k] = rv[q];
+                part[r] += (double)rv[q] * (double)rv[q];
+            }
+            if (st[r] == 0) {
+                int p0 = tv[0];
+#pragma unroll
+                for (int q = 0; q < 3; q++) R[(size_t)(3 * p0 + q) * NR + r] = (M)rv[q];
+                for (int l = 1; l < mv.L; l++) {
+                    int g = tv[l];
+#pragma unroll
+                    for (int q = 0; q < 3; q++) atomicAdd(R + (size_t)(3 * g + q) * NR + r, (M)rv[q]);
+                }
+            }
+        }
+    }
+    double tot[NR];
+    if (grid_sum<NR>(part, P.partial + NR * gridDim.x, P.ticket + 1, tot, smem) && threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            PcgScalars& s = P.sc[r];
+            if (st[r] == 2) continue;
+            s.rr = tot[r];
+            if (s.crit == SGIPC_CRIT_TRUE && s.state == 0 && tot[r] <= s.tol * s.tol * s.bnorm2) s.state = 1;
+        }
+    }
+}
+
+template <class M, int NR>
+__global__ void __launch_bounds__(192) k_pcg_domain(const int* __restrict__ info, const PcgScalars* __restrict__ sc,
+                                                    const M* __restrict__ inv, const M* __restrict__ R,
+                                                    M* __restrict__ Z) {
+    __shared__ M sR[4][48 * NR];
+    __shared__ int run[NR];
+    if (threadIdx.x < NR) run[threadIdx.x] = sc[threadIdx.x].state == 0;
+    const int ndom = info[16] >> 4;
+    const int ld = threadIdx.x / 48, i = threadIdx.x % 48;
+    const int d = blockIdx.x * 4 + ld;
+    if (d < ndom)
+#pragma unroll
+        for (int r = 0; r < NR; r++) sR[ld][i * NR + r] = R[(48 * (size_t)d + i) * NR + r];
+    __syncthreads();
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < NR; r++) any |= run[r] != 0;
+    if (!any || d >= ndom) return;
+    const M* Ad = inv + (size_t)d * 2304;
+    M acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r] = 0;
+#pragma unroll 4
+    for (int j = 0; j < 48; j++) {
+        M a = Ad[j * 48 + i];
+#pragma unroll
+        for (int r = 0; r < NR; r++) acc[r] += a * sR[ld][j * NR + r];
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++) Z[(48 * (size_t)d + i) * NR + r] = acc[r];
+}
+
+template <class T, class M, int NR>
+__global__ void __launch_bounds__(256) k_pcg_prolong_dot(int nv, PcgPtrs<T, NR> P, MasView mv,
+                                                         const M* __restrict__ Z, M* __restrict__ R) {
+    __shared__ double smem[NR * 8];
+    __shared__ int run[NR];
+    if (threadIdx.x < NR) run[threadIdx.x] = P.sc[threadIdx.x].state == 0;
+    __syncthreads();
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < NR; r++) any |= run[r] != 0;
+    if (!any) return;
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int total = mv.info[16];
+    for (long long k = (long long)mv.npos * 3 * NR + v; k < (long long)total * 3 * NR;
+         k += (long long)gridDim.x * blockDim.x)
+        R[k] = 0;
+    double part[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) part[r] = 0.0;
+    if (v < nv) {
+        const int* tv = mv.table + (size_t)v * mv.L;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            if (!run[r]) continue;
+            M a0 = 0, a1 = 0, a2 = 0;
+            for (int l = 0; l < mv.L; l++) {
+                int g = tv[l];
+                a0 += Z[(size_t)(3 * g) * NR + r];
+                a1 += Z[(size_t)(3 * g + 1) * NR + r];
+                a2 += Z[(size_t)(3 * g + 2) * NR + r];
+            }
+            T zz[3] = {(T)a0, (T)a1, (T)a2};
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const size_t k = (size_t)(3 * v + q) * NR + r;
+                P.z[k] = zz[q];
+                part[r] += (double)P.r[k] * (double)zz[q];
+            }
+        }
+    }
+    double tot[NR];
+    if (grid_sum<NR>(part, P.partial + 2 * NR * gridDim.x, P.ticket + 2, tot, smem) && threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (run[r]) P.sc[r].rz_next = tot[r];
+    }
+}
+
+template <class T, int NR>
+__global__ void __launch_bounds__(256) k_pcg_p_update(int n3, PcgPtrs<T, NR> P, cudaGraphConditionalHandle h,
+                                                      int use_cond) {
+    __shared__ int st[NR];
+    __shared__ double beta[NR];
+    if (threadIdx.x < NR) {
+        const PcgScalars& s = P.sc[threadIdx.x];
+        st[threadIdx.x] = s.state;
+        beta[threadIdx.x] = s.rz_next / s.rz;
+    }
+    __syncthreads();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n3) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            if (st[r] != 0) continue;
+            const size_t e = (size_t)k * NR + r;
+            P.p[e] = P.z[e] + (T)beta[r] * P.p[e];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int cont = 0;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            PcgScalars& s = P.sc[r];
+            if (s.state == 1) s.state = 2;
+            s.bodies += 1;
+            if (s.state == 0 && (s.iter + 1 >= s.max_iter || s.bodies >= s.max_iter + 2)) {
+                s.state = 2;
+                s.status = SGIPC_NOT_CONVERGED;
+            }
+            if (s.state == 0) cont = 1;
+        }
+        if (use_cond) cudaGraphSetConditional(h, cont);
+    }
+}
+
+// ---- solve set-up kernels -------------------------------------------------------------------
+template <class T, class M, int NR>
+__global__ void k_pcg_init(int nv, const double* __restrict__ b, PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R,
+                           double tol, int max_iter, int crit) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < NR) {
+        PcgScalars& s = P.sc[v];
+        s.state = 0;
+        s.status = SGIPC_OK;
+        s.iter = 0;
+        s.bodies = 0;
+        s.tol = tol;
+        s.max_iter = max_iter;
+        s.crit = crit;
+    }
+    if (v >= nv) return;
+    const int* tv = mv.table + (size_t)v * mv.L;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        T rv[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const size_t k = (size_t)(3 * v + q) * NR + r;
+            rv[q] = (T)b[k];
+            P.r[k] = rv[q];
+            P.x[k] = 0;
+        }
+        int p0 = tv[0];
+#pragma unroll
+        for (int q = 0; q < 3; q++) R[(size_t)(3 * p0 + q) * NR + r] = (M)rv[q];
+        for (int l = 1; l < mv.L; l++) {
+            int g = tv[l];
+#pragma unroll
+            for (int q = 0; q < 3; q++) atomicAdd(R + (size_t)(3 * g + q) * NR + r, (M)rv[q]);
+        }
+    }
+}
+
+template <class T, int NR>
+__global__ void k_pcg_init_finish(int n3, const double* __restrict__ b, PcgPtrs<T, NR> P) {
+    __shared__ double smem[NR * 8];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double part[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        part[r] = 0.0;
+        if (k < n3) {
+            const size_t e = (size_t)k * NR + r;
+            P.p[e] = P.z[e];
+            part[r] = b[e] * b[e];
+        }
+    }
+    double tot[NR];
+    if (grid_sum<NR>(part, P.partial + 3 * NR * gridDim.x, P.ticket + 3, tot, smem) && threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            PcgScalars& s = P.sc[r];
+            s.rz0 = s.rz = s.rz_next;
+            s.bnorm2 = tot[r];
+            s.rr = tot[r];
+            if (!(s.rz0 > 0.0) || !isfinite(s.rz0)) {
+                // b = 0 (or an indefinite preconditioner): nothing to iterate
+                s.state = 2;
+                if (!isfinite(s.rz0) || s.rz0 < 0.0) s.status = SGIPC_BREAKDOWN;
+            }
+        }
+    }
+}
+
+// ---- dot products and vector helpers --------------------------------------------------------
+__global__ void k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double* partial,
+                      unsigned int* ticket, double* out) {
+    __shared__ double smem[8];
+    double v[1] = {0.0};
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) v[0] += a[k] * b[k];
+    double tot[1];
+    if (grid_sum<1>(v, partial, ticket, tot, smem) && threadIdx.x == 0) out[0] = tot[0];
+}
+
+__global__ void k_axpby_res(int n, const double* __restrict__ b, const double* __restrict__ Ax, double* __restrict__ r) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) r[k] = b[k] - Ax[k];
+}
+
+template <class A, class B>
+__global__ void k_convert(int n, const A* __restrict__ a, B* __restrict__ b) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) b[k] = (B)a[k];
+}
+
+__global__ void k_add_f32(int n, const float* __restrict__ d, double* __restrict__ x) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) x[k] += (double)d[k];
+}
+
+// rhs-major [nrhs][n3] <-> interleaved [n3][nrhs]
+template <class A, class B>
+__global__ void k_interleave(int n3, int nrhs, const A* __restrict__ src, B* __restrict__ dst, int to_interleaved) {
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (long long)n3 * nrhs) return;
+    int r = (int)(k / n3), i = (int)(k % n3);
+    if (to_interleaved)
+        dst[(size_t)i * nrhs + r] = (B)src[k];
+    else
+        dst[k] = (B)src[(size_t)i * nrhs + r];
+}
+
+}  // namespace sgipc
+
+// --------------------------------------------------------------------------------------------
+// host side
+// --------------------------------------------------------------------------------------------
+namespace {
+
+template <class T, int NR>
+PcgPtrs<T, NR> ptrs_of(PcgWork& w) {
+    PcgPtrs<T, NR> P;
+    P.x = (T*)w.x;
+    P.r = (T*)w.r;
+    P.z = (T*)w.z;
+    P.p = (T*)w.p;
+    P.Ap = (T*)w.Ap;
+    P.sc = w.sc;
+    P.partial = w.partial;
+    P.ticket = w.ticket;
+    return P;
+}
+
+MasView mas_view(SgipcCtx* c) {
+    MasView m;
+    m.table = c->mas.table;
+    m.L = c->mas.levelnum;
+    m.npos = c->mas.npos;
+    m.info = c->mas.info;
+    return m;
+}
+
+template <class T>
+MatView<T> mat_view(SgipcCtx* c);
+template <>
+MatView<double> mat_view<double>(SgipcCtx* c) {
+    return {c->val64, c->uc64};
+}
+template <>
+MatView<float> mat_view<float>(SgipcCtx* c) {
+    return {c->val32, c->uc32};
+}
+
+// Enqueue one PCG iteration body (K1..K5) on stream s.
+template <class T, class M, int NR>
+void enqueue_body(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, cudaGraphConditionalHandle h, int use_cond,
+                  int ndom, cudaStream_t s) {
+    const int n = c->n, nv = c->nv;
+    PcgPtrs<T, NR> P = ptrs_of<T, NR>(w);
+    MasView mv = mas_view(c);
+    k_pcg_spmv_dot<T, NR><<<nblk(n), 256, 0, s>>>(topo_of(c), mat_view<T>(c), P);
+    k_pcg_update<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, R);
+    k_pcg_domain<M, NR><<<(ndom + 3) / 4, 192, 0, s>>>(c->mas.info, w.sc, inv, R, Z);
+    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z, R);
+    k_pcg_p_update<T, NR><<<nblk(3LL * n), 256, 0, s>>>(3 * n, P, h, use_cond);
+}
+
+// Build (or reuse) the executable graph of the iteration loop for this workspace.
+template <class T, class M, int NR>
+SgipcStatus get_loop_graph(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, int ndom, int tag) {
+    const long long key = (long long)tag * 100000000LL + ndom;
+    if (w.exec && w.captured_key == key) return SGIPC_OK;
+    if (w.exec) {
+        cudaGraphExecDestroy(w.exec);
+        w.exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    SG_CHECK(c, cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    bool ok = e == cudaSuccess;
+    cudaGraphNode_t node;
+    cudaGraph_t body = nullptr;
+    if (ok) {
+        cudaGraphNodeParams prm = {};
+        prm.type = cudaGraphNodeTypeConditional;
+        prm.conditional.handle = h;
+        prm.conditional.type = cudaGraphCondTypeWhile;
+        prm.conditional.size = 1;
+        e = cudaGraphAddNode(&node, g, nullptr, 0, &prm);
+        ok = e == cudaSuccess;
+        if (ok) body = prm.conditional.phGraph_out[0];
+    }
+    if (ok) {
+        e = cudaStreamBeginCaptureToGraph(c->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        ok = e == cudaSuccess;
+        if (ok) {
+            enqueue_body<T, M, NR>(c, w, inv, R, Z, h, 1, ndom, c->cap_stream);
+            cudaGraph_t out = nullptr;
+            e = cudaStreamEndCapture(c->cap_stream, &out);
+            ok = e == cudaSuccess;
+        }
+    }
+    if (ok) {
+        e = cudaGraphInstantiate(&w.exec, g, 0);
+        ok = e == cudaSuccess;
+    }
+    cudaGraphDestroy(g);
+    cudaGetLastError();
+    if (ok) {
+        w.cond_graph = true;
+        w.captured_key = key;
+        return SGIPC_OK;
+    }
+    // fallback: a graph of 8 iterations, relaunched until the state word says done
+    w.cond_graph = false;
+    w.exec = nullptr;
+    SG_CHECK(c, cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < 8; k++) enqueue_body<T, M, NR>(c, w, inv, R, Z, h, 0, ndom, c->cap_stream);
+    cudaGraph_t cg = nullptr;
+    SG_CHECK(c, cudaStreamEndCapture(c->cap_stream, &cg));
+    e = cudaGraphInstantiate(&w.exec, cg, 0);
+    cudaGraphDestroy(cg);
+    SG_CHECK(c, e);
+    w.captured_key = key;
+    return SGIPC_OK;
+}
+
+// One PCG solve of A x = b (b, x: interleaved [3n][NR], b FP64, x in T) with MAS type M.
+template <class T, class M, int NR>
+SgipcStatus run_pcg(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
+                    cudaStream_t s, int tag) {
+    MasWork& m = c->mas;
+    const int ndom = m.h_info[16] / 16;
+    const M* inv = fp32_mas ? (const M*)m.dom32 : (const M*)m.dom64;
+    M* R = fp32_mas ? (M*)m.R32 : (M*)m.R64;
+    M* Z = fp32_mas ? (M*)m.Z32 : (M*)m.Z64;
+    SgipcStatus st = get_loop_graph<T, M, NR>(c, w, inv, R, Z, ndom, tag);
+    if (st != SGIPC_OK) return st;
+    const int nv = c->nv, n = c->n;
+    PcgPtrs<T, NR> P = ptrs_of<T, NR>(w);
+    MasView mv = mas_view(c);
+    SG_CHECK(c, cudaMemsetAsync(R, 0, sizeof(M) * 3 * (size_t)m.h_info[16] * NR, s));
+    k_pcg_init<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, b, P, mv, R, tol, max_iter, crit);
+    k_pcg_domain<M, NR><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, w.sc, inv, R, Z);
+    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z, R);
+    k_pcg_init_finish<T, NR><<<nblk(3LL * n), 256, 0, s>>>(3 * n, b, P);
+    SG_LAUNCH_CHECK(c, "pcg init");
+    if (w.cond_graph) {
+        SG_CHECK(c, cudaGraphLaunch(w.exec, s));
+    } else {
+        for (int guard = 0; guard < 1 + max_iter / 8; guard++) {
+            SG_CHECK(c, cudaGraphLaunch(w.exec, s));
+            PcgScalars hs[NR];
+            SG_CHECK(c, cudaMemcpyAsync(hs, w.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
+            SG_CHECK(c, cudaStreamSynchronize(s));
+            bool run = false;
+            for (int r = 0; r < NR; r++) run |= hs[r].state == 0;
+            if (!run) break;
+        }
+    }
+    return SGIPC_OK;
+}
+
+SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
+    const size_t n3 = 3 * (size_t)c->n * nrhs;
+    void** vs[] = {&w.x, &w.r, &w.z, &w.p, &w.Ap};
+    for (void** v : vs) SG_CHECK(c, cudaMalloc(v, elem * n3));
+    SG_CHECK(c, cudaMalloc((void**)&w.sc, sizeof(PcgScalars) * nrhs));
+    SG_CHECK(c, cudaMalloc((void**)&w.partial, sizeof(double) * 4 * nrhs * c->max_blocks));
+    SG_CHECK(c, cudaMalloc((void**)&w.ticket, sizeof(unsigned int) * 8));
+    SG_CHECK(c, cudaMemset(w.ticket, 0, sizeof(unsigned int) * 8));
+    SG_CHECK(c, cudaMemset(w.sc, 0, sizeof(PcgScalars) * nrhs));
+    return SGIPC_OK;
+}
+
+void free_work(PcgWork& w) {
+    void* ps[] = {w.x, w.r, w.z, w.p, w.Ap, w.sc, w.partial, w.ticket};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (w.exec) cudaGraphExecDestroy(w.exec);
+}
+
+}  // namespace
+
+namespace sgipc {
+
+SgipcStatus pcg_create(SgipcCtx* c) {
+    int maxn = c->n > c->nv ? c->n : c->nv;
+    c->max_blocks = nblk(3LL * maxn, 256) + 8;
+    SgipcStatus st;
+    if ((st = alloc_work(c, c->pcg64, sizeof(double), c->max_rhs)) != SGIPC_OK) return st;
+    if ((st = alloc_work(c, c->pcg32, sizeof(float), c->max_rhs)) != SGIPC_OK) return st;
+    SG_CHECK(c, cudaMalloc((void**)&c->tmp64, sizeof(double) * 3 * (size_t)c->n * c->max_rhs));
+    SG_CHECK(c, cudaMalloc((void**)&c->tmp64b, sizeof(double) * 3 * (size_t)c->n * c->max_rhs));
+    SG_CHECK(c, cudaMalloc((void**)&c->dot_partial, sizeof(double) * 1024));
+    SG_CHECK(c, cudaMalloc((void**)&c->dot_ticket, sizeof(unsigned int) * 4));
+    SG_CHECK(c, cudaMemset(c->dot_ticket, 0, sizeof(unsigned int) * 4));
+    SG_CHECK(c, cudaMalloc((void**)&c->dot_out, sizeof(double) * 16));
+    SG_CHECK(c, cudaMallocHost((void**)&c->h_pinned, sizeof(double) * 64));
+    SG_CHECK(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+    return SGIPC_OK;
+}
+
+void pcg_destroy(SgipcCtx* c) {
+    free_work(c->pcg64);
+    free_work(c->pcg32);
+    void* ps[] = {c->tmp64, c->tmp64b, c->dot_partial, c->dot_ticket, c->dot_out};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+}
+
+template <class T>
+SgipcStatus spmv_t(SgipcCtx* c, const T* x, T* y, cudaStream_t s) {
+    k_spmv<T><<<nblk(c->n), 256, 0, s>>>(topo_of(c), mat_view<T>(c), x, y);
+    SG_LAUNCH_CHECK(c, "spmv");
+    return SGIPC_OK;
+}
+template SgipcStatus spmv_t<double>(SgipcCtx*, const double*, double*, cudaStream_t);
+template SgipcStatus spmv_t<float>(SgipcCtx*, const float*, float*, cudaStream_t);
+
+SgipcStatus dot64(SgipcCtx* c, const double* a, const double* b, int n, double* out_dev, cudaStream_t s) {
+    int g = nblk(n, 256);
+    if (g > 1024) g = 1024;
+    k_dot<<<g, 256, 0, s>>>(n, a, b, c->dot_partial, c->dot_ticket, out_dev);
+    SG_LAUNCH_CHECK(c, "dot");
+    return SGIPC_OK;
+}
+
+}  // namespace sgipc
+
+// --------------------------------------------------------------------------------------------
+// C ABI
+// --------------------------------------------------------------------------------------------
+extern "C" SgipcStatus sgipc_spmv(SgipcCtx* c, const double* x, double* y, void* stream) {
+    if (!c || !x || !y) return SGIPC_BAD_INPUT;
+    if (!c->assembled) return SGIPC_NOT_READY;
+    return spmv_t<double>(c, x, y, (cudaStream_t)stream);
+}
+
+// true relative residual ||b - A x|| / ||b|| (FP64), nrhs interleaved vectors
+static SgipcStatus true_residual(SgipcCtx* c, const double* b, const double* x, double* out, cudaStream_t s) {
+    const int n3 = 3 * c->n;
+    SgipcStatus st = spmv_t<double>(c, x, c->tmp64b, s);
+    if (st != SGIPC_OK) return st;
+    k_axpby_res<<<nblk(n3), 256, 0, s>>>(n3, b, c->tmp64b, c->tmp64b);
+    if ((st = dot64(c, c->tmp64b, c->tmp64b, n3, c->dot_out, s)) != SGIPC_OK) return st;
+    if ((st = dot64(c, b, b, n3, c->dot_out + 1, s)) != SGIPC_OK) return st;
+    SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    *out = c->h_pinned[1] > 0 ? sqrt(c->h_pinned[0] / c->h_pinned[1]) : 0.0;
+    return SGIPC_OK;
+}
+
+static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion crit, double tol, int max_iter,
+                             const double* b, double* x, SgipcSolveStats* stats, cudaStream_t s) {
+    const int n3 = 3 * c->n;
+    if (max_iter <= 0) max_iter = (int)(0.3 * n3);
+    if (max_iter < 2) max_iter = 2;
+    SgipcSolveStats out = {};
+    SgipcStatus st;
+    if (prec == SGIPC_FP64 || prec == SGIPC_REF) {
+        const int f32 = prec == SGIPC_REF ? 1 : 0;
+        if (f32)
+            st = run_pcg<double, float, 1>(c, c->pcg64, 1, b, tol, max_iter, (int)crit, s, 11);
+        else
+            st = run_pcg<double, double, 1>(c, c->pcg64, 0, b, tol, max_iter, (int)crit, s, 10);
+        if (st != SGIPC_OK) return st;
+        SG_CHECK(c, cudaMemcpyAsync(x, c->pcg64.x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+        PcgScalars hs;
+        SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg64.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        SG_CHECK(c, cudaStreamSynchronize(s));
+        out.iterations = hs.iter;
+        out.refinements = 0;
+        out.rz0 = hs.rz0;
+        out.rz = hs.rz_next;
+        out.status = hs.status;
+    } else {
+        // mixed: FP32 MAS-PCG inner solves on the FP32 matrix copy, FP64 residual refinement
+        double* r64 = c->tmp64;
+        SG_CHECK(c, cudaMemsetAsync(x, 0, sizeof(double) * n3, s));
+        SG_CHECK(c, cudaMemcpyAsync(r64, b, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+        double rz0 = -1.0, rz = 0.0, bn2 = 0.0;
+        int total_it = 0, ref = 0, status = SGIPC_OK;
+        for (ref = 0; ref < 8; ref++) {
+            double inner_tol = tol;
+            if (rz0 > 0 && rz > 0) inner_tol = fmin(1.0, fmax(tol * rz0 / rz, 1e-10));
+            if (crit == SGIPC_CRIT_TRUE && bn2 > 0 && rz > 0) inner_tol = tol;
+            st = run_pcg<float, float, 1>(c, c->pcg32, 1, r64, inner_tol, max_iter, (int)crit, s, 20);
+            if (st != SGIPC_OK) return st;
+            k_add_f32<<<nblk(n3), 256, 0, s>>>(n3, (const float*)c->pcg32.x, x);
+            // r = b - A x in FP64
+            if ((st = spmv_t<double>(c, x, c->tmp64b, s)) != SGIPC_OK) return st;
+            k_axpby_res<<<nblk(n3), 256, 0, s>>>(n3, b, c->tmp64b, r64);
+            PcgScalars hs;
+            SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg32.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
+            // rz of the refined residual with the same (FP32) preconditioner
+            if ((st = mas_apply_t<double>(c, r64, c->tmp64b, 1, s)) != SGIPC_OK) return st;
+            if ((st = dot64(c, r64, c->tmp64b, n3, c->dot_out, s)) != SGIPC_OK) return st;
+            if ((st = dot64(c, r64, r64, n3, c->dot_out + 1, s)) != SGIPC_OK) return st;
+            SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            SG_CHECK(c, cudaStreamSynchronize(s));
+            total_it += hs.iter;
+            if (ref == 0) {
+                rz0 = hs.rz0;
+                bn2 = hs.bnorm2;
+            }
+            rz = c->h_pinned[0];
+            if (hs.status == SGIPC_BREAKDOWN) {
+                status = SGIPC_BREAKDOWN;
+                break;
+            }
+            bool done = crit == SGIPC_CRIT_RZ ? fabs(rz) <= tol * rz0 : c->h_pinned[1] <= tol * tol * bn2;
+            if (done || total_it >= max_iter) {
+                if (!done) status = SGIPC_NOT_CONVERGED;
+                break;
+            }
+        }
+        out.iterations = total_it;
+        out.refinements = ref + 1;
+        out.rz0 = rz0;
+        out.rz = rz;
+        out.status = status;
+    }
+    if ((st = true_residual(c, b, x, &out.rel_residual, s)) != SGIPC_OK) return st;
+    if (stats) *stats = out;
+    return (SgipcStatus)out.status;
+}
+
+extern "C" SgipcStatus sgipc_pcg_solve(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion crit, double tol,
+                                       int32_t max_iter, const double* b, double* x, SgipcSolveStats* stats,
+                                       void* stream) {
+    if (!c || !b || !x || !(tol > 0.0)) return SGIPC_BAD_INPUT;
+    if (!c->assembled || !c->mas.built) return SGIPC_NOT_READY;
+    SG_CHECK(c, cudaSetDevice(c->device));
+    // the MAS inverses must exist in the precision the solve reads
+    if ((prec == SGIPC_FP64) != (c->mas.built == SGIPC_FP64 + 1)) return SGIPC_NOT_READY;
+    SgipcStatus fs = check_device_flag(c, (cudaStream_t)stream);
+    if (fs != SGIPC_OK) return fs;
+    return solve_one(c, prec, crit, tol, max_iter, b, x, stats, (cudaStream_t)stream);
+}
+
+extern "C" SgipcStatus sgipc_solve(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, SgipcCriterion crit,
+                                   double tol, int32_t max_iter, double* move_dir, SgipcSolveStats* stats,
+                                   void* stream) {
+    if (!c || !move_dir) return SGIPC_BAD_INPUT;
+    if (!c->assembled) return SGIPC_NOT_READY;
+    SgipcStatus st = sgipc_mas_build(c, con, prec, stream);
+    if (st != SGIPC_OK) return st;
+    return sgipc_pcg_solve(c, prec, crit, tol, max_iter, c->b, move_dir, stats, stream);
+}
+
+extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion crit, double tol,
+                                               int32_t max_iter, int32_t nrhs, const double* b, double* x,
+                                               SgipcSolveStats* stats, void* stream) {
+    if (!c || !b || !x || nrhs < 1 || !(tol > 0.0)) return SGIPC_BAD_INPUT;
+    if (nrhs > c->max_rhs) return SGIPC_CAPACITY;
+    if (!c->assembled || !c->mas.built) return SGIPC_NOT_READY;
+    if ((prec == SGIPC_FP64) != (c->mas.built == SGIPC_FP64 + 1)) return SGIPC_NOT_READY;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n3 = 3 * c->n;
+    if (max_iter <= 0) max_iter = (int)(0.3 * n3);
+    if (nrhs != 4) {
+        // one right-hand side at a time
+        SgipcStatus worst = SGIPC_OK;
+        for (int r = 0; r < nrhs; r++) {
+            SgipcStatus st = solve_one(c, prec, crit, tol, max_iter, b + (size_t)r * n3, x + (size_t)r * n3,
+                                       stats ? stats + r : nullptr, s);
+            if (st == SGIPC_CUDA_ERROR || st == SGIPC_BAD_INPUT) return st;
+            if (st != SGIPC_OK) worst = st;
+        }
+        return worst;
+    }
+    // four right-hand sides interleaved: every matrix / MAS block read serves all four
+    double* bi = c->tmp64;
+    k_interleave<double, double><<<nblk(4LL * n3), 256, 0, s>>>(n3, 4, b, bi, 1);
+    SgipcStatus st;
+    PcgWork& w = (prec == SGIPC_MIXED) ? c->pcg32 : c->pcg64;
+    if (prec == SGIPC_FP64)
+        st = run_pcg<double, double, 4>(c, w, 0, bi, tol, max_iter, (int)crit, s, 40);
+    else if (prec == SGIPC_REF)
+        st = run_pcg<double, float, 4>(c, w, 1, bi, tol, max_iter, (int)crit, s, 41);
+    else
+        st = run_pcg<float, float, 4>(c, w, 1, bi, tol, max_iter, (int)crit, s, 42);
+    if (st != SGIPC_OK) return st;
+    if (prec == SGIPC_MIXED)
+        k_interleave<float, double><<<nblk(4LL * n3), 256, 0, s>>>(n3, 4, (const float*)w.x, x, 0);
+    else
+        k_interleave<double, double><<<nblk(4LL * n3), 256, 0, s>>>(n3, 4, (const double*)w.x, x, 0);
+    PcgScalars hs[4];
+    SG_CHECK(c, cudaMemcpyAsync(hs, w.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    SgipcStatus worst = SGIPC_OK;
+    for (int r = 0; r < 4; r++) {
+        if (stats) {
+            stats[r] = SgipcSolveStats{};
+            stats[r].iterations = hs[r].iter;
+            stats[r].rz0 = hs[r].rz0;
+            stats[r].rz = hs[r].rz_next;
+            stats[r].status = hs[r].status;
+            double rel = 0;
+            if ((st = true_residual(c, b + (size_t)r * n3, x + (size_t)r * n3, &rel, s)) != SGIPC_OK) return st;
+            stats[r].rel_residual = rel;
+        }
+        if (hs[r].status != SGIPC_OK) worst = (SgipcStatus)hs[r].status;
+    }
+    return worst;
+}

@@ -1,0 +1,357 @@
+"""Host-side contact pair generation in StiffGIPC's int4 encoding, and lagged friction data.
+
+The reference finds pairs with an LBVH (StiffGIPC/mlbvh.cu:1306-1742) and encodes each
+one by its closest-feature type (StiffGIPC/mlbvh.cu:560-690 for point-triangle,
+690-1059 for edge-edge):
+
+* ``( a0,  a1,  b0,  b1)``           edge-edge
+* ``(-p-1, t0,  t1,  t2)``           point-triangle
+* ``(-p-1, e0,  e1,  w<0)``          point-edge
+* ``(-p-1, q,   -1,  w<0)``          point-point
+* ``( a0,  a1,  b0, -b1-1)``         mollified (nearly parallel) edge-edge
+* ``(-p-1, -q-1, c, -d-1)``          mollified point-edge
+* ``(-p-1, -q-1, -c-1, -d-1)``       mollified point-point
+
+The shipping reference generator never emits the three mollified forms (``smooth`` is
+false, StiffGIPC/mlbvh.cu:706); the barrier kernels still accept them.  This module is
+the harness's input generator (a k-d tree broad phase plus exact type tests) and is not
+part of the measured path.  ``lag_friction`` restates the once-per-frame lagged friction
+set-up ``_calFrictionLastH_DistAndTan`` / ``_calFrictionLastH_gd``
+(StiffGIPC/GIPC.cu:8362-8499).
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy.spatial import cKDTree
+
+PP, PE, PT, EE = 0, 1, 2, 3
+
+
+# ----------------------------------------------------------------------------------------
+# closest-feature classification (vectorised)
+# ----------------------------------------------------------------------------------------
+
+def pt_type(p, t0, t1, t2):
+    """Closest feature of triangle (t0,t1,t2) to point p.
+
+    Returns codes matching the reference's switch in ``_checkPTintersection``:
+    0/1/2 = point-vertex t0/t1/t2, 3/4/5 = point-edge (t0t1)/(t1t2)/(t2t0), 6 = interior.
+    """
+    ab = t1 - t0
+    ac = t2 - t0
+    ap = p - t0
+    d1 = (ab * ap).sum(1)
+    d2 = (ac * ap).sum(1)
+    bp = p - t1
+    d3 = (ab * bp).sum(1)
+    d4 = (ac * bp).sum(1)
+    cp = p - t2
+    d5 = (ab * cp).sum(1)
+    d6 = (ac * cp).sum(1)
+    va = d3 * d6 - d5 * d4
+    vb = d5 * d2 - d1 * d6
+    vc = d1 * d4 - d3 * d2
+    out = np.full(p.shape[0], 6, np.int32)
+    # evaluate regions in reverse priority so that the first match wins
+    e20 = (vb <= 0) & (d2 >= 0) & (d6 <= 0)
+    out[e20] = 5
+    e12 = (va <= 0) & ((d4 - d3) >= 0) & ((d5 - d6) >= 0)
+    out[e12] = 4
+    e01 = (vc <= 0) & (d1 >= 0) & (d3 <= 0)
+    out[e01] = 3
+    out[(d6 >= 0) & (d5 <= d6)] = 2
+    out[(d3 >= 0) & (d4 <= d3)] = 1
+    out[(d1 <= 0) & (d2 <= 0)] = 0
+    return out
+
+
+def ee_type(a0, a1, b0, b1):
+    """Closest features of segments (a0,a1) and (b0,b1).
+
+    Codes follow the reference's ``_dType_EE`` switch: 0 PP(a0,b0), 1 PP(a0,b1),
+    2 PE(a0; b0b1), 3 PP(a1,b0), 4 PP(a1,b1), 5 PE(a1; b0b1), 6 PE(b0; a0a1),
+    7 PE(b1; a0a1), 8 EE.
+    """
+    u = a1 - a0
+    v = b1 - b0
+    w = a0 - b0
+    a = (u * u).sum(1)
+    b = (u * v).sum(1)
+    c = (v * v).sum(1)
+    d = (u * w).sum(1)
+    e = (v * w).sum(1)
+    D = a * c - b * b
+    par = D < 1e-20 * a * c
+    sN = np.where(par, 0.0, b * e - c * d)
+    sD = np.where(par, 1.0, D)
+    tN = np.where(par, e, a * e - b * d)
+    tD = np.where(par, c, D)
+    s_at = np.full(a.shape, 1, np.int32)   # 0 = start, 1 = interior, 2 = end
+    s_at[par] = 0
+    neg = ~par & (sN <= 0)
+    sN = np.where(neg, 0.0, sN)
+    tN = np.where(neg, e, tN)
+    tD = np.where(neg, c, tD)
+    s_at[neg] = 0
+    big = ~par & ~neg & (sN >= sD)
+    sN = np.where(big, sD, sN)
+    tN = np.where(big, e + b, tN)
+    tD = np.where(big, c, tD)
+    s_at[big] = 2
+    t_at = np.ones(a.shape, np.int32)
+    tneg = tN <= 0
+    t_at[tneg] = 0
+    # re-derive s for clamped t
+    sN2 = np.where(tneg, -d, sN)
+    sD2 = np.where(tneg, a, sD)
+    tbig = ~tneg & (tN >= tD)
+    t_at[tbig] = 2
+    sN2 = np.where(tbig, -d + b, sN2)
+    sD2 = np.where(tbig, a, sD2)
+    clamp_t = tneg | tbig
+    s_at2 = s_at.copy()
+    s_at2[clamp_t & (sN2 <= 0)] = 0
+    s_at2[clamp_t & (sN2 >= sD2)] = 2
+    s_at2[clamp_t & (sN2 > 0) & (sN2 < sD2)] = 1
+    s_at = np.where(clamp_t, s_at2, s_at)
+    code = np.full(a.shape, 8, np.int32)
+    code[(s_at == 0) & (t_at == 0)] = 0
+    code[(s_at == 0) & (t_at == 2)] = 1
+    code[(s_at == 0) & (t_at == 1)] = 2
+    code[(s_at == 2) & (t_at == 0)] = 3
+    code[(s_at == 2) & (t_at == 2)] = 4
+    code[(s_at == 2) & (t_at == 1)] = 5
+    code[(s_at == 1) & (t_at == 0)] = 6
+    code[(s_at == 1) & (t_at == 2)] = 7
+    return code
+
+
+# squared distances by type (StiffGIPC/mlbvh.cu:229-262)
+def d_pp(a, b):
+    return ((a - b) ** 2).sum(1)
+
+
+def d_pe(p, e0, e1):
+    c = np.cross(e0 - p, e1 - p)
+    return (c * c).sum(1) / ((e1 - e0) ** 2).sum(1)
+
+
+def d_pt(p, t0, t1, t2):
+    n = np.cross(t1 - t0, t2 - t0)
+    s = ((p - t0) * n).sum(1)
+    return s * s / (n * n).sum(1)
+
+
+def d_ee(a0, a1, b0, b1):
+    n = np.cross(a1 - a0, b1 - b0)
+    s = ((b0 - a0) * n).sum(1)
+    return s * s / (n * n).sum(1)
+
+
+def eps_x(r0, r1, r2, r3):
+    """Mollifier threshold ``_compute_epx`` (StiffGIPC/mlbvh.cu:264-268)."""
+    return 1e-3 * ((r0 - r1) ** 2).sum(1) * ((r2 - r3) ** 2).sum(1)
+
+
+# ----------------------------------------------------------------------------------------
+# pair search
+# ----------------------------------------------------------------------------------------
+
+def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
+               inter_body_only=False):
+    """All barrier pairs with squared distance below ``dhat``, reference-encoded.
+
+    Returns an (P,4) int32 array ordered PT-derived pairs first, then EE-derived pairs.
+    """
+    out = []
+    if len(surf_tris) and len(surf_verts):
+        tri_c = x[surf_tris].mean(1)
+        tri_r = np.sqrt(((x[surf_tris] - tri_c[:, None]) ** 2).sum(2).max(1))
+        rq = float(tri_r.max()) + np.sqrt(dhat)
+        tree = cKDTree(tri_c)
+        nb = tree.query_ball_point(x[surf_verts], rq)
+        pi = np.repeat(surf_verts, [len(n) for n in nb])
+        ti = np.concatenate([np.asarray(n, np.int64) for n in nb]) if len(pi) else np.zeros(0, np.int64)
+        if len(pi):
+            t = surf_tris[ti]
+            keep = (t != pi[:, None]).all(1)
+            if inter_body_only and body is not None:
+                keep &= body[pi] != body[t[:, 0]]
+            pi, t = pi[keep], t[keep]
+            p, a, b, c = x[pi], x[t[:, 0]], x[t[:, 1]], x[t[:, 2]]
+            code = pt_type(p, a, b, c)
+            d = np.empty(len(pi))
+            m = code == 0; d[m] = d_pp(p[m], a[m])
+            m = code == 1; d[m] = d_pp(p[m], b[m])
+            m = code == 2; d[m] = d_pp(p[m], c[m])
+            m = code == 3; d[m] = d_pe(p[m], a[m], b[m])
+            m = code == 4; d[m] = d_pe(p[m], b[m], c[m])
+            m = code == 5; d[m] = d_pe(p[m], c[m], a[m])
+            m = code == 6; d[m] = d_pt(p[m], a[m], b[m], c[m])
+            hit = d < dhat
+            pi, t, code = pi[hit], t[hit], code[hit]
+            enc = np.full((len(pi), 4), -1, np.int64)
+            enc[:, 0] = -pi - 1
+            for k, (i1, i2, i3) in {0: (0, None, None), 1: (1, None, None), 2: (2, None, None),
+                                     3: (0, 1, None), 4: (1, 2, None), 5: (2, 0, None),
+                                     6: (0, 1, 2)}.items():
+                m = code == k
+                enc[m, 1] = t[m, i1]
+                if i2 is not None:
+                    enc[m, 2] = t[m, i2]
+                if i3 is not None:
+                    enc[m, 3] = t[m, i3]
+            # PT-derived point-point / point-edge pairs carry w = -1 (StiffGIPC/mlbvh.cu:560-640);
+            # like the reference, a point close to a shared vertex or edge of several
+            # triangles yields one pair per triangle
+            out.append(enc)
+    if len(surf_edges) > 1:
+        mid = x[surf_edges].mean(1)
+        hl = np.sqrt(((x[surf_edges[:, 0]] - x[surf_edges[:, 1]]) ** 2).sum(1)) * 0.5
+        tree = cKDTree(mid)
+        rq = 2.0 * float(hl.max()) + np.sqrt(dhat)
+        cand = tree.query_pairs(rq, output_type="ndarray")
+        if len(cand):
+            ea, eb = surf_edges[cand[:, 0]], surf_edges[cand[:, 1]]
+            keep = (ea[:, :, None] != eb[:, None, :]).all((1, 2))
+            if inter_body_only and body is not None:
+                keep &= body[ea[:, 0]] != body[eb[:, 0]]
+            ea, eb = ea[keep], eb[keep]
+            a0, a1, b0, b1 = x[ea[:, 0]], x[ea[:, 1]], x[eb[:, 0]], x[eb[:, 1]]
+            code = ee_type(a0, a1, b0, b1)
+            d = np.full(len(ea), np.inf)
+            m = code == 0; d[m] = d_pp(a0[m], b0[m])
+            m = code == 1; d[m] = d_pp(a0[m], b1[m])
+            m = code == 2; d[m] = d_pe(a0[m], b0[m], b1[m])
+            m = code == 3; d[m] = d_pp(a1[m], b0[m])
+            m = code == 4; d[m] = d_pp(a1[m], b1[m])
+            m = code == 5; d[m] = d_pe(a1[m], b0[m], b1[m])
+            m = code == 6; d[m] = d_pe(b0[m], a0[m], a1[m])
+            m = code == 7; d[m] = d_pe(b1[m], a0[m], a1[m])
+            m = code == 8; d[m] = d_ee(a0[m], a1[m], b0[m], b1[m])
+            hit = d < dhat
+            ea, eb, code = ea[hit], eb[hit], code[hit]
+            ep = eps_x(rest[ea[:, 0]], rest[ea[:, 1]], rest[eb[:, 0]], rest[eb[:, 1]])
+            cr = np.cross(x[ea[:, 0]] - x[ea[:, 1]], x[eb[:, 0]] - x[eb[:, 1]])
+            par = (cr * cr).sum(1) < ep
+            add_e = np.where(par, -2, -1)
+            enc = np.zeros((len(ea), 4), np.int64)
+            i0, i1, j0, j1 = ea[:, 0], ea[:, 1], eb[:, 0], eb[:, 1]
+            table = {0: (i0, j0, None), 1: (i0, j1, None), 2: (i0, j0, j1),
+                     3: (i1, j0, None), 4: (i1, j1, None), 5: (i1, j0, j1),
+                     6: (j0, i0, i1), 7: (j1, i0, i1)}
+            for k, (p, q, r) in table.items():
+                m = code == k
+                enc[m, 0] = -p[m] - 1
+                enc[m, 1] = q[m]
+                enc[m, 2] = -1 if r is None else r[m]
+                enc[m, 3] = add_e[m]
+            m = code == 8
+            enc[m] = np.stack([i0[m], i1[m], j0[m], j1[m]], 1)
+            out.append(enc)
+    if not out:
+        return np.zeros((0, 4), np.int32)
+    return np.concatenate(out, 0).astype(np.int32)
+
+
+def ground_pairs(x, surf_verts, dhat, offset=-1.0):
+    """``_GroundCollisionDetect`` (StiffGIPC/GIPC.cu:6420-6436): surface vertices within d-hat."""
+    d = x[surf_verts, 1] - offset
+    return surf_verts[d * d <= dhat].astype(np.int32)
+
+
+# ----------------------------------------------------------------------------------------
+# lagged friction (per frame)
+# ----------------------------------------------------------------------------------------
+
+def _barrier_lambda(d2, dhat, kappa):
+    """Normal-force magnitude of the RANK-2 barrier (StiffGIPC/GIPC.cu:8484-8491)."""
+    l = np.log(d2 / dhat)
+    return -kappa * 2.0 * np.sqrt(d2) * (l * l * (2 * d2 - 2 * dhat) + 2 * l * (d2 - dhat) ** 2 / d2)
+
+
+def lag_friction(x, pairs, gpairs, dhat, kappa, offset=-1.0):
+    """Lagged normal forces, closest-point coordinates and tangent bases of the pairs.
+
+    Restates ``_calFrictionLastH_DistAndTan`` and ``_calFrictionLastH_gd``
+    (StiffGIPC/GIPC.cu:8362-8499) and the tangent/closest-point helpers of
+    StiffGIPC/FrictionUtils.cuh:52-399.  Mollified pairs are skipped, as there.
+    """
+    lp, lam, coord, basis = [], [], [], []
+    for pr in pairs:
+        a, b, c, d = (int(v) for v in pr)
+        if a >= 0:
+            if d < 0:
+                continue
+            x0, x1, x2, x3 = x[a], x[b], x[c], x[d]
+            n = np.cross(x1 - x0, x3 - x2)
+            s = np.dot(x2 - x0, n)
+            d2 = s * s / np.dot(n, n)
+            e20, e01, e23 = x0 - x2, x1 - x0, x3 - x2
+            A = np.array([[e01 @ e01, -(e23 @ e01)], [-(e23 @ e01), e23 @ e23]])
+            r = np.array([-(e20 @ e01), e20 @ e23])
+            gam = np.linalg.solve(A, r)
+            t0 = e01 / np.linalg.norm(e01)
+            cc = np.cross(np.cross(e01, e23), e01)
+            bas = np.stack([t0, cc / np.linalg.norm(cc)], 1)
+        else:
+            p = -a - 1
+            if c < 0:
+                if b < 0:
+                    continue
+                x0, x1 = x[p], x[b]
+                d2 = np.dot(x0 - x1, x0 - x1)
+                gam = np.zeros(2)
+                v01 = x1 - x0
+                xc = np.array([0.0, -v01[2], v01[1]])
+                yc = np.array([v01[2], 0.0, -v01[0]])
+                t0 = xc if np.dot(xc, xc) > np.dot(yc, yc) else yc
+                t1 = np.cross(v01, t0)
+                bas = np.stack([t0 / np.linalg.norm(t0), t1 / np.linalg.norm(t1)], 1)
+            elif d < 0:
+                if b < 0:
+                    continue
+                x0, x1, x2 = x[p], x[b], x[c]
+                e12 = x2 - x1
+                d2 = np.dot(np.cross(x1 - x0, x2 - x0), np.cross(x1 - x0, x2 - x0)) / np.dot(e12, e12)
+                gam = np.array([np.dot(x0 - x1, e12) / np.dot(e12, e12), 0.0])
+                t0 = e12 / np.linalg.norm(e12)
+                t1 = np.cross(e12, x0 - x1)
+                bas = np.stack([t0, t1 / np.linalg.norm(t1)], 1)   # FrictionUtils.cuh:279-292
+            else:
+                x0, x1, x2, x3 = x[p], x[b], x[c], x[d]
+                n = np.cross(x2 - x1, x3 - x1)
+                s = np.dot(x0 - x1, n)
+                d2 = s * s / np.dot(n, n)
+                B = np.stack([x2 - x1, x3 - x1], 1)
+                gam = np.linalg.solve(B.T @ B, B.T @ (x0 - x1))
+                v12 = x2 - x1
+                cc = np.cross(np.cross(v12, x3 - x1), v12)
+                bas = np.stack([v12 / np.linalg.norm(v12), cc / np.linalg.norm(cc)], 1)
+        lp.append(pr)
+        lam.append(_barrier_lambda(d2, dhat, kappa))
+        coord.append(gam)
+        basis.append(bas)
+    gd = x[gpairs, 1] - offset if len(gpairs) else np.zeros(0)
+    d2g = gd * gd
+    t = d2g - dhat
+    gb = t * np.log(d2g / dhat) * -2.0 - (t * t) / d2g if len(gpairs) else np.zeros(0)
+    glam = -kappa * 2.0 * np.sqrt(d2g) * gb
+    if not lp:
+        return (np.zeros((0, 4), np.int32), np.zeros(0), np.zeros((0, 2)), np.zeros((0, 3, 2)),
+                gpairs.astype(np.int32), glam)
+    return (np.asarray(lp, np.int32), np.asarray(lam), np.asarray(coord), np.asarray(basis),
+            gpairs.astype(np.int32), glam)
+
+
+def attach_contacts(sc, inter_body_only: bool = False) -> None:
+    """Fill ``sc.pairs``, ``sc.ground_pairs`` and the lagged friction arrays in place."""
+    p = sc.params
+    sc.pairs = find_pairs(sc.vertexes, sc.rest_vertexes, sc.surf_tris, sc.surf_edges,
+                          sc.surf_verts, p["dHat"], sc.body_of_vertex, inter_body_only)
+    sc.ground_pairs = ground_pairs(sc.vertexes, sc.surf_verts, p["dHat"], p["ground_offset"])
+    if p.get("frictionRate", 0.0) > 0.0:
+        fp, fl, fc, fb, gp, gl = lag_friction(sc.o_vertexes, sc.pairs, sc.ground_pairs,
+                                              p["dHat"], p["kappa"], p["ground_offset"])
+        sc.fric_pairs, sc.fric_lambda, sc.fric_coord, sc.fric_basis = fp, fl, fc, fb
+        sc.fric_gd_pairs, sc.fric_gd_lambda = gp, gl

@@ -1,0 +1,280 @@
+"""Host-side mirror of StiffGIPC's Newton-system interfaces over the C ABI.
+
+Names follow the reference so that a caller of the reference finds the same entry
+points:
+
+* :class:`DeviceTetraData` — the SoA device arrays of ``device_TetraData``
+  (StiffGIPC/device_fem_data.cuh:17-78), held in torch CUDA tensors;
+* :class:`GIPC` — ``computeGradientAndHessian`` (GIPC.cu:10110),
+  ``calBarrierGradientAndHessian`` (GIPC.cu:9112), ``calFrictionGradientAndHessian``
+  (GIPC.cu:9164-9217) and ``calculateMovingDirection`` (GIPC.cu:10581);
+* :class:`MASPreconditioner` — ``setPreconditioner_bcoo`` / ``preconditioning``
+  (MASPreconditioner.cu:2180-2262);
+* :class:`PCGSolver` with :class:`PCGSolverConfig` (linear_system/solver/pcg_solver.h).
+
+Torch only provides device memory and the current stream; every computation is a call
+into ``libsgipc.so``.  Errors surface as :class:`sgipc._native.SgipcError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+
+def _dev():
+    if not torch.cuda.is_available():
+        raise RuntimeError("sgipc needs a CUDA device; there is no CPU path")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _t(a, dtype):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=_dev()).contiguous()
+
+
+def _p(t: Optional[torch.Tensor]):
+    return None if t is None or t.numel() == 0 else C.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class DeviceTetraData:
+    """Device copies of a :class:`sgipc.scenes.Scene`'s per-Newton arrays."""
+
+    def __init__(self, sc):
+        f64, i32 = torch.float64, torch.int32
+        self.vertexes = _t(sc.vertexes, f64)
+        self.o_vertexes = _t(sc.o_vertexes, f64)
+        self.rest_vertexes = _t(sc.rest_vertexes, f64)
+        self.xTilta = _t(sc.xTilta, f64)
+        self.masses = _t(sc.masses, f64)
+        self.BoundaryType = _t(sc.boundary_type, i32)
+        self.DmInverses = _t(sc.dm_inv.reshape(-1, 9), f64)
+        self.volum = _t(sc.volum, f64)
+        self.lengthRate = _t(sc.length_rate, f64)
+        self.volumeRate = _t(sc.volume_rate, f64)
+        self.triDmInverses = _t(sc.tri_dm_inv.reshape(-1, 4), f64)
+        self.area = _t(sc.area, f64)
+        self.quad_bending_Q = _t(np.transpose(sc.hinge_q, (0, 2, 1)).reshape(-1, 16), f64)
+        self.targetVert = _t(sc.soft_target.reshape(-1, 3), f64)
+        self.pairs = _t(sc.pairs.reshape(-1, 4), i32)
+        self.ground_pairs = _t(sc.ground_pairs, i32)
+        self.fric_pairs = _t(sc.fric_pairs.reshape(-1, 4), i32)
+        self.fric_lambda = _t(sc.fric_lambda, f64)
+        self.fric_coord = _t(sc.fric_coord.reshape(-1, 2), f64)
+        self.fric_basis = _t(sc.fric_basis.reshape(-1, 6), f64)
+        self.fric_gd_pairs = _t(sc.fric_gd_pairs, i32)
+        self.fric_gd_lambda = _t(sc.fric_gd_lambda, f64)
+
+    def fem_struct(self) -> N.SgipcFemData:
+        f = N.SgipcFemData()
+        for name in ("vertexes", "o_vertexes", "rest_vertexes", "xTilta", "masses", "BoundaryType", "DmInverses",
+                     "volum", "lengthRate", "volumeRate", "triDmInverses", "area", "quad_bending_Q", "targetVert"):
+            setattr(f, name, _p(getattr(self, name)))
+        return f
+
+    def contact_struct(self) -> N.SgipcContacts:
+        k = N.SgipcContacts()
+        k.pairs, k.pair_num = _p(self.pairs), self.pairs.shape[0]
+        k.ground_pairs, k.ground_num = _p(self.ground_pairs), self.ground_pairs.shape[0]
+        k.fric_pairs, k.fric_num = _p(self.fric_pairs), self.fric_pairs.shape[0]
+        k.fric_lambda, k.fric_coord, k.fric_basis = _p(self.fric_lambda), _p(self.fric_coord), _p(self.fric_basis)
+        k.fric_gd_pairs, k.fric_gd_num = _p(self.fric_gd_pairs), self.fric_gd_pairs.shape[0]
+        k.fric_gd_lambda = _p(self.fric_gd_lambda)
+        return k
+
+
+@dataclasses.dataclass
+class PCGSolverConfig:
+    """``PCGSolverConfig`` (linear_system/solver/pcg_solver.h:8-18)."""
+
+    max_iter_ratio: float = 0.3
+    global_tol_rate: float = 1e-4
+    precision: str = "fp64"       # "fp64" | "mixed" | "ref"
+    criterion: int = N.CRIT_RZ
+
+
+def params_struct(p: dict) -> N.SgipcParams:
+    s = N.SgipcParams()
+    for name, _ in N.SgipcParams._fields_:
+        setattr(s, name, float(p.get(name, 0.0)))
+    return s
+
+
+class GIPC:
+    """One Newton system on the GPU (context = static BSR pattern + MAS + PCG workspaces)."""
+
+    def __init__(self, sc, device: Optional[int] = None, max_rhs: int = 4, pair_capacity: Optional[int] = None):
+        self.scene = sc
+        dev = torch.cuda.current_device() if device is None else device
+        torch.cuda.set_device(dev)
+        L = N.lib()
+        self._host = []
+        t = N.SgipcTopology()
+        t.vertex_num, t.tet_num = sc.nv, sc.nt
+        t.tri_num, t.tri_edge_num, t.soft_num = len(sc.tris), len(sc.hinges), len(sc.soft_index)
+        t.tetrahedras = self._hp(sc.tets, np.uint32)
+        t.triangles = self._hp(sc.tris, np.uint32)
+        t.tri_edges = self._hp(sc.hinges, np.uint32)
+        t.tri_edge_adj_vertex = self._hp(sc.hinge_adj, np.int32)
+        t.targetIndex = self._hp(sc.soft_index, np.uint32)
+        t.part_map_size = len(sc.part_map_real)
+        t.partId_map_real = self._hp(sc.part_map_real, np.int32)
+        t.real_map_partId = self._hp(sc.real_map_part, np.int32)
+        t.neighborStart = self._hp(sc.nbr_start, np.uint32)
+        t.neighborList = self._hp(sc.nbr_list, np.uint32)
+        cap = pair_capacity if pair_capacity is not None else max(len(sc.pairs), 1)
+        t.max_pairs = cap
+        t.max_ground = max(len(sc.ground_pairs), len(sc.surf_verts))
+        t.max_fric_pairs = max(len(sc.fric_pairs), cap)
+        t.max_fric_ground = max(len(sc.fric_gd_pairs), len(sc.surf_verts))
+        t.max_rhs = max_rhs
+        h = C.c_void_p()
+        N.check(L.sgipc_create(C.byref(t), dev, C.byref(h)))
+        self.ctx = h
+        self._host = None
+        self.tet = DeviceTetraData(sc)
+        self.params = dict(sc.params)
+        self.n = sc.nv
+        self.moveDir = torch.zeros(3 * sc.nv, dtype=torch.float64, device=_dev())
+
+    def _hp(self, a, dt):
+        a = np.ascontiguousarray(a, dt)
+        self._host.append(a)
+        return None if a.size == 0 else a.ctypes.data_as(C.c_void_p)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            N.lib().sgipc_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- assembly -------------------------------------------------------------------
+    def computeGradientAndHessian(self, tet: Optional[DeviceTetraData] = None):
+        tet = tet or self.tet
+        self._fem, self._con, self._prm = tet.fem_struct(), tet.contact_struct(), params_struct(self.params)
+        N.check(N.lib().sgipc_assemble(self.ctx, C.byref(self._fem), C.byref(self._con), C.byref(self._prm),
+                                       _stream()), self.ctx)
+
+    def calBarrierGradientAndHessian(self, grad: torch.Tensor, tet: Optional[DeviceTetraData] = None):
+        tet = tet or self.tet
+        f, k, p = tet.fem_struct(), tet.contact_struct(), params_struct(self.params)
+        N.check(N.lib().sgipc_barrier_grad_hess(self.ctx, C.byref(f), C.byref(k), C.byref(p), _p(grad), _stream()),
+                self.ctx)
+
+    def calFrictionGradientAndHessian(self, grad: torch.Tensor, tet: Optional[DeviceTetraData] = None):
+        tet = tet or self.tet
+        f, k, p = tet.fem_struct(), tet.contact_struct(), params_struct(self.params)
+        N.check(N.lib().sgipc_friction_grad_hess(self.ctx, C.byref(f), C.byref(k), C.byref(p), _p(grad), _stream()),
+                self.ctx)
+
+    def calculate_fem_gradient_hessian(self, grad: torch.Tensor, tet: Optional[DeviceTetraData] = None):
+        tet = tet or self.tet
+        f, p = tet.fem_struct(), params_struct(self.params)
+        N.check(N.lib().sgipc_fem_grad_hess(self.ctx, C.byref(f), C.byref(p), _p(grad), _stream()), self.ctx)
+
+    def rhs(self) -> torch.Tensor:
+        b = torch.empty(3 * self.n, dtype=torch.float64, device=_dev())
+        N.check(N.lib().sgipc_get_rhs(self.ctx, _p(b), _stream()), self.ctx)
+        return b
+
+    def export_bcoo(self):
+        cnt = C.c_int32()
+        N.check(N.lib().sgipc_export_bcoo(self.ctx, 0, None, None, None, C.byref(cnt)), self.ctx)
+        n = cnt.value
+        rows, cols = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        vals = np.zeros((n, 3, 3))
+        N.check(N.lib().sgipc_export_bcoo(self.ctx, n, rows.ctypes.data_as(C.c_void_p),
+                                          cols.ctypes.data_as(C.c_void_p), vals.ctypes.data_as(C.c_void_p),
+                                          C.byref(cnt)), self.ctx)
+        return rows, cols, vals
+
+    def spmv(self, x: torch.Tensor) -> torch.Tensor:
+        y = torch.empty_like(x)
+        N.check(N.lib().sgipc_spmv(self.ctx, _p(x), _p(y), _stream()), self.ctx)
+        return y
+
+    # ---- solve ----------------------------------------------------------------------
+    def calculateMovingDirection(self, config: Optional[PCGSolverConfig] = None,
+                                 tet: Optional[DeviceTetraData] = None):
+        """MAS build + PCG; fills ``self.moveDir`` (dx of A dx = b) and returns the stats."""
+        config = config or PCGSolverConfig()
+        tet = tet or self.tet
+        con = tet.contact_struct()
+        st = N.SgipcSolveStats()
+        prec = N.PRECISION[config.precision]
+        max_iter = int(config.max_iter_ratio * 3 * self.n)
+        s = N.lib().sgipc_solve(self.ctx, C.byref(con), prec, config.criterion, config.global_tol_rate, max_iter,
+                                _p(self.moveDir), C.byref(st), _stream())
+        N.check(s, self.ctx, allow=(N.OK, N.NOT_CONVERGED))
+        return st
+
+
+class MASPreconditioner:
+    """``MASPreconditioner`` over a :class:`GIPC` context's assembled matrix."""
+
+    def __init__(self, gipc: GIPC):
+        self.g = gipc
+
+    def setPreconditioner(self, precision: str = "fp64", tet: Optional[DeviceTetraData] = None):
+        con = (tet or self.g.tet).contact_struct()
+        N.check(N.lib().sgipc_mas_build(self.g.ctx, C.byref(con), N.PRECISION[precision], _stream()), self.g.ctx)
+
+    def preconditioning(self, R: torch.Tensor, Z: Optional[torch.Tensor] = None) -> torch.Tensor:
+        Z = torch.empty_like(R) if Z is None else Z
+        N.check(N.lib().sgipc_mas_apply(self.g.ctx, _p(R), _p(Z), _stream()), self.g.ctx)
+        return Z
+
+    def info(self):
+        ln, tot = C.c_int32(), C.c_int32()
+        counts = (C.c_int32 * 8)()
+        N.check(N.lib().sgipc_mas_info(self.g.ctx, C.byref(ln), counts, C.byref(tot)), self.g.ctx)
+        return ln.value, np.array(counts[:ln.value]), tot.value
+
+    def tables(self):
+        L = self.info()[0]
+        t = np.zeros(self.g.n * L, np.int32)
+        N.check(N.lib().sgipc_mas_export_tables(self.g.ctx, t.ctypes.data_as(C.c_void_p)), self.g.ctx)
+        return t.reshape(self.g.n, L)
+
+
+class PCGSolver:
+    """``PCGSolver::solve(x, b)`` on a :class:`GIPC` context (MAS must be set)."""
+
+    def __init__(self, gipc: GIPC, config: Optional[PCGSolverConfig] = None):
+        self.g = gipc
+        self.config = config or PCGSolverConfig()
+
+    def solve(self, b: torch.Tensor, x: Optional[torch.Tensor] = None):
+        x = torch.empty_like(b) if x is None else x
+        st = N.SgipcSolveStats()
+        cfg = self.config
+        max_iter = int(cfg.max_iter_ratio * 3 * self.g.n)
+        s = N.lib().sgipc_pcg_solve(self.g.ctx, N.PRECISION[cfg.precision], cfg.criterion, cfg.global_tol_rate,
+                                    max_iter, _p(b), _p(x), C.byref(st), _stream())
+        N.check(s, self.g.ctx, allow=(N.OK, N.NOT_CONVERGED))
+        return x, st
+
+    def solve_batched(self, B: torch.Tensor, X: Optional[torch.Tensor] = None):
+        """B: (nrhs, 3n) float64 CUDA tensor; returns X and the per-rhs stats."""
+        nrhs = B.shape[0]
+        X = torch.empty_like(B) if X is None else X
+        st = (N.SgipcSolveStats * nrhs)()
+        cfg = self.config
+        max_iter = int(cfg.max_iter_ratio * 3 * self.g.n)
+        s = N.lib().sgipc_pcg_solve_batched(self.g.ctx, N.PRECISION[cfg.precision], cfg.criterion,
+                                            cfg.global_tol_rate, max_iter, nrhs, _p(B), _p(X), st, _stream())
+        N.check(s, self.g.ctx, allow=(N.OK, N.NOT_CONVERGED))
+        return X, list(st)

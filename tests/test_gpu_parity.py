@@ -1,0 +1,169 @@
+"""GPU parity: every CUDA path through the C ABI against the CPU oracle.
+
+Tolerances (FP64 unless stated):
+  * assembled blocks and right-hand side: 1e-9 of the largest entry (same formulas,
+    different evaluation order: analytic SNK eigensystem vs numeric projection, hand
+    derivatives vs dual numbers);
+  * SpMV: 1e-12 relative;
+  * MAS hierarchy: identical integer tables; MAS apply: 1e-9 (FP64), 2e-5 (FP32 inverses);
+  * PCG: same iteration count within 1, solution within 1e-6 relative of the oracle's.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover - CPU container
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from sgipc import scenes, system  # noqa: E402
+from sgipc import _native as N  # noqa: E402
+
+
+@pytest.fixture(scope="module", params=["cube_touch", "two_cubes"])
+def case(request):
+    if request.param == "cube_touch":
+        sc = scenes.scene_cube(6, touching=True, seed=3)
+    else:
+        sc = scenes.scene_two_cubes(7, seed=5)
+    g = system.GIPC(sc)
+    g.computeGradientAndHessian()
+    torch.cuda.synchronize()
+    ob, orow, ocol, oval, _ = oracle.assemble(sc)
+    yield sc, g, (ob, orow, ocol, oval)
+    g.close()
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def test_assembly_blocks(case):
+    sc, g, (ob, orow, ocol, oval) = case
+    rows, cols, vals = g.export_bcoo()
+    assert np.array_equal(rows, orow) and np.array_equal(cols, ocol)
+    assert _rel(vals, oval) < 1e-9
+
+
+def test_rhs(case):
+    sc, g, (ob, *_r) = case
+    b = g.rhs().cpu().numpy()
+    assert _rel(b, ob) < 1e-9
+
+
+def test_spmv(case):
+    sc, g, (ob, orow, ocol, oval) = case
+    x = np.random.default_rng(0).normal(size=3 * sc.nv)
+    y = g.spmv(torch.tensor(x, device="cuda")).cpu().numpy()
+    assert _rel(y, oracle.spmv(orow, ocol, oval, sc.nv, x)) < 1e-12
+
+
+def test_mas_hierarchy_and_apply(case):
+    sc, g, (ob, orow, ocol, oval) = case
+    mas = system.MASPreconditioner(g)
+    mas.setPreconditioner("fp64")
+    om = oracle.Mas(sc, orow, ocol, oval)
+    L, starts, counts, total = om.info()
+    gl, gcounts, gtotal = mas.info()
+    assert gl == L and gtotal == total and np.array_equal(gcounts, counts)
+    assert np.array_equal(mas.tables(), om.table())
+    r = np.random.default_rng(1).normal(size=3 * sc.nv)
+    z = mas.preconditioning(torch.tensor(r, device="cuda")).cpu().numpy()
+    assert _rel(z, om.apply(r)) < 1e-9
+    mas.setPreconditioner("ref")
+    z32 = mas.preconditioning(torch.tensor(r, device="cuda")).cpu().numpy()
+    assert _rel(z32, om.apply(r, single=True)) < 2e-5
+
+
+def test_pcg_fp64_matches_oracle(case):
+    sc, g, (ob, orow, ocol, oval) = case
+    mas = system.MASPreconditioner(g)
+    mas.setPreconditioner("fp64")
+    om = oracle.Mas(sc, orow, ocol, oval)
+    ox, oit, orz0, orz = oracle.pcg(orow, ocol, oval, sc.nv, om, ob, 1e-4)
+    solver = system.PCGSolver(g, system.PCGSolverConfig(precision="fp64"))
+    x, st = solver.solve(g.rhs())
+    x = x.cpu().numpy()
+    assert st.status == N.OK
+    assert abs(st.iterations - oit) <= 1
+    assert abs(st.rz0 - orz0) <= 1e-9 * abs(orz0)
+    if st.iterations == oit:
+        assert _rel(x, ox) < 1e-6
+
+
+def test_mixed_and_ref_meet_criterion(case):
+    sc, g, (ob, orow, ocol, oval) = case
+    A = oracle.dense(orow, ocol, oval, sc.nv)
+    exact = np.linalg.solve(A, ob)
+    for prec in ("mixed", "ref"):
+        mas = system.MASPreconditioner(g)
+        mas.setPreconditioner(prec)
+        solver = system.PCGSolver(g, system.PCGSolverConfig(precision=prec))
+        x, st = solver.solve(g.rhs())
+        x = x.cpu().numpy()
+        assert st.status == N.OK, prec
+        assert abs(st.rz) <= 1e-4 * st.rz0 * 1.0001, prec
+        res = np.linalg.norm(ob - A @ x) / np.linalg.norm(ob)
+        assert abs(res - st.rel_residual) < 1e-6 * max(1.0, res)
+        # the 1e-4 r.z criterion leaves about a 1e-2 relative error in x
+        assert np.linalg.norm(x - exact) / np.linalg.norm(exact) < 0.1
+
+
+def test_tight_mixed_matches_fp64(case):
+    sc, g, (ob, orow, ocol, oval) = case
+    A = oracle.dense(orow, ocol, oval, sc.nv)
+    exact = np.linalg.solve(A, ob)
+    for prec in ("fp64", "mixed"):
+        mas = system.MASPreconditioner(g)
+        mas.setPreconditioner(prec)
+        cfg = system.PCGSolverConfig(precision=prec, global_tol_rate=1e-9, criterion=N.CRIT_TRUE, max_iter_ratio=1.0)
+        x, st = system.PCGSolver(g, cfg).solve(g.rhs())
+        err = np.linalg.norm(x.cpu().numpy() - exact) / np.linalg.norm(exact)
+        assert st.status == N.OK and err < 1e-6, (prec, err, st.iterations, st.refinements)
+
+
+def test_solve_entry_point(case):
+    sc, g, (ob, orow, ocol, oval) = case
+    st = g.calculateMovingDirection(system.PCGSolverConfig(precision="fp64"))
+    assert st.status == N.OK and st.iterations > 0
+    A = oracle.dense(orow, ocol, oval, sc.nv)
+    dx = g.moveDir.cpu().numpy()
+    assert np.linalg.norm(ob - A @ dx) / np.linalg.norm(ob) == pytest.approx(st.rel_residual, rel=1e-6, abs=1e-12)
+
+
+def test_batched_four_rhs(case):
+    sc, g, (ob, orow, ocol, oval) = case
+    rng = np.random.default_rng(7)
+    B = rng.normal(size=(4, 3 * sc.nv)) * np.abs(ob).max()
+    for prec in ("fp64", "mixed", "ref"):
+        mas = system.MASPreconditioner(g)
+        mas.setPreconditioner(prec)
+        cfg = system.PCGSolverConfig(precision=prec, global_tol_rate=1e-10, criterion=N.CRIT_TRUE,
+                                     max_iter_ratio=1.0)
+        X, sts = system.PCGSolver(g, cfg).solve_batched(torch.tensor(B, device="cuda"))
+        A = oracle.dense(orow, ocol, oval, sc.nv)
+        tol = 1e-8 if prec != "mixed" else 1e-4
+        for r in range(4):
+            res = np.linalg.norm(B[r] - A @ X[r].cpu().numpy()) / np.linalg.norm(B[r])
+            assert res < max(tol, 1e-9), (prec, r, res, sts[r].iterations)
+
+
+def test_bad_inputs_are_reported(case):
+    sc, g, _ = case
+    L = N.lib()
+    prm = system.params_struct(g.params)
+    f = g.tet.fem_struct()
+    assert L.sgipc_assemble(g.ctx, None, None, None, None) == N.BAD_INPUT
+    bad = dict(g.params)
+    bad["dHat"] = -1.0
+    pb = system.params_struct(bad)
+    assert L.sgipc_assemble(g.ctx, f, None, pb, None) == N.BAD_INPUT
+    k = g.tet.contact_struct()
+    k.pair_num = 10 ** 7
+    assert L.sgipc_assemble(g.ctx, f, k, prm, None) == N.CAPACITY
+    # the context stays usable
+    g.computeGradientAndHessian()
+    torch.cuda.synchronize()
