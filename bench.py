@@ -1,0 +1,296 @@
+#!/usr/bin/env python
+"""Newton-system throughput on B200: assembly + MAS build + PCG of one implicit-step
+Newton iteration (StiffGIPC's per-iteration linear system), mixed FP32-MAS / FP64
+refinement vs plain FP64, plus adjoints/s.
+
+Workload (N=1): two stacked soft cubes, each a 21^3 vertex lattice (2 x 40000 tets,
+18522 vertices), E = 1e5 / 1e6 Pa, nu = 0.45, friction mu = 0.2, d-hat = 1e-3 m, top
+cube with a seeded 1 m/s initial velocity; seeded synthetic positions (uniform 1e-4 m
+perturbation).  A step = one Newton system: assembly, MAS hierarchy + inverses, PCG to
+the reference criterion r.z <= 1e-4 r0.z0.  Multi-GPU runs are independent replicas.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "stiff-gipc_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Newton-system solves/s, mixed vs FP64 MAS-PCG at 1e-4 residual; adjoints/s"
+WORKLOAD = ("two stacked soft cubes, 2 x 21^3 lattice (80000 tets, 18522 vertices), E 1e5/1e6 Pa, nu 0.45, "
+            "mu 0.2, d-hat 1e-3 m; one Newton system = assembly + MAS build + PCG to r.z <= 1e-4 r0.z0")
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=21, help="lattice vertices per cube edge")
+    ap.add_argument("--cpu-sample", type=int, default=0, help="CPU baseline solves (0 = auto, about 10 s)")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Per-launch DRAM bytes from an ncu capture (profiles/traffic.json), if committed."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.gpu = gpu_index
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(gpu_index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, power, reasons = [], None, [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        loaded = [s for s, p in zip(sm, power) if p > 200.0] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm), "samples_under_load": len(loaded)}
+
+
+# ------------------------------------------------------------------------------------------
+# CPU arms (oracle = CPU FP64 restatement of the reference's formulas)
+# ------------------------------------------------------------------------------------------
+def cpu_solves(sc, count):
+    import oracle
+
+    t0 = time.perf_counter()
+    for _ in range(count):
+        b, r, c, v, _ = oracle.assemble(sc)
+        m = oracle.Mas(sc, r, c, v)
+        oracle.pcg(r, c, v, sc.nv, m, b, 1e-4, single=True)
+        del m
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    from sgipc import scenes
+
+    sc = scenes.scene_two_cubes(args.n, seed=1)
+    for _ in range(args.warmup):
+        cpu_solves(sc, 1)
+    times = []
+    for _ in range(args.steps):
+        times.append(cpu_solves(sc, 1))
+    total = sum(times)
+    value = args.steps / total
+    out = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice scenes)",
+           "impl": "reference",
+           "config": {"workload": WORKLOAD, "solver": "reference PCG, FP64 matrix/vectors, FP32 MAS inverses"},
+           "cpu_baseline": {"value": value, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
+                            "sample": "%d full Newton systems of the workload (assembly + MAS + PCG), %d OpenMP threads"
+                                      % (args.steps, oracle.num_threads())},
+           "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from sgipc import adjoint, scenes, system
+    from sgipc import _native as N
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sc = scenes.scene_two_cubes(args.n, seed=1)
+    g = system.GIPC(sc, device=local, max_rhs=4)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    cfg = {p: system.PCGSolverConfig(precision=p) for p in ("mixed", "fp64")}
+    stream = torch.cuda.current_stream()
+
+    def step(prec):
+        g.computeGradientAndHessian()
+        return g.calculateMovingDirection(cfg[prec])
+
+    def timed(fn, k):
+        """Sum of per-step CUDA-event times; L2 flushed between steps (outside the events)."""
+        tot, last = 0.0, None
+        for _ in range(k):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            last = fn()
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1) / 1e3
+        return tot, last
+
+    for p in ("mixed", "fp64"):
+        for _ in range(max(3, args.warmup)):
+            step(p)
+    host = system.HostNewtonState(sc)
+    rng = torch.Generator(device="cpu").manual_seed(2)
+    dLdx = torch.empty((4, 3 * sc.nv), dtype=torch.float64).uniform_(-1e-3, 1e-3, generator=rng).cuda()
+
+    def adj_step():
+        g.computeGradientAndHessian()
+        return adjoint.adjoint(g, dLdx, precision="mixed", tol=1e-4, criterion=N.CRIT_RZ)
+
+    for _ in range(max(3, args.warmup)):
+        system.step_from_host(g, host, cfg["mixed"])
+        adj_step()
+
+    clocks = ClockSampler(local)
+    barrier()
+    l0 = g.launch_count()
+    t_mixed, st_mixed = timed(lambda: step("mixed"), args.steps)
+    launches = g.launch_count() - l0
+    t_fp64, st_fp64 = timed(lambda: step("fp64"), args.steps)
+    t_e2e, _ = timed(lambda: system.step_from_host(g, host, cfg["mixed"]), args.steps)
+    t_adj, adj_out = timed(adj_step, args.steps)
+    barrier()
+    clk = clocks.stop()
+
+    times = torch.tensor([t_mixed, t_fp64, t_e2e, t_adj], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    t_mixed, t_fp64, t_e2e, t_adj = times.tolist()
+    units = world * args.steps
+
+    # roofline of the dominant kernel: per-step share = avg launch time x launches per step
+    step("mixed")
+    torch.cuda.synchronize()
+    it = st_mixed.iterations
+    per_step = {"snk": 1, "gather_blocks": 1, "barrier": 1, "friction": 1, "mas_scatter": 1, "mas_invert": 1,
+                "spmv32": it, "mas_domain32": it + 2 * max(1, st_mixed.refinements)}
+    kern = {}
+    for name, cnt in per_step.items():
+        try:
+            ms, by = g.time_kernel(name, 20)
+            kern[name] = {"ms": ms, "bytes": by, "per_step": cnt, "ms_per_step": ms * cnt}
+        except Exception as e:  # a kernel not used by this scene
+            kern[name] = {"error": str(e)}
+    valid = {k: v for k, v in kern.items() if "ms" in v}
+    dom = max(valid, key=lambda k: valid[k]["ms_per_step"])
+    peak, peak_src = peaks()
+    ach = valid[dom]["bytes"] / (valid[dom]["ms"] * 1e-3) / 1e9
+    traffic = traffic_table().get(dom)
+
+    out = {"metric": METRIC, "value": units / t_mixed, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
+           "data": "synthetic (seeded lattice scenes, contacts from the host pair generator)",
+           "config": {"workload": WORKLOAD, "parallelism": "replicas x%d" % world,
+                      "l2": "flushed (256 MiB write) between timed steps",
+                      "solver_mixed": "FP32 BSR + FP32 MAS inner PCG, FP64 residual refinement",
+                      "pcg_iters_mixed": st_mixed.iterations, "refinements_mixed": st_mixed.refinements,
+                      "pcg_iters_fp64": st_fp64.iterations,
+                      "rel_residual_mixed": st_mixed.rel_residual, "rel_residual_fp64": st_fp64.rel_residual},
+           "fp64": {"value": units / t_fp64, "unit": "solves/s", "ms_per_step": 1e3 * t_fp64 / args.steps},
+           "mixed_over_fp64": t_fp64 / t_mixed,
+           "adjoints": {"value": units / t_adj, "unit": "adjoints/s (4 right-hand sides each)",
+                        "ms_per_step": 1e3 * t_adj / args.steps},
+           "e2e": {"value": units / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": host.h2d_bytes(),
+                   "d2h_bytes_per_step": host.d2h_bytes()},
+           "gpu_launches": int(launches),
+           "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "peak_source": peak_src,
+                        "unit": "GB/s", "frac": ach / peak, "traffic": traffic,
+                        "bytes_per_launch": valid[dom]["bytes"], "launch_ms": valid[dom]["ms"]},
+           "kernels": {k: {kk: (round(vv, 6) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                       for k, v in kern.items()},
+           "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
+
+        nsol = args.cpu_sample or 0
+        if nsol <= 0:
+            one = cpu_solves(sc, 1)
+            nsol = max(1, min(20, int(10.0 / max(one, 1e-3))))
+        t_cpu = cpu_solves(sc, nsol)
+        out["cpu_baseline"] = {"value": nsol / t_cpu, "unit": "solves/s", "cores": oracle.num_threads(),
+                               "kind": "port", "sample": "%d full Newton systems of the workload" % nsol}
+    g.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -232,6 +232,23 @@ SgipcStatus sgipc_adjoint_param_grads(SgipcCtx* ctx, const SgipcFemData* fem,
                                       const double* lambda, double* dLdE, double* dLdv0,
                                       void* stream);
 
+/* ---- instrumentation (the reference's gipc::Timer / cudaEvent phase timers,
+ *      StiffGIPC/gipc/utils/timer.h:19-136, GIPC.cu:10854-10964) ----------------------- */
+
+/* Number of this library's kernels launched on the context since creation (library
+ * kernels such as CUB sorts excluded; graph-resident PCG iterations counted by the
+ * iteration bodies they executed).  Synchronises. */
+SgipcStatus sgipc_launch_count(SgipcCtx* ctx, int64_t* launches);
+
+/* Re-launch one hot kernel `reps` times on `stream` against the context's current state,
+ * bracketed by CUDA events on that stream, and return its average duration [ms] and the
+ * algorithmic bytes one launch must move.  Names: "snk", "gather_blocks", "barrier",
+ * "friction", "spmv64", "spmv32", "mas_scatter", "mas_invert", "mas_domain64",
+ * "mas_domain32".  Leaves the assembled system and the MAS state as they were (the
+ * MAS kernels rebuild what they overwrite).  Synchronises. */
+SgipcStatus sgipc_time_kernel(SgipcCtx* ctx, const char* name, int32_t reps, void* stream,
+                              float* avg_ms, double* bytes_per_launch);
+
 #ifdef __cplusplus
 }
 #endif

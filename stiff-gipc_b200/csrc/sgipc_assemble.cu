@@ -673,6 +673,8 @@ static int launch_contacts(SgipcCtx* c, const SgipcFemData* f, const SgipcContac
                            double* grad, cudaStream_t s) {
     BlockSink bs = sink(c, f);
     int base = 0;
+    if (k) SG_COUNT(c, (k->pair_num > 0) + (k->fric_num > 0 && p->frictionRate > 0.0) + (k->ground_num > 0) +
+                           (k->fric_gd_num > 0 && p->gd_frictionRate > 0.0));
     if (k && k->pair_num > 0) {
         k_barrier<<<nblk(k->pair_num, 128), 128, 0, s>>>(k->pair_num, (const int4*)k->pairs, f->vertexes,
                                                           f->rest_vertexes, p->dHat, p->kappa, grad, bs, base);
@@ -707,6 +709,7 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
         return SGIPC_OK;
     }
     const int endbit = 2 * c->key_bits;
+    SG_COUNT(c, 5);
     size_t tb = c->cub_tmp_bytes;
     SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->ckey, c->ckey_s, c->cidx, c->cidx_s, m, 0, endbit, s));
     k_head_flags<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cflag);
@@ -725,6 +728,7 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
 
 static SgipcStatus launch_fem(SgipcCtx* c, const SgipcFemData* f, const SgipcParams* p, cudaStream_t s) {
     if (c->nt > 0) {
+        SG_COUNT(c, 1);
         k_snk<<<nblk(c->nt, 128), 128, 0, s>>>(c->nt, c->tets, f->vertexes, f->DmInverses, f->volum, f->lengthRate,
                                                f->volumeRate, p->dt * p->dt, c->eblk, c->egrad);
     }
@@ -733,6 +737,7 @@ static SgipcStatus launch_fem(SgipcCtx* c, const SgipcFemData* f, const SgipcPar
 }
 
 static SgipcStatus gather_static(SgipcCtx* c, const SgipcFemData* f, cudaStream_t s) {
+    SG_COUNT(c, 1 + (c->n_egrad > 0));
     k_gather_blocks<<<nblk(9LL * c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->contrib_ptr, c->contrib, c->eblk, c->slot_row,
                                                                 c->col, f->BoundaryType, f->masses, c->val64, c->val32);
     if (c->n_egrad > 0)
@@ -748,6 +753,11 @@ extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const 
     cudaStream_t s = (cudaStream_t)stream;
     SG_CHECK(c, cudaSetDevice(c->device));
     c->btype = f->BoundaryType;
+    c->last_fem = *f;
+    c->last_prm = *p;
+    c->last_has_con = k != nullptr;
+    if (k) c->last_con = *k;
+    SG_COUNT(c, 2 + (c->nsoft > 0));
     k_kinetic<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, f->vertexes, f->xTilta, f->masses, c->shape_grads, c->fb);
     int m = launch_contacts(c, f, k, p, c->fb, s);
     if (c->nsoft > 0) {
@@ -810,3 +820,50 @@ extern "C" SgipcStatus sgipc_fem_grad_hess(SgipcCtx* c, const SgipcFemData* f, c
     SG_LAUNCH_CHECK(c, "fem gradient");
     return SGIPC_OK;
 }
+
+// ------------------------------------------------------------------------------------------
+// timing hook
+// ------------------------------------------------------------------------------------------
+namespace sgipc {
+SgipcStatus assemble_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double* bytes) {
+    const SgipcFemData* f = &c->last_fem;
+    const SgipcParams* p = &c->last_prm;
+    const SgipcContacts* k = c->last_has_con ? &c->last_con : nullptr;
+    double* scratch = c->tmp64b;  // gradient sink that keeps fb untouched
+    if (!strcmp(name, "snk")) {
+        if (c->nt <= 0) return SGIPC_BAD_INPUT;
+        SG_COUNT(c, 1);
+        k_snk<<<nblk(c->nt, 128), 128, 0, s>>>(c->nt, c->tets, f->vertexes, f->DmInverses, f->volum, f->lengthRate,
+                                               f->volumeRate, p->dt * p->dt, c->eblk, c->egrad);
+        // positions, DmInv, volume, (mu, lambda), indices in; 10 FP64 blocks and 4 gradient rows out
+        *bytes = (double)c->nt * (4 * 24 + 72 + 8 + 16 + 16 + 10 * 72 + 12 * 8);
+    } else if (!strcmp(name, "gather_blocks")) {
+        SG_COUNT(c, 1);
+        k_gather_blocks<<<nblk(9LL * c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->contrib_ptr, c->contrib, c->eblk,
+                                                                    c->slot_row, c->col, f->BoundaryType, f->masses,
+                                                                    c->val64, c->val32);
+        *bytes = (double)c->n_eblk * (72 + 4) + (double)c->nnz * (72 + 36 + 8 + 4);
+    } else if (!strcmp(name, "barrier")) {
+        if (!k || k->pair_num <= 0) return SGIPC_BAD_INPUT;
+        SG_COUNT(c, 1);
+        BlockSink bs = sink(c, f);
+        k_barrier<<<nblk(k->pair_num, 128), 128, 0, s>>>(k->pair_num, (const int4*)k->pairs, f->vertexes,
+                                                          f->rest_vertexes, p->dHat, p->kappa, scratch, bs, 0);
+        // pair + 4 positions (+ 4 rest positions) in; 10 keyed FP64 blocks and 12 gradient entries out
+        *bytes = (double)k->pair_num * (16 + 4 * 24 + 4 * 24 + 10 * (72 + 8 + 4) + 12 * 8);
+    } else if (!strcmp(name, "friction")) {
+        if (!k || k->fric_num <= 0) return SGIPC_BAD_INPUT;
+        SG_COUNT(c, 1);
+        BlockSink bs = sink(c, f);
+        k_friction<<<nblk(k->fric_num, 128), 128, 0, s>>>(k->fric_num, (const int4*)k->fric_pairs, f->vertexes,
+                                                           f->o_vertexes, k->fric_lambda, k->fric_coord, k->fric_basis,
+                                                           p->frictionRate, p->fDhat * p->dt * p->dt, scratch, bs,
+                                                           10 * (k->pair_num > 0 ? k->pair_num : 0));
+        *bytes = (double)k->fric_num * (16 + 8 + 16 + 48 + 8 * 24 + 10 * (72 + 8 + 4) + 12 * 8);
+    } else {
+        return SGIPC_NOT_READY;
+    }
+    SG_LAUNCH_CHECK(c, name);
+    return SGIPC_OK;
+}
+}  // namespace sgipc

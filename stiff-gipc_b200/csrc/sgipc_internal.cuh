@@ -138,6 +138,14 @@ struct SgipcCtx {
     int key_bits;
     int assembled;
     int* dflag;                   // device: input errors found by kernels (bit 0: pair index)
+    // last inputs (for re-timing kernels against the current state)
+    SgipcFemData last_fem;
+    SgipcContacts last_con;
+    SgipcParams last_prm;
+    int last_has_con;
+    SgipcContacts mas_con;        // contacts of the last MAS build (to rebuild after timing)
+    int mas_has_con;
+    long long launches;           // kernels of this library launched on the context
 
     // ---- MAS and PCG ------------------------------------------------------------------
     sgipc::MasWork mas;
@@ -173,6 +181,16 @@ inline SgipcStatus cuda_fail(SgipcCtx* c, cudaError_t e, const char* what) {
     } while (0)
 
 inline int nblk(long long n, int b = SGIPC_BLOCK) { return (int)((n + b - 1) / b); }
+
+// count `k` kernel launches of this library on the context
+#define SG_COUNT(ctx, k) ((ctx)->launches += (k))
+
+// Per-unit hooks for sgipc_time_kernel: launch the named kernel once against the current
+// state; *bytes receives its algorithmic bytes per launch.  Returns SGIPC_NOT_READY when
+// the unit does not own the name.
+SgipcStatus assemble_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double* bytes);
+SgipcStatus mas_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double* bytes);
+SgipcStatus pcg_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double* bytes);
 
 // ---- cross-unit entry points ------------------------------------------------------------
 SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t);

@@ -286,6 +286,7 @@ SgipcStatus mas_apply_t(SgipcCtx* c, const T* r, T* z, int fp32_inv, cudaStream_
     if (!m.built) return SGIPC_NOT_READY;
     const int L = m.levelnum;
     const int ndom = m.h_info[16] / 16;
+    SG_COUNT(c, 3);
     if (fp32_inv) {
         k_restrict<T, float><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, r, m.table, L, m.R32);
         k_domain_mv<float><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom32, m.R32, m.Z32);
@@ -377,6 +378,7 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     const int nv = c->nv, L = m.levelnum;
     const int nbank_cap = m.npos / 16 + 1;
     k_init_level0<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, m.real_map, L, m.node, m.table, m.info, m.npos);
+    SG_COUNT(c, 1 + (L - 1) * (3 + (con && con->pair_num > 0)) + 3);
     for (int l = 0; l + 1 < L; l++) {
         SG_CHECK(c, cudaMemsetAsync(m.mask, 0, sizeof(uint32_t) * m.npos, s));
         k_mask_edges<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, m.nbr_ptr, m.nbr, m.node, m.mask);
@@ -424,8 +426,44 @@ extern "C" SgipcStatus sgipc_mas_build(SgipcCtx* c, const SgipcContacts* con, Sg
     if (!c) return SGIPC_BAD_INPUT;
     if (con && con->pair_num > 0 && !con->pairs) return SGIPC_BAD_INPUT;
     SG_CHECK(c, cudaSetDevice(c->device));
-    return mas_build(c, con, prec, (cudaStream_t)stream);
+    SgipcStatus st = mas_build(c, con, prec, (cudaStream_t)stream);
+    if (st == SGIPC_OK) {
+        c->mas_con = con ? *con : SgipcContacts{};
+        c->mas_has_con = con != nullptr;
+    }
+    return st;
 }
+
+namespace sgipc {
+SgipcStatus mas_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double* bytes) {
+    MasWork& m = c->mas;
+    if (strncmp(name, "mas_", 4)) return SGIPC_NOT_READY;
+    if (!m.built) return SGIPC_NOT_READY;
+    const int L = m.levelnum, total = m.h_info[16], ndom = total / 16;
+    SG_COUNT(c, 1);
+    if (!strcmp(name, "mas_scatter")) {
+        k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L,
+                                                               m.dom64);
+        *bytes = (double)c->nnz * (72 + 8) + (double)c->nv * L * 4 + (double)ndom * 2304 * 8;
+    } else if (!strcmp(name, "mas_invert")) {
+        k_invert<<<ndom, 256, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);
+        *bytes = (double)ndom * 2304 * (8 + 8 + 4);
+    } else if (!strcmp(name, "mas_domain64") || !strcmp(name, "mas_domain32")) {
+        const bool f32 = name[10] == '3';
+        if (f32)
+            k_domain_mv<float><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom32, m.R32, m.Z32);
+        else
+            k_domain_mv<double><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom64, m.R64, m.Z64);
+        // algorithmic: packed symmetric domain inverse (136 3x3 blocks) + R in + Z out
+        const double sm = f32 ? 4 : 8;
+        *bytes = (double)ndom * (136 * 9 * sm + 2 * 48 * sm);
+    } else {
+        return SGIPC_NOT_READY;
+    }
+    SG_LAUNCH_CHECK(c, name);
+    return SGIPC_OK;
+}
+}  // namespace sgipc
 
 extern "C" SgipcStatus sgipc_mas_apply(SgipcCtx* c, const double* r, double* z, void* stream) {
     if (!c || !r || !z) return SGIPC_BAD_INPUT;

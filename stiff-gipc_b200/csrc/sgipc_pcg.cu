@@ -647,6 +647,7 @@ SgipcStatus run_pcg(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, doub
     const int nv = c->nv, n = c->n;
     PcgPtrs<T, NR> P = ptrs_of<T, NR>(w);
     MasView mv = mas_view(c);
+    SG_COUNT(c, 4);
     SG_CHECK(c, cudaMemsetAsync(R, 0, sizeof(M) * 3 * (size_t)m.h_info[16] * NR, s));
     k_pcg_init<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, b, P, mv, R, tol, max_iter, crit);
     k_pcg_domain<M, NR><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, w.sc, inv, R, Z);
@@ -721,6 +722,7 @@ void pcg_destroy(SgipcCtx* c) {
 
 template <class T>
 SgipcStatus spmv_t(SgipcCtx* c, const T* x, T* y, cudaStream_t s) {
+    SG_COUNT(c, 1);
     k_spmv<T><<<nblk(c->n), 256, 0, s>>>(topo_of(c), mat_view<T>(c), x, y);
     SG_LAUNCH_CHECK(c, "spmv");
     return SGIPC_OK;
@@ -731,6 +733,7 @@ template SgipcStatus spmv_t<float>(SgipcCtx*, const float*, float*, cudaStream_t
 SgipcStatus dot64(SgipcCtx* c, const double* a, const double* b, int n, double* out_dev, cudaStream_t s) {
     int g = nblk(n, 256);
     if (g > 1024) g = 1024;
+    SG_COUNT(c, 1);
     k_dot<<<g, 256, 0, s>>>(n, a, b, c->dot_partial, c->dot_ticket, out_dev);
     SG_LAUNCH_CHECK(c, "dot");
     return SGIPC_OK;
@@ -752,6 +755,7 @@ static SgipcStatus true_residual(SgipcCtx* c, const double* b, const double* x, 
     const int n3 = 3 * c->n;
     SgipcStatus st = spmv_t<double>(c, x, c->tmp64b, s);
     if (st != SGIPC_OK) return st;
+    SG_COUNT(c, 1);
     k_axpby_res<<<nblk(n3), 256, 0, s>>>(n3, b, c->tmp64b, c->tmp64b);
     if ((st = dot64(c, c->tmp64b, c->tmp64b, n3, c->dot_out, s)) != SGIPC_OK) return st;
     if ((st = dot64(c, b, b, n3, c->dot_out + 1, s)) != SGIPC_OK) return st;
@@ -779,6 +783,7 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         PcgScalars hs;
         SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg64.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
         SG_CHECK(c, cudaStreamSynchronize(s));
+        SG_COUNT(c, 5LL * hs.bodies);
         out.iterations = hs.iter;
         out.refinements = 0;
         out.rz0 = hs.rz0;
@@ -797,6 +802,7 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
             if (crit == SGIPC_CRIT_TRUE && bn2 > 0 && rz > 0) inner_tol = tol;
             st = run_pcg<float, float, 1>(c, c->pcg32, 1, r64, inner_tol, max_iter, (int)crit, s, 20);
             if (st != SGIPC_OK) return st;
+            SG_COUNT(c, 2);
             k_add_f32<<<nblk(n3), 256, 0, s>>>(n3, (const float*)c->pcg32.x, x);
             // r = b - A x in FP64
             if ((st = spmv_t<double>(c, x, c->tmp64b, s)) != SGIPC_OK) return st;
@@ -810,6 +816,7 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
             SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
             SG_CHECK(c, cudaStreamSynchronize(s));
             total_it += hs.iter;
+            SG_COUNT(c, 5LL * hs.bodies);
             if (ref == 0) {
                 rz0 = hs.rz0;
                 bn2 = hs.bnorm2;
@@ -882,6 +889,7 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
     }
     // four right-hand sides interleaved: every matrix / MAS block read serves all four
     double* bi = c->tmp64;
+    SG_COUNT(c, 2);
     k_interleave<double, double><<<nblk(4LL * n3), 256, 0, s>>>(n3, 4, b, bi, 1);
     SgipcStatus st;
     PcgWork& w = (prec == SGIPC_MIXED) ? c->pcg32 : c->pcg64;
@@ -900,6 +908,7 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
     SG_CHECK(c, cudaMemcpyAsync(hs, w.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
     SG_CHECK(c, cudaStreamSynchronize(s));
     SgipcStatus worst = SGIPC_OK;
+    SG_COUNT(c, 5LL * hs[0].bodies);
     for (int r = 0; r < 4; r++) {
         if (stats) {
             stats[r] = SgipcSolveStats{};
@@ -914,4 +923,76 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
         if (hs[r].status != SGIPC_OK) worst = (SgipcStatus)hs[r].status;
     }
     return worst;
+}
+
+namespace sgipc {
+SgipcStatus pcg_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double* bytes) {
+    const bool f64 = !strcmp(name, "spmv64"), f32 = !strcmp(name, "spmv32");
+    if (!f64 && !f32) return SGIPC_NOT_READY;
+    int nuc = 0;
+    SG_CHECK(c, cudaMemcpyAsync(&nuc, c->nuc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    SG_COUNT(c, 1);
+    if (f64)
+        k_spmv<double><<<nblk(c->n), 256, 0, s>>>(topo_of(c), mat_view<double>(c), c->tmp64, c->tmp64b);
+    else
+        k_spmv<float><<<nblk(c->n), 256, 0, s>>>(topo_of(c), mat_view<float>(c), (const float*)c->tmp64,
+                                                  (float*)c->tmp64b);
+    // nb (sb + 4) + (n + 1) 4 + 2 * 3n * sv with nb = static + unique contact blocks
+    const double sb = f64 ? 72 : 36, sv = f64 ? 8 : 4;
+    *bytes = ((double)c->nnz + nuc) * (sb + 4) + (c->n + 1.0) * 4 + 2.0 * 3 * c->n * sv;
+    SG_LAUNCH_CHECK(c, name);
+    return SGIPC_OK;
+}
+}  // namespace sgipc
+
+extern "C" SgipcStatus sgipc_launch_count(SgipcCtx* c, int64_t* launches) {
+    if (!c || !launches) return SGIPC_BAD_INPUT;
+    SG_CHECK(c, cudaDeviceSynchronize());
+    *launches = c->launches;
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_time_kernel(SgipcCtx* c, const char* name, int32_t reps, void* stream, float* avg_ms,
+                                         double* bytes_per_launch) {
+    if (!c || !name || reps < 1 || !avg_ms) return SGIPC_BAD_INPUT;
+    if (!c->assembled) return SGIPC_NOT_READY;
+    cudaStream_t s = (cudaStream_t)stream;
+    SG_CHECK(c, cudaSetDevice(c->device));
+    // spmv reads tmp64: give it a defined vector
+    SG_CHECK(c, cudaMemsetAsync(c->tmp64, 0, sizeof(double) * 3 * c->n, s));
+    SgipcStatus (*hooks[3])(SgipcCtx*, const char*, cudaStream_t, double*) = {assemble_time_hook, mas_time_hook,
+                                                                              pcg_time_hook};
+    double bytes = 0;
+    int owner = -1;
+    for (int h = 0; h < 3 && owner < 0; h++) {
+        SgipcStatus st = hooks[h](c, name, s, &bytes);  // warm-up launch
+        if (st == SGIPC_OK) owner = h;
+        else if (st != SGIPC_NOT_READY) return st;
+    }
+    if (owner < 0) return SGIPC_BAD_INPUT;
+    cudaEvent_t e0, e1;
+    SG_CHECK(c, cudaEventCreate(&e0));
+    SG_CHECK(c, cudaEventCreate(&e1));
+    SG_CHECK(c, cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; r++) {
+        SgipcStatus st = hooks[owner](c, name, s, &bytes);
+        if (st != SGIPC_OK) return st;
+    }
+    SG_CHECK(c, cudaEventRecord(e1, s));
+    SG_CHECK(c, cudaEventSynchronize(e1));
+    float ms = 0;
+    SG_CHECK(c, cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *avg_ms = ms / reps;
+    if (bytes_per_launch) *bytes_per_launch = bytes;
+    // the MAS kernels overwrite the domain matrices: rebuild them as they were
+    if (owner == 1 && c->mas.built) {
+        SgipcPrecision prec = (SgipcPrecision)(c->mas.built - 1);
+        SgipcStatus st = mas_build(c, c->mas_has_con ? &c->mas_con : nullptr, prec, s);
+        if (st != SGIPC_OK) return st;
+    }
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    return SGIPC_OK;
 }

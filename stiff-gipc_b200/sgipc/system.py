@@ -201,6 +201,19 @@ class GIPC:
                                           C.byref(cnt)), self.ctx)
         return rows, cols, vals
 
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        N.check(N.lib().sgipc_launch_count(self.ctx, C.byref(n)), self.ctx)
+        return int(n.value)
+
+    def time_kernel(self, name: str, reps: int = 20):
+        """(avg ms, algorithmic bytes per launch) of one hot kernel, CUDA events on the
+        current stream."""
+        ms, by = C.c_float(), C.c_double()
+        N.check(N.lib().sgipc_time_kernel(self.ctx, name.encode(), reps, _stream(), C.byref(ms), C.byref(by)),
+                self.ctx)
+        return float(ms.value), float(by.value)
+
     def spmv(self, x: torch.Tensor) -> torch.Tensor:
         y = torch.empty_like(x)
         N.check(N.lib().sgipc_spmv(self.ctx, _p(x), _p(y), _stream()), self.ctx)
@@ -220,6 +233,48 @@ class GIPC:
                                 _p(self.moveDir), C.byref(st), _stream())
         N.check(s, self.ctx, allow=(N.OK, N.NOT_CONVERGED))
         return st
+
+
+class HostNewtonState:
+    """Pinned host copies of the per-Newton inputs (iterate x and the contact arrays),
+    for callers that keep their state on the host (``step_from_host``)."""
+
+    def __init__(self, sc):
+        def pin(a, dtype):
+            return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).pin_memory()
+
+        f64, i32 = torch.float64, torch.int32
+        self.vertexes = pin(sc.vertexes, f64)
+        self.pairs = pin(sc.pairs.reshape(-1, 4), i32)
+        self.ground_pairs = pin(sc.ground_pairs, i32)
+        self.fric_pairs = pin(sc.fric_pairs.reshape(-1, 4), i32)
+        self.fric_lambda = pin(sc.fric_lambda, f64)
+        self.fric_coord = pin(sc.fric_coord.reshape(-1, 2), f64)
+        self.fric_basis = pin(sc.fric_basis.reshape(-1, 6), f64)
+        self.fric_gd_pairs = pin(sc.fric_gd_pairs, i32)
+        self.fric_gd_lambda = pin(sc.fric_gd_lambda, f64)
+        self.move_dir = torch.empty(3 * sc.nv, dtype=f64).pin_memory()
+
+    NAMES = ("vertexes", "pairs", "ground_pairs", "fric_pairs", "fric_lambda", "fric_coord", "fric_basis",
+             "fric_gd_pairs", "fric_gd_lambda")
+
+    def h2d_bytes(self) -> int:
+        return int(sum(getattr(self, n).numel() * getattr(self, n).element_size() for n in self.NAMES))
+
+    def d2h_bytes(self) -> int:
+        return int(self.move_dir.numel() * self.move_dir.element_size())
+
+
+def step_from_host(g: "GIPC", host: HostNewtonState, config: Optional[PCGSolverConfig] = None):
+    """One Newton system from host inputs: H2D copies, assembly, MAS + PCG, D2H of dx."""
+    tet = g.tet
+    for n in HostNewtonState.NAMES:
+        getattr(tet, n).copy_(getattr(host, n), non_blocking=True)
+    g.computeGradientAndHessian(tet)
+    st = g.calculateMovingDirection(config, tet)
+    host.move_dir.copy_(g.moveDir, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    return st
 
 
 class MASPreconditioner:
