@@ -45,6 +45,8 @@ def lib():
         L.or_friction_pair.restype = C.c_int
         L.or_friction_ground.argtypes = [_d, _d, C.c_double, C.c_double, C.c_double, _d, _d, _d]
         L.or_make_pd.argtypes = [C.c_int, _d]
+        L.or_pair_geom.argtypes = [_i, _d, C.c_double, _d, _d, _d, _d]
+        L.or_pair_geom.restype = C.c_int
         L.or_eig.argtypes = [C.c_int, _d, _d, _d]
         L.or_assemble.argtypes = [C.c_void_p, _d, C.c_int, _i, _i, _d, _d]
         L.or_assemble.restype = C.c_int
@@ -111,6 +113,16 @@ def friction_pair(enc, X, X0, coord, basis, lastH, mu, eps2):
     nv = lib().or_friction_pair(_p(enc, _i), _p(X), _p(X0), _p(coord), _p(basis), lastH, mu, eps2,
                                 _p(vid, _i), _p(e), _p(g), _p(H))
     return vid[:nv], e[0], g[:3 * nv], H.reshape(12, 12)[:3 * nv, :3 * nv]
+
+
+def pair_geom(enc, X, dhat):
+    """(nv, f, grad f, c, grad c) of a barrier pair; X holds the scene's positions."""
+    enc = _i32(enc).reshape(4)
+    X = _f64(X).reshape(-1)
+    f, c = np.zeros(1), np.zeros(1)
+    gf, gc = np.zeros(12), np.zeros(12)
+    nv = lib().or_pair_geom(_p(enc, _i), _p(X), dhat, _p(f), _p(gf), _p(c), _p(gc))
+    return nv, f[0], gf[:3 * nv], c[0], gc[:3 * nv]
 
 
 def make_pd(A):

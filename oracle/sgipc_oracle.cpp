@@ -487,6 +487,30 @@ void or_friction_ground(const double* x, const double* x0, double lastH, double 
 
 void or_make_pd(int n, double* A) { make_pd(n, A); }
 
+// Geometry of a barrier pair: f = d / sqrt(dhat) and its gradient over the pair's
+// vertices (the last column of the reference's pFpx_* Jacobians), and for mollified
+// pairs c = |e0 x e1| with its gradient (column 4 of pFpx_pee/ppe/ppp).  Returns nv.
+int or_pair_geom(const int32_t* enc, const double* X, double dhat, double* f, double* gf, double* c, double* gc) {
+    Pair p = decode(enc);
+    D12 d2 = pair_dist2(p, X);
+    double dist = std::sqrt(d2.v), dsq = std::sqrt(dhat);
+    *f = dist / dsq;
+    for (int i = 0; i < 12; i++) gf[i] = d2.d[i] / (2.0 * dist * dsq);
+    *c = 0;
+    for (int i = 0; i < 12; i++) gc[i] = 0;
+    if (p.kind >= 4) {
+        int e[4];
+        moll_edges(p, e);
+        P3<D12> q0 = dvar(X + 3 * p.v[e[0]], e[0]), q1 = dvar(X + 3 * p.v[e[1]], e[1]);
+        P3<D12> q2 = dvar(X + 3 * p.v[e[2]], e[2]), q3 = dvar(X + 3 * p.v[e[3]], e[3]);
+        P3<D12> cr = cross(sub(q1, q0), sub(q3, q2));
+        D12 cc = dsqrt(dot(cr, cr));
+        *c = cc.v;
+        for (int i = 0; i < 12; i++) gc[i] = cc.d[i];
+    }
+    return p.nv;
+}
+
 void or_eig(int n, const double* A, double* w, double* V) { jacobi_eig(n, A, w, V); }
 
 // --------------------------------- system assembly -----------------------------------
