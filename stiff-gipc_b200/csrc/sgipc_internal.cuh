@@ -56,6 +56,7 @@ struct MasWork {
     int* nbr_ptr;            // [nv+1] mesh neighbour CSR
     int* nbr;                // [nnz]
     int* table;              // [nv * levelnum] global cluster per level (level 0 = position)
+    int* up;                 // [total_cap] global id of each cluster's parent at the next level (-1: none)
     int* node;               // [nv] node id at the level being built
     uint32_t* mask;          // [npos] bank-local connectivity
     int* comp_rank;          // [npos] new local id of the component a node belongs to

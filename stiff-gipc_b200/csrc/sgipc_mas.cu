@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "sgipc_internal.cuh"
+#include "sgipc_mas_dev.cuh"
 
 using namespace sgipc;
 
@@ -29,12 +30,14 @@ __device__ __forceinline__ void mask_edge(uint32_t* mask, int a, int b) {
 }
 
 __global__ void k_init_level0(int nv, const int* __restrict__ real_map, int L, int* __restrict__ node,
-                              int* __restrict__ table, int* __restrict__ info, int npos) {
+                              int* __restrict__ table, int* __restrict__ info, int npos, int* __restrict__ up) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v == 0) {
         info[0] = 0;     // start of level 0
         info[8] = npos;  // count of level 0 (positions, padding included)
+        if (L == 1) info[16] = npos;
     }
+    if (v < npos) up[v] = -1;  // padding positions have no parent
     if (v >= nv) return;
     int p = real_map[v];
     node[v] = p;
@@ -121,10 +124,12 @@ __global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, i
 }
 
 __global__ void k_assign(int nv, int L, int level, const int* __restrict__ bank_off, const int* __restrict__ rank,
-                         int* __restrict__ node, int* __restrict__ table, int* __restrict__ info) {
+                         int* __restrict__ node, int* __restrict__ table, int* __restrict__ info,
+                         int* __restrict__ up) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int count = info[8 + level];
-    const int start_next = info[level] + ((count + 15) & ~15);
+    const int start = info[level];
+    const int start_next = start + ((count + 15) & ~15);
     if (v == 0) {
         int nbank = (count + 15) >> 4;
         info[level + 1] = start_next;
@@ -136,25 +141,54 @@ __global__ void k_assign(int nv, int L, int level, const int* __restrict__ bank_
     int nn = bank_off[a >> 4] + rank[a];
     node[v] = nn;
     table[(size_t)v * L + level + 1] = start_next + nn;
+    up[start + a] = start_next + nn;  // every vertex of node a writes the same parent
+    if (level + 2 == L) up[start_next + nn] = -1;
 }
 
-// scatter one 3x3 block B at (r,c) (and B^T at (c,r)) into every level whose bank holds both
-__device__ __forceinline__ void scatter_block(double* dom, const int* __restrict__ table, int L, int r, int c,
-                                              const double* B) {
+// Scatter one 3x3 block B at (r,c) (and B^T at (c,r)) into every level whose bank holds
+// both endpoints.  Lanes of a warp that hit the same coarse entry first add their blocks
+// together (match + shuffles) so that one lane issues the atomics: at the coarsest levels
+// nearly every block of a warp lands on the same few entries.
+__device__ __forceinline__ void scatter_block_warp(double* dom, const int* __restrict__ table, int L, int r, int c,
+                                                   const double (&B)[9], bool valid) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     for (int l = 0; l < L; l++) {
-        int ga = table[(size_t)r * L + l], gb = table[(size_t)c * L + l];
-        if ((ga >> 4) != (gb >> 4)) continue;
-        double* D = dom + (size_t)(ga >> 4) * 2304;
-        int ra = 3 * (ga & 15), cb = 3 * (gb & 15);
+        int ga = -1, gb = -1;
+        if (valid) {
+            ga = table[(size_t)r * L + l];
+            gb = table[(size_t)c * L + l];
+        }
+        bool hit = valid && (ga >> 4) == (gb >> 4);
+        // key of the target: (ga, gb) and whether the block is a diagonal one
+        unsigned long long key = hit ? (((unsigned long long)(unsigned)ga << 33) | ((unsigned long long)(unsigned)gb << 1) |
+                                        (unsigned long long)(r == c))
+                                     : ~0ull;
+        unsigned grp = __match_any_sync(full, key);
+        int leader = __ffs(grp) - 1;
+        double S[9];
 #pragma unroll
-        for (int i = 0; i < 3; i++)
+        for (int q = 0; q < 9; q++) S[q] = 0.0;
+        unsigned m = grp;
+        while (m) {
+            int j = __ffs(m) - 1;
+            m &= m - 1;
 #pragma unroll
-            for (int j = 0; j < 3; j++) {
-                double v = B[3 * i + j];
-                if (v == 0.0) continue;
-                atomicAdd(D + (ra + i) * 48 + cb + j, v);
-                if (r != c) atomicAdd(D + (cb + j) * 48 + ra + i, v);
-            }
+            for (int q = 0; q < 9; q++) S[q] += __shfl_sync(grp, B[q], j);
+        }
+        if (hit && lane == leader) {
+            double* D = dom + (size_t)(ga >> 4) * 2304;
+            int ra = 3 * (ga & 15), cb = 3 * (gb & 15);
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    double v = S[3 * i + j];
+                    if (v == 0.0) continue;
+                    atomicAdd(D + (ra + i) * 48 + cb + j, v);
+                    if (r != c) atomicAdd(D + (cb + j) * 48 + ra + i, v);
+                }
+        }
     }
 }
 
@@ -162,57 +196,66 @@ __global__ void k_scatter_static(int nnz, const int* __restrict__ slot_row, cons
                                  const double* __restrict__ val, const int* __restrict__ table, int L,
                                  double* __restrict__ dom) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nnz) return;
+    bool valid = s < nnz;
     double B[9];
 #pragma unroll
-    for (int q = 0; q < 9; q++) B[q] = val[9 * (size_t)s + q];
-    scatter_block(dom, table, L, slot_row[s], col[s], B);
+    for (int q = 0; q < 9; q++) B[q] = valid ? val[9 * (size_t)s + q] : 0.0;
+    scatter_block_warp(dom, table, L, valid ? slot_row[s] : 0, valid ? col[s] : 0, B, valid);
 }
 
 __global__ void k_scatter_contact(int cap, const int* __restrict__ nuc, const int* __restrict__ ur,
                                   const int* __restrict__ uc, const double* __restrict__ val,
                                   const int* __restrict__ table, int L, double* __restrict__ dom) {
     int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= cap || u >= nuc[0]) return;
+    if (blockIdx.x * blockDim.x >= nuc[0]) return;  // whole block beyond the unique blocks
+    bool valid = u < cap && u < nuc[0];
     double B[9];
 #pragma unroll
-    for (int q = 0; q < 9; q++) B[q] = val[9 * (size_t)u + q];
-    scatter_block(dom, table, L, ur[u], uc[u], B);
+    for (int q = 0; q < 9; q++) B[q] = valid ? val[9 * (size_t)u + q] : 0.0;
+    scatter_block_warp(dom, table, L, valid ? ur[u] : 0, valid ? uc[u] : 0, B, valid);
 }
 
-// In-place Gauss-Jordan inversion of one 48x48 domain per CTA (FP64 in shared memory).
-__global__ void __launch_bounds__(256) k_invert(int ndom, double* __restrict__ dom, float* __restrict__ dom32,
+// Gauss-Jordan inversion without pivoting, one thread per column of a 48x48 domain held in
+// registers, four domains per 192-thread CTA; the pivot column is broadcast through shared
+// memory (double-buffered: one barrier per pivot step).  Column update for pivot k with
+// c = A(:,k), p = c[k]:  thread j != k:  f = A(k,j)/p;  A(i,j) -= c[i] f (i != k);  A(k,j) = f
+//                        thread k:       A(i,k) = -c[i]/p (i != k);  A(k,k) = 1/p
+__global__ void __launch_bounds__(192) k_invert(int ndom, double* __restrict__ dom, float* __restrict__ dom32,
                                                 int write64, int write32) {
-    __shared__ double A[48][49];
-    __shared__ double colk[48];
-    const int d = blockIdx.x;
-    if (d >= ndom) return;
-    double* D = dom + (size_t)d * 2304;
-    for (int e = threadIdx.x; e < 2304; e += blockDim.x) A[e / 48][e % 48] = D[e];
-    __syncthreads();
-    if (threadIdx.x < 48 && A[threadIdx.x][threadIdx.x] == 0.0) A[threadIdx.x][threadIdx.x] = 1.0;
-    __syncthreads();
+    __shared__ double piv[2][4][48];
+    const int ld = threadIdx.x / 48, j = threadIdx.x % 48;
+    const int d = blockIdx.x * 4 + ld;
+    const bool act = d < ndom;
+    double col[48];
+    const double* D = dom + (size_t)(act ? d : 0) * 2304;
+#pragma unroll
+    for (int i = 0; i < 48; i++) col[i] = act ? D[i * 48 + j] : (i == j ? 1.0 : 0.0);
+    if (col[j] == 0.0) col[j] = 1.0;  // a zero diagonal (padding node) becomes 1
+#pragma unroll
     for (int k = 0; k < 48; k++) {
-        const double piv = A[k][k];
-        if (threadIdx.x < 48) colk[threadIdx.x] = A[threadIdx.x][k];
-        __syncthreads();
-        if (threadIdx.x < 48) {
-            const int j = threadIdx.x;
-            A[k][j] = (j == k) ? 1.0 / piv : A[k][j] / piv;
+        double* pc = piv[k & 1][ld];
+        if (j == k) {
+#pragma unroll
+            for (int i = 0; i < 48; i++) pc[i] = col[i];
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < 2304; e += blockDim.x) {
-            const int i = e / 48, j = e % 48;
-            if (i == k) continue;
-            const double f = colk[i];
-            A[i][j] = (j == k) ? -f * A[k][k] : A[i][j] - f * A[k][j];
+        const double ip = 1.0 / pc[k];
+        if (j == k) {
+#pragma unroll
+            for (int i = 0; i < 48; i++) col[i] = (i == k) ? ip : -pc[i] * ip;
+        } else {
+            const double f = col[k] * ip;
+#pragma unroll
+            for (int i = 0; i < 48; i++) col[i] = (i == k) ? f : col[i] - pc[i] * f;
         }
-        __syncthreads();
     }
-    for (int e = threadIdx.x; e < 2304; e += blockDim.x) {
-        const double v = A[e / 48][e % 48];
-        if (write64) D[e] = v;
-        if (write32) dom32[(size_t)d * 2304 + e] = (float)v;
+    if (!act) return;
+    double* Dw = dom + (size_t)d * 2304;
+    float* Dw32 = dom32 + (size_t)d * 2304;
+#pragma unroll
+    for (int i = 0; i < 48; i++) {
+        if (write64) Dw[i * 48 + j] = col[i];
+        if (write32) Dw32[i * 48 + j] = (float)col[i];
     }
 }
 
@@ -223,22 +266,30 @@ __global__ void __launch_bounds__(256) k_invert(int ndom, double* __restrict__ d
 // ------------------------------------------------------------------------------------------
 namespace sgipc {
 
+// level 0 and level 1 of the restriction: one thread per position
 template <class T, class M>
-__global__ void k_restrict(int nv, const T* __restrict__ r, const int* __restrict__ table, int L, M* __restrict__ R) {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= nv) return;
-    const int* tv = table + (size_t)v * L;
-    M x = (M)r[3 * v], y = (M)r[3 * v + 1], z = (M)r[3 * v + 2];
-    int p = tv[0];
-    R[3 * p] = x;
-    R[3 * p + 1] = y;
-    R[3 * p + 2] = z;
-    for (int l = 1; l < L; l++) {
-        int g = tv[l];
-        atomicAdd(R + 3 * g, x);
-        atomicAdd(R + 3 * g + 1, y);
-        atomicAdd(R + 3 * g + 2, z);
+__global__ void k_restrict01(int npos, const T* __restrict__ r, const int* __restrict__ part_map,
+                             const int* __restrict__ up, M* __restrict__ R) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    int v = p < npos ? part_map[p] : -1;
+    M val[3] = {0, 0, 0};
+    if (v >= 0) {
+        val[0] = (M)r[3 * v];
+        val[1] = (M)r[3 * v + 1];
+        val[2] = (M)r[3 * v + 2];
     }
+    if (p < npos) {
+        R[3 * p] = val[0];
+        R[3 * p + 1] = val[1];
+        R[3 * p + 2] = val[2];
+    }
+    bank_reduce_store<M, 1>(v >= 0 ? up[p] : -1, val, R);
+}
+
+template <class M>
+__global__ void __launch_bounds__(1024) k_restrict_coarse(const int* __restrict__ info, const int* __restrict__ up,
+                                                          int L, M* __restrict__ R) {
+    restrict_coarse_cta<M, 1>(info, up, L, R);
 }
 
 // Z_d = A_d^-1 R_d, four domains per 192-thread CTA
@@ -260,12 +311,8 @@ __global__ void __launch_bounds__(192) k_domain_mv(const int* __restrict__ info,
 }
 
 template <class T, class M>
-__global__ void k_prolong(int nv, const int* __restrict__ table, int L, const M* __restrict__ Z, T* __restrict__ z,
-                          M* __restrict__ R, const int* __restrict__ info, int npos) {
+__global__ void k_prolong(int nv, const int* __restrict__ table, int L, const M* __restrict__ Z, T* __restrict__ z) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
-    // clear the coarse part of R for the next restriction
-    const int total = info[16];
-    for (int k = npos * 3 + v; k < total * 3; k += gridDim.x * blockDim.x) R[k] = 0;
     if (v >= nv) return;
     const int* tv = table + (size_t)v * L;
     M x = 0, y = 0, w = 0;
@@ -286,15 +333,17 @@ SgipcStatus mas_apply_t(SgipcCtx* c, const T* r, T* z, int fp32_inv, cudaStream_
     if (!m.built) return SGIPC_NOT_READY;
     const int L = m.levelnum;
     const int ndom = m.h_info[16] / 16;
-    SG_COUNT(c, 3);
+    SG_COUNT(c, 4);
     if (fp32_inv) {
-        k_restrict<T, float><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, r, m.table, L, m.R32);
+        k_restrict01<T, float><<<nblk(m.npos), SGIPC_BLOCK, 0, s>>>(m.npos, r, m.part_map, m.up, m.R32);
+        k_restrict_coarse<float><<<1, 1024, 0, s>>>(m.info, m.up, L, m.R32);
         k_domain_mv<float><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom32, m.R32, m.Z32);
-        k_prolong<T, float><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, m.table, L, m.Z32, z, m.R32, m.info, m.npos);
+        k_prolong<T, float><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, m.table, L, m.Z32, z);
     } else {
-        k_restrict<T, double><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, r, m.table, L, m.R64);
+        k_restrict01<T, double><<<nblk(m.npos), SGIPC_BLOCK, 0, s>>>(m.npos, r, m.part_map, m.up, m.R64);
+        k_restrict_coarse<double><<<1, 1024, 0, s>>>(m.info, m.up, L, m.R64);
         k_domain_mv<double><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom64, m.R64, m.Z64);
-        k_prolong<T, double><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, m.table, L, m.Z64, z, m.R64, m.info, m.npos);
+        k_prolong<T, double><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, m.table, L, m.Z64, z);
     }
     SG_LAUNCH_CHECK(c, "mas apply");
     return SGIPC_OK;
@@ -339,6 +388,7 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
     if (!A((void**)&m.part_map, sizeof(int) * m.npos) || !A((void**)&m.real_map, sizeof(int) * nv) ||
         !A((void**)&m.nbr_ptr, sizeof(int) * (nv + 1)) || !A((void**)&m.nbr, sizeof(int) * nb.size()) ||
         !A((void**)&m.table, sizeof(int) * (size_t)nv * m.levelnum) || !A((void**)&m.node, sizeof(int) * nv) ||
+        !A((void**)&m.up, sizeof(int) * (size_t)m.total_cap) ||
         !A((void**)&m.mask, sizeof(uint32_t) * m.npos) || !A((void**)&m.comp_rank, sizeof(int) * m.npos) ||
         !A((void**)&m.bank_cnt, sizeof(int) * (m.npos / 16 + 2)) ||
         !A((void**)&m.bank_off, sizeof(int) * (m.npos / 16 + 2)) || !A((void**)&m.info, sizeof(int) * 32) ||
@@ -366,7 +416,7 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
 
 void mas_destroy(SgipcCtx* c) {
     MasWork& m = c->mas;
-    void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.table, m.node, m.mask, m.comp_rank, m.bank_cnt,
+    void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.table, m.up, m.node, m.mask, m.comp_rank, m.bank_cnt,
                     m.bank_off, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32, m.scan_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -377,7 +427,8 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     if (!c->assembled) return SGIPC_NOT_READY;
     const int nv = c->nv, L = m.levelnum;
     const int nbank_cap = m.npos / 16 + 1;
-    k_init_level0<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, m.real_map, L, m.node, m.table, m.info, m.npos);
+    k_init_level0<<<nblk(nv > m.npos ? nv : m.npos), SGIPC_BLOCK, 0, s>>>(nv, m.real_map, L, m.node, m.table,
+                                                                          m.info, m.npos, m.up);
     SG_COUNT(c, 1 + (L - 1) * (3 + (con && con->pair_num > 0)) + 3);
     for (int l = 0; l + 1 < L; l++) {
         SG_CHECK(c, cudaMemsetAsync(m.mask, 0, sizeof(uint32_t) * m.npos, s));
@@ -389,13 +440,7 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
                                                                    m.bank_cnt);
         size_t tb = m.scan_tmp_bytes;
         SG_CHECK(c, cub::DeviceScan::ExclusiveSum(m.scan_tmp, tb, m.bank_cnt, m.bank_off, nbank_cap + 1, s));
-        k_assign<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, L, l, m.bank_off, m.comp_rank, m.node, m.table, m.info);
-    }
-    if (L == 1) {
-        int h[17] = {0};
-        h[8] = m.npos;
-        h[16] = m.npos;
-        SG_CHECK(c, cudaMemcpyAsync(m.info, h, sizeof(h), cudaMemcpyHostToDevice, s));
+        k_assign<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, L, l, m.bank_off, m.comp_rank, m.node, m.table, m.info, m.up);
     }
     SG_LAUNCH_CHECK(c, "mas hierarchy");
     SG_CHECK(c, cudaMemcpyAsync(m.h_info, m.info, sizeof(int) * 17, cudaMemcpyDeviceToHost, s));
@@ -407,11 +452,14 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     }
     const int ndom = total / 16;
     SG_CHECK(c, cudaMemsetAsync(m.dom64, 0, sizeof(double) * 2304 * (size_t)ndom, s));
+    // restricted vectors: entries outside the current levels' nodes must read as zero
+    SG_CHECK(c, cudaMemsetAsync(m.R64, 0, sizeof(double) * 3 * (size_t)total * c->max_rhs, s));
+    SG_CHECK(c, cudaMemsetAsync(m.R32, 0, sizeof(float) * 3 * (size_t)total * c->max_rhs, s));
     k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L, m.dom64);
     k_scatter_contact<<<nblk(c->cap_cblk), SGIPC_BLOCK, 0, s>>>(c->cap_cblk, c->nuc, c->uc_row, c->uc_col, c->uc64,
                                                                m.table, L, m.dom64);
     const int w64 = prec == SGIPC_FP64 ? 1 : 0, w32 = prec == SGIPC_FP64 ? 0 : 1;
-    k_invert<<<ndom, 256, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
+    k_invert<<<(ndom + 3) / 4, 192, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
     SG_LAUNCH_CHECK(c, "mas matrices");
     m.built = (int)prec + 1;
     return SGIPC_OK;
@@ -446,7 +494,7 @@ SgipcStatus mas_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
                                                                m.dom64);
         *bytes = (double)c->nnz * (72 + 8) + (double)c->nv * L * 4 + (double)ndom * 2304 * 8;
     } else if (!strcmp(name, "mas_invert")) {
-        k_invert<<<ndom, 256, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);
+        k_invert<<<(ndom + 3) / 4, 192, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);
         *bytes = (double)ndom * 2304 * (8 + 8 + 4);
     } else if (!strcmp(name, "mas_domain64") || !strcmp(name, "mas_domain32")) {
         const bool f32 = name[10] == '3';

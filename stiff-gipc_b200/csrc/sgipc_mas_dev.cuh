@@ -1,0 +1,69 @@
+// sgipc_mas_dev.cuh — device helpers of the MAS restriction shared by the MAS and PCG units.
+//
+// Every level-(l+1) node is a connected component inside ONE bank of 16 level-l nodes, so
+// restricting a vector to the next level is a bank-local reduction: the 16 lanes of a
+// half-warp hold one bank, each lane sums the values of the lanes that share its parent
+// and the lowest such lane stores the sum.  No atomics, a fixed summation order, and each
+// coarse entry written exactly once (replacing the atomic restriction of
+// __buildMultiLevelR_optimized_new, StiffGIPC/MASPreconditioner.cu:729-847).
+#pragma once
+#include "sgipc_internal.cuh"
+
+namespace sgipc {
+
+// All 32 lanes of the warp must call this (values of idle lanes: parent = -1).
+// v[NR*3] holds this node's value; the parent's sum is stored at R[3*parent+q][r].
+template <class M, int NR>
+__device__ __forceinline__ void bank_reduce_store(int parent, const M (&v)[NR * 3], M* __restrict__ R) {
+    const unsigned full = 0xffffffffu;
+    M s[NR * 3];
+#pragma unroll
+    for (int k = 0; k < NR * 3; k++) s[k] = 0;
+    int leader = -1;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        int pj = __shfl_sync(full, parent, j, 16);
+        bool same = pj == parent;
+        if (same && leader < 0) leader = j;
+#pragma unroll
+        for (int k = 0; k < NR * 3; k++) {
+            M vj = __shfl_sync(full, v[k], j, 16);
+            if (same) s[k] += vj;
+        }
+    }
+    if (parent >= 0 && (int)(threadIdx.x & 15) == leader) {
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) R[(size_t)(3 * parent + q) * NR + r] = s[r * 3 + q];
+    }
+}
+
+// Levels 1 .. L-2 -> 2 .. L-1, run by ONE CTA (levels >= 1 are at most npos/16 nodes).
+template <class M, int NR>
+__device__ __forceinline__ void restrict_coarse_cta(const int* __restrict__ info, const int* __restrict__ up, int L,
+                                                    M* __restrict__ R) {
+    for (int l = 1; l + 1 < L; l++) {
+        const int count = info[8 + l], start = info[l];
+        for (int base = 0; base < count; base += blockDim.x) {
+            const int a = base + threadIdx.x;
+            M v[NR * 3];
+            int par = -1;
+            if (a < count) {
+                const int g = start + a;
+                par = up[g];
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+#pragma unroll
+                    for (int r = 0; r < NR; r++) v[r * 3 + q] = R[(size_t)(3 * g + q) * NR + r];
+            } else {
+#pragma unroll
+                for (int k = 0; k < NR * 3; k++) v[k] = 0;
+            }
+            bank_reduce_store<M, NR>(par, v, R);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace sgipc

@@ -19,10 +19,12 @@
 //   K3 domain_mv   Z = A_d^-1 R for every 16-node domain (all NR columns per read of A_d^-1)
 //   K4 prolong_dot z = sum_l Z, r.z; last CTA: rz_next
 //   K5 p_update    p = z + beta p; sets the graph's loop condition
+#include <cstdlib>
 #include <cub/cub.cuh>
 #include <vector>
 
 #include "sgipc_internal.cuh"
+#include "sgipc_mas_dev.cuh"
 
 using namespace sgipc;
 
@@ -53,6 +55,8 @@ struct MasView {
     int L;
     int npos;
     const int* info;
+    const int* part_map;
+    const int* up;
 };
 
 inline Topo topo_of(SgipcCtx* c) {
@@ -150,32 +154,50 @@ __device__ __forceinline__ void block_mv(const T* __restrict__ B, const T* __res
     }
 }
 
+// Rows are processed by groups of kSpG lanes: lane g of a group takes every kSpG-th block of
+// the row's four lists (static upper, static transposed, contact upper, contact transposed)
+// and the group adds its partial results with shuffles.
+constexpr int kSpG = 4;
+inline int spmv_grid(int n) { return nblk((long long)n * kSpG, 256); }
+
 template <class T, int NR>
-__device__ __forceinline__ void row_mv(const Topo& tp, const MatView<T>& A, const T* __restrict__ x, int i,
+__device__ __forceinline__ void row_mv(const Topo& tp, const MatView<T>& A, const T* __restrict__ x, int i, int g,
                                        T (&acc)[NR][3]) {
 #pragma unroll
     for (int r = 0; r < NR; r++) acc[r][0] = acc[r][1] = acc[r][2] = 0;
-    for (int s = tp.row_ptr[i]; s < tp.row_ptr[i + 1]; s++) block_mv<T, NR>(A.val + 9 * (size_t)s, x, tp.col[s], false, acc);
-    for (int k = tp.low_ptr[i]; k < tp.low_ptr[i + 1]; k++) {
-        int s = tp.low_slot[k];
-        block_mv<T, NR>(A.val + 9 * (size_t)s, x, tp.slot_row[s], true, acc);
+    if (i < tp.n) {
+        for (int s = tp.row_ptr[i] + g; s < tp.row_ptr[i + 1]; s += kSpG)
+            block_mv<T, NR>(A.val + 9 * (size_t)s, x, tp.col[s], false, acc);
+        for (int k = tp.low_ptr[i] + g; k < tp.low_ptr[i + 1]; k += kSpG) {
+            int s = tp.low_slot[k];
+            block_mv<T, NR>(A.val + 9 * (size_t)s, x, tp.slot_row[s], true, acc);
+        }
+        for (int u = tp.cu_ptr[i] + g; u < tp.cu_ptr[i + 1]; u += kSpG)
+            block_mv<T, NR>(A.uc + 9 * (size_t)u, x, tp.uc_col[u], false, acc);
+        for (int k = tp.cl_ptr[i] + g; k < tp.cl_ptr[i + 1]; k += kSpG) {
+            int u = tp.cl_idx[k];
+            block_mv<T, NR>(A.uc + 9 * (size_t)u, x, tp.uc_row[u], true, acc);
+        }
     }
-    for (int u = tp.cu_ptr[i]; u < tp.cu_ptr[i + 1]; u++) block_mv<T, NR>(A.uc + 9 * (size_t)u, x, tp.uc_col[u], false, acc);
-    for (int k = tp.cl_ptr[i]; k < tp.cl_ptr[i + 1]; k++) {
-        int u = tp.cl_idx[k];
-        block_mv<T, NR>(A.uc + 9 * (size_t)u, x, tp.uc_row[u], true, acc);
-    }
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int o = 1; o < kSpG; o <<= 1) acc[r][q] += __shfl_xor_sync(0xffffffffu, acc[r][q], o, kSpG);
 }
 
 template <class T>
 __global__ void k_spmv(Topo tp, MatView<T> A, const T* __restrict__ x, T* __restrict__ y) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= tp.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / kSpG, g = t % kSpG;
     T acc[1][3];
-    row_mv<T, 1>(tp, A, x, i, acc);
-    y[3 * i] = acc[0][0];
-    y[3 * i + 1] = acc[0][1];
-    y[3 * i + 2] = acc[0][2];
+    row_mv<T, 1>(tp, A, x, i, g, acc);
+    if (i < tp.n && g == 0) {
+        y[3 * i] = acc[0][0];
+        y[3 * i + 1] = acc[0][1];
+        y[3 * i + 2] = acc[0][2];
+    }
 }
 
 // ---- PCG kernels ----------------------------------------------------------------------------
@@ -201,13 +223,14 @@ __global__ void __launch_bounds__(256) k_pcg_spmv_dot(Topo tp, MatView<T> A, Pcg
 #pragma unroll
     for (int r = 0; r < NR; r++) any |= st_run[r] != 0;
     if (!any) return;  // uniform across the grid: state only changes in the last CTA below
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / kSpG, g = t % kSpG;
     double part[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) part[r] = 0.0;
-    if (i < tp.n) {
-        T acc[NR][3];
-        row_mv<T, NR>(tp, A, P.p, i, acc);
+    T acc[NR][3];
+    row_mv<T, NR>(tp, A, P.p, i, g, acc);
+    if (i < tp.n && g == 0) {
 #pragma unroll
         for (int r = 0; r < NR; r++)
 #pragma unroll
@@ -236,8 +259,10 @@ __global__ void __launch_bounds__(256) k_pcg_spmv_dot(Topo tp, MatView<T> A, Pcg
     }
 }
 
+// K2: one thread per MAS position (16-lane banks), so that the restriction of the updated
+// residual to levels 0 and 1 is a bank-local reduction with plain stores
 template <class T, class M, int NR>
-__global__ void __launch_bounds__(256) k_pcg_update(int nv, PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R) {
+__global__ void __launch_bounds__(256) k_pcg_update(PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R) {
     __shared__ double smem[NR * 8];
     __shared__ int st[NR];
     __shared__ double alpha[NR];
@@ -250,37 +275,36 @@ __global__ void __launch_bounds__(256) k_pcg_update(int nv, PcgPtrs<T, NR> P, Ma
 #pragma unroll
     for (int r = 0; r < NR; r++) any |= st[r] < 2;
     if (!any) return;
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = p < mv.npos ? mv.part_map[p] : -1;
     double part[NR];
+    M val[NR * 3];
 #pragma unroll
     for (int r = 0; r < NR; r++) part[r] = 0.0;
-    if (v < nv) {
-        const int* tv = mv.table + (size_t)v * mv.L;
+#pragma unroll
+    for (int k = 0; k < NR * 3; k++) val[k] = 0;
+    if (v >= 0) {
 #pragma unroll
         for (int r = 0; r < NR; r++) {
             if (st[r] == 2) continue;
             T a = (T)alpha[r];
-            T rv[3];
 #pragma unroll
             for (int q = 0; q < 3; q++) {
                 const size_t k = (size_t)(3 * v + q) * NR + r;
                 P.x[k] += a * P.p[k];
-                rv[q] = P.r[k] - a * P.Ap[k];
-                P.r[k] = rv[q];
-                part[r] += (double)rv[q] * (double)rv[q];
-            }
-            if (st[r] == 0) {
-                int p0 = tv[0];
-#pragma unroll
-                for (int q = 0; q < 3; q++) R[(size_t)(3 * p0 + q) * NR + r] = (M)rv[q];
-                for (int l = 1; l < mv.L; l++) {
-                    int g = tv[l];
-#pragma unroll
-                    for (int q = 0; q < 3; q++) atomicAdd(R + (size_t)(3 * g + q) * NR + r, (M)rv[q]);
-                }
+                T rv = P.r[k] - a * P.Ap[k];
+                P.r[k] = rv;
+                part[r] += (double)rv * (double)rv;
+                if (st[r] == 0) val[r * 3 + q] = (M)rv;
             }
         }
     }
+    if (p < mv.npos)
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) R[(size_t)(3 * p + q) * NR + r] = val[r * 3 + q];
+    bank_reduce_store<M, NR>(v >= 0 ? mv.up[p] : -1, val, R);
     double tot[NR];
     if (grid_sum<NR>(part, P.partial + NR * gridDim.x, P.ticket + 1, tot, smem) && threadIdx.x == 0) {
 #pragma unroll
@@ -291,6 +315,21 @@ __global__ void __launch_bounds__(256) k_pcg_update(int nv, PcgPtrs<T, NR> P, Ma
             if (s.crit == SGIPC_CRIT_TRUE && s.state == 0 && tot[r] <= s.tol * s.tol * s.bnorm2) s.state = 1;
         }
     }
+}
+
+// K3a: restriction to levels 2 .. L-1 in one CTA
+template <class M, int NR>
+__global__ void __launch_bounds__(1024) k_pcg_restrict_coarse(MasView mv, const PcgScalars* __restrict__ sc,
+                                                               M* __restrict__ R) {
+    __shared__ int any;
+    if (threadIdx.x == 0) {
+        int a = 0;
+        for (int r = 0; r < NR; r++) a |= sc[r].state == 0;
+        any = a;
+    }
+    __syncthreads();
+    if (!any) return;
+    restrict_coarse_cta<M, NR>(mv.info, mv.up, mv.L, R);
 }
 
 template <class M, int NR>
@@ -327,7 +366,7 @@ __global__ void __launch_bounds__(192) k_pcg_domain(const int* __restrict__ info
 
 template <class T, class M, int NR>
 __global__ void __launch_bounds__(256) k_pcg_prolong_dot(int nv, PcgPtrs<T, NR> P, MasView mv,
-                                                         const M* __restrict__ Z, M* __restrict__ R) {
+                                                         const M* __restrict__ Z) {
     __shared__ double smem[NR * 8];
     __shared__ int run[NR];
     if (threadIdx.x < NR) run[threadIdx.x] = P.sc[threadIdx.x].state == 0;
@@ -337,10 +376,6 @@ __global__ void __launch_bounds__(256) k_pcg_prolong_dot(int nv, PcgPtrs<T, NR> 
     for (int r = 0; r < NR; r++) any |= run[r] != 0;
     if (!any) return;
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    const int total = mv.info[16];
-    for (long long k = (long long)mv.npos * 3 * NR + v; k < (long long)total * 3 * NR;
-         k += (long long)gridDim.x * blockDim.x)
-        R[k] = 0;
     double part[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) part[r] = 0.0;
@@ -412,11 +447,11 @@ __global__ void __launch_bounds__(256) k_pcg_p_update(int n3, PcgPtrs<T, NR> P, 
 
 // ---- solve set-up kernels -------------------------------------------------------------------
 template <class T, class M, int NR>
-__global__ void k_pcg_init(int nv, const double* __restrict__ b, PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R,
-                           double tol, int max_iter, int crit) {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < NR) {
-        PcgScalars& s = P.sc[v];
+__global__ void k_pcg_init(const double* __restrict__ b, PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R, double tol,
+                           int max_iter, int crit) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < NR) {
+        PcgScalars& s = P.sc[p];
         s.state = 0;
         s.status = SGIPC_OK;
         s.iter = 0;
@@ -425,27 +460,28 @@ __global__ void k_pcg_init(int nv, const double* __restrict__ b, PcgPtrs<T, NR> 
         s.max_iter = max_iter;
         s.crit = crit;
     }
-    if (v >= nv) return;
-    const int* tv = mv.table + (size_t)v * mv.L;
+    const int v = p < mv.npos ? mv.part_map[p] : -1;
+    M val[NR * 3];
 #pragma unroll
-    for (int r = 0; r < NR; r++) {
-        T rv[3];
+    for (int k = 0; k < NR * 3; k++) val[k] = 0;
+    if (v >= 0) {
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const size_t k = (size_t)(3 * v + q) * NR + r;
-            rv[q] = (T)b[k];
-            P.r[k] = rv[q];
-            P.x[k] = 0;
-        }
-        int p0 = tv[0];
+        for (int r = 0; r < NR; r++)
 #pragma unroll
-        for (int q = 0; q < 3; q++) R[(size_t)(3 * p0 + q) * NR + r] = (M)rv[q];
-        for (int l = 1; l < mv.L; l++) {
-            int g = tv[l];
-#pragma unroll
-            for (int q = 0; q < 3; q++) atomicAdd(R + (size_t)(3 * g + q) * NR + r, (M)rv[q]);
-        }
+            for (int q = 0; q < 3; q++) {
+                const size_t k = (size_t)(3 * v + q) * NR + r;
+                T rv = (T)b[k];
+                P.r[k] = rv;
+                P.x[k] = 0;
+                val[r * 3 + q] = (M)rv;
+            }
     }
+    if (p < mv.npos)
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) R[(size_t)(3 * p + q) * NR + r] = val[r * 3 + q];
+    bank_reduce_store<M, NR>(v >= 0 ? mv.up[p] : -1, val, R);
 }
 
 template <class T, int NR>
@@ -544,6 +580,8 @@ MasView mas_view(SgipcCtx* c) {
     m.L = c->mas.levelnum;
     m.npos = c->mas.npos;
     m.info = c->mas.info;
+    m.part_map = c->mas.part_map;
+    m.up = c->mas.up;
     return m;
 }
 
@@ -565,10 +603,11 @@ void enqueue_body(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, cudaGraphCo
     const int n = c->n, nv = c->nv;
     PcgPtrs<T, NR> P = ptrs_of<T, NR>(w);
     MasView mv = mas_view(c);
-    k_pcg_spmv_dot<T, NR><<<nblk(n), 256, 0, s>>>(topo_of(c), mat_view<T>(c), P);
-    k_pcg_update<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, R);
+    k_pcg_spmv_dot<T, NR><<<spmv_grid(n), 256, 0, s>>>(topo_of(c), mat_view<T>(c), P);
+    k_pcg_update<T, M, NR><<<nblk(mv.npos), 256, 0, s>>>(P, mv, R);
+    k_pcg_restrict_coarse<M, NR><<<1, 1024, 0, s>>>(mv, w.sc, R);
     k_pcg_domain<M, NR><<<(ndom + 3) / 4, 192, 0, s>>>(c->mas.info, w.sc, inv, R, Z);
-    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z, R);
+    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z);
     k_pcg_p_update<T, NR><<<nblk(3LL * n), 256, 0, s>>>(3 * n, P, h, use_cond);
 }
 
@@ -583,8 +622,12 @@ SgipcStatus get_loop_graph(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, in
     }
     cudaGraph_t g = nullptr;
     SG_CHECK(c, cudaGraphCreate(&g, 0));
-    cudaGraphConditionalHandle h;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphConditionalHandle h = 0;
+    // SGIPC_NO_COND_GRAPH=1 selects the relaunched fixed-length graph (profilers that do
+    // not descend into conditional bodies then see every iteration kernel)
+    const char* nc = getenv("SGIPC_NO_COND_GRAPH");
+    cudaError_t e = (nc && nc[0] == '1') ? cudaErrorNotSupported
+                                         : cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
     bool ok = e == cudaSuccess;
     cudaGraphNode_t node;
     cudaGraph_t body = nullptr;
@@ -647,11 +690,11 @@ SgipcStatus run_pcg(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, doub
     const int nv = c->nv, n = c->n;
     PcgPtrs<T, NR> P = ptrs_of<T, NR>(w);
     MasView mv = mas_view(c);
-    SG_COUNT(c, 4);
-    SG_CHECK(c, cudaMemsetAsync(R, 0, sizeof(M) * 3 * (size_t)m.h_info[16] * NR, s));
-    k_pcg_init<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, b, P, mv, R, tol, max_iter, crit);
+    SG_COUNT(c, 5);
+    k_pcg_init<T, M, NR><<<nblk(mv.npos), 256, 0, s>>>(b, P, mv, R, tol, max_iter, crit);
+    k_pcg_restrict_coarse<M, NR><<<1, 1024, 0, s>>>(mv, w.sc, R);
     k_pcg_domain<M, NR><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, w.sc, inv, R, Z);
-    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z, R);
+    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z);
     k_pcg_init_finish<T, NR><<<nblk(3LL * n), 256, 0, s>>>(3 * n, b, P);
     SG_LAUNCH_CHECK(c, "pcg init");
     if (w.cond_graph) {
@@ -695,7 +738,7 @@ namespace sgipc {
 
 SgipcStatus pcg_create(SgipcCtx* c) {
     int maxn = c->n > c->nv ? c->n : c->nv;
-    c->max_blocks = nblk(3LL * maxn, 256) + 8;
+    c->max_blocks = nblk((long long)kSpG * maxn, 256) + 8;
     SgipcStatus st;
     if ((st = alloc_work(c, c->pcg64, sizeof(double), c->max_rhs)) != SGIPC_OK) return st;
     if ((st = alloc_work(c, c->pcg32, sizeof(float), c->max_rhs)) != SGIPC_OK) return st;
@@ -723,7 +766,7 @@ void pcg_destroy(SgipcCtx* c) {
 template <class T>
 SgipcStatus spmv_t(SgipcCtx* c, const T* x, T* y, cudaStream_t s) {
     SG_COUNT(c, 1);
-    k_spmv<T><<<nblk(c->n), 256, 0, s>>>(topo_of(c), mat_view<T>(c), x, y);
+    k_spmv<T><<<spmv_grid(c->n), 256, 0, s>>>(topo_of(c), mat_view<T>(c), x, y);
     SG_LAUNCH_CHECK(c, "spmv");
     return SGIPC_OK;
 }
@@ -783,7 +826,7 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         PcgScalars hs;
         SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg64.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
         SG_CHECK(c, cudaStreamSynchronize(s));
-        SG_COUNT(c, 5LL * hs.bodies);
+        SG_COUNT(c, 6LL * hs.bodies);
         out.iterations = hs.iter;
         out.refinements = 0;
         out.rz0 = hs.rz0;
@@ -816,7 +859,7 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
             SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
             SG_CHECK(c, cudaStreamSynchronize(s));
             total_it += hs.iter;
-            SG_COUNT(c, 5LL * hs.bodies);
+            SG_COUNT(c, 6LL * hs.bodies);
             if (ref == 0) {
                 rz0 = hs.rz0;
                 bn2 = hs.bnorm2;
@@ -908,7 +951,7 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
     SG_CHECK(c, cudaMemcpyAsync(hs, w.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
     SG_CHECK(c, cudaStreamSynchronize(s));
     SgipcStatus worst = SGIPC_OK;
-    SG_COUNT(c, 5LL * hs[0].bodies);
+    SG_COUNT(c, 6LL * hs[0].bodies);
     for (int r = 0; r < 4; r++) {
         if (stats) {
             stats[r] = SgipcSolveStats{};
@@ -934,9 +977,9 @@ SgipcStatus pcg_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
     SG_CHECK(c, cudaStreamSynchronize(s));
     SG_COUNT(c, 1);
     if (f64)
-        k_spmv<double><<<nblk(c->n), 256, 0, s>>>(topo_of(c), mat_view<double>(c), c->tmp64, c->tmp64b);
+        k_spmv<double><<<spmv_grid(c->n), 256, 0, s>>>(topo_of(c), mat_view<double>(c), c->tmp64, c->tmp64b);
     else
-        k_spmv<float><<<nblk(c->n), 256, 0, s>>>(topo_of(c), mat_view<float>(c), (const float*)c->tmp64,
+        k_spmv<float><<<spmv_grid(c->n), 256, 0, s>>>(topo_of(c), mat_view<float>(c), (const float*)c->tmp64,
                                                   (float*)c->tmp64b);
     // nb (sb + 4) + (n + 1) 4 + 2 * 3n * sv with nb = static + unique contact blocks
     const double sb = f64 ? 72 : 36, sv = f64 ? 8 : 4;
