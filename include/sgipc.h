@@ -200,6 +200,12 @@ SgipcStatus sgipc_mas_info(SgipcCtx* ctx, int32_t* levelnum, int32_t* level_coun
  * levels 1..levelnum-1, int[V*(levelnum-1)]) for hierarchy parity tests. */
 SgipcStatus sgipc_mas_export_tables(SgipcCtx* ctx, int32_t* table);
 
+/* Host copy of the MAS domain inverses, total_clusters/16 dense row-major 48x48 blocks
+ * (FP64; FP32-built inverses are widened), in the order of the global cluster index —
+ * the contents of MASPreconditioner::d_inverseMatMas / d_precondMatMas
+ * (MASPreconditioner.cuh:44-45) unpacked.  For checkpoints and parity tests. */
+SgipcStatus sgipc_mas_export_domains(SgipcCtx* ctx, double* inverses);
+
 /* ---- solve ------------------------------------------------------------------------- */
 
 /* PCGSolver::pcg (pcg_solver.cu:174-267) on the assembled system: x [dev] = A^-1 b.

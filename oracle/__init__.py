@@ -58,6 +58,7 @@ def lib():
         L.or_mas_free.argtypes = [C.c_void_p]
         L.or_mas_info.argtypes = [C.c_void_p, _i, _i, _i, _i]
         L.or_mas_table.argtypes = [C.c_void_p, _i]
+        L.or_mas_domains.argtypes = [C.c_void_p, _d]
         L.or_mas_apply.argtypes = [C.c_void_p, _d, _d, C.c_int]
         L.or_pcg.argtypes = [C.c_int, _i, _i, _d, C.c_int, C.c_void_p, C.c_int, _d, _d, C.c_double,
                              C.c_int, _d, _d]
@@ -238,6 +239,12 @@ class Mas:
         t = np.zeros(self.nv * L, np.int32)
         lib().or_mas_table(self.h, _p(t, _i))
         return t.reshape(self.nv, L)
+
+    def domains(self):
+        total = self.info()[3]
+        d = np.zeros((total // 16, 48, 48))
+        lib().or_mas_domains(self.h, _p(d))
+        return d
 
     def apply(self, r, single=False):
         r = _f64(r)

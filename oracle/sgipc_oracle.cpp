@@ -907,6 +907,11 @@ void or_mas_info(void* h, int* levelnum, int* starts, int* counts, int* total) {
     *total = M->total;
 }
 
+void or_mas_domains(void* h, double* out) {
+    OrMas* M = (OrMas*)h;
+    std::copy(M->inv->begin(), M->inv->end(), out);
+}
+
 void or_mas_table(void* h, int32_t* out) {
     OrMas* M = (OrMas*)h;
     std::copy(M->table->begin(), M->table->end(), out);

@@ -535,3 +535,18 @@ extern "C" SgipcStatus sgipc_mas_export_tables(SgipcCtx* c, int32_t* table) {
     SG_CHECK(c, cudaMemcpy(table, c->mas.table, sizeof(int) * (size_t)c->nv * c->mas.levelnum, cudaMemcpyDeviceToHost));
     return SGIPC_OK;
 }
+
+extern "C" SgipcStatus sgipc_mas_export_domains(SgipcCtx* c, double* out) {
+    if (!c || !out) return SGIPC_BAD_INPUT;
+    if (!c->mas.built) return SGIPC_NOT_READY;
+    SG_CHECK(c, cudaDeviceSynchronize());
+    const size_t n = (size_t)(c->mas.h_info[16] / 16) * 2304;
+    if (c->mas.built == SGIPC_FP64 + 1) {
+        SG_CHECK(c, cudaMemcpy(out, c->mas.dom64, n * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp(n);
+        SG_CHECK(c, cudaMemcpy(tmp.data(), c->mas.dom32, n * sizeof(float), cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < n; k++) out[k] = tmp[k];
+    }
+    return SGIPC_OK;
+}

@@ -298,6 +298,13 @@ class MASPreconditioner:
         N.check(N.lib().sgipc_mas_info(self.g.ctx, C.byref(ln), counts, C.byref(tot)), self.g.ctx)
         return ln.value, np.array(counts[:ln.value]), tot.value
 
+    def domains(self):
+        """Dense 48x48 domain inverses, (total_clusters/16, 48, 48) float64."""
+        total = self.info()[2]
+        d = np.zeros((total // 16, 48, 48))
+        N.check(N.lib().sgipc_mas_export_domains(self.g.ctx, d.ctypes.data_as(C.c_void_p)), self.g.ctx)
+        return d
+
     def tables(self):
         L = self.info()[0]
         t = np.zeros(self.g.n * L, np.int32)

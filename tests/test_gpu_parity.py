@@ -70,6 +70,9 @@ def test_mas_hierarchy_and_apply(case):
     gl, gcounts, gtotal = mas.info()
     assert gl == L and gtotal == total and np.array_equal(gcounts, counts)
     assert np.array_equal(mas.tables(), om.table())
+    gd, od = mas.domains(), om.domains()
+    for d in range(len(od)):
+        assert _rel(gd[d], od[d]) < 1e-9, d
     r = np.random.default_rng(1).normal(size=3 * sc.nv)
     z = mas.preconditioning(torch.tensor(r, device="cuda")).cpu().numpy()
     assert _rel(z, om.apply(r)) < 1e-9
