@@ -206,6 +206,11 @@ SgipcStatus sgipc_mas_export_tables(SgipcCtx* ctx, int32_t* table);
  * (MASPreconditioner.cuh:44-45) unpacked.  For checkpoints and parity tests. */
 SgipcStatus sgipc_mas_export_domains(SgipcCtx* ctx, double* inverses);
 
+/* Restriction of r [dev double3[V]] to every level, R [host double[3*total_clusters]]
+ * indexed by global cluster (__buildMultiLevelR_optimized_new, MASPreconditioner.cu:729).
+ * Synchronises.  For parity tests of the restriction operator. */
+SgipcStatus sgipc_mas_restrict(SgipcCtx* ctx, const double* r, double* R);
+
 /* ---- solve ------------------------------------------------------------------------- */
 
 /* PCGSolver::pcg (pcg_solver.cu:174-267) on the assembled system: x [dev] = A^-1 b.

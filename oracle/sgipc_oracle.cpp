@@ -742,8 +742,11 @@ typedef struct OrMas {
 
 // Connected components of the bank-local graph given by per-node 16-bit masks; returns
 // the new node id of every node (numbered bank by bank, components ordered by their
-// lowest lane) and the number of new nodes.
-static int bank_components(int count, const std::vector<uint32_t>& mask, std::vector<int>& next) {
+// lowest lane) and the number of new nodes.  Nodes with real[i] == 0 (padding positions
+// of level 0) are no node: they are skipped, as _preparePrefixSumL0_new and
+// _buildLevel1_new skip partId_map_real < 0 (MASPreconditioner.cu:157-270).
+static int bank_components(int count, const std::vector<uint32_t>& mask, const std::vector<char>& real,
+                           std::vector<int>& next) {
     next.assign(count, -1);
     int nid = 0;
     int nbank = (count + 15) / 16;
@@ -751,7 +754,7 @@ static int bank_components(int count, const std::vector<uint32_t>& mask, std::ve
         int lo = bk * 16, hi = std::min(count, lo + 16);
         // transitive closure of masks within the bank
         std::vector<uint32_t> comp(16, 0);
-        for (int i = lo; i < hi; i++) comp[i - lo] = mask[i] | (1u << (i - lo));
+        for (int i = lo; i < hi; i++) comp[i - lo] = real[i] ? (mask[i] | (1u << (i - lo))) : 0u;
         bool changed = true;
         while (changed) {
             changed = false;
@@ -771,10 +774,12 @@ static int bank_components(int count, const std::vector<uint32_t>& mask, std::ve
             if (!ch) break;
         }
         for (int i = lo; i < hi; i++) {
+            if (!real[i]) continue;
             int lead = __builtin_ctz(comp[i - lo]);
             if (lead == i - lo) next[i] = nid++;
         }
-        for (int i = lo; i < hi; i++) next[i] = next[lo + __builtin_ctz(comp[i - lo])];
+        for (int i = lo; i < hi; i++)
+            if (real[i]) next[i] = next[lo + __builtin_ctz(comp[i - lo])];
     }
     return nid;
 }
@@ -838,7 +843,10 @@ void* or_mas_build(int nv, int npos, const int32_t* part_map, const int32_t* rea
             if (a != b && a / 16 == b / 16) mask[a] |= 1u << (b % 16);
         }
         std::vector<int> next;
-        int nnext = bank_components(count, mask, next);
+        std::vector<char> real(count, 1);
+        if (l == 0)
+            for (int p = 0; p < count; p++) real[p] = part_map[p] >= 0;
+        int nnext = bank_components(count, mask, real, next);
         start += padded;
         padded = (nnext + 15) / 16 * 16;
         M->level_start[l + 1] = start;

@@ -80,10 +80,12 @@ __global__ void k_mask_pairs(int np, const int4* __restrict__ pairs, int nv, con
             }
 }
 
-// One thread per bank: components by repeated OR closure, numbered by lowest lane.
+// One thread per bank: components by repeated OR closure, numbered by lowest lane.  At
+// level 0 the padding positions (part_map < 0) are no node and form no component
+// (_preparePrefixSumL0_new / _buildLevel1_new skip them, MASPreconditioner.cu:157-270).
 __global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, int level,
-                                  const uint32_t* __restrict__ mask, int* __restrict__ rank,
-                                  int* __restrict__ bank_cnt) {
+                                  const uint32_t* __restrict__ mask, const int* __restrict__ part_map,
+                                  int* __restrict__ rank, int* __restrict__ bank_cnt) {
     int bk = blockIdx.x * blockDim.x + threadIdx.x;
     if (bk > nbank_cap) return;
     const int count = info[8 + level];
@@ -95,7 +97,10 @@ __global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, i
     const int lo = bk << 4, hi = min(count, lo + 16);
     uint32_t comp[16];
 #pragma unroll
-    for (int i = 0; i < 16; i++) comp[i] = (lo + i < hi) ? (mask[lo + i] | (1u << i)) : (1u << i);
+    for (int i = 0; i < 16; i++) {
+        const bool real = lo + i < hi && (level > 0 || part_map[lo + i] >= 0);
+        comp[i] = real ? (mask[lo + i] | (1u << i)) : 0u;
+    }
     for (int it = 0; it < 16; it++) {
         bool changed = false;
 #pragma unroll
@@ -118,7 +123,7 @@ __global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, i
         if (lo + i < hi && (__ffs(comp[i]) - 1) == i) leaders |= 1u << i;
     for (int i = 0; i < hi - lo; i++) {
         int lead = __ffs(comp[i]) - 1;
-        rank[lo + i] = __popc(leaders & ((1u << lead) - 1u));
+        rank[lo + i] = lead < 0 ? 0 : __popc(leaders & ((1u << lead) - 1u));
     }
     bank_cnt[bk] = __popc(leaders);
 }
@@ -436,7 +441,8 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
         if (con && con->pair_num > 0)
             k_mask_pairs<<<nblk(con->pair_num), SGIPC_BLOCK, 0, s>>>(con->pair_num, (const int4*)con->pairs, nv,
                                                                      m.node, m.mask);
-        k_bank_components<<<nblk(nbank_cap + 1, 128), 128, 0, s>>>(nbank_cap, m.info, l, m.mask, m.comp_rank,
+        k_bank_components<<<nblk(nbank_cap + 1, 128), 128, 0, s>>>(nbank_cap, m.info, l, m.mask, m.part_map,
+                                                                   m.comp_rank,
                                                                    m.bank_cnt);
         size_t tb = m.scan_tmp_bytes;
         SG_CHECK(c, cub::DeviceScan::ExclusiveSum(m.scan_tmp, tb, m.bank_cnt, m.bank_off, nbank_cap + 1, s));
@@ -548,5 +554,19 @@ extern "C" SgipcStatus sgipc_mas_export_domains(SgipcCtx* c, double* out) {
         SG_CHECK(c, cudaMemcpy(tmp.data(), c->mas.dom32, n * sizeof(float), cudaMemcpyDeviceToHost));
         for (size_t k = 0; k < n; k++) out[k] = tmp[k];
     }
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_mas_restrict(SgipcCtx* c, const double* r, double* out) {
+    if (!c || !r || !out) return SGIPC_BAD_INPUT;
+    if (!c->mas.built) return SGIPC_NOT_READY;
+    MasWork& m = c->mas;
+    SG_CHECK(c, cudaDeviceSynchronize());
+    k_restrict01<double, double><<<nblk(m.npos), SGIPC_BLOCK>>>(m.npos, r, m.part_map, m.up, m.R64);
+    k_restrict_coarse<double><<<1, 1024>>>(m.info, m.up, m.levelnum, m.R64);
+    SG_COUNT(c, 2);
+    SG_LAUNCH_CHECK(c, "mas restrict");
+    SG_CHECK(c, cudaDeviceSynchronize());
+    SG_CHECK(c, cudaMemcpy(out, m.R64, sizeof(double) * 3 * (size_t)m.h_info[16], cudaMemcpyDeviceToHost));
     return SGIPC_OK;
 }

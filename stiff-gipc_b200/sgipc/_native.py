@@ -78,6 +78,7 @@ SIGNATURES = {
     "sgipc_adjoint_param_grads": ([_vp, C.POINTER(SgipcFemData), C.POINTER(SgipcParams), C.c_double, _i32, _vp,
                                    _vp, _vp, _vp], _i32),
     "sgipc_mas_export_domains": ([_vp, _vp], _i32),
+    "sgipc_mas_restrict": ([_vp, _vp, _vp], _i32),
     "sgipc_launch_count": ([_vp, C.POINTER(C.c_int64)], _i32),
     "sgipc_time_kernel": ([_vp, C.c_char_p, _i32, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)], _i32),
 }
