@@ -74,6 +74,16 @@ def test_mas_hierarchy_and_apply(case):
     for d in range(len(od)):
         assert _rel(gd[d], od[d]) < 1e-9, d
     r = np.random.default_rng(1).normal(size=3 * sc.nv)
+    # restriction operator: R[g] = sum of r over the vertices of cluster g, every level
+    import ctypes
+    R = np.zeros(3 * total)
+    rt = torch.tensor(r, device="cuda")
+    N.check(N.lib().sgipc_mas_restrict(g.ctx, ctypes.c_void_p(rt.data_ptr()), R.ctypes.data_as(ctypes.c_void_p)))
+    Rd = np.zeros((total, 3))
+    tab = om.table()
+    for lvl in range(L):
+        np.add.at(Rd, tab[:, lvl], r.reshape(-1, 3))
+    assert _rel(R.reshape(-1, 3), Rd) < 1e-12
     z = mas.preconditioning(torch.tensor(r, device="cuda")).cpu().numpy()
     assert _rel(z, om.apply(r)) < 1e-9
     mas.setPreconditioner("ref")
