@@ -166,10 +166,19 @@ __global__ void __launch_bounds__(128) k_snk(int nt, const uint32_t* __restrict_
 // ------------------------------------------------------------------------------------------
 // static gathers
 // ------------------------------------------------------------------------------------------
+struct StaticOut {
+    double* v64;       // upper slots
+    float* v32;
+    const int* fup;    // full-pattern index of each upper slot
+    const int* flo;    // full-pattern index of its transpose (-1 on the diagonal)
+    double* f64;       // full symmetric copy
+    float* f32;
+};
+
 __global__ void k_gather_blocks(int nnz, const int* __restrict__ cptr, const int* __restrict__ contrib,
                                 const double* __restrict__ eblk, const int* __restrict__ slot_row,
                                 const int* __restrict__ col, const int32_t* __restrict__ btype,
-                                const double* __restrict__ mass, double* __restrict__ v64, float* __restrict__ v32) {
+                                const double* __restrict__ mass, StaticOut o) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= 9LL * nnz) return;
     int s = (int)(tid / 9), q = (int)(tid % 9);
@@ -178,8 +187,28 @@ __global__ void k_gather_blocks(int nnz, const int* __restrict__ cptr, const int
     if (btype[r] == 0 && btype[c] == 0)
         for (int k = cptr[s]; k < cptr[s + 1]; k++) acc += eblk[9 * (size_t)contrib[k] + q];
     if (r == c && (q == 0 || q == 4 || q == 8)) acc += mass[r];
-    v64[tid] = acc;
-    v32[tid] = (float)acc;
+    o.v64[tid] = acc;
+    o.v32[tid] = (float)acc;
+    const size_t fu = 9 * (size_t)o.fup[s] + q;
+    o.f64[fu] = acc;
+    o.f32[fu] = (float)acc;
+    const int fl = o.flo[s];
+    if (fl >= 0) {
+        const size_t ft = 9 * (size_t)fl + 3 * (q % 3) + q / 3;
+        o.f64[ft] = acc;
+        o.f32[ft] = (float)acc;
+    }
+}
+
+static StaticOut static_out(SgipcCtx* c) {
+    StaticOut o;
+    o.v64 = c->val64;
+    o.v32 = c->val32;
+    o.fup = c->fup;
+    o.flo = c->flo;
+    o.f64 = c->fval64;
+    o.f32 = c->fval32;
+    return o;
 }
 
 __global__ void k_gather_grad(int nv, const int* __restrict__ vptr, const int* __restrict__ vinc,
@@ -618,6 +647,13 @@ __global__ void k_row_ptr_rows(int n, const int* __restrict__ nuc, const int* __
     ptr[i] = lo;
 }
 
+// column of each transposed contact entry: the row field of its (col << bits | row) key
+__global__ void k_lower_cols(int m, const unsigned long long* __restrict__ ks, int bits, int* __restrict__ cl_col) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    cl_col[k] = (int)(ks[k] & ((1ull << bits) - 1ull));
+}
+
 __global__ void k_row_ptr_keys(int n, int m, const unsigned long long* __restrict__ ks, int bits, int* __restrict__ ptr) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n) return;
@@ -709,7 +745,7 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
         return SGIPC_OK;
     }
     const int endbit = 2 * c->key_bits;
-    SG_COUNT(c, 5);
+    SG_COUNT(c, 6);
     size_t tb = c->cub_tmp_bytes;
     SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->ckey, c->ckey_s, c->cidx, c->cidx_s, m, 0, endbit, s));
     k_head_flags<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cflag);
@@ -722,6 +758,7 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
     tb = c->cub_tmp_bytes;
     SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->lkey, c->lkey_s, c->lidx, c->cl_idx, m, 0, endbit, s));
     k_row_ptr_keys<<<nblk(c->n + 1), SGIPC_BLOCK, 0, s>>>(c->n, m, c->lkey_s, c->key_bits, c->cl_ptr);
+    k_lower_cols<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->lkey_s, c->key_bits, c->cl_col);
     SG_LAUNCH_CHECK(c, "contact merge");
     return SGIPC_OK;
 }
@@ -739,7 +776,7 @@ static SgipcStatus launch_fem(SgipcCtx* c, const SgipcFemData* f, const SgipcPar
 static SgipcStatus gather_static(SgipcCtx* c, const SgipcFemData* f, cudaStream_t s) {
     SG_COUNT(c, 1 + (c->n_egrad > 0));
     k_gather_blocks<<<nblk(9LL * c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->contrib_ptr, c->contrib, c->eblk, c->slot_row,
-                                                                c->col, f->BoundaryType, f->masses, c->val64, c->val32);
+                                                                c->col, f->BoundaryType, f->masses, static_out(c));
     if (c->n_egrad > 0)
         k_gather_grad<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, c->vinc_ptr, c->vinc, c->egrad, c->shape_grads);
     SG_LAUNCH_CHECK(c, "static gather");
@@ -841,7 +878,7 @@ SgipcStatus assemble_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, do
         SG_COUNT(c, 1);
         k_gather_blocks<<<nblk(9LL * c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->contrib_ptr, c->contrib, c->eblk,
                                                                     c->slot_row, c->col, f->BoundaryType, f->masses,
-                                                                    c->val64, c->val32);
+                                                                    static_out(c));
         *bytes = (double)c->n_eblk * (72 + 4) + (double)c->nnz * (72 + 36 + 8 + 4);
     } else if (!strcmp(name, "barrier")) {
         if (!k || k->pair_num <= 0) return SGIPC_BAD_INPUT;

@@ -133,6 +133,31 @@ static SgipcStatus build_static(SgipcCtx* c, const SgipcTopology* t) {
     std::vector<int> vinc(std::max((size_t)1, egv.size())), vf(vptr.begin(), vptr.end() - 1);
     for (size_t e = 0; e < egv.size(); e++) vinc[vf[egv[e]]++] = (int)e;
 
+    // full symmetric pattern: row i holds its upper slots and the transposes of the
+    // upper slots (j, i), j < i; every block sits contiguously with its column index
+    std::vector<int> frow(n + 1, 0);
+    for (int i = 0; i < n; i++) frow[i + 1] = (row_ptr[i + 1] - row_ptr[i]) + (low_ptr[i + 1] - low_ptr[i]);
+    for (int i = 0; i < n; i++) frow[i + 1] += frow[i];
+    c->nnz_full = frow[n];
+    std::vector<int> fcol(std::max(c->nnz_full, 1)), fup(nnz), flo(nnz, -1);
+    for (int i = 0; i < n; i++) {
+        int k = frow[i];
+        for (int q = low_ptr[i]; q < low_ptr[i + 1]; q++) {  // (j, i) with j < i, as B^T
+            int s = low_slot[q];
+            fcol[k] = slot_row[s];
+            flo[s] = k++;
+        }
+        for (int s = row_ptr[i]; s < row_ptr[i + 1]; s++) {
+            fcol[k] = col[s];
+            fup[s] = k++;
+        }
+    }
+    SG_TRY(upload(c, &c->frow_ptr, frow));
+    SG_TRY(upload(c, &c->fcol, fcol));
+    SG_TRY(upload(c, &c->fup, fup));
+    SG_TRY(upload(c, &c->flo, flo));
+    SG_TRY(dalloc(c, &c->fval64, (size_t)c->nnz_full * 9));
+    SG_TRY(dalloc(c, &c->fval32, (size_t)c->nnz_full * 9));
     SG_TRY(upload(c, &c->row_ptr, row_ptr));
     SG_TRY(upload(c, &c->col, col));
     SG_TRY(upload(c, &c->slot_row, slot_row));
@@ -218,6 +243,7 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
         (st = dalloc(c, &c->uc_col, cap)) || (st = dalloc(c, &c->uc64, cap * 9)) ||
         (st = dalloc(c, &c->uc32, cap * 9)) || (st = dalloc(c, &c->cu_ptr, n + 1)) ||
         (st = dalloc(c, &c->cl_ptr, n + 1)) || (st = dalloc(c, &c->cl_idx, cap)) || (st = dalloc(c, &c->lkey, cap)) ||
+        (st = dalloc(c, &c->cl_col, cap)) ||
         (st = dalloc(c, &c->lkey_s, cap)) || (st = dalloc(c, &c->lidx, cap)) || (st = dalloc(c, &c->dflag, 4)))
         return fail(st);
     SG_CHECK(c, cudaMemset(c->dflag, 0, 4 * sizeof(int)));
@@ -250,7 +276,8 @@ extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
                     c->eblk, c->contrib_ptr, c->contrib, c->egrad, c->vinc_ptr, c->vinc, c->tets, c->tris,
                     c->hinges, c->hinge_adj, c->soft_idx, c->shape_grads, c->fb, c->b, c->ckey, c->ckey_s,
                     c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,
-                    c->cu_ptr, c->cl_ptr, c->cl_idx, c->lkey, c->lkey_s, c->lidx, c->cub_tmp, c->dflag};
+                    c->cu_ptr, c->cl_ptr, c->cl_idx, c->lkey, c->lkey_s, c->lidx, c->cub_tmp, c->dflag,
+                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete c;

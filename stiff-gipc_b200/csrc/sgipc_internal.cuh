@@ -30,6 +30,10 @@ struct PcgScalars {
     int32_t status;   // SgipcStatus
     int32_t crit;     // SgipcCriterion
     int32_t bodies;   // iteration bodies executed (hard bound on the graph's while loop)
+    int32_t first;    // 1 until the first SpMV (p = z, no beta)
+    int32_t pcur;     // which of the two p buffers holds the current direction
+    int32_t halt;     // [rhs 0 only] set once the loop must stop; later bodies return at once
+    int32_t pad;
 };
 
 // One precision's PCG workspace (T = double or float) for up to `nrhs` right-hand sides.
@@ -38,6 +42,7 @@ struct PcgWork {
     void* r;
     void* z;
     void* p;
+    void* p2;                // second direction buffer (the SpMV forms p = z + beta p_old on the fly)
     void* Ap;
     PcgScalars* sc;          // [nrhs]
     double* partial;         // reduction partials [nrhs][max_blocks]
@@ -94,6 +99,14 @@ struct SgipcCtx {
     int* low_slot;            // [nnz - n]
     double* val64;            // [nnz*9]
     float* val32;             // [nnz*9]
+    // full symmetric copy of the static blocks (both triangles) for the SpMV
+    int nnz_full;             // 2*nnz - n
+    int* frow_ptr;            // [n+1]
+    int* fcol;                // [nnz_full]
+    int* fup;                 // [nnz] full index of upper slot s
+    int* flo;                 // [nnz] full index of its transpose (-1 on the diagonal)
+    double* fval64;           // [nnz_full*9]
+    float* fval32;            // [nnz_full*9]
     // element blocks and their gather lists
     int n_eblk;               // 10 per tet, 6 per triangle, 10 per hinge
     double* eblk;             // [n_eblk*9] oriented element blocks
@@ -131,6 +144,7 @@ struct SgipcCtx {
     int* cu_ptr;                  // [n+1] unique contact blocks by row (upper)
     int* cl_ptr;                  // [n+1] transposed entries by row
     int* cl_idx;                  // [cap]
+    int* cl_col;                  // [cap] column of each transposed entry (= uc_row[cl_idx])
     unsigned long long* lkey;     // [cap]
     unsigned long long* lkey_s;
     int* lidx;

@@ -234,8 +234,10 @@ __global__ void __launch_bounds__(192) k_invert(int ndom, double* __restrict__ d
     double col[48];
     const double* D = dom + (size_t)(act ? d : 0) * 2304;
 #pragma unroll
-    for (int i = 0; i < 48; i++) col[i] = act ? D[i * 48 + j] : (i == j ? 1.0 : 0.0);
-    if (col[j] == 0.0) col[j] = 1.0;  // a zero diagonal (padding node) becomes 1
+    for (int i = 0; i < 48; i++) {
+        double a = act ? D[i * 48 + j] : (i == j ? 1.0 : 0.0);
+        col[i] = (i == j && a == 0.0) ? 1.0 : a;  // a zero diagonal (padding node) becomes 1
+    }
 #pragma unroll
     for (int k = 0; k < 48; k++) {
         double* pc = piv[k & 1][ld];

@@ -1,4 +1,4 @@
-// sgipc_pcg.cu — symmetric BSR SpMV and MAS-preconditioned conjugate gradients.
+// sgipc_pcg.cu — symmetric block SpMV and MAS-preconditioned conjugate gradients.
 //
 // Algorithm of PCGSolver::pcg (StiffGIPC/linear_system/solver/pcg_solver.cu:174-267):
 //   r = b, z = M r, p = z, rz0 = rz = r.z
@@ -7,18 +7,21 @@
 //     if |rz| <= tol * rz0: break          (tested on the rz from before the update)
 //     z = M r; rz_new = r.z; p = z + (rz_new / rz) p; rz = rz_new
 // The reference does each dot with a two-pass reduction and a blocking cudaMemcpy (two
-// host round trips per iteration).  Here every scalar stays in device memory: each
-// reduction finishes in the kernel's last CTA, a per-solve `state` word lets kernels of a
-// finished solve return at once, and the whole loop is one CUDA graph whose while-node
-// condition is set by the last kernel of the iteration body — one launch per solve.
+// host round trips per iteration).  Here every scalar stays in device memory, each
+// reduction finishes in the kernel's last CTA, and the whole loop is one CUDA graph whose
+// while-node condition is set on the device — one launch per solve.
 //
-// Kernels of one iteration (T = vector type, M = MAS type, NR = right-hand sides):
-//   K1 spmv_dot    Ap = A p over the static BSR (upper + transposed lists) and the unique
-//                  contact blocks, fused with p.Ap; last CTA: alpha, stop test, iteration cap
-//   K2 update      x += alpha p, r -= alpha Ap, MAS restriction of r (level 0 + coarse)
-//   K3 domain_mv   Z = A_d^-1 R for every 16-node domain (all NR columns per read of A_d^-1)
-//   K4 prolong_dot z = sum_l Z, r.z; last CTA: rz_next
-//   K5 p_update    p = z + beta p; sets the graph's loop condition
+// One iteration is four kernels (T = vector type, M = MAS type, NR = right-hand sides):
+//   K1 spmv_dot   p = z + beta p_old formed on the fly (ping-pong buffers), Ap = A p over
+//                 the full symmetric static CSR plus the unique contact blocks, p.Ap;
+//                 last CTA: rz, alpha, the r.z stop test
+//   K2 update     x += alpha p, r -= alpha Ap, restriction of r to MAS levels 0 and 1
+//                 (bank-local, no atomics); last CTA: ||r||^2, the true-residual stop test
+//   K3 domains    CTA 0 restricts r to the coarse levels and solves their domains, the
+//                 other CTAs solve the level-0/1 domains Z_d = A_d^-1 R_d
+//   K4 prolong    z = sum_l Z (gather), r.z; its first thread decides whether the graph
+//                 runs another body (stop state, iteration cap, body bound) and sets the
+//                 while-node condition; later bodies return at once once `halt` is set.
 #include <cstdlib>
 #include <cub/cub.cuh>
 #include <vector>
@@ -32,22 +35,19 @@ namespace sgipc {
 
 template <class T>
 struct MatView {
-    const T* val;      // static block values
-    const T* uc;       // unique contact block values
+    const T* fval;   // full symmetric static blocks
+    const T* uc;     // unique contact blocks (upper)
 };
 
 struct Topo {
     int n;
-    const int* row_ptr;
-    const int* col;
-    const int* slot_row;
-    const int* low_ptr;
-    const int* low_slot;
+    const int* frow_ptr;
+    const int* fcol;
     const int* cu_ptr;
+    const int* uc_col;
     const int* cl_ptr;
     const int* cl_idx;
-    const int* uc_row;
-    const int* uc_col;
+    const int* cl_col;
 };
 
 struct MasView {
@@ -62,16 +62,13 @@ struct MasView {
 inline Topo topo_of(SgipcCtx* c) {
     Topo t;
     t.n = c->n;
-    t.row_ptr = c->row_ptr;
-    t.col = c->col;
-    t.slot_row = c->slot_row;
-    t.low_ptr = c->low_ptr;
-    t.low_slot = c->low_slot;
+    t.frow_ptr = c->frow_ptr;
+    t.fcol = c->fcol;
     t.cu_ptr = c->cu_ptr;
+    t.uc_col = c->uc_col;
     t.cl_ptr = c->cl_ptr;
     t.cl_idx = c->cl_idx;
-    t.uc_row = c->uc_row;
-    t.uc_col = c->uc_col;
+    t.cl_col = c->cl_col;
     return t;
 }
 
@@ -99,7 +96,8 @@ __device__ __forceinline__ void block_sum(double (&v)[NR], double* smem /*[NR*8]
 }
 
 // Publishes this CTA's partial sums; returns true in every thread of the last CTA to
-// arrive, after which out[r] holds the deterministic (CTA-order) total.
+// arrive, after which out[r] holds the deterministic (CTA-order) total.  Every CTA of the
+// grid must call it (the early returns before it are grid-uniform).
 template <int NR>
 __device__ __forceinline__ bool grid_sum(double (&v)[NR], double* partial, unsigned int* ticket, double* out,
                                          double* smem) {
@@ -134,14 +132,14 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NR], double* partial, unsig
 
 // ---- SpMV core ------------------------------------------------------------------------------
 template <class T, int NR>
-__device__ __forceinline__ void block_mv(const T* __restrict__ B, const T* __restrict__ x, int j, bool transpose,
-                                         T (&acc)[NR][3]) {
+__device__ __forceinline__ void block_mv3(const T* __restrict__ B, const T (&xj)[NR][3], bool transpose,
+                                          T (&acc)[NR][3]) {
     T b[9];
 #pragma unroll
     for (int q = 0; q < 9; q++) b[q] = B[q];
 #pragma unroll
     for (int r = 0; r < NR; r++) {
-        T x0 = x[(3 * j) * NR + r], x1 = x[(3 * j + 1) * NR + r], x2 = x[(3 * j + 2) * NR + r];
+        const T x0 = xj[r][0], x1 = xj[r][1], x2 = xj[r][2];
         if (!transpose) {
             acc[r][0] += b[0] * x0 + b[1] * x1 + b[2] * x2;
             acc[r][1] += b[3] * x0 + b[4] * x1 + b[5] * x2;
@@ -154,29 +152,47 @@ __device__ __forceinline__ void block_mv(const T* __restrict__ B, const T* __res
     }
 }
 
+// Operand gather: x_j (plain vector) or p_j = z_j + beta p_old_j (direction formed on the fly)
+template <class T, int NR>
+struct Operand {
+    const T* a;       // x, or z
+    const T* b;       // nullptr, or p_old
+    T beta[NR];
+    __device__ __forceinline__ void load(int j, T (&xj)[NR][3]) const {
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const size_t k = (size_t)(3 * j + q) * NR + r;
+                xj[r][q] = b ? a[k] + beta[r] * b[k] : a[k];
+            }
+    }
+};
+
 // Rows are processed by groups of kSpG lanes: lane g of a group takes every kSpG-th block of
-// the row's four lists (static upper, static transposed, contact upper, contact transposed)
-// and the group adds its partial results with shuffles.
+// the row's lists (full static row, contact upper, contact transposed) and the group adds
+// its partial results with shuffles.
 constexpr int kSpG = 4;
 inline int spmv_grid(int n) { return nblk((long long)n * kSpG, 256); }
 
 template <class T, int NR>
-__device__ __forceinline__ void row_mv(const Topo& tp, const MatView<T>& A, const T* __restrict__ x, int i, int g,
+__device__ __forceinline__ void row_mv(const Topo& tp, const MatView<T>& A, const Operand<T, NR>& x, int i, int g,
                                        T (&acc)[NR][3]) {
 #pragma unroll
     for (int r = 0; r < NR; r++) acc[r][0] = acc[r][1] = acc[r][2] = 0;
     if (i < tp.n) {
-        for (int s = tp.row_ptr[i] + g; s < tp.row_ptr[i + 1]; s += kSpG)
-            block_mv<T, NR>(A.val + 9 * (size_t)s, x, tp.col[s], false, acc);
-        for (int k = tp.low_ptr[i] + g; k < tp.low_ptr[i + 1]; k += kSpG) {
-            int s = tp.low_slot[k];
-            block_mv<T, NR>(A.val + 9 * (size_t)s, x, tp.slot_row[s], true, acc);
+        T xj[NR][3];
+        for (int s = tp.frow_ptr[i] + g; s < tp.frow_ptr[i + 1]; s += kSpG) {
+            x.load(tp.fcol[s], xj);
+            block_mv3<T, NR>(A.fval + 9 * (size_t)s, xj, false, acc);
         }
-        for (int u = tp.cu_ptr[i] + g; u < tp.cu_ptr[i + 1]; u += kSpG)
-            block_mv<T, NR>(A.uc + 9 * (size_t)u, x, tp.uc_col[u], false, acc);
+        for (int u = tp.cu_ptr[i] + g; u < tp.cu_ptr[i + 1]; u += kSpG) {
+            x.load(tp.uc_col[u], xj);
+            block_mv3<T, NR>(A.uc + 9 * (size_t)u, xj, false, acc);
+        }
         for (int k = tp.cl_ptr[i] + g; k < tp.cl_ptr[i + 1]; k += kSpG) {
-            int u = tp.cl_idx[k];
-            block_mv<T, NR>(A.uc + 9 * (size_t)u, x, tp.uc_row[u], true, acc);
+            x.load(tp.cl_col[k], xj);
+            block_mv3<T, NR>(A.uc + 9 * (size_t)tp.cl_idx[k], xj, true, acc);
         }
     }
 #pragma unroll
@@ -191,8 +207,12 @@ template <class T>
 __global__ void k_spmv(Topo tp, MatView<T> A, const T* __restrict__ x, T* __restrict__ y) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = t / kSpG, g = t % kSpG;
+    Operand<T, 1> op;
+    op.a = x;
+    op.b = nullptr;
+    op.beta[0] = 0;
     T acc[1][3];
-    row_mv<T, 1>(tp, A, x, i, g, acc);
+    row_mv<T, 1>(tp, A, op, i, g, acc);
     if (i < tp.n && g == 0) {
         y[3 * i] = acc[0][0];
         y[3 * i + 1] = acc[0][1];
@@ -206,37 +226,67 @@ struct PcgPtrs {
     T* x;
     T* r;
     T* z;
-    T* p;
+    T* p[2];
     T* Ap;
     PcgScalars* sc;
     double* partial;
     unsigned int* ticket;
 };
 
+// K1
 template <class T, int NR>
 __global__ void __launch_bounds__(256) k_pcg_spmv_dot(Topo tp, MatView<T> A, PcgPtrs<T, NR> P) {
     __shared__ double smem[NR * 8];
-    __shared__ int st_run[NR];
-    if (threadIdx.x < NR) st_run[threadIdx.x] = P.sc[threadIdx.x].state == 0;
+    __shared__ int run[NR];
+    __shared__ double beta[NR];
+    __shared__ int halt, nb;
+    if (threadIdx.x < NR) {
+        const PcgScalars& s = P.sc[threadIdx.x];
+        run[threadIdx.x] = s.state == 0;
+        beta[threadIdx.x] = s.first ? 0.0 : s.rz_next / s.rz;
+    }
+    if (threadIdx.x == 0) {
+        halt = P.sc[0].halt;
+        // this iteration's direction buffer: the running right-hand sides have all done the
+        // same number of iterations
+        nb = 0;
+        for (int r = NR - 1; r >= 0; r--)
+            if (P.sc[r].state == 0) nb = P.sc[r].iter & 1;
+    }
     __syncthreads();
     bool any = false;
 #pragma unroll
-    for (int r = 0; r < NR; r++) any |= st_run[r] != 0;
-    if (!any) return;  // uniform across the grid: state only changes in the last CTA below
+    for (int r = 0; r < NR; r++) any |= run[r] != 0;
+    // grid-uniform: these words change only in this kernel's last CTA, after every CTA has
+    // read them, or in later kernels
+    if (!any || halt) return;
+    // rows of finished right-hand sides are computed too (cheaper than masking) and ignored
+    Operand<T, NR> op;
+    op.a = P.z;
+    op.b = nb ? P.p[0] : P.p[1];
+#pragma unroll
+    for (int r = 0; r < NR; r++) op.beta[r] = (T)beta[r];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = t / kSpG, g = t % kSpG;
     double part[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) part[r] = 0.0;
     T acc[NR][3];
-    row_mv<T, NR>(tp, A, P.p, i, g, acc);
+    row_mv<T, NR>(tp, A, op, i, g, acc);
     if (i < tp.n && g == 0) {
+        T* pw = nb ? P.p[1] : P.p[0];
+        T pi[NR][3];
+        op.load(i, pi);
 #pragma unroll
         for (int r = 0; r < NR; r++)
 #pragma unroll
             for (int q = 0; q < 3; q++) {
-                P.Ap[(3 * i + q) * NR + r] = acc[r][q];
-                part[r] += (double)P.p[(3 * i + q) * NR + r] * (double)acc[r][q];
+                const size_t k = (size_t)(3 * i + q) * NR + r;
+                if (run[r]) {
+                    pw[k] = pi[r][q];
+                    P.Ap[k] = acc[r][q];
+                }
+                part[r] += (double)pi[r][q] * (double)acc[r][q];
             }
     }
     double tot[NR];
@@ -244,9 +294,11 @@ __global__ void __launch_bounds__(256) k_pcg_spmv_dot(Topo tp, MatView<T> A, Pcg
 #pragma unroll
         for (int r = 0; r < NR; r++) {
             PcgScalars& s = P.sc[r];
-            if (!st_run[r]) continue;
+            if (!run[r]) continue;
             s.rz = s.rz_next;
             s.pAp = tot[r];
+            s.pcur = nb;
+            s.first = 0;
             s.iter += 1;
             if (!(tot[r] > 0.0) || !isfinite(tot[r]) || !isfinite(s.rz)) {
                 s.state = 2;
@@ -265,16 +317,20 @@ template <class T, class M, int NR>
 __global__ void __launch_bounds__(256) k_pcg_update(PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R) {
     __shared__ double smem[NR * 8];
     __shared__ int st[NR];
+    __shared__ int pc[NR];
     __shared__ double alpha[NR];
+    __shared__ int halt;
     if (threadIdx.x < NR) {
         st[threadIdx.x] = P.sc[threadIdx.x].state;
         alpha[threadIdx.x] = P.sc[threadIdx.x].alpha;
+        pc[threadIdx.x] = P.sc[threadIdx.x].pcur;
     }
+    if (threadIdx.x == 0) halt = P.sc[0].halt;
     __syncthreads();
     bool any = false;
 #pragma unroll
     for (int r = 0; r < NR; r++) any |= st[r] < 2;
-    if (!any) return;
+    if (!any || halt) return;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int v = p < mv.npos ? mv.part_map[p] : -1;
     double part[NR];
@@ -287,11 +343,12 @@ __global__ void __launch_bounds__(256) k_pcg_update(PcgPtrs<T, NR> P, MasView mv
 #pragma unroll
         for (int r = 0; r < NR; r++) {
             if (st[r] == 2) continue;
-            T a = (T)alpha[r];
+            const T a = (T)alpha[r];
+            const T* pr = pc[r] ? P.p[1] : P.p[0];
 #pragma unroll
             for (int q = 0; q < 3; q++) {
                 const size_t k = (size_t)(3 * v + q) * NR + r;
-                P.x[k] += a * P.p[k];
+                P.x[k] += a * pr[k];
                 T rv = P.r[k] - a * P.Ap[k];
                 P.r[k] = rv;
                 part[r] += (double)rv * (double)rv;
@@ -312,44 +369,17 @@ __global__ void __launch_bounds__(256) k_pcg_update(PcgPtrs<T, NR> P, MasView mv
             PcgScalars& s = P.sc[r];
             if (st[r] == 2) continue;
             s.rr = tot[r];
-            if (s.crit == SGIPC_CRIT_TRUE && s.state == 0 && tot[r] <= s.tol * s.tol * s.bnorm2) s.state = 1;
+            if (st[r] == 1) s.state = 2;  // the final update of an r.z-converged solve is applied
+            else if (s.crit == SGIPC_CRIT_TRUE && tot[r] <= s.tol * s.tol * s.bnorm2) s.state = 2;
         }
     }
 }
 
-// K3a: restriction to levels 2 .. L-1 in one CTA
+// K3: CTA 0 restricts to levels 2.. and solves the coarse domains; CTAs >= 1 take four
+// level-0/1 domains each (48 threads per domain, Z_d = A_d^-1 R_d read once for NR columns)
 template <class M, int NR>
-__global__ void __launch_bounds__(1024) k_pcg_restrict_coarse(MasView mv, const PcgScalars* __restrict__ sc,
-                                                               M* __restrict__ R) {
-    __shared__ int any;
-    if (threadIdx.x == 0) {
-        int a = 0;
-        for (int r = 0; r < NR; r++) a |= sc[r].state == 0;
-        any = a;
-    }
-    __syncthreads();
-    if (!any) return;
-    restrict_coarse_cta<M, NR>(mv.info, mv.up, mv.L, R);
-}
-
-template <class M, int NR>
-__global__ void __launch_bounds__(192) k_pcg_domain(const int* __restrict__ info, const PcgScalars* __restrict__ sc,
-                                                    const M* __restrict__ inv, const M* __restrict__ R,
-                                                    M* __restrict__ Z) {
-    __shared__ M sR[4][48 * NR];
-    __shared__ int run[NR];
-    if (threadIdx.x < NR) run[threadIdx.x] = sc[threadIdx.x].state == 0;
-    const int ndom = info[16] >> 4;
-    const int ld = threadIdx.x / 48, i = threadIdx.x % 48;
-    const int d = blockIdx.x * 4 + ld;
-    if (d < ndom)
-#pragma unroll
-        for (int r = 0; r < NR; r++) sR[ld][i * NR + r] = R[(48 * (size_t)d + i) * NR + r];
-    __syncthreads();
-    bool any = false;
-#pragma unroll
-    for (int r = 0; r < NR; r++) any |= run[r] != 0;
-    if (!any || d >= ndom) return;
+__device__ __forceinline__ void domain_solve(const M* __restrict__ inv, const M* __restrict__ R, M* __restrict__ Z,
+                                             int d, int i, M (*sR)[48 * NR]) {
     const M* Ad = inv + (size_t)d * 2304;
     M acc[NR];
 #pragma unroll
@@ -358,18 +388,69 @@ __global__ void __launch_bounds__(192) k_pcg_domain(const int* __restrict__ info
     for (int j = 0; j < 48; j++) {
         M a = Ad[j * 48 + i];
 #pragma unroll
-        for (int r = 0; r < NR; r++) acc[r] += a * sR[ld][j * NR + r];
+        for (int r = 0; r < NR; r++) acc[r] += a * (*sR)[j * NR + r];
     }
 #pragma unroll
     for (int r = 0; r < NR; r++) Z[(48 * (size_t)d + i) * NR + r] = acc[r];
 }
 
+template <class M, int NR>
+__global__ void __launch_bounds__(192) k_pcg_domains(MasView mv, const PcgScalars* __restrict__ sc,
+                                                     const M* __restrict__ inv, M* __restrict__ R, M* __restrict__ Z) {
+    __shared__ M sR[4][48 * NR];
+    __shared__ int go;
+    if (threadIdx.x == 0) {
+        int a = 0;
+        for (int r = 0; r < NR; r++) a |= sc[r].state == 0;
+        go = a && !sc[0].halt;
+    }
+    __syncthreads();
+    if (!go) return;
+    const int ld = threadIdx.x / 48, i = threadIdx.x % 48;
+    const int ndom = mv.info[16] >> 4;
+    const int nd01 = mv.L > 2 ? (mv.info[2] >> 4) : ndom;  // domains of levels 0 and 1
+    if (blockIdx.x == 0) {
+        restrict_coarse_cta<M, NR>(mv.info, mv.up, mv.L, R);
+        for (int d0 = nd01; d0 < ndom; d0 += 4) {
+            const int d = d0 + ld;
+            if (d < ndom)
+#pragma unroll
+                for (int r = 0; r < NR; r++) sR[ld][i * NR + r] = R[(48 * (size_t)d + i) * NR + r];
+            __syncthreads();
+            if (d < ndom) domain_solve<M, NR>(inv, R, Z, d, i, &sR[ld]);
+            __syncthreads();
+        }
+        return;
+    }
+    const int d = (blockIdx.x - 1) * 4 + ld;
+    if (d < nd01)
+#pragma unroll
+        for (int r = 0; r < NR; r++) sR[ld][i * NR + r] = R[(48 * (size_t)d + i) * NR + r];
+    __syncthreads();
+    if (d < nd01) domain_solve<M, NR>(inv, R, Z, d, i, &sR[ld]);
+}
+
+// K4
 template <class T, class M, int NR>
 __global__ void __launch_bounds__(256) k_pcg_prolong_dot(int nv, PcgPtrs<T, NR> P, MasView mv,
-                                                         const M* __restrict__ Z) {
+                                                         const M* __restrict__ Z, cudaGraphConditionalHandle h,
+                                                         int decide, int use_cond) {
     __shared__ double smem[NR * 8];
     __shared__ int run[NR];
     if (threadIdx.x < NR) run[threadIdx.x] = P.sc[threadIdx.x].state == 0;
+    if (decide && blockIdx.x == 0 && threadIdx.x == 0) {
+        // continuation of the iteration loop; reads only words final for this body
+        PcgScalars& s0 = P.sc[0];
+        int cont = 0;
+        for (int r = 0; r < NR; r++) {
+            const PcgScalars& s = P.sc[r];
+            if (s.state == 0 && s.iter + 1 < s.max_iter) cont = 1;
+        }
+        s0.bodies += 1;
+        if (s0.bodies >= s0.max_iter + 2) cont = 0;
+        if (!cont) s0.halt = 1;
+        if (use_cond) cudaGraphSetConditional(h, cont);
+    }
     __syncthreads();
     bool any = false;
 #pragma unroll
@@ -408,43 +489,6 @@ __global__ void __launch_bounds__(256) k_pcg_prolong_dot(int nv, PcgPtrs<T, NR> 
     }
 }
 
-template <class T, int NR>
-__global__ void __launch_bounds__(256) k_pcg_p_update(int n3, PcgPtrs<T, NR> P, cudaGraphConditionalHandle h,
-                                                      int use_cond) {
-    __shared__ int st[NR];
-    __shared__ double beta[NR];
-    if (threadIdx.x < NR) {
-        const PcgScalars& s = P.sc[threadIdx.x];
-        st[threadIdx.x] = s.state;
-        beta[threadIdx.x] = s.rz_next / s.rz;
-    }
-    __syncthreads();
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n3) {
-#pragma unroll
-        for (int r = 0; r < NR; r++) {
-            if (st[r] != 0) continue;
-            const size_t e = (size_t)k * NR + r;
-            P.p[e] = P.z[e] + (T)beta[r] * P.p[e];
-        }
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int cont = 0;
-#pragma unroll
-        for (int r = 0; r < NR; r++) {
-            PcgScalars& s = P.sc[r];
-            if (s.state == 1) s.state = 2;
-            s.bodies += 1;
-            if (s.state == 0 && (s.iter + 1 >= s.max_iter || s.bodies >= s.max_iter + 2)) {
-                s.state = 2;
-                s.status = SGIPC_NOT_CONVERGED;
-            }
-            if (s.state == 0) cont = 1;
-        }
-        if (use_cond) cudaGraphSetConditional(h, cont);
-    }
-}
-
 // ---- solve set-up kernels -------------------------------------------------------------------
 template <class T, class M, int NR>
 __global__ void k_pcg_init(const double* __restrict__ b, PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R, double tol,
@@ -456,6 +500,9 @@ __global__ void k_pcg_init(const double* __restrict__ b, PcgPtrs<T, NR> P, MasVi
         s.status = SGIPC_OK;
         s.iter = 0;
         s.bodies = 0;
+        s.first = 1;
+        s.pcur = 0;
+        s.halt = 0;
         s.tol = tol;
         s.max_iter = max_iter;
         s.crit = crit;
@@ -473,6 +520,8 @@ __global__ void k_pcg_init(const double* __restrict__ b, PcgPtrs<T, NR> P, MasVi
                 T rv = (T)b[k];
                 P.r[k] = rv;
                 P.x[k] = 0;
+                P.p[0][k] = 0;
+                P.p[1][k] = 0;
                 val[r * 3 + q] = (M)rv;
             }
     }
@@ -494,7 +543,6 @@ __global__ void k_pcg_init_finish(int n3, const double* __restrict__ b, PcgPtrs<
         part[r] = 0.0;
         if (k < n3) {
             const size_t e = (size_t)k * NR + r;
-            P.p[e] = P.z[e];
             part[r] = b[e] * b[e];
         }
     }
@@ -530,12 +578,6 @@ __global__ void k_axpby_res(int n, const double* __restrict__ b, const double* _
     if (k < n) r[k] = b[k] - Ax[k];
 }
 
-template <class A, class B>
-__global__ void k_convert(int n, const A* __restrict__ a, B* __restrict__ b) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) b[k] = (B)a[k];
-}
-
 __global__ void k_add_f32(int n, const float* __restrict__ d, double* __restrict__ x) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) x[k] += (double)d[k];
@@ -566,7 +608,8 @@ PcgPtrs<T, NR> ptrs_of(PcgWork& w) {
     P.x = (T*)w.x;
     P.r = (T*)w.r;
     P.z = (T*)w.z;
-    P.p = (T*)w.p;
+    P.p[0] = (T*)w.p;
+    P.p[1] = (T*)w.p2;
     P.Ap = (T*)w.Ap;
     P.sc = w.sc;
     P.partial = w.partial;
@@ -589,32 +632,37 @@ template <class T>
 MatView<T> mat_view(SgipcCtx* c);
 template <>
 MatView<double> mat_view<double>(SgipcCtx* c) {
-    return {c->val64, c->uc64};
+    return {c->fval64, c->uc64};
 }
 template <>
 MatView<float> mat_view<float>(SgipcCtx* c) {
-    return {c->val32, c->uc32};
+    return {c->fval32, c->uc32};
 }
 
-// Enqueue one PCG iteration body (K1..K5) on stream s.
+// grid of K3: one coarse CTA + the level-0/1 domains, four per CTA
+int domain_grid(SgipcCtx* c) {
+    const int* h = c->mas.h_info;
+    const int ndom = h[16] / 16;
+    const int nd01 = c->mas.levelnum > 2 ? h[2] / 16 : ndom;
+    return 1 + (nd01 + 3) / 4;
+}
+
 template <class T, class M, int NR>
 void enqueue_body(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, cudaGraphConditionalHandle h, int use_cond,
-                  int ndom, cudaStream_t s) {
+                  int k3grid, cudaStream_t s) {
     const int n = c->n, nv = c->nv;
     PcgPtrs<T, NR> P = ptrs_of<T, NR>(w);
     MasView mv = mas_view(c);
     k_pcg_spmv_dot<T, NR><<<spmv_grid(n), 256, 0, s>>>(topo_of(c), mat_view<T>(c), P);
     k_pcg_update<T, M, NR><<<nblk(mv.npos), 256, 0, s>>>(P, mv, R);
-    k_pcg_restrict_coarse<M, NR><<<1, 1024, 0, s>>>(mv, w.sc, R);
-    k_pcg_domain<M, NR><<<(ndom + 3) / 4, 192, 0, s>>>(c->mas.info, w.sc, inv, R, Z);
-    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z);
-    k_pcg_p_update<T, NR><<<nblk(3LL * n), 256, 0, s>>>(3 * n, P, h, use_cond);
+    k_pcg_domains<M, NR><<<k3grid, 192, 0, s>>>(mv, w.sc, inv, R, Z);
+    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z, h, 1, use_cond);
 }
 
 // Build (or reuse) the executable graph of the iteration loop for this workspace.
 template <class T, class M, int NR>
-SgipcStatus get_loop_graph(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, int ndom, int tag) {
-    const long long key = (long long)tag * 100000000LL + ndom;
+SgipcStatus get_loop_graph(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, int k3grid, int tag) {
+    const long long key = (long long)tag * 100000000LL + k3grid;
     if (w.exec && w.captured_key == key) return SGIPC_OK;
     if (w.exec) {
         cudaGraphExecDestroy(w.exec);
@@ -645,7 +693,7 @@ SgipcStatus get_loop_graph(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, in
         e = cudaStreamBeginCaptureToGraph(c->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
         ok = e == cudaSuccess;
         if (ok) {
-            enqueue_body<T, M, NR>(c, w, inv, R, Z, h, 1, ndom, c->cap_stream);
+            enqueue_body<T, M, NR>(c, w, inv, R, Z, h, 1, k3grid, c->cap_stream);
             cudaGraph_t out = nullptr;
             e = cudaStreamEndCapture(c->cap_stream, &out);
             ok = e == cudaSuccess;
@@ -662,11 +710,11 @@ SgipcStatus get_loop_graph(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, in
         w.captured_key = key;
         return SGIPC_OK;
     }
-    // fallback: a graph of 8 iterations, relaunched until the state word says done
+    // fallback: a graph of 8 iteration bodies, relaunched until the halt word is set
     w.cond_graph = false;
     w.exec = nullptr;
     SG_CHECK(c, cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < 8; k++) enqueue_body<T, M, NR>(c, w, inv, R, Z, h, 0, ndom, c->cap_stream);
+    for (int k = 0; k < 8; k++) enqueue_body<T, M, NR>(c, w, inv, R, Z, h, 0, k3grid, c->cap_stream);
     cudaGraph_t cg = nullptr;
     SG_CHECK(c, cudaStreamEndCapture(c->cap_stream, &cg));
     e = cudaGraphInstantiate(&w.exec, cg, 0);
@@ -681,41 +729,44 @@ template <class T, class M, int NR>
 SgipcStatus run_pcg(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
                     cudaStream_t s, int tag) {
     MasWork& m = c->mas;
-    const int ndom = m.h_info[16] / 16;
     const M* inv = fp32_mas ? (const M*)m.dom32 : (const M*)m.dom64;
     M* R = fp32_mas ? (M*)m.R32 : (M*)m.R64;
     M* Z = fp32_mas ? (M*)m.Z32 : (M*)m.Z64;
-    SgipcStatus st = get_loop_graph<T, M, NR>(c, w, inv, R, Z, ndom, tag);
+    const int k3grid = domain_grid(c);
+    SgipcStatus st = get_loop_graph<T, M, NR>(c, w, inv, R, Z, k3grid, tag);
     if (st != SGIPC_OK) return st;
     const int nv = c->nv, n = c->n;
     PcgPtrs<T, NR> P = ptrs_of<T, NR>(w);
     MasView mv = mas_view(c);
-    SG_COUNT(c, 5);
+    SG_COUNT(c, 4);
     k_pcg_init<T, M, NR><<<nblk(mv.npos), 256, 0, s>>>(b, P, mv, R, tol, max_iter, crit);
-    k_pcg_restrict_coarse<M, NR><<<1, 1024, 0, s>>>(mv, w.sc, R);
-    k_pcg_domain<M, NR><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, w.sc, inv, R, Z);
-    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z);
+    k_pcg_domains<M, NR><<<k3grid, 192, 0, s>>>(mv, w.sc, inv, R, Z);
+    k_pcg_prolong_dot<T, M, NR><<<nblk(nv), 256, 0, s>>>(nv, P, mv, Z, 0, 0, 0);
     k_pcg_init_finish<T, NR><<<nblk(3LL * n), 256, 0, s>>>(3 * n, b, P);
     SG_LAUNCH_CHECK(c, "pcg init");
     if (w.cond_graph) {
         SG_CHECK(c, cudaGraphLaunch(w.exec, s));
     } else {
-        for (int guard = 0; guard < 1 + max_iter / 8; guard++) {
+        for (int guard = 0; guard < 2 + max_iter / 8; guard++) {
             SG_CHECK(c, cudaGraphLaunch(w.exec, s));
             PcgScalars hs[NR];
             SG_CHECK(c, cudaMemcpyAsync(hs, w.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
             SG_CHECK(c, cudaStreamSynchronize(s));
-            bool run = false;
-            for (int r = 0; r < NR; r++) run |= hs[r].state == 0;
-            if (!run) break;
+            if (hs[0].halt) break;
         }
     }
     return SGIPC_OK;
 }
 
+// status of a finished solve: still running (state 0) means the iteration cap was hit
+int final_status(const PcgScalars& s) {
+    if (s.state == 0) return SGIPC_NOT_CONVERGED;
+    return s.status;
+}
+
 SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
     const size_t n3 = 3 * (size_t)c->n * nrhs;
-    void** vs[] = {&w.x, &w.r, &w.z, &w.p, &w.Ap};
+    void** vs[] = {&w.x, &w.r, &w.z, &w.p, &w.p2, &w.Ap};
     for (void** v : vs) SG_CHECK(c, cudaMalloc(v, elem * n3));
     SG_CHECK(c, cudaMalloc((void**)&w.sc, sizeof(PcgScalars) * nrhs));
     SG_CHECK(c, cudaMalloc((void**)&w.partial, sizeof(double) * 4 * nrhs * c->max_blocks));
@@ -726,7 +777,7 @@ SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
 }
 
 void free_work(PcgWork& w) {
-    void* ps[] = {w.x, w.r, w.z, w.p, w.Ap, w.sc, w.partial, w.ticket};
+    void* ps[] = {w.x, w.r, w.z, w.p, w.p2, w.Ap, w.sc, w.partial, w.ticket};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (w.exec) cudaGraphExecDestroy(w.exec);
@@ -793,7 +844,7 @@ extern "C" SgipcStatus sgipc_spmv(SgipcCtx* c, const double* x, double* y, void*
     return spmv_t<double>(c, x, y, (cudaStream_t)stream);
 }
 
-// true relative residual ||b - A x|| / ||b|| (FP64), nrhs interleaved vectors
+// true relative residual ||b - A x|| / ||b|| (FP64)
 static SgipcStatus true_residual(SgipcCtx* c, const double* b, const double* x, double* out, cudaStream_t s) {
     const int n3 = 3 * c->n;
     SgipcStatus st = spmv_t<double>(c, x, c->tmp64b, s);
@@ -826,12 +877,12 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         PcgScalars hs;
         SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg64.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
         SG_CHECK(c, cudaStreamSynchronize(s));
-        SG_COUNT(c, 6LL * hs.bodies);
+        SG_COUNT(c, 4LL * hs.bodies);
         out.iterations = hs.iter;
         out.refinements = 0;
         out.rz0 = hs.rz0;
         out.rz = hs.rz_next;
-        out.status = hs.status;
+        out.status = final_status(hs);
     } else {
         // mixed: FP32 MAS-PCG inner solves on the FP32 matrix copy, FP64 residual refinement
         double* r64 = c->tmp64;
@@ -859,7 +910,7 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
             SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
             SG_CHECK(c, cudaStreamSynchronize(s));
             total_it += hs.iter;
-            SG_COUNT(c, 6LL * hs.bodies);
+            SG_COUNT(c, 4LL * hs.bodies);
             if (ref == 0) {
                 rz0 = hs.rz0;
                 bn2 = hs.bnorm2;
@@ -919,6 +970,7 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
     cudaStream_t s = (cudaStream_t)stream;
     const int n3 = 3 * c->n;
     if (max_iter <= 0) max_iter = (int)(0.3 * n3);
+    if (max_iter < 2) max_iter = 2;
     if (nrhs != 4) {
         // one right-hand side at a time
         SgipcStatus worst = SGIPC_OK;
@@ -951,19 +1003,20 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
     SG_CHECK(c, cudaMemcpyAsync(hs, w.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
     SG_CHECK(c, cudaStreamSynchronize(s));
     SgipcStatus worst = SGIPC_OK;
-    SG_COUNT(c, 6LL * hs[0].bodies);
+    SG_COUNT(c, 4LL * hs[0].bodies);
     for (int r = 0; r < 4; r++) {
+        const int fs = final_status(hs[r]);
         if (stats) {
             stats[r] = SgipcSolveStats{};
             stats[r].iterations = hs[r].iter;
             stats[r].rz0 = hs[r].rz0;
             stats[r].rz = hs[r].rz_next;
-            stats[r].status = hs[r].status;
+            stats[r].status = fs;
             double rel = 0;
             if ((st = true_residual(c, b + (size_t)r * n3, x + (size_t)r * n3, &rel, s)) != SGIPC_OK) return st;
             stats[r].rel_residual = rel;
         }
-        if (hs[r].status != SGIPC_OK) worst = (SgipcStatus)hs[r].status;
+        if (fs != SGIPC_OK) worst = (SgipcStatus)fs;
     }
     return worst;
 }
@@ -980,8 +1033,8 @@ SgipcStatus pcg_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
         k_spmv<double><<<spmv_grid(c->n), 256, 0, s>>>(topo_of(c), mat_view<double>(c), c->tmp64, c->tmp64b);
     else
         k_spmv<float><<<spmv_grid(c->n), 256, 0, s>>>(topo_of(c), mat_view<float>(c), (const float*)c->tmp64,
-                                                  (float*)c->tmp64b);
-    // nb (sb + 4) + (n + 1) 4 + 2 * 3n * sv with nb = static + unique contact blocks
+                                                      (float*)c->tmp64b);
+    // algorithmic: nb (sb + 4) + (n + 1) 4 + 2 * 3n * sv, nb = upper static + unique contact blocks
     const double sb = f64 ? 72 : 36, sv = f64 ? 8 : 4;
     *bytes = ((double)c->nnz + nuc) * (sb + 4) + (c->n + 1.0) * 4 + 2.0 * 3 * c->n * sv;
     SG_LAUNCH_CHECK(c, name);
