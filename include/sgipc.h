@@ -193,6 +193,17 @@ SgipcStatus sgipc_mas_build(SgipcCtx* ctx, const SgipcContacts* con, SgipcPrecis
                             void* stream);
 /* MASPreconditioner::preconditioning (MASPreconditioner.cu:2221): z = M^-1 r. */
 SgipcStatus sgipc_mas_apply(SgipcCtx* ctx, const double* r, double* z, void* stream);
+/* The same z = M^-1 r, for callers that may not allocate device memory during a call (a
+ * host whose pool owns every device allocation, or a loop where an allocation's implicit
+ * synchronisation is not allowed).  No counterpart in the reference.  It allocates nothing:
+ * its two work vectors live in one fixed array compiled into the library, 3 MiB on every
+ * device that loads it, kept until the process exits, serving hierarchies of at most 65536
+ * clusters (sgipc_mas_info's total); larger ones return SGIPC_CAPACITY with a message.  The
+ * first call on a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  All calls on a device share the array:
+ * calls whose work overlaps on the GPU (other streams, other contexts) race and must be
+ * ordered by the caller. */
+SgipcStatus sgipc_mas_apply_noalloc(SgipcCtx* ctx, const double* r, double* z, void* stream);
 /* Host copy of the level structure: levels, per-level node counts, total clusters. */
 SgipcStatus sgipc_mas_info(SgipcCtx* ctx, int32_t* levelnum, int32_t* level_counts /*[8]*/,
                            int32_t* total_clusters);

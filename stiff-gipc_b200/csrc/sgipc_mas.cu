@@ -16,6 +16,7 @@
 // copy), builds the per-level masks with one thread per vertex / per contact pair and
 // resolves a bank's components with one thread per bank.
 #include <cub/cub.cuh>
+#include <mutex>
 #include <vector>
 
 #include "sgipc_internal.cuh"
@@ -570,5 +571,90 @@ extern "C" SgipcStatus sgipc_mas_restrict(SgipcCtx* c, const double* r, double* 
     SG_LAUNCH_CHECK(c, "mas restrict");
     SG_CHECK(c, cudaDeviceSynchronize());
     SG_CHECK(c, cudaMemcpy(out, m.R64, sizeof(double) * 3 * (size_t)m.h_info[16], cudaMemcpyDeviceToHost));
+    return SGIPC_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// MAS apply without any allocation
+// ------------------------------------------------------------------------------------------
+// Some hosts cannot let a call allocate device memory: a solver step running inside a
+// plugin whose host owns every device allocation through its own pool (a cudaMalloc there
+// would bypass the pool's accounting or fail under its memory cap), or a real-time loop in
+// which an allocation's implicit device synchronisation would stall other streams.  For
+// them sgipc_mas_apply_noalloc keeps the restricted residual R and the domain solutions Z
+// of the apply in a fixed array compiled into this library instead of the context's own
+// buffers.  The array exists once per device that loads the library and stays there until
+// the process exits; every call on that device shares it.
+
+// Largest hierarchy it serves, in clusters summed over all levels (padding included):
+// R and Z, 3 values each per cluster, FP64 = 2 * 3 * 65536 * 8 B = 3 MiB per device.
+#define SGIPC_NOALLOC_MAX_CLUSTERS 65536
+static __device__ __align__(256) double g_mas_noalloc_scratch[2 * 3 * SGIPC_NOALLOC_MAX_CLUSTERS];
+
+namespace {
+// Device address of the array, looked up once per device.  In host code the array's name
+// only stands for it and must never be handed to a kernel.
+constexpr int kNoAllocMaxDevices = 64;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_mu;
+}  // namespace
+
+extern "C" SgipcStatus sgipc_mas_apply_noalloc(SgipcCtx* c, const double* r, double* z, void* stream) {
+    if (!c || !r || !z) return SGIPC_BAD_INPUT;
+    MasWork& m = c->mas;
+    if (!m.built) return SGIPC_NOT_READY;
+    const int total = m.h_info[16];
+    if (total > SGIPC_NOALLOC_MAX_CLUSTERS) {
+        snprintf(c->err, sizeof(c->err),
+                 "mas_apply_noalloc: the hierarchy has %d clusters, the static scratch holds at most %d", total,
+                 SGIPC_NOALLOC_MAX_CLUSTERS);
+        return SGIPC_CAPACITY;
+    }
+    SG_CHECK(c, cudaSetDevice(c->device));
+    if (c->device < 0 || c->device >= kNoAllocMaxDevices) {
+        snprintf(c->err, sizeof(c->err), "mas_apply_noalloc: device %d beyond the %d supported", c->device,
+                 kNoAllocMaxDevices);
+        return SGIPC_BAD_INPUT;
+    }
+    // set-up on the first call on this device (with the device current): resolve the
+    // array's device address
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[c->device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_mas_noalloc_scratch);
+            if (e != cudaSuccess) return cuda_fail(c, e, "cudaGetSymbolAddress(g_mas_noalloc_scratch)");
+            g_noalloc_addr[c->device] = p;
+        }
+        base = g_noalloc_addr[c->device];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int L = m.levelnum;
+    const int ndom = total / 16;
+    const size_t n3 = 3 * (size_t)total;
+    // the restriction never writes the padding slots of levels >= 1, and the domain solve
+    // reads them: R must start at zero (the last call left its own values there).  Z is
+    // written in full by the domain solve.
+    if (m.built == SGIPC_FP64 + 1) {
+        double* R = (double*)base;
+        double* Z = R + n3;
+        SG_CHECK(c, cudaMemsetAsync(R, 0, n3 * sizeof(double), s));
+        SG_COUNT(c, 4);
+        k_restrict01<double, double><<<nblk(m.npos), SGIPC_BLOCK, 0, s>>>(m.npos, r, m.part_map, m.up, R);
+        k_restrict_coarse<double><<<1, 1024, 0, s>>>(m.info, m.up, L, R);
+        k_domain_mv<double><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom64, R, Z);
+        k_prolong<double, double><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, m.table, L, Z, z);
+    } else {
+        float* R = (float*)base;
+        float* Z = R + n3;
+        SG_CHECK(c, cudaMemsetAsync(R, 0, n3 * sizeof(float), s));
+        SG_COUNT(c, 4);
+        k_restrict01<double, float><<<nblk(m.npos), SGIPC_BLOCK, 0, s>>>(m.npos, r, m.part_map, m.up, R);
+        k_restrict_coarse<float><<<1, 1024, 0, s>>>(m.info, m.up, L, R);
+        k_domain_mv<float><<<(ndom + 3) / 4, 192, 0, s>>>(m.info, m.dom32, R, Z);
+        k_prolong<double, float><<<nblk(c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, m.table, L, Z, z);
+    }
+    SG_LAUNCH_CHECK(c, "mas apply noalloc");
     return SGIPC_OK;
 }

@@ -68,6 +68,7 @@ SIGNATURES = {
     "sgipc_spmv": ([_vp, _vp, _vp, _vp], _i32),
     "sgipc_mas_build": ([_vp, C.POINTER(SgipcContacts), _i32, _vp], _i32),
     "sgipc_mas_apply": ([_vp, _vp, _vp, _vp], _i32),
+    "sgipc_mas_apply_noalloc": ([_vp, _vp, _vp, _vp], _i32),
     "sgipc_mas_info": ([_vp, C.POINTER(_i32), _vp, C.POINTER(_i32)], _i32),
     "sgipc_mas_export_tables": ([_vp, _vp], _i32),
     "sgipc_pcg_solve": ([_vp, _i32, _i32, C.c_double, _i32, _vp, _vp, C.POINTER(SgipcSolveStats), _vp], _i32),
