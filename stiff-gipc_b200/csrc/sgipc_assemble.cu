@@ -647,11 +647,22 @@ __global__ void k_row_ptr_rows(int n, const int* __restrict__ nuc, const int* __
     ptr[i] = lo;
 }
 
-// column of each transposed contact entry: the row field of its (col << bits | row) key
-__global__ void k_lower_cols(int m, const unsigned long long* __restrict__ ks, int bits, int* __restrict__ cl_col) {
+// each transposed contact entry: its column (the row field of its (col << bits | row) key)
+// and the transpose of its block, so that the SpMV reads both lists the same way
+__global__ void k_lower_cols(int m, const unsigned long long* __restrict__ ks, int bits, const int* __restrict__ cl_idx,
+                             const double* __restrict__ u64, int* __restrict__ cl_col, double* __restrict__ l64,
+                             float* __restrict__ l32) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= m) return;
     cl_col[k] = (int)(ks[k] & ((1ull << bits) - 1ull));
+    if (ks[k] == kBadKey) return;
+    const double* src = u64 + 9 * (size_t)cl_idx[k];
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        const double v = src[3 * (q % 3) + q / 3];
+        l64[9 * (size_t)k + q] = v;
+        l32[9 * (size_t)k + q] = (float)v;
+    }
 }
 
 __global__ void k_row_ptr_keys(int n, int m, const unsigned long long* __restrict__ ks, int bits, int* __restrict__ ptr) {
@@ -758,7 +769,8 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
     tb = c->cub_tmp_bytes;
     SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->lkey, c->lkey_s, c->lidx, c->cl_idx, m, 0, endbit, s));
     k_row_ptr_keys<<<nblk(c->n + 1), SGIPC_BLOCK, 0, s>>>(c->n, m, c->lkey_s, c->key_bits, c->cl_ptr);
-    k_lower_cols<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->lkey_s, c->key_bits, c->cl_col);
+    k_lower_cols<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->lkey_s, c->key_bits, c->cl_idx, c->uc64, c->cl_col, c->cl64,
+                                                 c->cl32);
     SG_LAUNCH_CHECK(c, "contact merge");
     return SGIPC_OK;
 }

@@ -243,7 +243,7 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
         (st = dalloc(c, &c->uc_col, cap)) || (st = dalloc(c, &c->uc64, cap * 9)) ||
         (st = dalloc(c, &c->uc32, cap * 9)) || (st = dalloc(c, &c->cu_ptr, n + 1)) ||
         (st = dalloc(c, &c->cl_ptr, n + 1)) || (st = dalloc(c, &c->cl_idx, cap)) || (st = dalloc(c, &c->lkey, cap)) ||
-        (st = dalloc(c, &c->cl_col, cap)) ||
+        (st = dalloc(c, &c->cl_col, cap)) || (st = dalloc(c, &c->cl64, cap * 9)) || (st = dalloc(c, &c->cl32, cap * 9)) ||
         (st = dalloc(c, &c->lkey_s, cap)) || (st = dalloc(c, &c->lidx, cap)) || (st = dalloc(c, &c->dflag, 4)))
         return fail(st);
     SG_CHECK(c, cudaMemset(c->dflag, 0, 4 * sizeof(int)));
@@ -277,7 +277,7 @@ extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
                     c->hinges, c->hinge_adj, c->soft_idx, c->shape_grads, c->fb, c->b, c->ckey, c->ckey_s,
                     c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,
                     c->cu_ptr, c->cl_ptr, c->cl_idx, c->lkey, c->lkey_s, c->lidx, c->cub_tmp, c->dflag,
-                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col};
+                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete c;

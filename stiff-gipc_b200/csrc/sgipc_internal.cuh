@@ -46,7 +46,9 @@ struct PcgWork {
     void* Ap;
     PcgScalars* sc;          // [nrhs]
     double* partial;         // reduction partials [nrhs][max_blocks]
-    unsigned int* ticket;    // last-block counters [nrhs * 4]
+    unsigned int* ticket;    // [0..3] last-block counters; [4..5] grid barrier of the persistent solve
+    double* coop;            // persistent solve: block partials [2][nrhs][coop_cap]
+    int coop_cap;            // largest grid the persistent solve may use
     cudaGraphExec_t exec;    // captured iteration loop
     bool cond_graph;         // true: while-node graph (whole loop in one launch)
     long long captured_key;  // precision/rhs tag and domain count the graph was captured for
@@ -145,6 +147,8 @@ struct SgipcCtx {
     int* cl_ptr;                  // [n+1] transposed entries by row
     int* cl_idx;                  // [cap]
     int* cl_col;                  // [cap] column of each transposed entry (= uc_row[cl_idx])
+    double* cl64;                 // [cap*9] transposed copy of uc64[cl_idx[k]] (SpMV reads it directly)
+    float* cl32;
     unsigned long long* lkey;     // [cap]
     unsigned long long* lkey_s;
     int* lidx;
@@ -195,6 +199,16 @@ inline SgipcStatus cuda_fail(SgipcCtx* c, cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return sgipc::cuda_fail(ctx, e_, name); \
     } while (0)
 
+// Vector loads.  kL2 = true reads through L2 only (ld.global.cg): required for vectors that
+// other CTAs of the same (persistent) kernel wrote, which a non-coherent L1 line could hide.
+template <bool kL2, class T>
+__device__ __forceinline__ T ldv(const T* p) {
+    if constexpr (kL2)
+        return __ldcg(p);
+    else
+        return *p;
+}
+
 inline int nblk(long long n, int b = SGIPC_BLOCK) { return (int)((n + b - 1) / b); }
 
 // count `k` kernel launches of this library on the context
@@ -220,6 +234,13 @@ void pcg_destroy(SgipcCtx* c);
 template <class T>
 SgipcStatus spmv_t(SgipcCtx* c, const T* x, T* y, cudaStream_t s);
 SgipcStatus dot64(SgipcCtx* c, const double* a, const double* b, int n, double* out_dev, cudaStream_t s);
+// The whole PCG solve as one cooperative (persistent) kernel; *used = false when the device
+// cannot co-schedule it (the caller then runs the graph of per-phase kernels).
+template <class T, class M, int NR>
+SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
+                         cudaStream_t s, bool* used);
+// largest grid run_pcg_coop launches on `device` (sizes its reduction buffers)
+int coop_max_grid(int device);
 // BAD_INPUT if a kernel flagged an invalid input since the last check (synchronises)
 SgipcStatus check_device_flag(SgipcCtx* c, cudaStream_t s);
 

@@ -39,11 +39,13 @@ __device__ __forceinline__ void bank_reduce_store(int parent, const M (&v)[NR * 
     }
 }
 
-// Levels 1 .. L-2 -> 2 .. L-1, run by ONE CTA (levels >= 1 are at most npos/16 nodes).
-template <class M, int NR>
+// Levels l_first .. L-2 -> l_first+1 .. L-1, run by ONE CTA (levels >= 1 are at most npos/16
+// nodes).
+// kL2: level 1 was written by other CTAs of the same kernel (read it through L2).
+template <class M, int NR, bool kL2 = false>
 __device__ __forceinline__ void restrict_coarse_cta(const int* __restrict__ info, const int* __restrict__ up, int L,
-                                                    M* __restrict__ R) {
-    for (int l = 1; l + 1 < L; l++) {
+                                                    M* __restrict__ R, int l_first = 1) {
+    for (int l = l_first; l + 1 < L; l++) {
         const int count = info[8 + l], start = info[l];
         for (int base = 0; base < count; base += blockDim.x) {
             const int a = base + threadIdx.x;
@@ -55,7 +57,7 @@ __device__ __forceinline__ void restrict_coarse_cta(const int* __restrict__ info
 #pragma unroll
                 for (int q = 0; q < 3; q++)
 #pragma unroll
-                    for (int r = 0; r < NR; r++) v[r * 3 + q] = R[(size_t)(3 * g + q) * NR + r];
+                    for (int r = 0; r < NR; r++) v[r * 3 + q] = ldv<kL2>(R + (size_t)(3 * g + q) * NR + r);
             } else {
 #pragma unroll
                 for (int k = 0; k < NR * 3; k++) v[k] = 0;

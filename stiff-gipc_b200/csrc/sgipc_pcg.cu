@@ -28,72 +28,11 @@
 
 #include "sgipc_internal.cuh"
 #include "sgipc_mas_dev.cuh"
+#include "sgipc_pcg_dev.cuh"
 
 using namespace sgipc;
 
 namespace sgipc {
-
-template <class T>
-struct MatView {
-    const T* fval;   // full symmetric static blocks
-    const T* uc;     // unique contact blocks (upper)
-};
-
-struct Topo {
-    int n;
-    const int* frow_ptr;
-    const int* fcol;
-    const int* cu_ptr;
-    const int* uc_col;
-    const int* cl_ptr;
-    const int* cl_idx;
-    const int* cl_col;
-};
-
-struct MasView {
-    const int* table;
-    int L;
-    int npos;
-    const int* info;
-    const int* part_map;
-    const int* up;
-};
-
-inline Topo topo_of(SgipcCtx* c) {
-    Topo t;
-    t.n = c->n;
-    t.frow_ptr = c->frow_ptr;
-    t.fcol = c->fcol;
-    t.cu_ptr = c->cu_ptr;
-    t.uc_col = c->uc_col;
-    t.cl_ptr = c->cl_ptr;
-    t.cl_idx = c->cl_idx;
-    t.cl_col = c->cl_col;
-    return t;
-}
-
-// ---- block reduction helpers ---------------------------------------------------------------
-template <int NR>
-__device__ __forceinline__ void block_sum(double (&v)[NR], double* smem /*[NR*8]*/) {
-#pragma unroll
-    for (int r = 0; r < NR; r++)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[r] += __shfl_down_sync(0xffffffffu, v[r], o);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0)
-#pragma unroll
-        for (int r = 0; r < NR; r++) smem[r * 8 + w] = v[r];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-        for (int r = 0; r < NR; r++) {
-            double s = 0;
-            for (int k = 0; k < nw; k++) s += smem[r * 8 + k];
-            v[r] = s;
-        }
-    }
-}
 
 // Publishes this CTA's partial sums; returns true in every thread of the last CTA to
 // arrive, after which out[r] holds the deterministic (CTA-order) total.  Every CTA of the
@@ -130,79 +69,6 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NR], double* partial, unsig
     return true;
 }
 
-// ---- SpMV core ------------------------------------------------------------------------------
-template <class T, int NR>
-__device__ __forceinline__ void block_mv3(const T* __restrict__ B, const T (&xj)[NR][3], bool transpose,
-                                          T (&acc)[NR][3]) {
-    T b[9];
-#pragma unroll
-    for (int q = 0; q < 9; q++) b[q] = B[q];
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-        const T x0 = xj[r][0], x1 = xj[r][1], x2 = xj[r][2];
-        if (!transpose) {
-            acc[r][0] += b[0] * x0 + b[1] * x1 + b[2] * x2;
-            acc[r][1] += b[3] * x0 + b[4] * x1 + b[5] * x2;
-            acc[r][2] += b[6] * x0 + b[7] * x1 + b[8] * x2;
-        } else {
-            acc[r][0] += b[0] * x0 + b[3] * x1 + b[6] * x2;
-            acc[r][1] += b[1] * x0 + b[4] * x1 + b[7] * x2;
-            acc[r][2] += b[2] * x0 + b[5] * x1 + b[8] * x2;
-        }
-    }
-}
-
-// Operand gather: x_j (plain vector) or p_j = z_j + beta p_old_j (direction formed on the fly)
-template <class T, int NR>
-struct Operand {
-    const T* a;       // x, or z
-    const T* b;       // nullptr, or p_old
-    T beta[NR];
-    __device__ __forceinline__ void load(int j, T (&xj)[NR][3]) const {
-#pragma unroll
-        for (int q = 0; q < 3; q++)
-#pragma unroll
-            for (int r = 0; r < NR; r++) {
-                const size_t k = (size_t)(3 * j + q) * NR + r;
-                xj[r][q] = b ? a[k] + beta[r] * b[k] : a[k];
-            }
-    }
-};
-
-// Rows are processed by groups of kSpG lanes: lane g of a group takes every kSpG-th block of
-// the row's lists (full static row, contact upper, contact transposed) and the group adds
-// its partial results with shuffles.
-constexpr int kSpG = 4;
-inline int spmv_grid(int n) { return nblk((long long)n * kSpG, 256); }
-
-template <class T, int NR>
-__device__ __forceinline__ void row_mv(const Topo& tp, const MatView<T>& A, const Operand<T, NR>& x, int i, int g,
-                                       T (&acc)[NR][3]) {
-#pragma unroll
-    for (int r = 0; r < NR; r++) acc[r][0] = acc[r][1] = acc[r][2] = 0;
-    if (i < tp.n) {
-        T xj[NR][3];
-        for (int s = tp.frow_ptr[i] + g; s < tp.frow_ptr[i + 1]; s += kSpG) {
-            x.load(tp.fcol[s], xj);
-            block_mv3<T, NR>(A.fval + 9 * (size_t)s, xj, false, acc);
-        }
-        for (int u = tp.cu_ptr[i] + g; u < tp.cu_ptr[i + 1]; u += kSpG) {
-            x.load(tp.uc_col[u], xj);
-            block_mv3<T, NR>(A.uc + 9 * (size_t)u, xj, false, acc);
-        }
-        for (int k = tp.cl_ptr[i] + g; k < tp.cl_ptr[i + 1]; k += kSpG) {
-            x.load(tp.cl_col[k], xj);
-            block_mv3<T, NR>(A.uc + 9 * (size_t)tp.cl_idx[k], xj, true, acc);
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < NR; r++)
-#pragma unroll
-        for (int q = 0; q < 3; q++)
-#pragma unroll
-            for (int o = 1; o < kSpG; o <<= 1) acc[r][q] += __shfl_xor_sync(0xffffffffu, acc[r][q], o, kSpG);
-}
-
 template <class T>
 __global__ void k_spmv(Topo tp, MatView<T> A, const T* __restrict__ x, T* __restrict__ y) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -236,7 +102,7 @@ struct PcgPtrs {
 // K1
 template <class T, int NR>
 __global__ void __launch_bounds__(256) k_pcg_spmv_dot(Topo tp, MatView<T> A, PcgPtrs<T, NR> P) {
-    __shared__ double smem[NR * 8];
+    __shared__ double smem[NR * 32];
     __shared__ int run[NR];
     __shared__ double beta[NR];
     __shared__ int halt, nb;
@@ -315,7 +181,7 @@ __global__ void __launch_bounds__(256) k_pcg_spmv_dot(Topo tp, MatView<T> A, Pcg
 // residual to levels 0 and 1 is a bank-local reduction with plain stores
 template <class T, class M, int NR>
 __global__ void __launch_bounds__(256) k_pcg_update(PcgPtrs<T, NR> P, MasView mv, M* __restrict__ R) {
-    __shared__ double smem[NR * 8];
+    __shared__ double smem[NR * 32];
     __shared__ int st[NR];
     __shared__ int pc[NR];
     __shared__ double alpha[NR];
@@ -435,7 +301,7 @@ template <class T, class M, int NR>
 __global__ void __launch_bounds__(256) k_pcg_prolong_dot(int nv, PcgPtrs<T, NR> P, MasView mv,
                                                          const M* __restrict__ Z, cudaGraphConditionalHandle h,
                                                          int decide, int use_cond) {
-    __shared__ double smem[NR * 8];
+    __shared__ double smem[NR * 32];
     __shared__ int run[NR];
     if (threadIdx.x < NR) run[threadIdx.x] = P.sc[threadIdx.x].state == 0;
     if (decide && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -535,7 +401,7 @@ __global__ void k_pcg_init(const double* __restrict__ b, PcgPtrs<T, NR> P, MasVi
 
 template <class T, int NR>
 __global__ void k_pcg_init_finish(int n3, const double* __restrict__ b, PcgPtrs<T, NR> P) {
-    __shared__ double smem[NR * 8];
+    __shared__ double smem[NR * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double part[NR];
 #pragma unroll
@@ -566,7 +432,7 @@ __global__ void k_pcg_init_finish(int n3, const double* __restrict__ b, PcgPtrs<
 // ---- dot products and vector helpers --------------------------------------------------------
 __global__ void k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double* partial,
                       unsigned int* ticket, double* out) {
-    __shared__ double smem[8];
+    __shared__ double smem[32];
     double v[1] = {0.0};
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) v[0] += a[k] * b[k];
     double tot[1];
@@ -615,28 +481,6 @@ PcgPtrs<T, NR> ptrs_of(PcgWork& w) {
     P.partial = w.partial;
     P.ticket = w.ticket;
     return P;
-}
-
-MasView mas_view(SgipcCtx* c) {
-    MasView m;
-    m.table = c->mas.table;
-    m.L = c->mas.levelnum;
-    m.npos = c->mas.npos;
-    m.info = c->mas.info;
-    m.part_map = c->mas.part_map;
-    m.up = c->mas.up;
-    return m;
-}
-
-template <class T>
-MatView<T> mat_view(SgipcCtx* c);
-template <>
-MatView<double> mat_view<double>(SgipcCtx* c) {
-    return {c->fval64, c->uc64};
-}
-template <>
-MatView<float> mat_view<float>(SgipcCtx* c) {
-    return {c->fval32, c->uc32};
 }
 
 // grid of K3: one coarse CTA + the level-0/1 domains, four per CTA
@@ -732,8 +576,12 @@ SgipcStatus run_pcg(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, doub
     const M* inv = fp32_mas ? (const M*)m.dom32 : (const M*)m.dom64;
     M* R = fp32_mas ? (M*)m.R32 : (M*)m.R64;
     M* Z = fp32_mas ? (M*)m.Z32 : (M*)m.Z64;
+    // one persistent kernel for the whole solve where the device co-schedules it
+    bool coop = false;
+    SgipcStatus st = run_pcg_coop<T, M, NR>(c, w, fp32_mas, b, tol, max_iter, crit, s, &coop);
+    if (st != SGIPC_OK || coop) return st;
     const int k3grid = domain_grid(c);
-    SgipcStatus st = get_loop_graph<T, M, NR>(c, w, inv, R, Z, k3grid, tag);
+    st = get_loop_graph<T, M, NR>(c, w, inv, R, Z, k3grid, tag);
     if (st != SGIPC_OK) return st;
     const int nv = c->nv, n = c->n;
     PcgPtrs<T, NR> P = ptrs_of<T, NR>(w);
@@ -759,7 +607,9 @@ SgipcStatus run_pcg(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, doub
 }
 
 // status of a finished solve: still running (state 0) means the iteration cap was hit
-int final_status(const PcgScalars& s) {
+int final_status(SgipcCtx* c, const PcgScalars& s) {
+    if (s.status == SGIPC_CUDA_ERROR)
+        snprintf(c->err, sizeof(c->err), "pcg: a grid barrier of the persistent solve exceeded its wait limit");
     if (s.state == 0) return SGIPC_NOT_CONVERGED;
     return s.status;
 }
@@ -773,11 +623,14 @@ SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
     SG_CHECK(c, cudaMalloc((void**)&w.ticket, sizeof(unsigned int) * 8));
     SG_CHECK(c, cudaMemset(w.ticket, 0, sizeof(unsigned int) * 8));
     SG_CHECK(c, cudaMemset(w.sc, 0, sizeof(PcgScalars) * nrhs));
+    w.coop_cap = coop_max_grid(c->device);
+    if (w.coop_cap < 1) w.coop_cap = 1;
+    SG_CHECK(c, cudaMalloc((void**)&w.coop, sizeof(double) * 2 * nrhs * (size_t)w.coop_cap));
     return SGIPC_OK;
 }
 
 void free_work(PcgWork& w) {
-    void* ps[] = {w.x, w.r, w.z, w.p, w.p2, w.Ap, w.sc, w.partial, w.ticket};
+    void* ps[] = {w.x, w.r, w.z, w.p, w.p2, w.Ap, w.sc, w.partial, w.ticket, w.coop};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (w.exec) cudaGraphExecDestroy(w.exec);
@@ -882,7 +735,7 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         out.refinements = 0;
         out.rz0 = hs.rz0;
         out.rz = hs.rz_next;
-        out.status = final_status(hs);
+        out.status = final_status(c, hs);
     } else {
         // mixed: FP32 MAS-PCG inner solves on the FP32 matrix copy, FP64 residual refinement
         double* r64 = c->tmp64;
@@ -916,8 +769,8 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
                 bn2 = hs.bnorm2;
             }
             rz = c->h_pinned[0];
-            if (hs.status == SGIPC_BREAKDOWN) {
-                status = SGIPC_BREAKDOWN;
+            if (hs.status == SGIPC_BREAKDOWN || hs.status == SGIPC_CUDA_ERROR) {
+                status = final_status(c, hs);
                 break;
             }
             bool done = crit == SGIPC_CRIT_RZ ? fabs(rz) <= tol * rz0 : c->h_pinned[1] <= tol * tol * bn2;
@@ -1005,7 +858,7 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
     SgipcStatus worst = SGIPC_OK;
     SG_COUNT(c, 4LL * hs[0].bodies);
     for (int r = 0; r < 4; r++) {
-        const int fs = final_status(hs[r]);
+        const int fs = final_status(c, hs[r]);
         if (stats) {
             stats[r] = SgipcSolveStats{};
             stats[r].iterations = hs[r].iter;

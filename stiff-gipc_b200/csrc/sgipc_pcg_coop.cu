@@ -1,0 +1,545 @@
+// sgipc_pcg_coop.cu — the whole MAS-preconditioned CG solve as ONE persistent kernel.
+//
+// Same algorithm and stop rules as the graph of sgipc_pcg.cu (PCGSolver::pcg,
+// StiffGIPC/linear_system/solver/pcg_solver.cu:174-267), but the iteration never leaves
+// the GPU: a cooperative launch keeps every CTA resident, and the phases of an iteration
+// are separated by grid barriers instead of kernel boundaries.  At the sizes of one Newton
+// system (~20k block rows, ~25 MB of matrix, hierarchy and vectors, all L2-resident) an
+// iteration is a handful of dependent L2 round trips, so the design minimises round trips
+// per phase and barrier latency.  Per iteration:
+//   spmv    p = z + beta p_old (ping-pong buffers), Ap = A p, p.Ap          -> barrier + sum
+//   update  x += alpha p, r -= alpha Ap, restriction to MAS levels 0/1, r.r   -> barrier + sum
+//   mas 1   level-0/1 domain solves; restriction level 1 -> 2                 -> barrier
+//   mas 2   CTA 0: restriction to levels >= 3 and their domains; others: level-2 domains
+//                                                                             -> barrier
+//   prolong z = sum_l Z, r.z                                               -> barrier + sum
+// Barrier: one monotonic arrival counter (release add; acquire polling until it reaches
+// epoch x grid).  Dot products: every CTA stores its partial before arriving; after the
+// barrier every CTA adds all partials in the same fixed order, so all CTAs take identical
+// decisions from identical numbers (partials are double-buffered by epoch parity).  Values
+// written by one CTA and read by another inside the kernel are loaded through L2
+// (ld.global.cg).  Waits are bounded: past the limit a CTA raises the abort word, every
+// CTA leaves, and the solve reports SGIPC_CUDA_ERROR.
+#include <cstdlib>
+
+#include "sgipc_internal.cuh"
+#include "sgipc_mas_dev.cuh"
+#include "sgipc_pcg_dev.cuh"
+
+namespace sgipc {
+
+constexpr int kCoopThreads = 512;
+constexpr int kDomPerCta = kCoopThreads / 48;  // 10 domains of 48 rows per round
+constexpr int kCoopMaxCtasPerSm = 2;
+constexpr long long kSpinLimit = 1LL << 25;    // polls (~50 ns each once sleeping): ~2 s
+
+struct GridBarrier {
+    unsigned int* count;  // arrivals since launch (zeroed before the launch)
+    unsigned int* abort;
+};
+
+template <class T, class M, int NR>
+struct CoopArgs {
+    Topo tp;
+    MatView<T> A;
+    MasView mv;
+    const M* inv;
+    M* R;
+    M* Z;
+    const double* b;
+    T* x;
+    T* r;
+    T* z;
+    T* p0;
+    T* p1;
+    T* Ap;
+    PcgScalars* sc;
+    double* partial;   // [2][NR][gridDim.x]
+    GridBarrier br;
+    int nv;
+    int nd01;          // domains of levels 0 and 1
+    int nd2;           // domains of levels 0..2
+    int ndom;          // all domains
+    int max_iter;
+    int crit;
+    double tol;
+};
+
+__device__ __forceinline__ void red_add_release_gpu(unsigned int* p, unsigned int v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier number `epoch` (1, 2, ...).  All threads of every CTA call it.
+__device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch) {
+    __shared__ int s_ok;
+    __syncthreads();  // the CTA's writes of this phase precede thread 0's release
+    if (threadIdx.x == 0) {
+        const unsigned int target = epoch * gridDim.x;
+        red_add_release_gpu(br.count, 1u);
+        int ok = 1;
+        for (long long k = 0;; k++) {
+            if ((int)(ld_acquire_gpu(br.count) - target) >= 0) break;
+            if ((k & 63) == 63 && *(volatile unsigned int*)br.abort) {
+                ok = 0;
+                break;
+            }
+            if (k > kSpinLimit) {
+                atomicExch(br.abort, 1u);
+                ok = 0;
+                break;
+            }
+            if (k > 256) __nanosleep(32);
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Barrier + sum over CTAs: v[r] is this thread's contribution; on return out[r] holds the
+// grid total in every thread.  The partial buffer of parity epoch & 1 is rewritten two
+// barriers later at the earliest, after every CTA has read it.
+template <int NR>
+__device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, double (&v)[NR], double* partial,
+                            double* smem, double (&out)[NR]) {
+    __shared__ double s_tot[NR];
+    double* part = partial + (size_t)(epoch & 1) * NR * gridDim.x;
+    block_sum<NR>(v, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int r = 0; r < NR; r++) part[r * gridDim.x + blockIdx.x] = v[r];
+    const bool ok = grid_barrier(br, epoch);
+    if (threadIdx.x < 32) {
+        // warp 0 adds the partials (fixed lane assignment and shuffle tree: the same total
+        // in every CTA)
+        double acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            acc[r] = 0.0;
+#pragma unroll 4
+            for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) acc[r] += __ldcg(part + r * gridDim.x + k);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+        }
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int r = 0; r < NR; r++) s_tot[r] = acc[r];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NR; r++) out[r] = s_tot[r];
+    __syncthreads();  // s_tot is reused by the next call
+    return ok;
+}
+
+// ---- phases ---------------------------------------------------------------------------------
+// Loops over MAS positions and level-1 nodes are warp-mapped over the whole grid with
+// warp-uniform bounds, so that every 16-lane bank is a half-warp of consecutive entries
+// (bank_reduce_store needs all 32 lanes).
+__device__ __forceinline__ int grid_warp() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
+__device__ __forceinline__ int grid_warps() { return (int)((gridDim.x * blockDim.x) >> 5); }
+
+// r = b, x = 0, R (levels 0 and 1) = restriction of r, ||b||^2
+template <class T, class M, int NR>
+__device__ void phase_init(const CoopArgs<T, M, NR>& a, double (&bb)[NR]) {
+    const MasView& mv = a.mv;
+    const int lane = threadIdx.x & 31;
+    for (int pb = grid_warp() * 32; pb < mv.npos; pb += grid_warps() * 32) {
+        const int p = pb + lane;
+        const int v = p < mv.npos ? mv.part_map[p] : -1;
+        M val[NR * 3];
+#pragma unroll
+        for (int k = 0; k < NR * 3; k++) val[k] = 0;
+        if (v >= 0) {
+#pragma unroll
+            for (int r = 0; r < NR; r++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    const size_t k = (size_t)(3 * v + q) * NR + r;
+                    const double bv = a.b[k];
+                    a.r[k] = (T)bv;
+                    a.x[k] = 0;
+                    val[r * 3 + q] = (M)(T)bv;
+                    bb[r] += bv * bv;
+                }
+        }
+        if (p < mv.npos)
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) a.R[(size_t)(3 * p + q) * NR + r] = val[r * 3 + q];
+        bank_reduce_store<M, NR>(v >= 0 ? mv.up[p] : -1, val, a.R);
+    }
+}
+
+// Z_d = A_d^-1 R_d: 48-thread slot `threadIdx.x / 48` of the CTA takes domain d0 + slot
+// when it is below `hi`.  All loads of a row of the product are issued together.
+template <class M, int NR>
+__device__ __forceinline__ void solve_domains(const M* __restrict__ inv, const M* R, M* Z, int d0, int hi,
+                                              M (*sR)[48 * NR]) {
+    const int ld = threadIdx.x / 48, i = threadIdx.x % 48;
+    const int d = d0 + ld;
+    const bool act = ld < kDomPerCta && d < hi;
+    if (act)
+#pragma unroll
+        for (int r = 0; r < NR; r++) sR[ld][i * NR + r] = __ldcg(R + (48 * (size_t)d + i) * NR + r);
+    __syncthreads();
+    if (act) {
+        const M* Ad = inv + (size_t)d * 2304;
+        M acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) acc[r] = 0;
+        constexpr int kU = sizeof(M) == 4 ? (NR == 1 ? 24 : 12) : (NR == 1 ? 12 : 6);  // loads in flight
+#pragma unroll
+        for (int j0 = 0; j0 < 48; j0 += kU) {
+            M w[kU];
+#pragma unroll
+            for (int j = 0; j < kU; j++) w[j] = __ldg(Ad + (j0 + j) * 48 + i);
+#pragma unroll
+            for (int j = 0; j < kU; j++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) acc[r] += w[j] * sR[ld][(j0 + j) * NR + r];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) Z[(48 * (size_t)d + i) * NR + r] = acc[r];
+    }
+    __syncthreads();
+}
+
+// domains [lo, hi) over CTAs first .. first+ncta-1 (block-uniform loop bounds)
+template <class M, int NR>
+__device__ __forceinline__ void solve_domain_range(const M* inv, const M* R, M* Z, int lo, int hi, int first,
+                                                   int ncta, M (*sR)[48 * NR]) {
+    const int c = (int)blockIdx.x - first;
+    if (c < 0 || c >= ncta) return;
+    for (int d0 = lo + c * kDomPerCta; d0 < hi; d0 += ncta * kDomPerCta) solve_domains<M, NR>(inv, R, Z, d0, hi, sR);
+}
+
+// restriction level 1 -> 2, one half-warp per level-1 bank, taken by the LAST warps of the
+// grid (the level-0/1 domain solves fill the first CTAs)
+template <class M, int NR>
+__device__ void restrict_level1(const MasView& mv, M* R) {
+    const int count = mv.info[9], start = mv.info[1];
+    const int lane = threadIdx.x & 31;
+    for (int ab = (grid_warps() - 1 - grid_warp()) * 32; ab < count; ab += grid_warps() * 32) {
+        const int aa = ab + lane;
+        M v[NR * 3];
+        int par = -1;
+        if (aa < count) {
+            const int g = start + aa;
+            par = mv.up[g];
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) v[r * 3 + q] = __ldcg(R + (size_t)(3 * g + q) * NR + r);
+        } else {
+#pragma unroll
+            for (int k = 0; k < NR * 3; k++) v[k] = 0;
+        }
+        bank_reduce_store<M, NR>(par, v, R);
+    }
+}
+
+// z = M^-1 r given R at levels 0 and 1: two phases and two barriers (one when L <= 2)
+template <class T, class M, int NR>
+__device__ bool phase_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], unsigned int& epoch) {
+    const int L = a.mv.L, G = gridDim.x;
+    if (L > 2) restrict_level1<M, NR>(a.mv, a.R);
+    solve_domain_range<M, NR>(a.inv, a.R, a.Z, 0, a.nd01, 0, G, sR);
+    if (!grid_barrier(a.br, ++epoch)) return false;
+    if (L <= 2) return true;
+    if (blockIdx.x == 0) {
+        restrict_coarse_cta<M, NR, true>(a.mv.info, a.mv.up, L, a.R, 2);
+        solve_domain_range<M, NR>(a.inv, a.R, a.Z, a.nd2, a.ndom, 0, 1, sR);
+    }
+    if (G > 1)
+        solve_domain_range<M, NR>(a.inv, a.R, a.Z, a.nd01, a.nd2, 1, G - 1, sR);
+    else
+        solve_domain_range<M, NR>(a.inv, a.R, a.Z, a.nd01, a.nd2, 0, 1, sR);
+    return grid_barrier(a.br, ++epoch);
+}
+
+// z = sum over levels of Z at the vertex's clusters; r.z
+template <class T, class M, int NR>
+__device__ void phase_prolong(const CoopArgs<T, M, NR>& a, const bool (&run)[NR], double (&rz)[NR]) {
+    const MasView& mv = a.mv;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nv; v += gridDim.x * blockDim.x) {
+        const int* tv = mv.table + (size_t)v * mv.L;
+        int gl[SGIPC_MAX_LEVELS];
+#pragma unroll
+        for (int l = 0; l < SGIPC_MAX_LEVELS; l++) gl[l] = l < mv.L ? __ldg(tv + l) : -1;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            if (!run[r]) continue;
+            M s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+            for (int l = 0; l < SGIPC_MAX_LEVELS; l++) {
+                if (gl[l] < 0) continue;
+                s0 += __ldcg(a.Z + (size_t)(3 * gl[l]) * NR + r);
+                s1 += __ldcg(a.Z + (size_t)(3 * gl[l] + 1) * NR + r);
+                s2 += __ldcg(a.Z + (size_t)(3 * gl[l] + 2) * NR + r);
+            }
+            const T zz[3] = {(T)s0, (T)s1, (T)s2};
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const size_t k = (size_t)(3 * v + q) * NR + r;
+                a.z[k] = zz[q];
+                rz[r] += (double)__ldcg(a.r + k) * (double)zz[q];
+            }
+        }
+    }
+}
+
+// p = z + beta p_old (p = z on the first iteration), Ap = A p, p.Ap
+template <class T, class M, int NR>
+__device__ void phase_spmv(const CoopArgs<T, M, NR>& a, bool first, const double (&beta)[NR], const T* pold, T* pnew,
+                           const bool (&run)[NR], double (&pAp)[NR]) {
+    Operand<T, NR, true> op;
+    op.a = a.z;
+    op.b = first ? nullptr : pold;
+#pragma unroll
+    for (int r = 0; r < NR; r++) op.beta[r] = (T)beta[r];
+    constexpr int gpw = 32 / kSpG;  // rows per warp and pass
+    const int lane = threadIdx.x & 31;
+    const int n = a.tp.n;
+    for (int i0 = grid_warp() * gpw; i0 < n; i0 += grid_warps() * gpw) {  // warp-uniform bound
+        const int i = i0 + lane / kSpG, g = lane % kSpG;
+        T pi[NR][3];
+        if (i < n && g == 0) op.load(i, pi);  // issued before the row's gathers
+        T acc[NR][3];
+        row_mv<T, NR>(a.tp, a.A, op, i, g, acc);
+        if (i < n && g == 0) {
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                if (!run[r]) continue;
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    const size_t k = (size_t)(3 * i + q) * NR + r;
+                    pnew[k] = pi[r][q];
+                    a.Ap[k] = acc[r][q];
+                    pAp[r] += (double)pi[r][q] * (double)acc[r][q];
+                }
+            }
+        }
+    }
+}
+
+// x += alpha p, r -= alpha Ap, restriction of r to levels 0 and 1, r.r
+template <class T, class M, int NR>
+__device__ void phase_update(const CoopArgs<T, M, NR>& a, const double (&alpha)[NR], const T* p,
+                             const bool (&run)[NR], double (&rr)[NR]) {
+    const MasView& mv = a.mv;
+    const int lane = threadIdx.x & 31;
+    for (int pb = grid_warp() * 32; pb < mv.npos; pb += grid_warps() * 32) {
+        const int pos = pb + lane;
+        const int v = pos < mv.npos ? mv.part_map[pos] : -1;
+        M val[NR * 3];
+#pragma unroll
+        for (int k = 0; k < NR * 3; k++) val[k] = 0;
+        if (v >= 0) {
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                if (!run[r]) continue;
+                const T al = (T)alpha[r];
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    const size_t k = (size_t)(3 * v + q) * NR + r;
+                    a.x[k] = __ldcg(a.x + k) + al * __ldcg(p + k);
+                    const T rv = __ldcg(a.r + k) - al * __ldcg(a.Ap + k);
+                    a.r[k] = rv;
+                    rr[r] += (double)rv * (double)rv;
+                    val[r * 3 + q] = (M)rv;
+                }
+            }
+        }
+        if (pos < mv.npos)
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) a.R[(size_t)(3 * pos + q) * NR + r] = val[r * 3 + q];
+        bank_reduce_store<M, NR>(v >= 0 ? mv.up[pos] : -1, val, a.R);
+    }
+}
+
+// ---- the solve ------------------------------------------------------------------------------
+template <class T, class M, int NR>
+__global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a) {
+    __shared__ double smem[NR * 32];
+    __shared__ M sR[kDomPerCta][48 * NR];
+    unsigned int epoch = 0;
+    // per right-hand side state, identical in every thread (computed from the same totals)
+    bool run[NR];
+    int iters[NR], status[NR];
+    double rz0[NR], rz[NR], bn2[NR], rr[NR], beta[NR], v[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        run[r] = true;
+        iters[r] = 0;
+        status[r] = SGIPC_OK;
+        rz0[r] = rz[r] = rr[r] = beta[r] = v[r] = 0.0;
+    }
+    // ---- r = b, x = 0, z = M r, rz0 = r.z
+    phase_init(a, v);
+    bool ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, bn2);
+    ok = ok && phase_mas(a, sR, epoch);
+    if (ok) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) v[r] = 0.0;
+        phase_prolong(a, run, v);
+        ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, rz0);
+    }
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        rz[r] = rz0[r];
+        rr[r] = bn2[r];
+        if (!(rz0[r] > 0.0) || !isfinite(rz0[r])) {
+            // b = 0 (or an indefinite preconditioner): nothing to iterate
+            run[r] = false;
+            if (!isfinite(rz0[r]) || rz0[r] < 0.0) status[r] = SGIPC_BREAKDOWN;
+        }
+        any |= run[r];
+    }
+    // ---- iterations k = 1 .. max_iter-1
+    for (int k = 1; ok && any && k < a.max_iter; k++) {
+        T* pnew = (k & 1) ? a.p1 : a.p0;
+        const T* pold = (k & 1) ? a.p0 : a.p1;
+        double pAp[NR], alpha[NR];
+        bool stop_rz[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) pAp[r] = 0.0;
+        phase_spmv(a, k == 1, beta, pold, pnew, run, pAp);
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, pAp, a.partial, smem, pAp))) break;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            stop_rz[r] = false;
+            alpha[r] = 0.0;
+            if (!run[r]) continue;
+            iters[r] = k;
+            if (!(pAp[r] > 0.0) || !isfinite(pAp[r]) || !isfinite(rz[r])) {
+                run[r] = false;
+                status[r] = SGIPC_BREAKDOWN;
+                continue;
+            }
+            alpha[r] = rz[r] / pAp[r];
+            // the reference tests the r.z of the current iterate and stops after its update
+            stop_rz[r] = a.crit == SGIPC_CRIT_RZ && fabs(rz[r]) <= a.tol * rz0[r];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) v[r] = 0.0;
+        phase_update(a, alpha, pnew, run, v);
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, v))) break;
+        any = false;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            if (!run[r]) continue;
+            rr[r] = v[r];
+            if (stop_rz[r] || (a.crit == SGIPC_CRIT_TRUE && v[r] <= a.tol * a.tol * bn2[r])) run[r] = false;
+            any |= run[r];
+        }
+        if (!any || k + 1 >= a.max_iter) break;  // converged, or the iteration cap
+        if (!(ok = phase_mas(a, sR, epoch))) break;
+#pragma unroll
+        for (int r = 0; r < NR; r++) v[r] = 0.0;
+        phase_prolong(a, run, v);
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, v))) break;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            if (!run[r]) continue;
+            beta[r] = v[r] / rz[r];
+            rz[r] = v[r];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            PcgScalars& s = a.sc[r];
+            s.iter = iters[r];
+            s.rz0 = rz0[r];
+            s.rz = rz[r];
+            s.rz_next = rz[r];
+            s.bnorm2 = bn2[r];
+            s.rr = rr[r];
+            s.bodies = 0;
+            s.halt = 1;
+            // state 0 = still running when the iteration cap was reached
+            s.state = ok ? (run[r] ? 0 : 2) : 2;
+            s.status = ok ? status[r] : SGIPC_CUDA_ERROR;
+        }
+    }
+}
+
+// ---- host launcher ----------------------------------------------------------------------------
+template <class T, class M, int NR>
+SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
+                         cudaStream_t s, bool* used) {
+    *used = false;
+    const char* e = getenv("SGIPC_PCG_GRAPH");
+    if (e && e[0] == '1') return SGIPC_OK;  // the graph of per-phase kernels instead
+    int coop = 0, nsm = 0, per = 0;
+    SG_CHECK(c, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
+    SG_CHECK(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    SG_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_coop<T, M, NR>, kCoopThreads, 0));
+    if (!coop || per < 1) return SGIPC_OK;
+    if (per > kCoopMaxCtasPerSm) per = kCoopMaxCtasPerSm;
+    int grid = nsm * per;
+    if (grid > w.coop_cap) grid = w.coop_cap;
+    MasWork& m = c->mas;
+    CoopArgs<T, M, NR> a;
+    a.tp = topo_of(c);
+    a.A = mat_view<T>(c);
+    a.mv = mas_view(c);
+    a.inv = fp32_mas ? (const M*)m.dom32 : (const M*)m.dom64;
+    a.R = fp32_mas ? (M*)m.R32 : (M*)m.R64;
+    a.Z = fp32_mas ? (M*)m.Z32 : (M*)m.Z64;
+    a.b = b;
+    a.x = (T*)w.x;
+    a.r = (T*)w.r;
+    a.z = (T*)w.z;
+    a.p0 = (T*)w.p;
+    a.p1 = (T*)w.p2;
+    a.Ap = (T*)w.Ap;
+    a.sc = w.sc;
+    a.partial = w.coop;
+    a.br = {w.ticket + 4, w.ticket + 5};
+    a.nv = c->nv;
+    const int* h = m.h_info;
+    const int L = m.levelnum;
+    a.ndom = h[16] / 16;
+    a.nd01 = L > 2 ? h[2] / 16 : a.ndom;
+    a.nd2 = L > 3 ? h[3] / 16 : a.ndom;
+    a.max_iter = max_iter;
+    a.crit = crit;
+    a.tol = tol;
+    SG_CHECK(c, cudaMemsetAsync(w.ticket + 4, 0, 2 * sizeof(unsigned int), s));
+    void* args[] = {&a};
+    SG_COUNT(c, 1);
+    SG_CHECK(c, cudaLaunchCooperativeKernel((const void*)k_pcg_coop<T, M, NR>, dim3(grid), dim3(kCoopThreads), args,
+                                            0, s));
+    *used = true;
+    return SGIPC_OK;
+}
+
+#define SGIPC_COOP_INST(T, M, NR)                                                                             \
+    template SgipcStatus run_pcg_coop<T, M, NR>(SgipcCtx*, PcgWork&, int, const double*, double, int, int, \
+                                                cudaStream_t, bool*);
+SGIPC_COOP_INST(double, double, 1)
+SGIPC_COOP_INST(double, float, 1)
+SGIPC_COOP_INST(float, float, 1)
+SGIPC_COOP_INST(double, double, 4)
+SGIPC_COOP_INST(double, float, 4)
+SGIPC_COOP_INST(float, float, 4)
+
+int coop_max_grid(int device) {
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    return nsm * kCoopMaxCtasPerSm;
+}
+
+}  // namespace sgipc

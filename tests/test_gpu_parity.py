@@ -164,6 +164,50 @@ def test_batched_four_rhs(case):
             assert res < max(tol, 1e-9), (prec, r, res, sts[r].iterations)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "ref"])
+def test_persistent_and_graph_solves_agree(case, prec, monkeypatch):
+    """The one-kernel persistent solve and the graph of per-phase kernels run the same
+    algorithm; only the summation order of the dot products differs."""
+    sc, g, _ = case
+    mas = system.MASPreconditioner(g)
+    mas.setPreconditioner(prec)
+    solver = system.PCGSolver(g, system.PCGSolverConfig(precision=prec))
+    xa, sa = solver.solve(g.rhs())
+    xa = xa.cpu().numpy()
+    monkeypatch.setenv("SGIPC_PCG_GRAPH", "1")
+    xb, sb = solver.solve(g.rhs())
+    xb = xb.cpu().numpy()
+    monkeypatch.delenv("SGIPC_PCG_GRAPH")
+    assert sa.status == N.OK and sb.status == N.OK
+    assert abs(sa.iterations - sb.iterations) <= 1
+    assert abs(sa.rz0 - sb.rz0) <= 1e-9 * abs(sb.rz0)
+    if sa.iterations == sb.iterations:
+        assert _rel(xa, xb) < (1e-9 if prec == "fp64" else 1e-4)
+
+
+def test_iteration_cap_reports_not_converged(case):
+    sc, g, _ = case
+    mas = system.MASPreconditioner(g)
+    mas.setPreconditioner("fp64")
+    L = N.lib()
+    import ctypes
+    b = g.rhs()
+    x = torch.empty_like(b)
+    for graph in (False, True):
+        if graph:
+            import os
+            os.environ["SGIPC_PCG_GRAPH"] = "1"
+        try:
+            st = N.SgipcSolveStats()
+            s = L.sgipc_pcg_solve(g.ctx, N.FP64, N.CRIT_RZ, 1e-12, 4, ctypes.c_void_p(b.data_ptr()),
+                                  ctypes.c_void_p(x.data_ptr()), ctypes.byref(st), None)
+        finally:
+            if graph:
+                del os.environ["SGIPC_PCG_GRAPH"]
+        assert s == N.NOT_CONVERGED and st.status == N.NOT_CONVERGED, graph
+        assert st.iterations == 3, graph   # max_iter 4: SpMVs k = 1 .. max_iter-1
+
+
 def test_bad_inputs_are_reported(case):
     sc, g, _ = case
     L = N.lib()
