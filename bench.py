@@ -228,9 +228,8 @@ def run_ours(args):
     # roofline of the dominant kernel: per-step share = avg launch time x launches per step
     step("mixed")
     torch.cuda.synchronize()
-    it = st_mixed.iterations
     per_step = {"snk": 1, "gather_blocks": 1, "barrier": 1, "friction": 1, "mas_scatter": 1, "mas_invert": 1,
-                "spmv32": it, "mas_domain32": it + 2 * max(1, st_mixed.refinements)}
+                "pcg32": max(1, st_mixed.refinements)}
     kern = {}
     for name, cnt in per_step.items():
         try:

@@ -258,15 +258,17 @@ SgipcStatus sgipc_adjoint_param_grads(SgipcCtx* ctx, const SgipcFemData* fem,
  *      StiffGIPC/gipc/utils/timer.h:19-136, GIPC.cu:10854-10964) ----------------------- */
 
 /* Number of this library's kernels launched on the context since creation (library
- * kernels such as CUB sorts excluded; graph-resident PCG iterations counted by the
- * iteration bodies they executed).  Synchronises. */
+ * kernels such as CUB sorts excluded; a persistent PCG solve counts as one launch, a
+ * graph-resident PCG loop by the iteration bodies it executed).  Synchronises. */
 SgipcStatus sgipc_launch_count(SgipcCtx* ctx, int64_t* launches);
 
 /* Re-launch one hot kernel `reps` times on `stream` against the context's current state,
  * bracketed by CUDA events on that stream, and return its average duration [ms] and the
  * algorithmic bytes one launch must move.  Names: "snk", "gather_blocks", "barrier",
  * "friction", "spmv64", "spmv32", "mas_scatter", "mas_invert", "mas_domain64",
- * "mas_domain32".  Leaves the assembled system and the MAS state as they were (the
+ * "mas_domain32", and "pcg32" / "pcg64" (one whole persistent PCG solve of the last
+ * right-hand side to the 1e-4 r.z criterion, with FP32 / FP64 vectors; the MAS must have
+ * been built in that precision).  Leaves the assembled system and the MAS state as they were (the
  * MAS kernels rebuild what they overwrite).  Synchronises. */
 SgipcStatus sgipc_time_kernel(SgipcCtx* ctx, const char* name, int32_t reps, void* stream,
                               float* avg_ms, double* bytes_per_launch);

@@ -875,7 +875,42 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
 }
 
 namespace sgipc {
+// "pcg32" / "pcg64": one PCG solve of the last right-hand side to the 1e-4 r.z criterion
+// (FP32 vectors + FP32 MAS, the inner solve of the mixed mode / FP64 throughout), i.e. one
+// launch of the persistent solve.  Algorithmic bytes: iterations x (SpMV + 2 dots + 2
+// axpys + MAS apply), each compulsory array read or written once:
+//   SpMV nb (sb + 4) + (n + 1) 4 + 2 (3n) sv;  dots 2 x 2 (3n) sv;  axpys 6 (3n) sv + 3 (3n) sv;
+//   MAS (3n) sv + 12 Nc + (Nc / 16) 136 sb + 12 Nc + 4 L Nc + (3n) sv
+// with sv / sb the vector / 3x3-block bytes, nb the stored upper blocks, Nc the clusters.
+static SgipcStatus pcg_solve_hook(SgipcCtx* c, bool f64, cudaStream_t s, double* bytes) {
+    if (!c->mas.built || (c->mas.built == SGIPC_FP64 + 1) != f64) {
+        snprintf(c->err, sizeof(c->err), "time_kernel pcg%s: the MAS was built in the other precision",
+                 f64 ? "64" : "32");
+        return SGIPC_BAD_INPUT;
+    }
+    const int n3 = 3 * c->n;
+    const int max_iter = n3 * 3 / 10 > 2 ? n3 * 3 / 10 : 2;
+    SgipcStatus st = f64 ? run_pcg<double, double, 1>(c, c->pcg64, 0, c->b, 1e-4, max_iter, SGIPC_CRIT_RZ, s, 10)
+                         : run_pcg<float, float, 1>(c, c->pcg32, 1, c->b, 1e-4, max_iter, SGIPC_CRIT_RZ, s, 20);
+    if (st != SGIPC_OK) return st;
+    if (*bytes == 0.0) {  // untimed first launch: read the iteration count and block count
+        PcgScalars hs;
+        int nuc = 0;
+        SG_CHECK(c, cudaMemcpyAsync(&hs, (f64 ? c->pcg64 : c->pcg32).sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        SG_CHECK(c, cudaMemcpyAsync(&nuc, c->nuc, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SG_CHECK(c, cudaStreamSynchronize(s));
+        const double sv = f64 ? 8 : 4, sb = f64 ? 72 : 36, Nc = c->mas.h_info[16], L = c->mas.levelnum;
+        const double nb = (double)c->nnz + nuc;
+        const double spmv = nb * (sb + 4) + (c->n + 1.0) * 4 + 2.0 * n3 * sv;
+        const double dots = 2 * 2.0 * n3 * sv, axpy = 9.0 * n3 * sv;
+        const double mas = 2.0 * n3 * sv + 24 * Nc + Nc / 16 * 136 * sb + 4 * L * Nc;
+        *bytes = hs.iter * (spmv + dots + axpy + mas);
+    }
+    return SGIPC_OK;
+}
+
 SgipcStatus pcg_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double* bytes) {
+    if (!strcmp(name, "pcg32") || !strcmp(name, "pcg64")) return pcg_solve_hook(c, name[3] == '6', s, bytes);
     const bool f64 = !strcmp(name, "spmv64"), f32 = !strcmp(name, "spmv32");
     if (!f64 && !f32) return SGIPC_NOT_READY;
     // the contact block count is read once, on the untimed first launch (*bytes still 0),
