@@ -45,6 +45,7 @@ def lib():
         L.or_friction_pair.restype = C.c_int
         L.or_friction_ground.argtypes = [_d, _d, C.c_double, C.c_double, C.c_double, _d, _d, _d]
         L.or_make_pd.argtypes = [C.c_int, _d]
+        L.or_tri_bw.argtypes = [_d, _d, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _d, _d, _d]
         L.or_pair_geom.argtypes = [_i, _d, C.c_double, _d, _d, _d, _d]
         L.or_pair_geom.restype = C.c_int
         L.or_eig.argtypes = [C.c_int, _d, _d, _d]
@@ -126,6 +127,14 @@ def pair_geom(enc, X, dhat):
     return nv, f[0], gf[:3 * nv], c[0], gc[:3 * nv]
 
 
+def tri_bw(X, Dinv, area, kst, ksh, srate, dt2):
+    """(energy, grad (9,), H (9,9)) of one Baraff-Witkin cloth triangle."""
+    X, Dinv = _f64(X).reshape(9), _f64(Dinv).reshape(4)
+    e, g, H = np.zeros(1), np.zeros(9), np.zeros(81)
+    lib().or_tri_bw(_p(X), _p(Dinv), area, kst, ksh, srate, dt2, _p(e), _p(g), _p(H))
+    return e[0], g, H.reshape(9, 9)
+
+
 def make_pd(A):
     A = _f64(A).copy()
     lib().or_make_pd(A.shape[0], _p(A))
@@ -143,7 +152,9 @@ class _OrScene(C.Structure):
         ("fpairs", _i), ("flam", _d), ("fcoord", _d), ("fbasis", _d), ("fgpairs", _i), ("fglam", _d),
         ("soft_idx", _i), ("soft_target", _d)] + [
         (n, C.c_double) for n in ("dt", "dhat", "kappa", "fdhat", "mu", "mu_gd", "ground_offset",
-                                   "motion_rate", "soft_rate")]
+                                   "motion_rate", "soft_rate")] + [
+        ("nf", C.c_int), ("nh", C.c_int), ("tris", _i), ("tdminv", _d), ("tarea", _d), ("hinges", _i),
+        ("hadj", _i), ("hq", _d)] + [(n, C.c_double) for n in ("stretch", "shear", "strain_rate", "bend")]
 
 
 def _scene_struct(sc, x=None):
@@ -171,7 +182,11 @@ def _scene_struct(sc, x=None):
                  fglam=f(sc.fric_gd_lambda), soft_idx=i(sc.soft_index), soft_target=f(sc.soft_target.reshape(-1, 3)),
                  dt=p["dt"], dhat=p["dHat"], kappa=p["kappa"], fdhat=p["fDhat"], mu=p["frictionRate"],
                  mu_gd=p["gd_frictionRate"], ground_offset=p["ground_offset"], motion_rate=p["motionRate"],
-                 soft_rate=p["softRate"])
+                 soft_rate=p["softRate"], nf=len(sc.tris), nh=len(sc.hinges), tris=i(sc.tris.reshape(-1, 3)),
+                 tdminv=f(sc.tri_dm_inv.reshape(-1, 4)), tarea=f(sc.area), hinges=i(sc.hinges.reshape(-1, 2)),
+                 hadj=i(sc.hinge_adj.reshape(-1, 2)), hq=f(np.transpose(sc.hinge_q, (0, 2, 1)).reshape(-1, 16)),
+                 stretch=p.get("stretchStiff", 0.0), shear=p.get("shearStiff", 0.0),
+                 strain_rate=p.get("strainRate", 0.0), bend=p.get("bendStiff", 0.0))
     return s, keep
 
 

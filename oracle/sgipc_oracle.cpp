@@ -213,6 +213,96 @@ void snk_tet(const double* X /*4x3*/, const double* Dinv /*3x3 row-major*/, doub
 }
 
 // ---------------------------------------------------------------------------------------
+// Baraff-Witkin cloth membrane (femEnergy.cu:351-403 stress, 535-707 projected Hessians,
+// 2146-2215 element kernel).  F = Ds Dm^-1 (3x2) with columns f0, f1;
+//   E = area * dt^2 * [ k_st (S(|f0|) + S(|f1|)) + k_sh (f0.f1)^2 ],
+//   S(t) = (t-1)^2 + [t > 1] s (t-1)^3.
+// The reference projects the stretch Hessian (per column) and the shear Hessian to PSD
+// separately and adds them; here each exact Hessian is built in closed form and projected
+// by the numeric eigen-decomposition.  vec(F) is column-major (f0 then f1).
+// ---------------------------------------------------------------------------------------
+void tri_bw(const double* X /*3x3*/, const double* Dinv /*2x2 row-major*/, double area, double kst, double ksh,
+            double srate, double dt2, double* energy, double* grad /*9*/, double* H9 /*81*/) {
+    double f[2][3];
+    for (int j = 0; j < 2; j++)
+        for (int i = 0; i < 3; i++)
+            f[j][i] = (X[3 + i] - X[i]) * Dinv[0 * 2 + j] + (X[6 + i] - X[i]) * Dinv[1 * 2 + j];
+    double E = 0, P[6] = {0}, Hf[36] = {0};
+    for (int j = 0; j < 2; j++) {
+        double t = std::sqrt(f[j][0] * f[j][0] + f[j][1] * f[j][1] + f[j][2] * f[j][2]);
+        double u = t - 1.0;
+        double S = u * u + (t > 1.0 ? srate * u * u * u : 0.0);
+        double dS = 2.0 * u + (t > 1.0 ? 3.0 * srate * u * u : 0.0);
+        double d2S = 2.0 + (t > 1.0 ? 6.0 * srate * u : 0.0);
+        E += kst * S;
+        double H3[9];
+        for (int p = 0; p < 3; p++) {
+            P[3 * j + p] += kst * dS / t * f[j][p];
+            for (int q = 0; q < 3; q++) {
+                double n2 = f[j][p] * f[j][q] / (t * t);
+                H3[3 * p + q] = d2S * n2 + dS / t * ((p == q ? 1.0 : 0.0) - n2);
+            }
+        }
+        make_pd(3, H3);
+        for (int p = 0; p < 3; p++)
+            for (int q = 0; q < 3; q++) Hf[(3 * j + p) * 6 + 3 * j + q] += kst * H3[3 * p + q];
+    }
+    // shear: E = I6^2, gradient 2 I6 g with g = [f1; f0], Hessian 2 (g g^T + I6 swap)
+    double I6 = f[0][0] * f[1][0] + f[0][1] * f[1][1] + f[0][2] * f[1][2];
+    E += ksh * I6 * I6;
+    double g[6] = {f[1][0], f[1][1], f[1][2], f[0][0], f[0][1], f[0][2]};
+    double Hs[36];
+    for (int r = 0; r < 6; r++) {
+        P[r] += ksh * 2.0 * I6 * g[r];
+        for (int c = 0; c < 6; c++) Hs[r * 6 + c] = 2.0 * (g[r] * g[c] + ((c == (r + 3) % 6) ? I6 : 0.0));
+    }
+    make_pd(6, Hs);
+    for (int k = 0; k < 36; k++) Hf[k] += ksh * Hs[k];
+    // dF(:,j)/dx_a = D[a][j] I
+    double D[3][2];
+    for (int j = 0; j < 2; j++) {
+        D[0][j] = -(Dinv[0 * 2 + j] + Dinv[1 * 2 + j]);
+        D[1][j] = Dinv[0 * 2 + j];
+        D[2][j] = Dinv[1 * 2 + j];
+    }
+    double sc = area * dt2;
+    if (energy) *energy = E * sc;
+    if (grad)
+        for (int a = 0; a < 3; a++)
+            for (int p = 0; p < 3; p++) grad[3 * a + p] = sc * (D[a][0] * P[p] + D[a][1] * P[3 + p]);
+    if (H9)
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+                for (int p = 0; p < 3; p++)
+                    for (int q = 0; q < 3; q++) {
+                        double h = 0;
+                        for (int j = 0; j < 2; j++)
+                            for (int l = 0; l < 2; l++) h += D[a][j] * D[b][l] * Hf[(3 * j + p) * 6 + 3 * l + q];
+                        H9[(3 * a + p) * 9 + 3 * b + q] = sc * h;
+                    }
+}
+
+// ---------------------------------------------------------------------------------------
+// quadratic bending (femEnergy.cu:2623-2753): E = 1/2 c sum_ij Q_ij x_i . x_j with
+// c = |rest e0 - rest e1| * bendStiff * dt^2, Q column-major 4x4 per hinge.
+// ---------------------------------------------------------------------------------------
+void hinge_quad(const double* X /*4x3*/, const double* Qcm, double c, double* energy, double* grad /*12*/,
+                double* H12 /*144*/) {
+    double E = 0;
+    for (int i = 0; i < 4; i++)
+        for (int k = 0; k < 3; k++) {
+            double s = 0;
+            for (int j = 0; j < 4; j++) s += Qcm[4 * j + i] * X[3 * j + k];
+            if (grad) grad[3 * i + k] = c * s;
+            E += 0.5 * c * X[3 * i + k] * s;
+        }
+    if (energy) *energy = E;
+    if (H12)
+        for (int r = 0; r < 12; r++)
+            for (int cc = 0; cc < 12; cc++) H12[r * 12 + cc] = (r % 3 == cc % 3) ? c * Qcm[4 * (cc / 3) + r / 3] : 0.0;
+}
+
+// ---------------------------------------------------------------------------------------
 // IPC barrier (RANK 2): b(I) = kappa * dhat^2 * (I-1)^2 * ln(I)^2, I = d^2 / dhat
 // ---------------------------------------------------------------------------------------
 struct BarrierScalars { double B, dB, d2B; };
@@ -458,6 +548,25 @@ void push_pair_blocks(Coo& coo, int nv, const int* vid, const double* H, const i
         }
 }
 
+// upper blocks (a <= b by position in the element) of an element Hessian with stride 3nv,
+// oriented (min, max) by vertex id, zeroed when they touch a Dirichlet vertex
+void push_elem_blocks(Coo& coo, int nv, const int32_t* vid, const double* H, const int32_t* btype) {
+    const int st = 3 * nv;
+    for (int a = 0; a < nv; a++)
+        for (int b = a; b < nv; b++) {
+            int r = vid[a], c = vid[b];
+            bool tr = r > c;
+            bool dir = btype[r] != 0 || btype[c] != 0;
+            double blk[9];
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) {
+                    double v = tr ? H[(3 * b + i) * st + 3 * a + j] : H[(3 * a + i) * st + 3 * b + j];
+                    blk[i * 3 + j] = dir ? 0.0 : v;
+                }
+            if (tr) coo.add(c, r, blk); else coo.add(r, c, blk);
+        }
+}
+
 }  // namespace
 
 extern "C" {
@@ -486,6 +595,10 @@ void or_friction_ground(const double* x, const double* x0, double lastH, double 
 }
 
 void or_make_pd(int n, double* A) { make_pd(n, A); }
+void or_tri_bw(const double* X, const double* Dinv, double area, double kst, double ksh, double srate, double dt2,
+               double* energy, double* grad, double* H9) {
+    tri_bw(X, Dinv, area, kst, ksh, srate, dt2, energy, grad, H9);
+}
 
 // Geometry of a barrier pair: f = d / sqrt(dhat) and its gradient over the pair's
 // vertices (the last column of the reference's pFpx_* Jacobians), and for mollified
@@ -540,6 +653,15 @@ typedef struct OrScene {
     const int32_t* soft_idx;
     const double* soft_target;
     double dt, dhat, kappa, fdhat, mu, mu_gd, ground_offset, motion_rate, soft_rate;
+    // cloth: triangles (membrane) and hinges (quadratic bending)
+    int nf, nh;
+    const int32_t* tris;     // [nf*3]
+    const double* tdminv;    // [nf*4] row-major 2x2
+    const double* tarea;     // area * thickness
+    const int32_t* hinges;   // [nh*2]
+    const int32_t* hadj;     // [nh*2], -1 = boundary
+    const double* hq;        // [nh*16] column-major
+    double stretch, shear, strain_rate, bend;
 } OrScene;
 
 // Assemble gradient b (Dirichlet rows zeroed) and the merged upper BCOO.  Returns the
@@ -659,6 +781,34 @@ int or_assemble(const OrScene* s, double* b, int cap, int32_t* rows, int32_t* co
                         }
                     if (tr) coo.add(c, r, blk); else coo.add(r, c, blk);
                 }
+        }
+        // cloth membrane: 6 upper blocks per triangle; quadratic bending: 10 per hinge
+#pragma omp for schedule(static)
+        for (int f = 0; f < s->nf; f++) {
+            const int32_t* tv = s->tris + 3 * f;
+            double X[9], H9[81];
+            for (int a = 0; a < 3; a++)
+                for (int k = 0; k < 3; k++) X[3 * a + k] = s->x[3 * tv[a] + k];
+            tri_bw(X, s->tdminv + 4 * f, s->tarea[f], s->stretch, s->shear, s->strain_rate, dt2, &e, gr, H9);
+            en += e;
+            for (int a = 0; a < 3; a++)
+                for (int k = 0; k < 3; k++) g[3 * tv[a] + k] += gr[3 * a + k];
+            push_elem_blocks(coo, 3, tv, H9, s->btype);
+        }
+#pragma omp for schedule(static)
+        for (int h = 0; h < s->nh; h++) {
+            const int32_t hv[4] = {s->hinges[2 * h], s->hinges[2 * h + 1], s->hadj[2 * h], s->hadj[2 * h + 1]};
+            if (hv[2] < 0 || hv[3] < 0) continue;  // boundary edge: no bending term
+            double X[12], R0[3];
+            for (int a = 0; a < 4; a++)
+                for (int k = 0; k < 3; k++) X[3 * a + k] = s->x[3 * hv[a] + k];
+            for (int k = 0; k < 3; k++) R0[k] = s->rest[3 * hv[0] + k] - s->rest[3 * hv[1] + k];
+            double c = std::sqrt(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]) * s->bend * dt2;
+            hinge_quad(X, s->hq + 16 * h, c, &e, gr, H);
+            en += e;
+            for (int a = 0; a < 4; a++)
+                for (int k = 0; k < 3; k++) g[3 * hv[a] + k] += gr[3 * a + k];
+            push_elem_blocks(coo, 4, hv, H, s->btype);
         }
     }
     for (int t = 0; t < nth; t++) {

@@ -164,6 +164,178 @@ __global__ void __launch_bounds__(128) k_snk(int nt, const uint32_t* __restrict_
 }
 
 // ------------------------------------------------------------------------------------------
+// cloth membrane: Baraff-Witkin stretch + shear (femEnergy.cu:351-403 stress, 535-707 the
+// two projected Hessians, 2146-2215 the element kernel).  F = Ds Dm^-1 (3x2), columns
+// f0, f1.  Energy density k_st (S(|f0|) + S(|f1|)) + k_sh (f0.f1)^2 with
+// S(t) = (t-1)^2 + [t > 1] s (t-1)^3, times area*thickness*dt^2.  The reference projects
+// the stretch and the shear Hessian separately and sums them; both projections have closed
+// forms used here:
+//   stretch, per column (n = f/t):  [t > 1] S'(t)/t (I - n n^T) + c n n^T, with
+//     c = S''(t) for t > 1 and 2 otherwise (the negative transverse part clamped);
+//   shear, E = I6^2 with I6 = f0.f1, g = [f1; f0], a = [f0; f1], swap S = [[0,I],[I,0]]:
+//     the exact Hessian 2(g g^T + I6 S) has, in span{a, g}, the eigenpair
+//     2 lambda0 with q ~ I6 a + lambda0 g, lambda0 = (I2 + sqrt(I2^2 + 12 I6^2)) / 2, and in
+//     the complement +-2|I6| on the eigenspaces of S; the projection keeps
+//     2 lambda0 q q^T + |I6| [[Pw, sg Pw], [sg Pw, Pw]], sg = sign(I6) (+1 at 0),
+//     Pw = I - w w^T / |w|^2, w = f0 + sg f1 (the part of the sg-eigenspace outside span{a,g}).
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_tri_bw(int nf, const uint32_t* __restrict__ tris, const double* __restrict__ x,
+                                                const double* __restrict__ dminv, const double* __restrict__ area,
+                                                double kst, double ksh, double srate, double dt2, int eoff, int goff,
+                                                double* __restrict__ eblk, double* __restrict__ egrad) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    int vid[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) vid[a] = (int)tris[3 * f + a];
+    const d3 x0 = ld3(x, vid[0]), e1 = ld3(x, vid[1]) - x0, e2 = ld3(x, vid[2]) - x0;
+    const double* Di = dminv + 4 * (size_t)f;  // row-major 2x2
+    const d3 col[2] = {Di[0] * e1 + Di[2] * e2, Di[1] * e1 + Di[3] * e2};
+    // dF(:,j)/dx_a = D[a][j] I
+    const double D[3][2] = {{-(Di[0] + Di[2]), -(Di[1] + Di[3])}, {Di[0], Di[1]}, {Di[2], Di[3]}};
+    const double scale = area[f] * dt2;
+
+    // stress P (columns) and the 6x6 projected Hessian as 3x3 blocks Hq[j][k]
+    d3 P[2];
+    double Hq[2][2][3][3];
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int p = 0; p < 3; p++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) Hq[j][k][p][q] = 0.0;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const d3 fj = col[j];
+        const double t = sqrt(sq(fj));
+        const double u = t - 1.0;
+        const double dS = 2.0 * u + (t > 1.0 ? 3.0 * srate * u * u : 0.0);
+        P[j] = (kst * dS / t) * fj;
+        const double ct = t > 1.0 ? dS / t : 0.0;                    // transverse (clamped)
+        const double cn = t > 1.0 ? 2.0 + 6.0 * srate * u : 2.0;     // along n
+        const double n[3] = {fj.x / t, fj.y / t, fj.z / t};
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                Hq[j][j][p][q] += kst * ((p == q ? ct : 0.0) + (cn - ct) * n[p] * n[q]);
+    }
+    {
+        const d3 f0 = col[0], f1 = col[1];
+        const double I6 = dot(f0, f1), I2 = sq(f0) + sq(f1);
+        P[0] = P[0] + (2.0 * ksh * I6) * f1;
+        P[1] = P[1] + (2.0 * ksh * I6) * f0;
+        const double lam0 = 0.5 * (I2 + sqrt(I2 * I2 + 12.0 * I6 * I6));
+        const d3 qa = I6 * f0 + lam0 * f1, qb = I6 * f1 + lam0 * f0;  // q = [qa; qb] unnormalised
+        const double qn = sq(qa) + sq(qb);
+        const double iq = qn > 0.0 ? 1.0 / qn : 0.0;
+        const double sg = I6 >= 0.0 ? 1.0 : -1.0;
+        const d3 w = f0 + sg * f1;
+        const double ww = sq(w);
+        const double iw = ww > 0.0 ? 1.0 / ww : 0.0;
+        const double q0[2][3] = {{qa.x, qa.y, qa.z}, {qb.x, qb.y, qb.z}};
+        const double wv[3] = {w.x, w.y, w.z};
+        const double aI6 = fabs(I6);
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const double s = j == k ? 1.0 : sg;
+#pragma unroll
+                for (int p = 0; p < 3; p++)
+#pragma unroll
+                    for (int q = 0; q < 3; q++) {
+                        const double Pw = (p == q ? 1.0 : 0.0) - wv[p] * wv[q] * iw;
+                        Hq[j][k][p][q] += ksh * (2.0 * lam0 * q0[j][p] * q0[k][q] * iq + aI6 * s * Pw);
+                    }
+            }
+    }
+    // gradient rows and the 6 oriented upper blocks
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const d3 g = scale * (D[a][0] * P[0] + D[a][1] * P[1]);
+        double* o = egrad + 3 * ((size_t)goff + 3 * (size_t)f + a);
+        o[0] = g.x;
+        o[1] = g.y;
+        o[2] = g.z;
+    }
+    const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const int a = pa[k], b = pb[k];
+        const bool tr = vid[a] > vid[b];
+        double* o = eblk + 9 * ((size_t)eoff + 6 * (size_t)f + k);
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                double h = 0.0;
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int l = 0; l < 2; l++) h += D[a][j] * D[b][l] * Hq[j][l][p][q];
+                o[tr ? (3 * q + p) : (3 * p + q)] = scale * h;
+            }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// quadratic bending (femEnergy.cu:2623-2753; Q from the rest shape, :2492-2618): per
+// interior edge with vertices [e0, e1, opposite of triangle 1, opposite of triangle 2],
+// E = 1/2 c x^T (Q (x) I3) x, c = |rest e0 - rest e1| * bendStiff * dt^2: gradient c Q x,
+// constant Hessian c Q (x) I3.  Boundary edges (no second triangle) contribute nothing.
+// ------------------------------------------------------------------------------------------
+__global__ void k_hinge_quad(int nh, const uint32_t* __restrict__ edges, const int32_t* __restrict__ adj,
+                             const double* __restrict__ x, const double* __restrict__ rest,
+                             const double* __restrict__ Qcm, double kb_dt2, int eoff, int goff,
+                             double* __restrict__ eblk, double* __restrict__ egrad) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    const int v[4] = {(int)edges[2 * h], (int)edges[2 * h + 1], adj[2 * h], adj[2 * h + 1]};
+    const bool boundary = v[2] < 0 || v[3] < 0;
+    double Q[4][4];
+    double c = 0.0;
+    if (!boundary) {
+        c = sqrt(sq(ld3(rest, v[0]) - ld3(rest, v[1]))) * kb_dt2;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) Q[i][j] = Qcm[16 * (size_t)h + 4 * j + i];  // column-major
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) Q[i][j] = 0.0;
+    }
+    d3 xv[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) xv[a] = boundary ? mk(0, 0, 0) : ld3(x, v[a]);
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        d3 g = mk(0, 0, 0);
+#pragma unroll
+        for (int b = 0; b < 4; b++) g = g + (c * Q[a][b]) * xv[b];
+        double* o = egrad + 3 * ((size_t)goff + 4 * (size_t)h + a);
+        o[0] = g.x;
+        o[1] = g.y;
+        o[2] = g.z;
+    }
+    const int pa[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3}, pb[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+        // block (a, b) is c Q(a,b) I3; stored as the (min, max) block, i.e. from Q(b,a) when
+        // the element's vertex order is reversed
+        const bool tr = v[pa[k]] > v[pb[k]];
+        const double d = c * (tr ? Q[pb[k]][pa[k]] : Q[pa[k]][pb[k]]);
+        double* o = eblk + 9 * ((size_t)eoff + 10 * (size_t)h + k);
+#pragma unroll
+        for (int q = 0; q < 9; q++) o[q] = (q % 4 == 0) ? d : 0.0;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // static gathers
 // ------------------------------------------------------------------------------------------
 struct StaticOut {
@@ -686,6 +858,8 @@ static SgipcStatus check_inputs(SgipcCtx* c, const SgipcFemData* f, const SgipcC
     if (!c || !f || !p) return SGIPC_BAD_INPUT;
     if (!f->vertexes || !f->xTilta || !f->masses || !f->BoundaryType) return SGIPC_BAD_INPUT;
     if (c->nt && (!f->DmInverses || !f->volum || !f->lengthRate || !f->volumeRate)) return SGIPC_BAD_INPUT;
+    if (c->nf && (!f->triDmInverses || !f->area)) return SGIPC_BAD_INPUT;
+    if (c->nh && (!f->quad_bending_Q || !f->rest_vertexes)) return SGIPC_BAD_INPUT;
     if (c->nsoft && !f->targetVert) return SGIPC_BAD_INPUT;
     if (!(p->dt > 0.0) || !(p->dHat > 0.0) || !(p->kappa >= 0.0)) return SGIPC_BAD_INPUT;
     if (k) {
@@ -776,10 +950,25 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
 }
 
 static SgipcStatus launch_fem(SgipcCtx* c, const SgipcFemData* f, const SgipcParams* p, cudaStream_t s) {
+    const double dt2 = p->dt * p->dt;
     if (c->nt > 0) {
         SG_COUNT(c, 1);
         k_snk<<<nblk(c->nt, 128), 128, 0, s>>>(c->nt, c->tets, f->vertexes, f->DmInverses, f->volum, f->lengthRate,
-                                               f->volumeRate, p->dt * p->dt, c->eblk, c->egrad);
+                                               f->volumeRate, dt2, c->eblk, c->egrad);
+    }
+    // element block / gradient row offsets: tets (10 / 4 each), triangles (6 / 3), hinges (10 / 4)
+    if (c->nf > 0) {
+        SG_COUNT(c, 1);
+        k_tri_bw<<<nblk(c->nf, 128), 128, 0, s>>>(c->nf, c->tris, f->vertexes, f->triDmInverses, f->area,
+                                                  p->stretchStiff, p->shearStiff, p->strainRate, dt2, 10 * c->nt,
+                                                  4 * c->nt, c->eblk, c->egrad);
+    }
+    if (c->nh > 0) {
+        SG_COUNT(c, 1);
+        k_hinge_quad<<<nblk(c->nh), SGIPC_BLOCK, 0, s>>>(c->nh, c->hinges, c->hinge_adj, f->vertexes, f->rest_vertexes,
+                                                         f->quad_bending_Q, p->bendStiff * dt2,
+                                                         10 * c->nt + 6 * c->nf, 4 * c->nt + 3 * c->nf, c->eblk,
+                                                         c->egrad);
     }
     SG_LAUNCH_CHECK(c, "fem element kernels");
     return SGIPC_OK;

@@ -184,6 +184,103 @@ def tet_rest_data(verts: np.ndarray, tets: np.ndarray):
     return dm_inv, vol
 
 
+def cloth_grid(n: int, size: float, origin=(0.0, 0.0, 0.0)):
+    """n x n vertex grid over a size x size square in the x-z plane at height origin[1];
+    2 (n-1)^2 triangles with alternating diagonals, normals along +y."""
+    g = np.linspace(0.0, size, n)
+    ii, kk = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    verts = np.stack([g[ii.ravel()], np.zeros(n * n), g[kk.ravel()]], 1) + np.asarray(origin, np.float64)
+    c = np.arange(n - 1)
+    ci, ck = np.meshgrid(c, c, indexing="ij")
+    ci, ck = ci.ravel(), ck.ravel()
+    v00, v10, v01, v11 = ci * n + ck, (ci + 1) * n + ck, ci * n + ck + 1, (ci + 1) * n + ck + 1
+    even = ((ci + ck) % 2) == 0
+    t1 = np.where(even[:, None], np.stack([v00, v01, v11], 1), np.stack([v00, v01, v10], 1))
+    t2 = np.where(even[:, None], np.stack([v00, v11, v10], 1), np.stack([v01, v11, v10], 1))
+    return verts, np.concatenate([t1, t2], 0).astype(np.int32)
+
+
+def tri_rest_data(verts: np.ndarray, tris: np.ndarray, thickness: float):
+    """triDmInverses (row-major 2x2) and area*thickness (StiffGIPC/gl_main.cu:619-640).
+
+    As the reference's rest frame (femEnergy.cu:256-300), each triangle is rotated so that
+    its unit normal n goes to +z (Rodrigues: R = I + [v]x + [v]x^2 / (1 + n.z), v = n x z;
+    a half-turn about z when n = -z) and Dm = [u1 - u0, u2 - u0] of the rotated x, y."""
+    x = verts[tris]
+    e1, e2 = x[:, 1] - x[:, 0], x[:, 2] - x[:, 0]
+    nrm = np.cross(e1, e2)
+    area2 = np.linalg.norm(nrm, axis=1)
+    n = nrm / area2[:, None]
+    z = np.array([0.0, 0.0, 1.0])
+    v = np.cross(n, z)
+    c = n @ z
+    K = np.zeros((len(tris), 3, 3))
+    K[:, 0, 1], K[:, 0, 2], K[:, 1, 0] = -v[:, 2], v[:, 1], v[:, 2]
+    K[:, 1, 2], K[:, 2, 0], K[:, 2, 1] = -v[:, 0], -v[:, 1], v[:, 0]
+    anti = c + 1.0 == 0.0
+    denom = np.where(anti, 1.0, 1.0 + c)
+    R = np.eye(3)[None] + K + np.einsum("fij,fjk->fik", K, K) / denom[:, None, None]
+    R[anti] = np.diag([-1.0, -1.0, 1.0])
+    uv = np.einsum("fij,fvj->fvi", R, x)[:, :, :2]
+    dm = np.stack([uv[:, 1] - uv[:, 0], uv[:, 2] - uv[:, 0]], 2)  # columns u0, u1
+    return np.linalg.inv(dm), 0.5 * area2 * thickness
+
+
+def hinge_topology(tris: np.ndarray):
+    """tri_edges and tri_edge_adj_vertex: every mesh edge with the vertex opposite it in
+    its first and second triangle (-1 for a boundary edge)."""
+    e = np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [2, 0]]], 0)
+    opp = np.concatenate([tris[:, 2], tris[:, 0], tris[:, 1]], 0)
+    key = np.sort(e, 1)
+    order = np.lexsort((np.arange(len(key)), key[:, 1], key[:, 0]))
+    key, e, opp = key[order], e[order], opp[order]
+    uniq, first, cnt = np.unique(key, axis=0, return_index=True, return_counts=True)
+    edges = e[first]
+    adj = np.full((len(uniq), 2), -1, np.int64)
+    adj[:, 0] = opp[first]
+    two = cnt == 2
+    adj[two, 1] = opp[first[two] + 1]
+    return edges.astype(np.int32), adj.astype(np.int32)
+
+
+def quad_bending_q(rest: np.ndarray, edges: np.ndarray, adj: np.ndarray):
+    """Constant 4x4 bending matrices of the quadratic bending model (Bergou et al., "A
+    quadratic bending model for inextensible surfaces", 2006), as the reference's
+    PrepareQuadBendingQ (StiffGIPC/femEnergy.cu:2492-2618) computes them: for hinge
+    vertices [e0, e1, opposite 1, opposite 2], K = (c03 + c04, c01 + c02, -c01 - c03,
+    -c02 - c04) with the cotangents of the angles at e0 and e1, Q = 3 / (A1 + A2) K K^T;
+    boundary and degenerate hinges get Q = 0."""
+    Q = np.zeros((len(edges), 4, 4))
+    inner = adj[:, 1] >= 0
+    if not inner.any():
+        return Q
+    v0, v1 = rest[edges[inner, 0]], rest[edges[inner, 1]]
+    v2, v3 = rest[adj[inner, 0]], rest[adj[inner, 1]]
+    e0, e1, e2, e3, e4 = v1 - v0, v2 - v0, v3 - v0, v2 - v1, v3 - v1
+
+    def cot(a, b):
+        cn = np.linalg.norm(np.cross(a, b), axis=1)
+        return np.where(cn < 1e-12, 0.0, (a * b).sum(1) / np.where(cn < 1e-12, 1.0, cn))
+
+    n01 = np.linalg.norm(np.cross(e0, e1), axis=1)
+    n02 = np.linalg.norm(np.cross(e0, e2), axis=1)
+    c01, c02, c03, c04 = cot(e0, e1), cot(e0, e2), cot(-e0, e3), cot(-e0, e4)
+    K = np.stack([c03 + c04, c01 + c02, -c01 - c03, -c02 - c04], 1)
+    asum = 0.5 * (n01 + n02)
+    ok = (n01 >= 1e-12) & (n02 >= 1e-12) & (asum >= 1e-12)
+    q = 3.0 / np.where(ok, asum, 1.0)[:, None, None] * K[:, :, None] * K[:, None, :]
+    q[~ok] = 0.0
+    q[~np.isfinite(q).all((1, 2))] = 0.0
+    Q[inner] = q
+    return Q
+
+
+def cloth_stiffness(E: float, nu: float, strain_rate: float, bend_E: float, thickness: float):
+    """(stretchStiff, shearStiff, bendStiff) of StiffGIPC/gl_main.cu:578-583."""
+    stretch = E / (2.0 * (1.0 + nu))
+    return stretch, 0.03 * stretch * strain_rate, bend_E * thickness ** 3 / (24.0 * (1.0 - nu * nu))
+
+
 def snk_rates(E, nu):
     """(lengthRate, volumeRate) of the stable Neo-Hookean model, StiffGIPC/gl_main.cu:609-617."""
     E = np.asarray(E, np.float64)
@@ -292,29 +389,36 @@ def _empty_cloth():
 
 def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, density: float,
                     nu: float, mu_friction: float, seed: int, perturb: float,
-                    kappa: Optional[float] = None) -> Scene:
-    """Concatenate tet bodies, derive ``initFEM`` data and set up one Newton iterate.
+                    kappa: Optional[float] = None, cloth: Optional[dict] = None) -> Scene:
+    """Concatenate tet and cloth bodies, derive ``initFEM`` data and set up one Newton iterate.
 
-    Each body dict holds ``verts``, ``tets``, ``E`` and optional ``velocity`` (3,) and
-    ``boundary`` flag.  Vertex positions of the current iterate are the rest lattice plus
-    a seeded uniform perturbation of ``perturb`` metres.
+    Each body dict holds ``verts`` and either ``tets`` with ``E`` (a soft solid) or
+    ``tris`` (a cloth sheet), plus optional ``velocity`` (3,) and ``boundary`` flag.
+    ``cloth`` gives the sheet material: ``thickness``, ``E``, ``bend_E``, ``density``,
+    ``strain_rate`` (StiffGIPC/gl_main.cu:578-583, 619-640).  Vertex positions of the
+    current iterate are the rest shape plus a seeded uniform perturbation of ``perturb``
+    metres.
     """
     rng = np.random.default_rng(seed)
-    verts, tets, youngs, vel, btype, body_id = [], [], [], [], [], []
+    verts, tets, tris, youngs, vel, btype, body_id = [], [], [], [], [], [], []
     off = 0
     for b, body in enumerate(bodies):
         v = np.asarray(body["verts"], np.float64)
-        t = np.asarray(body["tets"], np.int64) + off
         verts.append(v)
-        tets.append(t)
-        youngs.append(np.full(len(t), float(body["E"])))
+        if "tets" in body:
+            t = np.asarray(body["tets"], np.int64) + off
+            tets.append(t)
+            youngs.append(np.full(len(t), float(body["E"])))
+        else:
+            tris.append(np.asarray(body["tris"], np.int64) + off)
         vel.append(np.tile(np.asarray(body.get("velocity", (0.0, 0.0, 0.0)), np.float64), (len(v), 1)))
         btype.append(np.full(len(v), int(body.get("boundary", 0)), np.int32))
         body_id.append(np.full(len(v), b, np.int32))
         off += len(v)
     rest = np.concatenate(verts)
-    tets = np.concatenate(tets).astype(np.int32)
-    youngs = np.concatenate(youngs)
+    tets = np.concatenate(tets).astype(np.int32) if tets else np.zeros((0, 4), np.int32)
+    tris = np.concatenate(tris).astype(np.int64) if tris else np.zeros((0, 3), np.int64)
+    youngs = np.concatenate(youngs) if youngs else np.zeros(0)
     vel = np.concatenate(vel)
     btype = np.concatenate(btype)
     body_id = np.concatenate(body_id)
@@ -329,19 +433,36 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
     inv[perm] = np.arange(nv)
     rest, vel, btype, body_id = rest[perm], vel[perm], btype[perm], body_id[perm]
     tets = inv[tets].astype(np.int32)
+    tris = inv[tris].astype(np.int32)
 
-    dm_inv, vol = tet_rest_data(rest, tets)
+    dm_inv, vol = tet_rest_data(rest, tets) if len(tets) else (np.zeros((0, 3, 3)), np.zeros(0))
     lr, vr = snk_rates(youngs, nu)
     masses = np.zeros(nv)
     np.add.at(masses, tets.ravel(), np.repeat(vol * density / 4.0, 4))
+    cl = _empty_cloth()
+    stretch = shear = bend = srate = 0.0
+    if len(tris):
+        cloth = dict(dict(thickness=1e-3, E=1e6, bend_E=1e5, density=200.0, strain_rate=100.0), **(cloth or {}))
+        tdm, tarea = tri_rest_data(rest, tris, cloth["thickness"])
+        np.add.at(masses, tris.ravel(), np.repeat(tarea * cloth["density"] / 3.0, 3))
+        hin, hadj = hinge_topology(tris)
+        cl = dict(tris=tris, tri_dm_inv=tdm, area=tarea, hinges=hin, hinge_adj=hadj,
+                  hinge_q=quad_bending_q(rest, hin, hadj))
+        srate = cloth["strain_rate"]
+        stretch, shear, bend = cloth_stiffness(cloth["E"], nu, srate, cloth["bend_E"], cloth["thickness"])
 
     x_prev = rest + rng.uniform(-perturb, perturb, rest.shape)
     x = x_prev.copy()
     g = np.asarray(GRAVITY)
     xt = x_prev + dt * vel + np.where(btype[:, None] == 0, dt * dt * g[None, :], 0.0)
 
-    stris, sedges, sverts = tet_surface(tets)
-    nbr_start, nbr_list = neighbour_csr(nv, tets, np.zeros((0, 3), np.int32))
+    stris, sedges, sverts = tet_surface(tets) if len(tets) else (np.zeros((0, 3), np.int32),
+                                                                 np.zeros((0, 2), np.int32), np.zeros(0, np.int32))
+    if len(tris):  # cloth sheets collide on both sides with every triangle, edge and vertex
+        stris = np.concatenate([stris, tris]).astype(np.int32)
+        sedges = np.unique(np.concatenate([sedges, tri_mesh_edges(tris)]), axis=0).astype(np.int32)
+        sverts = np.unique(np.concatenate([sverts, tris.ravel()])).astype(np.int32)
+    nbr_start, nbr_list = neighbour_csr(nv, tets, tris)
     part_map, real_map = ordered_partition(body_id)
 
     lo = np.minimum(rest.min(0), x.min(0))
@@ -353,14 +474,14 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
         kappa = suggest_kappa(bbox2, dhat, mean_mass)
     params = dict(dt=dt, dHat=dhat, kappa=float(kappa), fDhat=1e-4 * bbox2, bboxDiag2=bbox2,
                   frictionRate=mu_friction, gd_frictionRate=mu_friction, ground_offset=GROUND_OFFSET,
-                  stretchStiff=0.0, shearStiff=0.0, strainRate=0.0, bendStiff=0.0,
+                  stretchStiff=stretch, shearStiff=shear, strainRate=srate, bendStiff=bend,
                   motionRate=0.0, softRate=0.0, density=density, meanMass=mean_mass)
     return Scene(name=name, vertexes=x, o_vertexes=x_prev.copy(), rest_vertexes=rest,
                  xTilta=xt, velocities=vel, masses=masses, boundary_type=btype, tets=tets,
                  dm_inv=dm_inv, volum=vol, length_rate=lr, volume_rate=vr, youngs=youngs,
                  poisson=nu, surf_tris=stris, surf_edges=sedges, surf_verts=sverts,
                  body_of_vertex=body_id, part_map_real=part_map, real_map_part=real_map,
-                 nbr_start=nbr_start, nbr_list=nbr_list, params=params, **_empty_cloth())
+                 nbr_start=nbr_start, nbr_list=nbr_list, params=params, **cl)
 
 
 def scene_cube(n: int = 11, touching: bool = False, seed: int = 0) -> Scene:
@@ -401,7 +522,28 @@ def scene_two_cubes(n: int = 21, seed: int = 1, friction: float = 0.2) -> Scene:
     return sc
 
 
+def scene_cloth_on_cube(n_cloth: int = 24, n_cube: int = 6, seed: int = 2, friction: float = 0.4) -> Scene:
+    """A cloth sheet (n_cloth^2 grid, 0.2 m square, 1 mm thick, E 1e6, strain rate 100,
+    the reference's cloth settings StiffGIPC/gl_main.cu:650-667) lying 0.5 d-hat above
+    a soft 0.1 m cube (n_cube^3 lattice) that rests 0.5 d-hat above the ground, the sheet
+    overhanging on every side.  Exercises the membrane, quadratic bending, cloth-solid
+    barrier and friction terms together (a small stand-in for the cloth-over-sphere scene).
+    """
+    dhat_abs = 1e-3
+    gap = 0.5 * dhat_abs
+    v0, t0 = lattice_tets(n_cube, 0.1, (0.05, GROUND_OFFSET + gap, 0.05))
+    vc, tc = cloth_grid(n_cloth, 0.2, (0.0, GROUND_OFFSET + 2 * gap + 0.1, 0.0))
+    sc = build_tet_scene("cloth%d_cube%d" % (n_cloth, n_cube),
+                         [dict(verts=v0, tets=t0, E=1e5), dict(verts=vc, tris=tc)],
+                         dt=0.01, dhat_abs=dhat_abs, density=1000.0, nu=0.49, mu_friction=friction,
+                         seed=seed, perturb=1e-5)
+    from . import contacts
+    contacts.attach_contacts(sc)
+    return sc
+
+
 SCENES = {
     "cube": scene_cube,
     "two_cubes": scene_two_cubes,
+    "cloth_on_cube": scene_cloth_on_cube,
 }

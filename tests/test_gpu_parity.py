@@ -23,12 +23,14 @@ from sgipc import scenes, system  # noqa: E402
 from sgipc import _native as N  # noqa: E402
 
 
-@pytest.fixture(scope="module", params=["cube_touch", "two_cubes"])
+@pytest.fixture(scope="module", params=["cube_touch", "two_cubes", "cloth_on_cube"])
 def case(request):
     if request.param == "cube_touch":
         sc = scenes.scene_cube(6, touching=True, seed=3)
-    else:
+    elif request.param == "two_cubes":
         sc = scenes.scene_two_cubes(7, seed=5)
+    else:
+        sc = scenes.scene_cloth_on_cube(10, 5, seed=6)
     g = system.GIPC(sc)
     g.computeGradientAndHessian()
     torch.cuda.synchronize()

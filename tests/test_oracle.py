@@ -274,3 +274,91 @@ def test_contact_generator_encoding(small_two_cubes):
     for enc in p[:200]:
         nv, f, *_ = oracle.pair_geom(enc, sc.vertexes, sc.params["dHat"])
         assert 0.0 < f < 1.0
+
+
+# ------------------------------------------------------------------------------------------
+# cloth: Baraff-Witkin membrane and quadratic bending
+# ------------------------------------------------------------------------------------------
+def _cloth_tri():
+    v, t = scenes.cloth_grid(3, 0.1)
+    dm, area = scenes.tri_rest_data(v, t, 1e-3)
+    return v[t[0]], dm[0], area[0]
+
+
+def _bw_fd_grad(X, dm, area, k, h=1e-7):
+    g = np.zeros(9)
+    for i in range(9):
+        d = np.zeros(9)
+        d[i] = h
+        g[i] = (oracle.tri_bw(X.ravel() + d, dm, area, *k)[0] - oracle.tri_bw(X.ravel() - d, dm, area, *k)[0]) / (2 * h)
+    return g
+
+
+@pytest.mark.parametrize("scale", [0.9, 1.0, 1.15])
+def test_cloth_membrane_gradient_is_energy_derivative(scale):
+    X0, dm, area = _cloth_tri()
+    rng = np.random.default_rng(int(scale * 100))
+    k = (3.3e5, 1.0e6, 100.0, 1e-4)
+    for _ in range(3):
+        X = X0 * scale + rng.normal(scale=3e-3, size=(3, 3))
+        e, g, H = oracle.tri_bw(X, dm, area, *k)
+        assert np.allclose(g, _bw_fd_grad(X, dm, area, k), rtol=1e-5, atol=1e-6 * np.abs(g).max())
+        assert np.allclose(H, H.T) and np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()
+
+
+def test_cloth_membrane_rest_state_and_exact_hessian_under_pure_stretch():
+    X0, dm, area = _cloth_tri()
+    k = (3.3e5, 1.0e6, 100.0, 1e-4)
+    e, g, H = oracle.tri_bw(X0, dm, area, *k)
+    assert e == pytest.approx(0.0, abs=1e-18) and np.abs(g).max() < 1e-12
+    # stretch both material directions (|f0|, |f1| > 1, f0 . f1 = 0): every term is convex
+    # there, so the projected Hessian equals the exact one (finite differences of the gradient)
+    Dm = np.linalg.inv(dm)
+    F = np.array([[1.1, 0.0], [0.0, 1.2], [0.0, 0.0]])
+    Ds = F @ Dm
+    X = np.stack([np.zeros(3), Ds[:, 0], Ds[:, 1]])
+    e, g, H = oracle.tri_bw(X, dm, area, *k)
+    h = 1e-7
+    Hfd = np.zeros((9, 9))
+    for i in range(9):
+        d = np.zeros(9)
+        d[i] = h
+        Hfd[:, i] = (oracle.tri_bw(X.ravel() + d, dm, area, *k)[1] - oracle.tri_bw(X.ravel() - d, dm, area, *k)[1]) / (2 * h)
+    assert np.allclose(H, Hfd, rtol=1e-5, atol=1e-6 * np.abs(H).max())
+
+
+def test_quadratic_bending_matrix_properties():
+    v, t = scenes.cloth_grid(5, 0.2)
+    e, adj = scenes.hinge_topology(t)
+    Q = scenes.quad_bending_q(v, e, adj)
+    inner = adj[:, 1] >= 0
+    assert inner.sum() > 0 and np.abs(Q[~inner]).max() == 0.0
+    # symmetric, rank one, annihilates rigid translations and the flat rest shape
+    assert np.allclose(Q, np.transpose(Q, (0, 2, 1)))
+    assert np.allclose(Q[inner].sum(2), 0.0, atol=1e-9 * np.abs(Q).max())
+    X = np.stack([v[e[inner, 0]], v[e[inner, 1]], v[adj[inner, 0]], v[adj[inner, 1]]], 1)
+    assert np.abs(np.einsum("hij,hjk->hik", Q[inner], X)).max() < 1e-9 * np.abs(Q).max()
+
+
+@pytest.fixture(scope="module")
+def small_cloth():
+    return scenes.scene_cloth_on_cube(8, 4, seed=4)
+
+
+def test_cloth_scene_gradient_is_total_energy_derivative(small_cloth):
+    sc = small_cloth
+    assert len(sc.tris) and len(sc.hinges) and len(sc.pairs)
+    b, rows, cols, vals, e0 = oracle.assemble(sc)
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        d = rng.normal(size=3 * sc.nv) * 1e-8
+        ep = oracle.energy(sc, sc.vertexes + d.reshape(-1, 3))
+        em = oracle.energy(sc, sc.vertexes - d.reshape(-1, 3))
+        assert (ep - em) / 2 == pytest.approx(b @ d, rel=1e-4)
+
+
+def test_cloth_scene_matrix_symmetric_positive_definite(small_cloth):
+    sc = small_cloth
+    b, rows, cols, vals, _ = oracle.assemble(sc)
+    A = oracle.dense(rows, cols, vals, sc.nv)
+    assert np.allclose(A, A.T) and np.linalg.eigvalsh(A).min() > 0
