@@ -45,6 +45,7 @@ def lib():
         L.or_friction_pair.restype = C.c_int
         L.or_friction_ground.argtypes = [_d, _d, C.c_double, C.c_double, C.c_double, _d, _d, _d]
         L.or_make_pd.argtypes = [C.c_int, _d]
+        L.or_set_snk_projection.argtypes = [C.c_int]
         L.or_tri_bw.argtypes = [_d, _d, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _d, _d, _d]
         L.or_pair_geom.argtypes = [_i, _d, C.c_double, _d, _d, _d, _d]
         L.or_pair_geom.restype = C.c_int
@@ -133,6 +134,19 @@ def tri_bw(X, Dinv, area, kst, ksh, srate, dt2):
     e, g, H = np.zeros(1), np.zeros(9), np.zeros(81)
     lib().or_tri_bw(_p(X), _p(Dinv), area, kst, ksh, srate, dt2, _p(e), _p(g), _p(H))
     return e[0], g, H.reshape(9, 9)
+
+
+class exact_snk_hessian:
+    """Context manager: assemble the stable Neo-Hookean terms with their exact (unprojected)
+    Hessian, the true Jacobian of the gradient, instead of the PSD projection."""
+
+    def __enter__(self):
+        lib().or_set_snk_projection(0)
+        return self
+
+    def __exit__(self, *exc):
+        lib().or_set_snk_projection(1)
+        return False
 
 
 def make_pd(A):

@@ -124,6 +124,10 @@ void make_pd(int n, double* A) {
         }
 }
 
+// When 0, the SNK element Hessian is left unprojected (the exact second derivative), for
+// checks of derivatives that need the true Jacobian of the gradient.
+int g_project_snk = 1;
+
 // ---------------------------------------------------------------------------------------
 // stable Neo-Hookean tet (USE_SNK1)
 // ---------------------------------------------------------------------------------------
@@ -200,7 +204,7 @@ void snk_tet(const double* X /*4x3*/, const double* Dinv /*3x3 row-major*/, doub
                     H[(3 * j + a) * 9 + 3 * l + b] += lam * Jm * s;
                 }
         }
-    make_pd(9, H);
+    if (g_project_snk) make_pd(9, H);
     for (int r = 0; r < 12; r++)
         for (int c = 0; c < 12; c++) {
             double s = 0;
@@ -595,6 +599,7 @@ void or_friction_ground(const double* x, const double* x0, double lastH, double 
 }
 
 void or_make_pd(int n, double* A) { make_pd(n, A); }
+void or_set_snk_projection(int on) { g_project_snk = on; }
 void or_tri_bw(const double* X, const double* Dinv, double area, double kst, double ksh, double srate, double dt2,
                double* energy, double* grad, double* H9) {
     tri_bw(X, Dinv, area, kst, ksh, srate, dt2, energy, grad, H9);

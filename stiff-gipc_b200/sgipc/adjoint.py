@@ -47,3 +47,88 @@ def adjoint(g: GIPC, dLdx: torch.Tensor, precision: str = "fp64", tol: float = 1
     N.check(N.lib().sgipc_adjoint_param_grads(g.ctx, C.byref(f), C.byref(prm), float(g.scene.poisson), nrhs,
                                               _p(lam), _p(dLdE), _p(dLdv0), _stream()), g.ctx)
     return dLdE, dLdv0, lam, stats
+
+
+# ------------------------------------------------------------------------------------------
+# implicit step as a differentiable function
+# ------------------------------------------------------------------------------------------
+GRAVITY = (0.0, -9.8, 0.0)
+
+
+def set_parameters(g: GIPC, E: Optional[torch.Tensor] = None, v0: Optional[torch.Tensor] = None) -> None:
+    """Write per-tet Young's moduli E (T,) and initial velocities v0 (V,3) into the device
+    state: lengthRate / volumeRate of the stable Neo-Hookean model (StiffGIPC/gl_main.cu:
+    609-617) and the inertial target xTilta = x_prev + dt v0 (+ dt^2 g on free vertices,
+    StiffGIPC/GIPC.cu:8073-8097)."""
+    tet, nu = g.tet, float(g.scene.poisson)
+    if E is not None:
+        E = E.to(torch.float64).reshape(-1)
+        mu = E / (2.0 * (1.0 + nu))
+        lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+        tet.lengthRate.copy_(4.0 * mu / 3.0)
+        tet.volumeRate.copy_(lam + 5.0 * mu / 6.0)
+    if v0 is not None:
+        dt = float(g.params["dt"])
+        grav = torch.tensor(GRAVITY, dtype=torch.float64, device=tet.xTilta.device)
+        free = (tet.BoundaryType == 0).to(torch.float64)[:, None]
+        tet.xTilta.copy_(tet.o_vertexes + dt * v0.to(torch.float64).reshape(-1, 3) + dt * dt * free * grav[None])
+
+
+def newton_solve(g: GIPC, tol: float = 1e-11, max_newton: int = 30, precision: str = "fp64") -> torch.Tensor:
+    """Minimise the incremental potential for the current parameters with the contact set
+    held fixed: Newton steps x <- x - alpha dx with A dx = g(x) solved by the MAS-PCG, alpha
+    halved until ||g|| decreases.  Stops when ||g(x)|| <= tol * ||g(x_start)||, or when no
+    step length reduces ||g|| any more (round-off level), keeping the best iterate.
+    Returns x* (V,3), left in ``g.tet.vertexes``, with the system assembled at x*.
+
+    The reference's Newton loop (line search on energy, CCD, contact set updates,
+    GIPC.cu:10830-10976) is not part of this path; this driver exists so that the adjoint can
+    be checked against finite differences of a converged step."""
+    cfg = PCGSolverConfig(precision=precision, global_tol_rate=1e-13, criterion=N.CRIT_TRUE, max_iter_ratio=1.0)
+    x = g.tet.vertexes
+    g.computeGradientAndHessian()
+    r = g.rhs().norm().item()
+    r0 = max(r, 1e-300)
+    for _ in range(max_newton):
+        if r <= tol * r0:
+            break
+        g.calculateMovingDirection(cfg)
+        dx = g.moveDir.view(-1, 3).clone()
+        x_prev = x.clone()
+        alpha = 1.0
+        while True:
+            x.copy_(x_prev - alpha * dx)
+            g.computeGradientAndHessian()
+            rn = g.rhs().norm().item()
+            if rn < r or alpha < 1e-3:
+                break
+            alpha *= 0.5
+        if not rn < r:  # no decrease: x_prev is converged to round-off
+            x.copy_(x_prev)
+            g.computeGradientAndHessian()
+            break
+        r = rn
+    return x
+
+
+class ImplicitStep(torch.autograd.Function):
+    """x* = argmin_x E(x; E_t, v0) as a differentiable function of the per-tet Young's
+    moduli and the initial velocities.  Forward runs :func:`newton_solve`; backward solves
+    the adjoint system A lambda = dL/dx* with the same matrix and MAS-PCG and contracts it
+    with dg/dE_t and dg/dv0 (``sgipc_adjoint_param_grads``)."""
+
+    @staticmethod
+    def forward(ctx, E: torch.Tensor, v0: torch.Tensor, g: GIPC, tol: float = 1e-11):
+        set_parameters(g, E, v0)
+        x = newton_solve(g, tol=tol)
+        ctx.g = g
+        ctx.v0_shape = v0.shape
+        return x.clone()
+
+    @staticmethod
+    def backward(ctx, dLdx: torch.Tensor):
+        g = ctx.g
+        g.computeGradientAndHessian()  # A and dg/dtheta at x* (the state forward left)
+        dLdE, dLdv0, _, _ = adjoint(g, dLdx.reshape(1, -1).contiguous(), precision="fp64", tol=1e-12,
+                                    criterion=N.CRIT_TRUE)
+        return dLdE[0], dLdv0[0].reshape(ctx.v0_shape), None, None
