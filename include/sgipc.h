@@ -254,6 +254,60 @@ SgipcStatus sgipc_adjoint_param_grads(SgipcCtx* ctx, const SgipcFemData* fem,
                                       const double* lambda, double* dLdE, double* dLdv0,
                                       void* stream);
 
+/* ---- affine bodies (ABDSystem / ABDPreconditioner) ----------------------------------- */
+
+/* Static description of the affine bodies [host], what ABDSystem::init derives
+ * (StiffGIPC/abd_system/abd_system.cu:50-140).  Body b owns the block rows 4b..4b+3 of the
+ * global system (translation p, then the rows a1, a2, a3 of its affine matrix); FEM rows
+ * follow at 4 * body_num.  ABD points are numbered body by body (non-decreasing
+ * point_body), as the reference's unique points are. */
+typedef struct SgipcAbdTopology {
+    int32_t        body_num;
+    int32_t        point_num;           /* ABD points */
+    const int32_t* point_body;          /* int[point_num]  unique_point_id_to_body_id */
+    const double*  x_bar;               /* double3[point_num]  ABDJacobi::x_bar */
+    const double*  dyadic_mass;         /* double[13 * body_num]: m, m x_bar (3), m x_bar x_bar^T (9,
+                                         * row-major) -- ABDJacobiDyadicMass */
+    const double*  volume;              /* double[body_num] */
+    const int32_t* boundary_type;       /* int[body_num]: 0 free, 1 fixed (BodyBoundaryType) */
+    int32_t        max_abd_blocks;      /* capacity: ABD-ABD point blocks per call */
+    int32_t        max_fem_blocks;      /* capacity: ABD-FEM point blocks per call */
+} SgipcAbdTopology;
+
+typedef struct SgipcAbdCtx SgipcAbdCtx;
+
+SgipcStatus sgipc_abd_create(const SgipcAbdTopology* topo, int device, SgipcAbdCtx** out);
+SgipcStatus sgipc_abd_destroy(SgipcAbdCtx* ctx);
+const char* sgipc_abd_last_error(const SgipcAbdCtx* ctx);
+
+/* ABDSystem::setup_abd_system_gradient_hessian (setup_abd_system_gradient_and_hessian.cu:
+ * 162-181, 200-610): per body the kinetic term M (q - q_tilde) with the dyadic mass and the
+ * orthogonality potential kappa * volume * dt^2 * V_perp(q) (abd_energy.inl:9-127, its 9x9
+ * Hessian projected to PSD); point barrier gradients mapped to bodies with J^T
+ * (point_grad [dev double3[point_num]], may be null); point-space contact blocks mapped to
+ * body space: ABD-ABD blocks [dev] (rows, cols = ABD point ids, row <= col, row-major 3x3)
+ * to J_i^T H J_j, ABD-FEM blocks (rows = ABD point, cols = FEM-local vertex) to J_i^T H in
+ * column 4 * body_num + col (zeroed where fem_boundary [dev int per FEM vertex, may be
+ * null] is non-zero).  Fixed bodies: zero gradient, mass-only Hessian, zero contact
+ * blocks.  Writes body_grad [dev double[12 * body_num]] and keeps the merged upper
+ * body-space BCOO in the context. */
+SgipcStatus sgipc_abd_grad_hess(SgipcAbdCtx* ctx, const double* q, const double* q_tilde, double kappa,
+                                double dt, const double* point_grad, int32_t abd_blocks,
+                                const int32_t* abd_rows, const int32_t* abd_cols, const double* abd_vals,
+                                int32_t fem_blocks, const int32_t* fem_rows, const int32_t* fem_cols,
+                                const double* fem_vals, const int32_t* fem_boundary, double* body_grad,
+                                void* stream);
+/* Host copy of the merged upper body-space blocks of the last sgipc_abd_grad_hess (block
+ * rows < 4 * body_num; columns >= 4 * body_num are FEM rows).  Synchronises. */
+SgipcStatus sgipc_abd_export_bcoo(SgipcAbdCtx* ctx, int32_t cap, int32_t* rows, int32_t* cols,
+                                  double* vals, int32_t* count);
+/* ABDPreconditioner::assemble (abd_preconditioner.cu:15-38, _cal_abd_system_preconditioner
+ * setup_abd_system_gradient_and_hessian.cu:612-655): the inverse of every body's 12x12
+ * diagonal block of the assembled body-space matrix. */
+SgipcStatus sgipc_abd_precond_build(SgipcAbdCtx* ctx, void* stream);
+/* ABDPreconditioner::apply: z_b = P_b^-1 r_b, r and z [dev double[12 * body_num]]. */
+SgipcStatus sgipc_abd_precond_apply(SgipcAbdCtx* ctx, const double* r, double* z, void* stream);
+
 /* ---- instrumentation (the reference's gipc::Timer / cudaEvent phase timers,
  *      StiffGIPC/gipc/utils/timer.h:19-136, GIPC.cu:10854-10964) ----------------------- */
 

@@ -46,6 +46,9 @@ def lib():
         L.or_friction_ground.argtypes = [_d, _d, C.c_double, C.c_double, C.c_double, _d, _d, _d]
         L.or_make_pd.argtypes = [C.c_int, _d]
         L.or_set_snk_projection.argtypes = [C.c_int]
+        L.or_abd_assemble.argtypes = [C.c_int, C.c_int, _i, _d, _d, _d, _i, _d, _d, C.c_double, C.c_double, _d,
+                                      C.c_int, _i, _i, _d, C.c_int, _i, _i, _d, _i, _d, C.c_int, _i, _i, _d]
+        L.or_abd_assemble.restype = C.c_int
         L.or_tri_bw.argtypes = [_d, _d, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _d, _d, _d]
         L.or_pair_geom.argtypes = [_i, _d, C.c_double, _d, _d, _d, _d]
         L.or_pair_geom.restype = C.c_int
@@ -134,6 +137,29 @@ def tri_bw(X, Dinv, area, kst, ksh, srate, dt2):
     e, g, H = np.zeros(1), np.zeros(9), np.zeros(81)
     lib().or_tri_bw(_p(X), _p(Dinv), area, kst, ksh, srate, dt2, _p(e), _p(g), _p(H))
     return e[0], g, H.reshape(9, 9)
+
+
+def abd_assemble(bodies, q, q_tilde, kappa, dt, point_grad=None, abd_blocks=None, fem_blocks=None,
+                 fem_boundary=None):
+    """(body_grad (12B,), rows, cols, vals (n,3,3)): ABD body terms and contact mappings."""
+    B, P = len(bodies["volume"]), len(bodies["point_body"])
+    pb, xb = _i32(bodies["point_body"]), _f64(bodies["x_bar"]).reshape(-1)
+    dm, vol, bt = _f64(bodies["dyadic_mass"]).reshape(-1), _f64(bodies["volume"]), _i32(bodies["boundary_type"])
+    q, qt = _f64(q).reshape(-1), _f64(q_tilde).reshape(-1)
+    pg = None if point_grad is None else _f64(point_grad).reshape(-1)
+    ar, ac, av = (np.zeros(0, np.int32),) * 2 + (np.zeros(0),) if abd_blocks is None else \
+        (_i32(abd_blocks[0]), _i32(abd_blocks[1]), _f64(abd_blocks[2]).reshape(-1))
+    fr, fc, fv = (np.zeros(0, np.int32),) * 2 + (np.zeros(0),) if fem_blocks is None else \
+        (_i32(fem_blocks[0]), _i32(fem_blocks[1]), _f64(fem_blocks[2]).reshape(-1))
+    fb = None if fem_boundary is None else _i32(fem_boundary)
+    g = np.zeros(12 * B)
+    args = [B, P, _p(pb, _i), _p(xb), _p(dm), _p(vol), _p(bt, _i), _p(q), _p(qt), kappa, dt,
+            None if pg is None else _p(pg), len(ar), _p(ar, _i), _p(ac, _i), _p(av), len(fr), _p(fr, _i), _p(fc, _i),
+            _p(fv), None if fb is None else _p(fb, _i), _p(g)]
+    n = lib().or_abd_assemble(*args, 0, None, None, None)
+    rows, cols, vals = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros((n, 3, 3))
+    lib().or_abd_assemble(*args, n, _p(rows, _i), _p(cols, _i), _p(vals))
+    return g, rows, cols, vals
 
 
 class exact_snk_hessian:

@@ -571,6 +571,60 @@ void push_elem_blocks(Coo& coo, int nv, const int32_t* vid, const double* H, con
         }
 }
 
+// ---------------------------------------------------------------------------------------
+// affine bodies (abd_system/: abd_energy.inl:9-127, abd_jacobi_matrix.inl,
+// setup_abd_system_gradient_and_hessian.cu:162-610).  Written with explicit J matrices:
+// J(x) is 3x12 with J[r][r] = 1 and J[r][3 + 3r + c] = x_c (x = J q = p + A x_bar, the rows
+// of A being a1, a2, a3).
+// ---------------------------------------------------------------------------------------
+void abd_J(const double* x, double J[3][12]) {
+    for (int r = 0; r < 3; r++) {
+        for (int k = 0; k < 12; k++) J[r][k] = 0.0;
+        J[r][r] = 1.0;
+        for (int c = 0; c < 3; c++) J[r][3 + 3 * r + c] = x[c];
+    }
+}
+
+// orthogonality potential V = sum_i (|a_i|^2 - 1)^2 + sum_{i != j} (a_i . a_j)^2 and its
+// exact 9x9 Hessian, by forward-mode dual numbers over the 9 entries of A
+void abd_shape(const double* q, double* V, double* g9, double* H9) {
+    // gradient by duals; Hessian by differentiating the dual gradient expression again
+    // (each gradient component is a cubic polynomial: its derivative is taken with duals)
+    auto grad_dual = [&](const Dual<9>* a, Dual<9>* g) {
+        for (int i = 0; i < 3; i++) {
+            Dual<9> ai2 = a[3 * i] * a[3 * i] + a[3 * i + 1] * a[3 * i + 1] + a[3 * i + 2] * a[3 * i + 2];
+            for (int p = 0; p < 3; p++) {
+                Dual<9> gi = 4.0 * ((ai2 - Dual<9>(1.0)) * a[3 * i + p]);
+                for (int j = 0; j < 3; j++) {
+                    if (j == i) continue;
+                    Dual<9> aij = a[3 * i] * a[3 * j] + a[3 * i + 1] * a[3 * j + 1] + a[3 * i + 2] * a[3 * j + 2];
+                    gi = gi + 4.0 * (aij * a[3 * j + p]);
+                }
+                g[3 * i + p] = gi;
+            }
+        }
+    };
+    Dual<9> a[9], g[9];
+    for (int k = 0; k < 9; k++) a[k] = Dual<9>::var(q[3 + k], k);
+    grad_dual(a, g);
+    double v = 0;
+    for (int i = 0; i < 3; i++) {
+        double ai2 = q[3 + 3 * i] * q[3 + 3 * i] + q[4 + 3 * i] * q[4 + 3 * i] + q[5 + 3 * i] * q[5 + 3 * i];
+        v += (ai2 - 1) * (ai2 - 1);
+        for (int j = 0; j < 3; j++) {
+            if (j == i) continue;
+            double aij = q[3 + 3 * i] * q[3 + 3 * j] + q[4 + 3 * i] * q[4 + 3 * j] + q[5 + 3 * i] * q[5 + 3 * j];
+            v += aij * aij;
+        }
+    }
+    if (V) *V = v;
+    for (int k = 0; k < 9; k++) {
+        if (g9) g9[k] = g[k].v;
+        if (H9)
+            for (int l = 0; l < 9; l++) H9[9 * k + l] = g[k].d[l];
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -600,6 +654,138 @@ void or_friction_ground(const double* x, const double* x0, double lastH, double 
 
 void or_make_pd(int n, double* A) { make_pd(n, A); }
 void or_set_snk_projection(int on) { g_project_snk = on; }
+
+// body gradient (12 per body) and the merged upper body-space BCOO; returns the block
+// count, fills rows/cols/vals when rows != NULL (cap entries at most)
+int or_abd_assemble(int B, int P, const int32_t* point_body, const double* x_bar, const double* dmass,
+                    const double* vol, const int32_t* bt, const double* q, const double* qt, double kappa, double dt,
+                    const double* point_grad, int nabd, const int32_t* arows, const int32_t* acols,
+                    const double* avals, int nfem, const int32_t* frows, const int32_t* fcols, const double* fvals,
+                    const int32_t* fbt, double* body_grad, int cap, int32_t* rows, int32_t* cols, double* vals) {
+    Coo coo;
+    auto add12 = [&](int rb, int cb, const double (*K)[12], bool upper_only) {
+        for (int k = 0; k < 4; k++)
+            for (int l = 0; l < 4; l++) {
+                if (upper_only && k > l) continue;
+                double blk[9];
+                for (int p = 0; p < 3; p++)
+                    for (int t = 0; t < 3; t++) blk[3 * p + t] = K[3 * k + p][3 * l + t];
+                int r = 4 * rb + k, c = 4 * cb + l;
+                if (r <= c) coo.add(r, c, blk);
+                else {
+                    double bt2[9];
+                    for (int p = 0; p < 3; p++)
+                        for (int t = 0; t < 3; t++) bt2[3 * p + t] = blk[3 * t + p];
+                    coo.add(c, r, bt2);
+                }
+            }
+    };
+    for (int b = 0; b < B; b++) {
+        const double* dm = dmass + 13 * b;
+        // M = m J(0)^T J(0) generalised: entries 1, x_c, x_c x_d -> m, m x_c, m x_c x_d
+        double M[12][12] = {{0}};
+        for (int r = 0; r < 3; r++) {
+            M[r][r] = dm[0];
+            for (int c = 0; c < 3; c++) {
+                M[r][3 + 3 * r + c] = M[3 + 3 * r + c][r] = dm[1 + c];
+                for (int d = 0; d < 3; d++) M[3 + 3 * r + c][3 + 3 * r + d] = dm[4 + 3 * c + d];
+            }
+        }
+        double G[12] = {0}, H[12][12];
+        for (int i = 0; i < 12; i++)
+            for (int j = 0; j < 12; j++) H[i][j] = M[i][j];
+        if (bt[b] == 0) {
+            for (int i = 0; i < 12; i++)
+                for (int j = 0; j < 12; j++) G[i] += M[i][j] * (q[12 * b + j] - qt[12 * b + j]);
+            double kvt2 = kappa * vol[b] * dt * dt, g9[9], H9[81];
+            abd_shape(q + 12 * b, nullptr, g9, H9);
+            for (int k = 0; k < 81; k++) H9[k] *= kvt2;
+            make_pd(9, H9);
+            for (int i = 0; i < 9; i++) {
+                G[3 + i] += kvt2 * g9[i];
+                for (int j = 0; j < 9; j++) H[3 + i][3 + j] += H9[9 * i + j];
+            }
+            // point barrier gradients: J^T g
+            if (point_grad)
+                for (int p = 0; p < P; p++) {
+                    if (point_body[p] != b) continue;
+                    double J[3][12];
+                    abd_J(x_bar + 3 * p, J);
+                    for (int k = 0; k < 12; k++)
+                        for (int r = 0; r < 3; r++) G[k] += J[r][k] * point_grad[3 * p + r];
+                }
+        }
+        for (int k = 0; k < 12; k++) body_grad[12 * b + k] = G[k];
+        add12(b, b, H, true);
+    }
+    // ABD-ABD blocks: J_i^T H J_j (and its transpose for a same-body off-diagonal block)
+    for (int e = 0; e < nabd; e++) {
+        int i = arows[e], j = acols[e], bi = point_body[i], bj = point_body[j];
+        double Ji[3][12], Jj[3][12], K[12][12];
+        abd_J(x_bar + 3 * i, Ji);
+        abd_J(x_bar + 3 * j, Jj);
+        const double* Hp = avals + 9 * e;
+        bool zero = bt[bi] != 0 || bt[bj] != 0;
+        for (int k = 0; k < 12; k++)
+            for (int l = 0; l < 12; l++) {
+                double s = 0;
+                for (int p = 0; p < 3; p++)
+                    for (int t = 0; t < 3; t++) s += Ji[p][k] * Hp[3 * p + t] * Jj[t][l];
+                K[k][l] = zero ? 0.0 : s;
+            }
+        if (bi == bj) {
+            if (i != j) {
+                double S[12][12];
+                for (int k = 0; k < 12; k++)
+                    for (int l = 0; l < 12; l++) S[k][l] = K[k][l] + K[l][k];
+                add12(bi, bi, S, true);
+            } else {
+                add12(bi, bi, K, true);
+            }
+        } else {
+            add12(bi, bj, K, false);
+        }
+    }
+    // ABD-FEM blocks: J_i^T H into FEM column 4B + j
+    for (int e = 0; e < nfem; e++) {
+        int i = frows[e], j = fcols[e], b = point_body[i];
+        double Ji[3][12];
+        abd_J(x_bar + 3 * i, Ji);
+        const double* Hp = fvals + 9 * e;
+        bool zero = bt[b] != 0 || (fbt && fbt[j] != 0);
+        for (int k = 0; k < 4; k++) {
+            double blk[9];
+            for (int p = 0; p < 3; p++)
+                for (int t = 0; t < 3; t++) {
+                    double s = 0;
+                    for (int r = 0; r < 3; r++) s += Ji[r][3 * k + p] * Hp[3 * r + t];
+                    blk[3 * p + t] = zero ? 0.0 : s;
+                }
+            coo.add(4 * b + k, 4 * B + j, blk);
+        }
+    }
+    // merge
+    std::vector<size_t> order(coo.key.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t c) { return coo.key[a] < coo.key[c] || (coo.key[a] == coo.key[c] && a < c); });
+    int nu = 0;
+    for (size_t i = 0; i < order.size();) {
+        size_t j = i;
+        double acc[9] = {0};
+        while (j < order.size() && coo.key[order[j]] == coo.key[order[i]]) {
+            for (int k = 0; k < 9; k++) acc[k] += coo.val[9 * order[j] + k];
+            j++;
+        }
+        if (rows && nu < cap) {
+            rows[nu] = (int32_t)(coo.key[order[i]] >> 32);
+            cols[nu] = (int32_t)(coo.key[order[i]] & 0xffffffff);
+            std::memcpy(vals + 9 * nu, acc, sizeof(acc));
+        }
+        nu++;
+        i = j;
+    }
+    return nu;
+}
 void or_tri_bw(const double* X, const double* Dinv, double area, double kst, double ksh, double srate, double dt2,
                double* energy, double* grad, double* H9) {
     tri_bw(X, Dinv, area, kst, ksh, srate, dt2, energy, grad, H9);

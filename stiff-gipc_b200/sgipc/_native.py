@@ -51,6 +51,12 @@ class SgipcSolveStats(C.Structure):
                 ("rel_residual", C.c_double), ("status", _i32)]
 
 
+class SgipcAbdTopology(C.Structure):
+    _fields_ = [("body_num", _i32), ("point_num", _i32), ("point_body", _vp), ("x_bar", _vp),
+                ("dyadic_mass", _vp), ("volume", _vp), ("boundary_type", _vp), ("max_abd_blocks", _i32),
+                ("max_fem_blocks", _i32)]
+
+
 # every function the header declares, with its argument types
 SIGNATURES = {
     "sgipc_create": ([C.POINTER(SgipcTopology), C.c_int, C.POINTER(_vp)], _i32),
@@ -80,6 +86,14 @@ SIGNATURES = {
                                    _vp, _vp, _vp], _i32),
     "sgipc_mas_export_domains": ([_vp, _vp], _i32),
     "sgipc_mas_restrict": ([_vp, _vp, _vp], _i32),
+    "sgipc_abd_create": ([C.POINTER(SgipcAbdTopology), C.c_int, C.POINTER(_vp)], _i32),
+    "sgipc_abd_destroy": ([_vp], _i32),
+    "sgipc_abd_last_error": ([_vp], C.c_char_p),
+    "sgipc_abd_grad_hess": ([_vp, _vp, _vp, C.c_double, C.c_double, _vp, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
+                             _vp, _vp, _vp], _i32),
+    "sgipc_abd_export_bcoo": ([_vp, _i32, _vp, _vp, _vp, C.POINTER(_i32)], _i32),
+    "sgipc_abd_precond_build": ([_vp, _vp], _i32),
+    "sgipc_abd_precond_apply": ([_vp, _vp, _vp, _vp], _i32),
     "sgipc_launch_count": ([_vp, C.POINTER(C.c_int64)], _i32),
     "sgipc_time_kernel": ([_vp, C.c_char_p, _i32, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)], _i32),
 }

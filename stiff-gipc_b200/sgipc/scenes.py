@@ -542,6 +542,39 @@ def scene_cloth_on_cube(n_cloth: int = 24, n_cube: int = 6, seed: int = 2, frict
     return sc
 
 
+def scene_abd_boxes(nb: int = 500, seed: int = 3, edge: float = 0.05, density: float = 1000.0,
+                    dt: float = 0.01, kappa_abd: float = 1e8) -> dict:
+    """Affine bodies of the ABD configuration: nb boxes of 8 points and 5 tets (the
+    2x2x2 lattice split), edge 0.05 m, at seeded positions in a 1 m cube, kappa_ABD 1e8
+    (StiffGIPC/gipc/gipc.cu:18).  Returns the ABDSystem inputs: point_body, x_bar (points
+    relative to the body centroid), the lumped dyadic mass (each tet's mass / 4 at its
+    corners, abd_system.cu:527-600), volume, boundary_type, and one Newton iterate q
+    (translation + slightly perturbed identity rows) with its q_tilde (gravity on the
+    translation), plus the world positions x = J q."""
+    rng = np.random.default_rng(seed)
+    v, t = lattice_tets(2, edge)
+    v = v - v.mean(0)
+    _, vol_t = tet_rest_data(v, t)
+    node_m = np.zeros(8)
+    np.add.at(node_m, t.ravel(), np.repeat(vol_t * density / 4.0, 4))
+    dm = np.concatenate([[node_m.sum()], (node_m[:, None] * v).sum(0),
+                         np.einsum("p,pi,pj->ij", node_m, v, v).ravel()])
+    point_body = np.repeat(np.arange(nb), 8).astype(np.int32)
+    x_bar = np.tile(v, (nb, 1))
+    centres = rng.uniform(0.0, 1.0, (nb, 3))
+    A = np.eye(3)[None] + rng.normal(scale=1e-3, size=(nb, 3, 3))
+    q = np.concatenate([centres, A.reshape(nb, 9)], 1)
+    vel = rng.normal(scale=0.1, size=(nb, 3))
+    q_prev = q.copy()
+    q_prev[:, :3] -= dt * vel
+    q_tilde = q_prev.copy()
+    q_tilde[:, :3] += dt * vel + dt * dt * np.asarray(GRAVITY)
+    x = (np.einsum("bij,bpj->bpi", A, x_bar.reshape(nb, 8, 3)) + centres[:, None]).reshape(-1, 3)
+    return dict(point_body=point_body, x_bar=x_bar, dyadic_mass=np.tile(dm, (nb, 1)),
+                volume=np.full(nb, vol_t.sum()), boundary_type=np.zeros(nb, np.int32),
+                q=q, q_tilde=q_tilde, x=x, dt=dt, kappa=kappa_abd)
+
+
 SCENES = {
     "cube": scene_cube,
     "two_cubes": scene_two_cubes,

@@ -362,3 +362,111 @@ def test_cloth_scene_matrix_symmetric_positive_definite(small_cloth):
     b, rows, cols, vals, _ = oracle.assemble(sc)
     A = oracle.dense(rows, cols, vals, sc.nv)
     assert np.allclose(A, A.T) and np.linalg.eigvalsh(A).min() > 0
+
+
+# ------------------------------------------------------------------------------------------
+# affine bodies
+# ------------------------------------------------------------------------------------------
+def _abd_J(x):
+    J = np.zeros((3, 12))
+    J[:, :3] = np.eye(3)
+    for r in range(3):
+        J[r, 3 + 3 * r:6 + 3 * r] = x
+    return J
+
+
+def abd_contacts(bodies, n_fem=40, seed=0):
+    """Seeded point-space contact blocks: ABD-ABD (different bodies, row < col, and some
+    diagonal blocks), ABD-FEM, point gradients and a FEM Dirichlet mask."""
+    rng = np.random.default_rng(seed)
+    pb = bodies["point_body"]
+    P = len(pb)
+    pairs = []
+    while len(pairs) < 60:
+        i, j = sorted(rng.integers(0, P, 2))
+        if pb[i] != pb[j]:
+            pairs.append((i, j))
+    diag = rng.choice(P, 10, replace=False)
+    rows = np.array([p[0] for p in pairs] + list(diag), np.int32)
+    cols = np.array([p[1] for p in pairs] + list(diag), np.int32)
+
+    def spd(n):
+        M = rng.normal(size=(n, 3, 3))
+        return np.einsum("nij,nkj->nik", M, M) * 1e3
+
+    vals = spd(len(rows))
+    frows = rng.integers(0, P, 25).astype(np.int32)
+    fcols = rng.integers(0, n_fem, 25).astype(np.int32)
+    fvals = rng.normal(size=(25, 3, 3)) * 1e3
+    fbt = (rng.uniform(size=n_fem) < 0.2).astype(np.int32)
+    grad = rng.normal(size=(P, 3))
+    return dict(abd=(rows, cols, vals), fem=(frows, fcols, fvals), fem_boundary=fbt, point_grad=grad, n_fem=n_fem)
+
+
+def test_abd_orthogonality_potential():
+    rng = np.random.default_rng(1)
+    R, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+    b = scenes.scene_abd_boxes(2, seed=1)
+    q = b["q"].copy()
+    q[0, 3:] = R.ravel()
+    g, rows, cols, vals = oracle.abd_assemble(b, q, q, b["kappa"], b["dt"])
+    assert np.abs(g[:12]).max() < 1e-6 * b["kappa"] * b["volume"][0] * b["dt"] ** 2
+    # away from a rotation: the body gradient is the derivative of the body energy
+    bodies = dict(b, boundary_type=np.zeros(2, np.int32))
+    q = b["q"] + rng.normal(scale=1e-2, size=b["q"].shape)
+    g, *_ = oracle.abd_assemble(bodies, q, b["q_tilde"], b["kappa"], b["dt"])
+
+    def energy(qq):
+        E = 0.0
+        for k in range(2):
+            d = qq[k] - b["q_tilde"][k]
+            dm = b["dyadic_mass"][k]
+            M = np.zeros((12, 12))
+            for r in range(3):
+                M[r, r] = dm[0]
+                M[r, 3 + 3 * r:6 + 3 * r] = M[3 + 3 * r:6 + 3 * r, r] = dm[1:4]
+                M[3 + 3 * r:6 + 3 * r, 3 + 3 * r:6 + 3 * r] = dm[4:].reshape(3, 3)
+            A = qq[k, 3:].reshape(3, 3)
+            C = A @ A.T - np.eye(3)
+            E += 0.5 * d @ M @ d + b["kappa"] * b["volume"][k] * b["dt"] ** 2 * (C ** 2).sum()
+        return E
+
+    h = 1e-7
+    for k in rng.choice(24, 6, replace=False):
+        qp, qm = q.copy(), q.copy()
+        qp.flat[k] += h
+        qm.flat[k] -= h
+        assert (energy(qp) - energy(qm)) / (2 * h) == pytest.approx(g[k], rel=1e-5, abs=1e-9 * np.abs(g).max())
+
+
+def test_abd_contact_mapping_is_the_point_space_quadratic_form():
+    b = scenes.scene_abd_boxes(12, seed=4)
+    c = abd_contacts(b, seed=5)
+    B, F = 12, c["n_fem"]
+    g0, r0, c0, v0 = oracle.abd_assemble(b, b["q"], b["q_tilde"], b["kappa"], b["dt"])
+    g1, r1, c1, v1 = oracle.abd_assemble(b, b["q"], b["q_tilde"], b["kappa"], b["dt"], point_grad=c["point_grad"],
+                                         abd_blocks=c["abd"], fem_blocks=c["fem"], fem_boundary=c["fem_boundary"])
+    n = 4 * B + F
+
+    def quad(rows, cols, vals, y):
+        A = oracle.dense(rows, cols, vals, n)
+        return y @ A @ y
+
+    rng = np.random.default_rng(6)
+    y = rng.normal(size=3 * n)
+    d = np.stack([_abd_J(b["x_bar"][p]) @ y[12 * b["point_body"][p]:12 * b["point_body"][p] + 12]
+                  for p in range(len(b["point_body"]))])
+    yf = y[12 * B:].reshape(F, 3)
+    expect = 0.0
+    for i, j, H in zip(*c["abd"]):
+        expect += d[i] @ H @ d[j] * (1 if i == j else 2)
+    for i, f, H in zip(*c["fem"]):
+        if c["fem_boundary"][f] == 0:
+            expect += 2 * d[i] @ H @ yf[f]
+    assert quad(r1, c1, v1, y) - quad(r0, c0, v0, y) == pytest.approx(expect, rel=1e-10)
+    # point gradients: J^T g summed per body
+    ref = np.zeros(12 * B)
+    for p in range(len(b["point_body"])):
+        k = b["point_body"][p]
+        ref[12 * k:12 * k + 12] += _abd_J(b["x_bar"][p]).T @ c["point_grad"][p]
+    assert np.allclose(g1 - g0, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
