@@ -761,38 +761,58 @@ __global__ void k_soft(int ns, const uint32_t* __restrict__ idx, const double* _
 }
 
 // ---- contact block merge ------------------------------------------------------------------
-__global__ void k_head_flags(int m, const unsigned long long* __restrict__ ks, int* __restrict__ flag) {
+// run heads of the sorted keys (the unused-slot key forms no run); flag[m] = 0
+__global__ void k_run_heads(int m, const unsigned long long* __restrict__ ks, int* __restrict__ flag) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > m) return;
-    if (i == m) { flag[i] = 0; return; }
-    unsigned long long k = ks[i];
+    if (i == m) {
+        flag[m] = 0;
+        return;
+    }
+    const unsigned long long k = ks[i];
     flag[i] = (k != kBadKey && (i == 0 || ks[i - 1] != k)) ? 1 : 0;
 }
 
-__global__ void k_reduce_unique(int m, const unsigned long long* __restrict__ ks, const int* __restrict__ is,
-                                const int* __restrict__ uid, const double* __restrict__ cval, int bits,
-                                int* __restrict__ uc_row, int* __restrict__ uc_col, double* __restrict__ u64,
-                                float* __restrict__ u32, int* __restrict__ nuc) {
+// after the exclusive scan flag[i] = run id of head i; start[u] = first sorted index of run
+// u, start[nuc] = end of the last run; row / column of every unique block
+__global__ void k_run_starts(int m, const unsigned long long* __restrict__ ks, const int* __restrict__ rid, int bits,
+                             int* __restrict__ start, int* __restrict__ uc_row, int* __restrict__ uc_col,
+                             int* __restrict__ nuc) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) nuc[0] = uid[m];
-    if (i >= m) return;
-    unsigned long long k = ks[i];
-    if (k == kBadKey || (i > 0 && ks[i - 1] == k)) return;
-    int u = uid[i];
-    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int j = i; j < m && ks[j] == k; j++) {
-        const double* v = cval + 9 * (size_t)is[j];
-#pragma unroll
-        for (int q = 0; q < 9; q++) acc[q] += v[q];
+    if (i > m) return;
+    if (i == m) {
+        const int nu = rid[m];
+        nuc[0] = nu;
+        // end of the last run: the first unused-slot key (sorted last) or m
+        int lo = 0, hi = m;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (ks[mid] != kBadKey) lo = mid + 1; else hi = mid;
+        }
+        start[nu] = lo;
+        return;
     }
-    unsigned long long mask = (1ull << bits) - 1ull;
+    const unsigned long long k = ks[i];
+    if (k == kBadKey || (i > 0 && ks[i - 1] == k)) return;
+    const int u = rid[i];
+    start[u] = i;
+    const unsigned long long mask = (1ull << bits) - 1ull;
     uc_row[u] = (int)(k >> bits);
     uc_col[u] = (int)(k & mask);
-#pragma unroll
-    for (int q = 0; q < 9; q++) {
-        u64[9 * (size_t)u + q] = acc[q];
-        u32[9 * (size_t)u + q] = (float)acc[q];
-    }
+}
+
+__global__ void k_run_sums(int m, const int* __restrict__ nuc, const int* __restrict__ start,
+                           const int* __restrict__ is, const double* __restrict__ cval, double* __restrict__ u64,
+                           float* __restrict__ u32) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int u = (int)(t / 9), q = (int)(t % 9);
+    if (u >= nuc[0]) return;
+    const int j0 = start[u], j1 = start[u + 1];
+    double acc = 0.0;
+#pragma unroll 4
+    for (int j = j0; j < j1; j++) acc += cval[9 * (size_t)is[j] + q];
+    u64[9 * (size_t)u + q] = acc;
+    u32[9 * (size_t)u + q] = (float)acc;
 }
 
 __global__ void k_lower_keys(int m, const int* __restrict__ nuc, const int* __restrict__ uc_row,
@@ -930,14 +950,18 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
         return SGIPC_OK;
     }
     const int endbit = 2 * c->key_bits;
-    SG_COUNT(c, 6);
+    SG_COUNT(c, 7);
+    // keys sorted with their slot ids; runs of equal keys numbered by a scan of run heads;
+    // each unique block summed by 9 threads (one per entry) over its run in sorted order
+    // (deterministic), with every load of a run independent of the previous one
     size_t tb = c->cub_tmp_bytes;
     SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->ckey, c->ckey_s, c->cidx, c->cidx_s, m, 0, endbit, s));
-    k_head_flags<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cflag);
+    k_run_heads<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cflag);
     tb = c->cub_tmp_bytes;
     SG_CHECK(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp, tb, c->cflag, c->cflag, m + 1, s));
-    k_reduce_unique<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cidx_s, c->cflag, c->cval, c->key_bits, c->uc_row,
-                                                    c->uc_col, c->uc64, c->uc32, c->nuc);
+    k_run_starts<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cflag, c->key_bits, c->run_start, c->uc_row,
+                                                     c->uc_col, c->nuc);
+    k_run_sums<<<nblk(9LL * m), SGIPC_BLOCK, 0, s>>>(m, c->nuc, c->run_start, c->cidx_s, c->cval, c->uc64, c->uc32);
     k_row_ptr_rows<<<nblk(c->n + 1), SGIPC_BLOCK, 0, s>>>(c->n, c->nuc, c->uc_row, c->cu_ptr);
     k_lower_keys<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->nuc, c->uc_row, c->uc_col, c->key_bits, c->lkey, c->lidx);
     tb = c->cub_tmp_bytes;

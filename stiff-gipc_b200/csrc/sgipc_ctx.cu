@@ -139,6 +139,9 @@ static SgipcStatus build_static(SgipcCtx* c, const SgipcTopology* t) {
     for (int i = 0; i < n; i++) frow[i + 1] = (row_ptr[i + 1] - row_ptr[i]) + (low_ptr[i + 1] - low_ptr[i]);
     for (int i = 0; i < n; i++) frow[i + 1] += frow[i];
     c->nnz_full = frow[n];
+    c->h_frow_ptr = (int*)malloc(sizeof(int) * (n + 1));
+    if (!c->h_frow_ptr) return SGIPC_CUDA_ERROR;
+    std::copy(frow.begin(), frow.end(), c->h_frow_ptr);
     std::vector<int> fcol(std::max(c->nnz_full, 1)), fup(nnz), flo(nnz, -1);
     for (int i = 0; i < n; i++) {
         int k = frow[i];
@@ -239,6 +242,7 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
     c->cap_cblk = (int)cap;
     if ((st = dalloc(c, &c->ckey, cap)) || (st = dalloc(c, &c->ckey_s, cap)) || (st = dalloc(c, &c->cidx, cap)) ||
         (st = dalloc(c, &c->cidx_s, cap)) || (st = dalloc(c, &c->cval, cap * 9)) ||
+        (st = dalloc(c, &c->run_start, cap + 1)) ||
         (st = dalloc(c, &c->cflag, cap + 1)) || (st = dalloc(c, &c->nuc, 4)) || (st = dalloc(c, &c->uc_row, cap)) ||
         (st = dalloc(c, &c->uc_col, cap)) || (st = dalloc(c, &c->uc64, cap * 9)) ||
         (st = dalloc(c, &c->uc32, cap * 9)) || (st = dalloc(c, &c->cu_ptr, n + 1)) ||
@@ -277,9 +281,10 @@ extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
                     c->hinges, c->hinge_adj, c->soft_idx, c->shape_grads, c->fb, c->b, c->ckey, c->ckey_s,
                     c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,
                     c->cu_ptr, c->cl_ptr, c->cl_idx, c->lkey, c->lkey_s, c->lidx, c->cub_tmp, c->dflag,
-                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32};
+                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32, c->run_start};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    free(c->h_frow_ptr);
     delete c;
     return SGIPC_OK;
 }

@@ -104,6 +104,7 @@ struct SgipcCtx {
     // full symmetric copy of the static blocks (both triangles) for the SpMV
     int nnz_full;             // 2*nnz - n
     int* frow_ptr;            // [n+1]
+    int* h_frow_ptr;          // host copy (sizes the persistent solve's shared-memory residency)
     int* fcol;                // [nnz_full]
     int* fup;                 // [nnz] full index of upper slot s
     int* flo;                 // [nnz] full index of its transpose (-1 on the diagonal)
@@ -137,6 +138,7 @@ struct SgipcCtx {
     int* cidx;                    // [cap]
     int* cidx_s;
     double* cval;                 // [cap*9]
+    int* run_start;               // [cap+1] first sorted index of each unique block's run
     int* cflag;                   // [cap+1] segment heads -> unique ids
     int* nuc;                     // device: number of unique contact blocks
     int* uc_row;                  // [cap]

@@ -33,6 +33,21 @@ constexpr int kDomPerCta = kCoopThreads / 48;  // 10 domains of 48 rows per roun
 constexpr int kCoopMaxCtasPerSm = 2;
 constexpr long long kSpinLimit = 1LL << 25;    // polls (~50 ns each once sleeping): ~2 s
 
+// dynamic shared memory of the persistent solve: [rp (rows + 1)] [columns] [block values]
+// [domain inverses], each part 16-byte aligned
+__host__ __device__ constexpr int coop_pad4(int n) { return (n + 3) & ~3; }
+__host__ __device__ constexpr size_t coop_rows_bytes(int rows, int ecap, int tsize) {
+    return ecap > 0 ? (size_t)(coop_pad4(rows + 1) + coop_pad4(ecap)) * 4 + (((size_t)9 * ecap * tsize + 15) & ~(size_t)15)
+                    : 0;
+}
+
+// contact part: [ru (rows + 1)] [rl (rows + 1)] [columns] [block values]
+__host__ __device__ constexpr size_t coop_contact_bytes(int rows, int kcap, int tsize) {
+    return kcap > 0 ? (size_t)(2 * coop_pad4(rows + 1) + coop_pad4(kcap)) * 4 + (((size_t)9 * kcap * tsize + 15) & ~(size_t)15)
+                    : 0;
+}
+constexpr int kContactSlots = 768;  // contact entries per CTA held in shared memory
+
 struct GridBarrier {
     unsigned int* count;  // arrivals since launch (zeroed before the launch)
     unsigned int* abort;
@@ -63,6 +78,11 @@ struct CoopArgs {
     int max_iter;
     int crit;
     double tol;
+    // shared-memory residency (0 = off): static rows of the CTA's SpMV rows (up to ecap
+    // blocks) and the first dcap of its level-0/1 domain inverses, loaded once per solve
+    int ecap;
+    int kcap;
+    int dcap;
 };
 
 __device__ __forceinline__ void red_add_release_gpu(unsigned int* p, unsigned int v) {
@@ -96,6 +116,9 @@ __device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch) {
             }
             if (k > 256) __nanosleep(32);
         }
+        // gpu-scope fence after the acquire: the SM's L1 holds no line older than the
+        // barrier, so the CTA may read other CTAs' writes with ordinary (L1-cached) loads
+        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
@@ -182,7 +205,7 @@ __device__ void phase_init(const CoopArgs<T, M, NR>& a, double (&bb)[NR]) {
 // when it is below `hi`.  All loads of a row of the product are issued together.
 template <class M, int NR>
 __device__ __forceinline__ void solve_domains(const M* __restrict__ inv, const M* R, M* Z, int d0, int hi,
-                                              M (*sR)[48 * NR]) {
+                                              M (*sR)[48 * NR], const M* cache = nullptr, int ncached = 0) {
     const int ld = threadIdx.x / 48, i = threadIdx.x % 48;
     const int d = d0 + ld;
     const bool act = ld < kDomPerCta && d < hi;
@@ -191,7 +214,8 @@ __device__ __forceinline__ void solve_domains(const M* __restrict__ inv, const M
         for (int r = 0; r < NR; r++) sR[ld][i * NR + r] = __ldcg(R + (48 * (size_t)d + i) * NR + r);
     __syncthreads();
     if (act) {
-        const M* Ad = inv + (size_t)d * 2304;
+        const bool sm = ld < ncached;  // this slot's inverse is resident in shared memory
+        const M* Ad = sm ? cache + (size_t)ld * 2304 : inv + (size_t)d * 2304;
         M acc[NR];
 #pragma unroll
         for (int r = 0; r < NR; r++) acc[r] = 0;
@@ -200,7 +224,7 @@ __device__ __forceinline__ void solve_domains(const M* __restrict__ inv, const M
         for (int j0 = 0; j0 < 48; j0 += kU) {
             M w[kU];
 #pragma unroll
-            for (int j = 0; j < kU; j++) w[j] = __ldg(Ad + (j0 + j) * 48 + i);
+            for (int j = 0; j < kU; j++) w[j] = sm ? Ad[(j0 + j) * 48 + i] : __ldg(Ad + (j0 + j) * 48 + i);
 #pragma unroll
             for (int j = 0; j < kU; j++)
 #pragma unroll
@@ -213,12 +237,17 @@ __device__ __forceinline__ void solve_domains(const M* __restrict__ inv, const M
 }
 
 // domains [lo, hi) over CTAs first .. first+ncta-1 (block-uniform loop bounds)
+// (the first round may read `ncached` inverses from `cache`)
 template <class M, int NR>
 __device__ __forceinline__ void solve_domain_range(const M* inv, const M* R, M* Z, int lo, int hi, int first,
-                                                   int ncta, M (*sR)[48 * NR]) {
+                                                   int ncta, M (*sR)[48 * NR], const M* cache = nullptr,
+                                                   int ncached = 0) {
     const int c = (int)blockIdx.x - first;
     if (c < 0 || c >= ncta) return;
-    for (int d0 = lo + c * kDomPerCta; d0 < hi; d0 += ncta * kDomPerCta) solve_domains<M, NR>(inv, R, Z, d0, hi, sR);
+    for (int d0 = lo + c * kDomPerCta; d0 < hi; d0 += ncta * kDomPerCta) {
+        solve_domains<M, NR>(inv, R, Z, d0, hi, sR, cache, ncached);
+        ncached = 0;
+    }
 }
 
 // restriction level 1 -> 2, one half-warp per level-1 bank, taken by the LAST warps of the
@@ -248,10 +277,11 @@ __device__ void restrict_level1(const MasView& mv, M* R) {
 
 // z = M^-1 r given R at levels 0 and 1: two phases and two barriers (one when L <= 2)
 template <class T, class M, int NR>
-__device__ bool phase_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], unsigned int& epoch) {
+__device__ bool phase_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], unsigned int& epoch, const M* dcache,
+                          int ndc) {
     const int L = a.mv.L, G = gridDim.x;
     if (L > 2) restrict_level1<M, NR>(a.mv, a.R);
-    solve_domain_range<M, NR>(a.inv, a.R, a.Z, 0, a.nd01, 0, G, sR);
+    solve_domain_range<M, NR>(a.inv, a.R, a.Z, 0, a.nd01, 0, G, sR, dcache, ndc);
     if (!grid_barrier(a.br, ++epoch)) return false;
     if (L <= 2) return true;
     if (blockIdx.x == 0) {
@@ -281,9 +311,9 @@ __device__ void phase_prolong(const CoopArgs<T, M, NR>& a, const bool (&run)[NR]
 #pragma unroll
             for (int l = 0; l < SGIPC_MAX_LEVELS; l++) {
                 if (gl[l] < 0) continue;
-                s0 += __ldcg(a.Z + (size_t)(3 * gl[l]) * NR + r);
-                s1 += __ldcg(a.Z + (size_t)(3 * gl[l] + 1) * NR + r);
-                s2 += __ldcg(a.Z + (size_t)(3 * gl[l] + 2) * NR + r);
+                s0 += a.Z[(size_t)(3 * gl[l]) * NR + r];  // coarse clusters are shared: L1 reuse
+                s1 += a.Z[(size_t)(3 * gl[l] + 1) * NR + r];
+                s2 += a.Z[(size_t)(3 * gl[l] + 2) * NR + r];
             }
             const T zz[3] = {(T)s0, (T)s1, (T)s2};
 #pragma unroll
@@ -297,10 +327,133 @@ __device__ void phase_prolong(const CoopArgs<T, M, NR>& a, const bool (&run)[NR]
 }
 
 // p = z + beta p_old (p = z on the first iteration), Ap = A p, p.Ap
+// The static rows of this CTA's first SpMV pass, resident in shared memory: local row
+// pointers rp[0..rows], column indices and block values of entries [rp[0], rp[rows]).
+template <class T>
+struct RowCache {
+    const int* rp;
+    const int* col;
+    const T* val;
+    int r0, r1;  // rows held (r0 == r1: none)
+    // contact entries of the same rows (constant during a solve) when they fit: per row the
+    // upper entries [ru[li], ru[li+1]) and the transposed ones [rl[li], rl[li+1]) of kcol/kval
+    const int* ru;
+    const int* rl;
+    const int* kcol;
+    const T* kval;
+};
+
+// row_mv with the static part read from shared memory; the (few) contact entries of the
+// row come from global memory, their bounds loaded before the static work
+template <class T, int NR, class Op>
+__device__ __forceinline__ void row_mv_resident(const Topo& tp, const MatView<T>& A, const Op& x, int i, int g,
+                                                const RowCache<T>& rc, T (&acc)[NR][3]) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r][0] = acc[r][1] = acc[r][2] = 0;
+    if (i < tp.n && rc.kcol) {
+        // everything of the row in shared memory: one virtual list (static, contact,
+        // transposed contact), only the gathers of x touch global memory
+        const int li = i - rc.r0;
+        const int s0 = rc.rp[li], ns = rc.rp[li + 1] - s0;
+        const int u0 = rc.ru[li], nu = rc.ru[li + 1] - u0;
+        const int l0 = rc.rl[li], nl = rc.rl[li + 1] - l0;
+        const int len = ns + nu + nl;
+        constexpr int kB = NR == 1 ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 2 : 1);
+        for (int e0 = g; e0 < len; e0 += kB * kSpG) {
+            int cj[kB];
+            const T* bp[kB];
+            T xb[kB][NR][3];
+#pragma unroll
+            for (int u = 0; u < kB; u++) {
+                const int e = e0 + u * kSpG;
+                cj[u] = -1;
+                bp[u] = nullptr;
+                if (e < ns) {
+                    cj[u] = rc.col[s0 + e];
+                    bp[u] = rc.val + 9 * (s0 + e);
+                } else if (e < ns + nu) {
+                    cj[u] = rc.kcol[u0 + e - ns];
+                    bp[u] = rc.kval + 9 * (u0 + e - ns);
+                } else if (e < len) {
+                    cj[u] = rc.kcol[l0 + e - ns - nu];
+                    bp[u] = rc.kval + 9 * (l0 + e - ns - nu);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kB; u++)
+                if (cj[u] >= 0) x.load(cj[u], xb[u]);
+#pragma unroll
+            for (int u = 0; u < kB; u++) {
+                if (cj[u] < 0) continue;
+                const T* bv = bp[u];
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const T x0 = xb[u][r][0], x1 = xb[u][r][1], x2 = xb[u][r][2];
+                    acc[r][0] += bv[0] * x0 + bv[1] * x1 + bv[2] * x2;
+                    acc[r][1] += bv[3] * x0 + bv[4] * x1 + bv[5] * x2;
+                    acc[r][2] += bv[6] * x0 + bv[7] * x1 + bv[8] * x2;
+                }
+            }
+        }
+    } else if (i < tp.n) {
+        const int u0 = tp.cu_ptr[i], u1 = tp.cu_ptr[i + 1];
+        const int k0 = tp.cl_ptr[i], k1 = tp.cl_ptr[i + 1];
+        const int li = i - rc.r0;
+        const int s0 = rc.rp[li], s1 = rc.rp[li + 1];
+        constexpr int kB = NR == 1 ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 2 : 1);
+        for (int e0 = s0 + g; e0 < s1; e0 += kB * kSpG) {
+            int cj[kB];
+            T xb[kB][NR][3];
+#pragma unroll
+            for (int u = 0; u < kB; u++) {
+                const int e = e0 + u * kSpG;
+                cj[u] = e < s1 ? rc.col[e] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < kB; u++)
+                if (cj[u] >= 0) x.load(cj[u], xb[u]);
+#pragma unroll
+            for (int u = 0; u < kB; u++) {
+                if (cj[u] < 0) continue;
+                const T* bv = rc.val + 9 * (e0 + u * kSpG);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const T x0 = xb[u][r][0], x1 = xb[u][r][1], x2 = xb[u][r][2];
+                    acc[r][0] += bv[0] * x0 + bv[1] * x1 + bv[2] * x2;
+                    acc[r][1] += bv[3] * x0 + bv[4] * x1 + bv[5] * x2;
+                    acc[r][2] += bv[6] * x0 + bv[7] * x1 + bv[8] * x2;
+                }
+            }
+        }
+        const int nu = u1 - u0, len = nu + (k1 - k0);
+        for (int e = g; e < len; e += kSpG) {
+            const bool up = e < nu;
+            const int cj = up ? __ldg(tp.uc_col + u0 + e) : __ldg(tp.cl_col + k0 + (e - nu));
+            const T* src = up ? A.uc + 9 * (size_t)(u0 + e) : A.cl + 9 * (size_t)(k0 + (e - nu));
+            T bv[9], xb[NR][3];
+#pragma unroll
+            for (int q = 0; q < 9; q++) bv[q] = __ldg(src + q);
+            x.load(cj, xb);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                acc[r][0] += bv[0] * xb[r][0] + bv[1] * xb[r][1] + bv[2] * xb[r][2];
+                acc[r][1] += bv[3] * xb[r][0] + bv[4] * xb[r][1] + bv[5] * xb[r][2];
+                acc[r][2] += bv[6] * xb[r][0] + bv[7] * xb[r][1] + bv[8] * xb[r][2];
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int o = 1; o < kSpG; o <<= 1) acc[r][q] += __shfl_xor_sync(0xffffffffu, acc[r][q], o, kSpG);
+}
+
 template <class T, class M, int NR>
 __device__ void phase_spmv(const CoopArgs<T, M, NR>& a, bool first, const double (&beta)[NR], const T* pold, T* pnew,
-                           const bool (&run)[NR], double (&pAp)[NR]) {
-    Operand<T, NR, true> op;
+                           const bool (&run)[NR], double (&pAp)[NR], const RowCache<T>& rc) {
+    Operand<T, NR, false> op;  // L1-cached gathers: each x_j serves ~13 rows of the same CTA
     op.a = a.z;
     op.b = first ? nullptr : pold;
 #pragma unroll
@@ -313,7 +466,10 @@ __device__ void phase_spmv(const CoopArgs<T, M, NR>& a, bool first, const double
         T pi[NR][3];
         if (i < n && g == 0) op.load(i, pi);  // issued before the row's gathers
         T acc[NR][3];
-        row_mv<T, NR>(a.tp, a.A, op, i, g, acc);
+        if (i0 >= rc.r0 && i0 < rc.r1)  // warp-uniform: the warp's rows are resident
+            row_mv_resident<T, NR>(a.tp, a.A, op, i, g, rc, acc);
+        else
+            row_mv<T, NR>(a.tp, a.A, op, i, g, acc);
         if (i < n && g == 0) {
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -372,7 +528,62 @@ template <class T, class M, int NR>
 __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a) {
     __shared__ double smem[NR * 32];
     __shared__ M sR[kDomPerCta][48 * NR];
+    extern __shared__ __align__(16) unsigned char dsm[];
     unsigned int epoch = 0;
+
+    // ---- shared-memory residency of this CTA's static rows and level-0/1 domain inverses
+    // (constant for the whole solve): loaded once, read every iteration
+    constexpr int rpc = kCoopThreads / kSpG;  // rows of one CTA in one SpMV pass
+    RowCache<T> rc{nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, nullptr, nullptr};
+    const M* dcache = nullptr;
+    int ndc = 0;
+    {
+        int* rp = reinterpret_cast<int*>(dsm);
+        int* ccol = rp + coop_pad4(rpc + 1);
+        T* cval = reinterpret_cast<T*>(ccol + coop_pad4(a.ecap));
+        M* dom = reinterpret_cast<M*>(dsm + coop_rows_bytes(rpc, a.ecap, sizeof(T)) +
+                                      coop_contact_bytes(rpc, a.kcap, sizeof(T)));
+        if (a.ecap > 0) {
+            const int r0 = blockIdx.x * rpc, r1 = min(a.tp.n, r0 + rpc);
+            if (r0 < r1) {
+                const int e0 = __ldg(a.tp.frow_ptr + r0), e1 = __ldg(a.tp.frow_ptr + r1);
+                for (int k = threadIdx.x; k <= r1 - r0; k += blockDim.x) rp[k] = __ldg(a.tp.frow_ptr + r0 + k) - e0;
+                for (int k = threadIdx.x; k < e1 - e0; k += blockDim.x) ccol[k] = __ldg(a.tp.fcol + e0 + k);
+                for (int k = threadIdx.x; k < 9 * (e1 - e0); k += blockDim.x) cval[k] = __ldg(a.A.fval + 9 * (size_t)e0 + k);
+                rc = RowCache<T>{rp, ccol, cval, r0, r1, nullptr, nullptr, nullptr, nullptr};
+                // the rows' contact entries, when they fit the kcap slots
+                int* ru = reinterpret_cast<int*>(dsm + coop_rows_bytes(rpc, a.ecap, sizeof(T)));
+                int* rl = ru + coop_pad4(rpc + 1);
+                int* kcol = rl + coop_pad4(rpc + 1);
+                T* kval = reinterpret_cast<T*>(kcol + coop_pad4(a.kcap));
+                const int u0 = __ldg(a.tp.cu_ptr + r0), u1 = __ldg(a.tp.cu_ptr + r1);
+                const int q0 = __ldg(a.tp.cl_ptr + r0), q1 = __ldg(a.tp.cl_ptr + r1);
+                const int nu = u1 - u0, nl = q1 - q0;
+                if (a.kcap > 0 && nu + nl <= a.kcap) {
+                    for (int k = threadIdx.x; k <= r1 - r0; k += blockDim.x) {
+                        ru[k] = __ldg(a.tp.cu_ptr + r0 + k) - u0;
+                        rl[k] = __ldg(a.tp.cl_ptr + r0 + k) - q0 + nu;
+                    }
+                    for (int k = threadIdx.x; k < nu; k += blockDim.x) kcol[k] = __ldg(a.tp.uc_col + u0 + k);
+                    for (int k = threadIdx.x; k < nl; k += blockDim.x) kcol[nu + k] = __ldg(a.tp.cl_col + q0 + k);
+                    for (int k = threadIdx.x; k < 9 * nu; k += blockDim.x) kval[k] = __ldg(a.A.uc + 9 * (size_t)u0 + k);
+                    for (int k = threadIdx.x; k < 9 * nl; k += blockDim.x)
+                        kval[9 * nu + k] = __ldg(a.A.cl + 9 * (size_t)q0 + k);
+                    rc.ru = ru;
+                    rc.rl = rl;
+                    rc.kcol = kcol;
+                    rc.kval = kval;
+                }
+            }
+        }
+        if (a.dcap > 0) {
+            const int d0 = blockIdx.x * kDomPerCta;
+            ndc = max(0, min(a.dcap, a.nd01 - d0));
+            for (int k = threadIdx.x; k < ndc * 2304; k += blockDim.x) dom[k] = __ldg(a.inv + 2304 * (size_t)d0 + k);
+            dcache = dom;
+        }
+        __syncthreads();
+    }
     // per right-hand side state, identical in every thread (computed from the same totals)
     bool run[NR];
     int iters[NR], status[NR];
@@ -387,7 +598,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
     // ---- r = b, x = 0, z = M r, rz0 = r.z
     phase_init(a, v);
     bool ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, bn2);
-    ok = ok && phase_mas(a, sR, epoch);
+    ok = ok && phase_mas(a, sR, epoch, dcache, ndc);
     if (ok) {
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
@@ -414,7 +625,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
         bool stop_rz[NR];
 #pragma unroll
         for (int r = 0; r < NR; r++) pAp[r] = 0.0;
-        phase_spmv(a, k == 1, beta, pold, pnew, run, pAp);
+        phase_spmv(a, k == 1, beta, pold, pnew, run, pAp, rc);
         if (!(ok = grid_reduce<NR>(a.br, ++epoch, pAp, a.partial, smem, pAp))) break;
 #pragma unroll
         for (int r = 0; r < NR; r++) {
@@ -444,7 +655,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
             any |= run[r];
         }
         if (!any || k + 1 >= a.max_iter) break;  // converged, or the iteration cap
-        if (!(ok = phase_mas(a, sR, epoch))) break;
+        if (!(ok = phase_mas(a, sR, epoch, dcache, ndc))) break;
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
         phase_prolong(a, run, v);
@@ -482,15 +693,56 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     *used = false;
     const char* e = getenv("SGIPC_PCG_GRAPH");
     if (e && e[0] == '1') return SGIPC_OK;  // the graph of per-phase kernels instead
-    int coop = 0, nsm = 0, per = 0;
+    int coop = 0, nsm = 0, per = 0, optin = 0;
     SG_CHECK(c, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
     SG_CHECK(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-    SG_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_coop<T, M, NR>, kCoopThreads, 0));
-    if (!coop || per < 1) return SGIPC_OK;
-    if (per > kCoopMaxCtasPerSm) per = kCoopMaxCtasPerSm;
-    int grid = nsm * per;
-    if (grid > w.coop_cap) grid = w.coop_cap;
+    SG_CHECK(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    if (!coop) return SGIPC_OK;
     MasWork& m = c->mas;
+    const int* h = m.h_info;
+    const int L = m.levelnum;
+    const int ndom = h[16] / 16;
+    const int nd01 = L > 2 ? h[2] / 16 : ndom;
+    // shared-memory residency with one CTA per SM: the static rows of each CTA's SpMV pass
+    // (when one pass covers all rows) first, then as many of its level-0/1 domain
+    // inverses as still fit (when one round covers them)
+    const void* fn = (const void*)k_pcg_coop<T, M, NR>;
+    cudaFuncAttributes fa;
+    SG_CHECK(c, cudaFuncGetAttributes(&fa, fn));
+    const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
+    constexpr int rpc = kCoopThreads / kSpG;
+    int ecap = 0, dcap = 0;
+    size_t dyn = 0;
+    if (budget > 0 && c->h_frow_ptr && c->n <= (long long)nsm * rpc) {
+        for (int b = 0; b * rpc < c->n; b++) {
+            const int r0 = b * rpc, r1 = r0 + rpc < c->n ? r0 + rpc : c->n;
+            const int e = c->h_frow_ptr[r1] - c->h_frow_ptr[r0];
+            if (e > ecap) ecap = e;
+        }
+        if ((long long)coop_rows_bytes(rpc, ecap, sizeof(T)) > budget) ecap = 0;
+    }
+    int kcap = 0;
+    if (ecap > 0 && (long long)(coop_rows_bytes(rpc, ecap, sizeof(T)) +
+                                coop_contact_bytes(rpc, kContactSlots, sizeof(T))) <= budget)
+        kcap = kContactSlots;
+    const size_t rows_bytes = coop_rows_bytes(rpc, ecap, sizeof(T)) + coop_contact_bytes(rpc, kcap, sizeof(T));
+    if (budget > 0 && nd01 <= (long long)nsm * kDomPerCta) {
+        long long left = budget - (long long)rows_bytes;
+        dcap = left > 0 ? (int)(left / (2304 * (long long)sizeof(M))) : 0;
+        if (dcap > kDomPerCta) dcap = kDomPerCta;
+    }
+    dyn = rows_bytes + (size_t)dcap * 2304 * sizeof(M);
+    if (dyn > 0) SG_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    SG_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_coop<T, M, NR>, kCoopThreads, dyn));
+    if (per < 1 && dyn > 0) {  // residency does not fit next to the kernel: run without it
+        ecap = kcap = dcap = 0;
+        dyn = 0;
+        SG_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_coop<T, M, NR>, kCoopThreads, 0));
+    }
+    if (per < 1) return SGIPC_OK;
+    if (per > kCoopMaxCtasPerSm) per = kCoopMaxCtasPerSm;
+    int grid = dyn > 0 ? nsm : nsm * per;  // residency assumes the one-CTA-per-SM mapping
+    if (grid > w.coop_cap) grid = w.coop_cap;
     CoopArgs<T, M, NR> a;
     a.tp = topo_of(c);
     a.A = mat_view<T>(c);
@@ -509,19 +761,19 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     a.partial = w.coop;
     a.br = {w.ticket + 4, w.ticket + 5};
     a.nv = c->nv;
-    const int* h = m.h_info;
-    const int L = m.levelnum;
-    a.ndom = h[16] / 16;
-    a.nd01 = L > 2 ? h[2] / 16 : a.ndom;
+    a.ndom = ndom;
+    a.nd01 = nd01;
     a.nd2 = L > 3 ? h[3] / 16 : a.ndom;
+    a.ecap = ecap;
+    a.kcap = kcap;
+    a.dcap = dcap;
     a.max_iter = max_iter;
     a.crit = crit;
     a.tol = tol;
     SG_CHECK(c, cudaMemsetAsync(w.ticket + 4, 0, 2 * sizeof(unsigned int), s));
     void* args[] = {&a};
     SG_COUNT(c, 1);
-    SG_CHECK(c, cudaLaunchCooperativeKernel((const void*)k_pcg_coop<T, M, NR>, dim3(grid), dim3(kCoopThreads), args,
-                                            0, s));
+    SG_CHECK(c, cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kCoopThreads), args, dyn, s));
     *used = true;
     return SGIPC_OK;
 }
