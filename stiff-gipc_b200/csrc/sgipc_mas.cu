@@ -221,50 +221,78 @@ __global__ void k_scatter_contact(int cap, const int* __restrict__ nuc, const in
     scatter_block_warp(dom, table, L, valid ? ur[u] : 0, valid ? uc[u] : 0, B, valid);
 }
 
-// Gauss-Jordan inversion without pivoting, one thread per column of a 48x48 domain held in
-// registers, four domains per 192-thread CTA; the pivot column is broadcast through shared
-// memory (double-buffered: one barrier per pivot step).  Column update for pivot k with
-// c = A(:,k), p = c[k]:  thread j != k:  f = A(k,j)/p;  A(i,j) -= c[i] f (i != k);  A(k,j) = f
-//                        thread k:       A(i,k) = -c[i]/p (i != k);  A(k,k) = 1/p
+// Gauss-Jordan inversion without pivoting, in place, one 48x48 domain per 192-thread CTA
+// with each thread holding a 4 x 3 tile in registers (rows 4 rg.., columns 3 cg..).  For
+// pivot k with p = A(k,k):  A(i,j) -= A(i,k) A(k,j) / p  (i, j != k);  A(k,j) = A(k,j) / p;
+// A(i,k) = -A(i,k) / p;  A(k,k) = 1 / p.  The pivot row, column and 1/p (computed once, by
+// the pivot's owner) are published through shared memory (double-buffered: one barrier per
+// step), so a thread reads 8 values and does 12 updates per step.  (Larger tiles, fewer
+// threads per domain, measured slower: the FP64 chain per step then dominates.)
 __global__ void __launch_bounds__(192) k_invert(int ndom, double* __restrict__ dom, float* __restrict__ dom32,
                                                 int write64, int write32) {
-    __shared__ double piv[2][4][48];
-    const int ld = threadIdx.x / 48, j = threadIdx.x % 48;
-    const int d = blockIdx.x * 4 + ld;
-    const bool act = d < ndom;
-    double col[48];
-    const double* D = dom + (size_t)(act ? d : 0) * 2304;
+    __shared__ double prow[2][48], pcol[2][48], pinv[2];
+    const int d = blockIdx.x;
+    if (d >= ndom) return;
+    const int rg = threadIdx.x / 16, cg = threadIdx.x % 16;
+    const int i0 = 4 * rg, j0 = 3 * cg;
+    const double* D = dom + (size_t)d * 2304;
+    double t[4][3];
 #pragma unroll
-    for (int i = 0; i < 48; i++) {
-        double a = act ? D[i * 48 + j] : (i == j ? 1.0 : 0.0);
-        col[i] = (i == j && a == 0.0) ? 1.0 : a;  // a zero diagonal (padding node) becomes 1
-    }
+    for (int a = 0; a < 4; a++)
 #pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const double v = D[(i0 + a) * 48 + j0 + b];
+            t[a][b] = (i0 + a == j0 + b && v == 0.0) ? 1.0 : v;  // a zero diagonal (padding node) becomes 1
+        }
+#pragma unroll 1
     for (int k = 0; k < 48; k++) {
-        double* pc = piv[k & 1][ld];
-        if (j == k) {
+        const int q = k & 1;
+        // publish row k, column k and 1 / A(k,k) as they are before this step
 #pragma unroll
-            for (int i = 0; i < 48; i++) pc[i] = col[i];
-        }
+        for (int a = 0; a < 4; a++)
+            if (k == i0 + a)
+#pragma unroll
+                for (int b = 0; b < 3; b++) {
+                    prow[q][j0 + b] = t[a][b];
+                    if (k == j0 + b) pinv[q] = 1.0 / t[a][b];
+                }
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+            if (k == j0 + b)
+#pragma unroll
+                for (int a = 0; a < 4; a++) pcol[q][i0 + a] = t[a][b];
         __syncthreads();
-        const double ip = 1.0 / pc[k];
-        if (j == k) {
+        const double ip = pinv[q];
+        double rk[3], ck[4];
 #pragma unroll
-            for (int i = 0; i < 48; i++) col[i] = (i == k) ? ip : -pc[i] * ip;
-        } else {
-            const double f = col[k] * ip;
+        for (int b = 0; b < 3; b++) rk[b] = prow[q][j0 + b] * ip;
 #pragma unroll
-            for (int i = 0; i < 48; i++) col[i] = (i == k) ? f : col[i] - pc[i] * f;
-        }
+        for (int a = 0; a < 4; a++) ck[a] = pcol[q][i0 + a];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) t[a][b] -= ck[a] * rk[b];
+        // the pivot row and column (a few threads) are set instead of updated
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+            if (k == i0 + a)
+#pragma unroll
+                for (int b = 0; b < 3; b++) t[a][b] = rk[b];
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+            if (k == j0 + b)
+#pragma unroll
+                for (int a = 0; a < 4; a++) t[a][b] = (k == i0 + a) ? ip : -ck[a] * ip;
     }
-    if (!act) return;
     double* Dw = dom + (size_t)d * 2304;
     float* Dw32 = dom32 + (size_t)d * 2304;
 #pragma unroll
-    for (int i = 0; i < 48; i++) {
-        if (write64) Dw[i * 48 + j] = col[i];
-        if (write32) Dw32[i * 48 + j] = (float)col[i];
-    }
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            if (write64) Dw[(i0 + a) * 48 + j0 + b] = t[a][b];
+            if (write32) Dw32[(i0 + a) * 48 + j0 + b] = (float)t[a][b];
+        }
 }
 
 }  // namespace
@@ -468,7 +496,7 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     k_scatter_contact<<<nblk(c->cap_cblk), SGIPC_BLOCK, 0, s>>>(c->cap_cblk, c->nuc, c->uc_row, c->uc_col, c->uc64,
                                                                m.table, L, m.dom64);
     const int w64 = prec == SGIPC_FP64 ? 1 : 0, w32 = prec == SGIPC_FP64 ? 0 : 1;
-    k_invert<<<(ndom + 3) / 4, 192, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
+    k_invert<<<ndom, 192, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
     SG_LAUNCH_CHECK(c, "mas matrices");
     m.built = (int)prec + 1;
     return SGIPC_OK;
@@ -503,7 +531,7 @@ SgipcStatus mas_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
                                                                m.dom64);
         *bytes = (double)c->nnz * (72 + 8) + (double)c->nv * L * 4 + (double)ndom * 2304 * 8;
     } else if (!strcmp(name, "mas_invert")) {
-        k_invert<<<(ndom + 3) / 4, 192, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);
+        k_invert<<<ndom, 192, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);
         *bytes = (double)ndom * 2304 * (8 + 8 + 4);
     } else if (!strcmp(name, "mas_domain64") || !strcmp(name, "mas_domain32")) {
         const bool f32 = name[10] == '3';

@@ -784,8 +784,11 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         out.rz0 = rz0;
         out.rz = rz;
         out.status = status;
+        // the last refinement computed r = b - A x in FP64 and ||r||^2 (h_pinned[1]);
+        // ||b||^2 is the first inner solve's right-hand side norm
+        out.rel_residual = bn2 > 0.0 ? sqrt(c->h_pinned[1] / bn2) : 0.0;
     }
-    if ((st = true_residual(c, b, x, &out.rel_residual, s)) != SGIPC_OK) return st;
+    if (prec != SGIPC_MIXED && (st = true_residual(c, b, x, &out.rel_residual, s)) != SGIPC_OK) return st;
     if (stats) *stats = out;
     return (SgipcStatus)out.status;
 }
