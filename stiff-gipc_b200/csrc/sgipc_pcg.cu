@@ -712,6 +712,16 @@ static SgipcStatus true_residual(SgipcCtx* c, const double* b, const double* x, 
     return SGIPC_OK;
 }
 
+// pinned host word for the device input-error flag, read with a solve's final copies
+static int* input_flag(SgipcCtx* c) { return reinterpret_cast<int*>(c->h_pinned + 32); }
+
+static SgipcStatus input_error(SgipcCtx* c, cudaStream_t s) {
+    *input_flag(c) = 0;
+    SG_CHECK(c, cudaMemsetAsync(c->dflag, 0, sizeof(int), s));
+    snprintf(c->err, sizeof(c->err), "a contact pair names a vertex outside [0, vertex_num); it was skipped");
+    return SGIPC_BAD_INPUT;
+}
+
 static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion crit, double tol, int max_iter,
                              const double* b, double* x, SgipcSolveStats* stats, cudaStream_t s) {
     const int n3 = 3 * c->n;
@@ -729,7 +739,9 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         SG_CHECK(c, cudaMemcpyAsync(x, c->pcg64.x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
         PcgScalars hs;
         SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg64.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        SG_CHECK(c, cudaMemcpyAsync(input_flag(c), c->dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
         SG_CHECK(c, cudaStreamSynchronize(s));
+        if (*input_flag(c)) return input_error(c, s);
         SG_COUNT(c, 4LL * hs.bodies);
         out.iterations = hs.iter;
         out.refinements = 0;
@@ -761,7 +773,9 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
             if ((st = dot64(c, r64, c->tmp64b, n3, c->dot_out, s)) != SGIPC_OK) return st;
             if ((st = dot64(c, r64, r64, n3, c->dot_out + 1, s)) != SGIPC_OK) return st;
             SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            SG_CHECK(c, cudaMemcpyAsync(input_flag(c), c->dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
             SG_CHECK(c, cudaStreamSynchronize(s));
+            if (*input_flag(c)) return input_error(c, s);
             total_it += hs.iter;
             SG_COUNT(c, 4LL * hs.bodies);
             if (ref == 0) {
@@ -801,8 +815,8 @@ extern "C" SgipcStatus sgipc_pcg_solve(SgipcCtx* c, SgipcPrecision prec, SgipcCr
     SG_CHECK(c, cudaSetDevice(c->device));
     // the MAS inverses must exist in the precision the solve reads
     if ((prec == SGIPC_FP64) != (c->mas.built == SGIPC_FP64 + 1)) return SGIPC_NOT_READY;
-    SgipcStatus fs = check_device_flag(c, (cudaStream_t)stream);
-    if (fs != SGIPC_OK) return fs;
+    // a contact pair with an out-of-range vertex (flagged by the assembly kernels) is
+    // reported from the solve's own synchronisation, not from an extra one here
     return solve_one(c, prec, crit, tol, max_iter, b, x, stats, (cudaStream_t)stream);
 }
 

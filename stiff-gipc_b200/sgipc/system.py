@@ -73,14 +73,41 @@ class DeviceTetraData:
         self.fric_gd_pairs = _t(sc.fric_gd_pairs, i32)
         self.fric_gd_lambda = _t(sc.fric_gd_lambda, f64)
 
+    # The C structs hold raw device pointers; they are rebuilt only after an attribute of
+    # this object is (re)assigned -- in-place updates (copy_) keep the pointers valid.
+    def __setattr__(self, name, value):
+        object.__setattr__(self, name, value)
+        if not name.startswith("_"):
+            object.__setattr__(self, "_structs", {})
+
+    def _cached(self, key, build):
+        cache = self.__dict__.setdefault("_structs", {})
+        if key not in cache:
+            cache[key] = build()
+        return cache[key]
+
     def fem_struct(self) -> N.SgipcFemData:
+        return self._fem_struct()
+
+    def contact_struct(self) -> N.SgipcContacts:
+        return self._contact_struct()
+
+    def fem_struct_cached(self) -> N.SgipcFemData:
+        """Shared struct for the library's own calls (never modify it)."""
+        return self._cached("fem", self._fem_struct)
+
+    def contact_struct_cached(self) -> N.SgipcContacts:
+        """Shared struct for the library's own calls (never modify it)."""
+        return self._cached("con", self._contact_struct)
+
+    def _fem_struct(self) -> N.SgipcFemData:
         f = N.SgipcFemData()
         for name in ("vertexes", "o_vertexes", "rest_vertexes", "xTilta", "masses", "BoundaryType", "DmInverses",
                      "volum", "lengthRate", "volumeRate", "triDmInverses", "area", "quad_bending_Q", "targetVert"):
             setattr(f, name, _p(getattr(self, name)))
         return f
 
-    def contact_struct(self) -> N.SgipcContacts:
+    def _contact_struct(self) -> N.SgipcContacts:
         k = N.SgipcContacts()
         k.pairs, k.pair_num = _p(self.pairs), self.pairs.shape[0]
         k.ground_pairs, k.ground_num = _p(self.ground_pairs), self.ground_pairs.shape[0]
@@ -162,9 +189,15 @@ class GIPC:
             pass
 
     # ---- assembly -------------------------------------------------------------------
+    def _params(self):
+        key = tuple(sorted(self.params.items()))
+        if getattr(self, "_prm_key", None) != key:
+            self._prm_key, self._prm_cached = key, params_struct(self.params)
+        return self._prm_cached
+
     def computeGradientAndHessian(self, tet: Optional[DeviceTetraData] = None):
         tet = tet or self.tet
-        self._fem, self._con, self._prm = tet.fem_struct(), tet.contact_struct(), params_struct(self.params)
+        self._fem, self._con, self._prm = tet.fem_struct_cached(), tet.contact_struct_cached(), self._params()
         N.check(N.lib().sgipc_assemble(self.ctx, C.byref(self._fem), C.byref(self._con), C.byref(self._prm),
                                        _stream()), self.ctx)
 
@@ -225,7 +258,7 @@ class GIPC:
         """MAS build + PCG; fills ``self.moveDir`` (dx of A dx = b) and returns the stats."""
         config = config or PCGSolverConfig()
         tet = tet or self.tet
-        con = tet.contact_struct()
+        con = tet.contact_struct_cached()
         st = N.SgipcSolveStats()
         prec = N.PRECISION[config.precision]
         max_iter = int(config.max_iter_ratio * 3 * self.n)

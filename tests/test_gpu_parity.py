@@ -8,6 +8,8 @@ Tolerances (FP64 unless stated):
   * MAS hierarchy: identical integer tables; MAS apply: 1e-9 (FP64), 2e-5 (FP32 inverses);
   * PCG: same iteration count within 1, solution within 1e-6 relative of the oracle's.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -77,7 +79,6 @@ def test_mas_hierarchy_and_apply(case):
         assert _rel(gd[d], od[d]) < 1e-9, d
     r = np.random.default_rng(1).normal(size=3 * sc.nv)
     # restriction operator: R[g] = sum of r over the vertices of cluster g, every level
-    import ctypes
     R = np.zeros(3 * total)
     rt = torch.tensor(r, device="cuda")
     N.check(N.lib().sgipc_mas_restrict(g.ctx, ctypes.c_void_p(rt.data_ptr()), R.ctypes.data_as(ctypes.c_void_p)))
@@ -192,7 +193,6 @@ def test_iteration_cap_reports_not_converged(case):
     mas = system.MASPreconditioner(g)
     mas.setPreconditioner("fp64")
     L = N.lib()
-    import ctypes
     b = g.rhs()
     x = torch.empty_like(b)
     for graph in (False, True):
@@ -223,6 +223,20 @@ def test_bad_inputs_are_reported(case):
     k = g.tet.contact_struct()
     k.pair_num = 10 ** 7
     assert L.sgipc_assemble(g.ctx, f, k, prm, None) == N.CAPACITY
+    # a pair naming a vertex outside the mesh: skipped by the assembly, reported by the solve
+    if len(sc.pairs):
+        pairs = g.tet.pairs.clone()
+        pairs[0, 1] = 10 ** 6
+        k = g.tet.contact_struct()
+        k.pairs = system._p(pairs)
+        assert L.sgipc_assemble(g.ctx, f, k, prm, None) == N.OK
+        st = N.SgipcSolveStats()
+        dx = torch.empty(3 * sc.nv, dtype=torch.float64, device="cuda")
+        assert L.sgipc_solve(g.ctx, k, N.FP64, N.CRIT_RZ, 1e-4, 0, system._p(dx), ctypes.byref(st), None) \
+            == N.BAD_INPUT
+        assert b"outside" in L.sgipc_last_error(g.ctx)
     # the context stays usable
     g.computeGradientAndHessian()
+    st = g.calculateMovingDirection(system.PCGSolverConfig(precision="fp64"))
+    assert st.status == N.OK
     torch.cuda.synchronize()
