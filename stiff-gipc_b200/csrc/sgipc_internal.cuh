@@ -62,6 +62,8 @@ struct MasWork {
     int* real_map;           // [nv]
     int* nbr_ptr;            // [nv+1] mesh neighbour CSR
     int* nbr;                // [nnz]
+    int* nbr_row;            // [nnz] vertex of each neighbour slot
+    int nnbr;                // nnz
     int* table;              // [nv * levelnum] global cluster per level (level 0 = position)
     int* up;                 // [total_cap] global id of each cluster's parent at the next level (-1: none)
     int* node;               // [nv] node id at the level being built

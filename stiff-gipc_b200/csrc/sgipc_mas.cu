@@ -26,10 +26,6 @@ using namespace sgipc;
 
 namespace {
 
-__device__ __forceinline__ void mask_edge(uint32_t* mask, int a, int b) {
-    if (a != b && (a >> 4) == (b >> 4)) atomicOr(mask + a, 1u << (b & 15));
-}
-
 __global__ void k_init_level0(int nv, const int* __restrict__ real_map, int L, int* __restrict__ node,
                               int* __restrict__ table, int* __restrict__ info, int npos, int* __restrict__ up) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -45,21 +41,36 @@ __global__ void k_init_level0(int nv, const int* __restrict__ real_map, int L, i
     table[(size_t)v * L] = p;
 }
 
-__global__ void k_mask_edges(int nv, const int* __restrict__ ptr, const int* __restrict__ nbr,
+// OR `bit` into mask[a]; lanes of a warp with the same target combine their bits first
+// (at coarse levels most edges of a warp land on the same few nodes)
+__device__ __forceinline__ void mask_or_warp(uint32_t* mask, int a, uint32_t bit) {
+    const unsigned grp = __match_any_sync(0xffffffffu, a);
+    const uint32_t bits = __reduce_or_sync(grp, bit);
+    if (a >= 0 && bits && (int)(threadIdx.x & 31) == __ffs(grp) - 1) atomicOr(mask + a, bits);
+}
+
+// one thread per neighbour-list slot (row[k] is the slot's vertex)
+__global__ void k_mask_edges(int nnz, const int* __restrict__ row, const int* __restrict__ nbr,
                              const int* __restrict__ node, uint32_t* __restrict__ mask) {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= nv) return;
-    int a = node[v];
-    for (int k = ptr[v]; k < ptr[v + 1]; k++) mask_edge(mask, a, node[nbr[k]]);
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int a = -1;
+    uint32_t bit = 0;
+    if (k < nnz) {
+        a = node[row[k]];
+        const int b = node[nbr[k]];
+        if (a != b && (a >> 4) == (b >> 4)) bit = 1u << (b & 15);
+    }
+    mask_or_warp(mask, bit ? a : -1, bit);
 }
 
 __global__ void k_mask_pairs(int np, const int4* __restrict__ pairs, int nv, const int* __restrict__ node,
                              uint32_t* __restrict__ mask) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    int4 e = pairs[p];
-    int v[4], n = 0;
-    if (e.x >= 0) {
+    int v[4] = {-1, -1, -1, -1}, n = 0;
+    const int4 e = p < np ? pairs[p] : make_int4(0, 0, 0, 0);
+    if (p >= np) {
+        // idle lane: no vertices, but it still joins the warp-wide ORs below
+    } else if (e.x >= 0) {
         v[0] = e.x; v[1] = e.y; v[2] = e.z; v[3] = e.w < 0 ? -e.w - 1 : e.w; n = 4;
     } else {
         v[0] = -e.x - 1;
@@ -71,62 +82,50 @@ __global__ void k_mask_pairs(int np, const int4* __restrict__ pairs, int nv, con
             else { v[1] = e.y; v[2] = e.z; n = 3; }
         } else { v[1] = e.y; v[2] = e.z; v[3] = e.w; n = 4; }
     }
-    int a[4];
+    int a[4] = {-1, -1, -1, -1};
     for (int i = 0; i < n; i++) a[i] = (v[i] >= 0 && v[i] < nv) ? node[v[i]] : -1;
-    for (int i = 0; i < n; i++)
-        for (int j = i + 1; j < n; j++)
-            if (a[i] >= 0 && a[j] >= 0) {
-                mask_edge(mask, a[i], a[j]);
-                mask_edge(mask, a[j], a[i]);
-            }
+    // the 12 ordered vertex pairs, each one warp-aggregated OR
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (i == j) continue;
+            const int x = a[i], y = a[j];
+            const bool on = x >= 0 && y >= 0 && x != y && (x >> 4) == (y >> 4);
+            mask_or_warp(mask, on ? x : -1, on ? 1u << (y & 15) : 0u);
+        }
 }
 
-// One thread per bank: components by repeated OR closure, numbered by lowest lane.  At
-// level 0 the padding positions (part_map < 0) are no node and form no component
-// (_preparePrefixSumL0_new / _buildLevel1_new skip them, MASPreconditioner.cu:157-270).
+// Half a warp per bank, lane i holding node i's connectivity row: components by repeated
+// squaring of the reachability rows (each round doubles the path length, so five rounds
+// close 16 nodes), numbered by their lowest lane.  At level 0 the padding positions
+// (part_map < 0) are no node and form no component (_preparePrefixSumL0_new /
+// _buildLevel1_new skip them, MASPreconditioner.cu:157-270).
 __global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, int level,
                                   const uint32_t* __restrict__ mask, const int* __restrict__ part_map,
                                   int* __restrict__ rank, int* __restrict__ bank_cnt) {
-    int bk = blockIdx.x * blockDim.x + threadIdx.x;
-    if (bk > nbank_cap) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int bk = gt >> 4, i = gt & 15;
     const int count = info[8 + level];
     const int nbank = (count + 15) >> 4;
-    if (bk >= nbank) {
-        bank_cnt[bk] = 0;
-        return;
-    }
-    const int lo = bk << 4, hi = min(count, lo + 16);
-    uint32_t comp[16];
+    const int lo = bk << 4;
+    const bool inb = bk < nbank;
+    const bool real = inb && lo + i < count && (level > 0 || part_map[lo + i] >= 0);
+    uint32_t m = real ? (mask[lo + i] | (1u << i)) : 0u;
+#pragma unroll 1
+    for (int it = 0; it < 5; it++) {
+        uint32_t acc = m;
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const bool real = lo + i < hi && (level > 0 || part_map[lo + i] >= 0);
-        comp[i] = real ? (mask[lo + i] | (1u << i)) : 0u;
-    }
-    for (int it = 0; it < 16; it++) {
-        bool changed = false;
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            uint32_t m = comp[i], acc = m;
-#pragma unroll
-            for (int j = 0; j < 16; j++)
-                if (m & (1u << j)) acc |= comp[j];
-            if (acc != m) {
-                comp[i] = acc;
-                changed = true;
-            }
+        for (int j = 0; j < 16; j++) {
+            const uint32_t mj = __shfl_sync(0xffffffffu, m, j, 16);
+            if (m & (1u << j)) acc |= mj;
         }
-        if (!changed) break;
+        m = acc;
     }
-    // leaders: lowest lane of their component; rank = number of leaders below
-    uint32_t leaders = 0;
-#pragma unroll
-    for (int i = 0; i < 16; i++)
-        if (lo + i < hi && (__ffs(comp[i]) - 1) == i) leaders |= 1u << i;
-    for (int i = 0; i < hi - lo; i++) {
-        int lead = __ffs(comp[i]) - 1;
-        rank[lo + i] = lead < 0 ? 0 : __popc(leaders & ((1u << lead) - 1u));
-    }
-    bank_cnt[bk] = __popc(leaders);
+    const int lead = __ffs(m) - 1;
+    const uint32_t leaders = (__ballot_sync(0xffffffffu, real && lead == i) >> (threadIdx.x & 16)) & 0xffffu;
+    if (inb && lo + i < count) rank[lo + i] = lead < 0 ? 0 : __popc(leaders & ((1u << lead) - 1u));
+    if (i == 0 && bk <= nbank_cap) bank_cnt[bk] = inb ? __popc(leaders) : 0;
 }
 
 __global__ void k_assign(int nv, int L, int level, const int* __restrict__ bank_off, const int* __restrict__ rank,
@@ -412,17 +411,21 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
         if (pm[i] >= nv) return SGIPC_BAD_INPUT;
     for (int v = 0; v < nv; v++)
         if (rm[v] < 0 || rm[v] >= m.npos || pm[rm[v]] != v) return SGIPC_BAD_INPUT;
-    std::vector<int> ptr(nv + 1), nb(t->neighborStart[nv]);
+    std::vector<int> ptr(nv + 1), nb(t->neighborStart[nv]), nrow(t->neighborStart[nv]);
     for (int i = 0; i <= nv; i++) ptr[i] = (int)t->neighborStart[i];
     for (size_t k = 0; k < nb.size(); k++) {
         nb[k] = (int)t->neighborList[k];
         if (nb[k] < 0 || nb[k] >= nv) return SGIPC_BAD_INPUT;
     }
+    for (int v = 0; v < nv; v++)
+        for (int k = ptr[v]; k < ptr[v + 1]; k++) nrow[k] = v;
+    m.nnbr = (int)nb.size();
     const size_t ndom_cap = (size_t)m.total_cap / 16;
     const size_t rhs = (size_t)c->max_rhs;
     auto A = [&](void** p, size_t bytes) -> bool { return cudaMalloc(p, bytes ? bytes : 4) == cudaSuccess; };
     if (!A((void**)&m.part_map, sizeof(int) * m.npos) || !A((void**)&m.real_map, sizeof(int) * nv) ||
         !A((void**)&m.nbr_ptr, sizeof(int) * (nv + 1)) || !A((void**)&m.nbr, sizeof(int) * nb.size()) ||
+        !A((void**)&m.nbr_row, sizeof(int) * nb.size()) ||
         !A((void**)&m.table, sizeof(int) * (size_t)nv * m.levelnum) || !A((void**)&m.node, sizeof(int) * nv) ||
         !A((void**)&m.up, sizeof(int) * (size_t)m.total_cap) ||
         !A((void**)&m.mask, sizeof(uint32_t) * m.npos) || !A((void**)&m.comp_rank, sizeof(int) * m.npos) ||
@@ -440,6 +443,7 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
     SG_CHECK(c, cudaMemcpy(m.real_map, rm.data(), sizeof(int) * nv, cudaMemcpyHostToDevice));
     SG_CHECK(c, cudaMemcpy(m.nbr_ptr, ptr.data(), sizeof(int) * (nv + 1), cudaMemcpyHostToDevice));
     if (!nb.empty()) SG_CHECK(c, cudaMemcpy(m.nbr, nb.data(), sizeof(int) * nb.size(), cudaMemcpyHostToDevice));
+    if (!nb.empty()) SG_CHECK(c, cudaMemcpy(m.nbr_row, nrow.data(), sizeof(int) * nb.size(), cudaMemcpyHostToDevice));
     SG_CHECK(c, cudaMemset(m.R64, 0, sizeof(double) * 3 * m.total_cap * rhs));
     SG_CHECK(c, cudaMemset(m.R32, 0, sizeof(float) * 3 * m.total_cap * rhs));
     SG_CHECK(c, cudaMemset(m.info, 0, sizeof(int) * 32));
@@ -452,7 +456,7 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
 
 void mas_destroy(SgipcCtx* c) {
     MasWork& m = c->mas;
-    void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.table, m.up, m.node, m.mask, m.comp_rank, m.bank_cnt,
+    void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.nbr_row, m.table, m.up, m.node, m.mask, m.comp_rank, m.bank_cnt,
                     m.bank_off, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32, m.scan_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -468,13 +472,12 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     SG_COUNT(c, 1 + (L - 1) * (3 + (con && con->pair_num > 0)) + 3);
     for (int l = 0; l + 1 < L; l++) {
         SG_CHECK(c, cudaMemsetAsync(m.mask, 0, sizeof(uint32_t) * m.npos, s));
-        k_mask_edges<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, m.nbr_ptr, m.nbr, m.node, m.mask);
+        if (m.nnbr > 0) k_mask_edges<<<nblk(m.nnbr), SGIPC_BLOCK, 0, s>>>(m.nnbr, m.nbr_row, m.nbr, m.node, m.mask);
         if (con && con->pair_num > 0)
             k_mask_pairs<<<nblk(con->pair_num), SGIPC_BLOCK, 0, s>>>(con->pair_num, (const int4*)con->pairs, nv,
                                                                      m.node, m.mask);
-        k_bank_components<<<nblk(nbank_cap + 1, 128), 128, 0, s>>>(nbank_cap, m.info, l, m.mask, m.part_map,
-                                                                   m.comp_rank,
-                                                                   m.bank_cnt);
+        k_bank_components<<<nblk(16LL * (nbank_cap + 1), 128), 128, 0, s>>>(nbank_cap, m.info, l, m.mask, m.part_map,
+                                                                           m.comp_rank, m.bank_cnt);
         size_t tb = m.scan_tmp_bytes;
         SG_CHECK(c, cub::DeviceScan::ExclusiveSum(m.scan_tmp, tb, m.bank_cnt, m.bank_off, nbank_cap + 1, s));
         k_assign<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, L, l, m.bank_off, m.comp_rank, m.node, m.table, m.info, m.up);
