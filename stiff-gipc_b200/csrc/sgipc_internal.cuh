@@ -213,6 +213,37 @@ __device__ __forceinline__ T ldv(const T* p) {
         return *p;
 }
 
+// The NR right-hand-side values of one (row, component) are contiguous ([(3 v + q) * NR + r]):
+// four floats move as one 16-byte access, four doubles as two (the arrays are allocation-
+// aligned and 3 v + q steps by 16 or 32 bytes); other widths move as scalars.
+template <bool kL2, class T, int NR>
+__device__ __forceinline__ void ldn(const T* p, T (&v)[NR]) {
+    if constexpr (NR == 4 && sizeof(T) == 4) {
+        const float4 q = kL2 ? __ldcg(reinterpret_cast<const float4*>(p)) : *reinterpret_cast<const float4*>(p);
+        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+    } else if constexpr (NR == 4 && sizeof(T) == 8) {
+        const double2* d = reinterpret_cast<const double2*>(p);
+        const double2 q0 = kL2 ? __ldcg(d) : d[0], q1 = kL2 ? __ldcg(d + 1) : d[1];
+        v[0] = q0.x, v[1] = q0.y, v[2] = q1.x, v[3] = q1.y;
+    } else {
+#pragma unroll
+        for (int r = 0; r < NR; r++) v[r] = ldv<kL2>(p + r);
+    }
+}
+
+template <class T, int NR>
+__device__ __forceinline__ void stn(T* p, const T (&v)[NR]) {
+    if constexpr (NR == 4 && sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (NR == 4 && sizeof(T) == 8) {
+        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int r = 0; r < NR; r++) p[r] = v[r];
+    }
+}
+
 inline int nblk(long long n, int b = SGIPC_BLOCK) { return (int)((n + b - 1) / b); }
 
 // count `k` kernel launches of this library on the context

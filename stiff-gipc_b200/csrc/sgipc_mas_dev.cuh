@@ -33,9 +33,12 @@ __device__ __forceinline__ void bank_reduce_store(int parent, const M (&v)[NR * 
     }
     if (parent >= 0 && (int)(threadIdx.x & 15) == leader) {
 #pragma unroll
-        for (int q = 0; q < 3; q++)
+        for (int q = 0; q < 3; q++) {
+            M o[NR];
 #pragma unroll
-            for (int r = 0; r < NR; r++) R[(size_t)(3 * parent + q) * NR + r] = s[r * 3 + q];
+            for (int r = 0; r < NR; r++) o[r] = s[r * 3 + q];
+            stn<M, NR>(R + (size_t)(3 * parent + q) * NR, o);
+        }
     }
 }
 
@@ -55,9 +58,12 @@ __device__ __forceinline__ void restrict_coarse_cta(const int* __restrict__ info
                 const int g = start + a;
                 par = up[g];
 #pragma unroll
-                for (int q = 0; q < 3; q++)
+                for (int q = 0; q < 3; q++) {
+                    M t[NR];
+                    ldn<kL2, M, NR>(R + (size_t)(3 * g + q) * NR, t);
 #pragma unroll
-                    for (int r = 0; r < NR; r++) v[r * 3 + q] = ldv<kL2>(R + (size_t)(3 * g + q) * NR + r);
+                    for (int r = 0; r < NR; r++) v[r * 3 + q] = t[r];
+                }
             } else {
 #pragma unroll
                 for (int k = 0; k < NR * 3; k++) v[k] = 0;

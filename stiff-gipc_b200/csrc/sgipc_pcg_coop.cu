@@ -168,6 +168,18 @@ __device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, double (&
 __device__ __forceinline__ int grid_warp() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
 __device__ __forceinline__ int grid_warps() { return (int)((gridDim.x * blockDim.x) >> 5); }
 
+// R at MAS position p (level 0) from the per-(rhs, component) values val[r * 3 + q]
+template <class M, int NR>
+__device__ __forceinline__ void store_levels01(M* R, int p, const M (&val)[NR * 3]) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        M o[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) o[r] = val[r * 3 + q];
+        stn<M, NR>(R + (size_t)(3 * p + q) * NR, o);
+    }
+}
+
 // r = b, x = 0, R (levels 0 and 1) = restriction of r, ||b||^2
 template <class T, class M, int NR>
 __device__ void phase_init(const CoopArgs<T, M, NR>& a, double (&bb)[NR]) {
@@ -181,22 +193,23 @@ __device__ void phase_init(const CoopArgs<T, M, NR>& a, double (&bb)[NR]) {
         for (int k = 0; k < NR * 3; k++) val[k] = 0;
         if (v >= 0) {
 #pragma unroll
-            for (int r = 0; r < NR; r++)
+            for (int q = 0; q < 3; q++) {
+                const size_t k = (size_t)(3 * v + q) * NR;
+                double bv[NR];
+                ldn<false, double, NR>(a.b + k, bv);
+                T tr[NR], tx[NR];
 #pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    const size_t k = (size_t)(3 * v + q) * NR + r;
-                    const double bv = a.b[k];
-                    a.r[k] = (T)bv;
-                    a.x[k] = 0;
-                    val[r * 3 + q] = (M)(T)bv;
-                    bb[r] += bv * bv;
+                for (int r = 0; r < NR; r++) {
+                    tr[r] = (T)bv[r];
+                    tx[r] = 0;
+                    val[r * 3 + q] = (M)tr[r];
+                    bb[r] += bv[r] * bv[r];
                 }
+                stn<T, NR>(a.r + k, tr);
+                stn<T, NR>(a.x + k, tx);
+            }
         }
-        if (p < mv.npos)
-#pragma unroll
-            for (int q = 0; q < 3; q++)
-#pragma unroll
-                for (int r = 0; r < NR; r++) a.R[(size_t)(3 * p + q) * NR + r] = val[r * 3 + q];
+        if (p < mv.npos) store_levels01<M, NR>(a.R, p, val);
         bank_reduce_store<M, NR>(v >= 0 ? mv.up[p] : -1, val, a.R);
     }
 }
@@ -209,9 +222,11 @@ __device__ __forceinline__ void solve_domains(const M* __restrict__ inv, const M
     const int ld = threadIdx.x / 48, i = threadIdx.x % 48;
     const int d = d0 + ld;
     const bool act = ld < kDomPerCta && d < hi;
-    if (act)
-#pragma unroll
-        for (int r = 0; r < NR; r++) sR[ld][i * NR + r] = __ldcg(R + (48 * (size_t)d + i) * NR + r);
+    if (act) {
+        M t[NR];
+        ldn<true, M, NR>(R + (48 * (size_t)d + i) * NR, t);
+        stn<M, NR>(&sR[ld][i * NR], t);
+    }
     __syncthreads();
     if (act) {
         const bool sm = ld < ncached;  // this slot's inverse is resident in shared memory
@@ -226,12 +241,14 @@ __device__ __forceinline__ void solve_domains(const M* __restrict__ inv, const M
 #pragma unroll
             for (int j = 0; j < kU; j++) w[j] = sm ? Ad[(j0 + j) * 48 + i] : __ldg(Ad + (j0 + j) * 48 + i);
 #pragma unroll
-            for (int j = 0; j < kU; j++)
+            for (int j = 0; j < kU; j++) {
+                M rj[NR];
+                ldn<false, M, NR>(&sR[ld][(j0 + j) * NR], rj);
 #pragma unroll
-                for (int r = 0; r < NR; r++) acc[r] += w[j] * sR[ld][(j0 + j) * NR + r];
+                for (int r = 0; r < NR; r++) acc[r] += w[j] * rj[r];
+            }
         }
-#pragma unroll
-        for (int r = 0; r < NR; r++) Z[(48 * (size_t)d + i) * NR + r] = acc[r];
+        stn<M, NR>(Z + (48 * (size_t)d + i) * NR, acc);
     }
     __syncthreads();
 }
@@ -264,9 +281,12 @@ __device__ void restrict_level1(const MasView& mv, M* R) {
             const int g = start + aa;
             par = mv.up[g];
 #pragma unroll
-            for (int q = 0; q < 3; q++)
+            for (int q = 0; q < 3; q++) {
+                M t[NR];
+                ldn<true, M, NR>(R + (size_t)(3 * g + q) * NR, t);
 #pragma unroll
-                for (int r = 0; r < NR; r++) v[r * 3 + q] = __ldcg(R + (size_t)(3 * g + q) * NR + r);
+                for (int r = 0; r < NR; r++) v[r * 3 + q] = t[r];
+            }
         } else {
 #pragma unroll
             for (int k = 0; k < NR * 3; k++) v[k] = 0;
@@ -304,24 +324,35 @@ __device__ void phase_prolong(const CoopArgs<T, M, NR>& a, const bool (&run)[NR]
         int gl[SGIPC_MAX_LEVELS];
 #pragma unroll
         for (int l = 0; l < SGIPC_MAX_LEVELS; l++) gl[l] = l < mv.L ? __ldg(tv + l) : -1;
+        // every right-hand side is summed and stored (vector accesses); a stopped one's z
+        // is never used, and only running ones add to r.z
+        M sq[3][NR];
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
-            if (!run[r]) continue;
-            M s0 = 0, s1 = 0, s2 = 0;
+        for (int q = 0; q < 3; q++)
 #pragma unroll
-            for (int l = 0; l < SGIPC_MAX_LEVELS; l++) {
-                if (gl[l] < 0) continue;
-                s0 += a.Z[(size_t)(3 * gl[l]) * NR + r];  // coarse clusters are shared: L1 reuse
-                s1 += a.Z[(size_t)(3 * gl[l] + 1) * NR + r];
-                s2 += a.Z[(size_t)(3 * gl[l] + 2) * NR + r];
-            }
-            const T zz[3] = {(T)s0, (T)s1, (T)s2};
+            for (int r = 0; r < NR; r++) sq[q][r] = 0;
+#pragma unroll
+        for (int l = 0; l < SGIPC_MAX_LEVELS; l++) {
+            if (gl[l] < 0) continue;
 #pragma unroll
             for (int q = 0; q < 3; q++) {
-                const size_t k = (size_t)(3 * v + q) * NR + r;
-                a.z[k] = zz[q];
-                rz[r] += (double)__ldcg(a.r + k) * (double)zz[q];
+                M t[NR];
+                ldn<false, M, NR>(a.Z + (size_t)(3 * gl[l] + q) * NR, t);  // coarse clusters are shared: L1 reuse
+#pragma unroll
+                for (int r = 0; r < NR; r++) sq[q][r] += t[r];
             }
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const size_t k = (size_t)(3 * v + q) * NR;
+            T zz[NR], rv[NR];
+            ldn<true, T, NR>(a.r + k, rv);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                zz[r] = (T)sq[q][r];
+                if (run[r]) rz[r] += (double)rv[r] * (double)zz[r];
+            }
+            stn<T, NR>(a.z + k, zz);
         }
     }
 }
@@ -358,7 +389,7 @@ __device__ __forceinline__ void row_mv_resident(const Topo& tp, const MatView<T>
         const int u0 = rc.ru[li], nu = rc.ru[li + 1] - u0;
         const int l0 = rc.rl[li], nl = rc.rl[li + 1] - l0;
         const int len = ns + nu + nl;
-        constexpr int kB = NR == 1 ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 2 : 1);
+        constexpr int kB = NR == 1 ? (sizeof(T) == 4 ? 4 : 2) : 1;
         for (int e0 = g; e0 < len; e0 += kB * kSpG) {
             int cj[kB];
             const T* bp[kB];
@@ -400,7 +431,7 @@ __device__ __forceinline__ void row_mv_resident(const Topo& tp, const MatView<T>
         const int k0 = tp.cl_ptr[i], k1 = tp.cl_ptr[i + 1];
         const int li = i - rc.r0;
         const int s0 = rc.rp[li], s1 = rc.rp[li + 1];
-        constexpr int kB = NR == 1 ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 2 : 1);
+        constexpr int kB = NR == 1 ? (sizeof(T) == 4 ? 4 : 2) : 1;
         for (int e0 = s0 + g; e0 < s1; e0 += kB * kSpG) {
             int cj[kB];
             T xb[kB][NR][3];
@@ -472,15 +503,17 @@ __device__ void phase_spmv(const CoopArgs<T, M, NR>& a, bool first, const double
             row_mv<T, NR>(a.tp, a.A, op, i, g, acc);
         if (i < n && g == 0) {
 #pragma unroll
-            for (int r = 0; r < NR; r++) {
-                if (!run[r]) continue;
+            for (int q = 0; q < 3; q++) {
+                const size_t k = (size_t)(3 * i + q) * NR;
+                T pv[NR], av[NR];
 #pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    const size_t k = (size_t)(3 * i + q) * NR + r;
-                    pnew[k] = pi[r][q];
-                    a.Ap[k] = acc[r][q];
-                    pAp[r] += (double)pi[r][q] * (double)acc[r][q];
+                for (int r = 0; r < NR; r++) {
+                    pv[r] = pi[r][q];
+                    av[r] = acc[r][q];
+                    if (run[r]) pAp[r] += (double)pi[r][q] * (double)acc[r][q];
                 }
+                stn<T, NR>(pnew + k, pv);
+                stn<T, NR>(a.Ap + k, av);
             }
         }
     }
@@ -500,40 +533,55 @@ __device__ void phase_update(const CoopArgs<T, M, NR>& a, const double (&alpha)[
         for (int k = 0; k < NR * 3; k++) val[k] = 0;
         if (v >= 0) {
 #pragma unroll
-            for (int r = 0; r < NR; r++) {
-                if (!run[r]) continue;
-                const T al = (T)alpha[r];
+            for (int q = 0; q < 3; q++) {
+                const size_t k = (size_t)(3 * v + q) * NR;
+                T xv[NR], pv[NR], rv[NR], av[NR];
+                ldn<true, T, NR>(a.x + k, xv);
+                ldn<true, T, NR>(p + k, pv);
+                ldn<true, T, NR>(a.r + k, rv);
+                ldn<true, T, NR>(a.Ap + k, av);
 #pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    const size_t k = (size_t)(3 * v + q) * NR + r;
-                    a.x[k] = __ldcg(a.x + k) + al * __ldcg(p + k);
-                    const T rv = __ldcg(a.r + k) - al * __ldcg(a.Ap + k);
-                    a.r[k] = rv;
-                    rr[r] += (double)rv * (double)rv;
-                    val[r * 3 + q] = (M)rv;
+                for (int r = 0; r < NR; r++) {
+                    // a stopped right-hand side keeps x and r (selected, not multiplied by 0,
+                    // so that non-finite p of a broken-down one cannot leak in)
+                    const T al = (T)alpha[r];
+                    if (run[r]) {
+                        xv[r] = xv[r] + al * pv[r];
+                        rv[r] = rv[r] - al * av[r];
+                        rr[r] += (double)rv[r] * (double)rv[r];
+                    }
+                    val[r * 3 + q] = run[r] ? (M)rv[r] : (M)0;
                 }
+                stn<T, NR>(a.x + k, xv);
+                stn<T, NR>(a.r + k, rv);
             }
         }
-        if (pos < mv.npos)
-#pragma unroll
-            for (int q = 0; q < 3; q++)
-#pragma unroll
-                for (int r = 0; r < NR; r++) a.R[(size_t)(3 * pos + q) * NR + r] = val[r * 3 + q];
+        if (pos < mv.npos) store_levels01<M, NR>(a.R, pos, val);
         bank_reduce_store<M, NR>(v >= 0 ? mv.up[pos] : -1, val, a.R);
     }
 }
+
+// per right-hand-side scalars of the solve (shared memory, see k_pcg_coop)
+template <int NR>
+struct RhsState {
+    double rz0[NR], rz[NR], bn2[NR], rr[NR], beta[NR], alpha[NR];
+    int iters[NR], status[NR];
+    bool run[NR], stop_rz[NR];
+};
 
 // ---- the solve ------------------------------------------------------------------------------
 template <class T, class M, int NR>
 __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a) {
     __shared__ double smem[NR * 32];
-    __shared__ M sR[kDomPerCta][48 * NR];
+    __shared__ __align__(16) M sR[kDomPerCta][48 * NR];
     extern __shared__ __align__(16) unsigned char dsm[];
     unsigned int epoch = 0;
 
     // ---- shared-memory residency of this CTA's static rows and level-0/1 domain inverses
     // (constant for the whole solve): loaded once, read every iteration
     constexpr int rpc = kCoopThreads / kSpG;  // rows of one CTA in one SpMV pass
+    // held in shared memory (uniform over the CTA) rather than in every thread's registers
+    __shared__ RowCache<T> rcs;
     RowCache<T> rc{nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, nullptr, nullptr};
     const M* dcache = nullptr;
     int ndc = 0;
@@ -582,106 +630,125 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
             for (int k = threadIdx.x; k < ndc * 2304; k += blockDim.x) dom[k] = __ldg(a.inv + 2304 * (size_t)d0 + k);
             dcache = dom;
         }
+        if (threadIdx.x == 0) rcs = rc;
         __syncthreads();
     }
-    // per right-hand side state, identical in every thread (computed from the same totals)
-    bool run[NR];
-    int iters[NR], status[NR];
-    double rz0[NR], rz[NR], bn2[NR], rr[NR], beta[NR], v[NR];
+    // Per right-hand-side state in shared memory: thread 0 updates it from the grid totals
+    // (identical in every CTA) after each reduction, the CTA reads it after a __syncthreads.
+    // Kept out of the threads' registers, which the phases need for their loads in flight.
+    __shared__ RhsState<NR> S;
+    if (threadIdx.x == 0)
 #pragma unroll
-    for (int r = 0; r < NR; r++) {
-        run[r] = true;
-        iters[r] = 0;
-        status[r] = SGIPC_OK;
-        rz0[r] = rz[r] = rr[r] = beta[r] = v[r] = 0.0;
-    }
+        for (int r = 0; r < NR; r++) {
+            S.run[r] = true;
+            S.stop_rz[r] = false;
+            S.iters[r] = 0;
+            S.status[r] = SGIPC_OK;
+            S.rz0[r] = S.rz[r] = S.rr[r] = S.bn2[r] = S.beta[r] = S.alpha[r] = 0.0;
+        }
+    double v[NR], t[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) v[r] = 0.0;
     // ---- r = b, x = 0, z = M r, rz0 = r.z
     phase_init(a, v);
-    bool ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, bn2);
+    bool ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);  // starts with __syncthreads
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int r = 0; r < NR; r++) S.bn2[r] = t[r];
     ok = ok && phase_mas(a, sR, epoch, dcache, ndc);
     if (ok) {
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
-        phase_prolong(a, run, v);
-        ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, rz0);
+        phase_prolong(a, S.run, v);
+        ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);
     }
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            const double rz0 = ok ? t[r] : 0.0;
+            S.rz0[r] = S.rz[r] = rz0;
+            S.rr[r] = S.bn2[r];
+            if (!(rz0 > 0.0) || !isfinite(rz0)) {
+                // b = 0 (or an indefinite preconditioner): nothing to iterate
+                S.run[r] = false;
+                if (!isfinite(rz0) || rz0 < 0.0) S.status[r] = SGIPC_BREAKDOWN;
+            }
+        }
+    __syncthreads();
     bool any = false;
 #pragma unroll
-    for (int r = 0; r < NR; r++) {
-        rz[r] = rz0[r];
-        rr[r] = bn2[r];
-        if (!(rz0[r] > 0.0) || !isfinite(rz0[r])) {
-            // b = 0 (or an indefinite preconditioner): nothing to iterate
-            run[r] = false;
-            if (!isfinite(rz0[r]) || rz0[r] < 0.0) status[r] = SGIPC_BREAKDOWN;
-        }
-        any |= run[r];
-    }
+    for (int r = 0; r < NR; r++) any |= S.run[r];
     // ---- iterations k = 1 .. max_iter-1
     for (int k = 1; ok && any && k < a.max_iter; k++) {
         T* pnew = (k & 1) ? a.p1 : a.p0;
         const T* pold = (k & 1) ? a.p0 : a.p1;
-        double pAp[NR], alpha[NR];
-        bool stop_rz[NR];
-#pragma unroll
-        for (int r = 0; r < NR; r++) pAp[r] = 0.0;
-        phase_spmv(a, k == 1, beta, pold, pnew, run, pAp, rc);
-        if (!(ok = grid_reduce<NR>(a.br, ++epoch, pAp, a.partial, smem, pAp))) break;
-#pragma unroll
-        for (int r = 0; r < NR; r++) {
-            stop_rz[r] = false;
-            alpha[r] = 0.0;
-            if (!run[r]) continue;
-            iters[r] = k;
-            if (!(pAp[r] > 0.0) || !isfinite(pAp[r]) || !isfinite(rz[r])) {
-                run[r] = false;
-                status[r] = SGIPC_BREAKDOWN;
-                continue;
-            }
-            alpha[r] = rz[r] / pAp[r];
-            // the reference tests the r.z of the current iterate and stops after its update
-            stop_rz[r] = a.crit == SGIPC_CRIT_RZ && fabs(rz[r]) <= a.tol * rz0[r];
-        }
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
-        phase_update(a, alpha, pnew, run, v);
-        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, v))) break;
+        phase_spmv(a, k == 1, S.beta, pold, pnew, S.run, v, rcs);
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t))) break;
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                S.stop_rz[r] = false;
+                S.alpha[r] = 0.0;
+                if (!S.run[r]) continue;
+                S.iters[r] = k;
+                const double pAp = t[r], rz = S.rz[r];
+                if (!(pAp > 0.0) || !isfinite(pAp) || !isfinite(rz)) {
+                    S.run[r] = false;
+                    S.status[r] = SGIPC_BREAKDOWN;
+                    continue;
+                }
+                S.alpha[r] = rz / pAp;
+                // the reference tests the r.z of the current iterate and stops after its update
+                S.stop_rz[r] = a.crit == SGIPC_CRIT_RZ && fabs(rz) <= a.tol * S.rz0[r];
+            }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < NR; r++) v[r] = 0.0;
+        phase_update(a, S.alpha, pnew, S.run, v);
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t))) break;
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                if (!S.run[r]) continue;
+                S.rr[r] = t[r];
+                if (S.stop_rz[r] || (a.crit == SGIPC_CRIT_TRUE && t[r] <= a.tol * a.tol * S.bn2[r])) S.run[r] = false;
+            }
+        __syncthreads();
         any = false;
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
-            if (!run[r]) continue;
-            rr[r] = v[r];
-            if (stop_rz[r] || (a.crit == SGIPC_CRIT_TRUE && v[r] <= a.tol * a.tol * bn2[r])) run[r] = false;
-            any |= run[r];
-        }
+        for (int r = 0; r < NR; r++) any |= S.run[r];
         if (!any || k + 1 >= a.max_iter) break;  // converged, or the iteration cap
         if (!(ok = phase_mas(a, sR, epoch, dcache, ndc))) break;
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
-        phase_prolong(a, run, v);
-        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, v))) break;
+        phase_prolong(a, S.run, v);
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t))) break;
+        if (threadIdx.x == 0)
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
-            if (!run[r]) continue;
-            beta[r] = v[r] / rz[r];
-            rz[r] = v[r];
-        }
+            for (int r = 0; r < NR; r++) {
+                if (!S.run[r]) continue;
+                S.beta[r] = t[r] / S.rz[r];
+                S.rz[r] = t[r];
+            }
+        __syncthreads();
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
 #pragma unroll
         for (int r = 0; r < NR; r++) {
-            PcgScalars& s = a.sc[r];
-            s.iter = iters[r];
-            s.rz0 = rz0[r];
-            s.rz = rz[r];
-            s.rz_next = rz[r];
-            s.bnorm2 = bn2[r];
-            s.rr = rr[r];
-            s.bodies = 0;
-            s.halt = 1;
+            PcgScalars& sc = a.sc[r];
+            sc.iter = S.iters[r];
+            sc.rz0 = S.rz0[r];
+            sc.rz = S.rz[r];
+            sc.rz_next = S.rz[r];
+            sc.bnorm2 = S.bn2[r];
+            sc.rr = S.rr[r];
+            sc.bodies = 0;
+            sc.halt = 1;
             // state 0 = still running when the iteration cap was reached
-            s.state = ok ? (run[r] ? 0 : 2) : 2;
-            s.status = ok ? status[r] : SGIPC_CUDA_ERROR;
+            sc.state = ok ? (S.run[r] ? 0 : 2) : 2;
+            sc.status = ok ? S.status[r] : SGIPC_CUDA_ERROR;
         }
     }
 }

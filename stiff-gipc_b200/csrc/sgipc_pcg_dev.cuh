@@ -74,13 +74,22 @@ struct Operand {
     const T* b;       // nullptr, or p_old
     T beta[NR];
     __device__ __forceinline__ void load(int j, T (&xj)[NR][3]) const {
+        T va[3][NR], vb[3][NR];
 #pragma unroll
-        for (int q = 0; q < 3; q++)
+        for (int q = 0; q < 3; q++) ldn<kL2, T, NR>(a + (size_t)(3 * j + q) * NR, va[q]);
+        if (b) {
 #pragma unroll
-            for (int r = 0; r < NR; r++) {
-                const size_t k = (size_t)(3 * j + q) * NR + r;
-                xj[r][q] = b ? ldv<kL2>(a + k) + beta[r] * ldv<kL2>(b + k) : ldv<kL2>(a + k);
-            }
+            for (int q = 0; q < 3; q++) ldn<kL2, T, NR>(b + (size_t)(3 * j + q) * NR, vb[q]);
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) xj[r][q] = va[q][r] + beta[r] * vb[q][r];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) xj[r][q] = va[q][r];
+        }
     }
 };
 
