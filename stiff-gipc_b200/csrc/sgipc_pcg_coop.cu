@@ -167,6 +167,10 @@ __device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, double (&
 // (bank_reduce_store needs all 32 lanes).
 __device__ __forceinline__ int grid_warp() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
 __device__ __forceinline__ int grid_warps() { return (int)((gridDim.x * blockDim.x) >> 5); }
+// The same warps numbered CTA-fastest: a phase with fewer warps of work than the grid holds
+// (one warp per 32 MAS positions or vertices) spreads over every SM instead of filling the
+// first CTAs
+__device__ __forceinline__ int spread_warp() { return (int)((threadIdx.x >> 5) * gridDim.x + blockIdx.x); }
 
 // R at MAS position p (level 0) from the per-(rhs, component) values val[r * 3 + q]
 template <class M, int NR>
@@ -185,7 +189,7 @@ template <class T, class M, int NR>
 __device__ void phase_init(const CoopArgs<T, M, NR>& a, double (&bb)[NR]) {
     const MasView& mv = a.mv;
     const int lane = threadIdx.x & 31;
-    for (int pb = grid_warp() * 32; pb < mv.npos; pb += grid_warps() * 32) {
+    for (int pb = spread_warp() * 32; pb < mv.npos; pb += grid_warps() * 32) {
         const int p = pb + lane;
         const int v = p < mv.npos ? mv.part_map[p] : -1;
         M val[NR * 3];
@@ -319,7 +323,7 @@ __device__ bool phase_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], unsigne
 template <class T, class M, int NR>
 __device__ void phase_prolong(const CoopArgs<T, M, NR>& a, const bool (&run)[NR], double (&rz)[NR]) {
     const MasView& mv = a.mv;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nv; v += gridDim.x * blockDim.x) {
+    for (int v = spread_warp() * 32 + (int)(threadIdx.x & 31); v < a.nv; v += gridDim.x * blockDim.x) {
         const int* tv = mv.table + (size_t)v * mv.L;
         int gl[SGIPC_MAX_LEVELS];
 #pragma unroll
@@ -525,7 +529,7 @@ __device__ void phase_update(const CoopArgs<T, M, NR>& a, const double (&alpha)[
                              const bool (&run)[NR], double (&rr)[NR]) {
     const MasView& mv = a.mv;
     const int lane = threadIdx.x & 31;
-    for (int pb = grid_warp() * 32; pb < mv.npos; pb += grid_warps() * 32) {
+    for (int pb = spread_warp() * 32; pb < mv.npos; pb += grid_warps() * 32) {
         const int pos = pb + lane;
         const int v = pos < mv.npos ? mv.part_map[pos] : -1;
         M val[NR * 3];
