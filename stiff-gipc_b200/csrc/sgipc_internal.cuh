@@ -40,6 +40,7 @@ struct PcgScalars {
 struct PcgWork {
     void* x;
     void* r;
+    void* r2;                // second residual buffer of the persistent solve
     void* z;
     void* p;
     void* p2;                // second direction buffer (the SpMV forms p = z + beta p_old on the fly)
@@ -71,6 +72,8 @@ struct MasWork {
     int* comp_rank;          // [npos] new local id of the component a node belongs to
     int* bank_cnt;           // [npos/16 + 1]
     int* bank_off;           // [npos/16 + 1]
+    int* l1_first;           // [npos/16 + 2] per level-1 bank: first and last level-0 bank holding
+    int* l1_last;            //   one of its nodes' positions (levels >= 3)
     int* info;               // device: [0..7] level starts, [8..15] level counts, [16] total
     int h_info[17];          // host copy after build
     double* dom64;           // [total_cap/16][48*48] FP64 domain matrices / inverses

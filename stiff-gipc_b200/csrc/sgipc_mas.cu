@@ -399,6 +399,28 @@ static int num_levels(int nodes) {
     return nLevel > SGIPC_MAX_LEVELS ? SGIPC_MAX_LEVELS : nLevel;
 }
 
+// For each level-1 bank m (nodes 16 m .. 16 m + 15): the first and last level-0 bank whose
+// positions have a parent in it.  Level-1 ids grow with the level-0 bank (components are
+// numbered bank by bank), so the banks in between feed m as well.
+// One thread per level-0 bank: its components span at most two level-1 banks.
+__global__ void k_l1_ranges(int npos, const int* __restrict__ up, const int* __restrict__ info,
+                            int* __restrict__ first, int* __restrict__ last) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= (npos >> 4)) return;
+    const int start1 = info[1];
+    int lo = 0x7fffffff, hi = -1;
+    for (int k = 0; k < 16; k++) {
+        const int g = up[16 * b + k];
+        if (g < 0) continue;
+        lo = min(lo, (g - start1) >> 4);
+        hi = max(hi, (g - start1) >> 4);
+    }
+    for (int m = lo; m <= hi; m++) {
+        atomicMin(first + m, b);
+        atomicMax(last + m, b);
+    }
+}
+
 SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
     MasWork& m = c->mas;
     m.npos = t->part_map_size;
@@ -431,6 +453,8 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
         !A((void**)&m.mask, sizeof(uint32_t) * m.npos) || !A((void**)&m.comp_rank, sizeof(int) * m.npos) ||
         !A((void**)&m.bank_cnt, sizeof(int) * (m.npos / 16 + 2)) ||
         !A((void**)&m.bank_off, sizeof(int) * (m.npos / 16 + 2)) || !A((void**)&m.info, sizeof(int) * 32) ||
+        !A((void**)&m.l1_first, sizeof(int) * (m.npos / 16 + 2)) ||
+        !A((void**)&m.l1_last, sizeof(int) * (m.npos / 16 + 2)) ||
         !A((void**)&m.dom64, sizeof(double) * ndom_cap * 2304) || !A((void**)&m.dom32, sizeof(float) * ndom_cap * 2304) ||
         !A((void**)&m.R64, sizeof(double) * 3 * m.total_cap * rhs) ||
         !A((void**)&m.Z64, sizeof(double) * 3 * m.total_cap * rhs) ||
@@ -457,7 +481,8 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
 void mas_destroy(SgipcCtx* c) {
     MasWork& m = c->mas;
     void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.nbr_row, m.table, m.up, m.node, m.mask, m.comp_rank, m.bank_cnt,
-                    m.bank_off, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32, m.scan_tmp};
+                    m.bank_off, m.l1_first, m.l1_last, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32,
+                    m.scan_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -469,7 +494,7 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     const int nbank_cap = m.npos / 16 + 1;
     k_init_level0<<<nblk(nv > m.npos ? nv : m.npos), SGIPC_BLOCK, 0, s>>>(nv, m.real_map, L, m.node, m.table,
                                                                           m.info, m.npos, m.up);
-    SG_COUNT(c, 1 + (L - 1) * (3 + (con && con->pair_num > 0)) + 3);
+    SG_COUNT(c, 1 + (L - 1) * (3 + (con && con->pair_num > 0)) + 3 + (L >= 3));
     for (int l = 0; l + 1 < L; l++) {
         SG_CHECK(c, cudaMemsetAsync(m.mask, 0, sizeof(uint32_t) * m.npos, s));
         if (m.nnbr > 0) k_mask_edges<<<nblk(m.nnbr), SGIPC_BLOCK, 0, s>>>(m.nnbr, m.nbr_row, m.nbr, m.node, m.mask);
@@ -481,6 +506,13 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
         size_t tb = m.scan_tmp_bytes;
         SG_CHECK(c, cub::DeviceScan::ExclusiveSum(m.scan_tmp, tb, m.bank_cnt, m.bank_off, nbank_cap + 1, s));
         k_assign<<<nblk(nv), SGIPC_BLOCK, 0, s>>>(nv, L, l, m.bank_off, m.comp_rank, m.node, m.table, m.info, m.up);
+    }
+    if (L >= 3) {
+        // level-0 bank range of every level-1 bank (the persistent solve restricts a level-1
+        // bank to level 2 inside one CTA)
+        SG_CHECK(c, cudaMemsetAsync(m.l1_first, 0x7f, sizeof(int) * (m.npos / 16 + 2), s));
+        SG_CHECK(c, cudaMemsetAsync(m.l1_last, 0xff, sizeof(int) * (m.npos / 16 + 2), s));
+        k_l1_ranges<<<nblk(m.npos / 16), SGIPC_BLOCK, 0, s>>>(m.npos, m.up, m.info, m.l1_first, m.l1_last);
     }
     SG_LAUNCH_CHECK(c, "mas hierarchy");
     SG_CHECK(c, cudaMemcpyAsync(m.h_info, m.info, sizeof(int) * 17, cudaMemcpyDeviceToHost, s));

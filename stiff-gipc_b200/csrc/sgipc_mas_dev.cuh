@@ -12,11 +12,11 @@
 namespace sgipc {
 
 // All 32 lanes of the warp must call this (values of idle lanes: parent = -1).
-// v[NR*3] holds this node's value; the parent's sum is stored at R[3*parent+q][r].
+// v[NR*3] holds this node's value; s receives the sum over the lanes of the half-warp with
+// the same parent, added in lane order; returns true on the lowest such lane.
 template <class M, int NR>
-__device__ __forceinline__ void bank_reduce_store(int parent, const M (&v)[NR * 3], M* __restrict__ R) {
+__device__ __forceinline__ bool bank_group_sum(int parent, const M (&v)[NR * 3], M (&s)[NR * 3]) {
     const unsigned full = 0xffffffffu;
-    M s[NR * 3];
 #pragma unroll
     for (int k = 0; k < NR * 3; k++) s[k] = 0;
     int leader = -1;
@@ -31,7 +31,15 @@ __device__ __forceinline__ void bank_reduce_store(int parent, const M (&v)[NR * 
             if (same) s[k] += vj;
         }
     }
-    if (parent >= 0 && (int)(threadIdx.x & 15) == leader) {
+    return (int)(threadIdx.x & 15) == leader;
+}
+
+// The group sum above, stored at R[3*parent+q][r] (when parent >= 0) by the group's leader.
+template <class M, int NR>
+__device__ __forceinline__ void bank_reduce_store(int parent, const M (&v)[NR * 3], M* __restrict__ R) {
+    M s[NR * 3];
+    const bool lead = bank_group_sum<M, NR>(parent, v, s);
+    if (parent >= 0 && lead) {
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             M o[NR];

@@ -616,7 +616,7 @@ int final_status(SgipcCtx* c, const PcgScalars& s) {
 
 SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
     const size_t n3 = 3 * (size_t)c->n * nrhs;
-    void** vs[] = {&w.x, &w.r, &w.z, &w.p, &w.p2, &w.Ap};
+    void** vs[] = {&w.x, &w.r, &w.r2, &w.z, &w.p, &w.p2, &w.Ap};
     for (void** v : vs) SG_CHECK(c, cudaMalloc(v, elem * n3));
     SG_CHECK(c, cudaMalloc((void**)&w.sc, sizeof(PcgScalars) * nrhs));
     SG_CHECK(c, cudaMalloc((void**)&w.partial, sizeof(double) * 4 * nrhs * c->max_blocks));
@@ -630,7 +630,7 @@ SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
 }
 
 void free_work(PcgWork& w) {
-    void* ps[] = {w.x, w.r, w.z, w.p, w.p2, w.Ap, w.sc, w.partial, w.ticket, w.coop};
+    void* ps[] = {w.x, w.r, w.r2, w.z, w.p, w.p2, w.Ap, w.sc, w.partial, w.ticket, w.coop};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (w.exec) cudaGraphExecDestroy(w.exec);

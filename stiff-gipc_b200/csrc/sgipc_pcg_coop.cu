@@ -64,6 +64,7 @@ struct CoopArgs {
     const double* b;
     T* x;
     T* r;
+    T* r2;             // second residual buffer (level-1-aligned passes read the old one)
     T* z;
     T* p0;
     T* p1;
@@ -83,6 +84,11 @@ struct CoopArgs {
     int ecap;
     int kcap;
     int dcap;
+    // >= 3 levels: position passes aligned to level-1 banks restrict to level 2 in the CTA,
+    // and one MAS phase solves levels 0..2 while one CTA takes the levels above
+    int l2mode;
+    const int* l1_first;
+    const int* l1_last;
 };
 
 __device__ __forceinline__ void red_add_release_gpu(unsigned int* p, unsigned int v) {
@@ -304,6 +310,17 @@ template <class T, class M, int NR>
 __device__ bool phase_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], unsigned int& epoch, const M* dcache,
                           int ndc) {
     const int L = a.mv.L, G = gridDim.x;
+    if (a.l2mode) {
+        // levels 0..2 are complete: the grid solves their domains; with more levels the last
+        // CTA restricts 2 -> 3 -> ... and solves the (few) domains above
+        if (L > 3 && blockIdx.x == G - 1) {
+            restrict_coarse_cta<M, NR, true>(a.mv.info, a.mv.up, L, a.R, 2);
+            solve_domain_range<M, NR>(a.inv, a.R, a.Z, a.nd2, a.ndom, G - 1, 1, sR);
+        } else {
+            solve_domain_range<M, NR>(a.inv, a.R, a.Z, 0, a.nd2, 0, L > 3 ? G - 1 : G, sR, dcache, ndc);
+        }
+        return grid_barrier(a.br, ++epoch);
+    }
     if (L > 2) restrict_level1<M, NR>(a.mv, a.R);
     solve_domain_range<M, NR>(a.inv, a.R, a.Z, 0, a.nd01, 0, G, sR, dcache, ndc);
     if (!grid_barrier(a.br, ++epoch)) return false;
@@ -321,7 +338,7 @@ __device__ bool phase_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], unsigne
 
 // z = sum over levels of Z at the vertex's clusters; r.z
 template <class T, class M, int NR>
-__device__ void phase_prolong(const CoopArgs<T, M, NR>& a, const bool (&run)[NR], double (&rz)[NR]) {
+__device__ void phase_prolong(const CoopArgs<T, M, NR>& a, const T* rcur, const bool (&run)[NR], double (&rz)[NR]) {
     const MasView& mv = a.mv;
     for (int v = spread_warp() * 32 + (int)(threadIdx.x & 31); v < a.nv; v += gridDim.x * blockDim.x) {
         const int* tv = mv.table + (size_t)v * mv.L;
@@ -350,7 +367,7 @@ __device__ void phase_prolong(const CoopArgs<T, M, NR>& a, const bool (&run)[NR]
         for (int q = 0; q < 3; q++) {
             const size_t k = (size_t)(3 * v + q) * NR;
             T zz[NR], rv[NR];
-            ldn<true, T, NR>(a.r + k, rv);
+            ldn<true, T, NR>(rcur + k, rv);
 #pragma unroll
             for (int r = 0; r < NR; r++) {
                 zz[r] = (T)sq[q][r];
@@ -565,6 +582,110 @@ __device__ void phase_update(const CoopArgs<T, M, NR>& a, const double (&alpha)[
     }
 }
 
+// Position pass aligned to level-1 banks (l2mode), for the initial restriction (kInit:
+// r = b, x = 0) and for the update (x += alpha p, r_new = r_old - alpha Ap).  CTA c takes
+// level-1 banks m = c, c + G, ...; for each, the level-0 banks l1_first[m] .. l1_last[m]
+// that feed it, two per warp.  A level-0 bank belongs to the level-1 bank of its first
+// component: only there are x, r and its level-0 R written and r.r accumulated.  A bank
+// whose components straddle two level-1 banks is recomputed by the second one from the
+// old residual (identical arithmetic), so that every CTA holds its level-1 bank complete
+// (level-1 sums: the same 16-lane groups and order as bank_reduce_store), keeps it in shared
+// memory and restricts it to level 2 itself.
+template <class T, class M, int NR, bool kInit>
+__device__ void phase_positions_l2(const CoopArgs<T, M, NR>& a, const double (&alpha)[NR], const T* p,
+                                   const T* r_old, T* r_new, const bool (&run)[NR], double (&acc)[NR],
+                                   M (*s_l1)[3 * NR]) {
+    const MasView& mv = a.mv;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int start1 = mv.info[1], count1 = mv.info[9];
+    const int nb1 = (count1 + 15) >> 4;
+    for (int m = blockIdx.x; m < nb1; m += gridDim.x) {  // block-uniform
+        const int b_lo = __ldg(a.l1_first + m), b_hi = __ldg(a.l1_last + m);
+        const int id_lo = 16 * m, id_hi = min(16 * m + 16, count1);
+        for (int b0 = b_lo + 2 * w; b0 <= b_hi; b0 += 2 * (kCoopThreads / 32)) {  // warp-uniform
+            const int bank = b0 + (lane >> 4);
+            const int pos = bank * 16 + (lane & 15);
+            const int v = bank <= b_hi ? __ldg(mv.part_map + pos) : -1;
+            const int par = v >= 0 ? __ldg(mv.up + pos) - start1 : -1;  // local level-1 id
+            int first = par >= 0 ? par : 0x7fffffff;  // the bank's first component
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, o, 16));
+            const bool own = first >= id_lo;
+            M val[NR * 3];
+#pragma unroll
+            for (int k = 0; k < NR * 3; k++) val[k] = 0;
+            if (v >= 0) {
+                T pq[3][NR];
+                if (!kInit)
+#pragma unroll
+                    for (int q = 0; q < 3; q++) ldn<true, T, NR>(p + (size_t)(3 * v + q) * NR, pq[q]);
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    const size_t k = (size_t)(3 * v + q) * NR;
+                    T rv[NR];
+                    if (kInit) {
+                        double bv[NR];
+                        ldn<false, double, NR>(a.b + k, bv);
+                        T tx[NR];
+#pragma unroll
+                        for (int r = 0; r < NR; r++) {
+                            rv[r] = (T)bv[r];
+                            tx[r] = 0;
+                            if (own) acc[r] += bv[r] * bv[r];
+                        }
+                        if (own) {
+                            stn<T, NR>(r_new + k, rv);
+                            stn<T, NR>(a.x + k, tx);
+                        }
+                    } else {
+                        T xv[NR], av[NR];
+#pragma unroll
+                        for (int r = 0; r < NR; r++) xv[r] = 0;
+                        ldn<true, T, NR>(r_old + k, rv);
+                        ldn<true, T, NR>(a.Ap + k, av);
+                        if (own) ldn<true, T, NR>(a.x + k, xv);
+#pragma unroll
+                        for (int r = 0; r < NR; r++) {
+                            const T al = (T)alpha[r];
+                            if (run[r]) {
+                                rv[r] = rv[r] - al * av[r];
+                                xv[r] = xv[r] + al * pq[q][r];
+                                if (own) acc[r] += (double)rv[r] * (double)rv[r];
+                            }
+                        }
+                        if (own) {
+                            stn<T, NR>(a.x + k, xv);
+                            stn<T, NR>(r_new + k, rv);
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < NR; r++) val[r * 3 + q] = (kInit || run[r]) ? (M)rv[r] : (M)0;
+                }
+            }
+            if (own && bank <= b_hi) store_levels01<M, NR>(a.R, pos, val);
+            // level-1 sums of this bank's components inside [id_lo, id_hi)
+            const int gp = (par >= id_lo && par < id_hi) ? par : -1;
+            M sum[NR * 3];
+            const bool lead = bank_group_sum<M, NR>(gp, val, sum);
+            if (lead && gp >= 0) {
+#pragma unroll
+                for (int k = 0; k < NR * 3; k++) s_l1[gp - id_lo][k] = sum[k];
+                store_levels01<M, NR>(a.R, start1 + gp, sum);
+            }
+        }
+        __syncthreads();
+        if (w == 0) {  // level 1 -> 2 for this bank (same groups and order as restrict_level1)
+            const int a1 = id_lo + (lane & 15);
+            const bool ok = lane < 16 && a1 < id_hi;
+            M v1[NR * 3];
+#pragma unroll
+            for (int k = 0; k < NR * 3; k++) v1[k] = ok ? s_l1[lane & 15][k] : (M)0;
+            bank_reduce_store<M, NR>(ok ? __ldg(mv.up + start1 + a1) : -1, v1, a.R);
+        }
+        __syncthreads();  // s_l1 is rewritten for the next bank
+    }
+}
+
 // per right-hand-side scalars of the solve (shared memory, see k_pcg_coop)
 template <int NR>
 struct RhsState {
@@ -654,7 +775,14 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
 #pragma unroll
     for (int r = 0; r < NR; r++) v[r] = 0.0;
     // ---- r = b, x = 0, z = M r, rz0 = r.z
-    phase_init(a, v);
+    // (level-1-aligned passes keep the residual in two buffers: rcur holds the current one)
+    __shared__ M s_l1[16][3 * NR];
+    T* rcur = a.r;
+    T* ralt = a.r2;
+    if (a.l2mode)
+        phase_positions_l2<T, M, NR, true>(a, S.alpha, nullptr, nullptr, rcur, S.run, v, s_l1);
+    else
+        phase_init(a, v);
     bool ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);  // starts with __syncthreads
     if (threadIdx.x == 0)
 #pragma unroll
@@ -663,7 +791,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
     if (ok) {
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
-        phase_prolong(a, S.run, v);
+        phase_prolong(a, rcur, S.run, v);
         ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);
     }
     if (threadIdx.x == 0)
@@ -710,7 +838,14 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
-        phase_update(a, S.alpha, pnew, S.run, v);
+        if (a.l2mode) {
+            phase_positions_l2<T, M, NR, false>(a, S.alpha, pnew, rcur, ralt, S.run, v, s_l1);
+            T* t2 = rcur;
+            rcur = ralt;
+            ralt = t2;
+        } else {
+            phase_update(a, S.alpha, pnew, S.run, v);
+        }
         if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t))) break;
         if (threadIdx.x == 0)
 #pragma unroll
@@ -727,7 +862,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
         if (!(ok = phase_mas(a, sR, epoch, dcache, ndc))) break;
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
-        phase_prolong(a, S.run, v);
+        phase_prolong(a, rcur, S.run, v);
         if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t))) break;
         if (threadIdx.x == 0)
 #pragma unroll
@@ -824,6 +959,7 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     a.b = b;
     a.x = (T*)w.x;
     a.r = (T*)w.r;
+    a.r2 = (T*)w.r2;
     a.z = (T*)w.z;
     a.p0 = (T*)w.p;
     a.p1 = (T*)w.p2;
@@ -838,10 +974,16 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     a.ecap = ecap;
     a.kcap = kcap;
     a.dcap = dcap;
+    a.l2mode = L >= 3 && grid >= 2;
+    a.l1_first = m.l1_first;
+    a.l1_last = m.l1_last;
     a.max_iter = max_iter;
     a.crit = crit;
     a.tol = tol;
     SG_CHECK(c, cudaMemsetAsync(w.ticket + 4, 0, 2 * sizeof(unsigned int), s));
+    // level-1-aligned passes write the level-0 entries of the banks that hold vertices only:
+    // the others must read as zero in every solve, whatever the right-hand-side count
+    if (a.l2mode) SG_CHECK(c, cudaMemsetAsync(a.R, 0, sizeof(M) * 3 * (size_t)m.npos * NR, s));
     void* args[] = {&a};
     SG_COUNT(c, 1);
     SG_CHECK(c, cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kCoopThreads), args, dyn, s));
