@@ -308,6 +308,23 @@ SgipcStatus sgipc_abd_precond_build(SgipcAbdCtx* ctx, void* stream);
 /* ABDPreconditioner::apply: z_b = P_b^-1 r_b, r and z [dev double[12 * body_num]]. */
 SgipcStatus sgipc_abd_precond_apply(SgipcAbdCtx* ctx, const double* r, double* z, void* stream);
 
+/* ---- the global FEM + ABD system ------------------------------------------------------- */
+
+/* GlobalLinearSystem::solve_linear_system + distribute_solution (global_linear_system.cu:
+ * 8-166, gipc/gipc.cu:42-70) with the ABD and FEM subsystems: PCGSolver::pcg
+ * (pcg_solver.cu:174-267, FP64 vectors) on the global vector [12 * body_num ABD DOFs |
+ * 3 * n FEM DOFs].  A = the FEM context's assembled matrix on the FEM rows plus the ABD
+ * context's merged body-space blocks (body rows and body x FEM coupling) with their
+ * transposes; M = the ABD block Jacobi (sgipc_abd_precond_build) on the body rows and the
+ * FEM context's MAS (sgipc_mas_build; FP64 or FP32 inverses as built) on the FEM rows.
+ * b, x [dev double[12 * body_num + 3 n]]; abd_point_dx [dev double3[point_num], may be
+ * null] receives J(x_bar) dq of every ABD point.  max_iter <= 0: 0.3 x DOFs.  Returns
+ * SGIPC_NOT_READY unless both systems are assembled and both preconditioners built.
+ * Synchronises (two scalar reads per iteration). */
+SgipcStatus sgipc_global_pcg_solve(SgipcCtx* fem, SgipcAbdCtx* abd, SgipcCriterion crit, double tol,
+                                   int32_t max_iter, const double* b, double* x, double* abd_point_dx,
+                                   SgipcSolveStats* stats, void* stream);
+
 /* ---- instrumentation (the reference's gipc::Timer / cudaEvent phase timers,
  *      StiffGIPC/gipc/utils/timer.h:19-136, GIPC.cu:10854-10964) ----------------------- */
 

@@ -325,5 +325,56 @@ def pcg(rows, cols, vals, n, mas, b, tol=1e-4, max_iter=None, single=False):
     return x, it, rz0[0], rz[0]
 
 
+def global_pcg(A, body_num, mas, b, tol=1e-4, max_iter=None, single=False):
+    """PCGSolver::pcg (StiffGIPC/linear_system/solver/pcg_solver.cu:174-267; the loop of
+    or_pcg above) on the global FEM + ABD system of GlobalLinearSystem
+    (linear_system/linear_system/global_linear_system.cu:8-166, created in gipc/gipc.cu:
+    42-70): DOFs [12 body_num ABD | FEM], A (N x N, dense or scipy sparse) symmetric, the
+    preconditioner the identity overwritten per subsystem (apply_preconditioner,
+    global_linear_system.cu:152-166): ABDPreconditioner's inverse 12x12 diagonal blocks
+    (abd_preconditioner.cu:15-38) on the ABD DOFs and the oracle MAS on the FEM DOFs.
+    Returns x, the iteration count (or_pcg's convention), r0.z0 and the final r.z."""
+    b = _f64(b)
+    N = len(b)
+    na = 12 * body_num
+    dense = A if isinstance(A, np.ndarray) else None
+    inv = []
+    for k in range(body_num):
+        blk = (dense[12 * k:12 * k + 12, 12 * k:12 * k + 12] if dense is not None
+               else A[12 * k:12 * k + 12, 12 * k:12 * k + 12].toarray())
+        inv.append(np.linalg.inv(blk))
+
+    def prec(r):
+        z = r.copy()
+        for k in range(body_num):
+            z[12 * k:12 * k + 12] = inv[k] @ r[12 * k:12 * k + 12]
+        if N > na:
+            z[na:] = mas.apply(r[na:], single)
+        return z
+
+    if max_iter is None:
+        max_iter = int(0.3 * N)
+    x = np.zeros(N)
+    r = b.copy()
+    z = prec(r)
+    rz = float(r @ z)
+    rz0 = rz
+    p = z.copy()
+    k = 1
+    while k < max_iter:
+        Ap = A @ p
+        alpha = rz / float(p @ Ap)
+        x += alpha * p
+        r -= alpha * Ap
+        if abs(rz) <= tol * rz0:
+            break
+        z = prec(r)
+        rz_new = float(r @ z)
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+        k += 1
+    return x, k, rz0, rz
+
+
 def num_threads():
     return lib().or_num_threads()

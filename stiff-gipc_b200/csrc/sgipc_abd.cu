@@ -18,37 +18,10 @@
 #include <cub/cub.cuh>
 #include <vector>
 
-#include "sgipc_internal.cuh"
+#include "sgipc_abd_ctx.cuh"
 
 using namespace sgipc;
 
-struct SgipcAbdCtx {
-    int device;
-    int B, P, max_abd, max_fem, cap;
-    char err[256];
-    int* point_body;
-    int* body_ptr;       // [B+1] points of each body
-    int* bt;             // [B]
-    double* x_bar;       // [3P]
-    double* dmass;       // [13B]
-    double* vol;         // [B]
-    // merge
-    unsigned long long* key;
-    unsigned long long* key_s;
-    int* idx;
-    int* idx_s;
-    double* val;         // [9 cap]
-    int* flag;           // [cap+1]
-    int* nu;             // device: unique blocks
-    int* u_row;
-    int* u_col;
-    double* u_val;
-    int m_last;          // emitted slots of the last call
-    double* pinv;        // [144 B]
-    int assembled;
-    void* cub_tmp;
-    size_t cub_bytes;
-};
 
 namespace {
 
@@ -440,7 +413,9 @@ extern "C" SgipcStatus sgipc_abd_destroy(SgipcAbdCtx* c) {
     if (!c) return SGIPC_BAD_INPUT;
     cudaSetDevice(c->device);
     void* ps[] = {c->point_body, c->body_ptr, c->bt, c->x_bar, c->dmass, c->vol, c->key, c->key_s, c->idx,
-                  c->idx_s, c->val, c->flag, c->nu, c->u_row, c->u_col, c->u_val, c->pinv, c->cub_tmp};
+                  c->idx_s, c->val, c->flag, c->nu, c->u_row, c->u_col, c->u_val, c->pinv, c->cub_tmp,
+                  c->g_rptr, c->g_cptr, c->g_tkey, c->g_tkey_s, c->g_tidx, c->g_tidx_s, c->g_vec, c->g_dot,
+                  c->g_cub};
     for (void* p : ps)
         if (p) cudaFree(p);
     delete c;
@@ -540,6 +515,7 @@ extern "C" SgipcStatus sgipc_abd_grad_hess(SgipcAbdCtx* c, const double* q, cons
                                              c->nu);
     AB_CHECK(c, cudaGetLastError());
     c->assembled = 1;
+    c->pbuilt = 0;
     return SGIPC_OK;
 }
 
@@ -570,6 +546,7 @@ extern "C" SgipcStatus sgipc_abd_precond_build(SgipcAbdCtx* c, void* stream) {
                                                                        c->pinv);
     k_pinv<<<nblk(c->B, 64), 64, 0, s>>>(c->B, c->pinv);
     AB_CHECK(c, cudaGetLastError());
+    c->pbuilt = 1;
     return SGIPC_OK;
 }
 
@@ -580,4 +557,8 @@ extern "C" SgipcStatus sgipc_abd_precond_apply(SgipcAbdCtx* c, const double* r, 
     k_papply<<<nblk(12LL * c->B), SGIPC_BLOCK, 0, (cudaStream_t)stream>>>(c->B, c->pinv, r, z);
     AB_CHECK(c, cudaGetLastError());
     return SGIPC_OK;
+}
+
+void sgipc::abd_precond_apply_async(SgipcAbdCtx* c, const double* r, double* z, cudaStream_t s) {
+    k_papply<<<nblk(12LL * c->B), SGIPC_BLOCK, 0, s>>>(c->B, c->pinv, r, z);
 }

@@ -94,6 +94,8 @@ SIGNATURES = {
     "sgipc_abd_export_bcoo": ([_vp, _i32, _vp, _vp, _vp, C.POINTER(_i32)], _i32),
     "sgipc_abd_precond_build": ([_vp, _vp], _i32),
     "sgipc_abd_precond_apply": ([_vp, _vp, _vp, _vp], _i32),
+    "sgipc_global_pcg_solve": ([_vp, _vp, _i32, C.c_double, _i32, _vp, _vp, _vp, C.POINTER(SgipcSolveStats), _vp],
+                               _i32),
     "sgipc_launch_count": ([_vp, C.POINTER(C.c_int64)], _i32),
     "sgipc_time_kernel": ([_vp, C.c_char_p, _i32, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)], _i32),
 }

@@ -50,6 +50,7 @@ class ABDSystem:
             raise N.SgipcError(st, "sgipc_abd_create")
         self.ctx = h
         self.body_num = t.body_num
+        self.point_num = t.point_num
         self.body_grad = torch.zeros(12 * self.body_num, dtype=torch.float64, device=_dev())
 
     def close(self):
@@ -109,3 +110,46 @@ class ABDPreconditioner:
         z = torch.empty_like(r) if z is None else z
         self.abd._check(N.lib().sgipc_abd_precond_apply(self.abd.ctx, _p(r), _p(z), _stream()))
         return z
+
+
+class GlobalLinearSystem:
+    """The global FEM + ABD system (``GlobalLinearSystem`` with ``ABDLinearSubsystem`` first
+    and ``FEMLinearSubsystem`` after it, StiffGIPC/gipc/gipc.cu:42-70): one PCG
+    (``PCGSolver::pcg``) over [12 * body_num ABD DOFs | 3 n FEM DOFs] with the ABD block
+    Jacobi on the body rows and the MAS on the FEM rows
+    (``GlobalLinearSystem::apply_preconditioner``, global_linear_system.cu:152-166).
+
+    ``gipc`` is a :class:`sgipc.system.GIPC` whose system is assembled and whose MAS is built;
+    ``abd`` an :class:`ABDSystem` after ``setup_abd_system_gradient_hessian`` and
+    :meth:`ABDPreconditioner.assemble`."""
+
+    def __init__(self, gipc, abd: ABDSystem):
+        self.gipc = gipc
+        self.abd = abd
+        self.nb = 4 * abd.body_num
+        self.dof = 3 * (self.nb + gipc.n)
+
+    def right_hand_side(self, fem_rhs: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """b = [body gradient | FEM right-hand side] (``build_linear_system``'s rhs assembly)."""
+        fem = self.gipc.rhs() if fem_rhs is None else fem_rhs
+        return torch.cat([self.abd.body_grad, fem.reshape(-1).to(torch.float64)])
+
+    def solve_linear_system(self, b: torch.Tensor, tol: float = 1e-4, criterion: int = N.CRIT_RZ,
+                            max_iter_ratio: float = 0.3):
+        """x (dof,), the ABD points' dx (P, 3) = J(x_bar) dq, and the solve stats."""
+        b = b.reshape(-1).to(torch.float64).contiguous()
+        if b.numel() != self.dof:
+            raise ValueError("global right-hand side has %d entries, expected %d" % (b.numel(), self.dof))
+        x = torch.empty_like(b)
+        P = int(self.abd.point_num)
+        pdx = torch.empty((max(P, 1), 3), dtype=torch.float64, device=b.device)
+        st = N.SgipcSolveStats()
+        s = N.lib().sgipc_global_pcg_solve(self.gipc.ctx, self.abd.ctx, int(criterion), float(tol),
+                                           int(max_iter_ratio * self.dof), _p(b), _p(x), _p(pdx) if P else None,
+                                           C.byref(st), _stream())
+        N.check(s, self.gipc.ctx, allow=(N.OK, N.NOT_CONVERGED))
+        return x, pdx[:P], st
+
+    def distribute_solution(self, x: torch.Tensor):
+        """(body dq (B, 12), FEM move direction (n, 3)) of a global solution."""
+        return x[:3 * self.nb].reshape(-1, 12), x[3 * self.nb:].reshape(-1, 3)

@@ -470,3 +470,68 @@ def test_abd_contact_mapping_is_the_point_space_quadratic_form():
         k = b["point_body"][p]
         ref[12 * k:12 * k + 12] += _abd_J(b["x_bar"][p]).T @ c["point_grad"][p]
     assert np.allclose(g1 - g0, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def global_system(sc, bodies, seed=0, coupling=0.05):
+    """A coupled FEM + ABD test system: the oracle's FEM matrix of ``sc``, the body-space
+    matrix of ``bodies`` with seeded ABD-ABD contact blocks, and ABD-FEM coupling blocks
+    scaled to ``coupling`` x the smallest FEM / body diagonal so that A stays SPD.  Returns
+    (A dense, FEM rows/cols/vals, ABD contact inputs, the body-space bcoo)."""
+    fb, frow, fcol, fval, _ = oracle.assemble(sc)
+    Aff = oracle.dense(frow, fcol, fval, sc.nv)
+    rng = np.random.default_rng(seed)
+    c = abd_contacts(bodies, n_fem=sc.nv, seed=seed)
+    # ABD-ABD contacts as PSD pair Hessians: H on both diagonal blocks, -H between
+    pb = bodies["point_body"]
+    pairs = []
+    while len(pairs) < 40:
+        i, j = sorted(rng.integers(0, len(pb), 2))
+        if pb[i] != pb[j]:
+            pairs.append((i, j))
+    M = rng.normal(size=(len(pairs), 3, 3))
+    H = np.einsum("nij,nkj->nik", M, M) * 1e2
+    pi = np.array([p[0] for p in pairs], np.int32)
+    pj = np.array([p[1] for p in pairs], np.int32)
+    c["abd"] = (np.concatenate([pi, pj, pi]), np.concatenate([pi, pj, pj]), np.concatenate([H, H, -H]))
+    g0, r0, c0, v0 = oracle.abd_assemble(bodies, bodies["q"], bodies["q_tilde"], bodies["kappa"], bodies["dt"],
+                                         abd_blocks=c["abd"])
+    Aaa = oracle.dense(r0, c0, v0, 4 * len(bodies["volume"]))
+    scale = coupling * np.sqrt(np.linalg.eigvalsh(Aff).min() * np.linalg.eigvalsh(Aaa).min())
+    frows, fcols, fvals = c["fem"]
+    fvals = rng.normal(size=fvals.shape)
+    fvals *= scale / np.abs(fvals).max()
+    c["fem"] = (frows, fcols, fvals)
+    c["fem_boundary"] = (sc.boundary_type != 0).astype(np.int32)
+    g, rows, cols, vals = oracle.abd_assemble(bodies, bodies["q"], bodies["q_tilde"], bodies["kappa"],
+                                              bodies["dt"], point_grad=c["point_grad"], abd_blocks=c["abd"],
+                                              fem_blocks=c["fem"], fem_boundary=c["fem_boundary"])
+    nb = 4 * len(bodies["volume"])
+    A = oracle.dense(np.concatenate([rows, frow + nb]), np.concatenate([cols, fcol + nb]),
+                     np.concatenate([vals, fval]), nb + sc.nv)
+    return A, (frow, fcol, fval), c, g
+
+
+def test_global_pcg_without_bodies_is_the_fem_pcg(small_two_cubes):
+    """The oracle's global PCG with no ABD rows runs or_pcg's loop on the FEM system."""
+    sc = small_two_cubes
+    b, rows, cols, vals, _ = oracle.assemble(sc)
+    A = oracle.dense(rows, cols, vals, sc.nv)
+    M = oracle.Mas(sc, rows, cols, vals)
+    x, it, rz0, rz = oracle.pcg(rows, cols, vals, sc.nv, M, b, 1e-4)
+    xg, itg, rz0g, rzg = oracle.global_pcg(A, 0, M, b, 1e-4)
+    assert itg == it
+    assert rz0g == pytest.approx(rz0, rel=1e-12)
+    # numpy's dense products and dots round differently from the C loop's sparse ones
+    assert np.abs(xg - x).max() <= 1e-7 * np.abs(x).max()
+
+
+def test_global_pcg_solves_the_coupled_system():
+    sc = scenes.scene_cube(4, touching=True, seed=3)
+    bodies = scenes.scene_abd_boxes(6, seed=7)
+    A, (frow, fcol, fval), c, g = global_system(sc, bodies, seed=4)
+    assert np.linalg.eigvalsh(A).min() > 0
+    M = oracle.Mas(sc, frow, fcol, fval)
+    b = np.random.default_rng(5).normal(size=A.shape[0])
+    x, it, rz0, rz = oracle.global_pcg(A, 6, M, b, 1e-20, max_iter=10 * A.shape[0])
+    ex = np.linalg.solve(A, b)
+    assert np.linalg.norm(x - ex) / np.linalg.norm(ex) < 1e-8
