@@ -172,6 +172,12 @@ struct SgipcCtx {
     SgipcContacts mas_con;        // contacts of the last MAS build (to rebuild after timing)
     int mas_has_con;
     long long launches;           // kernels of this library launched on the context
+    // launch configuration of the persistent solve per (T, M, NR) instance, computed on its
+    // first use (it depends on the device and the static pattern only)
+    struct CoopCfg {
+        int valid, usable, grid, ecap, kcap, dcap;
+        size_t dyn;
+    } coop_cfg[6];
 
     // ---- MAS and PCG ------------------------------------------------------------------
     sgipc::MasWork mas;

@@ -893,25 +893,21 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
 }
 
 // ---- host launcher ----------------------------------------------------------------------------
+// Launch configuration of one instance on this context (device attributes, shared-memory
+// residency sizes, occupancy): computed once, it depends only on the device and the static
+// pattern.  usable = 0 when the device cannot co-schedule the grid.
 template <class T, class M, int NR>
-SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
-                         cudaStream_t s, bool* used) {
-    *used = false;
-    const char* e = getenv("SGIPC_PCG_GRAPH");
-    if (e && e[0] == '1') return SGIPC_OK;  // the graph of per-phase kernels instead
+SgipcStatus coop_configure(SgipcCtx* c, SgipcCtx::CoopCfg& cfg) {
+    cfg = SgipcCtx::CoopCfg{};
     int coop = 0, nsm = 0, per = 0, optin = 0;
     SG_CHECK(c, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
     SG_CHECK(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
     SG_CHECK(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    cfg.valid = 1;
     if (!coop) return SGIPC_OK;
-    MasWork& m = c->mas;
-    const int* h = m.h_info;
-    const int L = m.levelnum;
-    const int ndom = h[16] / 16;
-    const int nd01 = L > 2 ? h[2] / 16 : ndom;
     // shared-memory residency with one CTA per SM: the static rows of each CTA's SpMV pass
     // (when one pass covers all rows) first, then as many of its level-0/1 domain
-    // inverses as still fit (when one round covers them)
+    // inverses as still fit (the first round of a CTA's domains)
     const void* fn = (const void*)k_pcg_coop<T, M, NR>;
     cudaFuncAttributes fa;
     SG_CHECK(c, cudaFuncGetAttributes(&fa, fn));
@@ -932,7 +928,7 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
                                 coop_contact_bytes(rpc, kContactSlots, sizeof(T))) <= budget)
         kcap = kContactSlots;
     const size_t rows_bytes = coop_rows_bytes(rpc, ecap, sizeof(T)) + coop_contact_bytes(rpc, kcap, sizeof(T));
-    if (budget > 0 && nd01 <= (long long)nsm * kDomPerCta) {
+    if (budget > 0) {
         long long left = budget - (long long)rows_bytes;
         dcap = left > 0 ? (int)(left / (2304 * (long long)sizeof(M))) : 0;
         if (dcap > kDomPerCta) dcap = kDomPerCta;
@@ -948,7 +944,38 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     if (per < 1) return SGIPC_OK;
     if (per > kCoopMaxCtasPerSm) per = kCoopMaxCtasPerSm;
     int grid = dyn > 0 ? nsm : nsm * per;  // residency assumes the one-CTA-per-SM mapping
-    if (grid > w.coop_cap) grid = w.coop_cap;
+    if (grid > c->pcg64.coop_cap) grid = c->pcg64.coop_cap;
+    if (grid > c->pcg32.coop_cap) grid = c->pcg32.coop_cap;
+    cfg.usable = 1;
+    cfg.grid = grid;
+    cfg.ecap = ecap;
+    cfg.kcap = kcap;
+    cfg.dcap = dcap;
+    cfg.dyn = dyn;
+    return SGIPC_OK;
+}
+
+template <class T, class M, int NR>
+SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
+                         cudaStream_t s, bool* used) {
+    *used = false;
+    const char* e = getenv("SGIPC_PCG_GRAPH");
+    if (e && e[0] == '1') return SGIPC_OK;  // the graph of per-phase kernels instead
+    constexpr int inst = (sizeof(T) == 8 ? (sizeof(M) == 8 ? 0 : 1) : 2) + (NR == 4 ? 3 : 0);
+    SgipcCtx::CoopCfg& cfg = c->coop_cfg[inst];
+    if (!cfg.valid) {
+        SgipcStatus st = coop_configure<T, M, NR>(c, cfg);
+        if (st != SGIPC_OK) return st;
+    }
+    if (!cfg.usable) return SGIPC_OK;  // the graph of per-phase kernels instead
+    MasWork& m = c->mas;
+    const int* h = m.h_info;
+    const int L = m.levelnum;
+    const int ndom = h[16] / 16;
+    const int nd01 = L > 2 ? h[2] / 16 : ndom;
+    const int grid = cfg.grid, ecap = cfg.ecap, kcap = cfg.kcap, dcap = cfg.dcap;
+    const size_t dyn = cfg.dyn;
+    const void* fn = (const void*)k_pcg_coop<T, M, NR>;
     CoopArgs<T, M, NR> a;
     a.tp = topo_of(c);
     a.A = mat_view<T>(c);
