@@ -72,6 +72,8 @@ struct MasWork {
     int* comp_rank;          // [npos] new local id of the component a node belongs to
     int* bank_cnt;           // [npos/16 + 1]
     int* bank_off;           // [npos/16 + 1]
+    int* map0;               // [npos/16 * 256] static slot of each level-0 domain entry (a, b):
+                             //   s + 1 (block s), -(s + 1) (its transpose), 0 (none)
     int* l1_first;           // [npos/16 + 2] per level-1 bank: first and last level-0 bank holding
     int* l1_last;            //   one of its nodes' positions (levels >= 3)
     int* info;               // device: [0..7] level starts, [8..15] level counts, [16] total

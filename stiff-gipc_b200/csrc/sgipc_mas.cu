@@ -150,39 +150,48 @@ __global__ void k_assign(int nv, int L, int level, const int* __restrict__ bank_
     if (level + 2 == L) up[start_next + nn] = -1;
 }
 
-// Scatter one 3x3 block B at (r,c) (and B^T at (c,r)) into every level whose bank holds
-// both endpoints.  Lanes of a warp that hit the same coarse entry first add their blocks
-// together (match + shuffles) so that one lane issues the atomics: at the coarsest levels
-// nearly every block of a warp lands on the same few entries.
+// Scatter one 3x3 block B at (r,c) (and B^T at (c,r)) into every level from l_first on whose
+// bank holds both endpoints.  Lanes of a warp whose blocks land on the same coarse entry
+// add them first (match + shuffles) so that one lane issues the atomics.  The groups nest
+// (blocks with the same (cluster(r), cluster(c)) at level l share it at level l + 1), so
+// each level adds only the previous level's group sums, carried by their leaders: a few
+// per warp at the coarse levels, where nearly every block of the warp lands on one entry.
+// Levels l >= l_top (at most kTopLevels of them, each one domain of <= 16 nodes) go to the
+// CTA's shared copies s_top[l - l_top] of their domains instead (flushed by flush_top).
+constexpr int kTopLevels = 2;
 __device__ __forceinline__ void scatter_block_warp(double* dom, const int* __restrict__ table, int L, int r, int c,
-                                                   const double (&B)[9], bool valid) {
+                                                   const double (&B)[9], bool valid, int l_first, int l_top,
+                                                   double (*s_top)[2304]) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    for (int l = 0; l < L; l++) {
+    double V[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) V[q] = valid ? B[q] : 0.0;
+    unsigned carriers = __ballot_sync(full, valid);  // lanes holding a partial sum
+    const unsigned long long diag = r == c ? 1ull : 0ull;
+    for (int l = l_first; l < L; l++) {
         int ga = -1, gb = -1;
         if (valid) {
             ga = table[(size_t)r * L + l];
             gb = table[(size_t)c * L + l];
         }
-        bool hit = valid && (ga >> 4) == (gb >> 4);
-        // key of the target: (ga, gb) and whether the block is a diagonal one
-        unsigned long long key = hit ? (((unsigned long long)(unsigned)ga << 33) | ((unsigned long long)(unsigned)gb << 1) |
-                                        (unsigned long long)(r == c))
-                                     : ~0ull;
-        unsigned grp = __match_any_sync(full, key);
-        int leader = __ffs(grp) - 1;
+        // target (ga, gb) and whether the block is a diagonal one
+        const unsigned long long key =
+            valid ? (((unsigned long long)(unsigned)ga << 33) | ((unsigned long long)(unsigned)gb << 1) | diag) : ~0ull;
+        const unsigned grp = __match_any_sync(full, key);
+        const bool lead = lane == __ffs(grp) - 1;
         double S[9];
 #pragma unroll
         for (int q = 0; q < 9; q++) S[q] = 0.0;
-        unsigned m = grp;
+        unsigned m = grp & carriers;
         while (m) {
-            int j = __ffs(m) - 1;
+            const int j = __ffs(m) - 1;
             m &= m - 1;
 #pragma unroll
-            for (int q = 0; q < 9; q++) S[q] += __shfl_sync(grp, B[q], j);
+            for (int q = 0; q < 9; q++) S[q] += __shfl_sync(grp, V[q], j);
         }
-        if (hit && lane == leader) {
-            double* D = dom + (size_t)(ga >> 4) * 2304;
+        if (valid && lead && (ga >> 4) == (gb >> 4)) {
+            double* D = l >= l_top ? s_top[l - l_top] : dom + (size_t)(ga >> 4) * 2304;
             int ra = 3 * (ga & 15), cb = 3 * (gb & 15);
 #pragma unroll
             for (int i = 0; i < 3; i++)
@@ -194,30 +203,87 @@ __device__ __forceinline__ void scatter_block_warp(double* dom, const int* __res
                     if (r != c) atomicAdd(D + (cb + j) * 48 + ra + i, v);
                 }
         }
+#pragma unroll
+        for (int q = 0; q < 9; q++) V[q] = lead ? S[q] : 0.0;
+        carriers = __ballot_sync(full, valid && lead);
+    }
+}
+
+// The top levels' domain copies of the CTA: zeroed, filled by scatter_block_warp, then added
+// to the global domains (one atomic per non-zero entry and CTA instead of one per warp
+// group: every block of the grid lands on the few entries of these levels).
+__device__ __forceinline__ void zero_top(int ntop, double (*s_top)[2304]) {
+    for (int k = threadIdx.x; k < ntop * 2304; k += blockDim.x) s_top[k / 2304][k % 2304] = 0.0;
+    __syncthreads();
+}
+
+__device__ __forceinline__ void flush_top(const int* __restrict__ info, int l_top, int ntop, double (*s_top)[2304],
+                                          double* __restrict__ dom) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < ntop * 2304; k += blockDim.x) {
+        const double v = s_top[k / 2304][k % 2304];
+        if (v != 0.0) atomicAdd(dom + (size_t)(info[l_top + k / 2304] >> 4) * 2304 + k % 2304, v);
     }
 }
 
 __global__ void k_scatter_static(int nnz, const int* __restrict__ slot_row, const int* __restrict__ col,
                                  const double* __restrict__ val, const int* __restrict__ table, int L,
-                                 double* __restrict__ dom) {
+                                 const int* __restrict__ info, int l_top, double* __restrict__ dom) {
+    __shared__ double s_top[kTopLevels][2304];
+    const int ntop = L - l_top;
+    zero_top(ntop, s_top);
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = s < nnz;
     double B[9];
 #pragma unroll
     for (int q = 0; q < 9; q++) B[q] = valid ? val[9 * (size_t)s + q] : 0.0;
-    scatter_block_warp(dom, table, L, valid ? slot_row[s] : 0, valid ? col[s] : 0, B, valid);
+    scatter_block_warp(dom, table, L, valid ? slot_row[s] : 0, valid ? col[s] : 0, B, valid, 1, l_top, s_top);
+    flush_top(info, l_top, ntop, s_top, dom);
+}
+
+// Level 0 of the static blocks, without atomics: the level-0 domains are the banks of the
+// fixed position map, so each entry (a, b) of domain d takes one static block (or its
+// transpose, or nothing) known at creation.  One thread per 3x3 entry writes it whole.
+__global__ void k_fill_level0(int nd0, const int* __restrict__ map0, const double* __restrict__ val,
+                              double* __restrict__ dom) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nd0 * 256) return;
+    const int d = t >> 8, a = (t >> 4) & 15, b = t & 15;
+    const int m = map0[t];
+    double B[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) B[q] = 0.0;
+    if (m > 0) {
+#pragma unroll
+        for (int q = 0; q < 9; q++) B[q] = val[9 * (size_t)(m - 1) + q];
+    } else if (m < 0) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) B[3 * i + j] = val[9 * (size_t)(-m - 1) + 3 * j + i];
+    }
+    double* D = dom + (size_t)d * 2304 + (3 * a) * 48 + 3 * b;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) D[i * 48 + j] = B[3 * i + j];
 }
 
 __global__ void k_scatter_contact(int cap, const int* __restrict__ nuc, const int* __restrict__ ur,
                                   const int* __restrict__ uc, const double* __restrict__ val,
-                                  const int* __restrict__ table, int L, double* __restrict__ dom) {
+                                  const int* __restrict__ table, int L, const int* __restrict__ info, int l_top,
+                                  double* __restrict__ dom) {
+    __shared__ double s_top[kTopLevels][2304];
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x * blockDim.x >= nuc[0]) return;  // whole block beyond the unique blocks
+    const int ntop = L - l_top;
+    zero_top(ntop, s_top);
     bool valid = u < cap && u < nuc[0];
     double B[9];
 #pragma unroll
     for (int q = 0; q < 9; q++) B[q] = valid ? val[9 * (size_t)u + q] : 0.0;
-    scatter_block_warp(dom, table, L, valid ? ur[u] : 0, valid ? uc[u] : 0, B, valid);
+    scatter_block_warp(dom, table, L, valid ? ur[u] : 0, valid ? uc[u] : 0, B, valid, 0, l_top, s_top);
+    flush_top(info, l_top, ntop, s_top, dom);
 }
 
 // Gauss-Jordan inversion without pivoting, in place, one 48x48 domain per 192-thread CTA
@@ -387,6 +453,14 @@ SgipcStatus mas_apply_t(SgipcCtx* c, const T* r, T* z, int fp32_inv, cudaStream_
 template SgipcStatus mas_apply_t<double>(SgipcCtx*, const double*, double*, int, cudaStream_t);
 template SgipcStatus mas_apply_t<float>(SgipcCtx*, const float*, float*, int, cudaStream_t);
 
+// First of the coarsest levels (at most kTopLevels, each with <= 16 nodes, i.e. one domain
+// starting at a multiple of 16) that the scatter accumulates per CTA; L when none.
+static int top_levels(const MasWork& m) {
+    int l = m.levelnum;
+    while (l > 1 && m.levelnum - (l - 1) <= kTopLevels && m.h_info[8 + l - 1] <= 16 && (m.h_info[l - 1] & 15) == 0) l--;
+    return l;
+}
+
 static int num_levels(int nodes) {
     int nLevel = 1;
     int levelSz = (nodes + 15) / 16 * 16;
@@ -453,6 +527,7 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
         !A((void**)&m.mask, sizeof(uint32_t) * m.npos) || !A((void**)&m.comp_rank, sizeof(int) * m.npos) ||
         !A((void**)&m.bank_cnt, sizeof(int) * (m.npos / 16 + 2)) ||
         !A((void**)&m.bank_off, sizeof(int) * (m.npos / 16 + 2)) || !A((void**)&m.info, sizeof(int) * 32) ||
+        !A((void**)&m.map0, sizeof(int) * (size_t)(m.npos / 16) * 256) ||
         !A((void**)&m.l1_first, sizeof(int) * (m.npos / 16 + 2)) ||
         !A((void**)&m.l1_last, sizeof(int) * (m.npos / 16 + 2)) ||
         !A((void**)&m.dom64, sizeof(double) * ndom_cap * 2304) || !A((void**)&m.dom32, sizeof(float) * ndom_cap * 2304) ||
@@ -468,6 +543,22 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
     SG_CHECK(c, cudaMemcpy(m.nbr_ptr, ptr.data(), sizeof(int) * (nv + 1), cudaMemcpyHostToDevice));
     if (!nb.empty()) SG_CHECK(c, cudaMemcpy(m.nbr, nb.data(), sizeof(int) * nb.size(), cudaMemcpyHostToDevice));
     if (!nb.empty()) SG_CHECK(c, cudaMemcpy(m.nbr_row, nrow.data(), sizeof(int) * nb.size(), cudaMemcpyHostToDevice));
+    {
+        // static slot of every level-0 domain entry (the static pattern is on the device)
+        std::vector<int> srow(c->nnz), scol(c->nnz), map0((size_t)(m.npos / 16) * 256, 0);
+        if (c->nnz) {
+            SG_CHECK(c, cudaMemcpy(srow.data(), c->slot_row, sizeof(int) * c->nnz, cudaMemcpyDeviceToHost));
+            SG_CHECK(c, cudaMemcpy(scol.data(), c->col, sizeof(int) * c->nnz, cudaMemcpyDeviceToHost));
+        }
+        for (int k = 0; k < c->nnz; k++) {
+            const int pa = rm[srow[k]], pb = rm[scol[k]];
+            if ((pa >> 4) != (pb >> 4)) continue;
+            const size_t d = (size_t)(pa >> 4) * 256;
+            map0[d + (pa & 15) * 16 + (pb & 15)] = k + 1;
+            if (pa != pb) map0[d + (pb & 15) * 16 + (pa & 15)] = -(k + 1);
+        }
+        SG_CHECK(c, cudaMemcpy(m.map0, map0.data(), sizeof(int) * map0.size(), cudaMemcpyHostToDevice));
+    }
     SG_CHECK(c, cudaMemset(m.R64, 0, sizeof(double) * 3 * m.total_cap * rhs));
     SG_CHECK(c, cudaMemset(m.R32, 0, sizeof(float) * 3 * m.total_cap * rhs));
     SG_CHECK(c, cudaMemset(m.info, 0, sizeof(int) * 32));
@@ -481,7 +572,7 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
 void mas_destroy(SgipcCtx* c) {
     MasWork& m = c->mas;
     void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.nbr_row, m.table, m.up, m.node, m.mask, m.comp_rank, m.bank_cnt,
-                    m.bank_off, m.l1_first, m.l1_last, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32,
+                    m.bank_off, m.map0, m.l1_first, m.l1_last, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32,
                     m.scan_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -522,14 +613,20 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
         snprintf(c->err, sizeof(c->err), "MAS cluster count %d exceeds capacity %d", total, m.total_cap);
         return SGIPC_CAPACITY;
     }
-    const int ndom = total / 16;
-    SG_CHECK(c, cudaMemsetAsync(m.dom64, 0, sizeof(double) * 2304 * (size_t)ndom, s));
+    const int ndom = total / 16, nd0 = m.npos / 16;
+    // level 0 is written whole by k_fill_level0; the coarser domains start from zero
+    if (ndom > nd0)
+        SG_CHECK(c, cudaMemsetAsync(m.dom64 + (size_t)nd0 * 2304, 0, sizeof(double) * 2304 * (size_t)(ndom - nd0), s));
     // restricted vectors: entries outside the current levels' nodes must read as zero
     SG_CHECK(c, cudaMemsetAsync(m.R64, 0, sizeof(double) * 3 * (size_t)total * c->max_rhs, s));
     SG_CHECK(c, cudaMemsetAsync(m.R32, 0, sizeof(float) * 3 * (size_t)total * c->max_rhs, s));
-    k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L, m.dom64);
+    SG_COUNT(c, 1);
+    const int l_top = top_levels(m);
+    k_fill_level0<<<nblk(256LL * nd0), SGIPC_BLOCK, 0, s>>>(nd0, m.map0, c->val64, m.dom64);
+    k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L, m.info,
+                                                          l_top, m.dom64);
     k_scatter_contact<<<nblk(c->cap_cblk), SGIPC_BLOCK, 0, s>>>(c->cap_cblk, c->nuc, c->uc_row, c->uc_col, c->uc64,
-                                                               m.table, L, m.dom64);
+                                                               m.table, L, m.info, l_top, m.dom64);
     const int w64 = prec == SGIPC_FP64 ? 1 : 0, w32 = prec == SGIPC_FP64 ? 0 : 1;
     k_invert<<<ndom, 192, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
     SG_LAUNCH_CHECK(c, "mas matrices");
@@ -561,9 +658,11 @@ SgipcStatus mas_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
     if (!m.built) return SGIPC_NOT_READY;
     const int L = m.levelnum, total = m.h_info[16], ndom = total / 16;
     SG_COUNT(c, 1);
-    if (!strcmp(name, "mas_scatter")) {
+    if (!strcmp(name, "mas_scatter")) {  // static blocks: level-0 fill + coarser levels' scatter
+        SG_COUNT(c, 1);
+        k_fill_level0<<<nblk(256LL * (m.npos / 16)), SGIPC_BLOCK, 0, s>>>(m.npos / 16, m.map0, c->val64, m.dom64);
         k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L,
-                                                               m.dom64);
+                                                               m.info, top_levels(m), m.dom64);
         *bytes = (double)c->nnz * (72 + 8) + (double)c->nv * L * 4 + (double)ndom * 2304 * 8;
     } else if (!strcmp(name, "mas_invert")) {
         k_invert<<<ndom, 192, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);
