@@ -312,20 +312,27 @@ __global__ void __launch_bounds__(192) k_invert(int ndom, double* __restrict__ d
 #pragma unroll 1
     for (int k = 0; k < 48; k++) {
         const int q = k & 1;
-        // publish row k, column k and 1 / A(k,k) as they are before this step
+        // this tile holds row k (16 threads) / column k (12 threads) / the pivot (1 thread):
+        // the publishing and fix-up paths are branches only those threads take
+        const int ka = k - i0, kb = k - j0;
+        const bool own_r = (unsigned)ka < 4u, own_c = (unsigned)kb < 3u;
+        if (own_r) {  // publish row k (and 1 / A(k,k)) as it is before this step
 #pragma unroll
-        for (int a = 0; a < 4; a++)
-            if (k == i0 + a)
+            for (int a = 0; a < 4; a++)
+                if (a == ka)
 #pragma unroll
-                for (int b = 0; b < 3; b++) {
-                    prow[q][j0 + b] = t[a][b];
-                    if (k == j0 + b) pinv[q] = 1.0 / t[a][b];
-                }
+                    for (int b = 0; b < 3; b++) {
+                        prow[q][j0 + b] = t[a][b];
+                        if (b == kb) pinv[q] = 1.0 / t[a][b];
+                    }
+        }
+        if (own_c) {  // publish column k
 #pragma unroll
-        for (int b = 0; b < 3; b++)
-            if (k == j0 + b)
+            for (int b = 0; b < 3; b++)
+                if (b == kb)
 #pragma unroll
-                for (int a = 0; a < 4; a++) pcol[q][i0 + a] = t[a][b];
+                    for (int a = 0; a < 4; a++) pcol[q][i0 + a] = t[a][b];
+        }
         __syncthreads();
         const double ip = pinv[q];
         double rk[3], ck[4];
@@ -337,17 +344,20 @@ __global__ void __launch_bounds__(192) k_invert(int ndom, double* __restrict__ d
         for (int a = 0; a < 4; a++)
 #pragma unroll
             for (int b = 0; b < 3; b++) t[a][b] -= ck[a] * rk[b];
-        // the pivot row and column (a few threads) are set instead of updated
+        if (own_r) {  // the pivot row is set instead of updated
 #pragma unroll
-        for (int a = 0; a < 4; a++)
-            if (k == i0 + a)
+            for (int a = 0; a < 4; a++)
+                if (a == ka)
 #pragma unroll
-                for (int b = 0; b < 3; b++) t[a][b] = rk[b];
+                    for (int b = 0; b < 3; b++) t[a][b] = rk[b];
+        }
+        if (own_c) {  // and so is the pivot column
 #pragma unroll
-        for (int b = 0; b < 3; b++)
-            if (k == j0 + b)
+            for (int b = 0; b < 3; b++)
+                if (b == kb)
 #pragma unroll
-                for (int a = 0; a < 4; a++) t[a][b] = (k == i0 + a) ? ip : -ck[a] * ip;
+                    for (int a = 0; a < 4; a++) t[a][b] = (a == ka) ? ip : -ck[a] * ip;
+        }
     }
     double* Dw = dom + (size_t)d * 2304;
     float* Dw32 = dom32 + (size_t)d * 2304;

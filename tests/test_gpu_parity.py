@@ -25,9 +25,12 @@ from sgipc import scenes, system  # noqa: E402
 from sgipc import _native as N  # noqa: E402
 
 
-@pytest.fixture(scope="module", params=["cube_touch", "two_cubes", "cloth_on_cube"])
+@pytest.fixture(scope="module", params=["c1_cube", "cube_touch", "two_cubes", "cloth_on_cube"])
 def case(request):
-    if request.param == "cube_touch":
+    if request.param == "c1_cube":
+        # the smallest workload: an 11^3 cube 0.05 m above the ground, no contact yet
+        sc = scenes.scene_cube(11, touching=False, seed=0)
+    elif request.param == "cube_touch":
         sc = scenes.scene_cube(6, touching=True, seed=3)
     elif request.param == "two_cubes":
         sc = scenes.scene_two_cubes(7, seed=5)
@@ -186,6 +189,16 @@ def test_persistent_and_graph_solves_agree(case, prec, monkeypatch):
     assert abs(sa.rz0 - sb.rz0) <= 1e-9 * abs(sb.rz0)
     if sa.iterations == sb.iterations:
         assert _rel(xa, xb) < (1e-9 if prec == "fp64" else 1e-4)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_zero_rhs_gives_zero_solution(case, prec):
+    sc, g, _ = case
+    system.MASPreconditioner(g).setPreconditioner(prec)
+    b = torch.zeros(3 * sc.nv, dtype=torch.float64, device="cuda")
+    x, st = system.PCGSolver(g, system.PCGSolverConfig(precision=prec)).solve(b)
+    assert st.status == N.OK and st.iterations == 0
+    assert float(x.abs().max()) == 0.0
 
 
 def test_iteration_cap_reports_not_converged(case):
