@@ -11,23 +11,37 @@
 
 namespace sgipc {
 
-// All 32 lanes of the warp must call this (values of idle lanes: parent = -1).
+// All 16 lanes of a half-warp call this together (values of idle lanes: parent = -1).
 // v[NR*3] holds this node's value; s receives the sum over the lanes of the half-warp with
-// the same parent, added in lane order; returns true on the lowest such lane.
+// the same parent (a butterfly when the half-warp is one group, else added in lane order);
+// returns true on the lowest such lane.
 template <class M, int NR>
 __device__ __forceinline__ bool bank_group_sum(int parent, const M (&v)[NR * 3], M (&s)[NR * 3]) {
-    const unsigned full = 0xffffffffu;
+    // Each half-warp (one bank) decides for itself, with half-warp masks, so that a bank's
+    // sums never depend on the bank beside it: one group (a connected bank, the common
+    // case) adds by a butterfly, several groups in lane order.
+    const unsigned half = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+    const bool one = __all_sync(half, parent == __shfl_sync(half, parent, 0, 16));
+    if (one) {
+#pragma unroll
+        for (int k = 0; k < NR * 3; k++) {
+            s[k] = v[k];
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) s[k] += __shfl_xor_sync(half, s[k], o, 16);
+        }
+        return (threadIdx.x & 15) == 0;
+    }
 #pragma unroll
     for (int k = 0; k < NR * 3; k++) s[k] = 0;
     int leader = -1;
 #pragma unroll
     for (int j = 0; j < 16; j++) {
-        int pj = __shfl_sync(full, parent, j, 16);
+        int pj = __shfl_sync(half, parent, j, 16);
         bool same = pj == parent;
         if (same && leader < 0) leader = j;
 #pragma unroll
         for (int k = 0; k < NR * 3; k++) {
-            M vj = __shfl_sync(full, v[k], j, 16);
+            M vj = __shfl_sync(half, v[k], j, 16);
             if (same) s[k] += vj;
         }
     }
