@@ -1014,6 +1014,7 @@ extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const 
     if (st != SGIPC_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     SG_CHECK(c, cudaSetDevice(c->device));
+    if ((st = mas_mark_start(c, s)) != SGIPC_OK) return st;
     c->btype = f->BoundaryType;
     c->last_fem = *f;
     c->last_prm = *p;
@@ -1034,6 +1035,8 @@ extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const 
     if ((st = merge_contacts(c, m, s)) != SGIPC_OK) return st;
     k_rhs<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, c->fb, c->shape_grads, f->BoundaryType, c->b);
     SG_LAUNCH_CHECK(c, "rhs");
+    // the MAS hierarchy of these contacts, beside the assembly (sgipc_mas_build reuses it)
+    if ((st = mas_prebuild(c, k, s)) != SGIPC_OK) return st;
     c->assembled = 1;
     c->mas.built = 0;
     return SGIPC_OK;

@@ -87,6 +87,14 @@ struct MasWork {
     void* scan_tmp;
     size_t scan_tmp_bytes;
     int built;               // 0 none, else SgipcPrecision+1 of the stored inverses
+    // hierarchy prebuilt by sgipc_assemble on `side` (it needs the contacts only, not the
+    // matrix), overlapping the assembly; consumed by the next mas_build with the same pairs
+    cudaStream_t side;
+    cudaEvent_t ev_start, ev_hier;
+    int* h_info_pinned;      // [32] pinned landing area of the level counts
+    int hier_pending;
+    const void* hier_pairs;
+    int hier_pair_num;
 };
 
 }  // namespace sgipc
@@ -271,6 +279,11 @@ SgipcStatus pcg_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
 SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t);
 void mas_destroy(SgipcCtx* c);
 SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, cudaStream_t s);
+// Start the hierarchy for these contacts on the MAS side stream, after the work queued on
+// s so far (called by sgipc_assemble: the hierarchy needs no matrix values).
+SgipcStatus mas_prebuild(SgipcCtx* c, const SgipcContacts* con, cudaStream_t s);
+// Record the point of s after which the side stream may rewrite the hierarchy.
+SgipcStatus mas_mark_start(SgipcCtx* c, cudaStream_t s);
 // z = M^-1 r for T in {double, float}; r, z are [3n] vectors of T (rz accumulated into
 // out_dot[0] when out_dot != nullptr, using r . z with r in T precision).
 template <class T>

@@ -572,6 +572,10 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
     SG_CHECK(c, cudaMemset(m.R64, 0, sizeof(double) * 3 * m.total_cap * rhs));
     SG_CHECK(c, cudaMemset(m.R32, 0, sizeof(float) * 3 * m.total_cap * rhs));
     SG_CHECK(c, cudaMemset(m.info, 0, sizeof(int) * 32));
+    SG_CHECK(c, cudaStreamCreateWithFlags(&m.side, cudaStreamNonBlocking));
+    SG_CHECK(c, cudaEventCreateWithFlags(&m.ev_start, cudaEventDisableTiming));
+    SG_CHECK(c, cudaEventCreateWithFlags(&m.ev_hier, cudaEventDisableTiming));
+    SG_CHECK(c, cudaMallocHost((void**)&m.h_info_pinned, sizeof(int) * 32));
     size_t tb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tb, m.bank_cnt, m.bank_off, m.npos / 16 + 2);
     m.scan_tmp_bytes = tb + 256;
@@ -581,6 +585,13 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
 
 void mas_destroy(SgipcCtx* c) {
     MasWork& m = c->mas;
+    if (m.side) {
+        cudaStreamSynchronize(m.side);  // a prebuild may still read the caller's pairs
+        cudaStreamDestroy(m.side);
+    }
+    if (m.ev_start) cudaEventDestroy(m.ev_start);
+    if (m.ev_hier) cudaEventDestroy(m.ev_hier);
+    if (m.h_info_pinned) cudaFreeHost(m.h_info_pinned);
     void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.nbr_row, m.table, m.up, m.node, m.mask, m.comp_rank, m.bank_cnt,
                     m.bank_off, m.map0, m.l1_first, m.l1_last, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32,
                     m.scan_tmp};
@@ -588,14 +599,15 @@ void mas_destroy(SgipcCtx* c) {
         if (p) cudaFree(p);
 }
 
-SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, cudaStream_t s) {
+// The hierarchy (levels, cluster tables, parents, level-1 bank ranges) for these contacts
+// on stream s; the level counts land in the pinned buffer (read after s reaches them).
+static SgipcStatus mas_hierarchy(SgipcCtx* c, const SgipcContacts* con, cudaStream_t s) {
     MasWork& m = c->mas;
-    if (!c->assembled) return SGIPC_NOT_READY;
     const int nv = c->nv, L = m.levelnum;
     const int nbank_cap = m.npos / 16 + 1;
     k_init_level0<<<nblk(nv > m.npos ? nv : m.npos), SGIPC_BLOCK, 0, s>>>(nv, m.real_map, L, m.node, m.table,
                                                                           m.info, m.npos, m.up);
-    SG_COUNT(c, 1 + (L - 1) * (3 + (con && con->pair_num > 0)) + 3 + (L >= 3));
+    SG_COUNT(c, 1 + (L - 1) * (3 + (con && con->pair_num > 0)) + (L >= 3));
     for (int l = 0; l + 1 < L; l++) {
         SG_CHECK(c, cudaMemsetAsync(m.mask, 0, sizeof(uint32_t) * m.npos, s));
         if (m.nnbr > 0) k_mask_edges<<<nblk(m.nnbr), SGIPC_BLOCK, 0, s>>>(m.nnbr, m.nbr_row, m.nbr, m.node, m.mask);
@@ -616,8 +628,52 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
         k_l1_ranges<<<nblk(m.npos / 16), SGIPC_BLOCK, 0, s>>>(m.npos, m.up, m.info, m.l1_first, m.l1_last);
     }
     SG_LAUNCH_CHECK(c, "mas hierarchy");
-    SG_CHECK(c, cudaMemcpyAsync(m.h_info, m.info, sizeof(int) * 17, cudaMemcpyDeviceToHost, s));
-    SG_CHECK(c, cudaStreamSynchronize(s));
+    SG_CHECK(c, cudaMemcpyAsync(m.h_info_pinned, m.info, sizeof(int) * 17, cudaMemcpyDeviceToHost, s));
+    return SGIPC_OK;
+}
+
+static bool same_pairs(const MasWork& m, const SgipcContacts* con) {
+    const void* p = con && con->pair_num > 0 ? (const void*)con->pairs : nullptr;
+    const int n = con && con->pair_num > 0 ? con->pair_num : 0;
+    return p == m.hier_pairs && n == m.hier_pair_num;
+}
+
+SgipcStatus mas_mark_start(SgipcCtx* c, cudaStream_t s) {
+    SG_CHECK(c, cudaEventRecord(c->mas.ev_start, s));
+    return SGIPC_OK;
+}
+
+SgipcStatus mas_prebuild(SgipcCtx* c, const SgipcContacts* con, cudaStream_t s) {
+    MasWork& m = c->mas;
+    (void)s;
+    // the side stream rewrites the tables only after the work queued before the assembly
+    // (a previous solve reads them)
+    SG_CHECK(c, cudaStreamWaitEvent(m.side, m.ev_start, 0));
+    SgipcStatus st = mas_hierarchy(c, con, m.side);
+    if (st != SGIPC_OK) return st;
+    SG_CHECK(c, cudaEventRecord(m.ev_hier, m.side));
+    m.hier_pending = 1;
+    m.hier_pairs = con && con->pair_num > 0 ? (const void*)con->pairs : nullptr;
+    m.hier_pair_num = con && con->pair_num > 0 ? con->pair_num : 0;
+    return SGIPC_OK;
+}
+
+SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, cudaStream_t s) {
+    MasWork& m = c->mas;
+    if (!c->assembled) return SGIPC_NOT_READY;
+    const int L = m.levelnum;
+    if (m.hier_pending) {
+        // the prebuilt hierarchy (or, for other contacts, its end before this one rewrites it)
+        SG_CHECK(c, cudaStreamWaitEvent(s, m.ev_hier, 0));
+        SG_CHECK(c, cudaEventSynchronize(m.ev_hier));
+    }
+    if (!m.hier_pending || !same_pairs(m, con)) {
+        SgipcStatus st = mas_hierarchy(c, con, s);
+        if (st != SGIPC_OK) return st;
+        SG_CHECK(c, cudaStreamSynchronize(s));
+    }
+    m.hier_pending = 0;
+    memcpy(m.h_info, m.h_info_pinned, sizeof(int) * 17);
     const int total = m.h_info[16];
     if (total > m.total_cap || total <= 0) {
         snprintf(c->err, sizeof(c->err), "MAS cluster count %d exceeds capacity %d", total, m.total_cap);
@@ -630,7 +686,7 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     // restricted vectors: entries outside the current levels' nodes must read as zero
     SG_CHECK(c, cudaMemsetAsync(m.R64, 0, sizeof(double) * 3 * (size_t)total * c->max_rhs, s));
     SG_CHECK(c, cudaMemsetAsync(m.R32, 0, sizeof(float) * 3 * (size_t)total * c->max_rhs, s));
-    SG_COUNT(c, 1);
+    SG_COUNT(c, 4);
     const int l_top = top_levels(m);
     k_fill_level0<<<nblk(256LL * nd0), SGIPC_BLOCK, 0, s>>>(nd0, m.map0, c->val64, m.dom64);
     k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L, m.info,
