@@ -1014,7 +1014,11 @@ extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const 
     if (st != SGIPC_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     SG_CHECK(c, cudaSetDevice(c->device));
+    // the MAS hierarchy of these contacts on its own stream, first (it needs the contact
+    // graph only; started before the assembly kernels, it runs beside them and
+    // sgipc_mas_build reuses it)
     if ((st = mas_mark_start(c, s)) != SGIPC_OK) return st;
+    if ((st = mas_prebuild(c, k, s)) != SGIPC_OK) return st;
     c->btype = f->BoundaryType;
     c->last_fem = *f;
     c->last_prm = *p;
@@ -1022,21 +1026,29 @@ extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const 
     if (k) c->last_con = *k;
     SG_COUNT(c, 2 + (c->nsoft > 0));
     k_kinetic<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, f->vertexes, f->xTilta, f->masses, c->shape_grads, c->fb);
-    int m = launch_contacts(c, f, k, p, c->fb, s);
+    // contacts (fb, contact block slots) on asm_stream, elements (element blocks, static
+    // matrix, shape_grads) on s; the merge needs the soft-constraint slots from s, the
+    // right-hand side both
+    cudaStream_t sc = c->asm_stream;
+    SG_CHECK(c, cudaEventRecord(c->ev_asm[0], s));
+    SG_CHECK(c, cudaStreamWaitEvent(sc, c->ev_asm[0], 0));
+    int m = launch_contacts(c, f, k, p, c->fb, sc);
+    SG_LAUNCH_CHECK(c, "contact kernels");
+    if ((st = launch_fem(c, f, p, s)) != SGIPC_OK) return st;
+    if ((st = gather_static(c, f, s)) != SGIPC_OK) return st;
     if (c->nsoft > 0) {
         BlockSink bs = sink(c, f);
         k_soft<<<nblk(c->nsoft), SGIPC_BLOCK, 0, s>>>(c->nsoft, c->soft_idx, f->vertexes, f->targetVert,
                                                       p->motionRate * p->softRate * p->softRate, c->shape_grads, bs, m);
         m += c->nsoft;
     }
-    SG_LAUNCH_CHECK(c, "contact kernels");
-    if ((st = launch_fem(c, f, p, s)) != SGIPC_OK) return st;
-    if ((st = gather_static(c, f, s)) != SGIPC_OK) return st;
-    if ((st = merge_contacts(c, m, s)) != SGIPC_OK) return st;
+    SG_CHECK(c, cudaEventRecord(c->ev_asm[1], s));
+    SG_CHECK(c, cudaStreamWaitEvent(sc, c->ev_asm[1], 0));
+    if ((st = merge_contacts(c, m, sc)) != SGIPC_OK) return st;
+    SG_CHECK(c, cudaEventRecord(c->ev_asm[2], sc));
+    SG_CHECK(c, cudaStreamWaitEvent(s, c->ev_asm[2], 0));
     k_rhs<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, c->fb, c->shape_grads, f->BoundaryType, c->b);
     SG_LAUNCH_CHECK(c, "rhs");
-    // the MAS hierarchy of these contacts, beside the assembly (sgipc_mas_build reuses it)
-    if ((st = mas_prebuild(c, k, s)) != SGIPC_OK) return st;
     c->assembled = 1;
     c->mas.built = 0;
     return SGIPC_OK;

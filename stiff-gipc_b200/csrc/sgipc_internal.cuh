@@ -91,7 +91,9 @@ struct MasWork {
     // matrix), overlapping the assembly; consumed by the next mas_build with the same pairs
     cudaStream_t side;
     cudaEvent_t ev_start, ev_hier;
-    int* h_info_pinned;      // [32] pinned landing area of the level counts
+    int* h_info_pinned;      // [32] pinned landing area of the level counts (and [21]: abort)
+    int* hier_part;          // [32] chunk totals of the fused hierarchy kernel's scan
+    int hier_grid;           // CTAs of the fused hierarchy kernel (0: per-level kernels), -1 unset
     int hier_pending;
     const void* hier_pairs;
     int hier_pair_num;
@@ -200,6 +202,10 @@ struct SgipcCtx {
     double* dot_out;          // [16]
     double* h_pinned;         // host pinned scalars
     cudaStream_t cap_stream;  // capture stream
+    // assembly: the contact kernels and their merge run on asm_stream beside the element
+    // kernels on the caller's stream (joined before the right-hand side)
+    cudaStream_t asm_stream;
+    cudaEvent_t ev_asm[3];
     int max_blocks;           // reduction grid cap
 };
 

@@ -63,24 +63,25 @@ __global__ void k_mask_edges(int nnz, const int* __restrict__ row, const int* __
     mask_or_warp(mask, bit ? a : -1, bit);
 }
 
-__global__ void k_mask_pairs(int np, const int4* __restrict__ pairs, int nv, const int* __restrict__ node,
-                             uint32_t* __restrict__ mask) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
+// The connectivity bits of one contact pair (its decoded vertices, all ordered pairs inside
+// one bank); every lane of the warp calls it (idle lanes: e = nullptr).
+__device__ __forceinline__ void mask_pair_warp(const int4* e_ptr, int nv, const int* __restrict__ node,
+                                               uint32_t* __restrict__ mask) {
     int v[4] = {-1, -1, -1, -1}, n = 0;
-    const int4 e = p < np ? pairs[p] : make_int4(0, 0, 0, 0);
-    if (p >= np) {
-        // idle lane: no vertices, but it still joins the warp-wide ORs below
-    } else if (e.x >= 0) {
-        v[0] = e.x; v[1] = e.y; v[2] = e.z; v[3] = e.w < 0 ? -e.w - 1 : e.w; n = 4;
-    } else {
-        v[0] = -e.x - 1;
-        if (e.z < 0) {
-            if (e.y < 0) { v[1] = -e.y - 1; v[2] = -e.z - 1; v[3] = -e.w - 1; n = 4; }
-            else { v[1] = e.y; n = 2; }
-        } else if (e.w < 0) {
-            if (e.y < 0) { v[1] = -e.y - 1; v[2] = e.z; v[3] = -e.w - 1; n = 4; }
-            else { v[1] = e.y; v[2] = e.z; n = 3; }
-        } else { v[1] = e.y; v[2] = e.z; v[3] = e.w; n = 4; }
+    if (e_ptr) {
+        const int4 e = *e_ptr;
+        if (e.x >= 0) {
+            v[0] = e.x; v[1] = e.y; v[2] = e.z; v[3] = e.w < 0 ? -e.w - 1 : e.w; n = 4;
+        } else {
+            v[0] = -e.x - 1;
+            if (e.z < 0) {
+                if (e.y < 0) { v[1] = -e.y - 1; v[2] = -e.z - 1; v[3] = -e.w - 1; n = 4; }
+                else { v[1] = e.y; n = 2; }
+            } else if (e.w < 0) {
+                if (e.y < 0) { v[1] = -e.y - 1; v[2] = e.z; v[3] = -e.w - 1; n = 4; }
+                else { v[1] = e.y; v[2] = e.z; n = 3; }
+            } else { v[1] = e.y; v[2] = e.z; v[3] = e.w; n = 4; }
+        }
     }
     int a[4] = {-1, -1, -1, -1};
     for (int i = 0; i < n; i++) a[i] = (v[i] >= 0 && v[i] < nv) ? node[v[i]] : -1;
@@ -96,17 +97,19 @@ __global__ void k_mask_pairs(int np, const int4* __restrict__ pairs, int nv, con
         }
 }
 
-// Half a warp per bank, lane i holding node i's connectivity row: components by repeated
-// squaring of the reachability rows (each round doubles the path length, so five rounds
-// close 16 nodes), numbered by their lowest lane.  At level 0 the padding positions
-// (part_map < 0) are no node and form no component (_preparePrefixSumL0_new /
-// _buildLevel1_new skip them, MASPreconditioner.cu:157-270).
-__global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, int level,
-                                  const uint32_t* __restrict__ mask, const int* __restrict__ part_map,
-                                  int* __restrict__ rank, int* __restrict__ bank_cnt) {
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int bk = gt >> 4, i = gt & 15;
-    const int count = info[8 + level];
+__global__ void k_mask_pairs(int np, const int4* __restrict__ pairs, int nv, const int* __restrict__ node,
+                             uint32_t* __restrict__ mask) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    mask_pair_warp(p < np ? pairs + p : nullptr, nv, node, mask);
+}
+
+// Half a warp per bank (bk; all 32 lanes call it), writing its nodes' component ranks and
+// its component count (bank_cnt[bk], for bk <= bank_last; zero beyond the level's banks).
+__device__ __forceinline__ void bank_components_half(int bk, int bank_last, int count, int level,
+                                                     const uint32_t* __restrict__ mask,
+                                                     const int* __restrict__ part_map, int* __restrict__ rank,
+                                                     int* __restrict__ bank_cnt) {
+    const int i = threadIdx.x & 15;
     const int nbank = (count + 15) >> 4;
     const int lo = bk << 4;
     const bool inb = bk < nbank;
@@ -125,7 +128,19 @@ __global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, i
     const int lead = __ffs(m) - 1;
     const uint32_t leaders = (__ballot_sync(0xffffffffu, real && lead == i) >> (threadIdx.x & 16)) & 0xffffu;
     if (inb && lo + i < count) rank[lo + i] = lead < 0 ? 0 : __popc(leaders & ((1u << lead) - 1u));
-    if (i == 0 && bk <= nbank_cap) bank_cnt[bk] = inb ? __popc(leaders) : 0;
+    if (i == 0 && bk <= bank_last) bank_cnt[bk] = inb ? __popc(leaders) : 0;
+}
+
+// Half a warp per bank, lane i holding node i's connectivity row: components by repeated
+// squaring of the reachability rows (each round doubles the path length, so five rounds
+// close 16 nodes), numbered by their lowest lane.  At level 0 the padding positions
+// (part_map < 0) are no node and form no component (_preparePrefixSumL0_new /
+// _buildLevel1_new skip them, MASPreconditioner.cu:157-270).
+__global__ void k_bank_components(int nbank_cap, const int* __restrict__ info, int level,
+                                  const uint32_t* __restrict__ mask, const int* __restrict__ part_map,
+                                  int* __restrict__ rank, int* __restrict__ bank_cnt) {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    bank_components_half(gt >> 4, nbank_cap, info[8 + level], level, mask, part_map, rank, bank_cnt);
 }
 
 __global__ void k_assign(int nv, int L, int level, const int* __restrict__ bank_off, const int* __restrict__ rank,
@@ -483,6 +498,184 @@ static int num_levels(int nodes) {
     return nLevel > SGIPC_MAX_LEVELS ? SGIPC_MAX_LEVELS : nLevel;
 }
 
+// ---- the whole hierarchy as one cooperative launch -------------------------------------------
+// The phases of the per-level kernels below (level-0 init; per level: mask reset, edge and
+// pair masks, bank components, the exclusive scan of the component counts, assignment;
+// then the level-1 bank ranges) separated by grid barriers: one launch instead of about
+// thirty runtime calls, which matters because the hierarchy is enqueued beside the
+// assembly and the host's enqueue time is on the critical path.  Barrier words live in
+// info[20] (arrivals) and info[21] (abort, set when a wait exceeds its limit).
+constexpr int kHierThreads = 256;
+constexpr int kHierMaxCtas = 32;
+constexpr long long kHierSpinLimit = 1LL << 24;
+
+struct HierArgs {
+    int nv, npos, L, nnbr, npairs;
+    const int* real_map;
+    const int* part_map;
+    const int* nbr_row;
+    const int* nbr;
+    const int4* pairs;
+    int* node;
+    int* table;
+    int* up;
+    int* info;
+    uint32_t* mask;
+    int* rank;
+    int* bank_cnt;
+    int* bank_off;
+    int* part;      // [gridDim.x] chunk totals of the scan (bank_off's tail beyond the banks)
+    int* l1_first;
+    int* l1_last;
+};
+
+__device__ bool hier_barrier(int* info, unsigned int& epoch) {
+    __shared__ int s_ok;
+    __syncthreads();
+    epoch++;
+    if (threadIdx.x == 0) {
+        unsigned int* cnt = reinterpret_cast<unsigned int*>(info + 20);
+        volatile unsigned int* abort = reinterpret_cast<volatile unsigned int*>(info + 21);
+        __threadfence();
+        atomicAdd(cnt, 1u);
+        const unsigned int target = epoch * gridDim.x;
+        int ok = 1;
+        for (long long k = 0;; k++) {
+            if ((int)(*reinterpret_cast<volatile unsigned int*>(cnt) - target) >= 0) break;
+            if (*abort) {
+                ok = 0;
+                break;
+            }
+            if (k > kHierSpinLimit) {
+                atomicExch(reinterpret_cast<unsigned int*>(info + 21), 1u);
+                ok = 0;
+                break;
+            }
+            if (k > 64) __nanosleep(64);
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
+    typedef cub::BlockScan<int, kHierThreads> Scan;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ int s_carry;
+    unsigned int epoch = 0;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const int gw = tid >> 5, nw = nth >> 5;  // global warp index / count
+    int* info = h.info;
+    // level 0: positions
+    if (tid == 0) {
+        info[0] = 0;
+        info[8] = h.npos;
+        if (h.L == 1) info[16] = h.npos;
+    }
+    for (int v = tid; v < max(h.nv, h.npos); v += nth) {
+        if (v < h.npos) h.up[v] = -1;  // padding positions have no parent
+        if (v < h.nv) {
+            const int p = h.real_map[v];
+            h.node[v] = p;
+            h.table[(size_t)v * h.L] = p;
+        }
+    }
+    if (!hier_barrier(info, epoch)) return;
+    for (int l = 0; l + 1 < h.L; l++) {
+        const int count = info[8 + l], start = info[l];
+        const int nbank = (count + 15) >> 4;
+        for (int k = tid; k < count; k += nth) h.mask[k] = 0u;
+        if (!hier_barrier(info, epoch)) return;
+        // edge masks (one lane per neighbour slot) and contact-pair masks, warp-aggregated
+        for (int k0 = gw * 32; k0 < h.nnbr; k0 += nw * 32) {
+            const int k = k0 + lane;
+            int a = -1;
+            uint32_t bit = 0;
+            if (k < h.nnbr) {
+                a = h.node[h.nbr_row[k]];
+                const int b = h.node[h.nbr[k]];
+                if (a != b && (a >> 4) == (b >> 4)) bit = 1u << (b & 15);
+            }
+            mask_or_warp(h.mask, bit ? a : -1, bit);
+        }
+        for (int p0 = gw * 32; p0 < h.npairs; p0 += nw * 32)
+            mask_pair_warp(p0 + lane < h.npairs ? h.pairs + p0 + lane : nullptr, h.nv, h.node, h.mask);
+        if (!hier_barrier(info, epoch)) return;
+        // components, half a warp per bank; bank nbank gets a zero count (the scan's total)
+        for (int b0 = gw * 2; b0 <= nbank; b0 += nw * 2)
+            bank_components_half(b0 + (lane >> 4), nbank, count, l, h.mask, h.part_map, h.rank, h.bank_cnt);
+        if (!hier_barrier(info, epoch)) return;
+        // exclusive scan of bank_cnt[0 .. nbank]: per CTA a chunk, then the chunk offsets
+        const int n1 = nbank + 1, cs = (n1 + gridDim.x - 1) / gridDim.x;
+        const int c0 = min(n1, (int)blockIdx.x * cs), c1 = min(n1, c0 + cs);
+        if (threadIdx.x == 0) s_carry = 0;
+        __syncthreads();
+        for (int t0 = c0; t0 < c1; t0 += blockDim.x) {
+            const int i = t0 + threadIdx.x;
+            int x = i < c1 ? h.bank_cnt[i] : 0, y, agg;
+            Scan(scan_tmp).ExclusiveSum(x, y, agg);
+            const int carry = s_carry;
+            if (i < c1) h.bank_off[i] = y + carry;
+            __syncthreads();
+            if (threadIdx.x == 0) s_carry = carry + agg;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) h.part[blockIdx.x] = s_carry;
+        if (!hier_barrier(info, epoch)) return;
+        if (threadIdx.x < 32) {
+            int o = 0;
+            for (int k = threadIdx.x; k < (int)blockIdx.x; k += 32) o += h.part[k];
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) o += __shfl_xor_sync(0xffffffffu, o, d);
+            if (threadIdx.x == 0) s_carry = o;
+        }
+        __syncthreads();
+        for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) h.bank_off[i] += s_carry;
+        if (!hier_barrier(info, epoch)) return;
+        // assignment of the next level's ids
+        const int start_next = start + ((count + 15) & ~15);
+        if (tid == 0) {
+            info[l + 1] = start_next;
+            info[8 + l + 1] = h.bank_off[nbank];
+            if (l + 2 == h.L) info[16] = start_next + ((h.bank_off[nbank] + 15) & ~15);
+        }
+        for (int v = tid; v < h.nv; v += nth) {
+            const int a = h.node[v];
+            const int nn = h.bank_off[a >> 4] + h.rank[a];
+            h.node[v] = nn;
+            h.table[(size_t)v * h.L + l + 1] = start_next + nn;
+            h.up[start + a] = start_next + nn;  // every vertex of node a writes the same parent
+            if (l + 2 == h.L) h.up[start_next + nn] = -1;
+        }
+        if (!hier_barrier(info, epoch)) return;
+    }
+    if (h.L >= 3) {
+        const int nb0 = h.npos >> 4;
+        for (int k = tid; k < nb0 + 2; k += nth) {
+            h.l1_first[k] = 0x7f7f7f7f;
+            h.l1_last[k] = -1;
+        }
+        if (!hier_barrier(info, epoch)) return;
+        const int start1 = info[1];
+        for (int b = tid; b < nb0; b += nth) {
+            int lo = 0x7fffffff, hi = -1;
+            for (int k = 0; k < 16; k++) {
+                const int g = h.up[16 * b + k];
+                if (g < 0) continue;
+                lo = min(lo, (g - start1) >> 4);
+                hi = max(hi, (g - start1) >> 4);
+            }
+            for (int m = lo; m <= hi; m++) {
+                atomicMin(h.l1_first + m, b);
+                atomicMax(h.l1_last + m, b);
+            }
+        }
+    }
+}
+
 // For each level-1 bank m (nodes 16 m .. 16 m + 15): the first and last level-0 bank whose
 // positions have a parent in it.  Level-1 ids grow with the level-0 bank (components are
 // numbered bank by bank), so the banks in between feed m as well.
@@ -576,6 +769,14 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
     SG_CHECK(c, cudaEventCreateWithFlags(&m.ev_start, cudaEventDisableTiming));
     SG_CHECK(c, cudaEventCreateWithFlags(&m.ev_hier, cudaEventDisableTiming));
     SG_CHECK(c, cudaMallocHost((void**)&m.h_info_pinned, sizeof(int) * 32));
+    SG_CHECK(c, cudaMalloc((void**)&m.hier_part, sizeof(int) * kHierMaxCtas));
+    {
+        int coop = 0, nsm = 0, per = 0;
+        SG_CHECK(c, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
+        SG_CHECK(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+        SG_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_hierarchy, kHierThreads, 0));
+        m.hier_grid = coop && per > 0 ? (nsm * per < kHierMaxCtas ? nsm * per : kHierMaxCtas) : 0;
+    }
     size_t tb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tb, m.bank_cnt, m.bank_off, m.npos / 16 + 2);
     m.scan_tmp_bytes = tb + 256;
@@ -592,6 +793,7 @@ void mas_destroy(SgipcCtx* c) {
     if (m.ev_start) cudaEventDestroy(m.ev_start);
     if (m.ev_hier) cudaEventDestroy(m.ev_hier);
     if (m.h_info_pinned) cudaFreeHost(m.h_info_pinned);
+    if (m.hier_part) cudaFree(m.hier_part);
     void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.nbr_row, m.table, m.up, m.node, m.mask, m.comp_rank, m.bank_cnt,
                     m.bank_off, m.map0, m.l1_first, m.l1_last, m.info, m.dom64, m.dom32, m.R64, m.Z64, m.R32, m.Z32,
                     m.scan_tmp};
@@ -605,6 +807,37 @@ static SgipcStatus mas_hierarchy(SgipcCtx* c, const SgipcContacts* con, cudaStre
     MasWork& m = c->mas;
     const int nv = c->nv, L = m.levelnum;
     const int nbank_cap = m.npos / 16 + 1;
+    if (m.hier_grid > 0) {  // one cooperative launch
+        HierArgs h;
+        h.nv = nv;
+        h.npos = m.npos;
+        h.L = L;
+        h.nnbr = m.nnbr;
+        h.npairs = con && con->pair_num > 0 ? con->pair_num : 0;
+        h.real_map = m.real_map;
+        h.part_map = m.part_map;
+        h.nbr_row = m.nbr_row;
+        h.nbr = m.nbr;
+        h.pairs = h.npairs ? (const int4*)con->pairs : nullptr;
+        h.node = m.node;
+        h.table = m.table;
+        h.up = m.up;
+        h.info = m.info;
+        h.mask = m.mask;
+        h.rank = m.comp_rank;
+        h.bank_cnt = m.bank_cnt;
+        h.bank_off = m.bank_off;
+        h.part = m.hier_part;
+        h.l1_first = m.l1_first;
+        h.l1_last = m.l1_last;
+        SG_CHECK(c, cudaMemsetAsync(m.info + 20, 0, 2 * sizeof(int), s));
+        void* args[] = {&h};
+        SG_COUNT(c, 1);
+        SG_CHECK(c, cudaLaunchCooperativeKernel((const void*)k_hierarchy, dim3(m.hier_grid), dim3(kHierThreads), args,
+                                                0, s));
+        SG_CHECK(c, cudaMemcpyAsync(m.h_info_pinned, m.info, sizeof(int) * 22, cudaMemcpyDeviceToHost, s));
+        return SGIPC_OK;
+    }
     k_init_level0<<<nblk(nv > m.npos ? nv : m.npos), SGIPC_BLOCK, 0, s>>>(nv, m.real_map, L, m.node, m.table,
                                                                           m.info, m.npos, m.up);
     SG_COUNT(c, 1 + (L - 1) * (3 + (con && con->pair_num > 0)) + (L >= 3));
@@ -628,7 +861,8 @@ static SgipcStatus mas_hierarchy(SgipcCtx* c, const SgipcContacts* con, cudaStre
         k_l1_ranges<<<nblk(m.npos / 16), SGIPC_BLOCK, 0, s>>>(m.npos, m.up, m.info, m.l1_first, m.l1_last);
     }
     SG_LAUNCH_CHECK(c, "mas hierarchy");
-    SG_CHECK(c, cudaMemcpyAsync(m.h_info_pinned, m.info, sizeof(int) * 17, cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaMemsetAsync(m.info + 21, 0, sizeof(int), s));
+    SG_CHECK(c, cudaMemcpyAsync(m.h_info_pinned, m.info, sizeof(int) * 22, cudaMemcpyDeviceToHost, s));
     return SGIPC_OK;
 }
 
@@ -673,6 +907,10 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
         SG_CHECK(c, cudaStreamSynchronize(s));
     }
     m.hier_pending = 0;
+    if (m.h_info_pinned[21]) {
+        snprintf(c->err, sizeof(c->err), "mas: a grid barrier of the hierarchy build exceeded its wait limit");
+        return SGIPC_CUDA_ERROR;
+    }
     memcpy(m.h_info, m.h_info_pinned, sizeof(int) * 17);
     const int total = m.h_info[16];
     if (total > m.total_cap || total <= 0) {

@@ -654,6 +654,8 @@ SgipcStatus pcg_create(SgipcCtx* c) {
     SG_CHECK(c, cudaMalloc((void**)&c->dot_out, sizeof(double) * 16));
     SG_CHECK(c, cudaMallocHost((void**)&c->h_pinned, sizeof(double) * 64));
     SG_CHECK(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+    SG_CHECK(c, cudaStreamCreateWithFlags(&c->asm_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : c->ev_asm) SG_CHECK(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return SGIPC_OK;
 }
 
@@ -665,6 +667,12 @@ void pcg_destroy(SgipcCtx* c) {
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    if (c->asm_stream) {
+        cudaStreamSynchronize(c->asm_stream);
+        cudaStreamDestroy(c->asm_stream);
+    }
+    for (cudaEvent_t e : c->ev_asm)
+        if (e) cudaEventDestroy(e);
 }
 
 template <class T>
