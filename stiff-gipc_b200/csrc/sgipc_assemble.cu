@@ -909,6 +909,17 @@ static BlockSink sink(SgipcCtx* c, const SgipcFemData* f) {
     return bs;
 }
 
+// contact block slots launch_contacts will use (soft constraints follow them)
+static int contact_slots(const SgipcContacts* k, const SgipcParams* p) {
+    if (!k) return 0;
+    int m = 0;
+    if (k->pair_num > 0) m += 10 * k->pair_num;
+    if (k->fric_num > 0 && p->frictionRate > 0.0) m += 10 * k->fric_num;
+    if (k->ground_num > 0) m += k->ground_num;
+    if (k->fric_gd_num > 0 && p->gd_frictionRate > 0.0) m += k->fric_gd_num;
+    return m;
+}
+
 // launch the contact kernels; returns the number of contact block slots used
 static int launch_contacts(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k, const SgipcParams* p,
                            double* grad, cudaStream_t s) {
@@ -1029,22 +1040,24 @@ extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const 
     // contacts (fb, contact block slots) on asm_stream, elements (element blocks, static
     // matrix, shape_grads) on s; the merge needs the soft-constraint slots from s, the
     // right-hand side both
+    // (the soft constraints go first on s: the merge needs their block slots, and they add
+    // to shape_grads before the element gradients do)
     cudaStream_t sc = c->asm_stream;
+    const int m_con = contact_slots(k, p);
+    if (c->nsoft > 0) {
+        BlockSink bs = sink(c, f);
+        k_soft<<<nblk(c->nsoft), SGIPC_BLOCK, 0, s>>>(c->nsoft, c->soft_idx, f->vertexes, f->targetVert,
+                                                      p->motionRate * p->softRate * p->softRate, c->shape_grads, bs,
+                                                      m_con);
+    }
     SG_CHECK(c, cudaEventRecord(c->ev_asm[0], s));
     SG_CHECK(c, cudaStreamWaitEvent(sc, c->ev_asm[0], 0));
     int m = launch_contacts(c, f, k, p, c->fb, sc);
     SG_LAUNCH_CHECK(c, "contact kernels");
+    m += c->nsoft;
+    if ((st = merge_contacts(c, m, sc)) != SGIPC_OK) return st;
     if ((st = launch_fem(c, f, p, s)) != SGIPC_OK) return st;
     if ((st = gather_static(c, f, s)) != SGIPC_OK) return st;
-    if (c->nsoft > 0) {
-        BlockSink bs = sink(c, f);
-        k_soft<<<nblk(c->nsoft), SGIPC_BLOCK, 0, s>>>(c->nsoft, c->soft_idx, f->vertexes, f->targetVert,
-                                                      p->motionRate * p->softRate * p->softRate, c->shape_grads, bs, m);
-        m += c->nsoft;
-    }
-    SG_CHECK(c, cudaEventRecord(c->ev_asm[1], s));
-    SG_CHECK(c, cudaStreamWaitEvent(sc, c->ev_asm[1], 0));
-    if ((st = merge_contacts(c, m, sc)) != SGIPC_OK) return st;
     SG_CHECK(c, cudaEventRecord(c->ev_asm[2], sc));
     SG_CHECK(c, cudaStreamWaitEvent(s, c->ev_asm[2], 0));
     k_rhs<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, c->fb, c->shape_grads, f->BoundaryType, c->b);

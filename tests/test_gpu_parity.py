@@ -25,9 +25,22 @@ from sgipc import scenes, system  # noqa: E402
 from sgipc import _native as N  # noqa: E402
 
 
-@pytest.fixture(scope="module", params=["c1_cube", "cube_touch", "two_cubes", "cloth_on_cube"])
+def _soft_cube():
+    """A touching cube with soft constraints pulling a few vertices toward offset targets."""
+    sc = scenes.scene_cube(5, touching=True, seed=4)
+    idx = np.arange(0, sc.nv, 11, dtype=np.int32)
+    sc.soft_index = idx
+    sc.soft_target = sc.vertexes[idx] + np.array([1e-3, 2e-3, -1e-3])
+    sc.params["motionRate"] = 1.0
+    sc.params["softRate"] = 1.0
+    return sc
+
+
+@pytest.fixture(scope="module", params=["c1_cube", "cube_touch", "two_cubes", "cloth_on_cube", "cube_soft"])
 def case(request):
-    if request.param == "c1_cube":
+    if request.param == "cube_soft":
+        sc = _soft_cube()
+    elif request.param == "c1_cube":
         # the smallest workload: an 11^3 cube 0.05 m above the ground, no contact yet
         sc = scenes.scene_cube(11, touching=False, seed=0)
     elif request.param == "cube_touch":
