@@ -34,6 +34,18 @@ struct PcgScalars {
     int32_t pcur;     // which of the two p buffers holds the current direction
     int32_t halt;     // [rhs 0 only] set once the loop must stop; later bodies return at once
     int32_t pad;
+    double rz_ref;    // refinement epilogue: r64 . M r64 and r64 . r64 of the FP64 residual
+    double rr_ref;
+};
+
+// Mixed-precision refinement run by the persistent FP32 solve as its epilogue: x64 += x,
+// r64 = b64 - A x64 (FP64 matrix), then r64 . M r64 (FP32 MAS) and r64 . r64 into the
+// solve's scalars.  done = true when the epilogue ran (else the caller refines itself).
+struct RefineArgs {
+    double* x64;
+    const double* b64;
+    double* r64;
+    bool done;
 };
 
 // One precision's PCG workspace (T = double or float) for up to `nrhs` right-hand sides.
@@ -303,7 +315,7 @@ SgipcStatus dot64(SgipcCtx* c, const double* a, const double* b, int n, double* 
 // cannot co-schedule it (the caller then runs the graph of per-phase kernels).
 template <class T, class M, int NR>
 SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
-                         cudaStream_t s, bool* used);
+                         cudaStream_t s, bool* used, RefineArgs* ref = nullptr);
 // largest grid run_pcg_coop launches on `device` (sizes its reduction buffers)
 int coop_max_grid(int device);
 // BAD_INPUT if a kernel flagged an invalid input since the last check (synchronises)

@@ -571,14 +571,15 @@ SgipcStatus get_loop_graph(SgipcCtx* c, PcgWork& w, const M* inv, M* R, M* Z, in
 // One PCG solve of A x = b (b, x: interleaved [3n][NR], b FP64, x in T) with MAS type M.
 template <class T, class M, int NR>
 SgipcStatus run_pcg(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
-                    cudaStream_t s, int tag) {
+                    cudaStream_t s, int tag, RefineArgs* ref = nullptr) {
     MasWork& m = c->mas;
     const M* inv = fp32_mas ? (const M*)m.dom32 : (const M*)m.dom64;
     M* R = fp32_mas ? (M*)m.R32 : (M*)m.R64;
     M* Z = fp32_mas ? (M*)m.Z32 : (M*)m.Z64;
     // one persistent kernel for the whole solve where the device co-schedules it
     bool coop = false;
-    SgipcStatus st = run_pcg_coop<T, M, NR>(c, w, fp32_mas, b, tol, max_iter, crit, s, &coop);
+    if (ref) ref->done = false;
+    SgipcStatus st = run_pcg_coop<T, M, NR>(c, w, fp32_mas, b, tol, max_iter, crit, s, &coop, ref);
     if (st != SGIPC_OK || coop) return st;
     const int k3grid = domain_grid(c);
     st = get_loop_graph<T, M, NR>(c, w, inv, R, Z, k3grid, tag);
@@ -767,23 +768,32 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
             double inner_tol = tol;
             if (rz0 > 0 && rz > 0) inner_tol = fmin(1.0, fmax(tol * rz0 / rz, 1e-10));
             if (crit == SGIPC_CRIT_TRUE && bn2 > 0 && rz > 0) inner_tol = tol;
-            st = run_pcg<float, float, 1>(c, c->pcg32, 1, r64, inner_tol, max_iter, (int)crit, s, 20);
+            // the persistent solve refines itself where it can (x += x32, FP64 residual, its
+            // r.z and r.r); otherwise the same steps follow here
+            RefineArgs rf{x, b, r64, false};
+            st = run_pcg<float, float, 1>(c, c->pcg32, 1, r64, inner_tol, max_iter, (int)crit, s, 20, &rf);
             if (st != SGIPC_OK) return st;
-            SG_COUNT(c, 2);
-            k_add_f32<<<nblk(n3), 256, 0, s>>>(n3, (const float*)c->pcg32.x, x);
-            // r = b - A x in FP64
-            if ((st = spmv_t<double>(c, x, c->tmp64b, s)) != SGIPC_OK) return st;
-            k_axpby_res<<<nblk(n3), 256, 0, s>>>(n3, b, c->tmp64b, r64);
             PcgScalars hs;
+            if (!rf.done) {
+                SG_COUNT(c, 2);
+                k_add_f32<<<nblk(n3), 256, 0, s>>>(n3, (const float*)c->pcg32.x, x);
+                // r = b - A x in FP64
+                if ((st = spmv_t<double>(c, x, c->tmp64b, s)) != SGIPC_OK) return st;
+                k_axpby_res<<<nblk(n3), 256, 0, s>>>(n3, b, c->tmp64b, r64);
+                // rz of the refined residual with the same (FP32) preconditioner
+                if ((st = mas_apply_t<double>(c, r64, c->tmp64b, 1, s)) != SGIPC_OK) return st;
+                if ((st = dot64(c, r64, c->tmp64b, n3, c->dot_out, s)) != SGIPC_OK) return st;
+                if ((st = dot64(c, r64, r64, n3, c->dot_out + 1, s)) != SGIPC_OK) return st;
+                SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            }
             SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg32.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
-            // rz of the refined residual with the same (FP32) preconditioner
-            if ((st = mas_apply_t<double>(c, r64, c->tmp64b, 1, s)) != SGIPC_OK) return st;
-            if ((st = dot64(c, r64, c->tmp64b, n3, c->dot_out, s)) != SGIPC_OK) return st;
-            if ((st = dot64(c, r64, r64, n3, c->dot_out + 1, s)) != SGIPC_OK) return st;
-            SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
             SG_CHECK(c, cudaMemcpyAsync(input_flag(c), c->dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
             SG_CHECK(c, cudaStreamSynchronize(s));
             if (*input_flag(c)) return input_error(c, s);
+            if (rf.done) {
+                c->h_pinned[0] = hs.rz_ref;
+                c->h_pinned[1] = hs.rr_ref;
+            }
             total_it += hs.iter;
             SG_COUNT(c, 4LL * hs.bodies);
             if (ref == 0) {

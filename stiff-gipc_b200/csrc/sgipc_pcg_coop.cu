@@ -89,6 +89,11 @@ struct CoopArgs {
     int l2mode;
     const int* l1_first;
     const int* l1_last;
+    // refinement epilogue (FP32 inner solve, one right-hand side; x64 == nullptr: none)
+    double* x64;
+    const double* b64;
+    double* r64;
+    MatView<double> A64;
 };
 
 __device__ __forceinline__ void red_add_release_gpu(unsigned int* p, unsigned int v) {
@@ -591,7 +596,8 @@ __device__ void phase_update(const CoopArgs<T, M, NR>& a, const double (&alpha)[
 // old residual (identical arithmetic), so that every CTA holds its level-1 bank complete
 // (level-1 sums: the same 16-lane groups and order as bank_reduce_store), keeps it in shared
 // memory and restricts it to level 2 itself.
-template <class T, class M, int NR, bool kInit>
+// kMode: 0 update, 1 init (r = b, x = 0), 2 restriction of the FP64 vector r_src only
+template <class T, class M, int NR, int kMode>
 __device__ void phase_positions_l2(const CoopArgs<T, M, NR>& a, const double (&alpha)[NR], const T* p,
                                    const T* r_old, T* r_new, const bool (&run)[NR], double (&acc)[NR],
                                    M (*s_l1)[3 * NR]) {
@@ -616,14 +622,19 @@ __device__ void phase_positions_l2(const CoopArgs<T, M, NR>& a, const double (&a
             for (int k = 0; k < NR * 3; k++) val[k] = 0;
             if (v >= 0) {
                 T pq[3][NR];
-                if (!kInit)
+                if (kMode == 0)
 #pragma unroll
                     for (int q = 0; q < 3; q++) ldn<true, T, NR>(p + (size_t)(3 * v + q) * NR, pq[q]);
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
                     const size_t k = (size_t)(3 * v + q) * NR;
                     T rv[NR];
-                    if (kInit) {
+                    if (kMode == 2) {
+                        double sv[NR];
+                        ldn<true, double, NR>(a.r64 + k, sv);
+#pragma unroll
+                        for (int r = 0; r < NR; r++) rv[r] = (T)sv[r];
+                    } else if (kMode == 1) {
                         double bv[NR];
                         ldn<false, double, NR>(a.b + k, bv);
                         T tx[NR];
@@ -659,7 +670,7 @@ __device__ void phase_positions_l2(const CoopArgs<T, M, NR>& a, const double (&a
                         }
                     }
 #pragma unroll
-                    for (int r = 0; r < NR; r++) val[r * 3 + q] = (kInit || run[r]) ? (M)rv[r] : (M)0;
+                    for (int r = 0; r < NR; r++) val[r * 3 + q] = (kMode != 0 || run[r]) ? (M)rv[r] : (M)0;
                 }
             }
             if (own && bank <= b_hi) store_levels01<M, NR>(a.R, pos, val);
@@ -683,6 +694,57 @@ __device__ void phase_positions_l2(const CoopArgs<T, M, NR>& a, const double (&a
             bank_reduce_store<M, NR>(ok ? __ldg(mv.up + start1 + a1) : -1, v1, a.R);
         }
         __syncthreads();  // s_l1 is rewritten for the next bank
+    }
+}
+
+// ---- refinement epilogue of the mixed solve (FP32 inner solve, one right-hand side) --------
+// x64 += x (the inner solve's correction)
+template <class T, class M, int NR>
+__device__ void phase_accumulate64(const CoopArgs<T, M, NR>& a) {
+    const int n3 = 3 * a.tp.n;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x)
+        a.x64[k] += (double)__ldcg(a.x + k);
+}
+
+// r64 = b64 - A x64 with the FP64 matrix, r64 . r64
+template <class T, class M, int NR>
+__device__ void phase_residual64(const CoopArgs<T, M, NR>& a, double& rr) {
+    Operand<double, 1, true> op;  // x64 was written by every CTA: read through L2
+    op.a = a.x64;
+    op.b = nullptr;
+    op.beta[0] = 0.0;
+    constexpr int gpw = 32 / kSpG;
+    const int lane = threadIdx.x & 31, n = a.tp.n;
+    for (int i0 = grid_warp() * gpw; i0 < n; i0 += grid_warps() * gpw) {  // warp-uniform bound
+        const int i = i0 + lane / kSpG, g = lane % kSpG;
+        double acc[1][3];
+        row_mv<double, 1>(a.tp, a.A64, op, i, g, acc);
+        if (i < n && g == 0)
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const double r = a.b64[3 * (size_t)i + q] - acc[0][q];
+                a.r64[3 * (size_t)i + q] = r;
+                rr += r * r;
+            }
+    }
+}
+
+// r64 . z with z = M r64 from the current Z (as the prolongation, z in T)
+template <class T, class M, int NR>
+__device__ void phase_prolong_ref(const CoopArgs<T, M, NR>& a, double& rz) {
+    const MasView& mv = a.mv;
+    for (int v = spread_warp() * 32 + (int)(threadIdx.x & 31); v < a.nv; v += gridDim.x * blockDim.x) {
+        const int* tv = mv.table + (size_t)v * mv.L;
+        M s0 = 0, s1 = 0, s2 = 0;
+        for (int l = 0; l < mv.L; l++) {
+            const int gl = __ldg(tv + l);
+            s0 += a.Z[3 * (size_t)gl];
+            s1 += a.Z[3 * (size_t)gl + 1];
+            s2 += a.Z[3 * (size_t)gl + 2];
+        }
+        const size_t k = 3 * (size_t)v;
+        rz += __ldcg(a.r64 + k) * (double)(T)s0 + __ldcg(a.r64 + k + 1) * (double)(T)s1 +
+              __ldcg(a.r64 + k + 2) * (double)(T)s2;
     }
 }
 
@@ -780,7 +842,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
     T* rcur = a.r;
     T* ralt = a.r2;
     if (a.l2mode)
-        phase_positions_l2<T, M, NR, true>(a, S.alpha, nullptr, nullptr, rcur, S.run, v, s_l1);
+        phase_positions_l2<T, M, NR, 1>(a, S.alpha, nullptr, nullptr, rcur, S.run, v, s_l1);
     else
         phase_init(a, v);
     bool ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);  // starts with __syncthreads
@@ -839,7 +901,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
         if (a.l2mode) {
-            phase_positions_l2<T, M, NR, false>(a, S.alpha, pnew, rcur, ralt, S.run, v, s_l1);
+            phase_positions_l2<T, M, NR, 0>(a, S.alpha, pnew, rcur, ralt, S.run, v, s_l1);
             T* t2 = rcur;
             rcur = ralt;
             ralt = t2;
@@ -873,10 +935,32 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
             }
         __syncthreads();
     }
+    double rz_ref = 0.0, rr_ref = 0.0;
+    if constexpr (sizeof(T) == 4 && NR == 1) {
+        if (ok && a.x64 && a.l2mode) {
+            // x64 += x; r64 = b64 - A x64; r64 . r64; M r64 (FP32 MAS); r64 . M r64
+            phase_accumulate64(a);
+            ok = grid_barrier(a.br, ++epoch);
+            v[0] = 0.0;
+            if (ok) phase_residual64(a, v[0]);
+            ok = ok && grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);
+            rr_ref = t[0];
+            v[0] = 0.0;
+            if (ok) phase_positions_l2<T, M, NR, 2>(a, S.alpha, nullptr, nullptr, nullptr, S.run, v, s_l1);
+            ok = ok && grid_barrier(a.br, ++epoch);
+            ok = ok && phase_mas(a, sR, epoch, dcache, ndc);
+            v[0] = 0.0;
+            if (ok) phase_prolong_ref(a, v[0]);
+            ok = ok && grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);
+            rz_ref = t[0];
+        }
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
 #pragma unroll
         for (int r = 0; r < NR; r++) {
             PcgScalars& sc = a.sc[r];
+            sc.rz_ref = rz_ref;
+            sc.rr_ref = rr_ref;
             sc.iter = S.iters[r];
             sc.rz0 = S.rz0[r];
             sc.rz = S.rz[r];
@@ -957,7 +1041,7 @@ SgipcStatus coop_configure(SgipcCtx* c, SgipcCtx::CoopCfg& cfg) {
 
 template <class T, class M, int NR>
 SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
-                         cudaStream_t s, bool* used) {
+                         cudaStream_t s, bool* used, RefineArgs* ref) {
     *used = false;
     const char* e = getenv("SGIPC_PCG_GRAPH");
     if (e && e[0] == '1') return SGIPC_OK;  // the graph of per-phase kernels instead
@@ -1004,6 +1088,12 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     a.l2mode = L >= 3 && grid >= 2;
     a.l1_first = m.l1_first;
     a.l1_last = m.l1_last;
+    const bool refine = ref && sizeof(T) == 4 && NR == 1 && a.l2mode;
+    a.x64 = refine ? ref->x64 : nullptr;
+    a.b64 = refine ? ref->b64 : nullptr;
+    a.r64 = refine ? ref->r64 : nullptr;
+    a.A64 = mat_view<double>(c);
+    if (ref) ref->done = refine;
     a.max_iter = max_iter;
     a.crit = crit;
     a.tol = tol;
@@ -1020,7 +1110,7 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
 
 #define SGIPC_COOP_INST(T, M, NR)                                                                             \
     template SgipcStatus run_pcg_coop<T, M, NR>(SgipcCtx*, PcgWork&, int, const double*, double, int, int, \
-                                                cudaStream_t, bool*);
+                                                cudaStream_t, bool*, RefineArgs*);
 SGIPC_COOP_INST(double, double, 1)
 SGIPC_COOP_INST(double, float, 1)
 SGIPC_COOP_INST(float, float, 1)
