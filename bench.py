@@ -120,6 +120,19 @@ def cpu_solves(sc, count):
     return time.perf_counter() - t0
 
 
+def max_over_ranks(values, world, device):
+    """The job's times: every rank's device-timed values, maximum over the ranks (each rank
+    runs an independent replica of the workload; the whole job takes as long as the
+    slowest one)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -219,10 +232,7 @@ def run_ours(args):
     barrier()
     clk = clocks.stop()
 
-    times = torch.tensor([t_mixed, t_fp64, t_e2e, t_adj], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    t_mixed, t_fp64, t_e2e, t_adj = times.tolist()
+    t_mixed, t_fp64, t_e2e, t_adj = max_over_ranks([t_mixed, t_fp64, t_e2e, t_adj], world, "cuda")
     units = world * args.steps
 
     # roofline of the dominant kernel: per-step share = avg launch time x launches per step
