@@ -204,6 +204,19 @@ def test_persistent_and_graph_solves_agree(case, prec, monkeypatch):
         assert _rel(xa, xb) < (1e-9 if prec == "fp64" else 1e-4)
 
 
+def test_mas_build_with_other_contacts_rebuilds_the_hierarchy(case):
+    """sgipc_assemble prebuilds the hierarchy for its contacts; a build given other contacts
+    (here none) must build its own, equal to the oracle's for those contacts."""
+    sc, g, (ob, orow, ocol, oval) = case
+    g.computeGradientAndHessian()
+    N.check(N.lib().sgipc_mas_build(g.ctx, None, N.PRECISION["fp64"], None), g.ctx)
+    om = oracle.Mas(sc, orow, ocol, oval, pairs=np.zeros((0, 4), np.int32))
+    mas = system.MASPreconditioner(g)
+    assert np.array_equal(mas.tables(), om.table())
+    mas.setPreconditioner("fp64")  # back to the assembled contacts
+    assert np.array_equal(mas.tables(), oracle.Mas(sc, orow, ocol, oval).table())
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_zero_rhs_gives_zero_solution(case, prec):
     sc, g, _ = case
