@@ -6,20 +6,27 @@
 // are separated by grid barriers instead of kernel boundaries.  At the sizes of one Newton
 // system (~20k block rows, ~25 MB of matrix, hierarchy and vectors, all L2-resident) an
 // iteration is a handful of dependent L2 round trips, so the design minimises round trips
-// per phase and barrier latency.  Per iteration:
+// per phase and barrier latency.  Per iteration, with three or more MAS levels:
 //   spmv    p = z + beta p_old (ping-pong buffers), Ap = A p, p.Ap          -> barrier + sum
-//   update  x += alpha p, r -= alpha Ap, restriction to MAS levels 0/1, r.r   -> barrier + sum
-//   mas 1   level-0/1 domain solves; restriction level 1 -> 2                 -> barrier
-//   mas 2   CTA 0: restriction to levels >= 3 and their domains; others: level-2 domains
-//                                                                             -> barrier
+//   update  x += alpha p, r_new = r_old - alpha Ap (two residual buffers), r.r, restriction
+//           to MAS levels 0, 1 and 2: CTAs aligned to level-1 banks (phase_positions_l2)
+//                                                                         -> barrier + sum
+//   mas     level-0..2 domain solves on all CTAs but the last, which restricts 2 -> 3 ->
+//           ... and solves the few domains above                           -> barrier
 //   prolong z = sum_l Z, r.z                                               -> barrier + sum
+// With one or two levels the update restricts to levels 0/1 only and the MAS takes two
+// phases (level 0/1 domains with the restriction 1 -> 2; then the coarser levels).  The
+// mixed solve's FP32 instance ends with the refinement epilogue (x64 += x, the FP64
+// residual, its r.z and r.r).  Shared memory holds each CTA's SpMV rows, their contact
+// blocks and its first level-0/1 domain inverses for the whole solve.
 // Barrier: one monotonic arrival counter (release add; acquire polling until it reaches
 // epoch x grid).  Dot products: every CTA stores its partial before arriving; after the
 // barrier every CTA adds all partials in the same fixed order, so all CTAs take identical
 // decisions from identical numbers (partials are double-buffered by epoch parity).  Values
 // written by one CTA and read by another inside the kernel are loaded through L2
-// (ld.global.cg).  Waits are bounded: past the limit a CTA raises the abort word, every
-// CTA leaves, and the solve reports SGIPC_CUDA_ERROR.
+// (ld.global.cg) or, after the barrier's gpu-scope fence, through L1.  Waits are bounded:
+// past the limit a CTA raises the abort word, every CTA leaves, and the solve reports
+// SGIPC_CUDA_ERROR.
 #include <cstdlib>
 
 #include "sgipc_internal.cuh"
