@@ -777,7 +777,7 @@ __global__ void k_run_heads(int m, const unsigned long long* __restrict__ ks, in
 // u, start[nuc] = end of the last run; row / column of every unique block
 __global__ void k_run_starts(int m, const unsigned long long* __restrict__ ks, const int* __restrict__ rid, int bits,
                              int* __restrict__ start, int* __restrict__ uc_row, int* __restrict__ uc_col,
-                             int* __restrict__ nuc) {
+                             int* __restrict__ nuc, int* __restrict__ lcount) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > m) return;
     if (i == m) {
@@ -797,13 +797,19 @@ __global__ void k_run_starts(int m, const unsigned long long* __restrict__ ks, c
     const int u = rid[i];
     start[u] = i;
     const unsigned long long mask = (1ull << bits) - 1ull;
-    uc_row[u] = (int)(k >> bits);
-    uc_col[u] = (int)(k & mask);
+    const int row = (int)(k >> bits), col = (int)(k & mask);
+    uc_row[u] = row;
+    uc_col[u] = col;
+    // off-diagonal blocks also appear transposed, in the list of row `col`
+    if (row != col) atomicAdd(lcount + col, 1);
 }
 
+// ... and entry q of the transposed copy at slot lpos[u] gets entry q of the block, at its
+// transposed place 3 (q % 3) + q / 3
 __global__ void k_run_sums(int m, const int* __restrict__ nuc, const int* __restrict__ start,
-                           const int* __restrict__ is, const double* __restrict__ cval, double* __restrict__ u64,
-                           float* __restrict__ u32) {
+                           const int* __restrict__ is, const double* __restrict__ cval, const int* __restrict__ lpos,
+                           double* __restrict__ u64, float* __restrict__ u32, double* __restrict__ l64,
+                           float* __restrict__ l32) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int u = (int)(t / 9), q = (int)(t % 9);
     if (u >= nuc[0]) return;
@@ -813,60 +819,54 @@ __global__ void k_run_sums(int m, const int* __restrict__ nuc, const int* __rest
     for (int j = j0; j < j1; j++) acc += cval[9 * (size_t)is[j] + q];
     u64[9 * (size_t)u + q] = acc;
     u32[9 * (size_t)u + q] = (float)acc;
-}
-
-__global__ void k_lower_keys(int m, const int* __restrict__ nuc, const int* __restrict__ uc_row,
-                             const int* __restrict__ uc_col, int bits, unsigned long long* __restrict__ lk,
-                             int* __restrict__ li) {
-    int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= m) return;
-    li[u] = u;
-    if (u < nuc[0] && uc_row[u] != uc_col[u])
-        lk[u] = ((unsigned long long)uc_col[u] << bits) | (unsigned long long)uc_row[u];
-    else
-        lk[u] = kBadKey;
-}
-
-// row pointers: first index whose row field >= i (binary search over sorted keys / rows)
-__global__ void k_row_ptr_rows(int n, const int* __restrict__ nuc, const int* __restrict__ rows, int* __restrict__ ptr) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > n) return;
-    int lo = 0, hi = nuc[0];
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (rows[mid] < i) lo = mid + 1; else hi = mid;
-    }
-    ptr[i] = lo;
-}
-
-// each transposed contact entry: its column (the row field of its (col << bits | row) key)
-// and the transpose of its block, so that the SpMV reads both lists the same way
-__global__ void k_lower_cols(int m, const unsigned long long* __restrict__ ks, int bits, const int* __restrict__ cl_idx,
-                             const double* __restrict__ u64, int* __restrict__ cl_col, double* __restrict__ l64,
-                             float* __restrict__ l32) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= m) return;
-    cl_col[k] = (int)(ks[k] & ((1ull << bits) - 1ull));
-    if (ks[k] == kBadKey) return;
-    const double* src = u64 + 9 * (size_t)cl_idx[k];
-#pragma unroll
-    for (int q = 0; q < 9; q++) {
-        const double v = src[3 * (q % 3) + q / 3];
-        l64[9 * (size_t)k + q] = v;
-        l32[9 * (size_t)k + q] = (float)v;
+    const int k = lpos[u];
+    if (k >= 0) {
+        const int qt = 3 * (q % 3) + q / 3;
+        l64[9 * (size_t)k + qt] = acc;
+        l32[9 * (size_t)k + qt] = (float)acc;
     }
 }
 
-__global__ void k_row_ptr_keys(int n, int m, const unsigned long long* __restrict__ ks, int bits, int* __restrict__ ptr) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > n) return;
-    unsigned long long target = (unsigned long long)i << bits;
-    int lo = 0, hi = m;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (ks[mid] < target) lo = mid + 1; else hi = mid;
+// upper row pointers (thread i <= n: first unique block whose row >= i, by binary search over
+// the row-sorted blocks) and placement of each off-diagonal block u in the transposed list of
+// row uc_col[u], in the order the atomics hand out the slots
+__global__ void k_lower_place(int m, int n, const int* __restrict__ nuc, const int* __restrict__ uc_row,
+                              const int* __restrict__ uc_col, const int* __restrict__ cl_ptr, int* __restrict__ fill,
+                              int* __restrict__ cu_ptr, int* __restrict__ cl_idx) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nu = nuc[0];
+    if (t <= n) {
+        int lo = 0, hi = nu;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (uc_row[mid] < t) lo = mid + 1; else hi = mid;
+        }
+        cu_ptr[t] = lo;
     }
-    ptr[i] = lo;
+    if (t < nu) {
+        const int col = uc_col[t];
+        if (uc_row[t] != col) cl_idx[cl_ptr[col] + atomicAdd(fill + col, 1)] = t;
+    }
+}
+
+// final slot of each off-diagonal block in its transposed list: its rank by row among the
+// blocks of the same column, so that every transposed list is sorted by column whatever order
+// the placement atomics took; lpos[u] = -1 for diagonal blocks
+__global__ void k_lower_rank(const int* __restrict__ nuc, const int* __restrict__ uc_row,
+                             const int* __restrict__ uc_col, const int* __restrict__ cl_ptr,
+                             const int* __restrict__ cl_idx, int* __restrict__ lpos, int* __restrict__ cl_col) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nuc[0]) return;
+    const int row = uc_row[u], col = uc_col[u];
+    if (row == col) {
+        lpos[u] = -1;
+        return;
+    }
+    const int k0 = cl_ptr[col], k1 = cl_ptr[col + 1];
+    int rank = 0;
+    for (int k = k0; k < k1; k++) rank += __ldg(uc_row + __ldg(cl_idx + k)) < row;
+    lpos[u] = k0 + rank;
+    cl_col[k0 + rank] = row;
 }
 
 }  // namespace
@@ -960,26 +960,30 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
         SG_CHECK(c, cudaMemsetAsync(c->cl_ptr, 0, sizeof(int) * (c->n + 1), s));
         return SGIPC_OK;
     }
-    const int endbit = 2 * c->key_bits;
-    SG_COUNT(c, 7);
+    const int endbit = 2 * c->key_bits, n = c->n;
+    SG_COUNT(c, 5);
     // keys sorted with their slot ids; runs of equal keys numbered by a scan of run heads;
     // each unique block summed by 9 threads (one per entry) over its run in sorted order
-    // (deterministic), with every load of a run independent of the previous one
+    // (deterministic), with every load of a run independent of the previous one.  The
+    // transposed lists need no second sort: the run heads count the blocks of each column,
+    // a scan of the counts gives the row pointers, and each block's rank by row within its
+    // column gives its slot.
+    SG_CHECK(c, cudaMemsetAsync(c->lcount, 0, sizeof(int) * (2 * (size_t)n + 1), s));
     size_t tb = c->cub_tmp_bytes;
     SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->ckey, c->ckey_s, c->cidx, c->cidx_s, m, 0, endbit, s));
     k_run_heads<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cflag);
     tb = c->cub_tmp_bytes;
     SG_CHECK(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp, tb, c->cflag, c->cflag, m + 1, s));
     k_run_starts<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey_s, c->cflag, c->key_bits, c->run_start, c->uc_row,
-                                                     c->uc_col, c->nuc);
-    k_run_sums<<<nblk(9LL * m), SGIPC_BLOCK, 0, s>>>(m, c->nuc, c->run_start, c->cidx_s, c->cval, c->uc64, c->uc32);
-    k_row_ptr_rows<<<nblk(c->n + 1), SGIPC_BLOCK, 0, s>>>(c->n, c->nuc, c->uc_row, c->cu_ptr);
-    k_lower_keys<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->nuc, c->uc_row, c->uc_col, c->key_bits, c->lkey, c->lidx);
+                                                     c->uc_col, c->nuc, c->lcount);
     tb = c->cub_tmp_bytes;
-    SG_CHECK(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tb, c->lkey, c->lkey_s, c->lidx, c->cl_idx, m, 0, endbit, s));
-    k_row_ptr_keys<<<nblk(c->n + 1), SGIPC_BLOCK, 0, s>>>(c->n, m, c->lkey_s, c->key_bits, c->cl_ptr);
-    k_lower_cols<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->lkey_s, c->key_bits, c->cl_idx, c->uc64, c->cl_col, c->cl64,
-                                                 c->cl32);
+    SG_CHECK(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp, tb, c->lcount, c->cl_ptr, n + 1, s));
+    k_lower_place<<<nblk(std::max(m, n + 1)), SGIPC_BLOCK, 0, s>>>(m, n, c->nuc, c->uc_row, c->uc_col, c->cl_ptr,
+                                                                   c->lcount + n + 1, c->cu_ptr, c->cl_idx);
+    k_lower_rank<<<nblk(m), SGIPC_BLOCK, 0, s>>>(c->nuc, c->uc_row, c->uc_col, c->cl_ptr, c->cl_idx, c->lpos,
+                                                 c->cl_col);
+    k_run_sums<<<nblk(9LL * m), SGIPC_BLOCK, 0, s>>>(m, c->nuc, c->run_start, c->cidx_s, c->cval, c->lpos, c->uc64,
+                                                     c->uc32, c->cl64, c->cl32);
     SG_LAUNCH_CHECK(c, "contact merge");
     return SGIPC_OK;
 }

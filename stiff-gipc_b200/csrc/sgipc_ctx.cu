@@ -246,9 +246,9 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
         (st = dalloc(c, &c->cflag, cap + 1)) || (st = dalloc(c, &c->nuc, 4)) || (st = dalloc(c, &c->uc_row, cap)) ||
         (st = dalloc(c, &c->uc_col, cap)) || (st = dalloc(c, &c->uc64, cap * 9)) ||
         (st = dalloc(c, &c->uc32, cap * 9)) || (st = dalloc(c, &c->cu_ptr, n + 1)) ||
-        (st = dalloc(c, &c->cl_ptr, n + 1)) || (st = dalloc(c, &c->cl_idx, cap)) || (st = dalloc(c, &c->lkey, cap)) ||
+        (st = dalloc(c, &c->cl_ptr, n + 1)) || (st = dalloc(c, &c->cl_idx, cap)) || (st = dalloc(c, &c->lcount, 2 * (size_t)n + 1)) ||
         (st = dalloc(c, &c->cl_col, cap)) || (st = dalloc(c, &c->cl64, cap * 9)) || (st = dalloc(c, &c->cl32, cap * 9)) ||
-        (st = dalloc(c, &c->lkey_s, cap)) || (st = dalloc(c, &c->lidx, cap)) || (st = dalloc(c, &c->dflag, 4)))
+        (st = dalloc(c, &c->lpos, cap)) || (st = dalloc(c, &c->dflag, 4)))
         return fail(st);
     SG_CHECK(c, cudaMemset(c->dflag, 0, 4 * sizeof(int)));
     // contact block keys are (row << bits) | col with row, col < 2^bits - 1, so that the
@@ -256,11 +256,12 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
     int bits = 1;
     while ((1LL << bits) < (long long)n + 2) bits++;
     c->key_bits = bits;
-    // CUB temporary storage: radix sort of cap pairs and an exclusive scan of cap ints
-    size_t b1 = 0, b2 = 0;
+    // CUB temporary storage: radix sort of cap pairs, exclusive scans of cap + 1 and n + 1 ints
+    size_t b1 = 0, b2 = 0, b3 = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, b1, c->ckey, c->ckey_s, c->cidx, c->cidx_s, (int)cap, 0, 64);
     cub::DeviceScan::ExclusiveSum(nullptr, b2, c->cflag, c->cflag, (int)cap + 1);
-    c->cub_tmp_bytes = std::max(b1, b2) + 256;
+    cub::DeviceScan::ExclusiveSum(nullptr, b3, c->lcount, c->cl_ptr, n + 1);
+    c->cub_tmp_bytes = std::max(std::max(b1, b2), b3) + 256;
     if ((st = dalloc(c, (char**)&c->cub_tmp, c->cub_tmp_bytes)) != SGIPC_OK) return fail(st);
     SG_CHECK(c, cudaMemset(c->nuc, 0, 4 * sizeof(int)));
     if ((st = mas_create(c, t)) != SGIPC_OK) return fail(st);
@@ -280,7 +281,7 @@ extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
                     c->eblk, c->contrib_ptr, c->contrib, c->egrad, c->vinc_ptr, c->vinc, c->tets, c->tris,
                     c->hinges, c->hinge_adj, c->soft_idx, c->shape_grads, c->fb, c->b, c->ckey, c->ckey_s,
                     c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,
-                    c->cu_ptr, c->cl_ptr, c->cl_idx, c->lkey, c->lkey_s, c->lidx, c->cub_tmp, c->dflag,
+                    c->cu_ptr, c->cl_ptr, c->cl_idx, c->lcount, c->lpos, c->cub_tmp, c->dflag,
                     c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32, c->run_start};
     for (void* p : ptrs)
         if (p) cudaFree(p);

@@ -176,13 +176,12 @@ struct SgipcCtx {
     float* uc32;
     int* cu_ptr;                  // [n+1] unique contact blocks by row (upper)
     int* cl_ptr;                  // [n+1] transposed entries by row
-    int* cl_idx;                  // [cap]
-    int* cl_col;                  // [cap] column of each transposed entry (= uc_row[cl_idx])
-    double* cl64;                 // [cap*9] transposed copy of uc64[cl_idx[k]] (SpMV reads it directly)
+    int* cl_idx;                  // [cap] unique block of each transposed slot, in placement order
+    int* cl_col;                  // [cap] column of each transposed entry (= uc_row of its block)
+    double* cl64;                 // [cap*9] transposed copy of the block (SpMV reads it directly)
     float* cl32;
-    unsigned long long* lkey;     // [cap]
-    unsigned long long* lkey_s;
-    int* lidx;
+    int* lcount;                  // [2n+1] transposed entries per row [0, n], then fill cursors [n+1, 2n]
+    int* lpos;                    // [cap] transposed slot of each unique block (-1: diagonal)
     void* cub_tmp;
     size_t cub_tmp_bytes;
     int key_bits;
