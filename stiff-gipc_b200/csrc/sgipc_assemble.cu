@@ -1014,6 +1014,7 @@ static SgipcStatus launch_fem(SgipcCtx* c, const SgipcFemData* f, const SgipcPar
 }
 
 static SgipcStatus gather_static(SgipcCtx* c, const SgipcFemData* f, cudaStream_t s) {
+    c->mas.pre_scattered = 0;  // a scatter of the previous static matrix is stale
     SG_COUNT(c, 1 + (c->n_egrad > 0));
     k_gather_blocks<<<nblk(9LL * c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->contrib_ptr, c->contrib, c->eblk, c->slot_row,
                                                                 c->col, f->BoundaryType, f->masses, static_out(c));
@@ -1062,6 +1063,8 @@ extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const 
     if ((st = merge_contacts(c, m, sc)) != SGIPC_OK) return st;
     if ((st = launch_fem(c, f, p, s)) != SGIPC_OK) return st;
     if ((st = gather_static(c, f, s)) != SGIPC_OK) return st;
+    // the static blocks into the prebuilt hierarchy's domains, on the MAS stream beside the merge
+    if ((st = mas_prescatter(c, s)) != SGIPC_OK) return st;
     SG_CHECK(c, cudaEventRecord(c->ev_asm[2], sc));
     SG_CHECK(c, cudaStreamWaitEvent(s, c->ev_asm[2], 0));
     k_rhs<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, c->fb, c->shape_grads, f->BoundaryType, c->b);

@@ -103,6 +103,11 @@ struct MasWork {
     // matrix), overlapping the assembly; consumed by the next mas_build with the same pairs
     cudaStream_t side;
     cudaEvent_t ev_start, ev_hier;
+    // static blocks scattered into the domains on `side` once the hierarchy and the static
+    // matrix are ready (ev_static: static matrix written on the caller's stream; ev_pre: the
+    // scatter done), overlapping the contact merge; consumed with the prebuilt hierarchy
+    cudaEvent_t ev_static, ev_pre;
+    int pre_scattered;
     int* h_info_pinned;      // [32] pinned landing area of the level counts (and [21]: abort)
     int* hier_part;          // [32] chunk totals of the fused hierarchy kernel's scan
     int hier_grid;           // CTAs of the fused hierarchy kernel (0: per-level kernels), -1 unset
@@ -301,6 +306,8 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
 SgipcStatus mas_prebuild(SgipcCtx* c, const SgipcContacts* con, cudaStream_t s);
 // Record the point of s after which the side stream may rewrite the hierarchy.
 SgipcStatus mas_mark_start(SgipcCtx* c, cudaStream_t s);
+// after the static matrix is written on s: scatter it into the prebuilt hierarchy's domains
+SgipcStatus mas_prescatter(SgipcCtx* c, cudaStream_t s);
 // z = M^-1 r for T in {double, float}; r, z are [3n] vectors of T (rz accumulated into
 // out_dot[0] when out_dot != nullptr, using r . z with r in T precision).
 template <class T>

@@ -227,6 +227,14 @@ __device__ __forceinline__ void scatter_block_warp(double* dom, const int* __res
 // The top levels' domain copies of the CTA: zeroed, filled by scatter_block_warp, then added
 // to the global domains (one atomic per non-zero entry and CTA instead of one per warp
 // group: every block of the grid lands on the few entries of these levels).
+// levels l >= l_top accumulated per CTA: the top levels (at most kTopLevels) whose nodes
+// form one domain starting on a domain boundary (info[l] = first node, info[8 + l] = count)
+__device__ __forceinline__ int top_levels_dev(const int* __restrict__ info, int L) {
+    int l = L;
+    while (l > 1 && L - (l - 1) <= kTopLevels && info[8 + l - 1] <= 16 && (info[l - 1] & 15) == 0) l--;
+    return l;
+}
+
 __device__ __forceinline__ void zero_top(int ntop, double (*s_top)[2304]) {
     for (int k = threadIdx.x; k < ntop * 2304; k += blockDim.x) s_top[k / 2304][k % 2304] = 0.0;
     __syncthreads();
@@ -243,9 +251,10 @@ __device__ __forceinline__ void flush_top(const int* __restrict__ info, int l_to
 
 __global__ void k_scatter_static(int nnz, const int* __restrict__ slot_row, const int* __restrict__ col,
                                  const double* __restrict__ val, const int* __restrict__ table, int L,
-                                 const int* __restrict__ info, int l_top, double* __restrict__ dom) {
+                                 const int* __restrict__ info, double* __restrict__ dom) {
     __shared__ double s_top[kTopLevels][2304];
-    const int ntop = L - l_top;
+    if (info[21]) return;  // aborted hierarchy build: the host rejects its tables
+    const int l_top = top_levels_dev(info, L), ntop = L - l_top;
     zero_top(ntop, s_top);
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = s < nnz;
@@ -259,9 +268,19 @@ __global__ void k_scatter_static(int nnz, const int* __restrict__ slot_row, cons
 // Level 0 of the static blocks, without atomics: the level-0 domains are the banks of the
 // fixed position map, so each entry (a, b) of domain d takes one static block (or its
 // transpose, or nothing) known at creation.  One thread per 3x3 entry writes it whole.
-__global__ void k_fill_level0(int nd0, const int* __restrict__ map0, const double* __restrict__ val,
-                              double* __restrict__ dom) {
+// The grid also zeroes the coarser domains [nd0, info[16] / 16) that the scatters add to
+// (at most ndom_cap domains in all).  Nothing is written after an aborted hierarchy build
+// (info[21] set), whose tables the host rejects.
+__global__ void k_fill_level0(int nd0, int ndom_cap, const int* __restrict__ map0, const double* __restrict__ val,
+                              const int* __restrict__ info, double* __restrict__ dom) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (info[21]) return;
+    {
+        const int ndom = min(info[16] / 16, ndom_cap);
+        const size_t n2 = ndom > nd0 ? (size_t)(ndom - nd0) * (2304 / 2) : 0;
+        double2* coarse = reinterpret_cast<double2*>(dom + (size_t)nd0 * 2304);
+        for (size_t e = t; e < n2; e += (size_t)gridDim.x * blockDim.x) coarse[e] = make_double2(0.0, 0.0);
+    }
     if (t >= nd0 * 256) return;
     const int d = t >> 8, a = (t >> 4) & 15, b = t & 15;
     const int m = map0[t];
@@ -286,9 +305,10 @@ __global__ void k_fill_level0(int nd0, const int* __restrict__ map0, const doubl
 
 __global__ void k_scatter_contact(int cap, const int* __restrict__ nuc, const int* __restrict__ ur,
                                   const int* __restrict__ uc, const double* __restrict__ val,
-                                  const int* __restrict__ table, int L, const int* __restrict__ info, int l_top,
+                                  const int* __restrict__ table, int L, const int* __restrict__ info,
                                   double* __restrict__ dom) {
     __shared__ double s_top[kTopLevels][2304];
+    const int l_top = top_levels_dev(info, L);
     int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x * blockDim.x >= nuc[0]) return;  // whole block beyond the unique blocks
     const int ntop = L - l_top;
@@ -480,12 +500,6 @@ template SgipcStatus mas_apply_t<float>(SgipcCtx*, const float*, float*, int, cu
 
 // First of the coarsest levels (at most kTopLevels, each with <= 16 nodes, i.e. one domain
 // starting at a multiple of 16) that the scatter accumulates per CTA; L when none.
-static int top_levels(const MasWork& m) {
-    int l = m.levelnum;
-    while (l > 1 && m.levelnum - (l - 1) <= kTopLevels && m.h_info[8 + l - 1] <= 16 && (m.h_info[l - 1] & 15) == 0) l--;
-    return l;
-}
-
 static int num_levels(int nodes) {
     int nLevel = 1;
     int levelSz = (nodes + 15) / 16 * 16;
@@ -768,6 +782,8 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
     SG_CHECK(c, cudaStreamCreateWithFlags(&m.side, cudaStreamNonBlocking));
     SG_CHECK(c, cudaEventCreateWithFlags(&m.ev_start, cudaEventDisableTiming));
     SG_CHECK(c, cudaEventCreateWithFlags(&m.ev_hier, cudaEventDisableTiming));
+    SG_CHECK(c, cudaEventCreateWithFlags(&m.ev_static, cudaEventDisableTiming));
+    SG_CHECK(c, cudaEventCreateWithFlags(&m.ev_pre, cudaEventDisableTiming));
     SG_CHECK(c, cudaMallocHost((void**)&m.h_info_pinned, sizeof(int) * 32));
     SG_CHECK(c, cudaMalloc((void**)&m.hier_part, sizeof(int) * kHierMaxCtas));
     {
@@ -792,6 +808,8 @@ void mas_destroy(SgipcCtx* c) {
     }
     if (m.ev_start) cudaEventDestroy(m.ev_start);
     if (m.ev_hier) cudaEventDestroy(m.ev_hier);
+    if (m.ev_static) cudaEventDestroy(m.ev_static);
+    if (m.ev_pre) cudaEventDestroy(m.ev_pre);
     if (m.h_info_pinned) cudaFreeHost(m.h_info_pinned);
     if (m.hier_part) cudaFree(m.hier_part);
     void* ptrs[] = {m.part_map, m.real_map, m.nbr_ptr, m.nbr, m.nbr_row, m.table, m.up, m.node, m.mask, m.comp_rank, m.bank_cnt,
@@ -886,9 +904,28 @@ SgipcStatus mas_prebuild(SgipcCtx* c, const SgipcContacts* con, cudaStream_t s) 
     SgipcStatus st = mas_hierarchy(c, con, m.side);
     if (st != SGIPC_OK) return st;
     SG_CHECK(c, cudaEventRecord(m.ev_hier, m.side));
+    SG_CHECK(c, cudaEventRecord(m.ev_pre, m.side));  // the last work on `side` (moved by a prescatter)
     m.hier_pending = 1;
     m.hier_pairs = con && con->pair_num > 0 ? (const void*)con->pairs : nullptr;
     m.hier_pair_num = con && con->pair_num > 0 ? con->pair_num : 0;
+    return SGIPC_OK;
+}
+
+SgipcStatus mas_prescatter(SgipcCtx* c, cudaStream_t s) {
+    MasWork& m = c->mas;
+    m.pre_scattered = 0;
+    if (!m.hier_pending) return SGIPC_OK;
+    const int nd0 = m.npos / 16;
+    SG_CHECK(c, cudaEventRecord(m.ev_static, s));
+    SG_CHECK(c, cudaStreamWaitEvent(m.side, m.ev_static, 0));
+    SG_COUNT(c, 2);
+    k_fill_level0<<<nblk(256LL * nd0), SGIPC_BLOCK, 0, m.side>>>(nd0, m.total_cap / 16, m.map0, c->val64, m.info,
+                                                                 m.dom64);
+    k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, m.side>>>(c->nnz, c->slot_row, c->col, c->val64, m.table,
+                                                               m.levelnum, m.info, m.dom64);
+    SG_LAUNCH_CHECK(c, "mas static scatter");
+    SG_CHECK(c, cudaEventRecord(m.ev_pre, m.side));
+    m.pre_scattered = 1;
     return SGIPC_OK;
 }
 
@@ -896,17 +933,21 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     MasWork& m = c->mas;
     if (!c->assembled) return SGIPC_NOT_READY;
     const int L = m.levelnum;
+    const bool reuse = m.hier_pending && same_pairs(m, con);
+    const bool pre = reuse && m.pre_scattered;
     if (m.hier_pending) {
-        // the prebuilt hierarchy (or, for other contacts, its end before this one rewrites it)
-        SG_CHECK(c, cudaStreamWaitEvent(s, m.ev_hier, 0));
+        // the prebuilt hierarchy and static scatter (or, for other contacts or a stale scatter,
+        // their end before this build rewrites them)
+        SG_CHECK(c, cudaStreamWaitEvent(s, m.ev_pre, 0));
         SG_CHECK(c, cudaEventSynchronize(m.ev_hier));
     }
-    if (!m.hier_pending || !same_pairs(m, con)) {
+    if (!reuse) {
         SgipcStatus st = mas_hierarchy(c, con, s);
         if (st != SGIPC_OK) return st;
         SG_CHECK(c, cudaStreamSynchronize(s));
     }
     m.hier_pending = 0;
+    m.pre_scattered = 0;
     if (m.h_info_pinned[21]) {
         snprintf(c->err, sizeof(c->err), "mas: a grid barrier of the hierarchy build exceeded its wait limit");
         return SGIPC_CUDA_ERROR;
@@ -918,19 +959,20 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
         return SGIPC_CAPACITY;
     }
     const int ndom = total / 16, nd0 = m.npos / 16;
-    // level 0 is written whole by k_fill_level0; the coarser domains start from zero
-    if (ndom > nd0)
-        SG_CHECK(c, cudaMemsetAsync(m.dom64 + (size_t)nd0 * 2304, 0, sizeof(double) * 2304 * (size_t)(ndom - nd0), s));
     // restricted vectors: entries outside the current levels' nodes must read as zero
     SG_CHECK(c, cudaMemsetAsync(m.R64, 0, sizeof(double) * 3 * (size_t)total * c->max_rhs, s));
     SG_CHECK(c, cudaMemsetAsync(m.R32, 0, sizeof(float) * 3 * (size_t)total * c->max_rhs, s));
-    SG_COUNT(c, 4);
-    const int l_top = top_levels(m);
-    k_fill_level0<<<nblk(256LL * nd0), SGIPC_BLOCK, 0, s>>>(nd0, m.map0, c->val64, m.dom64);
-    k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L, m.info,
-                                                          l_top, m.dom64);
+    if (!pre) {
+        // level 0 written whole and the coarser domains zeroed, then the static blocks added
+        SG_COUNT(c, 2);
+        k_fill_level0<<<nblk(256LL * nd0), SGIPC_BLOCK, 0, s>>>(nd0, m.total_cap / 16, m.map0, c->val64, m.info,
+                                                                m.dom64);
+        k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L,
+                                                              m.info, m.dom64);
+    }
+    SG_COUNT(c, 2);
     k_scatter_contact<<<nblk(c->cap_cblk), SGIPC_BLOCK, 0, s>>>(c->cap_cblk, c->nuc, c->uc_row, c->uc_col, c->uc64,
-                                                               m.table, L, m.info, l_top, m.dom64);
+                                                               m.table, L, m.info, m.dom64);
     const int w64 = prec == SGIPC_FP64 ? 1 : 0, w32 = prec == SGIPC_FP64 ? 0 : 1;
     k_invert<<<ndom, 192, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
     SG_LAUNCH_CHECK(c, "mas matrices");
@@ -964,9 +1006,10 @@ SgipcStatus mas_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
     SG_COUNT(c, 1);
     if (!strcmp(name, "mas_scatter")) {  // static blocks: level-0 fill + coarser levels' scatter
         SG_COUNT(c, 1);
-        k_fill_level0<<<nblk(256LL * (m.npos / 16)), SGIPC_BLOCK, 0, s>>>(m.npos / 16, m.map0, c->val64, m.dom64);
+        k_fill_level0<<<nblk(256LL * (m.npos / 16)), SGIPC_BLOCK, 0, s>>>(m.npos / 16, m.total_cap / 16, m.map0,
+                                                                         c->val64, m.info, m.dom64);
         k_scatter_static<<<nblk(c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->slot_row, c->col, c->val64, m.table, L,
-                                                               m.info, top_levels(m), m.dom64);
+                                                               m.info, m.dom64);
         *bytes = (double)c->nnz * (72 + 8) + (double)c->nv * L * 4 + (double)ndom * 2304 * 8;
     } else if (!strcmp(name, "mas_invert")) {
         k_invert<<<ndom, 192, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);

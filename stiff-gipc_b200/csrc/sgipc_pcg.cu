@@ -655,7 +655,12 @@ SgipcStatus pcg_create(SgipcCtx* c) {
     SG_CHECK(c, cudaMalloc((void**)&c->dot_out, sizeof(double) * 16));
     SG_CHECK(c, cudaMallocHost((void**)&c->h_pinned, sizeof(double) * 64));
     SG_CHECK(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
-    SG_CHECK(c, cudaStreamCreateWithFlags(&c->asm_stream, cudaStreamNonBlocking));
+    // the contact merge is a chain of small dependent kernels on the assembly's critical path:
+    // its stream gets the highest priority, so that its blocks go ahead of the element and MAS
+    // kernels running beside it
+    int prio_least = 0, prio_greatest = 0;
+    SG_CHECK(c, cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+    SG_CHECK(c, cudaStreamCreateWithPriority(&c->asm_stream, cudaStreamNonBlocking, prio_greatest));
     for (cudaEvent_t& e : c->ev_asm) SG_CHECK(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return SGIPC_OK;
 }

@@ -217,6 +217,33 @@ def test_mas_build_with_other_contacts_rebuilds_the_hierarchy(case):
     assert np.array_equal(mas.tables(), oracle.Mas(sc, orow, ocol, oval).table())
 
 
+def test_mas_build_after_a_new_static_matrix_uses_it(case):
+    """sgipc_assemble scatters its static blocks into the prebuilt hierarchy's domains ahead of
+    the build; a static matrix rewritten in between (sgipc_fem_grad_hess at other positions)
+    must replace them: the build equals one that scatters everything itself."""
+    sc, g, _ = case
+    mas = system.MASPreconditioner(g)
+    g.computeGradientAndHessian()
+    mas.setPreconditioner("fp64")
+    d0 = mas.domains()
+    tet2 = system.DeviceTetraData(sc)
+    gen = torch.Generator(device="cuda").manual_seed(8)
+    tet2.vertexes = tet2.vertexes + 1e-3 * torch.randn(tet2.vertexes.shape, dtype=torch.float64, device="cuda",
+                                                       generator=gen)
+    grad = torch.zeros(3 * sc.nv, dtype=torch.float64, device="cuda")
+    try:
+        g.computeGradientAndHessian()
+        g.calculate_fem_gradient_hessian(grad, tet2)
+        mas.setPreconditioner("fp64")  # the prebuilt hierarchy, its scatter stale
+        d1 = mas.domains()
+        mas.setPreconditioner("fp64")  # hierarchy rebuilt, everything scattered by the build
+        d2 = mas.domains()
+    finally:
+        g.computeGradientAndHessian()
+    assert _rel(d1, d2) < 1e-9
+    assert np.abs(d2 - d0).max() > 100 * np.abs(d1 - d2).max()
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_zero_rhs_gives_zero_solution(case, prec):
     sc, g, _ = case
