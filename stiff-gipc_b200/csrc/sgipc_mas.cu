@@ -321,87 +321,83 @@ __global__ void k_scatter_contact(int cap, const int* __restrict__ nuc, const in
     flush_top(info, l_top, ntop, s_top, dom);
 }
 
-// Gauss-Jordan inversion without pivoting, in place, one 48x48 domain per 192-thread CTA
-// with each thread holding a 4 x 3 tile in registers (rows 4 rg.., columns 3 cg..).  For
-// pivot k with p = A(k,k):  A(i,j) -= A(i,k) A(k,j) / p  (i, j != k);  A(k,j) = A(k,j) / p;
-// A(i,k) = -A(i,k) / p;  A(k,k) = 1 / p.  The pivot row, column and 1/p (computed once, by
-// the pivot's owner) are published through shared memory (double-buffered: one barrier per
-// step), so a thread reads 8 values and does 12 updates per step.  (Larger tiles, fewer
-// threads per domain, measured slower: the FP64 chain per step then dominates.)
-__global__ void __launch_bounds__(192) k_invert(int ndom, double* __restrict__ dom, float* __restrict__ dom32,
-                                                int write64, int write32) {
-    __shared__ double prow[2][48], pcol[2][48], pinv[2];
+// Gauss-Jordan inversion without pivoting, in place, one 48x48 domain per 64-thread CTA.
+// Thread 8 r + c holds the 6 x 6 tile of rows 6r.., columns 6c.. in registers.  For pivot k
+// with p = A(k,k):  A(i,j) -= A(i,k) A(k,j) / p  (i, j != k);  A(k,j) = A(k,j) / p;
+// A(i,k) = -A(i,k) / p;  A(k,k) = 1 / p.  The owners publish row k and column k to shared
+// memory (double-buffered: one barrier per step), and the pivot loop is unrolled by 6 so that
+// row k's and column k's offsets inside a tile are compile-time constants.  Six domains per
+// SM (three warps per scheduler, up to 170 registers, no spills) measured faster than one warp
+// per domain or eight two-warp domains per SM (128 registers, spilling).
+__global__ void __launch_bounds__(64, 6) k_invert(int ndom, double* __restrict__ dom, float* __restrict__ dom32,
+                                                  int write64, int write32) {
+    __shared__ __align__(16) double srow[2][48], scol[2][48];
     const int d = blockIdx.x;
     if (d >= ndom) return;
-    const int rg = threadIdx.x / 16, cg = threadIdx.x % 16;
-    const int i0 = 4 * rg, j0 = 3 * cg;
+    const int r = threadIdx.x >> 3, c = threadIdx.x & 7;
+    const int i0 = 6 * r, j0 = 6 * c;
     const double* D = dom + (size_t)d * 2304;
-    double t[4][3];
+    double t[6][6];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+    for (int a = 0; a < 6; a++)
 #pragma unroll
-        for (int b = 0; b < 3; b++) {
-            const double v = D[(i0 + a) * 48 + j0 + b];
-            t[a][b] = (i0 + a == j0 + b && v == 0.0) ? 1.0 : v;  // a zero diagonal (padding node) becomes 1
+        for (int b = 0; b < 6; b += 2) {
+            const double2 v = *reinterpret_cast<const double2*>(D + (i0 + a) * 48 + j0 + b);
+            // a zero diagonal (padding node) becomes 1
+            t[a][b] = (i0 + a == j0 + b && v.x == 0.0) ? 1.0 : v.x;
+            t[a][b + 1] = (i0 + a == j0 + b + 1 && v.y == 0.0) ? 1.0 : v.y;
         }
 #pragma unroll 1
-    for (int k = 0; k < 48; k++) {
-        const int q = k & 1;
-        // this tile holds row k (16 threads) / column k (12 threads) / the pivot (1 thread):
-        // the publishing and fix-up paths are branches only those threads take
-        const int ka = k - i0, kb = k - j0;
-        const bool own_r = (unsigned)ka < 4u, own_c = (unsigned)kb < 3u;
-        if (own_r) {  // publish row k (and 1 / A(k,k)) as it is before this step
+    for (int kk = 0; kk < 8; kk++) {  // pivots 6 kk .. 6 kk + 5: row group and column group kk
 #pragma unroll
-            for (int a = 0; a < 4; a++)
-                if (a == ka)
+        for (int j = 0; j < 6; j++) {
+            const int q = j & 1;
+            if (r == kk)  // row k = 6 kk + j as it is before this step
 #pragma unroll
-                    for (int b = 0; b < 3; b++) {
-                        prow[q][j0 + b] = t[a][b];
-                        if (b == kb) pinv[q] = 1.0 / t[a][b];
-                    }
-        }
-        if (own_c) {  // publish column k
+                for (int b = 0; b < 6; b += 2)
+                    *reinterpret_cast<double2*>(&srow[q][j0 + b]) = make_double2(t[j][b], t[j][b + 1]);
+            if (c == kk)  // column k
 #pragma unroll
-            for (int b = 0; b < 3; b++)
-                if (b == kb)
+                for (int a = 0; a < 6; a += 2)
+                    *reinterpret_cast<double2*>(&scol[q][i0 + a]) = make_double2(t[a][j], t[a + 1][j]);
+            __syncthreads();
+            double rk[6], ck[6];
 #pragma unroll
-                    for (int a = 0; a < 4; a++) pcol[q][i0 + a] = t[a][b];
-        }
-        __syncthreads();
-        const double ip = pinv[q];
-        double rk[3], ck[4];
+            for (int b = 0; b < 6; b += 2) {
+                const double2 v = *reinterpret_cast<const double2*>(&srow[q][j0 + b]);
+                rk[b] = v.x;
+                rk[b + 1] = v.y;
+            }
 #pragma unroll
-        for (int b = 0; b < 3; b++) rk[b] = prow[q][j0 + b] * ip;
+            for (int a = 0; a < 6; a += 2) {
+                const double2 v = *reinterpret_cast<const double2*>(&scol[q][i0 + a]);
+                ck[a] = v.x;
+                ck[a + 1] = v.y;
+            }
+            const double ip = 1.0 / srow[q][6 * kk + j];
 #pragma unroll
-        for (int a = 0; a < 4; a++) ck[a] = pcol[q][i0 + a];
+            for (int b = 0; b < 6; b++) rk[b] *= ip;
 #pragma unroll
-        for (int a = 0; a < 4; a++)
+            for (int a = 0; a < 6; a++)
 #pragma unroll
-            for (int b = 0; b < 3; b++) t[a][b] -= ck[a] * rk[b];
-        if (own_r) {  // the pivot row is set instead of updated
+                for (int b = 0; b < 6; b++) t[a][b] -= ck[a] * rk[b];
+            if (r == kk)  // the pivot row is set instead of updated
 #pragma unroll
-            for (int a = 0; a < 4; a++)
-                if (a == ka)
+                for (int b = 0; b < 6; b++) t[j][b] = rk[b];
+            if (c == kk)  // and so is the pivot column
 #pragma unroll
-                    for (int b = 0; b < 3; b++) t[a][b] = rk[b];
-        }
-        if (own_c) {  // and so is the pivot column
-#pragma unroll
-            for (int b = 0; b < 3; b++)
-                if (b == kb)
-#pragma unroll
-                    for (int a = 0; a < 4; a++) t[a][b] = (a == ka) ? ip : -ck[a] * ip;
+                for (int a = 0; a < 6; a++) t[a][j] = (r == kk && a == j) ? ip : -ck[a] * ip;
         }
     }
     double* Dw = dom + (size_t)d * 2304;
     float* Dw32 = dom32 + (size_t)d * 2304;
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+    for (int a = 0; a < 6; a++)
 #pragma unroll
-        for (int b = 0; b < 3; b++) {
-            if (write64) Dw[(i0 + a) * 48 + j0 + b] = t[a][b];
-            if (write32) Dw32[(i0 + a) * 48 + j0 + b] = (float)t[a][b];
+        for (int b = 0; b < 6; b += 2) {
+            const int o = (i0 + a) * 48 + j0 + b;
+            if (write64) *reinterpret_cast<double2*>(Dw + o) = make_double2(t[a][b], t[a][b + 1]);
+            if (write32) *reinterpret_cast<float2*>(Dw32 + o) = make_float2((float)t[a][b], (float)t[a][b + 1]);
         }
 }
 
@@ -974,7 +970,7 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
     k_scatter_contact<<<nblk(c->cap_cblk), SGIPC_BLOCK, 0, s>>>(c->cap_cblk, c->nuc, c->uc_row, c->uc_col, c->uc64,
                                                                m.table, L, m.info, m.dom64);
     const int w64 = prec == SGIPC_FP64 ? 1 : 0, w32 = prec == SGIPC_FP64 ? 0 : 1;
-    k_invert<<<ndom, 192, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
+    k_invert<<<ndom, 64, 0, s>>>(ndom, m.dom64, m.dom32, w64, w32);
     SG_LAUNCH_CHECK(c, "mas matrices");
     m.built = (int)prec + 1;
     return SGIPC_OK;
@@ -1012,7 +1008,7 @@ SgipcStatus mas_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
                                                                m.info, m.dom64);
         *bytes = (double)c->nnz * (72 + 8) + (double)c->nv * L * 4 + (double)ndom * 2304 * 8;
     } else if (!strcmp(name, "mas_invert")) {
-        k_invert<<<ndom, 192, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);
+        k_invert<<<ndom, 64, 0, s>>>(ndom, m.dom64, m.dom32, 1, 1);
         *bytes = (double)ndom * 2304 * (8 + 8 + 4);
     } else if (!strcmp(name, "mas_domain64") || !strcmp(name, "mas_domain32")) {
         const bool f32 = name[10] == '3';
