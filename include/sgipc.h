@@ -158,7 +158,8 @@ const char* sgipc_last_error(const SgipcCtx* ctx);
  * (dynamic part), plus the right-hand side b = fb + shape_grads with Dirichlet rows
  * zeroed (FEMLinearSubsystem::assemble, fem_linear_subsystem.cu:56-84).  Stream-ordered.
  * It also starts the MAS hierarchy for con's pairs on the context's own stream, beside the
- * assembly (the hierarchy needs the contact graph, not the matrix); the next
+ * assembly (the hierarchy needs the contact graph, not the matrix), and scatters the static
+ * blocks into its domains there once they are assembled; the next
  * sgipc_mas_build / sgipc_solve given the same pair array and count uses it, so the pair
  * array must stay unchanged until that call. */
 SgipcStatus sgipc_assemble(SgipcCtx* ctx, const SgipcFemData* fem, const SgipcContacts* con,
