@@ -239,7 +239,7 @@ def run_ours(args):
     step("mixed")
     torch.cuda.synchronize()
     per_step = {"snk": 1, "gather_blocks": 1, "barrier": 1, "friction": 1, "mas_scatter": 1, "mas_invert": 1,
-                "pcg32": max(1, st_mixed.refinements)}
+                "pcg32": max(1, st_mixed.refinements), "energy": 0}
     kern = {}
     for name, cnt in per_step.items():
         try:
@@ -276,6 +276,17 @@ def run_ours(args):
            "kernels": {k: {kk: (round(vv, 6) if isinstance(vv, float) else vv) for kk, vv in v.items()}
                        for k, v in kern.items()},
            "clocks": clk}
+    # line-search energy (not part of the Newton system): kernels alone, and the C-ABI call
+    # with its readback and synchronisation, wall clock
+    if "ms" in kern.get("energy", {}):
+        ek = kern["energy"]
+        tw = []
+        for _ in range(25):
+            t0 = time.perf_counter()
+            g.computeEnergy()
+            tw.append(time.perf_counter() - t0)
+        out["line_search_energy"] = {"kernels_us": 1e3 * ek["ms"], "call_us": 1e6 * sorted(tw)[len(tw) // 2],
+                                     "achieved_GBs": ek["bytes"] / (ek["ms"] * 1e-3) / 1e9}
     if rank == 0 and world == 1 and not args.no_cpu:
         import oracle
 

@@ -186,6 +186,15 @@ SgipcStatus sgipc_export_bcoo(SgipcCtx* ctx, int32_t cap, int32_t* rows, int32_t
                               double* vals, int32_t* count);
 /* Right-hand side b [dev double[3n]] of the last assembly. */
 SgipcStatus sgipc_get_rhs(SgipcCtx* ctx, double* b, void* stream);
+/* GIPC::computeEnergy (GIPC.cu:10520-10580), the line-search objective, for the FEM part at
+ * fem->vertexes: kinetic + dt^2 (tets + triangles + hinges) + soft constraints + barrier +
+ * kappa ground + frictionRate friction + gd_frictionRate ground friction, with the per-term
+ * reductions of Energy_Add_Reduction_Algorithm (GIPC.cu:10347-10518).  Each term is summed
+ * in a fixed order, so the result is the same on every run.  *energy receives the total;
+ * terms (optional, host, double[9]) the nine parts in that order.  Needs no assembly first;
+ * synchronises the stream. */
+SgipcStatus sgipc_compute_energy(SgipcCtx* ctx, const SgipcFemData* fem, const SgipcContacts* con,
+                                 const SgipcParams* prm, double* energy, double* terms, void* stream);
 
 /* ---- operators --------------------------------------------------------------------- */
 

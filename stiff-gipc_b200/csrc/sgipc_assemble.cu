@@ -869,11 +869,262 @@ __global__ void k_lower_rank(const int* __restrict__ nuc, const int* __restrict_
     cl_col[k0 + rank] = row;
 }
 
+
+// ------------------------------------------------------------------------------------------
+// line-search energy (GIPC::computeEnergy, GIPC.cu:10520-10580; per-term reductions
+// Energy_Add_Reduction_Algorithm, GIPC.cu:10347-10518).  Each kernel writes one partial sum
+// per CTA; every sum runs in a fixed order, so the energy is the same bit for bit on every
+// run.  The scalings of computeEnergy (dt^2 on the elastic terms, kappa, the friction rates)
+// are applied per element, as in the gradient kernels above.
+// ------------------------------------------------------------------------------------------
+// fixed-order CTA sum of one value per thread into part[blockIdx.x]; every thread calls it
+__device__ __forceinline__ void cta_energy(double e, double* __restrict__ part) {
+    __shared__ double sw[SGIPC_BLOCK / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sw[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+// kinetic 1/2 m |x - x_tilde|^2 (_getKineticEnergy_Reduction_3D)
+__global__ void k_en_kinetic(int nv, const double* __restrict__ x, const double* __restrict__ xt,
+                             const double* __restrict__ m, double* __restrict__ part) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (i < nv) {
+        const d3 d = ld3(x, i) - ld3(xt, i);
+        e = 0.5 * m[i] * sq(d);
+    }
+    cta_energy(e, part);
+}
+
+// stable Neo-Hookean: dt^2 vol 1/2 (mu (|F|^2 - 3) + lam (J - 1 - mu/lam)^2)
+// (_getFEMEnergy_Reduction_3D; femEnergy.cu:1042-1050)
+__global__ void k_en_snk(int nt, const uint32_t* __restrict__ tets, const double* __restrict__ x,
+                         const double* __restrict__ dminv, const double* __restrict__ vol,
+                         const double* __restrict__ lr, const double* __restrict__ vr, double dt2,
+                         double* __restrict__ part) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (t < nt) {
+        const uint4 tv = reinterpret_cast<const uint4*>(tets)[t];
+        const d3 X0 = ld3(x, tv.x), e1 = ld3(x, tv.y) - X0, e2 = ld3(x, tv.z) - X0, e3 = ld3(x, tv.w) - X0;
+        const double* Di = dminv + 9 * (size_t)t;
+        double F[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) F[i][j] = comp(e1, i) * Di[j] + comp(e2, i) * Di[3 + j] + comp(e3, i) * Di[6 + j];
+        double I2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) I2 += F[i][j] * F[i][j];
+        const double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                         F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                         F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+        const double mu = lr[t], lam = vr[t], Jm = J - 1.0 - mu / lam;
+        e = 0.5 * (mu * (I2 - 3.0) + lam * Jm * Jm) * vol[t] * dt2;
+    }
+    cta_energy(e, part);
+}
+
+// cloth membrane: dt^2 area (kst sum_j S(|f_j|) + ksh (f_0 . f_1)^2), S(t) = (t-1)^2 (+ srate
+// (t-1)^3 when stretched) (_getFEMEnergy_Reduction_3D_triangle, femEnergy.cu:351-403)
+__global__ void k_en_tri(int nf, const uint32_t* __restrict__ tris, const double* __restrict__ x,
+                         const double* __restrict__ dminv, const double* __restrict__ area, double kst, double ksh,
+                         double srate, double dt2, double* __restrict__ part) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (f < nf) {
+        const d3 x0 = ld3(x, tris[3 * f]), e1 = ld3(x, tris[3 * f + 1]) - x0, e2 = ld3(x, tris[3 * f + 2]) - x0;
+        const double* Di = dminv + 4 * (size_t)f;
+        const d3 col[2] = {Di[0] * e1 + Di[2] * e2, Di[1] * e1 + Di[3] * e2};
+        double E = 0.0;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const double t = sqrt(sq(col[j])), u = t - 1.0;
+            E += kst * (u * u + (t > 1.0 ? srate * u * u * u : 0.0));
+        }
+        const double I6 = dot(col[0], col[1]);
+        E += ksh * I6 * I6;
+        e = E * area[f] * dt2;
+    }
+    cta_energy(e, part);
+}
+
+// quadratic bending: 1/2 c sum_ab Q_ab x_a . x_b, c = |rest e| bendStiff dt^2; boundary
+// edges (a missing wing) carry none (femEnergy.cu:2623-2753)
+__global__ void k_en_hinge(int nh, const uint32_t* __restrict__ edges, const int32_t* __restrict__ adj,
+                           const double* __restrict__ x, const double* __restrict__ rest,
+                           const double* __restrict__ Qcm, double kb_dt2, double* __restrict__ part) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (h < nh && adj[2 * h] >= 0 && adj[2 * h + 1] >= 0) {
+        const int v[4] = {(int)edges[2 * h], (int)edges[2 * h + 1], adj[2 * h], adj[2 * h + 1]};
+        const double c = sqrt(sq(ld3(rest, v[0]) - ld3(rest, v[1]))) * kb_dt2;
+        d3 xv[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) xv[a] = ld3(x, v[a]);
+        double E = 0.0;
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            d3 g = mk(0, 0, 0);
+#pragma unroll
+            for (int b = 0; b < 4; b++) g = g + Qcm[16 * (size_t)h + 4 * b + a] * xv[b];
+            E += 0.5 * c * dot(xv[a], g);
+        }
+        e = E;
+    }
+    cta_energy(e, part);
+}
+
+// soft constraints 1/2 k |x - target|^2, k = motionRate softRate^2 (GIPC.cu:6363-6407)
+__global__ void k_en_soft(int ns, const uint32_t* __restrict__ idx, const double* __restrict__ x,
+                          const double* __restrict__ target, double k, double* __restrict__ part) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (p < ns) e = 0.5 * k * sq(ld3(x, idx[p]) - ld3(target, p));
+    cta_energy(e, part);
+}
+
+// barrier pairs: kappa dhat^2 (I-1)^2 ln^2 I, I = d^2/dhat; mollified EE / PE / PP pairs
+// times e(c^2) (_getBarrierEnergy_Reduction_3D, GIPC.cu:701-958)
+__global__ void k_en_barrier(int np, int nv, const int4* __restrict__ pairs, const double* __restrict__ x,
+                             const double* __restrict__ rest, double dhat, double kappa, double* __restrict__ part) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (p < np) {
+        int v[4], nvp;
+        const int kind = decode_pair(pairs[p], v, nvp);
+        bool ok = true;
+        for (int a = 0; a < nvp; a++) ok = ok && v[a] >= 0 && v[a] < nv;
+        if (ok) {
+            d3 X[4], gd2[4];
+#pragma unroll
+            for (int a = 0; a < 4; a++) X[a] = a < nvp ? ld3(x, v[a]) : mk(0, 0, 0);
+            const double I = dist2_grad(kind, X, gd2) / dhat;
+            double B, dB, d2B;
+            if (kind <= 3) {
+                barrier_s(I, kappa * dhat * dhat, B, dB, d2B);
+                e = B;
+            } else {
+                int ea0, ea1, eb0, eb1;
+                if (kind == 4) { ea0 = 0; ea1 = 1; eb0 = 2; eb1 = 3; }
+                else if (kind == 6) { ea0 = 0; ea1 = 2; eb0 = 1; eb1 = 3; }
+                else { ea0 = 0; ea1 = 3; eb0 = 1; eb1 = 2; }
+                const double I1 = sq(cross(X[ea1] - X[ea0], X[eb1] - X[eb0]));
+                if (I1 != 0.0) {
+                    const double ex = 1e-3 * sq(ld3(rest, v[ea0]) - ld3(rest, v[ea1])) *
+                                      sq(ld3(rest, v[eb0]) - ld3(rest, v[eb1]));
+                    const double em = -I1 * I1 / (ex * ex) + 2.0 * I1 / ex;
+                    barrier_s(I, dhat * dhat, B, dB, d2B);
+                    e = kappa * em * B;
+                }
+            }
+        }
+    }
+    cta_energy(e, part);
+}
+
+// ground barrier -kappa (d^2 - dhat)^2 ln(d^2/dhat), d = y - offset (GIPC.cu:6463-6514)
+__global__ void k_en_ground(int ng, int nv, const uint32_t* __restrict__ gp, const double* __restrict__ x,
+                            double offset, double dhat, double kappa, double* __restrict__ part) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (p < ng && (int)gp[p] < nv) {
+        const double dist = x[3 * gp[p] + 1] - offset, d2 = dist * dist, t = d2 - dhat;
+        e = -kappa * t * t * log(d2 / dhat);
+    }
+    cta_energy(e, part);
+}
+
+// pair friction mu lambda f0(|u|): f0 = |u| beyond eps, else |u|^2 (eps - |u|/3) / eps^2 +
+// eps/3 (_getFrictionEnergy_Reduction_3D, GIPC.cu:1252-1356)
+__global__ void k_en_friction(int np, int nv, const int4* __restrict__ pairs, const double* __restrict__ x,
+                              const double* __restrict__ x0, const double* __restrict__ lam,
+                              const double* __restrict__ coord, const double* __restrict__ basis, double mu,
+                              double eps2, double* __restrict__ part) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (p < np) {
+        const int4 q = pairs[p];
+        int v[4] = {0, 0, 0, 0}, nvp = 0;
+        double cf[4] = {0, 0, 0, 0};
+        const double g1 = coord[2 * p], g2 = coord[2 * p + 1];
+        if (q.x >= 0) {
+            if (q.w >= 0) {
+                v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w; nvp = 4;
+                cf[0] = 1.0 - g1; cf[1] = g1; cf[2] = g2 - 1.0; cf[3] = -g2;
+            }
+        } else if (q.y >= 0) {
+            v[0] = -q.x - 1;
+            if (q.z < 0) { v[1] = q.y; nvp = 2; cf[0] = 1.0; cf[1] = -1.0; }
+            else if (q.w < 0) { v[1] = q.y; v[2] = q.z; nvp = 3; cf[0] = 1.0; cf[1] = g1 - 1.0; cf[2] = -g1; }
+            else { v[1] = q.y; v[2] = q.z; v[3] = q.w; nvp = 4; cf[0] = 1.0; cf[1] = -1.0 + g1 + g2; cf[2] = -g1; cf[3] = -g2; }
+        }
+        bool ok = nvp > 0;
+        for (int a = 0; a < nvp; a++) ok = ok && v[a] >= 0 && v[a] < nv;
+        if (ok) {
+            const double* Tb = basis + 6 * (size_t)p;
+            const d3 t0 = mk(Tb[0], Tb[2], Tb[4]), t1 = mk(Tb[1], Tb[3], Tb[5]);
+            d3 rel = mk(0, 0, 0);
+            for (int a = 0; a < nvp; a++) rel = rel + cf[a] * (ld3(x, v[a]) - ld3(x0, v[a]));
+            const double u0 = dot(t0, rel), u1 = dot(t1, rel);
+            const double un2 = u0 * u0 + u1 * u1, un = sqrt(un2), eps = sqrt(eps2);
+            const double f0 = un2 > eps2 ? un : un2 * (-un / 3.0 + eps) / (eps * eps) + eps / 3.0;
+            e = mu * lam[p] * f0;
+        }
+    }
+    cta_energy(e, part);
+}
+
+// ground friction mu lambda (|v| - eps/2) beyond eps, else mu lambda |v|^2 / (2 eps), v the
+// tangential (x, z) step (_getFrictionEnergy_gd_Reduction_3D, GIPC.cu:1357-1437)
+__global__ void k_en_fric_ground(int ng, int nv, const uint32_t* __restrict__ gp, const double* __restrict__ x,
+                                 const double* __restrict__ x0, const double* __restrict__ lam, double mu,
+                                 double eps2, double* __restrict__ part) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (p < ng && (int)gp[p] < nv) {
+        const int v = gp[p];
+        const double vx = x[3 * v] - x0[3 * v], vz = x[3 * v + 2] - x0[3 * v + 2];
+        const double m2 = vx * vx + vz * vz, s = mu * lam[p], eps = sqrt(eps2);
+        e = m2 > eps2 ? s * (sqrt(m2) - eps * 0.5) : s * m2 / eps * 0.5;
+    }
+    cta_energy(e, part);
+}
+
+// one warp: term t = sum of its CTA partials [off[t], off[t+1]) in a fixed order; terms[9]
+// = the terms summed in order
+struct EnergyOffsets {
+    int off[10];
+};
+__global__ void k_en_sum(const double* __restrict__ part, EnergyOffsets o, double* __restrict__ terms) {
+    double total = 0.0;
+    for (int t = 0; t < 9; t++) {
+        double s = 0.0;
+        for (int i = o.off[t] + (int)threadIdx.x; i < o.off[t + 1]; i += 32) s += part[i];
+#pragma unroll
+        for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
+        if (threadIdx.x == 0) terms[t] = s;
+        total += s;
+    }
+    if (threadIdx.x == 0) terms[9] = total;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------------
+static SgipcStatus energy_launch(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k, const SgipcParams* p,
+                                 cudaStream_t s, double* bytes);
 static SgipcStatus check_inputs(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k, const SgipcParams* p) {
     if (!c || !f || !p) return SGIPC_BAD_INPUT;
     if (!f->vertexes || !f->xTilta || !f->masses || !f->BoundaryType) return SGIPC_BAD_INPUT;
@@ -1127,6 +1378,7 @@ SgipcStatus assemble_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, do
     const SgipcParams* p = &c->last_prm;
     const SgipcContacts* k = c->last_has_con ? &c->last_con : nullptr;
     double* scratch = c->tmp64b;  // gradient sink that keeps fb untouched
+    if (!strcmp(name, "energy")) return energy_launch(c, f, k, p, s, bytes);
     if (!strcmp(name, "snk")) {
         if (c->nt <= 0) return SGIPC_BAD_INPUT;
         SG_COUNT(c, 1);
@@ -1164,3 +1416,95 @@ SgipcStatus assemble_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, do
     return SGIPC_OK;
 }
 }  // namespace sgipc
+
+// ------------------------------------------------------------------------------------------
+// line-search energy: host side
+// ------------------------------------------------------------------------------------------
+// Launch the energy kernels and the final sum into c->en_terms on s (no synchronisation).
+// Terms: 0 kinetic, 1 tets, 2 triangles, 3 hinges, 4 soft, 5 barrier, 6 ground, 7 friction,
+// 8 ground friction; 9 the total.  *bytes: algorithmic bytes of the launch sequence.
+static SgipcStatus energy_launch(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k, const SgipcParams* p,
+                                 cudaStream_t s, double* bytes) {
+    const double dt2 = p->dt * p->dt, eps2 = p->fDhat * dt2;
+    const int npair = k ? k->pair_num : 0, nground = k ? k->ground_num : 0;
+    const int nfric = k && p->frictionRate > 0.0 ? k->fric_num : 0;
+    const int nfg = k && p->gd_frictionRate > 0.0 ? k->fric_gd_num : 0;
+    const int cnt[9] = {c->nv, c->nt, c->nf, c->nh, c->nsoft, npair, nground, nfric, nfg};
+    EnergyOffsets o;
+    o.off[0] = 0;
+    for (int t = 0; t < 9; t++) o.off[t + 1] = o.off[t] + nblk(cnt[t]);
+    if (o.off[9] > c->en_cap) {
+        snprintf(c->err, sizeof(c->err), "energy: %d partial sums exceed the context's %d", o.off[9], c->en_cap);
+        return SGIPC_CAPACITY;
+    }
+    double* P = c->en_part;
+    const int B = SGIPC_BLOCK;
+    int nl = 1;
+    k_en_kinetic<<<nblk(c->nv), B, 0, s>>>(c->nv, f->vertexes, f->xTilta, f->masses, P + o.off[0]);
+    if (c->nt > 0) {
+        nl++;
+        k_en_snk<<<nblk(c->nt), B, 0, s>>>(c->nt, c->tets, f->vertexes, f->DmInverses, f->volum, f->lengthRate,
+                                          f->volumeRate, dt2, P + o.off[1]);
+    }
+    if (c->nf > 0) {
+        nl++;
+        k_en_tri<<<nblk(c->nf), B, 0, s>>>(c->nf, c->tris, f->vertexes, f->triDmInverses, f->area, p->stretchStiff,
+                                          p->shearStiff, p->strainRate, dt2, P + o.off[2]);
+    }
+    if (c->nh > 0) {
+        nl++;
+        k_en_hinge<<<nblk(c->nh), B, 0, s>>>(c->nh, c->hinges, c->hinge_adj, f->vertexes, f->rest_vertexes,
+                                            f->quad_bending_Q, p->bendStiff * dt2, P + o.off[3]);
+    }
+    if (c->nsoft > 0) {
+        nl++;
+        k_en_soft<<<nblk(c->nsoft), B, 0, s>>>(c->nsoft, c->soft_idx, f->vertexes, f->targetVert,
+                                              p->motionRate * p->softRate * p->softRate, P + o.off[4]);
+    }
+    if (npair > 0) {
+        nl++;
+        k_en_barrier<<<nblk(npair), B, 0, s>>>(npair, c->nv, (const int4*)k->pairs, f->vertexes, f->rest_vertexes,
+                                              p->dHat, p->kappa, P + o.off[5]);
+    }
+    if (nground > 0) {
+        nl++;
+        k_en_ground<<<nblk(nground), B, 0, s>>>(nground, c->nv, k->ground_pairs, f->vertexes, p->ground_offset,
+                                               p->dHat, p->kappa, P + o.off[6]);
+    }
+    if (nfric > 0) {
+        nl++;
+        k_en_friction<<<nblk(nfric), B, 0, s>>>(nfric, c->nv, (const int4*)k->fric_pairs, f->vertexes,
+                                               f->o_vertexes, k->fric_lambda, k->fric_coord, k->fric_basis,
+                                               p->frictionRate, eps2, P + o.off[7]);
+    }
+    if (nfg > 0) {
+        nl++;
+        k_en_fric_ground<<<nblk(nfg), B, 0, s>>>(nfg, c->nv, k->fric_gd_pairs, f->vertexes, f->o_vertexes,
+                                                  k->fric_gd_lambda, p->gd_frictionRate, eps2, P + o.off[8]);
+    }
+    k_en_sum<<<1, 32, 0, s>>>(P, o, c->en_terms);
+    SG_COUNT(c, nl + 1);
+    SG_LAUNCH_CHECK(c, "energy");
+    if (bytes)  // positions (and the per-element inputs) in, one partial per CTA out and back
+        *bytes = (double)c->nv * (24 + 24 + 8) + (double)c->nt * (16 + 4 * 24 + 72 + 8 + 16) +
+                 (double)c->nf * (12 + 3 * 24 + 32 + 8) + (double)c->nh * (16 + 4 * 24 + 2 * 24 + 128) +
+                 (double)c->nsoft * (4 + 24 + 24) + (double)npair * (16 + 4 * 24 + 4 * 24) + (double)nground * (4 + 8) +
+                 (double)nfric * (16 + 8 + 16 + 48 + 8 * 24) + (double)nfg * (4 + 8 + 48) + 2.0 * 8 * o.off[9];
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_compute_energy(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k,
+                                            const SgipcParams* p, double* energy, double* terms, void* stream) {
+    SgipcStatus st = check_inputs(c, f, k, p);
+    if (st != SGIPC_OK) return st;
+    if (!energy) return SGIPC_BAD_INPUT;
+    cudaStream_t s = (cudaStream_t)stream;
+    SG_CHECK(c, cudaSetDevice(c->device));
+    if ((st = energy_launch(c, f, k, p, s, nullptr)) != SGIPC_OK) return st;
+    SG_CHECK(c, cudaMemcpyAsync(c->h_en, c->en_terms, sizeof(double) * 10, cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    *energy = c->h_en[9];
+    if (terms)
+        for (int t = 0; t < 9; t++) terms[t] = c->h_en[t];
+    return SGIPC_OK;
+}

@@ -192,6 +192,10 @@ struct SgipcCtx {
     int key_bits;
     int assembled;
     int* dflag;                   // device: input errors found by kernels (bit 0: pair index)
+    double* en_part;              // [en_cap] per-CTA partial sums of the line-search energy terms
+    int en_cap;
+    double* en_terms;             // [16] device: the nine terms and their total
+    double* h_en;                 // [16] pinned landing area of en_terms
     // last inputs (for re-timing kernels against the current state)
     SgipcFemData last_fem;
     SgipcContacts last_con;

@@ -71,6 +71,8 @@ SIGNATURES = {
     "sgipc_fem_grad_hess": ([_vp, C.POINTER(SgipcFemData), C.POINTER(SgipcParams), _vp, _vp], _i32),
     "sgipc_export_bcoo": ([_vp, _i32, _vp, _vp, _vp, C.POINTER(_i32)], _i32),
     "sgipc_get_rhs": ([_vp, _vp, _vp], _i32),
+    "sgipc_compute_energy": ([_vp, C.POINTER(SgipcFemData), C.POINTER(SgipcContacts), C.POINTER(SgipcParams),
+                              C.POINTER(C.c_double), _vp, _vp], _i32),
     "sgipc_spmv": ([_vp, _vp, _vp, _vp], _i32),
     "sgipc_mas_build": ([_vp, C.POINTER(SgipcContacts), _i32, _vp], _i32),
     "sgipc_mas_apply": ([_vp, _vp, _vp, _vp], _i32),

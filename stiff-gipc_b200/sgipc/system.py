@@ -218,6 +218,18 @@ class GIPC:
         f, p = tet.fem_struct(), params_struct(self.params)
         N.check(N.lib().sgipc_fem_grad_hess(self.ctx, C.byref(f), C.byref(p), _p(grad), _stream()), self.ctx)
 
+    def computeEnergy(self, tet: Optional[DeviceTetraData] = None, terms: bool = False):
+        """GIPC::computeEnergy (GIPC.cu:10520): the line-search objective at tet's vertexes.
+        With terms=True also the nine parts (kinetic, tets, triangles, hinges, soft, barrier,
+        ground, friction, ground friction) as a numpy array."""
+        tet = tet or self.tet
+        f, k, p = tet.fem_struct(), tet.contact_struct(), params_struct(self.params)
+        e = C.c_double(0.0)
+        parts = np.zeros(9)
+        N.check(N.lib().sgipc_compute_energy(self.ctx, C.byref(f), C.byref(k), C.byref(p), C.byref(e),
+                                             parts.ctypes.data_as(C.c_void_p), _stream()), self.ctx)
+        return (e.value, parts) if terms else e.value
+
     def rhs(self) -> torch.Tensor:
         b = torch.empty(3 * self.n, dtype=torch.float64, device=_dev())
         N.check(N.lib().sgipc_get_rhs(self.ctx, _p(b), _stream()), self.ctx)
