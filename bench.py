@@ -20,6 +20,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 for _p in (ROOT, os.path.join(ROOT, "stiff-gipc_b200")):
     if _p not in sys.path:
@@ -287,6 +289,24 @@ def run_ours(args):
             tw.append(time.perf_counter() - t0)
         out["line_search_energy"] = {"kernels_us": 1e3 * ek["ms"], "call_us": 1e6 * sorted(tw)[len(tw) // 2],
                                      "achieved_GBs": ek["bytes"] / (ek["ms"] * 1e-3) / 1e9}
+    # line-search step bound (GIPC::self_largestFeasibleStepSize) along the solve's direction,
+    # over the point-triangle and edge-edge pairs of the workload's contact list as candidates
+    enc = np.asarray(sc.pairs, np.int32).reshape(-1, 4)
+    pt = (enc[:, 0] < 0) & (enc[:, 2] >= 0) & (enc[:, 3] >= 0)
+    ee = enc[:, 0] >= 0
+    cand = enc[pt | ee].copy()
+    mol = cand[:, 0] >= 0
+    cand[mol, 3] = np.where(cand[mol, 3] < 0, -cand[mol, 3] - 1, cand[mol, 3])
+    if len(cand):
+        step("mixed")
+        cand_d = torch.tensor(cand, device="cuda")
+        tw = []
+        for _ in range(25):
+            t0 = time.perf_counter()
+            alpha = g.self_largestFeasibleStepSize(0.8, g.moveDir, cand_d)
+            tw.append(time.perf_counter() - t0)
+        out["line_search_ccd"] = {"call_us": 1e6 * sorted(tw)[len(tw) // 2], "candidates": int(len(cand)),
+                                  "alpha": alpha}
     if rank == 0 and world == 1 and not args.no_cpu:
         import oracle
 

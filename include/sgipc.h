@@ -195,6 +195,23 @@ SgipcStatus sgipc_get_rhs(SgipcCtx* ctx, double* b, void* stream);
  * synchronises the stream. */
 SgipcStatus sgipc_compute_energy(SgipcCtx* ctx, const SgipcFemData* fem, const SgipcContacts* con,
                                  const SgipcParams* prm, double* energy, double* terms, void* stream);
+/* GIPC::self_largestFeasibleStepSize (GIPC.cu:8880-8914; per candidate
+ * _reduct_min_selfTimeStep_to_double GIPC.cu:7052 with the additive CCD of ACCD.cu:373-535):
+ * the largest step alpha <= 1 along -move_dir (the reference's moveDir) that keeps every
+ * candidate pair apart by the fraction 1 - slackness of its current distance.  pairs:
+ * int32[4] per candidate, x < 0 for point -x-1 against triangle (y, z, w), else edge (x, y)
+ * against edge (z, w).  x, move_dir: device double3 per vertex; toi (optional, device,
+ * double[npairs]) receives each candidate's time of impact.  Returns SGIPC_BAD_INPUT for a
+ * vertex index outside the context's vertices.  Synchronises the stream. */
+SgipcStatus sgipc_self_step_size(SgipcCtx* ctx, const double* x, const double* move_dir, const int32_t* pairs,
+                                 int32_t npairs, double slackness, double* alpha, double* toi, void* stream);
+/* GIPC::ground_largestFeasibleStepSize (GIPC.cu:8986-9025; per vertex
+ * _reduct_min_groundTimeStep_to_double GIPC.cu:6902): the step bound of the vertices verts
+ * against the plane y = ground_offset (normal +y), alpha = 1 / max(1, move_dir_y / ((y -
+ * offset) slackness)) over the vertices with move_dir_y > 0.  Synchronises the stream. */
+SgipcStatus sgipc_ground_step_size(SgipcCtx* ctx, const double* x, const double* move_dir, const uint32_t* verts,
+                                   int32_t nverts, double ground_offset, double slackness, double* alpha,
+                                   void* stream);
 
 /* ---- operators --------------------------------------------------------------------- */
 

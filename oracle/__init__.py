@@ -68,6 +68,10 @@ def lib():
         L.or_pcg.argtypes = [C.c_int, _i, _i, _d, C.c_int, C.c_void_p, C.c_int, _d, _d, C.c_double,
                              C.c_int, _d, _d]
         L.or_pcg.restype = C.c_int
+        L.or_self_step.argtypes = [_d, _d, _i, C.c_int, C.c_double, _d]
+        L.or_self_step.restype = C.c_double
+        L.or_ground_step.argtypes = [_d, _d, _u, C.c_int, C.c_double, C.c_double]
+        L.or_ground_step.restype = C.c_double
         L.or_num_threads.restype = C.c_int
     return _LIB
 
@@ -250,6 +254,23 @@ def energy(sc, x=None):
     b = np.zeros(3 * sc.nv)
     lib().or_assemble(C.byref(s), _p(b), 0, None, None, None, _p(e))
     return e[0]
+
+
+def self_step(x, move_dir, pairs, slackness):
+    """(alpha, toi): GIPC::self_largestFeasibleStepSize (GIPC.cu:8880) over int32[4]
+    candidates (x < 0: point -x-1 vs triangle, else edge vs edge) with the additive CCD of
+    ACCD.cu:373-535, along -move_dir."""
+    x, move_dir, pairs = _f64(x), _f64(move_dir), _i32(np.asarray(pairs).reshape(-1, 4))
+    toi = np.zeros(len(pairs))
+    a = lib().or_self_step(_p(x), _p(move_dir), _p(pairs, _i), len(pairs), slackness, _p(toi))
+    return a, toi
+
+
+def ground_step(x, move_dir, verts, offset, slackness):
+    """GIPC::ground_largestFeasibleStepSize (GIPC.cu:8986), plane y = offset."""
+    x, move_dir = _f64(x), _f64(move_dir)
+    verts = np.ascontiguousarray(verts, dtype=np.uint32)
+    return lib().or_ground_step(_p(x), _p(move_dir), verts.ctypes.data_as(_u), len(verts), offset, slackness)
 
 
 def spmv(rows, cols, vals, n, x):

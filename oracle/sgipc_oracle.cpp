@@ -1334,6 +1334,149 @@ int or_pcg(int nb, const int32_t* rows, const int32_t* cols, const double* vals,
     return k;
 }
 
+
+// ---------------------------------------------------------------------------------------
+// line-search step bounds (test infrastructure): additive CCD of point-triangle and
+// edge-edge candidates (StiffGIPC/ACCD.cu:15-535, Li, Kaufman and Jiang 2021), the
+// reference's per-candidate reduction (GIPC.cu:7052, self_largestFeasibleStepSize
+// :8880-8914) and the ground plane bound (GIPC.cu:6902, ground_largestFeasibleStepSize
+// :8986-9025).  Scalar FP64 loops over plain arrays.
+// ---------------------------------------------------------------------------------------
+namespace ccd {
+struct V3 { double v[3]; };
+static V3 sub(const V3& a, const V3& b) { return {{a.v[0] - b.v[0], a.v[1] - b.v[1], a.v[2] - b.v[2]}}; }
+static V3 add(const V3& a, const V3& b) { return {{a.v[0] + b.v[0], a.v[1] + b.v[1], a.v[2] + b.v[2]}}; }
+static V3 scl(double s, const V3& a) { return {{s * a.v[0], s * a.v[1], s * a.v[2]}}; }
+static double dt(const V3& a, const V3& b) { return a.v[0] * b.v[0] + a.v[1] * b.v[1] + a.v[2] * b.v[2]; }
+static V3 cr(const V3& a, const V3& b) {
+    return {{a.v[1] * b.v[2] - a.v[2] * b.v[1], a.v[2] * b.v[0] - a.v[0] * b.v[2], a.v[0] * b.v[1] - a.v[1] * b.v[0]}};
+}
+static double n2(const V3& a) { return dt(a, a); }
+// 3x3 determinant of the columns a, b, c
+static double det3(const V3& a, const V3& b, const V3& c) {
+    return a.v[0] * (b.v[1] * c.v[2] - b.v[2] * c.v[1]) - b.v[0] * (a.v[1] * c.v[2] - a.v[2] * c.v[1]) +
+           c.v[0] * (a.v[1] * b.v[2] - a.v[2] * b.v[1]);
+}
+static double d_pp(const V3& a, const V3& b) { return n2(sub(a, b)); }
+static double d_pe(const V3& p, const V3& e0, const V3& e1) { return n2(cr(sub(e0, p), sub(e1, p))) / n2(sub(e1, e0)); }
+static double d_pplane(const V3& p, const V3& t0, const V3& t1, const V3& t2) {
+    V3 n = cr(sub(t1, t0), sub(t2, t0));
+    double s = dt(sub(p, t0), n);
+    return s * s / n2(n);
+}
+static double d_ll(const V3& a0, const V3& a1, const V3& b0, const V3& b1) {
+    V3 n = cr(sub(a1, a0), sub(b1, b0));
+    double s = dt(sub(b0, a0), n);
+    return s * s / n2(n);
+}
+static double d_pt(const V3& p, const V3& t0, const V3& t1, const V3& t2) {
+    V3 n = cr(sub(t1, t0), sub(t2, t0));
+    const V3* A[3] = {&t0, &t1, &t2};
+    const V3* B[3] = {&t1, &t2, &t0};
+    double s[3];
+    for (int i = 0; i < 3; i++) {
+        V3 e = sub(*B[i], *A[i]), f = cr(e, n), w = sub(p, *A[i]);
+        double D = det3(e, f, n);
+        s[i] = det3(w, f, n) / D;
+        double h = det3(e, w, n) / D;
+        if (s[i] > 0.0 && s[i] < 1.0 && h >= 0.0) return d_pe(p, *A[i], *B[i]);
+    }
+    if (s[0] <= 0.0 && s[2] >= 1.0) return d_pp(p, t0);
+    if (s[1] <= 0.0 && s[0] >= 1.0) return d_pp(p, t1);
+    if (s[2] <= 0.0 && s[1] >= 1.0) return d_pp(p, t2);
+    return d_pplane(p, t0, t1, t2);
+}
+static double d_ee(const V3& a0, const V3& a1, const V3& b0, const V3& b1) {
+    V3 u = sub(a1, a0), v = sub(b1, b0), w = sub(a0, b0);
+    double a = n2(u), b = dt(u, v), c = n2(v), d = dt(u, w), e = dt(v, w);
+    double D = a * c - b * b, sN = b * e - c * d, tN, tD = D;
+    int kind = 8;
+    if (sN <= 0.0) { tN = e; tD = c; kind = 2; }
+    else if (sN >= D) { tN = e + b; tD = c; kind = 5; }
+    else {
+        tN = a * e - b * d;
+        V3 uv = cr(u, v);
+        if (tN > 0.0 && tN < tD && (dt(w, uv) == 0.0 || n2(uv) < 1.0e-20 * a * c)) {
+            if (sN < D / 2) { tN = e; tD = c; kind = 2; }
+            else { tN = e + b; tD = c; kind = 5; }
+        }
+    }
+    if (tN <= 0.0) kind = (-d <= 0.0) ? 0 : ((-d >= a) ? 3 : 6);
+    else if (tN >= tD) kind = (b - d <= 0.0) ? 1 : ((b - d >= a) ? 4 : 7);
+    switch (kind) {
+        case 0: return d_pp(a0, b0);
+        case 1: return d_pp(a0, b1);
+        case 2: return d_pe(a0, b0, b1);
+        case 3: return d_pp(a1, b0);
+        case 4: return d_pp(a1, b1);
+        case 5: return d_pe(a1, b0, b1);
+        case 6: return d_pe(b0, a0, a1);
+        case 7: return d_pe(b1, a0, a1);
+        default: return d_ll(a0, a1, b0, b1);
+    }
+}
+// additive CCD: X[4] positions, M[4] displacements, eta the separation ratio kept
+static double accd(bool ee, V3 X[4], V3 M[4], double eta) {
+    V3 mov = ee ? scl(-0.25, add(add(M[0], M[1]), add(M[2], M[3]))) : scl(-0.25, add(add(M[1], M[2]), add(M[3], M[0])));
+    for (int a = 0; a < 4; a++) M[a] = add(M[a], mov);
+    double L = ee ? std::sqrt(std::max(n2(M[0]), n2(M[1]))) + std::sqrt(std::max(n2(M[2]), n2(M[3])))
+                  : std::sqrt(n2(M[0])) + std::sqrt(std::max(n2(M[1]), std::max(n2(M[2]), n2(M[3]))));
+    if (L == 0.0) return 1.0;
+    auto dist2 = [&]() {
+        double d2 = ee ? d_ee(X[0], X[1], X[2], X[3]) : d_pt(X[0], X[1], X[2], X[3]);
+        if (ee && d2 <= 0.0)
+            d2 = std::min(std::min(d_pp(X[0], X[2]), d_pp(X[0], X[3])), std::min(d_pp(X[1], X[2]), d_pp(X[1], X[3])));
+        return d2;
+    };
+    double d2 = dist2(), d = std::sqrt(d2);
+    const double gap = eta * d2 / d;
+    double toc = 0.0;
+    for (int it = 0; it < 50000; it++) {
+        double step = (1.0 - eta) * d2 / (d * L);
+        for (int a = 0; a < 4; a++) X[a] = add(X[a], scl(step, M[a]));
+        d2 = dist2();
+        d = std::sqrt(d2);
+        if (toc != 0.0 && d2 / d < gap) return toc;
+        toc += step;
+        if (toc > 1.0) return 1.0;
+    }
+    return toc;
+}
+}  // namespace ccd
+
+// step along -dir keeping every candidate (int32[4]: x < 0 point -x-1 vs triangle y z w,
+// else edge x y vs edge z w) apart; toi (optional) per candidate
+double or_self_step(const double* x, const double* dir, const int32_t* pairs, int n, double slackness, double* toi) {
+    double vmax = 1.0;
+    for (int i = 0; i < n; i++) {
+        int v[4] = {pairs[4 * i], pairs[4 * i + 1], pairs[4 * i + 2], pairs[4 * i + 3]};
+        bool ee = v[0] >= 0;
+        if (!ee) v[0] = -v[0] - 1;
+        ccd::V3 X[4], M[4];
+        for (int a = 0; a < 4; a++)
+            for (int k = 0; k < 3; k++) {
+                X[a].v[k] = x[3 * v[a] + k];
+                M[a].v[k] = -dir[3 * v[a] + k];
+            }
+        double t = ccd::accd(ee, X, M, 1.0 - slackness);
+        if (toi) toi[i] = t;
+        vmax = std::max(vmax, 1.0 / t);
+    }
+    return 1.0 / vmax;
+}
+
+// step bound of vertices verts against the plane y = offset, normal +y
+double or_ground_step(const double* x, const double* dir, const uint32_t* verts, int n, double offset,
+                      double slackness) {
+    double vmax = 1.0;
+    for (int i = 0; i < n; i++) {
+        uint32_t v = verts[i];
+        double coef = dir[3 * v + 1];
+        if (coef > 0.0) vmax = std::max(vmax, coef / ((x[3 * v + 1] - offset) * slackness));
+    }
+    return 1.0 / vmax;
+}
+
 int or_num_threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();

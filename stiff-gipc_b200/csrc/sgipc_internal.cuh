@@ -195,7 +195,10 @@ struct SgipcCtx {
     double* en_part;              // [en_cap] per-CTA partial sums of the line-search energy terms
     int en_cap;
     double* en_terms;             // [16] device: the nine terms and their total
-    double* h_en;                 // [16] pinned landing area of en_terms
+    double* h_en;                 // [16] pinned landing area of en_terms ([12], [13]: step sizes)
+    double* ccd_part;             // [592] per-CTA maxima of the step-size kernels
+    double* ccd_out;              // [1] the step
+    int* ccd_bad;                 // [1] a candidate with an out-of-range vertex
     // last inputs (for re-timing kernels against the current state)
     SgipcFemData last_fem;
     SgipcContacts last_con;

@@ -230,6 +230,31 @@ class GIPC:
                                              parts.ctypes.data_as(C.c_void_p), _stream()), self.ctx)
         return (e.value, parts) if terms else e.value
 
+    def self_largestFeasibleStepSize(self, slackness: float, move_dir: torch.Tensor, pairs: torch.Tensor,
+                                     x: Optional[torch.Tensor] = None, toi: Optional[torch.Tensor] = None):
+        """GIPC::self_largestFeasibleStepSize (GIPC.cu:8880): the step along -move_dir that keeps
+        every CCD candidate (int32 [n, 4] on the device: x < 0 point -x-1 vs triangle, else edge
+        vs edge) apart; toi (optional, float64 [n]) receives each candidate's time of impact."""
+        x = self.tet.vertexes if x is None else x
+        pairs = pairs.contiguous()
+        a = C.c_double(0.0)
+        N.check(N.lib().sgipc_self_step_size(self.ctx, _p(x), _p(move_dir), _p(pairs), pairs.shape[0], slackness,
+                                             C.byref(a), _p(toi) if toi is not None else None, _stream()),
+                self.ctx)
+        return a.value
+
+    def ground_largestFeasibleStepSize(self, slackness: float, move_dir: torch.Tensor, verts: torch.Tensor,
+                                       x: Optional[torch.Tensor] = None):
+        """GIPC::ground_largestFeasibleStepSize (GIPC.cu:8986) for the vertices verts (uint32 /
+        int32 on the device) against the plane y = ground_offset."""
+        x = self.tet.vertexes if x is None else x
+        verts = verts.contiguous()
+        a = C.c_double(0.0)
+        N.check(N.lib().sgipc_ground_step_size(self.ctx, _p(x), _p(move_dir), _p(verts), verts.shape[0],
+                                               self.params.get("ground_offset", 0.0), slackness, C.byref(a),
+                                               _stream()), self.ctx)
+        return a.value
+
     def rhs(self) -> torch.Tensor:
         b = torch.empty(3 * self.n, dtype=torch.float64, device=_dev())
         N.check(N.lib().sgipc_get_rhs(self.ctx, _p(b), _stream()), self.ctx)
