@@ -892,24 +892,23 @@ __device__ __forceinline__ void cta_energy(double e, double* __restrict__ part) 
 }
 
 // kinetic 1/2 m |x - x_tilde|^2 (_getKineticEnergy_Reduction_3D)
-__global__ void k_en_kinetic(int nv, const double* __restrict__ x, const double* __restrict__ xt,
-                             const double* __restrict__ m, double* __restrict__ part) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double en_kinetic(int gi, int nv, const double* __restrict__ x, const double* __restrict__ xt,
+                             const double* __restrict__ m) {
+    const int i = gi;
     double e = 0.0;
     if (i < nv) {
         const d3 d = ld3(x, i) - ld3(xt, i);
         e = 0.5 * m[i] * sq(d);
     }
-    cta_energy(e, part);
+    return e;
 }
 
 // stable Neo-Hookean: dt^2 vol 1/2 (mu (|F|^2 - 3) + lam (J - 1 - mu/lam)^2)
 // (_getFEMEnergy_Reduction_3D; femEnergy.cu:1042-1050)
-__global__ void k_en_snk(int nt, const uint32_t* __restrict__ tets, const double* __restrict__ x,
+__device__ __forceinline__ double en_snk(int gi, int nt, const uint32_t* __restrict__ tets, const double* __restrict__ x,
                          const double* __restrict__ dminv, const double* __restrict__ vol,
-                         const double* __restrict__ lr, const double* __restrict__ vr, double dt2,
-                         double* __restrict__ part) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+                         const double* __restrict__ lr, const double* __restrict__ vr, double dt2) {
+    const int t = gi;
     double e = 0.0;
     if (t < nt) {
         const uint4 tv = reinterpret_cast<const uint4*>(tets)[t];
@@ -931,15 +930,15 @@ __global__ void k_en_snk(int nt, const uint32_t* __restrict__ tets, const double
         const double mu = lr[t], lam = vr[t], Jm = J - 1.0 - mu / lam;
         e = 0.5 * (mu * (I2 - 3.0) + lam * Jm * Jm) * vol[t] * dt2;
     }
-    cta_energy(e, part);
+    return e;
 }
 
 // cloth membrane: dt^2 area (kst sum_j S(|f_j|) + ksh (f_0 . f_1)^2), S(t) = (t-1)^2 (+ srate
 // (t-1)^3 when stretched) (_getFEMEnergy_Reduction_3D_triangle, femEnergy.cu:351-403)
-__global__ void k_en_tri(int nf, const uint32_t* __restrict__ tris, const double* __restrict__ x,
+__device__ __forceinline__ double en_tri(int gi, int nf, const uint32_t* __restrict__ tris, const double* __restrict__ x,
                          const double* __restrict__ dminv, const double* __restrict__ area, double kst, double ksh,
-                         double srate, double dt2, double* __restrict__ part) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+                         double srate, double dt2) {
+    const int f = gi;
     double e = 0.0;
     if (f < nf) {
         const d3 x0 = ld3(x, tris[3 * f]), e1 = ld3(x, tris[3 * f + 1]) - x0, e2 = ld3(x, tris[3 * f + 2]) - x0;
@@ -955,15 +954,15 @@ __global__ void k_en_tri(int nf, const uint32_t* __restrict__ tris, const double
         E += ksh * I6 * I6;
         e = E * area[f] * dt2;
     }
-    cta_energy(e, part);
+    return e;
 }
 
 // quadratic bending: 1/2 c sum_ab Q_ab x_a . x_b, c = |rest e| bendStiff dt^2; boundary
 // edges (a missing wing) carry none (femEnergy.cu:2623-2753)
-__global__ void k_en_hinge(int nh, const uint32_t* __restrict__ edges, const int32_t* __restrict__ adj,
+__device__ __forceinline__ double en_hinge(int gi, int nh, const uint32_t* __restrict__ edges, const int32_t* __restrict__ adj,
                            const double* __restrict__ x, const double* __restrict__ rest,
-                           const double* __restrict__ Qcm, double kb_dt2, double* __restrict__ part) {
-    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+                           const double* __restrict__ Qcm, double kb_dt2) {
+    const int h = gi;
     double e = 0.0;
     if (h < nh && adj[2 * h] >= 0 && adj[2 * h + 1] >= 0) {
         const int v[4] = {(int)edges[2 * h], (int)edges[2 * h + 1], adj[2 * h], adj[2 * h + 1]};
@@ -981,23 +980,23 @@ __global__ void k_en_hinge(int nh, const uint32_t* __restrict__ edges, const int
         }
         e = E;
     }
-    cta_energy(e, part);
+    return e;
 }
 
 // soft constraints 1/2 k |x - target|^2, k = motionRate softRate^2 (GIPC.cu:6363-6407)
-__global__ void k_en_soft(int ns, const uint32_t* __restrict__ idx, const double* __restrict__ x,
-                          const double* __restrict__ target, double k, double* __restrict__ part) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double en_soft(int gi, int ns, const uint32_t* __restrict__ idx, const double* __restrict__ x,
+                          const double* __restrict__ target, double k) {
+    const int p = gi;
     double e = 0.0;
     if (p < ns) e = 0.5 * k * sq(ld3(x, idx[p]) - ld3(target, p));
-    cta_energy(e, part);
+    return e;
 }
 
 // barrier pairs: kappa dhat^2 (I-1)^2 ln^2 I, I = d^2/dhat; mollified EE / PE / PP pairs
 // times e(c^2) (_getBarrierEnergy_Reduction_3D, GIPC.cu:701-958)
-__global__ void k_en_barrier(int np, int nv, const int4* __restrict__ pairs, const double* __restrict__ x,
-                             const double* __restrict__ rest, double dhat, double kappa, double* __restrict__ part) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double en_barrier(int gi, int np, int nv, const int4* __restrict__ pairs, const double* __restrict__ x,
+                             const double* __restrict__ rest, double dhat, double kappa) {
+    const int p = gi;
     double e = 0.0;
     if (p < np) {
         int v[4], nvp;
@@ -1029,28 +1028,28 @@ __global__ void k_en_barrier(int np, int nv, const int4* __restrict__ pairs, con
             }
         }
     }
-    cta_energy(e, part);
+    return e;
 }
 
 // ground barrier -kappa (d^2 - dhat)^2 ln(d^2/dhat), d = y - offset (GIPC.cu:6463-6514)
-__global__ void k_en_ground(int ng, int nv, const uint32_t* __restrict__ gp, const double* __restrict__ x,
-                            double offset, double dhat, double kappa, double* __restrict__ part) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double en_ground(int gi, int ng, int nv, const uint32_t* __restrict__ gp, const double* __restrict__ x,
+                            double offset, double dhat, double kappa) {
+    const int p = gi;
     double e = 0.0;
     if (p < ng && (int)gp[p] < nv) {
         const double dist = x[3 * gp[p] + 1] - offset, d2 = dist * dist, t = d2 - dhat;
         e = -kappa * t * t * log(d2 / dhat);
     }
-    cta_energy(e, part);
+    return e;
 }
 
 // pair friction mu lambda f0(|u|): f0 = |u| beyond eps, else |u|^2 (eps - |u|/3) / eps^2 +
 // eps/3 (_getFrictionEnergy_Reduction_3D, GIPC.cu:1252-1356)
-__global__ void k_en_friction(int np, int nv, const int4* __restrict__ pairs, const double* __restrict__ x,
+__device__ __forceinline__ double en_friction(int gi, int np, int nv, const int4* __restrict__ pairs, const double* __restrict__ x,
                               const double* __restrict__ x0, const double* __restrict__ lam,
                               const double* __restrict__ coord, const double* __restrict__ basis, double mu,
-                              double eps2, double* __restrict__ part) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+                              double eps2) {
+    const int p = gi;
     double e = 0.0;
     if (p < np) {
         const int4 q = pairs[p];
@@ -1081,15 +1080,15 @@ __global__ void k_en_friction(int np, int nv, const int4* __restrict__ pairs, co
             e = mu * lam[p] * f0;
         }
     }
-    cta_energy(e, part);
+    return e;
 }
 
 // ground friction mu lambda (|v| - eps/2) beyond eps, else mu lambda |v|^2 / (2 eps), v the
 // tangential (x, z) step (_getFrictionEnergy_gd_Reduction_3D, GIPC.cu:1357-1437)
-__global__ void k_en_fric_ground(int ng, int nv, const uint32_t* __restrict__ gp, const double* __restrict__ x,
+__device__ __forceinline__ double en_fric_ground(int gi, int ng, int nv, const uint32_t* __restrict__ gp, const double* __restrict__ x,
                                  const double* __restrict__ x0, const double* __restrict__ lam, double mu,
-                                 double eps2, double* __restrict__ part) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+                                 double eps2) {
+    const int p = gi;
     double e = 0.0;
     if (p < ng && (int)gp[p] < nv) {
         const int v = gp[p];
@@ -1097,25 +1096,64 @@ __global__ void k_en_fric_ground(int ng, int nv, const uint32_t* __restrict__ gp
         const double m2 = vx * vx + vz * vz, s = mu * lam[p], eps = sqrt(eps2);
         e = m2 > eps2 ? s * (sqrt(m2) - eps * 0.5) : s * m2 / eps * 0.5;
     }
-    cta_energy(e, part);
+    return e;
 }
 
-// one warp: term t = sum of its CTA partials [off[t], off[t+1]) in a fixed order; terms[9]
-// = the terms summed in order
+// Everything in one launch: CTA b evaluates term t where off[t] <= b < off[t + 1] (its
+// elements (b - off[t]) * blockDim + threadIdx), stores its partial, and the last CTA to
+// finish (a ticket counter, reset by that CTA) sums each term's partials in order into
+// terms[t] and their total into terms[9].
 struct EnergyOffsets {
     int off[10];
 };
-__global__ void k_en_sum(const double* __restrict__ part, EnergyOffsets o, double* __restrict__ terms) {
-    double total = 0.0;
-    for (int t = 0; t < 9; t++) {
-        double s = 0.0;
-        for (int i = o.off[t] + (int)threadIdx.x; i < o.off[t + 1]; i += 32) s += part[i];
-#pragma unroll
-        for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
-        if (threadIdx.x == 0) terms[t] = s;
-        total += s;
+struct EnergyArgs {
+    int nv, nt, nf, nh, ns, npair, nground, nfric, nfg;
+    const double *x, *xt, *m, *x0, *rest;
+    const uint32_t *tets, *tris, *hinges, *soft_idx, *gp, *fgp;
+    const int32_t* adj;
+    const int4 *pairs, *fpairs;
+    const double *dminv, *vol, *lr, *vr, *tdminv, *area, *Q, *target, *flam, *coord, *basis, *fglam;
+    double dt2, kst, ksh, srate, kb_dt2, ksoft, dhat, kappa, offset, mu, mu_gd, eps2;
+};
+__global__ void __launch_bounds__(SGIPC_BLOCK) k_energy(EnergyArgs a, EnergyOffsets o, double* __restrict__ part,
+                                                        double* __restrict__ terms, unsigned int* __restrict__ ticket) {
+    int t = 0;
+    while (t < 8 && (int)blockIdx.x >= o.off[t + 1]) t++;
+    const int gi = ((int)blockIdx.x - o.off[t]) * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    switch (t) {
+        case 0: e = en_kinetic(gi, a.nv, a.x, a.xt, a.m); break;
+        case 1: e = en_snk(gi, a.nt, a.tets, a.x, a.dminv, a.vol, a.lr, a.vr, a.dt2); break;
+        case 2: e = en_tri(gi, a.nf, a.tris, a.x, a.tdminv, a.area, a.kst, a.ksh, a.srate, a.dt2); break;
+        case 3: e = en_hinge(gi, a.nh, a.hinges, a.adj, a.x, a.rest, a.Q, a.kb_dt2); break;
+        case 4: e = en_soft(gi, a.ns, a.soft_idx, a.x, a.target, a.ksoft); break;
+        case 5: e = en_barrier(gi, a.npair, a.nv, a.pairs, a.x, a.rest, a.dhat, a.kappa); break;
+        case 6: e = en_ground(gi, a.nground, a.nv, a.gp, a.x, a.offset, a.dhat, a.kappa); break;
+        case 7: e = en_friction(gi, a.nfric, a.nv, a.fpairs, a.x, a.x0, a.flam, a.coord, a.basis, a.mu, a.eps2); break;
+        default: e = en_fric_ground(gi, a.nfg, a.nv, a.fgp, a.x, a.x0, a.fglam, a.mu_gd, a.eps2); break;
     }
-    if (threadIdx.x == 0) terms[9] = total;
+    cta_energy(e, part);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    double total = 0.0;
+    for (int q = 0; q < 9; q++) {
+        double sum = 0.0;
+        for (int i = o.off[q] + (int)threadIdx.x; i < o.off[q + 1]; i += 32) sum += __ldcg(part + i);
+#pragma unroll
+        for (int k = 16; k > 0; k >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, k);
+        if (threadIdx.x == 0) terms[q] = sum;
+        total += sum;
+    }
+    if (threadIdx.x == 0) {
+        terms[9] = total;
+        *ticket = 0u;
+    }
 }
 
 }  // namespace
@@ -1437,53 +1475,22 @@ static SgipcStatus energy_launch(SgipcCtx* c, const SgipcFemData* f, const Sgipc
         snprintf(c->err, sizeof(c->err), "energy: %d partial sums exceed the context's %d", o.off[9], c->en_cap);
         return SGIPC_CAPACITY;
     }
-    double* P = c->en_part;
-    const int B = SGIPC_BLOCK;
-    int nl = 1;
-    k_en_kinetic<<<nblk(c->nv), B, 0, s>>>(c->nv, f->vertexes, f->xTilta, f->masses, P + o.off[0]);
-    if (c->nt > 0) {
-        nl++;
-        k_en_snk<<<nblk(c->nt), B, 0, s>>>(c->nt, c->tets, f->vertexes, f->DmInverses, f->volum, f->lengthRate,
-                                          f->volumeRate, dt2, P + o.off[1]);
-    }
-    if (c->nf > 0) {
-        nl++;
-        k_en_tri<<<nblk(c->nf), B, 0, s>>>(c->nf, c->tris, f->vertexes, f->triDmInverses, f->area, p->stretchStiff,
-                                          p->shearStiff, p->strainRate, dt2, P + o.off[2]);
-    }
-    if (c->nh > 0) {
-        nl++;
-        k_en_hinge<<<nblk(c->nh), B, 0, s>>>(c->nh, c->hinges, c->hinge_adj, f->vertexes, f->rest_vertexes,
-                                            f->quad_bending_Q, p->bendStiff * dt2, P + o.off[3]);
-    }
-    if (c->nsoft > 0) {
-        nl++;
-        k_en_soft<<<nblk(c->nsoft), B, 0, s>>>(c->nsoft, c->soft_idx, f->vertexes, f->targetVert,
-                                              p->motionRate * p->softRate * p->softRate, P + o.off[4]);
-    }
-    if (npair > 0) {
-        nl++;
-        k_en_barrier<<<nblk(npair), B, 0, s>>>(npair, c->nv, (const int4*)k->pairs, f->vertexes, f->rest_vertexes,
-                                              p->dHat, p->kappa, P + o.off[5]);
-    }
-    if (nground > 0) {
-        nl++;
-        k_en_ground<<<nblk(nground), B, 0, s>>>(nground, c->nv, k->ground_pairs, f->vertexes, p->ground_offset,
-                                               p->dHat, p->kappa, P + o.off[6]);
-    }
-    if (nfric > 0) {
-        nl++;
-        k_en_friction<<<nblk(nfric), B, 0, s>>>(nfric, c->nv, (const int4*)k->fric_pairs, f->vertexes,
-                                               f->o_vertexes, k->fric_lambda, k->fric_coord, k->fric_basis,
-                                               p->frictionRate, eps2, P + o.off[7]);
-    }
-    if (nfg > 0) {
-        nl++;
-        k_en_fric_ground<<<nblk(nfg), B, 0, s>>>(nfg, c->nv, k->fric_gd_pairs, f->vertexes, f->o_vertexes,
-                                                  k->fric_gd_lambda, p->gd_frictionRate, eps2, P + o.off[8]);
-    }
-    k_en_sum<<<1, 32, 0, s>>>(P, o, c->en_terms);
-    SG_COUNT(c, nl + 1);
+    EnergyArgs a;
+    a.nv = c->nv; a.nt = c->nt; a.nf = c->nf; a.nh = c->nh; a.ns = c->nsoft;
+    a.npair = npair; a.nground = nground; a.nfric = nfric; a.nfg = nfg;
+    a.x = f->vertexes; a.xt = f->xTilta; a.m = f->masses; a.x0 = f->o_vertexes; a.rest = f->rest_vertexes;
+    a.tets = c->tets; a.tris = c->tris; a.hinges = c->hinges; a.soft_idx = c->soft_idx;
+    a.gp = k ? k->ground_pairs : nullptr; a.fgp = k ? k->fric_gd_pairs : nullptr; a.adj = c->hinge_adj;
+    a.pairs = k ? (const int4*)k->pairs : nullptr; a.fpairs = k ? (const int4*)k->fric_pairs : nullptr;
+    a.dminv = f->DmInverses; a.vol = f->volum; a.lr = f->lengthRate; a.vr = f->volumeRate;
+    a.tdminv = f->triDmInverses; a.area = f->area; a.Q = f->quad_bending_Q; a.target = f->targetVert;
+    a.flam = k ? k->fric_lambda : nullptr; a.coord = k ? k->fric_coord : nullptr; a.basis = k ? k->fric_basis : nullptr;
+    a.fglam = k ? k->fric_gd_lambda : nullptr;
+    a.dt2 = dt2; a.kst = p->stretchStiff; a.ksh = p->shearStiff; a.srate = p->strainRate; a.kb_dt2 = p->bendStiff * dt2;
+    a.ksoft = p->motionRate * p->softRate * p->softRate; a.dhat = p->dHat; a.kappa = p->kappa;
+    a.offset = p->ground_offset; a.mu = p->frictionRate; a.mu_gd = p->gd_frictionRate; a.eps2 = eps2;
+    k_energy<<<o.off[9], SGIPC_BLOCK, 0, s>>>(a, o, c->en_part, c->en_terms, c->en_ticket);
+    SG_COUNT(c, 1);
     SG_LAUNCH_CHECK(c, "energy");
     if (bytes)  // positions (and the per-element inputs) in, one partial per CTA out and back
         *bytes = (double)c->nv * (24 + 24 + 8) + (double)c->nt * (16 + 4 * 24 + 72 + 8 + 16) +

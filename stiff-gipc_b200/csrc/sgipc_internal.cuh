@@ -195,6 +195,7 @@ struct SgipcCtx {
     double* en_part;              // [en_cap] per-CTA partial sums of the line-search energy terms
     int en_cap;
     double* en_terms;             // [16] device: the nine terms and their total
+    unsigned int* en_ticket;      // [1] device: CTAs of the energy launch done (0 between launches)
     double* h_en;                 // [16] pinned landing area of en_terms ([12], [13]: step sizes)
     double* ccd_part;             // [592] per-CTA maxima of the step-size kernels
     double* ccd_out;              // [1] the step
