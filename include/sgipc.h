@@ -212,6 +212,11 @@ SgipcStatus sgipc_self_step_size(SgipcCtx* ctx, const double* x, const double* m
 SgipcStatus sgipc_ground_step_size(SgipcCtx* ctx, const double* x, const double* move_dir, const uint32_t* verts,
                                    int32_t nverts, double ground_offset, double slackness, double* alpha,
                                    void* stream);
+/* GIPC::cfl_largestSpeed (GIPC.cu:8916-8944; per vertex _reduct_max_cfl_to_double
+ * GIPC.cu:7157): the largest |move_dir| over the vertices verts (0 for none), from which
+ * the reference bounds the step by sqrt(dHat) / (2 speed).  Synchronises the stream. */
+SgipcStatus sgipc_cfl_largest_speed(SgipcCtx* ctx, const double* move_dir, const uint32_t* verts, int32_t nverts,
+                                    double* speed, void* stream);
 
 /* ---- operators --------------------------------------------------------------------- */
 

@@ -72,6 +72,8 @@ def lib():
         L.or_self_step.restype = C.c_double
         L.or_ground_step.argtypes = [_d, _d, _u, C.c_int, C.c_double, C.c_double]
         L.or_ground_step.restype = C.c_double
+        L.or_cfl_speed.argtypes = [_d, _u, C.c_int]
+        L.or_cfl_speed.restype = C.c_double
         L.or_num_threads.restype = C.c_int
     return _LIB
 
@@ -271,6 +273,13 @@ def ground_step(x, move_dir, verts, offset, slackness):
     x, move_dir = _f64(x), _f64(move_dir)
     verts = np.ascontiguousarray(verts, dtype=np.uint32)
     return lib().or_ground_step(_p(x), _p(move_dir), verts.ctypes.data_as(_u), len(verts), offset, slackness)
+
+
+def cfl_speed(move_dir, verts):
+    """GIPC::cfl_largestSpeed (GIPC.cu:8916): the largest |move_dir| over verts."""
+    move_dir = _f64(move_dir)
+    verts = np.ascontiguousarray(verts, dtype=np.uint32)
+    return lib().or_cfl_speed(_p(move_dir), verts.ctypes.data_as(_u), len(verts))
 
 
 def spmv(rows, cols, vals, n, x):

@@ -1477,6 +1477,16 @@ double or_ground_step(const double* x, const double* dir, const uint32_t* verts,
     return 1.0 / vmax;
 }
 
+// largest |dir| over the vertices verts (GIPC.cu:7157, cfl_largestSpeed :8916-8944)
+double or_cfl_speed(const double* dir, const uint32_t* verts, int n) {
+    double m = 0.0;
+    for (int i = 0; i < n; i++) {
+        const double* d = dir + 3 * verts[i];
+        m = std::max(m, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+    }
+    return m;
+}
+
 int or_num_threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();

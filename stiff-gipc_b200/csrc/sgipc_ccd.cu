@@ -249,17 +249,34 @@ __global__ void __launch_bounds__(SGIPC_BLOCK) k_ground_step(int ns, int nv, con
     cta_max(vmax, part);
 }
 
-// one warp: out = 1 / max of the n partials
-__global__ void k_step_final(int n, const double* __restrict__ part, double* __restrict__ out) {
-    double m = 1.0;
+// largest |dir| over the vertices verts (_reduct_max_cfl_to_double, GIPC.cu:7157)
+__global__ void __launch_bounds__(SGIPC_BLOCK) k_cfl_speed(int ns, int nv, const uint32_t* __restrict__ verts,
+                                                           const double* __restrict__ dir, double* __restrict__ part,
+                                                           int* __restrict__ bad) {
+    double vmax = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
+        const uint32_t v = verts[i];
+        if (v >= (uint32_t)nv) {
+            atomicOr(bad, 1);
+            continue;
+        }
+        vmax = fmax(vmax, sqrt(sq(ld3(dir, (int)v))));
+    }
+    cta_max(vmax, part);
+}
+
+// one warp: m = max(init, the n partials); out = 1 / m (step sizes) or m (speeds)
+__global__ void k_step_final(int n, const double* __restrict__ part, double init, int invert,
+                             double* __restrict__ out) {
+    double m = init;
     for (int i = threadIdx.x; i < n; i += 32) m = fmax(m, part[i]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (threadIdx.x == 0) out[0] = 1.0 / m;
+    if (threadIdx.x == 0) out[0] = invert ? 1.0 / m : m;
 }
 
-SgipcStatus finish_step(SgipcCtx* c, int grid, cudaStream_t s, double* alpha, const char* what) {
-    k_step_final<<<1, 32, 0, s>>>(grid, c->ccd_part, c->ccd_out);
+SgipcStatus finish_step(SgipcCtx* c, int grid, cudaStream_t s, double* alpha, const char* what, bool speed = false) {
+    k_step_final<<<1, 32, 0, s>>>(grid, c->ccd_part, speed ? 0.0 : 1.0, speed ? 0 : 1, c->ccd_out);
     SG_COUNT(c, 2);
     SG_LAUNCH_CHECK(c, what);
     SG_CHECK(c, cudaMemcpyAsync(c->h_en + 12, c->ccd_out, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -303,4 +320,15 @@ extern "C" SgipcStatus sgipc_ground_step_size(SgipcCtx* c, const double* x, cons
     k_ground_step<<<grid, SGIPC_BLOCK, 0, s>>>(nverts, c->nv, verts, x, move_dir, ground_offset, slackness,
                                                c->ccd_part, c->ccd_bad);
     return finish_step(c, grid, s, alpha, "ground step size");
+}
+
+extern "C" SgipcStatus sgipc_cfl_largest_speed(SgipcCtx* c, const double* move_dir, const uint32_t* verts,
+                                               int32_t nverts, double* speed, void* stream) {
+    if (!c || !move_dir || !speed || nverts < 0 || (nverts > 0 && !verts)) return SGIPC_BAD_INPUT;
+    SG_CHECK(c, cudaSetDevice(c->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int grid = std::max(1, std::min(nblk(nverts), kCcdGrid));
+    SG_CHECK(c, cudaMemsetAsync(c->ccd_bad, 0, sizeof(int), s));
+    k_cfl_speed<<<grid, SGIPC_BLOCK, 0, s>>>(nverts, c->nv, verts, move_dir, c->ccd_part, c->ccd_bad);
+    return finish_step(c, grid, s, speed, "cfl speed", true);
 }

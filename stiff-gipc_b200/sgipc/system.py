@@ -255,6 +255,14 @@ class GIPC:
                                                _stream()), self.ctx)
         return a.value
 
+    def cfl_largestSpeed(self, move_dir: torch.Tensor, verts: torch.Tensor):
+        """GIPC::cfl_largestSpeed (GIPC.cu:8916): the largest |move_dir| over the vertices."""
+        verts = verts.contiguous()
+        v = C.c_double(0.0)
+        N.check(N.lib().sgipc_cfl_largest_speed(self.ctx, _p(move_dir), _p(verts), verts.shape[0], C.byref(v),
+                                                _stream()), self.ctx)
+        return v.value
+
     def rhs(self) -> torch.Tensor:
         b = torch.empty(3 * self.n, dtype=torch.float64, device=_dev())
         N.check(N.lib().sgipc_get_rhs(self.ctx, _p(b), _stream()), self.ctx)

@@ -84,6 +84,15 @@ def test_ground_bound_matches_oracle(g):
     assert a == pytest.approx(ao, rel=1e-12)
 
 
+def test_cfl_speed_matches_oracle(g):
+    sc, gg = g
+    d = np.random.default_rng(4).standard_normal((sc.nv, 3))
+    verts = np.arange(0, sc.nv, 3, dtype=np.int32)
+    v = gg.cfl_largestSpeed(_dev(d), _dev(verts, torch.int32))
+    assert v == pytest.approx(oracle.cfl_speed(d, verts.astype(np.uint32)), rel=1e-14)
+    assert gg.cfl_largestSpeed(_dev(d), torch.zeros(0, dtype=torch.int32, device="cuda")) == 0.0
+
+
 def test_empty_sets_and_bad_indices(g):
     sc, gg = g
     z = _dev(np.zeros((sc.nv, 3)))

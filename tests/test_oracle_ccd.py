@@ -65,3 +65,10 @@ def test_ground_bound():
     d = np.array([[0.0, 2.0, 0.0], [0.0, -1.0, 0.0]])  # the first falls, the second rises
     assert oracle.ground_step(x, d, [0, 1], 0.0, 0.8) == pytest.approx(0.4, rel=1e-12)
     assert oracle.ground_step(x, d, [1], 0.0, 0.8) == 1.0
+
+
+def test_cfl_speed():
+    d = np.array([[3.0, 4.0, 0.0], [0.0, 0.0, -12.0], [1.0, 0.0, 0.0]])
+    assert oracle.cfl_speed(d, [0, 2]) == 5.0
+    assert oracle.cfl_speed(d, [0, 1, 2]) == 12.0
+    assert oracle.cfl_speed(d, []) == 0.0
