@@ -179,9 +179,21 @@ __device__ double accd(bool ee, d3* X, d3* D, double eta, double thick) {
 // fixed-size grid of the step-size kernels (grid-stride loops over the candidates)
 constexpr int kCcdGrid = 148 * 4;
 
-// max over the CTA of v into part[blockIdx.x] (every thread calls it)
-__device__ __forceinline__ void cta_max(double v, double* __restrict__ part) {
+// How a step-size launch ends: the last CTA to finish (ticket) takes m = max(init, every
+// CTA's maximum), writes out[0] = 1 / m (step sizes) or m (speeds) and out[1] = the
+// out-of-range flag, and resets the flag and the ticket for the next launch.
+struct StepFinish {
+    double init;
+    int invert;
+    double* out;
+    int* bad;
+    unsigned int* ticket;
+};
+
+// max over the CTA of v into part[blockIdx.x], then the finish above (every thread calls it)
+__device__ __forceinline__ void cta_max(double v, double* __restrict__ part, const StepFinish& fin) {
     __shared__ double sw[SGIPC_BLOCK / 32];
+    __shared__ bool last;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = v;
@@ -190,6 +202,20 @@ __device__ __forceinline__ void cta_max(double v, double* __restrict__ part) {
         double m = sw[0];
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmax(m, sw[w]);
         part[blockIdx.x] = m;
+        __threadfence();
+        last = atomicAdd(fin.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    double m = fin.init;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) m = fmax(m, __ldcg(part + i));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) {
+        fin.out[0] = fin.invert ? 1.0 / m : m;
+        fin.out[1] = (double)atomicExch(fin.bad, 0);
+        *fin.ticket = 0u;
     }
 }
 
@@ -199,7 +225,7 @@ __global__ void __launch_bounds__(SGIPC_BLOCK) k_self_step(int np, int nv, const
                                                            const double* __restrict__ x,
                                                            const double* __restrict__ dir, double eta,
                                                            double* __restrict__ toi, double* __restrict__ part,
-                                                           int* __restrict__ bad) {
+                                                           StepFinish fin) {
     double vmax = 1.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
         int4 q = pairs[i];
@@ -221,12 +247,12 @@ __global__ void __launch_bounds__(SGIPC_BLOCK) k_self_step(int np, int nv, const
             inv = 1.0 / t;
             if (toi) toi[i] = t;
         } else {
-            atomicOr(bad, 1);
+            atomicOr(fin.bad, 1);
             if (toi) toi[i] = 1.0;
         }
         vmax = fmax(vmax, inv);
     }
-    cta_max(vmax, part);
+    cta_max(vmax, part, fin);
 }
 
 // per surface vertex approaching the plane y = offset (dir . n > 0 with n = +y):
@@ -235,60 +261,50 @@ __global__ void __launch_bounds__(SGIPC_BLOCK) k_ground_step(int ns, int nv, con
                                                              const double* __restrict__ x,
                                                              const double* __restrict__ dir, double offset,
                                                              double slackness, double* __restrict__ part,
-                                                             int* __restrict__ bad) {
+                                                             StepFinish fin) {
     double vmax = 1.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
         const uint32_t v = verts[i];
         if (v >= (uint32_t)nv) {
-            atomicOr(bad, 1);
+            atomicOr(fin.bad, 1);
             continue;
         }
         const double coef = dir[3 * v + 1];
         if (coef > 0.0) vmax = fmax(vmax, coef / ((x[3 * v + 1] - offset) * slackness));
     }
-    cta_max(vmax, part);
+    cta_max(vmax, part, fin);
 }
 
 // largest |dir| over the vertices verts (_reduct_max_cfl_to_double, GIPC.cu:7157)
 __global__ void __launch_bounds__(SGIPC_BLOCK) k_cfl_speed(int ns, int nv, const uint32_t* __restrict__ verts,
                                                            const double* __restrict__ dir, double* __restrict__ part,
-                                                           int* __restrict__ bad) {
+                                                           StepFinish fin) {
     double vmax = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
         const uint32_t v = verts[i];
         if (v >= (uint32_t)nv) {
-            atomicOr(bad, 1);
+            atomicOr(fin.bad, 1);
             continue;
         }
         vmax = fmax(vmax, sqrt(sq(ld3(dir, (int)v))));
     }
-    cta_max(vmax, part);
+    cta_max(vmax, part, fin);
 }
 
-// one warp: m = max(init, the n partials); out = 1 / m (step sizes) or m (speeds)
-__global__ void k_step_final(int n, const double* __restrict__ part, double init, int invert,
-                             double* __restrict__ out) {
-    double m = init;
-    for (int i = threadIdx.x; i < n; i += 32) m = fmax(m, part[i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (threadIdx.x == 0) out[0] = invert ? 1.0 / m : m;
+StepFinish step_finish(SgipcCtx* c, bool speed) {
+    return {speed ? 0.0 : 1.0, speed ? 0 : 1, c->ccd_out, c->ccd_bad, c->ccd_ticket};
 }
 
-SgipcStatus finish_step(SgipcCtx* c, int grid, cudaStream_t s, double* alpha, const char* what, bool speed = false) {
-    k_step_final<<<1, 32, 0, s>>>(grid, c->ccd_part, speed ? 0.0 : 1.0, speed ? 0 : 1, c->ccd_out);
-    SG_COUNT(c, 2);
+SgipcStatus read_step(SgipcCtx* c, cudaStream_t s, double* value, const char* what) {
+    SG_COUNT(c, 1);
     SG_LAUNCH_CHECK(c, what);
-    SG_CHECK(c, cudaMemcpyAsync(c->h_en + 12, c->ccd_out, sizeof(double), cudaMemcpyDeviceToHost, s));
-    SG_CHECK(c, cudaMemcpyAsync(c->h_en + 13, c->ccd_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaMemcpyAsync(c->h_en + 12, c->ccd_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     SG_CHECK(c, cudaStreamSynchronize(s));
-    int bad = 0;
-    memcpy(&bad, c->h_en + 13, sizeof(int));
-    if (bad) {
+    if (c->h_en[13] != 0.0) {
         snprintf(c->err, sizeof(c->err), "%s: a candidate names a vertex outside [0, %d)", what, c->nv);
         return SGIPC_BAD_INPUT;
     }
-    *alpha = c->h_en[12];
+    *value = c->h_en[12];
     return SGIPC_OK;
 }
 
@@ -302,10 +318,9 @@ extern "C" SgipcStatus sgipc_self_step_size(SgipcCtx* c, const double* x, const 
     SG_CHECK(c, cudaSetDevice(c->device));
     cudaStream_t s = (cudaStream_t)stream;
     const int grid = std::max(1, std::min(nblk(npairs), kCcdGrid));
-    SG_CHECK(c, cudaMemsetAsync(c->ccd_bad, 0, sizeof(int), s));
     k_self_step<<<grid, SGIPC_BLOCK, 0, s>>>(npairs, c->nv, (const int4*)pairs, x, move_dir, 1.0 - slackness, toi,
-                                             c->ccd_part, c->ccd_bad);
-    return finish_step(c, grid, s, alpha, "self step size");
+                                             c->ccd_part, step_finish(c, false));
+    return read_step(c, s, alpha, "self step size");
 }
 
 extern "C" SgipcStatus sgipc_ground_step_size(SgipcCtx* c, const double* x, const double* move_dir,
@@ -316,10 +331,9 @@ extern "C" SgipcStatus sgipc_ground_step_size(SgipcCtx* c, const double* x, cons
     SG_CHECK(c, cudaSetDevice(c->device));
     cudaStream_t s = (cudaStream_t)stream;
     const int grid = std::max(1, std::min(nblk(nverts), kCcdGrid));
-    SG_CHECK(c, cudaMemsetAsync(c->ccd_bad, 0, sizeof(int), s));
     k_ground_step<<<grid, SGIPC_BLOCK, 0, s>>>(nverts, c->nv, verts, x, move_dir, ground_offset, slackness,
-                                               c->ccd_part, c->ccd_bad);
-    return finish_step(c, grid, s, alpha, "ground step size");
+                                               c->ccd_part, step_finish(c, false));
+    return read_step(c, s, alpha, "ground step size");
 }
 
 extern "C" SgipcStatus sgipc_cfl_largest_speed(SgipcCtx* c, const double* move_dir, const uint32_t* verts,
@@ -328,7 +342,6 @@ extern "C" SgipcStatus sgipc_cfl_largest_speed(SgipcCtx* c, const double* move_d
     SG_CHECK(c, cudaSetDevice(c->device));
     cudaStream_t s = (cudaStream_t)stream;
     const int grid = std::max(1, std::min(nblk(nverts), kCcdGrid));
-    SG_CHECK(c, cudaMemsetAsync(c->ccd_bad, 0, sizeof(int), s));
-    k_cfl_speed<<<grid, SGIPC_BLOCK, 0, s>>>(nverts, c->nv, verts, move_dir, c->ccd_part, c->ccd_bad);
-    return finish_step(c, grid, s, speed, "cfl speed", true);
+    k_cfl_speed<<<grid, SGIPC_BLOCK, 0, s>>>(nverts, c->nv, verts, move_dir, c->ccd_part, step_finish(c, true));
+    return read_step(c, s, speed, "cfl speed");
 }

@@ -259,9 +259,12 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
         for (long long v : cnt) ecap += nblk(v);
         c->en_cap = (int)ecap;
         if ((st = dalloc(c, &c->en_part, ecap)) || (st = dalloc(c, &c->en_terms, 16)) ||
-            (st = dalloc(c, &c->ccd_part, 148 * 4)) || (st = dalloc(c, &c->ccd_out, 1)) ||
-            (st = dalloc(c, &c->ccd_bad, 1)) || (st = dalloc(c, &c->en_ticket, 1)))
+            (st = dalloc(c, &c->ccd_part, 148 * 4)) || (st = dalloc(c, &c->ccd_out, 2)) ||
+            (st = dalloc(c, &c->ccd_bad, 1)) || (st = dalloc(c, &c->en_ticket, 1)) ||
+            (st = dalloc(c, &c->ccd_ticket, 1)))
             return fail(st);
+        SG_CHECK(c, cudaMemset(c->ccd_bad, 0, sizeof(int)));
+        SG_CHECK(c, cudaMemset(c->ccd_ticket, 0, sizeof(unsigned int)));
         SG_CHECK(c, cudaMemset(c->en_ticket, 0, sizeof(unsigned int)));
         SG_CHECK(c, cudaMallocHost((void**)&c->h_en, sizeof(double) * 16));
     }
@@ -296,7 +299,7 @@ extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
                     c->hinges, c->hinge_adj, c->soft_idx, c->shape_grads, c->fb, c->b, c->ckey, c->ckey_s,
                     c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,
                     c->cu_ptr, c->cl_ptr, c->cl_idx, c->lcount, c->lpos, c->cub_tmp, c->dflag,
-                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32, c->run_start, c->en_part, c->en_terms, c->ccd_part, c->ccd_out, c->ccd_bad, c->en_ticket};
+                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32, c->run_start, c->en_part, c->en_terms, c->ccd_part, c->ccd_out, c->ccd_bad, c->en_ticket, c->ccd_ticket};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_en) cudaFreeHost(c->h_en);

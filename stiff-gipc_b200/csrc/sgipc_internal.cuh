@@ -198,8 +198,9 @@ struct SgipcCtx {
     unsigned int* en_ticket;      // [1] device: CTAs of the energy launch done (0 between launches)
     double* h_en;                 // [16] pinned landing area of en_terms ([12], [13]: step sizes)
     double* ccd_part;             // [592] per-CTA maxima of the step-size kernels
-    double* ccd_out;              // [1] the step
-    int* ccd_bad;                 // [1] a candidate with an out-of-range vertex
+    double* ccd_out;              // [2] the step (or speed) and the out-of-range flag
+    int* ccd_bad;                 // [1] a candidate with an out-of-range vertex (0 between launches)
+    unsigned int* ccd_ticket;     // [1] CTAs of a step-size launch done (0 between launches)
     // last inputs (for re-timing kernels against the current state)
     SgipcFemData last_fem;
     SgipcContacts last_con;
