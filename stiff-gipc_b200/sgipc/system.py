@@ -223,7 +223,7 @@ class GIPC:
         With terms=True also the nine parts (kinetic, tets, triangles, hinges, soft, barrier,
         ground, friction, ground friction) as a numpy array."""
         tet = tet or self.tet
-        f, k, p = tet.fem_struct(), tet.contact_struct(), params_struct(self.params)
+        f, k, p = tet.fem_struct_cached(), tet.contact_struct_cached(), self._params()
         e = C.c_double(0.0)
         parts = np.zeros(9)
         N.check(N.lib().sgipc_compute_energy(self.ctx, C.byref(f), C.byref(k), C.byref(p), C.byref(e),
