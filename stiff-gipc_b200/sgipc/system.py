@@ -315,26 +315,55 @@ class GIPC:
 
 class HostNewtonState:
     """Pinned host copies of the per-Newton inputs (iterate x and the contact arrays),
-    for callers that keep their state on the host (``step_from_host``)."""
+    for callers that keep their state on the host (``step_from_host``).
 
-    def __init__(self, sc):
-        def pin(a, dtype):
-            return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).pin_memory()
-
-        f64, i32 = torch.float64, torch.int32
-        self.vertexes = pin(sc.vertexes, f64)
-        self.pairs = pin(sc.pairs.reshape(-1, 4), i32)
-        self.ground_pairs = pin(sc.ground_pairs, i32)
-        self.fric_pairs = pin(sc.fric_pairs.reshape(-1, 4), i32)
-        self.fric_lambda = pin(sc.fric_lambda, f64)
-        self.fric_coord = pin(sc.fric_coord.reshape(-1, 2), f64)
-        self.fric_basis = pin(sc.fric_basis.reshape(-1, 6), f64)
-        self.fric_gd_pairs = pin(sc.fric_gd_pairs, i32)
-        self.fric_gd_lambda = pin(sc.fric_gd_lambda, f64)
-        self.move_dir = torch.empty(3 * sc.nv, dtype=f64).pin_memory()
+    The arrays are packed into one pinned buffer (each at a 256-byte boundary).  The first
+    ``step_from_host`` on a GIPC rebinds that GIPC's device arrays to views of one device
+    buffer of the same layout, so that every later step moves all inputs with a single
+    host-to-device copy instead of one copy per array."""
 
     NAMES = ("vertexes", "pairs", "ground_pairs", "fric_pairs", "fric_lambda", "fric_coord", "fric_basis",
              "fric_gd_pairs", "fric_gd_lambda")
+
+    def __init__(self, sc):
+        f64, i32 = torch.float64, torch.int32
+        src = {"vertexes": (sc.vertexes, f64), "pairs": (sc.pairs.reshape(-1, 4), i32),
+               "ground_pairs": (sc.ground_pairs, i32), "fric_pairs": (sc.fric_pairs.reshape(-1, 4), i32),
+               "fric_lambda": (sc.fric_lambda, f64), "fric_coord": (sc.fric_coord.reshape(-1, 2), f64),
+               "fric_basis": (sc.fric_basis.reshape(-1, 6), f64), "fric_gd_pairs": (sc.fric_gd_pairs, i32),
+               "fric_gd_lambda": (sc.fric_gd_lambda, f64)}
+        self._layout, off = [], 0
+        for n in self.NAMES:
+            a, dt = src[n]
+            t = torch.as_tensor(np.ascontiguousarray(a), dtype=dt)
+            self._layout.append((n, off, dt, tuple(t.shape)))
+            off += (t.numel() * t.element_size() + 255) // 256 * 256
+        self._bytes = max(off, 256)
+        self._host = torch.zeros(self._bytes, dtype=torch.uint8).pin_memory()
+        for n, o, dt, shape in self._layout:
+            v = self._views(self._host, n)
+            v.copy_(torch.as_tensor(np.ascontiguousarray(src[n][0]), dtype=dt).reshape(shape))
+            setattr(self, n, v)
+        self.move_dir = torch.empty(3 * sc.nv, dtype=f64).pin_memory()
+        self._dev = None
+        self._bound = None
+
+    def _views(self, buf, name):
+        for n, o, dt, shape in self._layout:
+            if n == name:
+                nb = int(np.prod(shape)) * torch.tensor([], dtype=dt).element_size()
+                return buf[o:o + nb].view(dt).view(shape)
+        raise KeyError(name)
+
+    def bind(self, tet: "DeviceTetraData"):
+        """Make tet's input arrays views of one device buffer laid out like the host one."""
+        if self._bound is tet:
+            return
+        self._dev = torch.empty(self._bytes, dtype=torch.uint8, device=_dev())
+        self._dev.copy_(self._host)
+        for n, _, _, _ in self._layout:
+            setattr(tet, n, self._views(self._dev, n))
+        self._bound = tet
 
     def h2d_bytes(self) -> int:
         return int(sum(getattr(self, n).numel() * getattr(self, n).element_size() for n in self.NAMES))
@@ -344,10 +373,10 @@ class HostNewtonState:
 
 
 def step_from_host(g: "GIPC", host: HostNewtonState, config: Optional[PCGSolverConfig] = None):
-    """One Newton system from host inputs: H2D copies, assembly, MAS + PCG, D2H of dx."""
+    """One Newton system from host inputs: one H2D copy, assembly, MAS + PCG, D2H of dx."""
     tet = g.tet
-    for n in HostNewtonState.NAMES:
-        getattr(tet, n).copy_(getattr(host, n), non_blocking=True)
+    host.bind(tet)
+    host._dev.copy_(host._host, non_blocking=True)
     g.computeGradientAndHessian(tet)
     st = g.calculateMovingDirection(config, tet)
     host.move_dir.copy_(g.moveDir, non_blocking=True)

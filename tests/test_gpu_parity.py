@@ -244,6 +244,23 @@ def test_mas_build_after_a_new_static_matrix_uses_it(case):
     assert np.abs(d2 - d0).max() > 100 * np.abs(d1 - d2).max()
 
 
+def test_step_from_host_matches_device_step(case):
+    """The host-state path (inputs packed in one pinned buffer, one copy per step) solves the
+    same system as the device path; twice, the second time through the bound buffers."""
+    sc, g, _ = case
+    cfg = system.PCGSolverConfig(precision="fp64")
+    g.computeGradientAndHessian()
+    st0 = g.calculateMovingDirection(cfg)
+    x0 = g.moveDir.cpu().numpy()
+    host = system.HostNewtonState(sc)
+    for _ in range(2):
+        host.move_dir.zero_()
+        st = system.step_from_host(g, host, cfg)
+        assert st.status == N.OK and abs(st.iterations - st0.iterations) <= 1
+        assert _rel(host.move_dir.numpy(), x0) < 1e-9
+    g.computeGradientAndHessian()
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_zero_rhs_gives_zero_solution(case, prec):
     sc, g, _ = case
