@@ -217,6 +217,12 @@ SgipcStatus sgipc_ground_step_size(SgipcCtx* ctx, const double* x, const double*
  * the reference bounds the step by sqrt(dHat) / (2 speed).  Synchronises the stream. */
 SgipcStatus sgipc_cfl_largest_speed(SgipcCtx* ctx, const double* move_dir, const uint32_t* verts, int32_t nverts,
                                     double* speed, void* stream);
+/* GIPC::step_forward (GIPC.cu:9637; _stepForward :7937): the line search's trial positions
+ * x = x_base - alpha move_dir for the vertices with boundary_type 0 (all of them when
+ * move_boundary is nonzero); the others keep their x.  Device double3 arrays of the
+ * context's vertices; x may not alias x_base.  Stream-ordered. */
+SgipcStatus sgipc_step_forward(SgipcCtx* ctx, double* x, const double* x_base, const double* move_dir,
+                               const int32_t* boundary_type, double alpha, int32_t move_boundary, void* stream);
 
 /* ---- operators --------------------------------------------------------------------- */
 

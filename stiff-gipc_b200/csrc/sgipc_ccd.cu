@@ -308,7 +308,29 @@ SgipcStatus read_step(SgipcCtx* c, cudaStream_t s, double* value, const char* wh
     return SGIPC_OK;
 }
 
+// x = x_base - alpha dir for the free vertices (all with move_boundary), GIPC.cu:7937
+__global__ void k_step_forward(int nv, double* __restrict__ x, const double* __restrict__ xb,
+                               const double* __restrict__ dir, const int* __restrict__ btype, double alpha,
+                               int move_boundary) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * nv) return;
+    if (move_boundary || btype[i / 3] == 0) x[i] = xb[i] - alpha * dir[i];
+}
+
 }  // namespace
+
+extern "C" SgipcStatus sgipc_step_forward(SgipcCtx* c, double* x, const double* x_base, const double* move_dir,
+                                          const int32_t* boundary_type, double alpha, int32_t move_boundary,
+                                          void* stream) {
+    if (!c || !x || !x_base || !move_dir || (!move_boundary && !boundary_type)) return SGIPC_BAD_INPUT;
+    SG_CHECK(c, cudaSetDevice(c->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    SG_COUNT(c, 1);
+    k_step_forward<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, x, x_base, move_dir, boundary_type, alpha,
+                                                             move_boundary);
+    SG_LAUNCH_CHECK(c, "step forward");
+    return SGIPC_OK;
+}
 
 extern "C" SgipcStatus sgipc_self_step_size(SgipcCtx* c, const double* x, const double* move_dir,
                                             const int32_t* pairs, int32_t npairs, double slackness, double* alpha,

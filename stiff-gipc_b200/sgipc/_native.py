@@ -77,6 +77,7 @@ SIGNATURES = {
     "sgipc_ground_step_size": ([_vp, _vp, _vp, _vp, _i32, C.c_double, C.c_double, C.POINTER(C.c_double), _vp],
                                _i32),
     "sgipc_cfl_largest_speed": ([_vp, _vp, _vp, _i32, C.POINTER(C.c_double), _vp], _i32),
+    "sgipc_step_forward": ([_vp, _vp, _vp, _vp, _vp, C.c_double, _i32, _vp], _i32),
     "sgipc_spmv": ([_vp, _vp, _vp, _vp], _i32),
     "sgipc_mas_build": ([_vp, C.POINTER(SgipcContacts), _i32, _vp], _i32),
     "sgipc_mas_apply": ([_vp, _vp, _vp, _vp], _i32),

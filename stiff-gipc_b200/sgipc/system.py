@@ -263,6 +263,15 @@ class GIPC:
                                                 _stream()), self.ctx)
         return v.value
 
+    def step_forward(self, alpha: float, x_base: torch.Tensor, move_dir: Optional[torch.Tensor] = None,
+                     tet: Optional[DeviceTetraData] = None, move_boundary: bool = False):
+        """GIPC::step_forward (GIPC.cu:9637): tet.vertexes = x_base - alpha move_dir (default
+        ``self.moveDir``) for the free vertices, in place (the cached structs stay valid)."""
+        tet = tet or self.tet
+        d = self.moveDir if move_dir is None else move_dir
+        N.check(N.lib().sgipc_step_forward(self.ctx, _p(tet.vertexes), _p(x_base), _p(d), _p(tet.BoundaryType),
+                                           alpha, int(move_boundary), _stream()), self.ctx)
+
     def rhs(self) -> torch.Tensor:
         b = torch.empty(3 * self.n, dtype=torch.float64, device=_dev())
         N.check(N.lib().sgipc_get_rhs(self.ctx, _p(b), _stream()), self.ctx)
