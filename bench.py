@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--n", type=int, default=21, help="lattice vertices per cube edge")
     ap.add_argument("--cpu-sample", type=int, default=0, help="CPU baseline solves (0 = auto, about 10 s)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--pcg-phases", action="store_true",
+                    help="print the per-phase profile of the persistent PCG solve instead of the bench line")
     return ap.parse_args()
 
 
@@ -120,6 +122,39 @@ def cpu_solves(sc, count):
         oracle.pcg(r, c, v, sc.nv, m, b, 1e-4, single=True)
         del m
     return time.perf_counter() - t0
+
+
+def step_accuracy(g, sc, system, N, adjoint, dLdx):
+    """Errors of the timed settings against a tight FP64 solve of the same system: the
+    Newton direction dx of the mixed and FP64 solves at the r.z <= 1e-4 r0.z0 stop and at the
+    true-residual 1e-4 stop (relative to the tight dx, and mixed against FP64 at each stop),
+    and the adjoint gradients (dL/dE, dL/dv0) of the timed adjoint setting (mixed, r.z 1e-4)
+    against the adjoint of a tight FP64 solve."""
+    def rel(a, b):
+        return float((a - b).norm() / b.norm())
+
+    def solve(prec, crit, tol):
+        g.computeGradientAndHessian()
+        st = g.calculateMovingDirection(system.PCGSolverConfig(precision=prec, criterion=crit, global_tol_rate=tol,
+                                                               max_iter_ratio=1.0))
+        return g.moveDir.clone(), st
+
+    tight, st_t = solve("fp64", N.CRIT_TRUE, 1e-12)
+    out = {"reference_solve": {"precision": "fp64", "criterion": "true residual", "tol": 1e-12,
+                               "pcg_iters": st_t.iterations, "rel_residual": st_t.rel_residual}}
+    for label, crit in (("rz_1e-4", N.CRIT_RZ), ("true_1e-4", N.CRIT_TRUE)):
+        dm, sm = solve("mixed", crit, 1e-4)
+        d64, s64 = solve("fp64", crit, 1e-4)
+        out[label] = {"dx_rel_err_mixed_vs_fp64": rel(dm, d64), "dx_rel_err_mixed_vs_tight": rel(dm, tight),
+                      "dx_rel_err_fp64_vs_tight": rel(d64, tight), "rel_residual_mixed": sm.rel_residual,
+                      "rel_residual_fp64": s64.rel_residual}
+    g.computeGradientAndHessian()
+    dE, dv, _, _ = adjoint.adjoint(g, dLdx, precision="mixed", tol=1e-4, criterion=N.CRIT_RZ)
+    g.computeGradientAndHessian()
+    dE_t, dv_t, _, _ = adjoint.adjoint(g, dLdx, precision="fp64", tol=1e-12, criterion=N.CRIT_TRUE)
+    out["adjoint_mixed_rz_1e-4"] = {"dLdE_rel_err_vs_tight_fp64": rel(dE, dE_t),
+                                    "dLdv0_rel_err_vs_tight_fp64": rel(dv, dv_t)}
+    return out
 
 
 def max_over_ranks(values, world, device):
@@ -234,8 +269,29 @@ def run_ours(args):
     barrier()
     clk = clocks.stop()
 
-    t_mixed, t_fp64, t_e2e, t_adj = max_over_ranks([t_mixed, t_fp64, t_e2e, t_adj], world, "cuda")
+    # the same pair of steps stopping on the true relative residual ||b - A dx|| <= 1e-4 ||b||
+    # (a quarter of the steps: each takes about twice the iterations)
+    k_true = max(1, args.steps // 4)
+    cfg_true = {p: system.PCGSolverConfig(precision=p, criterion=N.CRIT_TRUE, max_iter_ratio=1.0)
+                for p in ("mixed", "fp64")}
+
+    def step_true(prec):
+        g.computeGradientAndHessian()
+        return g.calculateMovingDirection(cfg_true[prec])
+
+    for p in ("mixed", "fp64"):
+        step_true(p)
+    clocks2 = ClockSampler(local)
+    barrier()
+    t_mixed_true, st_mixed_true = timed(lambda: step_true("mixed"), k_true)
+    t_fp64_true, st_fp64_true = timed(lambda: step_true("fp64"), k_true)
+    barrier()
+    clk2 = clocks2.stop()
+
+    t_mixed, t_fp64, t_e2e, t_adj, t_mixed_true, t_fp64_true = max_over_ranks(
+        [t_mixed, t_fp64, t_e2e, t_adj, t_mixed_true, t_fp64_true], world, "cuda")
     units = world * args.steps
+    accuracy = step_accuracy(g, sc, system, N, adjoint, dLdx)
 
     # roofline of the dominant kernel: per-step share = avg launch time x launches per step
     step("mixed")
@@ -267,6 +323,18 @@ def run_ours(args):
                       "rel_residual_mixed": st_mixed.rel_residual, "rel_residual_fp64": st_fp64.rel_residual},
            "fp64": {"value": units / t_fp64, "unit": "solves/s", "ms_per_step": 1e3 * t_fp64 / args.steps},
            "mixed_over_fp64": t_fp64 / t_mixed,
+           "true_residual": {"criterion": "||b - A dx|| <= 1e-4 ||b||", "steps": k_true,
+                             "mixed": {"value": world * k_true / t_mixed_true, "unit": "solves/s",
+                                       "ms_per_step": 1e3 * t_mixed_true / k_true,
+                                       "pcg_iters": st_mixed_true.iterations,
+                                       "refinements": st_mixed_true.refinements,
+                                       "rel_residual": st_mixed_true.rel_residual},
+                             "fp64": {"value": world * k_true / t_fp64_true, "unit": "solves/s",
+                                      "ms_per_step": 1e3 * t_fp64_true / k_true,
+                                      "pcg_iters": st_fp64_true.iterations,
+                                      "rel_residual": st_fp64_true.rel_residual},
+                             "mixed_over_fp64": t_fp64_true / t_mixed_true, "clocks": clk2},
+           "accuracy": accuracy,
            "adjoints": {"value": units / t_adj, "unit": "adjoints/s (4 right-hand sides each)",
                         "ms_per_step": 1e3 * t_adj / args.steps},
            "e2e": {"value": units / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": host.h2d_bytes(),
@@ -325,10 +393,68 @@ def run_ours(args):
     return 0
 
 
+def phase_table(stamps, phases):
+    """Per-phase timing of one persistent solve from its barrier stamps: for every phase, the
+    critical path (the last CTA's release from the previous barrier to the last CTA's
+    arrival), the barrier latency (last arrival to last release), the mean CTA's busy time
+    and the CTA that arrived last most often."""
+    arrive, leave = stamps[:, :, 0], stamps[:, :, 1]
+    out = {}
+    for e in range(1, stamps.shape[1]):
+        name = phases[e]
+        crit = float(arrive[:, e].max() - leave[:, e - 1].max())
+        lat = float(leave[:, e].max() - arrive[:, e].max())
+        busy = float(np.mean(arrive[:, e] - leave[:, e - 1]))
+        d = out.setdefault(name, {"count": 0, "crit_ns": 0.0, "barrier_ns": 0.0, "busy_ns": 0.0, "last": {}})
+        d["count"] += 1
+        d["crit_ns"] += crit
+        d["barrier_ns"] += lat
+        d["busy_ns"] += busy
+        last = int(np.argmax(arrive[:, e]))
+        d["last"][last] = d["last"].get(last, 0) + 1
+    total = float(leave[:, -1].max() - arrive[:, 0].min())
+    table = {"total_us": total / 1e3, "grid": int(stamps.shape[0]), "barriers": int(stamps.shape[1] - 1),
+             "load_us": float(leave[:, 0].max() - arrive[:, 0].min()) / 1e3, "phases": {}}
+    for name, d in out.items():
+        n = d["count"]
+        top = max(d["last"].items(), key=lambda kv: kv[1])
+        table["phases"][name] = {"count": n, "crit_us": d["crit_ns"] / n / 1e3, "barrier_us": d["barrier_ns"] / n / 1e3,
+                                 "busy_mean_us": d["busy_ns"] / n / 1e3, "total_us": (d["crit_ns"] + d["barrier_ns"]) / 1e3,
+                                 "last_cta": top[0], "last_cta_share": top[1] / n}
+    return table
+
+
+def run_pcg_phases(args):
+    """Barrier-stamp profile of the persistent PCG solve on the workload (one GPU)."""
+    import torch
+
+    from sgipc import scenes, system
+
+    torch.cuda.set_device(0)
+    sc = scenes.scene_two_cubes(args.n, seed=1)
+    g = system.GIPC(sc, device=0, max_rhs=4)
+    out = {"workload": WORKLOAD}
+    for prec, names in (("mixed", ("pcg32", "pcg32x4")), ("fp64", ("pcg64", "pcg64x4"))):
+        g.computeGradientAndHessian()
+        g.calculateMovingDirection(system.PCGSolverConfig(precision=prec))
+        for name in names:
+            for _ in range(3):  # warm-up
+                g.profile_pcg(name)
+            reps = [phase_table(*g.profile_pcg(name)) for _ in range(5)]
+            best = min(reps, key=lambda t: t["total_us"])
+            best["total_us_all"] = [round(t["total_us"], 1) for t in reps]
+            out[name] = best
+    g.close()
+    print(json.dumps(out, indent=1))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.pcg_phases:
+        return run_pcg_phases(args)
     return run_ours(args)
 
 

@@ -386,6 +386,23 @@ SgipcStatus sgipc_launch_count(SgipcCtx* ctx, int64_t* launches);
 SgipcStatus sgipc_time_kernel(SgipcCtx* ctx, const char* name, int32_t reps, void* stream,
                               float* avg_ms, double* bytes_per_launch);
 
+/* Phase profile of one persistent PCG solve (the reference's per-phase gipc::Timer, here
+ * inside the one-kernel solve): runs one solve of the last assembled right-hand side to the
+ * 1e-4 r.z criterion ("pcg32" / "pcg64": FP32 / FP64 vectors, one right-hand side;
+ * "pcg32x4" / "pcg64x4": four copies of it interleaved, as the adjoint's batched solve) with
+ * every CTA recording the device clock (%globaltimer, ns) when it arrives at and leaves each
+ * grid barrier.  stamps [host uint64, (grid capacity) x max_epochs x 2 + max_epochs]: entry
+ * [(cta * max_epochs + e) * 2 + {0, 1}] = arrival at / departure from barrier e (e = 0: the
+ * kernel's start and the end of its shared-memory loads; later epochs past the solve's last
+ * barrier stay 0), then at [capacity * max_epochs * 2 + e] the phase that ends at barrier e
+ * (1 init, 2 MAS domain solves, 3 coarser-level solves, 4 prolongation, 5 SpMV, 6 update and
+ * restriction, 7-10 the mixed solve's refinement epilogue).  *grid receives the CTAs of the
+ * launch, *epochs the barriers recorded.  The grid capacity is 2 x the device's SM count.
+ * Allocates and frees a device buffer, and synchronises.  SGIPC_NOT_READY when the device
+ * runs the per-phase-kernel graph instead. */
+SgipcStatus sgipc_profile_pcg(SgipcCtx* ctx, const char* name, int32_t max_epochs, uint64_t* stamps,
+                              int32_t* grid, int32_t* epochs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,8 @@ def lib():
         L.or_self_step.restype = C.c_double
         L.or_ground_step.argtypes = [_d, _d, _u, C.c_int, C.c_double, C.c_double]
         L.or_ground_step.restype = C.c_double
+        L.or_accd.argtypes = [C.c_int, _d, _d, C.c_double]
+        L.or_accd.restype = C.c_double
         L.or_cfl_speed.argtypes = [_d, _u, C.c_int]
         L.or_cfl_speed.restype = C.c_double
         L.or_num_threads.restype = C.c_int
@@ -273,6 +275,13 @@ def ground_step(x, move_dir, verts, offset, slackness):
     x, move_dir = _f64(x), _f64(move_dir)
     verts = np.ascontiguousarray(verts, dtype=np.uint32)
     return lib().or_ground_step(_p(x), _p(move_dir), verts.ctypes.data_as(_u), len(verts), offset, slackness)
+
+
+def accd(edge_edge, x, d, eta):
+    """time of impact of one point-triangle (edge_edge False) or edge-edge candidate:
+    x, d the four positions and displacements (4, 3), eta the separation ratio kept"""
+    x, d = _f64(x).reshape(12), _f64(d).reshape(12)
+    return lib().or_accd(int(bool(edge_edge)), _p(x), _p(d), eta)
 
 
 def cfl_speed(move_dir, verts):

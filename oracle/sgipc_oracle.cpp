@@ -1465,6 +1465,19 @@ double or_self_step(const double* x, const double* dir, const int32_t* pairs, in
     return 1.0 / vmax;
 }
 
+// one additive-CCD time of impact: x12 / d12 the four positions and displacements (point,
+// triangle or edge, edge), eta the separation ratio kept (point_triangle_ccd /
+// edge_edge_ccd, ACCD.cu:373-535, thickness 0)
+double or_accd(int ee, const double* x12, const double* d12, double eta) {
+    ccd::V3 X[4], M[4];
+    for (int a = 0; a < 4; a++)
+        for (int k = 0; k < 3; k++) {
+            X[a].v[k] = x12[3 * a + k];
+            M[a].v[k] = d12[3 * a + k];
+        }
+    return ccd::accd(ee != 0, X, M, eta);
+}
+
 // step bound of vertices verts against the plane y = offset, normal +y
 double or_ground_step(const double* x, const double* dir, const uint32_t* verts, int n, double offset,
                       double slackness) {

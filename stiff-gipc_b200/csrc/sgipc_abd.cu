@@ -411,7 +411,7 @@ extern "C" const char* sgipc_abd_last_error(const SgipcAbdCtx* c) { return c ? c
 
 extern "C" SgipcStatus sgipc_abd_destroy(SgipcAbdCtx* c) {
     if (!c) return SGIPC_BAD_INPUT;
-    cudaSetDevice(c->device);
+    sgipc::DeviceScope dev_scope(c->device);
     void* ps[] = {c->point_body, c->body_ptr, c->bt, c->x_bar, c->dmass, c->vol, c->key, c->key_s, c->idx,
                   c->idx_s, c->val, c->flag, c->nu, c->u_row, c->u_col, c->u_val, c->pinv, c->cub_tmp,
                   c->g_rptr, c->g_cptr, c->g_tkey, c->g_tkey_s, c->g_tidx, c->g_tidx_s, c->g_vec, c->g_dot,
@@ -447,7 +447,8 @@ extern "C" SgipcStatus sgipc_abd_create(const SgipcAbdTopology* t, int device, S
         sgipc_abd_destroy(c);
         return st;
     };
-    if (cudaSetDevice(device) != cudaSuccess) return fail(SGIPC_CUDA_ERROR);
+    sgipc::DeviceScope dev_scope(device);
+    if (dev_scope.err != cudaSuccess) return fail(SGIPC_CUDA_ERROR);
     SgipcStatus st;
     if ((st = upload(c, &c->point_body, t->point_body, P)) || (st = upload(c, &c->body_ptr, ptr.data(), B + 1)) ||
         (st = upload(c, &c->bt, t->boundary_type, B)) || (st = upload(c, &c->x_bar, t->x_bar, 3 * (size_t)P)) ||
@@ -479,7 +480,8 @@ extern "C" SgipcStatus sgipc_abd_grad_hess(SgipcAbdCtx* c, const double* q, cons
         return SGIPC_CAPACITY;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    AB_CHECK(c, cudaSetDevice(c->device));
+    sgipc::DeviceScope dev_scope(c->device);
+    AB_CHECK(c, dev_scope.err);
     const int B = c->B;
     AB_CHECK(c, cudaMemsetAsync(c->flag + c->cap, 0, sizeof(int), s));  // input-error word
     int* eflag = c->flag + c->cap;
@@ -523,7 +525,8 @@ extern "C" SgipcStatus sgipc_abd_export_bcoo(SgipcAbdCtx* c, int32_t cap, int32_
                                              int32_t* count) {
     if (!c || !count) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;
-    AB_CHECK(c, cudaSetDevice(c->device));
+    sgipc::DeviceScope dev_scope(c->device);
+    AB_CHECK(c, dev_scope.err);
     AB_CHECK(c, cudaDeviceSynchronize());
     int nu = 0;
     AB_CHECK(c, cudaMemcpy(&nu, c->nu, sizeof(int), cudaMemcpyDeviceToHost));
@@ -540,7 +543,8 @@ extern "C" SgipcStatus sgipc_abd_precond_build(SgipcAbdCtx* c, void* stream) {
     if (!c) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;
     cudaStream_t s = (cudaStream_t)stream;
-    AB_CHECK(c, cudaSetDevice(c->device));
+    sgipc::DeviceScope dev_scope(c->device);
+    AB_CHECK(c, dev_scope.err);
     AB_CHECK(c, cudaMemsetAsync(c->pinv, 0, sizeof(double) * 144 * c->B, s));
     k_pfill<<<nblk(c->m_last > 0 ? c->m_last : 1), SGIPC_BLOCK, 0, s>>>(c->nu, c->u_row, c->u_col, c->u_val, c->B,
                                                                        c->pinv);
@@ -553,7 +557,8 @@ extern "C" SgipcStatus sgipc_abd_precond_build(SgipcAbdCtx* c, void* stream) {
 extern "C" SgipcStatus sgipc_abd_precond_apply(SgipcAbdCtx* c, const double* r, double* z, void* stream) {
     if (!c || !r || !z) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;
-    AB_CHECK(c, cudaSetDevice(c->device));
+    sgipc::DeviceScope dev_scope(c->device);
+    AB_CHECK(c, dev_scope.err);
     k_papply<<<nblk(12LL * c->B), SGIPC_BLOCK, 0, (cudaStream_t)stream>>>(c->B, c->pinv, r, z);
     AB_CHECK(c, cudaGetLastError());
     return SGIPC_OK;

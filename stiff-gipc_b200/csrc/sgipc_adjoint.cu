@@ -70,6 +70,7 @@ extern "C" SgipcStatus sgipc_adjoint_param_grads(SgipcCtx* c, const SgipcFemData
     if (!f->vertexes || !f->masses || !f->BoundaryType || (c->nt && (!f->DmInverses || !f->volum)))
         return SGIPC_BAD_INPUT;
     if (!(poisson > -1.0 && poisson < 0.5)) return SGIPC_BAD_INPUT;
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     const double shear = 1.0 / (2.0 * (1.0 + poisson));
     const double amu = 4.0 * shear / 3.0;

@@ -1318,7 +1318,7 @@ extern "C" SgipcStatus sgipc_assemble(SgipcCtx* c, const SgipcFemData* f, const 
     SgipcStatus st = check_inputs(c, f, k, p);
     if (st != SGIPC_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     // the MAS hierarchy of these contacts on its own stream, first (it needs the contact
     // graph only; started before the assembly kernels, it runs beside them and
     // sgipc_mas_build reuses it)
@@ -1368,6 +1368,7 @@ extern "C" SgipcStatus sgipc_barrier_grad_hess(SgipcCtx* c, const SgipcFemData* 
     SgipcStatus st = check_inputs(c, f, k, p);
     if (st != SGIPC_OK) return st;
     if (!grad || !k) return SGIPC_BAD_INPUT;
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     SgipcContacts only = *k;
     only.fric_num = 0;
@@ -1383,6 +1384,7 @@ extern "C" SgipcStatus sgipc_friction_grad_hess(SgipcCtx* c, const SgipcFemData*
     SgipcStatus st = check_inputs(c, f, k, p);
     if (st != SGIPC_OK) return st;
     if (!grad || !k) return SGIPC_BAD_INPUT;
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     SgipcContacts only = *k;
     only.pair_num = 0;
@@ -1397,6 +1399,7 @@ extern "C" SgipcStatus sgipc_fem_grad_hess(SgipcCtx* c, const SgipcFemData* f, c
     SgipcStatus st = check_inputs(c, f, nullptr, p);
     if (st != SGIPC_OK) return st;
     if (!grad) return SGIPC_BAD_INPUT;
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     if ((st = launch_fem(c, f, p, s)) != SGIPC_OK) return st;
     if ((st = gather_static(c, f, s)) != SGIPC_OK) return st;
@@ -1506,7 +1509,7 @@ extern "C" SgipcStatus sgipc_compute_energy(SgipcCtx* c, const SgipcFemData* f, 
     if (st != SGIPC_OK) return st;
     if (!energy) return SGIPC_BAD_INPUT;
     cudaStream_t s = (cudaStream_t)stream;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     if ((st = energy_launch(c, f, k, p, s, nullptr)) != SGIPC_OK) return st;
     SG_CHECK(c, cudaMemcpyAsync(c->h_en, c->en_terms, sizeof(double) * 10, cudaMemcpyDeviceToHost, s));
     SG_CHECK(c, cudaStreamSynchronize(s));

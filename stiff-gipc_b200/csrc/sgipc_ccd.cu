@@ -314,7 +314,9 @@ __global__ void k_step_forward(int nv, double* __restrict__ x, const double* __r
                                int move_boundary) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 3 * nv) return;
-    if (move_boundary || btype[i / 3] == 0) x[i] = xb[i] - alpha * dir[i];
+    // product and difference rounded separately (no fused multiply-add), as the reference's
+    // __minus(x, __s_vec_multiply(dir, alpha)) evaluates it: the trial positions are bitwise the same
+    if (move_boundary || btype[i / 3] == 0) x[i] = __dsub_rn(xb[i], __dmul_rn(dir[i], alpha));
 }
 
 }  // namespace
@@ -323,7 +325,7 @@ extern "C" SgipcStatus sgipc_step_forward(SgipcCtx* c, double* x, const double* 
                                           const int32_t* boundary_type, double alpha, int32_t move_boundary,
                                           void* stream) {
     if (!c || !x || !x_base || !move_dir || (!move_boundary && !boundary_type)) return SGIPC_BAD_INPUT;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     SG_COUNT(c, 1);
     k_step_forward<<<nblk(3LL * c->nv), SGIPC_BLOCK, 0, s>>>(c->nv, x, x_base, move_dir, boundary_type, alpha,
@@ -337,7 +339,7 @@ extern "C" SgipcStatus sgipc_self_step_size(SgipcCtx* c, const double* x, const 
                                             double* toi, void* stream) {
     if (!c || !x || !move_dir || !alpha || npairs < 0 || (npairs > 0 && !pairs)) return SGIPC_BAD_INPUT;
     if (!(slackness > 0.0 && slackness <= 1.0)) return SGIPC_BAD_INPUT;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     const int grid = std::max(1, std::min(nblk(npairs), kCcdGrid));
     k_self_step<<<grid, SGIPC_BLOCK, 0, s>>>(npairs, c->nv, (const int4*)pairs, x, move_dir, 1.0 - slackness, toi,
@@ -350,7 +352,7 @@ extern "C" SgipcStatus sgipc_ground_step_size(SgipcCtx* c, const double* x, cons
                                               double slackness, double* alpha, void* stream) {
     if (!c || !x || !move_dir || !alpha || nverts < 0 || (nverts > 0 && !verts)) return SGIPC_BAD_INPUT;
     if (!(slackness > 0.0 && slackness <= 1.0)) return SGIPC_BAD_INPUT;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     const int grid = std::max(1, std::min(nblk(nverts), kCcdGrid));
     k_ground_step<<<grid, SGIPC_BLOCK, 0, s>>>(nverts, c->nv, verts, x, move_dir, ground_offset, slackness,
@@ -361,7 +363,7 @@ extern "C" SgipcStatus sgipc_ground_step_size(SgipcCtx* c, const double* x, cons
 extern "C" SgipcStatus sgipc_cfl_largest_speed(SgipcCtx* c, const double* move_dir, const uint32_t* verts,
                                                int32_t nverts, double* speed, void* stream) {
     if (!c || !move_dir || !speed || nverts < 0 || (nverts > 0 && !verts)) return SGIPC_BAD_INPUT;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     const int grid = std::max(1, std::min(nblk(nverts), kCcdGrid));
     k_cfl_speed<<<grid, SGIPC_BLOCK, 0, s>>>(nverts, c->nv, verts, move_dir, c->ccd_part, step_finish(c, true));

@@ -192,7 +192,8 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
     SgipcCtx* c = new SgipcCtx();
     memset(c, 0, sizeof(SgipcCtx));
     c->device = device;
-    cudaError_t e = cudaSetDevice(device);
+    sgipc::DeviceScope dev_scope(device);
+    cudaError_t e = dev_scope.err;
     if (e != cudaSuccess) {
         delete c;
         return SGIPC_CUDA_ERROR;
@@ -291,7 +292,7 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
 
 extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
     if (!c) return SGIPC_OK;
-    cudaSetDevice(c->device);
+    sgipc::DeviceScope dev_scope(c->device);
     pcg_destroy(c);
     mas_destroy(c);
     void* ptrs[] = {c->row_ptr, c->col, c->slot_row, c->diag_slot, c->low_ptr, c->low_slot, c->val64, c->val32,
@@ -326,6 +327,7 @@ extern "C" const char* sgipc_last_error(const SgipcCtx* c) { return c ? c->err :
 extern "C" SgipcStatus sgipc_get_rhs(SgipcCtx* c, double* b, void* stream) {
     if (!c || !b) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;
+    SG_DEVICE(c);
     SG_CHECK(c, cudaMemcpyAsync(b, c->b, 3 * sizeof(double) * c->n, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
     return SGIPC_OK;
 }
@@ -348,6 +350,7 @@ extern "C" SgipcStatus sgipc_export_bcoo(SgipcCtx* c, int32_t cap, int32_t* rows
                                          int32_t* count) {
     if (!c || !count) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;
+    SG_DEVICE(c);
     SG_CHECK(c, cudaDeviceSynchronize());
     {
         SgipcStatus fs = check_device_flag(c, 0);

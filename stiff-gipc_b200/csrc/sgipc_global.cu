@@ -210,7 +210,7 @@ extern "C" SgipcStatus sgipc_global_pcg_solve(SgipcCtx* f, SgipcAbdCtx* a, Sgipc
         snprintf(f->err, sizeof(f->err), "global solve: assemble both systems and build both preconditioners first");
         return SGIPC_NOT_READY;
     }
-    SG_CHECK(f, cudaSetDevice(f->device));
+    SG_DEVICE(f);
     Global g{f, a, 4 * a->B, f->n, 3LL * (4LL * a->B + f->n), (cudaStream_t)stream, f->mas.built == SGIPC_FP64 + 1 ? 0 : 1};
     if (g.N > 0x7fffffffLL) return SGIPC_CAPACITY;
     if (max_iter <= 0) max_iter = (int)(0.3 * (double)g.N);

@@ -209,6 +209,9 @@ struct SgipcCtx {
     SgipcContacts mas_con;        // contacts of the last MAS build (to rebuild after timing)
     int mas_has_con;
     long long launches;           // kernels of this library launched on the context
+    // phase profile of the persistent solve (sgipc_profile_pcg; nullptr otherwise)
+    unsigned long long* stamps;
+    int stamp_epochs;
     // launch configuration of the persistent solve per (T, M, NR) instance, computed on its
     // first use (it depends on the device and the static pattern only)
     struct CoopCfg {
@@ -252,6 +255,29 @@ inline SgipcStatus cuda_fail(SgipcCtx* c, cudaError_t e, const char* what) {
         cudaError_t e_ = cudaGetLastError();                         \
         if (e_ != cudaSuccess) return sgipc::cuda_fail(ctx, e_, name); \
     } while (0)
+
+// Makes `dev` current for the rest of the scope and gives the caller's current device back
+// when the scope ends, so an entry point never leaves another device selected for its host.
+struct DeviceScope {
+    int prev = -1;
+    bool switched = false;
+    cudaError_t err;
+    explicit DeviceScope(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        err = (prev == dev) ? cudaSuccess : cudaSetDevice(dev);
+        switched = (prev != dev) && err == cudaSuccess;
+    }
+    ~DeviceScope() {
+        if (switched && prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
+#define SG_DEVICE(ctx)                                                           \
+    sgipc::DeviceScope sg_device_scope_((ctx)->device);                          \
+    if (sg_device_scope_.err != cudaSuccess)                                     \
+        return sgipc::cuda_fail(ctx, sg_device_scope_.err, "cudaSetDevice")
 
 // Vector loads.  kL2 = true reads through L2 only (ld.global.cg): required for vectors that
 // other CTAs of the same (persistent) kernel wrote, which a non-coherent L1 line could hide.

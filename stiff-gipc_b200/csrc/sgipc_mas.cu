@@ -984,7 +984,7 @@ SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec
 extern "C" SgipcStatus sgipc_mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, void* stream) {
     if (!c) return SGIPC_BAD_INPUT;
     if (con && con->pair_num > 0 && !con->pairs) return SGIPC_BAD_INPUT;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     SgipcStatus st = mas_build(c, con, prec, (cudaStream_t)stream);
     if (st == SGIPC_OK) {
         c->mas_con = con ? *con : SgipcContacts{};
@@ -1029,6 +1029,7 @@ SgipcStatus mas_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
 
 extern "C" SgipcStatus sgipc_mas_apply(SgipcCtx* c, const double* r, double* z, void* stream) {
     if (!c || !r || !z) return SGIPC_BAD_INPUT;
+    SG_DEVICE(c);
     return mas_apply_t<double>(c, r, z, c->mas.built == SGIPC_FP64 + 1 ? 0 : 1, (cudaStream_t)stream);
 }
 
@@ -1045,6 +1046,7 @@ extern "C" SgipcStatus sgipc_mas_info(SgipcCtx* c, int32_t* levelnum, int32_t* l
 extern "C" SgipcStatus sgipc_mas_export_tables(SgipcCtx* c, int32_t* table) {
     if (!c || !table) return SGIPC_BAD_INPUT;
     if (!c->mas.built) return SGIPC_NOT_READY;
+    SG_DEVICE(c);
     SG_CHECK(c, cudaDeviceSynchronize());
     SG_CHECK(c, cudaMemcpy(table, c->mas.table, sizeof(int) * (size_t)c->nv * c->mas.levelnum, cudaMemcpyDeviceToHost));
     return SGIPC_OK;
@@ -1053,6 +1055,7 @@ extern "C" SgipcStatus sgipc_mas_export_tables(SgipcCtx* c, int32_t* table) {
 extern "C" SgipcStatus sgipc_mas_export_domains(SgipcCtx* c, double* out) {
     if (!c || !out) return SGIPC_BAD_INPUT;
     if (!c->mas.built) return SGIPC_NOT_READY;
+    SG_DEVICE(c);
     SG_CHECK(c, cudaDeviceSynchronize());
     const size_t n = (size_t)(c->mas.h_info[16] / 16) * 2304;
     if (c->mas.built == SGIPC_FP64 + 1) {
@@ -1068,6 +1071,7 @@ extern "C" SgipcStatus sgipc_mas_export_domains(SgipcCtx* c, double* out) {
 extern "C" SgipcStatus sgipc_mas_restrict(SgipcCtx* c, const double* r, double* out) {
     if (!c || !r || !out) return SGIPC_BAD_INPUT;
     if (!c->mas.built) return SGIPC_NOT_READY;
+    SG_DEVICE(c);
     MasWork& m = c->mas;
     SG_CHECK(c, cudaDeviceSynchronize());
     k_restrict01<double, double><<<nblk(m.npos), SGIPC_BLOCK>>>(m.npos, r, m.part_map, m.up, m.R64);
@@ -1115,12 +1119,13 @@ extern "C" SgipcStatus sgipc_mas_apply_noalloc(SgipcCtx* c, const double* r, dou
                  SGIPC_NOALLOC_MAX_CLUSTERS);
         return SGIPC_CAPACITY;
     }
-    SG_CHECK(c, cudaSetDevice(c->device));
     if (c->device < 0 || c->device >= kNoAllocMaxDevices) {
         snprintf(c->err, sizeof(c->err), "mas_apply_noalloc: device %d beyond the %d supported", c->device,
                  kNoAllocMaxDevices);
         return SGIPC_BAD_INPUT;
     }
+    // the context's device is current until this call returns; the caller's is restored then
+    SG_DEVICE(c);
     // set-up on the first call on this device (with the device current): resolve the
     // array's device address
     void* base = nullptr;

@@ -708,6 +708,7 @@ SgipcStatus dot64(SgipcCtx* c, const double* a, const double* b, int n, double* 
 extern "C" SgipcStatus sgipc_spmv(SgipcCtx* c, const double* x, double* y, void* stream) {
     if (!c || !x || !y) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;
+    SG_DEVICE(c);
     return spmv_t<double>(c, x, y, (cudaStream_t)stream);
 }
 
@@ -835,7 +836,7 @@ extern "C" SgipcStatus sgipc_pcg_solve(SgipcCtx* c, SgipcPrecision prec, SgipcCr
                                        void* stream) {
     if (!c || !b || !x || !(tol > 0.0)) return SGIPC_BAD_INPUT;
     if (!c->assembled || !c->mas.built) return SGIPC_NOT_READY;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     // the MAS inverses must exist in the precision the solve reads
     if ((prec == SGIPC_FP64) != (c->mas.built == SGIPC_FP64 + 1)) return SGIPC_NOT_READY;
     // a contact pair with an out-of-range vertex (flagged by the assembly kernels) is
@@ -848,6 +849,7 @@ extern "C" SgipcStatus sgipc_solve(SgipcCtx* c, const SgipcContacts* con, SgipcP
                                    void* stream) {
     if (!c || !move_dir) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;
+    SG_DEVICE(c);
     SgipcStatus st = sgipc_mas_build(c, con, prec, stream);
     if (st != SGIPC_OK) return st;
     return sgipc_pcg_solve(c, prec, crit, tol, max_iter, c->b, move_dir, stats, stream);
@@ -860,6 +862,7 @@ extern "C" SgipcStatus sgipc_pcg_solve_batched(SgipcCtx* c, SgipcPrecision prec,
     if (nrhs > c->max_rhs) return SGIPC_CAPACITY;
     if (!c->assembled || !c->mas.built) return SGIPC_NOT_READY;
     if ((prec == SGIPC_FP64) != (c->mas.built == SGIPC_FP64 + 1)) return SGIPC_NOT_READY;
+    SG_DEVICE(c);
     cudaStream_t s = (cudaStream_t)stream;
     const int n3 = 3 * c->n;
     if (max_iter <= 0) max_iter = (int)(0.3 * n3);
@@ -976,8 +979,82 @@ SgipcStatus pcg_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
 
 extern "C" SgipcStatus sgipc_launch_count(SgipcCtx* c, int64_t* launches) {
     if (!c || !launches) return SGIPC_BAD_INPUT;
+    SG_DEVICE(c);
     SG_CHECK(c, cudaDeviceSynchronize());
     *launches = c->launches;
+    return SGIPC_OK;
+}
+
+namespace {
+// four copies of b interleaved ([3n][4]) for the 4-right-hand-side phase profile
+__global__ void k_replicate4(int n3, const double* __restrict__ b, double* __restrict__ bi) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n3) {
+        const double v = b[k];
+        reinterpret_cast<double2*>(bi)[2 * k] = make_double2(v, v);
+        reinterpret_cast<double2*>(bi)[2 * k + 1] = make_double2(v, v);
+    }
+}
+}  // namespace
+
+extern "C" SgipcStatus sgipc_profile_pcg(SgipcCtx* c, const char* name, int32_t max_epochs, uint64_t* stamps,
+                                         int32_t* grid, int32_t* epochs, void* stream) {
+    if (!c || !name || max_epochs < 2 || !stamps || !grid || !epochs) return SGIPC_BAD_INPUT;
+    if (!c->assembled || !c->mas.built) return SGIPC_NOT_READY;
+    const bool x4 = !strcmp(name, "pcg32x4") || !strcmp(name, "pcg64x4");
+    const bool f64 = !strcmp(name, "pcg64") || !strcmp(name, "pcg64x4");
+    if (!x4 && strcmp(name, "pcg32") && strcmp(name, "pcg64")) return SGIPC_BAD_INPUT;
+    if ((c->mas.built == SGIPC_FP64 + 1) != f64) {
+        snprintf(c->err, sizeof(c->err), "profile_pcg %s: the MAS was built in the other precision", name);
+        return SGIPC_BAD_INPUT;
+    }
+    if (x4 && c->max_rhs < 4) return SGIPC_CAPACITY;
+    SG_DEVICE(c);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int cap = c->pcg64.coop_cap > c->pcg32.coop_cap ? c->pcg64.coop_cap : c->pcg32.coop_cap;
+    const size_t words = (size_t)cap * max_epochs * 2 + max_epochs;  // stamps, then the phase tags
+    unsigned long long* d = nullptr;
+    SG_CHECK(c, cudaMalloc((void**)&d, words * sizeof(unsigned long long)));
+    SgipcStatus st = SGIPC_OK;
+    cudaError_t e = cudaMemsetAsync(d, 0, words * sizeof(unsigned long long), s);
+    const int n3 = 3 * c->n;
+    const int max_iter = n3 * 3 / 10 > 2 ? n3 * 3 / 10 : 2;
+    if (e == cudaSuccess) {
+        c->stamps = d;
+        c->stamp_epochs = max_epochs;
+        if (!x4) {
+            st = f64 ? run_pcg<double, double, 1>(c, c->pcg64, 0, c->b, 1e-4, max_iter, SGIPC_CRIT_RZ, s, 10)
+                     : run_pcg<float, float, 1>(c, c->pcg32, 1, c->b, 1e-4, max_iter, SGIPC_CRIT_RZ, s, 20);
+        } else {
+            SG_COUNT(c, 1);
+            k_replicate4<<<nblk(n3), 256, 0, s>>>(n3, c->b, c->tmp64);
+            st = f64 ? run_pcg<double, double, 4>(c, c->pcg64, 0, c->tmp64, 1e-4, max_iter, SGIPC_CRIT_RZ, s, 40)
+                     : run_pcg<float, float, 4>(c, c->pcg32, 1, c->tmp64, 1e-4, max_iter, SGIPC_CRIT_RZ, s, 42);
+        }
+        c->stamps = nullptr;
+        c->stamp_epochs = 0;
+        e = cudaStreamSynchronize(s);
+    }
+    // the grid the solve ran with: the CTAs that stamped epoch 0
+    if (st == SGIPC_OK && e == cudaSuccess)
+        e = cudaMemcpy(stamps, d, words * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (st != SGIPC_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(c, e, "profile_pcg");
+    int g = 0, ep = 0;
+    while (g < cap && stamps[(size_t)g * max_epochs * 2] != 0) g++;
+    if (g == 0) {
+        snprintf(c->err, sizeof(c->err), "profile_pcg: the solve ran as the graph of per-phase kernels");
+        return SGIPC_NOT_READY;
+    }
+    while (ep < max_epochs && stamps[(size_t)ep * 2 + 1] != 0) ep++;
+    // the launch wrote its phase tags after its own grid's stamps: move them behind the
+    // capacity's, where the caller finds them
+    if (g < cap)
+        memmove(stamps + (size_t)cap * max_epochs * 2, stamps + (size_t)g * max_epochs * 2,
+                sizeof(uint64_t) * max_epochs);
+    *grid = g;
+    *epochs = ep;
     return SGIPC_OK;
 }
 
@@ -986,7 +1063,7 @@ extern "C" SgipcStatus sgipc_time_kernel(SgipcCtx* c, const char* name, int32_t 
     if (!c || !name || reps < 1 || !avg_ms) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;
     cudaStream_t s = (cudaStream_t)stream;
-    SG_CHECK(c, cudaSetDevice(c->device));
+    SG_DEVICE(c);
     // spmv reads tmp64: give it a defined vector
     SG_CHECK(c, cudaMemsetAsync(c->tmp64, 0, sizeof(double) * 3 * c->n, s));
     SgipcStatus (*hooks[3])(SgipcCtx*, const char*, cudaStream_t, double*) = {assemble_time_hook, mas_time_hook,

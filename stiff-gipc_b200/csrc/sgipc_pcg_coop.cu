@@ -58,7 +58,44 @@ constexpr int kContactSlots = 768;  // contact entries per CTA held in shared me
 struct GridBarrier {
     unsigned int* count;  // arrivals since launch (zeroed before the launch)
     unsigned int* abort;
+    // phase profile (nullptr: off): per CTA and barrier epoch e < stamp_epochs, the
+    // %globaltimer values when the CTA arrives at barrier e and when it leaves it, at
+    // stamps[(cta * stamp_epochs + e) * 2 + {0, 1}]; epoch 0 holds the kernel's start and
+    // the end of its shared-memory loads
+    unsigned long long* stamps;
+    int stamp_epochs;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void stamp(const GridBarrier& br, unsigned int epoch, int which) {
+    if (br.stamps && epoch < (unsigned int)br.stamp_epochs)
+        br.stamps[((size_t)blockIdx.x * br.stamp_epochs + epoch) * 2 + which] = global_ns();
+}
+
+// the phase that ends at a barrier, recorded with the profile (after the stamps of all
+// gridDim.x CTAs: stamps[gridDim.x * stamp_epochs * 2 + epoch])
+enum PhaseTag : int {
+    kPhInit = 1,       // r = b, x = 0, restriction
+    kPhMas = 2,        // domain solves (levels 0..2, or 0..1)
+    kPhMasCoarse = 3,  // domain solves of the coarser levels (one- and two-level-restriction mode)
+    kPhProlong = 4,    // z = sum of the levels' Z, r.z
+    kPhSpmv = 5,       // p = z + beta p, Ap, p.Ap
+    kPhUpdate = 6,     // x, r, restriction, r.r
+    kPhAcc64 = 7,      // refinement: x64 += x
+    kPhRes64 = 8,      // refinement: r64 = b64 - A x64
+    kPhRestr64 = 9,    // refinement: restriction of r64
+    kPhProlong64 = 10  // refinement: r64 . M r64
+};
+
+__device__ __forceinline__ void tag_phase(const GridBarrier& br, unsigned int epoch, int tag) {
+    if (br.stamps && blockIdx.x == 0 && epoch < (unsigned int)br.stamp_epochs)
+        br.stamps[(size_t)gridDim.x * br.stamp_epochs * 2 + epoch] = (unsigned long long)tag;
+}
 
 template <class T, class M, int NR>
 struct CoopArgs {
@@ -114,11 +151,13 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
 }
 
 // Grid barrier number `epoch` (1, 2, ...).  All threads of every CTA call it.
-__device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch) {
+__device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch, int tag) {
     __shared__ int s_ok;
     __syncthreads();  // the CTA's writes of this phase precede thread 0's release
     if (threadIdx.x == 0) {
         const unsigned int target = epoch * gridDim.x;
+        stamp(br, epoch, 0);
+        tag_phase(br, epoch, tag);
         red_add_release_gpu(br.count, 1u);
         int ok = 1;
         for (long long k = 0;; k++) {
@@ -137,6 +176,7 @@ __device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch) {
         // gpu-scope fence after the acquire: the SM's L1 holds no line older than the
         // barrier, so the CTA may read other CTAs' writes with ordinary (L1-cached) loads
         __threadfence();
+        stamp(br, epoch, 1);
         s_ok = ok;
     }
     __syncthreads();
@@ -147,7 +187,7 @@ __device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch) {
 // grid total in every thread.  The partial buffer of parity epoch & 1 is rewritten two
 // barriers later at the earliest, after every CTA has read it.
 template <int NR>
-__device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, double (&v)[NR], double* partial,
+__device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, int tag, double (&v)[NR], double* partial,
                             double* smem, double (&out)[NR]) {
     __shared__ double s_tot[NR];
     double* part = partial + (size_t)(epoch & 1) * NR * gridDim.x;
@@ -155,7 +195,7 @@ __device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, double (&
     if (threadIdx.x == 0)
 #pragma unroll
         for (int r = 0; r < NR; r++) part[r * gridDim.x + blockIdx.x] = v[r];
-    const bool ok = grid_barrier(br, epoch);
+    const bool ok = grid_barrier(br, epoch, tag);
     if (threadIdx.x < 32) {
         // warp 0 adds the partials (fixed lane assignment and shuffle tree: the same total
         // in every CTA)
@@ -331,11 +371,11 @@ __device__ bool phase_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], unsigne
         } else {
             solve_domain_range<M, NR>(a.inv, a.R, a.Z, 0, a.nd2, 0, L > 3 ? G - 1 : G, sR, dcache, ndc);
         }
-        return grid_barrier(a.br, ++epoch);
+        return grid_barrier(a.br, ++epoch, kPhMas);
     }
     if (L > 2) restrict_level1<M, NR>(a.mv, a.R);
     solve_domain_range<M, NR>(a.inv, a.R, a.Z, 0, a.nd01, 0, G, sR, dcache, ndc);
-    if (!grid_barrier(a.br, ++epoch)) return false;
+    if (!grid_barrier(a.br, ++epoch, kPhMas)) return false;
     if (L <= 2) return true;
     if (blockIdx.x == 0) {
         restrict_coarse_cta<M, NR, true>(a.mv.info, a.mv.up, L, a.R, 2);
@@ -345,7 +385,7 @@ __device__ bool phase_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], unsigne
         solve_domain_range<M, NR>(a.inv, a.R, a.Z, a.nd01, a.nd2, 1, G - 1, sR);
     else
         solve_domain_range<M, NR>(a.inv, a.R, a.Z, a.nd01, a.nd2, 0, 1, sR);
-    return grid_barrier(a.br, ++epoch);
+    return grid_barrier(a.br, ++epoch, kPhMasCoarse);
 }
 
 // z = sum over levels of Z at the vertex's clusters; r.z
@@ -770,6 +810,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
     __shared__ __align__(16) M sR[kDomPerCta][48 * NR];
     extern __shared__ __align__(16) unsigned char dsm[];
     unsigned int epoch = 0;
+    if (threadIdx.x == 0) stamp(a.br, 0, 0);
 
     // ---- shared-memory residency of this CTA's static rows and level-0/1 domain inverses
     // (constant for the whole solve): loaded once, read every iteration
@@ -826,6 +867,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
         }
         if (threadIdx.x == 0) rcs = rc;
         __syncthreads();
+        if (threadIdx.x == 0) stamp(a.br, 0, 1);
     }
     // Per right-hand-side state in shared memory: thread 0 updates it from the grid totals
     // (identical in every CTA) after each reduction, the CTA reads it after a __syncthreads.
@@ -852,7 +894,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
         phase_positions_l2<T, M, NR, 1>(a, S.alpha, nullptr, nullptr, rcur, S.run, v, s_l1);
     else
         phase_init(a, v);
-    bool ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);  // starts with __syncthreads
+    bool ok = grid_reduce<NR>(a.br, ++epoch, kPhInit, v, a.partial, smem, t);  // starts with __syncthreads
     if (threadIdx.x == 0)
 #pragma unroll
         for (int r = 0; r < NR; r++) S.bn2[r] = t[r];
@@ -861,7 +903,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
         phase_prolong(a, rcur, S.run, v);
-        ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);
+        ok = grid_reduce<NR>(a.br, ++epoch, kPhProlong, v, a.partial, smem, t);
     }
     if (threadIdx.x == 0)
 #pragma unroll
@@ -886,7 +928,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
         phase_spmv(a, k == 1, S.beta, pold, pnew, S.run, v, rcs);
-        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t))) break;
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, kPhSpmv, v, a.partial, smem, t))) break;
         if (threadIdx.x == 0)
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -915,7 +957,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
         } else {
             phase_update(a, S.alpha, pnew, S.run, v);
         }
-        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t))) break;
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, kPhUpdate, v, a.partial, smem, t))) break;
         if (threadIdx.x == 0)
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -932,7 +974,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = 0.0;
         phase_prolong(a, rcur, S.run, v);
-        if (!(ok = grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t))) break;
+        if (!(ok = grid_reduce<NR>(a.br, ++epoch, kPhProlong, v, a.partial, smem, t))) break;
         if (threadIdx.x == 0)
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -947,18 +989,18 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
         if (ok && a.x64 && a.l2mode) {
             // x64 += x; r64 = b64 - A x64; r64 . r64; M r64 (FP32 MAS); r64 . M r64
             phase_accumulate64(a);
-            ok = grid_barrier(a.br, ++epoch);
+            ok = grid_barrier(a.br, ++epoch, kPhAcc64);
             v[0] = 0.0;
             if (ok) phase_residual64(a, v[0]);
-            ok = ok && grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);
+            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhRes64, v, a.partial, smem, t);
             rr_ref = t[0];
             v[0] = 0.0;
             if (ok) phase_positions_l2<T, M, NR, 2>(a, S.alpha, nullptr, nullptr, nullptr, S.run, v, s_l1);
-            ok = ok && grid_barrier(a.br, ++epoch);
+            ok = ok && grid_barrier(a.br, ++epoch, kPhRestr64);
             ok = ok && phase_mas(a, sR, epoch, dcache, ndc);
             v[0] = 0.0;
             if (ok) phase_prolong_ref(a, v[0]);
-            ok = ok && grid_reduce<NR>(a.br, ++epoch, v, a.partial, smem, t);
+            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhProlong64, v, a.partial, smem, t);
             rz_ref = t[0];
         }
     }
@@ -1084,7 +1126,7 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     a.Ap = (T*)w.Ap;
     a.sc = w.sc;
     a.partial = w.coop;
-    a.br = {w.ticket + 4, w.ticket + 5};
+    a.br = {w.ticket + 4, w.ticket + 5, c->stamps, c->stamp_epochs};
     a.nv = c->nv;
     a.ndom = ndom;
     a.nd01 = nd01;

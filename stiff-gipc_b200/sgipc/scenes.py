@@ -381,6 +381,16 @@ def suggest_kappa(bbox_diag2: float, dhat: float, mean_mass: float, min_kappa_co
 # scene assembly
 # ----------------------------------------------------------------------------------------
 
+def inertial_target(x_prev, vel, btype, dt, apply_gravity=None):
+    """``xTilta = x_prev + (dt v + dt^2 g)``, gravity on free vertices that take it
+    (``_computeXTilta``, StiffGIPC/GIPC.cu:8073-8096; ``apply_gravity`` all ones when None)."""
+    g = np.asarray(GRAVITY) * (dt * dt)
+    on = np.asarray(btype) == 0
+    if apply_gravity is not None:
+        on &= np.asarray(apply_gravity) != 0
+    return x_prev + (vel * dt + np.where(on[:, None], g[None, :], 0.0))
+
+
 def _empty_cloth():
     return dict(tris=np.zeros((0, 3), np.int32), tri_dm_inv=np.zeros((0, 2, 2)),
                 area=np.zeros(0), hinges=np.zeros((0, 2), np.int32),
@@ -454,7 +464,7 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
     x_prev = rest + rng.uniform(-perturb, perturb, rest.shape)
     x = x_prev.copy()
     g = np.asarray(GRAVITY)
-    xt = x_prev + dt * vel + np.where(btype[:, None] == 0, dt * dt * g[None, :], 0.0)
+    xt = inertial_target(x_prev, vel, btype, dt)
 
     stris, sedges, sverts = tet_surface(tets) if len(tets) else (np.zeros((0, 3), np.int32),
                                                                  np.zeros((0, 2), np.int32), np.zeros(0, np.int32))

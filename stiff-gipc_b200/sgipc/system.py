@@ -301,6 +301,24 @@ class GIPC:
                 self.ctx)
         return float(ms.value), float(by.value)
 
+    PHASES = {1: "init", 2: "mas", 3: "mas_coarse", 4: "prolong", 5: "spmv", 6: "update", 7: "acc64",
+              8: "res64", 9: "restrict64", 10: "prolong64"}
+
+    def profile_pcg(self, name: str = "pcg32", max_epochs: int = 1024):
+        """Barrier stamps of one persistent PCG solve (``sgipc_profile_pcg``): (stamps, phases)
+        with stamps an int64 array [grid, epochs, 2] of device-clock nanoseconds, arrival at and
+        departure from every grid barrier per CTA (epoch 0: kernel start, end of its
+        shared-memory loads), and phases[e] the name of the phase that ends at barrier e."""
+        nsm = torch.cuda.get_device_properties(_dev()).multi_processor_count
+        cap = 2 * nsm
+        buf = np.zeros(cap * max_epochs * 2 + max_epochs, np.uint64)
+        grid, ep = C.c_int32(), C.c_int32()
+        N.check(N.lib().sgipc_profile_pcg(self.ctx, name.encode(), max_epochs, buf.ctypes.data_as(C.c_void_p),
+                                          C.byref(grid), C.byref(ep), _stream()), self.ctx)
+        st = buf[:cap * max_epochs * 2].reshape(cap, max_epochs, 2)[:grid.value, :ep.value].astype(np.int64)
+        tags = buf[cap * max_epochs * 2:][:ep.value]
+        return st, ["start"] + [self.PHASES.get(int(t), "?") for t in tags[1:]]
+
     def spmv(self, x: torch.Tensor) -> torch.Tensor:
         y = torch.empty_like(x)
         N.check(N.lib().sgipc_spmv(self.ctx, _p(x), _p(y), _stream()), self.ctx)

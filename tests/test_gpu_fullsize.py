@@ -1,6 +1,8 @@
 """The bench workload at full size (two stacked 21^3 cubes, 18 522 vertices, 80 000 tets,
-contacts) through size-independent properties; the oracle covers the same code paths on the
-smaller parity scenes.
+contacts): against the oracle (the CPU restatement finishes this size in about a second:
+assembled blocks and right-hand side 1e-9 of the largest entry, MAS tables identical and
+domain inverses 1e-9, the FP64 solve's iteration count within one of the oracle's and its
+solution 1e-6), and through size-independent properties.
 
 Tolerances: SpMV and FP64 MAS symmetry 1e-12 / 1e-10 relative to |u||A v|; reported relative
 residual within 1e-6 of one recomputed with the library's FP64 SpMV; persistent vs graph
@@ -9,6 +11,8 @@ a 4-RHS batch within its tolerance and 1e-8 of the single-RHS solve.
 """
 import numpy as np
 import pytest
+
+import oracle
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -35,6 +39,45 @@ def _rel(a, b):
 
 def _residual(g, b, x):
     return float((b - g.spmv(x)).norm() / b.norm())
+
+
+@pytest.fixture(scope="module")
+def c2_oracle(c2):
+    sc, _ = c2
+    ob, orow, ocol, oval, _ = oracle.assemble(sc)
+    return ob, orow, ocol, oval
+
+
+def test_fullsize_assembly_matches_oracle(c2, c2_oracle):
+    sc, g = c2
+    ob, orow, ocol, oval = c2_oracle
+    rows, cols, vals = g.export_bcoo()
+    assert np.array_equal(rows, orow) and np.array_equal(cols, ocol)
+    assert np.abs(vals - oval).max() < 1e-9 * np.abs(oval).max()
+    b = g.rhs().cpu().numpy()
+    assert np.abs(b - ob).max() < 1e-9 * np.abs(ob).max()
+
+
+def test_fullsize_mas_and_fp64_solve_match_oracle(c2, c2_oracle):
+    sc, g = c2
+    ob, orow, ocol, oval = c2_oracle
+    g.computeGradientAndHessian()
+    mas = system.MASPreconditioner(g)
+    mas.setPreconditioner("fp64")
+    om = oracle.Mas(sc, orow, ocol, oval)
+    L, _, counts, total = om.info()
+    gl, gcounts, gtotal = mas.info()
+    assert gl == L and gtotal == total and np.array_equal(gcounts, counts)
+    assert np.array_equal(mas.tables(), om.table())
+    gd, od = mas.domains(), om.domains()
+    assert np.abs(gd - od).max(axis=(1, 2)).max() < 1e-9 * np.abs(od).max()
+    ox, oit, orz0, _ = oracle.pcg(orow, ocol, oval, sc.nv, om, ob, 1e-4)
+    x, st = system.PCGSolver(g, system.PCGSolverConfig(precision="fp64")).solve(g.rhs())
+    assert st.status == N.OK and abs(st.iterations - oit) <= 1, (st.iterations, oit)
+    assert abs(st.rz0 - orz0) <= 1e-9 * abs(orz0)
+    if st.iterations == oit:
+        x = x.cpu().numpy()
+        assert np.linalg.norm(x - ox) / np.linalg.norm(ox) < 1e-6
 
 
 def test_fullsize_operators_are_symmetric_and_positive(c2):

@@ -9,6 +9,7 @@ Tolerances (FP64 unless stated):
   * PCG: same iteration count within 1, solution within 1e-6 relative of the oracle's.
 """
 import ctypes
+import os
 
 import numpy as np
 import pytest
@@ -36,9 +37,19 @@ def _soft_cube():
     return sc
 
 
-@pytest.fixture(scope="module", params=["c1_cube", "cube_touch", "two_cubes", "cloth_on_cube", "cube_soft"])
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module", params=["c1_cube", "cube_touch", "two_cubes", "cloth_on_cube", "cube_soft",
+                                        "cubes_dirichlet"])
 def case(request):
-    if request.param == "cube_soft":
+    if request.param == "cubes_dirichlet":
+        # two 4^3 cubes with Dirichlet vertices (every ninth), soft constraints, ground and
+        # pair friction at a moved iterate (the scene of the reference golden vectors):
+        # Dirichlet rows and columns zeroed, mass diagonal kept (GIPC.cu:10295-10336)
+        sc = scenes.Scene.load(os.path.join(GOLDEN, "scene_two_cubes4.npz"))
+        assert (sc.boundary_type != 0).any()
+    elif request.param == "cube_soft":
         sc = _soft_cube()
     elif request.param == "c1_cube":
         # the smallest workload: an 11^3 cube 0.05 m above the ground, no contact yet
