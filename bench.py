@@ -31,6 +31,8 @@ METRIC = "Newton-system solves/s, mixed vs FP64 MAS-PCG at 1e-4 residual; adjoin
 WORKLOAD = ("two stacked soft cubes, 2 x 21^3 lattice (80000 tets, 18522 vertices), E 1e5/1e6 Pa, nu 0.45, "
             "mu 0.2, d-hat 1e-3 m; one Newton system = assembly + MAS build + PCG to r.z <= 1e-4 r0.z0")
 L2_FLUSH_BYTES = 256 << 20
+CPU_SOLVER = ("Eigen unavailable: the oracle's OpenMP restatement of the reference's assembly and "
+              "MAS-preconditioned CG (FP64 vectors, FP32 MAS inverses), not an Eigen ConjugateGradient")
 
 
 def parse():
@@ -44,6 +46,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--pcg-phases", action="store_true",
                     help="print the per-phase profile of the persistent PCG solve instead of the bench line")
+    ap.add_argument("--kernel", default=None,
+                    help="only re-launch this hot kernel (sgipc_time_kernel names) on the workload and print its "
+                         "time: the launch an ncu capture of the roofline kernel should see")
     return ap.parse_args()
 
 
@@ -192,7 +197,7 @@ def run_reference(args):
            "config": {"workload": WORKLOAD, "solver": "reference PCG, FP64 matrix/vectors, FP32 MAS inverses"},
            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
                             "sample": "%d full Newton systems of the workload (assembly + MAS + PCG), %d OpenMP threads"
-                                      % (args.steps, oracle.num_threads())},
+                                      % (args.steps, oracle.num_threads()), "solver": CPU_SOLVER},
            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -384,7 +389,8 @@ def run_ours(args):
             nsol = max(1, min(20, int(10.0 / max(one, 1e-3))))
         t_cpu = cpu_solves(sc, nsol)
         out["cpu_baseline"] = {"value": nsol / t_cpu, "unit": "solves/s", "cores": oracle.num_threads(),
-                               "kind": "port", "sample": "%d full Newton systems of the workload" % nsol}
+                               "kind": "port", "sample": "%d full Newton systems of the workload" % nsol,
+                               "solver": CPU_SOLVER}
     g.close()
     if world > 1:
         dist.destroy_process_group()
@@ -449,12 +455,33 @@ def run_pcg_phases(args):
     return 0
 
 
+def run_kernel_only(args):
+    """Assemble the workload, build the MAS in the precision the kernel reads, then time the
+    named kernel with sgipc_time_kernel (one untimed launch, then args.steps timed ones)."""
+    import torch
+
+    from sgipc import scenes, system
+
+    torch.cuda.set_device(0)
+    sc = scenes.scene_two_cubes(args.n, seed=1)
+    g = system.GIPC(sc, device=0, max_rhs=4)
+    g.computeGradientAndHessian()
+    system.MASPreconditioner(g).setPreconditioner("fp64" if args.kernel in ("pcg64", "mas_domain64") else "mixed")
+    ms, by = g.time_kernel(args.kernel, args.steps)
+    g.close()
+    print(json.dumps({"kernel": args.kernel, "launches": args.steps + 1, "avg_ms": ms, "bytes_per_launch": by,
+                      "achieved_GBs": by / (ms * 1e-3) / 1e9}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.pcg_phases:
         return run_pcg_phases(args)
+    if args.kernel:
+        return run_kernel_only(args)
     return run_ours(args)
 
 

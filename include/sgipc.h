@@ -149,6 +149,13 @@ SgipcStatus sgipc_destroy(SgipcCtx* ctx);
 const char* sgipc_status_string(SgipcStatus s);
 /* Last CUDA error text recorded on the context (empty if none). */
 const char* sgipc_last_error(const SgipcCtx* ctx);
+/* How long a grid-barrier wait inside the persistent PCG solve and the one-launch MAS
+ * hierarchy build may last, in polls of the arrival counter (0 = the defaults, about 2 s;
+ * new; the reference synchronises on the host and has no device waits).  A wait that runs
+ * out raises the kernel's abort word, every CTA leaves, and the call returns
+ * SGIPC_CUDA_ERROR with a message, the context staying usable.  A watchdog for hosts that
+ * must bound a call's time; 1 makes nearly every wait run out. */
+SgipcStatus sgipc_set_wait_limit(SgipcCtx* ctx, int64_t polls);
 
 /* ---- assembly (GIPC::computeGradientAndHessian, StiffGIPC/GIPC.cu:10110-10344) -------- */
 

@@ -324,6 +324,12 @@ extern "C" const char* sgipc_status_string(SgipcStatus s) {
 
 extern "C" const char* sgipc_last_error(const SgipcCtx* c) { return c ? c->err : ""; }
 
+extern "C" SgipcStatus sgipc_set_wait_limit(SgipcCtx* c, int64_t polls) {
+    if (!c || polls < 0) return SGIPC_BAD_INPUT;
+    c->wait_limit = polls;
+    return SGIPC_OK;
+}
+
 extern "C" SgipcStatus sgipc_get_rhs(SgipcCtx* c, double* b, void* stream) {
     if (!c || !b) return SGIPC_BAD_INPUT;
     if (!c->assembled) return SGIPC_NOT_READY;

@@ -209,6 +209,9 @@ struct SgipcCtx {
     SgipcContacts mas_con;        // contacts of the last MAS build (to rebuild after timing)
     int mas_has_con;
     long long launches;           // kernels of this library launched on the context
+    // polls a grid-barrier wait of the persistent solve or the hierarchy build makes before
+    // it gives up (0: the kernels' defaults, about 2 s); sgipc_set_wait_limit
+    long long wait_limit;
     // phase profile of the persistent solve (sgipc_profile_pcg; nullptr otherwise)
     unsigned long long* stamps;
     int stamp_epochs;

@@ -537,9 +537,10 @@ struct HierArgs {
     int* part;      // [gridDim.x] chunk totals of the scan (bank_off's tail beyond the banks)
     int* l1_first;
     int* l1_last;
+    long long spin_limit;  // polls of a barrier wait before the build gives up
 };
 
-__device__ bool hier_barrier(int* info, unsigned int& epoch) {
+__device__ bool hier_barrier(int* info, unsigned int& epoch, long long limit) {
     __shared__ int s_ok;
     __syncthreads();
     epoch++;
@@ -556,7 +557,7 @@ __device__ bool hier_barrier(int* info, unsigned int& epoch) {
                 ok = 0;
                 break;
             }
-            if (k > kHierSpinLimit) {
+            if (k > limit) {
                 atomicExch(reinterpret_cast<unsigned int*>(info + 21), 1u);
                 ok = 0;
                 break;
@@ -593,12 +594,12 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
             h.table[(size_t)v * h.L] = p;
         }
     }
-    if (!hier_barrier(info, epoch)) return;
+    if (!hier_barrier(info, epoch, h.spin_limit)) return;
     for (int l = 0; l + 1 < h.L; l++) {
         const int count = info[8 + l], start = info[l];
         const int nbank = (count + 15) >> 4;
         for (int k = tid; k < count; k += nth) h.mask[k] = 0u;
-        if (!hier_barrier(info, epoch)) return;
+        if (!hier_barrier(info, epoch, h.spin_limit)) return;
         // edge masks (one lane per neighbour slot) and contact-pair masks, warp-aggregated
         for (int k0 = gw * 32; k0 < h.nnbr; k0 += nw * 32) {
             const int k = k0 + lane;
@@ -613,11 +614,11 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
         }
         for (int p0 = gw * 32; p0 < h.npairs; p0 += nw * 32)
             mask_pair_warp(p0 + lane < h.npairs ? h.pairs + p0 + lane : nullptr, h.nv, h.node, h.mask);
-        if (!hier_barrier(info, epoch)) return;
+        if (!hier_barrier(info, epoch, h.spin_limit)) return;
         // components, half a warp per bank; bank nbank gets a zero count (the scan's total)
         for (int b0 = gw * 2; b0 <= nbank; b0 += nw * 2)
             bank_components_half(b0 + (lane >> 4), nbank, count, l, h.mask, h.part_map, h.rank, h.bank_cnt);
-        if (!hier_barrier(info, epoch)) return;
+        if (!hier_barrier(info, epoch, h.spin_limit)) return;
         // exclusive scan of bank_cnt[0 .. nbank]: per CTA a chunk, then the chunk offsets
         const int n1 = nbank + 1, cs = (n1 + gridDim.x - 1) / gridDim.x;
         const int c0 = min(n1, (int)blockIdx.x * cs), c1 = min(n1, c0 + cs);
@@ -634,7 +635,7 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
             __syncthreads();
         }
         if (threadIdx.x == 0) h.part[blockIdx.x] = s_carry;
-        if (!hier_barrier(info, epoch)) return;
+        if (!hier_barrier(info, epoch, h.spin_limit)) return;
         if (threadIdx.x < 32) {
             int o = 0;
             for (int k = threadIdx.x; k < (int)blockIdx.x; k += 32) o += h.part[k];
@@ -644,7 +645,7 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
         }
         __syncthreads();
         for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) h.bank_off[i] += s_carry;
-        if (!hier_barrier(info, epoch)) return;
+        if (!hier_barrier(info, epoch, h.spin_limit)) return;
         // assignment of the next level's ids
         const int start_next = start + ((count + 15) & ~15);
         if (tid == 0) {
@@ -660,7 +661,7 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
             h.up[start + a] = start_next + nn;  // every vertex of node a writes the same parent
             if (l + 2 == h.L) h.up[start_next + nn] = -1;
         }
-        if (!hier_barrier(info, epoch)) return;
+        if (!hier_barrier(info, epoch, h.spin_limit)) return;
     }
     if (h.L >= 3) {
         const int nb0 = h.npos >> 4;
@@ -668,7 +669,7 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
             h.l1_first[k] = 0x7f7f7f7f;
             h.l1_last[k] = -1;
         }
-        if (!hier_barrier(info, epoch)) return;
+        if (!hier_barrier(info, epoch, h.spin_limit)) return;
         const int start1 = info[1];
         for (int b = tid; b < nb0; b += nth) {
             int lo = 0x7fffffff, hi = -1;
@@ -844,6 +845,7 @@ static SgipcStatus mas_hierarchy(SgipcCtx* c, const SgipcContacts* con, cudaStre
         h.part = m.hier_part;
         h.l1_first = m.l1_first;
         h.l1_last = m.l1_last;
+        h.spin_limit = c->wait_limit > 0 ? c->wait_limit : kHierSpinLimit;
         SG_CHECK(c, cudaMemsetAsync(m.info + 20, 0, 2 * sizeof(int), s));
         void* args[] = {&h};
         SG_COUNT(c, 1);

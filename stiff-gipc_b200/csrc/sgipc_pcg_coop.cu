@@ -58,6 +58,7 @@ constexpr int kContactSlots = 768;  // contact entries per CTA held in shared me
 struct GridBarrier {
     unsigned int* count;  // arrivals since launch (zeroed before the launch)
     unsigned int* abort;
+    long long spin_limit;  // polls of one wait before the solve gives up
     // phase profile (nullptr: off): per CTA and barrier epoch e < stamp_epochs, the
     // %globaltimer values when the CTA arrives at barrier e and when it leaves it, at
     // stamps[(cta * stamp_epochs + e) * 2 + {0, 1}]; epoch 0 holds the kernel's start and
@@ -166,7 +167,7 @@ __device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch, int tag)
                 ok = 0;
                 break;
             }
-            if (k > kSpinLimit) {
+            if (k > br.spin_limit) {
                 atomicExch(br.abort, 1u);
                 ok = 0;
                 break;
@@ -1126,7 +1127,7 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     a.Ap = (T*)w.Ap;
     a.sc = w.sc;
     a.partial = w.coop;
-    a.br = {w.ticket + 4, w.ticket + 5, c->stamps, c->stamp_epochs};
+    a.br = {w.ticket + 4, w.ticket + 5, c->wait_limit > 0 ? c->wait_limit : kSpinLimit, c->stamps, c->stamp_epochs};
     a.nv = c->nv;
     a.ndom = ndom;
     a.nd01 = nd01;

@@ -105,6 +105,7 @@ SIGNATURES = {
                                _i32),
     "sgipc_launch_count": ([_vp, C.POINTER(C.c_int64)], _i32),
     "sgipc_time_kernel": ([_vp, C.c_char_p, _i32, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)], _i32),
+    "sgipc_set_wait_limit": ([_vp, C.c_int64], _i32),
     "sgipc_profile_pcg": ([_vp, C.c_char_p, _i32, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _vp], _i32),
 }
 

@@ -334,3 +334,23 @@ def test_bad_inputs_are_reported(case):
     st = g.calculateMovingDirection(system.PCGSolverConfig(precision="fp64"))
     assert st.status == N.OK
     torch.cuda.synchronize()
+
+
+def test_phase_profile_of_the_persistent_solve(case):
+    """sgipc_profile_pcg: every CTA stamps every barrier of one solve in order (arrival
+    before departure, departure before the next arrival), the phases follow the solve's
+    structure, and the profiled solve takes the iterations of an ordinary one."""
+    sc, g, _ = case
+    mas = system.MASPreconditioner(g)
+    mas.setPreconditioner("fp64")
+    _, st = system.PCGSolver(g, system.PCGSolverConfig(precision="fp64")).solve(g.rhs())
+    stamps, phases = g.profile_pcg("pcg64")
+    grid, epochs = stamps.shape[0], stamps.shape[1]
+    assert grid >= 1 and epochs >= 3
+    assert (stamps[:, :, 1] >= stamps[:, :, 0]).all()
+    assert (stamps[:, 1:, 0] >= stamps[:, :-1, 1]).all()
+    assert phases[0] == "start" and phases[1] == "init" and "?" not in phases
+    assert phases.count("spmv") == st.iterations
+    mas.setPreconditioner("mixed")
+    stamps4, phases4 = g.profile_pcg("pcg32x4")
+    assert phases4.count("spmv") >= 1 and (stamps4[:, :, 1] >= stamps4[:, :, 0]).all()
