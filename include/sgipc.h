@@ -374,6 +374,58 @@ SgipcStatus sgipc_global_pcg_solve(SgipcCtx* fem, SgipcAbdCtx* abd, SgipcCriteri
                                    int32_t max_iter, const double* b, double* x, double* abd_point_dx,
                                    SgipcSolveStats* stats, void* stream);
 
+/* ---- contact pairs and the lagged friction set-up -------------------------------------- */
+
+/* Collision surface [dev]: the surface points, triangles (uint3) and edges (uint2) the
+ * contact-pair search reads (GIPC's _surfVerts, bvh_f._faces, bvh_e._edges).  Every vertex
+ * of a triangle or an edge must be a surface point. */
+typedef struct SgipcSurface {
+    const uint32_t* surf_verts;
+    int32_t         surf_vert_num;
+    const uint32_t* faces;
+    int32_t         face_num;
+    const uint32_t* edges;
+    int32_t         edge_num;
+} SgipcSurface;
+
+/* GIPC::buildCP (GIPC.cu:9065-9083: the LBVH queries _selfQuery_vf / _selfQuery_ee with
+ * _checkPTintersection / _checkEEintersection, mlbvh.cu:534-1059, 1306-1742, and
+ * _GroundCollisionDetect GIPC.cu:6433): every surface point within sqrt(dHat) of a triangle
+ * and every edge pair within it, at positions x [dev double3[V]], mollifier thresholds from
+ * rest [dev double3[V]].  A pair is tested when its vertices belong to different bodies or
+ * the body id is -1 (body_id [dev int[V]]; -1 everywhere collides every body with itself),
+ * shares no vertex, and not all of its vertices have boundary type >= 2 (boundary_type [dev
+ * int[V]], may be null).  Writes [dev] pairs int4[cap] in the reference encoding, ccd_pairs
+ * int4[cap] (the point with the whole triangle, or the two edges), mat_index int[cap] (rank
+ * among the pairs of the same size), cp_num uint[5] (total, 0, two-, three-, four-vertex
+ * pairs), ground_pairs uint[ground_cap] (surface points with (y - ground_offset)^2 <= dHat,
+ * normal +y) and gp_num uint[1]; h_cp_num [host uint[5]] and h_gp_num [host] receive the
+ * counts, as the reference copies h_cpNum / h_gpNum.  The order is deterministic:
+ * point-triangle pairs by surface point then triangle, then edge-edge pairs by edge then
+ * other edge.  SGIPC_CAPACITY (counts reported, pairs unwritten) when cap or ground_cap is
+ * too small; cap must stay below 2^21.  Synchronises the stream. */
+SgipcStatus sgipc_build_cp(SgipcCtx* ctx, const double* x, const double* rest, const SgipcSurface* surf,
+                           const int32_t* body_id, const int32_t* boundary_type, double dHat, double ground_offset,
+                           int32_t cap, int32_t* pairs, int32_t* ccd_pairs, int32_t* mat_index, uint32_t* cp_num,
+                           int32_t ground_cap, uint32_t* ground_pairs, uint32_t* gp_num, uint32_t* h_cp_num,
+                           uint32_t* h_gp_num, void* stream);
+
+/* The lagged friction set-up of a frame (_calFrictionLastH_DistAndTan / _calFrictionLastH_gd,
+ * GIPC.cu:8362-8499, called from GIPC.cu:8660-8696), at the frame's positions x [dev]: for
+ * every pair [dev int4[pair_num]] that is not mollified, in input order, the pair, its lagged
+ * normal force, closest-point coordinates (double2) and tangent basis (3 x 2 row-major) into
+ * fric_pairs / fric_lambda / fric_coord / fric_basis [dev, pair_num entries at most];
+ * cp_num_last [dev uint[5]] = (kept pairs, 0, point-point, point-edge, point-triangle and
+ * edge-edge); and for the ground pairs [dev uint[ground_num]] their vertices and normal forces
+ * (fric_gd_pairs, fric_gd_lambda).  A pair or ground pair naming a vertex outside the mesh is
+ * left out and sets cp_num_last[1].  h_cp_num_last [host uint[5], may be null] receives the
+ * counts (then the call synchronises the stream, and returns SGIPC_BAD_INPUT for such a pair). */
+SgipcStatus sgipc_friction_setup(SgipcCtx* ctx, const double* x, const int32_t* pairs, int32_t pair_num,
+                                 const uint32_t* ground_pairs, int32_t ground_num, double dHat, double kappa,
+                                 double ground_offset, int32_t* fric_pairs, double* fric_lambda, double* fric_coord,
+                                 double* fric_basis, uint32_t* cp_num_last, uint32_t* fric_gd_pairs,
+                                 double* fric_gd_lambda, uint32_t* h_cp_num_last, void* stream);
+
 /* ---- instrumentation (the reference's gipc::Timer / cudaEvent phase timers,
  *      StiffGIPC/gipc/utils/timer.h:19-136, GIPC.cu:10854-10964) ----------------------- */
 

@@ -59,7 +59,12 @@ ROOTS = [
     ("StiffGIPC/femEnergy.cu", "__cal_quad_bending_energy"),          # hinge energy
     ("StiffGIPC/GIPC.cu", "__cal_Friction_energy"),                   # pair friction energy
     ("StiffGIPC/GIPC.cu", "__cal_Friction_gd_energy"),                # ground friction energy
+    ("StiffGIPC/mlbvh.cu", "_checkPTintersection"),                   # mlbvh.cu:534-645
+    ("StiffGIPC/mlbvh.cu", "_checkEEintersection"),                   # mlbvh.cu:685-1059
+    ("StiffGIPC/GIPC.cu", "_GroundCollisionDetect"),                  # GIPC.cu:6433-6450
 ]
+
+VOID_CHECKS = ("_checkPTintersection", "_checkEEintersection")
 
 PRELUDE = r"""
 // ---- host stand-ins for the CUDA qualifiers, vector types and built-ins -------------
@@ -299,6 +304,12 @@ def generate(root: str) -> str:
             inner = "using namespace __GEIGEN__;\n" + inner
         return "".join("namespace %s {\n" % n for n in ns) + inner + "\n" + "}" * len(ns)
 
+    # _checkPTintersection / _checkEEintersection are declared bool but end without returning a
+    # value, and no caller reads one; g++ traps at such an end, nvcc lets it pass: give them the
+    # void they behave as
+    for d in defs:
+        if d.name in VOID_CHECKS:
+            d.header = re.sub(r"\bbool\s+(%s)\b" % d.name, r"void \1", d.header)
     parts.append("// ---- prototypes")
     for d in defs:
         if "template" in d.header:

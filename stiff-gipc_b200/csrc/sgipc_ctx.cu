@@ -293,6 +293,7 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx
 extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
     if (!c) return SGIPC_OK;
     sgipc::DeviceScope dev_scope(c->device);
+    broad_destroy(c);
     pcg_destroy(c);
     mas_destroy(c);
     void* ptrs[] = {c->row_ptr, c->col, c->slot_row, c->diag_slot, c->low_ptr, c->low_slot, c->val64, c->val32,

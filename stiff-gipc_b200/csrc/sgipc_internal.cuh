@@ -14,6 +14,8 @@
 
 namespace sgipc {
 
+struct BroadWork;  // buffers of the contact-pair search (sgipc_broad.cu)
+
 // Device-resident PCG scalars (no host round trip per iteration).
 struct PcgScalars {
     double rz;        // r.z of the current iterate (reference: rz)
@@ -209,6 +211,7 @@ struct SgipcCtx {
     SgipcContacts mas_con;        // contacts of the last MAS build (to rebuild after timing)
     int mas_has_con;
     long long launches;           // kernels of this library launched on the context
+    sgipc::BroadWork* broad;      // contact-pair search buffers, made on its first call
     // polls a grid-barrier wait of the persistent solve or the hierarchy build makes before
     // it gives up (0: the kernels' defaults, about 2 s); sgipc_set_wait_limit
     long long wait_limit;
@@ -337,6 +340,7 @@ SgipcStatus pcg_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double*
 
 // ---- cross-unit entry points ------------------------------------------------------------
 SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t);
+void broad_destroy(SgipcCtx* c);
 void mas_destroy(SgipcCtx* c);
 SgipcStatus mas_build(SgipcCtx* c, const SgipcContacts* con, SgipcPrecision prec, cudaStream_t s);
 // Start the hierarchy for these contacts on the MAS side stream, after the work queued on

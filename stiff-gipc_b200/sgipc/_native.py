@@ -51,6 +51,11 @@ class SgipcSolveStats(C.Structure):
                 ("rel_residual", C.c_double), ("status", _i32)]
 
 
+class SgipcSurface(C.Structure):
+    _fields_ = [("surf_verts", _vp), ("surf_vert_num", _i32), ("faces", _vp), ("face_num", _i32), ("edges", _vp),
+                ("edge_num", _i32)]
+
+
 class SgipcAbdTopology(C.Structure):
     _fields_ = [("body_num", _i32), ("point_num", _i32), ("point_body", _vp), ("x_bar", _vp),
                 ("dyadic_mass", _vp), ("volume", _vp), ("boundary_type", _vp), ("max_abd_blocks", _i32),
@@ -106,6 +111,10 @@ SIGNATURES = {
     "sgipc_launch_count": ([_vp, C.POINTER(C.c_int64)], _i32),
     "sgipc_time_kernel": ([_vp, C.c_char_p, _i32, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)], _i32),
     "sgipc_set_wait_limit": ([_vp, C.c_int64], _i32),
+    "sgipc_build_cp": ([_vp, _vp, _vp, C.POINTER(SgipcSurface), _vp, _vp, C.c_double, C.c_double, _i32, _vp, _vp,
+                        _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp], _i32),
+    "sgipc_friction_setup": ([_vp, _vp, _vp, _i32, _vp, _i32, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp,
+                              _vp, _vp, _vp, _vp, _vp, _vp], _i32),
     "sgipc_profile_pcg": ([_vp, C.c_char_p, _i32, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _vp], _i32),
 }
 

@@ -31,46 +31,48 @@ PP, PE, PT, EE = 0, 1, 2, 3
 # closest-feature classification (vectorised)
 # ----------------------------------------------------------------------------------------
 
+def _det_cols(a, b, c):
+    """det[a b c] (columns), term by term in the order of the reference's __Determiant
+    (StiffGIPC/gpu_eigen_libs.cu:1193-1201)."""
+    return (a[:, 0] * b[:, 1] * c[:, 2] + a[:, 1] * b[:, 2] * c[:, 0] + a[:, 2] * b[:, 0] * c[:, 1]
+            - a[:, 2] * b[:, 1] * c[:, 0] - a[:, 0] * c[:, 1] * b[:, 2] - b[:, 0] * a[:, 1] * c[:, 2])
+
+
 def pt_type(p, t0, t1, t2):
-    """Closest feature of triangle (t0,t1,t2) to point p.
+    """Closest feature of triangle (t0,t1,t2) to point p (``_dType_PT``, StiffGIPC/mlbvh.cu:288-447).
 
     Returns codes matching the reference's switch in ``_checkPTintersection``:
     0/1/2 = point-vertex t0/t1/t2, 3/4/5 = point-edge (t0t1)/(t1t2)/(t2t0), 6 = interior.
+    For each edge (a, b) the parameters (s, h) of p - a in the frame [e, e x n, n] come from
+    Cramer's rule; the edge is closest when 0 < s < 1 and h >= 0.
     """
-    ab = t1 - t0
-    ac = t2 - t0
-    ap = p - t0
-    d1 = (ab * ap).sum(1)
-    d2 = (ac * ap).sum(1)
-    bp = p - t1
-    d3 = (ab * bp).sum(1)
-    d4 = (ac * bp).sum(1)
-    cp = p - t2
-    d5 = (ab * cp).sum(1)
-    d6 = (ac * cp).sum(1)
-    va = d3 * d6 - d5 * d4
-    vb = d5 * d2 - d1 * d6
-    vc = d1 * d4 - d3 * d2
+    n = np.cross(t1 - t0, t2 - t0)
+    s, h = [], []
+    for a, b in ((t0, t1), (t1, t2), (t2, t0)):
+        e = b - a
+        f = np.cross(e, n)
+        w = p - a
+        D = _det_cols(e, f, n)
+        s.append(_det_cols(w, f, n) / D)
+        h.append(_det_cols(e, w, n) / D)
     out = np.full(p.shape[0], 6, np.int32)
-    # evaluate regions in reverse priority so that the first match wins
-    e20 = (vb <= 0) & (d2 >= 0) & (d6 <= 0)
-    out[e20] = 5
-    e12 = (va <= 0) & ((d4 - d3) >= 0) & ((d5 - d6) >= 0)
-    out[e12] = 4
-    e01 = (vc <= 0) & (d1 >= 0) & (d3 <= 0)
-    out[e01] = 3
-    out[(d6 >= 0) & (d5 <= d6)] = 2
-    out[(d3 >= 0) & (d4 <= d3)] = 1
-    out[(d1 <= 0) & (d2 <= 0)] = 0
+    # evaluate in reverse priority so that the reference's first match wins
+    out[(s[2] <= 0.0) & (s[1] >= 1.0)] = 2
+    out[(s[1] <= 0.0) & (s[0] >= 1.0)] = 1
+    out[(s[0] <= 0.0) & (s[2] >= 1.0)] = 0
+    for i in (2, 1, 0):
+        out[(s[i] > 0.0) & (s[i] < 1.0) & (h[i] >= 0.0)] = 3 + i
     return out
 
 
 def ee_type(a0, a1, b0, b1):
-    """Closest features of segments (a0,a1) and (b0,b1).
+    """Closest features of segments (a0,a1) and (b0,b1) (``_dType_EE``, StiffGIPC/mlbvh.cu:449-530,
+    D. Sunday's clamped closest-point parameters s on a, t on b).
 
-    Codes follow the reference's ``_dType_EE`` switch: 0 PP(a0,b0), 1 PP(a0,b1),
-    2 PE(a0; b0b1), 3 PP(a1,b0), 4 PP(a1,b1), 5 PE(a1; b0b1), 6 PE(b0; a0a1),
-    7 PE(b1; a0a1), 8 EE.
+    Codes follow the reference's switch: 0 PP(a0,b0), 1 PP(a0,b1), 2 PE(a0; b0b1),
+    3 PP(a1,b0), 4 PP(a1,b1), 5 PE(a1; b0b1), 6 PE(b0; a0a1), 7 PE(b1; a0a1), 8 EE.
+    Nearly parallel segments whose interior parameters fall inside both take an endpoint
+    case (2 or 5) instead of the lines.
     """
     u = a1 - a0
     v = b1 - b0
@@ -81,48 +83,29 @@ def ee_type(a0, a1, b0, b1):
     d = (u * w).sum(1)
     e = (v * w).sum(1)
     D = a * c - b * b
-    par = D < 1e-20 * a * c
-    sN = np.where(par, 0.0, b * e - c * d)
-    sD = np.where(par, 1.0, D)
-    tN = np.where(par, e, a * e - b * d)
-    tD = np.where(par, c, D)
-    s_at = np.full(a.shape, 1, np.int32)   # 0 = start, 1 = interior, 2 = end
-    s_at[par] = 0
-    neg = ~par & (sN <= 0)
-    sN = np.where(neg, 0.0, sN)
-    tN = np.where(neg, e, tN)
-    tD = np.where(neg, c, tD)
-    s_at[neg] = 0
-    big = ~par & ~neg & (sN >= sD)
-    sN = np.where(big, sD, sN)
-    tN = np.where(big, e + b, tN)
-    tD = np.where(big, c, tD)
-    s_at[big] = 2
-    t_at = np.ones(a.shape, np.int32)
-    tneg = tN <= 0
-    t_at[tneg] = 0
-    # re-derive s for clamped t
-    sN2 = np.where(tneg, -d, sN)
-    sD2 = np.where(tneg, a, sD)
-    tbig = ~tneg & (tN >= tD)
-    t_at[tbig] = 2
-    sN2 = np.where(tbig, -d + b, sN2)
-    sD2 = np.where(tbig, a, sD2)
-    clamp_t = tneg | tbig
-    s_at2 = s_at.copy()
-    s_at2[clamp_t & (sN2 <= 0)] = 0
-    s_at2[clamp_t & (sN2 >= sD2)] = 2
-    s_at2[clamp_t & (sN2 > 0) & (sN2 < sD2)] = 1
-    s_at = np.where(clamp_t, s_at2, s_at)
-    code = np.full(a.shape, 8, np.int32)
-    code[(s_at == 0) & (t_at == 0)] = 0
-    code[(s_at == 0) & (t_at == 2)] = 1
-    code[(s_at == 0) & (t_at == 1)] = 2
-    code[(s_at == 2) & (t_at == 0)] = 3
-    code[(s_at == 2) & (t_at == 2)] = 4
-    code[(s_at == 2) & (t_at == 1)] = 5
-    code[(s_at == 1) & (t_at == 0)] = 6
-    code[(s_at == 1) & (t_at == 2)] = 7
+    sN = b * e - c * d
+    res = np.full(a.shape, 8, np.int32)
+    lo = sN <= 0.0
+    hi = ~lo & (sN >= D)
+    mid = ~lo & ~hi
+    tN = np.where(lo, e, np.where(hi, e + b, a * e - b * d))
+    tD = np.where(lo | hi, c, D)
+    res[lo] = 2
+    res[hi] = 5
+    uv = np.cross(u, v)
+    flat = mid & (tN > 0.0) & (tN < tD) & (((w * uv).sum(1) == 0.0) | ((uv * uv).sum(1) < 1.0e-20 * a * c))
+    first = flat & (sN < D / 2)
+    second = flat & ~(sN < D / 2)
+    tN = np.where(first, e, np.where(second, e + b, tN))
+    tD = np.where(flat, c, tD)
+    res[first] = 2
+    res[second] = 5
+    code = res.copy()
+    t0 = tN <= 0.0
+    code[t0] = np.where(-d[t0] <= 0.0, 0, np.where(-d[t0] >= a[t0], 3, 6))
+    t1 = ~t0 & (tN >= tD)
+    s1 = -d[t1] + b[t1]
+    code[t1] = np.where(s1 <= 0.0, 1, np.where(s1 >= a[t1], 4, 7))
     return code
 
 
@@ -158,12 +141,14 @@ def eps_x(r0, r1, r2, r3):
 # ----------------------------------------------------------------------------------------
 
 def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
-               inter_body_only=False):
+               inter_body_only=False, with_ccd=False):
     """All barrier pairs with squared distance below ``dhat``, reference-encoded.
 
-    Returns an (P,4) int32 array ordered PT-derived pairs first, then EE-derived pairs.
+    Returns an (P,4) int32 array ordered PT-derived pairs first, then EE-derived pairs; with
+    ``with_ccd`` also the CCD candidate of each pair (the point with its whole triangle, or the
+    two edges: _ccd_collisionPair, StiffGIPC/mlbvh.cu:534-1059).
     """
-    out = []
+    out, ccd = [], []
     if len(surf_tris) and len(surf_verts):
         tri_c = x[surf_tris].mean(1)
         tri_r = np.sqrt(((x[surf_tris] - tri_c[:, None]) ** 2).sum(2).max(1))
@@ -205,6 +190,7 @@ def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
             # like the reference, a point close to a shared vertex or edge of several
             # triangles yields one pair per triangle
             out.append(enc)
+            ccd.append(np.concatenate([(-pi - 1)[:, None], t.astype(np.int64)], 1))
     if len(surf_edges) > 1:
         mid = x[surf_edges].mean(1)
         hl = np.sqrt(((x[surf_edges[:, 0]] - x[surf_edges[:, 1]]) ** 2).sum(1)) * 0.5
@@ -212,11 +198,12 @@ def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
         rq = 2.0 * float(hl.max()) + np.sqrt(dhat)
         cand = tree.query_pairs(rq, output_type="ndarray")
         if len(cand):
+            cand = np.sort(cand, axis=1)  # (self, other) with other > self, as _selfQuery_ee takes them
             ea, eb = surf_edges[cand[:, 0]], surf_edges[cand[:, 1]]
             keep = (ea[:, :, None] != eb[:, None, :]).all((1, 2))
             if inter_body_only and body is not None:
                 keep &= body[ea[:, 0]] != body[eb[:, 0]]
-            ea, eb = ea[keep], eb[keep]
+            ea, eb, other = ea[keep], eb[keep], cand[keep, 1]
             a0, a1, b0, b1 = x[ea[:, 0]], x[ea[:, 1]], x[eb[:, 0]], x[eb[:, 1]]
             code = ee_type(a0, a1, b0, b1)
             d = np.full(len(ea), np.inf)
@@ -230,11 +217,13 @@ def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
             m = code == 7; d[m] = d_pe(b1[m], a0[m], a1[m])
             m = code == 8; d[m] = d_ee(a0[m], a1[m], b0[m], b1[m])
             hit = d < dhat
-            ea, eb, code = ea[hit], eb[hit], code[hit]
+            ea, eb, code, other = ea[hit], eb[hit], code[hit], other[hit]
             ep = eps_x(rest[ea[:, 0]], rest[ea[:, 1]], rest[eb[:, 0]], rest[eb[:, 1]])
             cr = np.cross(x[ea[:, 0]] - x[ea[:, 1]], x[eb[:, 0]] - x[eb[:, 1]])
             par = (cr * cr).sum(1) < ep
-            add_e = np.where(par, -2, -1)
+            # nearly parallel edges: the point-point / point-edge pair carries w = -(other edge) - 2
+            # (add_e, StiffGIPC/mlbvh.cu:722); the mollified encodings stay off there (smooth = false)
+            add_e = np.where(par, -other.astype(np.int64) - 2, -1)
             enc = np.zeros((len(ea), 4), np.int64)
             i0, i1, j0, j1 = ea[:, 0], ea[:, 1], eb[:, 0], eb[:, 1]
             table = {0: (i0, j0, None), 1: (i0, j1, None), 2: (i0, j0, j1),
@@ -249,9 +238,12 @@ def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
             m = code == 8
             enc[m] = np.stack([i0[m], i1[m], j0[m], j1[m]], 1)
             out.append(enc)
+            ccd.append(np.stack([i0, i1, j0, j1], 1))
     if not out:
-        return np.zeros((0, 4), np.int32)
-    return np.concatenate(out, 0).astype(np.int32)
+        empty = np.zeros((0, 4), np.int32)
+        return (empty, empty.copy()) if with_ccd else empty
+    pairs = np.concatenate(out, 0).astype(np.int32)
+    return (pairs, np.concatenate(ccd, 0).astype(np.int32)) if with_ccd else pairs
 
 
 def ground_pairs(x, surf_verts, dhat, offset=-1.0):

@@ -159,6 +159,7 @@ class GIPC:
         t.neighborList = self._hp(sc.nbr_list, np.uint32)
         cap = pair_capacity if pair_capacity is not None else max(len(sc.pairs), 1)
         t.max_pairs = cap
+        self.pair_capacity = cap
         t.max_ground = max(len(sc.ground_pairs), len(sc.surf_verts))
         t.max_fric_pairs = max(len(sc.fric_pairs), cap)
         t.max_fric_ground = max(len(sc.fric_gd_pairs), len(sc.surf_verts))
@@ -318,6 +319,77 @@ class GIPC:
         st = buf[:cap * max_epochs * 2].reshape(cap, max_epochs, 2)[:grid.value, :ep.value].astype(np.int64)
         tags = buf[cap * max_epochs * 2:][:ep.value]
         return st, ["start"] + [self.PHASES.get(int(t), "?") for t in tags[1:]]
+
+    # ---- contact pairs of an iterate and the frame's friction sets --------------------------
+    def _surface(self):
+        if getattr(self, "_surf", None) is None:
+            sc = self.scene
+            self._surf_arrays = (_t(np.asarray(sc.surf_verts, np.int64).astype(np.int32), torch.int32),
+                                 _t(np.asarray(sc.surf_tris, np.int64).astype(np.int32).reshape(-1, 3), torch.int32),
+                                 _t(np.asarray(sc.surf_edges, np.int64).astype(np.int32).reshape(-1, 2), torch.int32))
+            sv, sf, se = self._surf_arrays
+            self._surf = N.SgipcSurface(_p(sv), sv.shape[0], _p(sf), sf.shape[0], _p(se), se.shape[0])
+        return self._surf
+
+    def buildCP(self, tet: Optional[DeviceTetraData] = None, body: Optional[torch.Tensor] = None,
+                capacity: Optional[int] = None, update: bool = True):
+        """GIPC::buildCP (GIPC.cu:9065): the contact pairs of tet.vertexes on the GPU
+        (``sgipc_build_cp``).  body: int32 per vertex (default -1 everywhere: every body also
+        collides with itself).  Returns a dict of device tensors (pairs, ccd_pairs, mat_index,
+        ground_pairs) and the host counts cp_num (5) and gp_num; with update=True the pairs and
+        ground pairs also replace tet's (the Newton system's contact inputs)."""
+        tet = tet or self.tet
+        surf = self._surface()
+        cap = capacity or self.pair_capacity
+        dev = _dev()
+        if body is None:
+            body = torch.full((self.scene.nv,), -1, dtype=torch.int32, device=dev)
+        out = {"pairs": torch.empty((cap, 4), dtype=torch.int32, device=dev),
+               "ccd_pairs": torch.empty((cap, 4), dtype=torch.int32, device=dev),
+               "mat_index": torch.empty(cap, dtype=torch.int32, device=dev),
+               "cp_num_dev": torch.zeros(5, dtype=torch.int32, device=dev),
+               "ground_pairs": torch.empty(max(1, surf.surf_vert_num), dtype=torch.int32, device=dev),
+               "gp_num_dev": torch.zeros(1, dtype=torch.int32, device=dev)}
+        cp = (C.c_uint32 * 5)()
+        gp = C.c_uint32()
+        N.check(N.lib().sgipc_build_cp(self.ctx, _p(tet.vertexes), _p(tet.rest_vertexes), C.byref(surf), _p(body),
+                                       _p(tet.BoundaryType), float(self.params["dHat"]),
+                                       float(self.params.get("ground_offset", 0.0)), cap, _p(out["pairs"]),
+                                       _p(out["ccd_pairs"]), _p(out["mat_index"]), _p(out["cp_num_dev"]),
+                                       out["ground_pairs"].shape[0], _p(out["ground_pairs"]), _p(out["gp_num_dev"]),
+                                       cp, C.byref(gp), _stream()), self.ctx)
+        n, ng = int(cp[0]), int(gp.value)
+        out.update(pairs=out["pairs"][:n], ccd_pairs=out["ccd_pairs"][:n], mat_index=out["mat_index"][:n],
+                   ground_pairs=out["ground_pairs"][:ng], cp_num=list(cp), gp_num=ng)
+        if update:
+            tet.pairs = out["pairs"]
+            tet.ground_pairs = out["ground_pairs"]
+        return out
+
+    def buildFrictionSets(self, tet: Optional[DeviceTetraData] = None, x: Optional[torch.Tensor] = None):
+        """GIPC::buildFrictionSets (GIPC.cu:8660-8696): the lagged friction arrays of tet's pairs
+        and ground pairs at the frame's positions x (default tet.o_vertexes), on the GPU
+        (``sgipc_friction_setup``); they replace tet's friction inputs.  Returns cp_num_last."""
+        tet = tet or self.tet
+        x = tet.o_vertexes if x is None else x
+        n, ng = tet.pairs.shape[0], tet.ground_pairs.shape[0]
+        dev = _dev()
+        fp = torch.empty((max(n, 1), 4), dtype=torch.int32, device=dev)
+        fl = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+        fc = torch.empty((max(n, 1), 2), dtype=torch.float64, device=dev)
+        fb = torch.empty((max(n, 1), 6), dtype=torch.float64, device=dev)
+        gpp = torch.empty(max(ng, 1), dtype=torch.int32, device=dev)
+        gl = torch.empty(max(ng, 1), dtype=torch.float64, device=dev)
+        cpd = torch.zeros(5, dtype=torch.int32, device=dev)
+        cp = (C.c_uint32 * 5)()
+        N.check(N.lib().sgipc_friction_setup(self.ctx, _p(x), _p(tet.pairs), n, _p(tet.ground_pairs), ng,
+                                             float(self.params["dHat"]), float(self.params["kappa"]),
+                                             float(self.params.get("ground_offset", 0.0)), _p(fp), _p(fl), _p(fc),
+                                             _p(fb), _p(cpd), _p(gpp), _p(gl), cp, _stream()), self.ctx)
+        m = int(cp[0])
+        tet.fric_pairs, tet.fric_lambda, tet.fric_coord, tet.fric_basis = fp[:m], fl[:m], fc[:m], fb[:m]
+        tet.fric_gd_pairs, tet.fric_gd_lambda = gpp[:ng], gl[:ng]
+        return list(cp)
 
     def spmv(self, x: torch.Tensor) -> torch.Tensor:
         y = torch.empty_like(x)

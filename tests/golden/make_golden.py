@@ -15,7 +15,8 @@ Two fixtures, both numbers only (no reference source is stored):
   pair kind, friction energy and gradient, the lagged friction set-up, ground barrier and
   ground friction, the line-search step bounds (additive CCD), stable Neo-Hookean PK1,
   energy and gradient, cloth membrane energy and gradient, kinetic and soft-constraint
-  gradients, the inertial target and the trial step).  Inputs are two small seeded scenes
+  gradients, the inertial target, the trial step, and the contact pairs of GIPC::buildCP with
+  their MatIndex and counters).  Inputs are two small seeded scenes
   (stored beside it as ``scene_two_cubes4.npz`` and ``scene_cloth6_cube4.npz``) and seeded
   synthetic pairs of every barrier kind, the mollified ones included.
 
@@ -162,6 +163,8 @@ def load_ref(path):
         "ref_tri_gradient": (None, [_d, _u, I32, _d, _d, D, D, D, D, _d]),
         "ref_point_triangle_ccd": (D, [_d, _d, D, D]),
         "ref_edge_edge_ccd": (D, [_d, _d, D, D]),
+        "ref_find_pairs": (I32, [_d, _d, I32, _u, I32, _u, I32, _u, _i, _i, D, I32, _i, _i, _i, _u]),
+        "ref_ground_pairs": (I32, [_d, I32, _u, D, _d, D, _u]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -427,6 +430,26 @@ def make_ref(ref_root):
                          for v in gp])
         out.update({pre + "move": move, pre + "ccd_cand": cand, pre + "ccd_inv": inv, pre + "gmove": gmove,
                     pre + "ground_step_inv": ginv})
+        # contact pairs of GIPC::buildCP at the iterate: self-collision everywhere (body -1), and
+        # between bodies only (the scene's body ids)
+        sv = np.ascontiguousarray(sc.surf_verts, np.uint32)
+        sf = np.ascontiguousarray(sc.surf_tris, np.uint32)
+        se = np.ascontiguousarray(sc.surf_edges, np.uint32)
+        bt = np.ascontiguousarray(sc.boundary_type, np.int32)
+        for variant, body in (("self", np.full(sc.nv, -1, np.int32)),
+                              ("bodies", np.ascontiguousarray(sc.body_of_vertex, np.int32))):
+            cap = 200000
+            cpp, ccp, mi = np.zeros((cap, 4), np.int32), np.zeros((cap, 4), np.int32), np.zeros(cap, np.int32)
+            cpn = np.zeros(5, np.uint32)
+            n = L.ref_find_pairs(_p(xs), _p(rest), len(sv), _p(sv, _u), len(sf), _p(sf, _u), len(se), _p(se, _u),
+                                 _p(body, _i), _p(bt, _i), dh, cap, _p(cpp, _i), _p(ccp, _i), _p(mi, _i), _p(cpn, _u))
+            assert 0 < n < cap, n
+            q = "%scp_%s_" % (pre, variant)
+            out.update({q + "pairs": cpp[:n].copy(), q + "ccd": ccp[:n].copy(), q + "matindex": mi[:n].copy(),
+                        q + "cpnum": cpn.astype(np.int64), q + "body": body})
+        gout = np.zeros(len(sv), np.uint32)
+        ng = L.ref_ground_pairs(_p(xs), len(sv), _p(sv, _u), prm["ground_offset"], _p(up), dh, _p(gout, _u))
+        out[pre + "cp_ground"] = gout[:ng].astype(np.int32)
         # trial step with mixed boundary types, with and without move_boundary
         for mb in (0, 1):
             xn = np.zeros_like(xs)

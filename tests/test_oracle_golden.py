@@ -255,3 +255,32 @@ def test_inertial_target(tag):
     xt = scenes.inertial_target(sc.o_vertexes, sc.velocities, sc.boundary_type, sc.params["dt"],
                                 G[tag + "_xtilta_gravity"])
     assert np.abs(xt - G[tag + "_xtilta"]).max() <= 1e-15
+
+
+def _rows_sorted(*arrays):
+    return np.array(sorted(map(tuple, np.concatenate([np.asarray(a).reshape(len(a), -1) for a in arrays], 1))))
+
+
+@pytest.mark.parametrize("tag", ["cubes", "cloth"])
+@pytest.mark.parametrize("variant", ["self", "bodies"])
+def test_host_pair_generator_matches_reference_build_cp(tag, variant):
+    """sgipc.contacts.find_pairs against the reference's pair checks (_checkPTintersection /
+    _checkEEintersection with the BVH queries' filters, mlbvh.cu:534-1059, 1306-1742): the same
+    multiset of (pair, CCD candidate) rows, nearly parallel edge pairs with w = -other - 2
+    included; and the ground pairs of _GroundCollisionDetect."""
+    sc = _scene(tag)
+    q = "%s_cp_%s_" % (tag, variant)
+    pairs, ccd = contacts.find_pairs(sc.vertexes, sc.rest_vertexes, sc.surf_tris, sc.surf_edges, sc.surf_verts,
+                                     sc.params["dHat"], sc.body_of_vertex, inter_body_only=(variant == "bodies"),
+                                     with_ccd=True)
+    assert np.array_equal(_rows_sorted(pairs, ccd), _rows_sorted(G[q + "pairs"], G[q + "ccd"]))
+    cp = G[q + "cpnum"]
+    assert cp[0] == len(pairs) == cp[2] + cp[3] + cp[4] and cp[1] == 0
+    # MatIndex: each pair's rank among the pairs of its size (the reference's order is that of
+    # its atomics; any order gives every size the ranks 0 .. count-1 once)
+    mi, p = G[q + "matindex"], G[q + "pairs"]
+    size = np.where(p[:, 0] >= 0, 4, np.where(p[:, 2] < 0, 2, np.where(p[:, 3] < 0, 3, 4)))
+    for g, nv in ((2, 2), (3, 3), (4, 4)):
+        assert np.array_equal(np.sort(mi[size == nv]), np.arange(cp[g]))
+    gp = contacts.ground_pairs(sc.vertexes, sc.surf_verts, sc.params["dHat"], sc.params["ground_offset"])
+    assert np.array_equal(np.sort(gp), np.sort(G[tag + "_cp_ground"]))
