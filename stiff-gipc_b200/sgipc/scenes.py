@@ -436,9 +436,20 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
 
     # renumber vertices in MAS part order, as the METIS-sorted meshes are, so that
     # real_map_partId is monotone (the reference's level-0 scatter assumes it,
-    # StiffGIPC/MASPreconditioner.cu:1856-1867)
-    part_map, _ = mas_partition(rest, body_id)
-    perm = part_map[part_map >= 0].astype(np.int64)
+    # StiffGIPC/MASPreconditioner.cu:1856-1867); bodies given with their own part ids (read
+    # from .part files, or partitioned by sgipc.meshio) keep them and their numbering
+    given = all("parts" in b for b in bodies)
+    if given:
+        offs, gparts = 0, []
+        for body in bodies:
+            p = np.asarray(body["parts"], np.int64)
+            gparts.append(p - (p.min() if len(p) else 0) + offs)
+            offs = int(gparts[-1].max()) + 1 if len(p) else offs
+        gparts = np.concatenate(gparts)
+        perm = np.arange(len(rest), dtype=np.int64)
+    else:
+        part_map, _ = mas_partition(rest, body_id)
+        perm = part_map[part_map >= 0].astype(np.int64)
     inv = np.empty(nv, np.int64)
     inv[perm] = np.arange(nv)
     rest, vel, btype, body_id = rest[perm], vel[perm], btype[perm], body_id[perm]
@@ -473,7 +484,11 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
         sedges = np.unique(np.concatenate([sedges, tri_mesh_edges(tris)]), axis=0).astype(np.int32)
         sverts = np.unique(np.concatenate([sverts, tris.ravel()])).astype(np.int32)
     nbr_start, nbr_list = neighbour_csr(nv, tets, tris)
-    part_map, real_map = ordered_partition(body_id)
+    if given:
+        from . import meshio
+        part_map, real_map = meshio.part_maps(gparts)
+    else:
+        part_map, real_map = ordered_partition(body_id)
 
     lo = np.minimum(rest.min(0), x.min(0))
     hi = np.maximum(rest.max(0), x.max(0))
@@ -492,6 +507,33 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
                  poisson=nu, surf_tris=stris, surf_edges=sedges, surf_verts=sverts,
                  body_of_vertex=body_id, part_map_real=part_map, real_map_part=real_map,
                  nbr_start=nbr_start, nbr_list=nbr_list, params=params, **cl)
+
+
+def scene_from_files(bodies: List[dict], dt: float = 0.01, dhat_abs: float = 1e-3, density: float = 1000.0,
+                     nu: float = 0.45, mu_friction: float = 0.2, seed: int = 0, perturb: float = 0.0,
+                     kappa: Optional[float] = None, cloth: Optional[dict] = None, name: str = "files") -> Scene:
+    """A Newton system of meshes read from files, as the reference's initScene loads them
+    (StiffGIPC/gl_main.cu:1095-1438): each body names ``mesh`` (a ``.msh`` tet mesh or an
+    ``.obj`` cloth), optionally ``part`` (its ``.part`` file; without one the vertices are
+    partitioned and renumbered by :func:`sgipc.meshio.partition`), ``transform`` (4 x 4), and
+    ``E`` (tets), ``velocity``, ``boundary`` as :func:`build_tet_scene` takes them."""
+    from . import meshio
+    loaded = []
+    for b in bodies:
+        v, e, p = meshio.load_body(b["mesh"], b.get("part"), b.get("transform"))
+        d = {k: val for k, val in b.items() if k not in ("mesh", "part", "transform")}
+        d["verts"], d["parts"] = v, p
+        if e.shape[1] == 4:
+            d["tets"] = e
+            d.setdefault("E", 1e5)
+        else:
+            d["tris"] = e
+        loaded.append(d)
+    sc = build_tet_scene(name, loaded, dt=dt, dhat_abs=dhat_abs, density=density, nu=nu,
+                         mu_friction=mu_friction, seed=seed, perturb=perturb, kappa=kappa, cloth=cloth)
+    from . import contacts
+    contacts.attach_contacts(sc)
+    return sc
 
 
 def scene_cube(n: int = 11, touching: bool = False, seed: int = 0) -> Scene:
