@@ -28,8 +28,16 @@ for _p in (ROOT, os.path.join(ROOT, "stiff-gipc_b200")):
         sys.path.insert(0, _p)
 
 METRIC = "Newton-system solves/s, mixed vs FP64 MAS-PCG at 1e-4 residual; adjoints/s"
-WORKLOAD = ("two stacked soft cubes, 2 x 21^3 lattice (80000 tets, 18522 vertices), E 1e5/1e6 Pa, nu 0.45, "
-            "mu 0.2, d-hat 1e-3 m; one Newton system = assembly + MAS build + PCG to r.z <= 1e-4 r0.z0")
+STEP = "; one Newton system = assembly + MAS build + PCG to r.z <= 1e-4 r0.z0"
+WORKLOADS = {
+    "two_cubes": "two stacked soft cubes, 2 x 21^3 lattice (80000 tets, 18522 vertices), E 1e5/1e6 Pa, nu 0.45, "
+                 "mu 0.2, d-hat 1e-3 m, contacts from the host pair generator" + STEP,
+    "cube": "one soft cube, 11^3 lattice (5000 tets, 1331 vertices), E 1e5 Pa, nu 0.4, dropped from 0.05 m, "
+            "d-hat 1e-3 m, no contact yet" + STEP,
+    "cloth_sphere": "256^2 cloth (130050 triangles, 195585 hinges) rolled in layers 0.4 mm apart over a tet "
+                    "sphere (20000 tets, r 0.3 m) on the ground, d-hat 5e-4 m, mu 0.2; about a million contact "
+                    "pairs from the GPU pair search, lagged friction from the GPU set-up" + STEP,
+}
 L2_FLUSH_BYTES = 256 << 20
 CPU_SOLVER = ("Eigen unavailable: the oracle's OpenMP restatement of the reference's assembly and "
               "MAS-preconditioned CG (FP64 vectors, FP32 MAS inverses), not an Eigen ConjugateGradient")
@@ -41,7 +49,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=21, help="lattice vertices per cube edge")
+    ap.add_argument("--n", type=int, default=21, help="lattice vertices per cube edge (two_cubes)")
+    ap.add_argument("--workload", default="two_cubes", choices=sorted(WORKLOADS),
+                    help="two_cubes (the headline), cube, or cloth_sphere")
     ap.add_argument("--cpu-sample", type=int, default=0, help="CPU baseline solves (0 = auto, about 10 s)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--pcg-phases", action="store_true",
@@ -117,6 +127,43 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 # CPU arms (oracle = CPU FP64 restatement of the reference's formulas)
 # ------------------------------------------------------------------------------------------
+def make_scene(args, host_contacts=True):
+    """The workload's scene.  cloth_sphere leaves its contacts to the GPU pair search (see
+    gpu_contacts) unless host_contacts asks for the host generator (about two minutes)."""
+    from sgipc import scenes
+
+    if args.workload == "cube":
+        return scenes.scene_cube(11, touching=False, seed=0)
+    if args.workload == "cloth_sphere":
+        return scenes.scene_cloth_on_sphere(256, 4000, contacts=host_contacts)
+    return scenes.scene_two_cubes(args.n, seed=1)
+
+
+def gpu_contacts(g, sc):
+    """Contact pairs, ground pairs and lagged friction sets found on the GPU, written back
+    into the scene's host arrays (the inputs of the host-state step and the CPU legs)."""
+    g.buildCP()
+    g.buildFrictionSets()
+    t = g.tet
+    sc.pairs, sc.ground_pairs = t.pairs.cpu().numpy(), t.ground_pairs.cpu().numpy()
+    sc.fric_pairs, sc.fric_lambda = t.fric_pairs.cpu().numpy(), t.fric_lambda.cpu().numpy()
+    sc.fric_coord, sc.fric_basis = t.fric_coord.cpu().numpy(), t.fric_basis.cpu().numpy().reshape(-1, 3, 2)
+    sc.fric_gd_pairs, sc.fric_gd_lambda = t.fric_gd_pairs.cpu().numpy(), t.fric_gd_lambda.cpu().numpy()
+
+
+def make_system(args, device):
+    """(scene, GIPC) of the workload on one GPU, contacts in place."""
+    from sgipc import system
+
+    sc = make_scene(args, host_contacts=False)
+    if args.workload == "cloth_sphere":
+        g = system.GIPC(sc, device=device, max_rhs=4, pair_capacity=2_000_000)
+        gpu_contacts(g, sc)
+    else:
+        g = system.GIPC(sc, device=device, max_rhs=4)
+    return sc, g
+
+
 def cpu_solves(sc, count):
     import oracle
 
@@ -182,7 +229,7 @@ def run_reference(args):
     import oracle
     from sgipc import scenes
 
-    sc = scenes.scene_two_cubes(args.n, seed=1)
+    sc = make_scene(args)
     for _ in range(args.warmup):
         cpu_solves(sc, 1)
     times = []
@@ -194,7 +241,8 @@ def run_reference(args):
            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice scenes)",
            "impl": "reference",
-           "config": {"workload": WORKLOAD, "solver": "reference PCG, FP64 matrix/vectors, FP32 MAS inverses"},
+           "config": {"workload": WORKLOADS[args.workload],
+                      "solver": "reference PCG, FP64 matrix/vectors, FP32 MAS inverses"},
            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
                             "sample": "%d full Newton systems of the workload (assembly + MAS + PCG), %d OpenMP threads"
                                       % (args.steps, oracle.num_threads()), "solver": CPU_SOLVER},
@@ -225,8 +273,7 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    sc = scenes.scene_two_cubes(args.n, seed=1)
-    g = system.GIPC(sc, device=local, max_rhs=4)
+    sc, g = make_system(args, local)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     cfg = {p: system.PCGSolverConfig(precision=p) for p in ("mixed", "fp64")}
     stream = torch.cuda.current_stream()
@@ -319,8 +366,8 @@ def run_ours(args):
     out = {"metric": METRIC, "value": units / t_mixed, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
-           "data": "synthetic (seeded lattice scenes, contacts from the host pair generator)",
-           "config": {"workload": WORKLOAD, "parallelism": "replicas x%d" % world,
+           "data": "synthetic (seeded lattice scenes)",
+           "config": {"workload": WORKLOADS[args.workload], "parallelism": "replicas x%d" % world,
                       "l2": "flushed (256 MiB write) between timed steps",
                       "solver_mixed": "FP32 BSR + FP32 MAS inner PCG, FP64 residual refinement",
                       "pcg_iters_mixed": st_mixed.iterations, "refinements_mixed": st_mixed.refinements,
@@ -434,12 +481,11 @@ def run_pcg_phases(args):
     """Barrier-stamp profile of the persistent PCG solve on the workload (one GPU)."""
     import torch
 
-    from sgipc import scenes, system
+    from sgipc import system
 
     torch.cuda.set_device(0)
-    sc = scenes.scene_two_cubes(args.n, seed=1)
-    g = system.GIPC(sc, device=0, max_rhs=4)
-    out = {"workload": WORKLOAD}
+    sc, g = make_system(args, 0)
+    out = {"workload": WORKLOADS[args.workload]}
     for prec, names in (("mixed", ("pcg32", "pcg32x4")), ("fp64", ("pcg64", "pcg64x4"))):
         g.computeGradientAndHessian()
         g.calculateMovingDirection(system.PCGSolverConfig(precision=prec))
@@ -460,11 +506,10 @@ def run_kernel_only(args):
     named kernel with sgipc_time_kernel (one untimed launch, then args.steps timed ones)."""
     import torch
 
-    from sgipc import scenes, system
+    from sgipc import system
 
     torch.cuda.set_device(0)
-    sc = scenes.scene_two_cubes(args.n, seed=1)
-    g = system.GIPC(sc, device=0, max_rhs=4)
+    sc, g = make_system(args, 0)
     g.computeGradientAndHessian()
     system.MASPreconditioner(g).setPreconditioner("fp64" if args.kernel in ("pcg64", "mas_domain64") else "mixed")
     ms, by = g.time_kernel(args.kernel, args.steps)

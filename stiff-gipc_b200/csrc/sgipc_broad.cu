@@ -70,6 +70,7 @@ namespace {
 constexpr int kCellBits = 21;
 constexpr unsigned long long kNoKey = ~0ull;
 constexpr int kGroupBits = 21;  // packed rank fields: three 21-bit counters in one 64-bit word
+constexpr int kQueryThreads = 128;
 
 // order-preserving map of doubles to unsigned integers (min / max by integer atomics)
 __device__ __forceinline__ unsigned long long ord(double v) {
@@ -743,7 +744,7 @@ extern "C" SgipcStatus sgipc_build_cp(SgipcCtx* c, const double* x, const double
     SG_CHECK(c, cudaMemsetAsync(w.counts, 0, sizeof(int) * (size_t)(nq + 1), s));
     if (nq > 0) {
         SG_COUNT(c, 1);
-        k_query<false><<<nblk(nq), 128, 0, s>>>(qa, w.counts, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+        k_query<false><<<nblk(nq, kQueryThreads), kQueryThreads, 0, s>>>(qa, w.counts, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                                                 nullptr, nullptr);
     }
     size_t t = w.cub_bytes;
@@ -785,7 +786,7 @@ extern "C" SgipcStatus sgipc_build_cp(SgipcCtx* c, const double* x, const double
     int* group = reinterpret_cast<int*>(w.gscan);
     if (nq > 0) {
         SG_COUNT(c, 1);
-        k_query<true><<<nblk(nq), 128, 0, s>>>(qa, nullptr, w.offs, P, Q, group, w.rec_pair, w.rec_ccd, w.reckey,
+        k_query<true><<<nblk(nq, kQueryThreads), kQueryThreads, 0, s>>>(qa, nullptr, w.offs, P, Q, group, w.rec_pair, w.rec_ccd, w.reckey,
                                                w.recidx);
     }
     const int nee = total - npt;

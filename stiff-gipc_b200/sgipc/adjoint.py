@@ -74,21 +74,39 @@ def set_parameters(g: GIPC, E: Optional[torch.Tensor] = None, v0: Optional[torch
         tet.xTilta.copy_(tet.o_vertexes + dt * v0.to(torch.float64).reshape(-1, 3) + dt * dt * free * grav[None])
 
 
-def newton_solve(g: GIPC, tol: float = 1e-11, max_newton: int = 30, precision: str = "fp64") -> torch.Tensor:
-    """Minimise the incremental potential for the current parameters with the contact set
-    held fixed: Newton steps x <- x - alpha dx with A dx = g(x) solved by the MAS-PCG, alpha
-    halved until ||g|| decreases.  Stops when ||g(x)|| <= tol * ||g(x_start)||, or when no
-    step length reduces ||g|| any more (round-off level), keeping the best iterate.
-    Returns x* (V,3), left in ``g.tet.vertexes``, with the system assembled at x*.
+def newton_solve(g: GIPC, tol: float = 1e-11, max_newton: int = 30, precision: str = "fp64",
+                 contacts: bool = False, max_move: Optional[float] = None) -> torch.Tensor:
+    """Minimise the incremental potential for the current parameters: Newton steps
+    x <- x - alpha dx with A dx = g(x) solved by the MAS-PCG.  alpha is first bounded as the
+    reference bounds it before its line search (GIPC.cu:10895-10901): by the ground plane's
+    largest feasible step over every surface vertex and, with ``contacts``, by the additive
+    CCD's over the candidate pairs of the step, both at slackness 0.8; then it is halved until
+    ||g|| decreases.  Stops when ||g(x)|| <= tol * ||g(x_start)||, or when no step length
+    reduces ||g|| any more (round-off level), keeping the best iterate.  Returns x* (V,3),
+    left in ``g.tet.vertexes``, with the system assembled at x*.
 
-    The reference's Newton loop (line search on energy, CCD, contact set updates,
-    GIPC.cu:10830-10976) is not part of this path; this driver exists so that the adjoint can
-    be checked against finite differences of a converged step."""
+    contacts=False keeps the contact pairs and ground pairs of ``g.tet`` fixed.  contacts=True
+    finds them again at every trial iterate with the GPU pair search (``GIPC.buildCP``), as the
+    reference's line search does, so that x* minimises the energy with the contacts of x*.  A
+    step then moves no vertex further than ``max_move`` (default 2 d-hat), and its CCD
+    candidates are the pairs within d-hat + 2 max_move of the current iterate: every pair that
+    the step can bring into contact.  The lagged friction sets stay those of the frame start,
+    as in the reference (buildFrictionSets once per frame, GIPC.cu:11119).
+
+    The reference's Newton loop (energy line search, kappa updates, GIPC.cu:10830-10976) is not
+    part of this path; this driver exists so that the adjoint can be checked against finite
+    differences of a converged step."""
     cfg = PCGSolverConfig(precision=precision, global_tol_rate=1e-13, criterion=N.CRIT_TRUE, max_iter_ratio=1.0)
     x = g.tet.vertexes
+    dhat = float(g.params["dHat"]) ** 0.5
+    max_move = 2.0 * dhat if max_move is None else max_move
+    if contacts:
+        g.buildCP()
     g.computeGradientAndHessian()
     r = g.rhs().norm().item()
     r0 = max(r, 1e-300)
+    g._surface()
+    surf = g._surf_arrays[0]
     for _ in range(max_newton):
         if r <= tol * r0:
             break
@@ -96,8 +114,20 @@ def newton_solve(g: GIPC, tol: float = 1e-11, max_newton: int = 30, precision: s
         dx = g.moveDir.view(-1, 3).clone()
         x_prev = x.clone()
         alpha = 1.0
+        if surf.numel():
+            alpha = min(alpha, g.ground_largestFeasibleStepSize(0.8, g.moveDir, surf))
+        if contacts:
+            far = dx.norm(dim=1).max().item()
+            if far * alpha > max_move:
+                alpha = max_move / far
+            reach = dhat + 2.0 * alpha * far
+            cand = g.buildCP(update=False, dHat=reach * reach)["ccd_pairs"]
+            if cand.shape[0]:
+                alpha = min(alpha, g.self_largestFeasibleStepSize(0.8, g.moveDir, cand.contiguous()))
         while True:
             x.copy_(x_prev - alpha * dx)
+            if contacts:
+                g.buildCP()
             g.computeGradientAndHessian()
             rn = g.rhs().norm().item()
             if rn < r or alpha < 1e-3:
@@ -105,6 +135,8 @@ def newton_solve(g: GIPC, tol: float = 1e-11, max_newton: int = 30, precision: s
             alpha *= 0.5
         if not rn < r:  # no decrease: x_prev is converged to round-off
             x.copy_(x_prev)
+            if contacts:
+                g.buildCP()
             g.computeGradientAndHessian()
             break
         r = rn
@@ -118,9 +150,10 @@ class ImplicitStep(torch.autograd.Function):
     with dg/dE_t and dg/dv0 (``sgipc_adjoint_param_grads``)."""
 
     @staticmethod
-    def forward(ctx, E: torch.Tensor, v0: torch.Tensor, g: GIPC, tol: float = 1e-11):
+    def forward(ctx, E: torch.Tensor, v0: torch.Tensor, g: GIPC, tol: float = 1e-11,
+                contacts: bool = False):
         set_parameters(g, E, v0)
-        x = newton_solve(g, tol=tol)
+        x = newton_solve(g, tol=tol, contacts=contacts)
         ctx.g = g
         ctx.v0_shape = v0.shape
         return x.clone()
@@ -131,4 +164,4 @@ class ImplicitStep(torch.autograd.Function):
         g.computeGradientAndHessian()  # A and dg/dtheta at x* (the state forward left)
         dLdE, dLdv0, _, _ = adjoint(g, dLdx.reshape(1, -1).contiguous(), precision="fp64", tol=1e-12,
                                     criterion=N.CRIT_TRUE)
-        return dLdE[0], dLdv0[0].reshape(ctx.v0_shape), None, None
+        return dLdE[0], dLdv0[0].reshape(ctx.v0_shape), None, None, None

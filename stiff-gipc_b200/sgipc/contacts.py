@@ -140,6 +140,13 @@ def eps_x(r0, r1, r2, r3):
 # pair search
 # ----------------------------------------------------------------------------------------
 
+def _size_classes(radius):
+    """Index sets of the primitives grouped by size (powers of two of their radius)."""
+    r = np.maximum(np.asarray(radius, np.float64), 1e-300)
+    key = np.floor(np.log2(r)).astype(np.int64)
+    return [np.nonzero(key == k)[0] for k in np.unique(key)]
+
+
 def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
                inter_body_only=False, with_ccd=False):
     """All barrier pairs with squared distance below ``dhat``, reference-encoded.
@@ -149,14 +156,25 @@ def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
     two edges: _ccd_collisionPair, StiffGIPC/mlbvh.cu:534-1059).
     """
     out, ccd = [], []
+    gap = np.sqrt(dhat)
     if len(surf_tris) and len(surf_verts):
         tri_c = x[surf_tris].mean(1)
         tri_r = np.sqrt(((x[surf_tris] - tri_c[:, None]) ** 2).sum(2).max(1))
-        rq = float(tri_r.max()) + np.sqrt(dhat)
-        tree = cKDTree(tri_c)
-        nb = tree.query_ball_point(x[surf_verts], rq)
-        pi = np.repeat(surf_verts, [len(n) for n in nb])
-        ti = np.concatenate([np.asarray(n, np.int64) for n in nb]) if len(pi) else np.zeros(0, np.int64)
+        # candidates class by class of triangle size, so that a few large triangles do not
+        # widen the search around every point; then by point, then by triangle
+        qpos = np.empty(len(x), np.int64)
+        qpos[surf_verts] = np.arange(len(surf_verts))
+        cand_p, cand_t = [], []
+        for members in _size_classes(tri_r):
+            tree = cKDTree(tri_c[members])
+            nb = tree.query_ball_point(x[surf_verts], float(tri_r[members].max()) + gap)
+            cand_p.append(np.repeat(surf_verts, [len(n) for n in nb]))
+            cand_t.append(members[np.concatenate([np.asarray(n, np.int64) for n in nb])] if len(cand_p[-1])
+                          else np.zeros(0, np.int64))
+        pi = np.concatenate(cand_p).astype(np.int64)
+        ti = np.concatenate(cand_t).astype(np.int64)
+        order = np.lexsort((ti, qpos[pi]))
+        pi, ti = pi[order], ti[order]
         if len(pi):
             t = surf_tris[ti]
             keep = (t != pi[:, None]).all(1)
@@ -194,9 +212,26 @@ def find_pairs(x, rest, surf_tris, surf_edges, surf_verts, dhat, body=None,
     if len(surf_edges) > 1:
         mid = x[surf_edges].mean(1)
         hl = np.sqrt(((x[surf_edges[:, 0]] - x[surf_edges[:, 1]]) ** 2).sum(1)) * 0.5
-        tree = cKDTree(mid)
-        rq = 2.0 * float(hl.max()) + np.sqrt(dhat)
-        cand = tree.query_pairs(rq, output_type="ndarray")
+        classes = _size_classes(hl)
+        trees = [cKDTree(mid[m]) for m in classes]
+        found = []
+        for a, ma in enumerate(classes):
+            for b in range(a, len(classes)):
+                mb = classes[b]
+                rq = float(hl[ma].max()) + float(hl[mb].max()) + gap
+                if a == b:
+                    pr = trees[a].query_pairs(rq, output_type="ndarray")
+                    if len(pr):
+                        found.append(np.stack([ma[pr[:, 0]], ma[pr[:, 1]]], 1))
+                else:
+                    lists = trees[a].query_ball_tree(trees[b], rq)
+                    ia = np.repeat(np.arange(len(ma)), [len(l) for l in lists])
+                    if len(ia):
+                        ib = np.concatenate([np.asarray(l, np.int64) for l in lists])
+                        found.append(np.stack([ma[ia], mb[ib]], 1))
+        cand = np.concatenate(found) if found else np.zeros((0, 2), np.int64)
+        cand = np.sort(cand, axis=1)
+        cand = cand[np.lexsort((cand[:, 1], cand[:, 0]))]
         if len(cand):
             cand = np.sort(cand, axis=1)  # (self, other) with other > self, as _selfQuery_ee takes them
             ea, eb = surf_edges[cand[:, 0]], surf_edges[cand[:, 1]]

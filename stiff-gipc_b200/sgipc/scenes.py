@@ -406,15 +406,17 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
     ``tris`` (a cloth sheet), plus optional ``velocity`` (3,) and ``boundary`` flag.
     ``cloth`` gives the sheet material: ``thickness``, ``E``, ``bend_E``, ``density``,
     ``strain_rate`` (StiffGIPC/gl_main.cu:578-583, 619-640).  Vertex positions of the
-    current iterate are the rest shape plus a seeded uniform perturbation of ``perturb``
-    metres.
+    current iterate are the body's positions (``verts``) plus a seeded uniform perturbation of
+    ``perturb`` metres; its rest shape is ``rest`` when given (a cloth posed away from its flat
+    rest state), else ``verts``.
     """
     rng = np.random.default_rng(seed)
-    verts, tets, tris, youngs, vel, btype, body_id = [], [], [], [], [], [], []
+    verts, cur, tets, tris, youngs, vel, btype, body_id = [], [], [], [], [], [], [], []
     off = 0
     for b, body in enumerate(bodies):
         v = np.asarray(body["verts"], np.float64)
-        verts.append(v)
+        cur.append(v)
+        verts.append(np.asarray(body.get("rest", v), np.float64))
         if "tets" in body:
             t = np.asarray(body["tets"], np.int64) + off
             tets.append(t)
@@ -426,6 +428,7 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
         body_id.append(np.full(len(v), b, np.int32))
         off += len(v)
     rest = np.concatenate(verts)
+    pose = np.concatenate(cur)
     tets = np.concatenate(tets).astype(np.int32) if tets else np.zeros((0, 4), np.int32)
     tris = np.concatenate(tris).astype(np.int64) if tris else np.zeros((0, 3), np.int64)
     youngs = np.concatenate(youngs) if youngs else np.zeros(0)
@@ -452,7 +455,7 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
         perm = part_map[part_map >= 0].astype(np.int64)
     inv = np.empty(nv, np.int64)
     inv[perm] = np.arange(nv)
-    rest, vel, btype, body_id = rest[perm], vel[perm], btype[perm], body_id[perm]
+    rest, pose, vel, btype, body_id = rest[perm], pose[perm], vel[perm], btype[perm], body_id[perm]
     tets = inv[tets].astype(np.int32)
     tris = inv[tris].astype(np.int32)
 
@@ -472,7 +475,7 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
         srate = cloth["strain_rate"]
         stretch, shear, bend = cloth_stiffness(cloth["E"], nu, srate, cloth["bend_E"], cloth["thickness"])
 
-    x_prev = rest + rng.uniform(-perturb, perturb, rest.shape)
+    x_prev = pose + rng.uniform(-perturb, perturb, rest.shape)
     x = x_prev.copy()
     g = np.asarray(GRAVITY)
     xt = inertial_target(x_prev, vel, btype, dt)
@@ -537,7 +540,7 @@ def scene_from_files(bodies: List[dict], dt: float = 0.01, dhat_abs: float = 1e-
 
 
 def scene_cube(n: int = 11, touching: bool = False, seed: int = 0) -> Scene:
-    """Config C1: one 0.1 m soft cube (n^3 lattice) dropped from 0.05 m (or touching)."""
+    """The single-cube workload: one 0.1 m soft cube (n^3 lattice) dropped from 0.05 m (or touching)."""
     dhat_abs = 1e-3
     gap = 0.5 * dhat_abs if touching else 0.05
     v, t = lattice_tets(n, 0.1, (0.0, GROUND_OFFSET + gap, 0.0))
@@ -550,7 +553,7 @@ def scene_cube(n: int = 11, touching: bool = False, seed: int = 0) -> Scene:
 
 
 def scene_two_cubes(n: int = 21, seed: int = 1, friction: float = 0.2) -> Scene:
-    """Config C2: two stacked n^3 cubes, E = 1e5 / 1e6, nu = 0.45, mu = 0.2.
+    """The two-cube workload: two stacked n^3 cubes, E = 1e5 / 1e6, nu = 0.45, mu = 0.2.
 
     The bottom cube rests 0.5 d-hat above the ground plane, the top cube 0.5 d-hat above
     the bottom one; the top cube's initial velocity has magnitude 1 m/s in a seeded
@@ -591,6 +594,78 @@ def scene_cloth_on_cube(n_cloth: int = 24, n_cube: int = 6, seed: int = 2, frict
                          seed=seed, perturb=1e-5)
     from . import contacts
     contacts.attach_contacts(sc)
+    return sc
+
+
+def sphere_tets(n_cells: int = 4000, radius: float = 0.3, center=(0.0, 0.0, 0.0)):
+    """A tet ball: the n_cells cells of a regular lattice whose centres lie nearest the ball's
+    centre (ties by index), 5 tets each, the lattice spacing chosen so that n_cells cells fill
+    the ball's volume.  Returns (verts, tets) with the unused lattice vertices dropped."""
+    h = radius * (4.0 * math.pi / 3.0 / n_cells) ** (1.0 / 3.0)
+    n = int(math.ceil(2.0 * radius / h)) + 2
+    c0 = np.asarray(center, np.float64) - 0.5 * n * h
+    verts, tets = lattice_tets(n + 1, n * h, c0)
+    ncell = n ** 3
+    cc = np.arange(n)
+    ci, cj, ck = np.meshgrid(cc, cc, cc, indexing="ij")
+    centre = c0 + h * (np.stack([ci.ravel(), cj.ravel(), ck.ravel()], 1) + 0.5)
+    d = np.linalg.norm(centre - np.asarray(center), axis=1)
+    keep = np.sort(np.argsort(d, kind="stable")[:n_cells])
+    # lattice_tets lists the 5 tets of each split as whole-lattice blocks: tet k * ncell + c
+    t = tets.reshape(5, ncell, 4)[:, keep].reshape(-1, 4)
+    used, inv = np.unique(t, return_inverse=True)
+    return verts[used], inv.reshape(-1, 4).astype(np.int32)
+
+
+def cloth_roll(n: int = 256, length: float = 1.0, r0: float = 0.05, spacing: float = 4e-4,
+               center=(0.0, 0.0, 0.0)):
+    """An n x n cloth grid (length x length, :func:`cloth_grid`) rolled without stretch into
+    an Archimedean spiral r = r0 + spacing theta / 2 pi about an axis along z through centre:
+    the rows follow the spiral, so each layer lies ``spacing`` from the next.  With spacing
+    below d-hat every layer is in contact with its neighbours (dense self-contact) and none
+    crosses another.  Returns (verts, tris); the rest shape is the flat grid."""
+    flat, tris = cloth_grid(n, length)
+    a = spacing / (2.0 * math.pi)
+    s = flat[:, 0]
+    theta = (np.sqrt(r0 * r0 + 2.0 * a * s) - r0) / a  # arc length r0 t + a t^2 / 2 = s
+    r = r0 + a * theta
+    c = np.asarray(center, np.float64)
+    verts = np.stack([c[0] + r * np.cos(theta), c[1] + r * np.sin(theta), c[2] + flat[:, 2] - 0.5 * length], 1)
+    return verts, tris, flat
+
+
+def scene_cloth_on_sphere(n_cloth: int = 256, sphere_cells: int = 4000, seed: int = 2,
+                          friction: float = 0.2, contacts: bool = True) -> Scene:
+    """The cloth-on-sphere workload: a 256 x 256 cloth (130 050 triangles; 1 m square, thickness 1 mm, membrane
+    E 1e6 Pa, bending stiffness 1e-4) over a tet sphere (20 000 tets, radius 0.3 m, E 1e5 Pa)
+    resting 0.5 d-hat above the ground, d-hat 5e-4 m.  The cloth lies rolled (:func:`cloth_roll`,
+    layers 0.4 mm apart, about three turns) with its lowest layer 0.5 d-hat above the sphere's
+    top and falls at 0.5 m/s: every layer touches the next, the dense self-contact of a draped,
+    folded sheet.  Smaller n_cloth / sphere_cells give the same scene at parity-test sizes.
+    With contacts=False the contact and friction arrays are left empty, for a caller that
+    finds them on the GPU (``GIPC.buildCP`` and ``GIPC.buildFrictionSets``)."""
+    dhat_abs = 5e-4
+    radius = 0.3
+    ctr = np.array([0.0, GROUND_OFFSET + radius + 0.5 * dhat_abs, 0.0])
+    sv, st = sphere_tets(sphere_cells, radius, ctr)
+    # the lattice's extent is not the ball's: put its lowest vertex 0.5 d-hat above the ground
+    sv = sv + np.array([0.0, GROUND_OFFSET + 0.5 * dhat_abs - float(sv[:, 1].min()), 0.0])
+    top = float(sv[:, 1].max())
+    length = 1.0 * n_cloth / 256.0 if n_cloth < 256 else 1.0
+    r0 = length / (2.0 * math.pi * 3.2)  # about three turns at any size
+    spacing = 4e-4
+    turns_r = r0 + spacing / (2 * math.pi) * ((math.sqrt(r0 * r0 + 2 * spacing / (2 * math.pi) * length) - r0)
+                                             / (spacing / (2 * math.pi)))
+    roll_c = (0.0, top + turns_r + 0.5 * dhat_abs, 0.0)
+    cv, ct, flat = cloth_roll(n_cloth, length, r0, spacing, roll_c)
+    bodies = [dict(verts=sv, tets=st, E=1e5), dict(verts=cv, tris=ct, velocity=(0.0, -0.5, 0.0), rest=flat)]
+    sc = build_tet_scene("cloth%d_sphere%d" % (n_cloth, len(st)), bodies, dt=0.01, dhat_abs=dhat_abs,
+                         density=1000.0, nu=0.4, mu_friction=friction, seed=seed, perturb=1e-6,
+                         cloth=dict(thickness=1e-3, E=1e6, density=200.0, strain_rate=100.0, bend_E=1e5))
+    sc.params["bendStiff"] = 1e-4
+    if contacts:
+        from . import contacts as _contacts
+        _contacts.attach_contacts(sc)
     return sc
 
 

@@ -332,12 +332,13 @@ class GIPC:
         return self._surf
 
     def buildCP(self, tet: Optional[DeviceTetraData] = None, body: Optional[torch.Tensor] = None,
-                capacity: Optional[int] = None, update: bool = True):
+                capacity: Optional[int] = None, update: bool = True, dHat: Optional[float] = None):
         """GIPC::buildCP (GIPC.cu:9065): the contact pairs of tet.vertexes on the GPU
         (``sgipc_build_cp``).  body: int32 per vertex (default -1 everywhere: every body also
         collides with itself).  Returns a dict of device tensors (pairs, ccd_pairs, mat_index,
         ground_pairs) and the host counts cp_num (5) and gp_num; with update=True the pairs and
-        ground pairs also replace tet's (the Newton system's contact inputs)."""
+        ground pairs also replace tet's (the Newton system's contact inputs).  dHat (squared
+        distance, default the scene's) widens the search, e.g. for CCD candidates of a step."""
         tet = tet or self.tet
         surf = self._surface()
         cap = capacity or self.pair_capacity
@@ -353,7 +354,7 @@ class GIPC:
         cp = (C.c_uint32 * 5)()
         gp = C.c_uint32()
         N.check(N.lib().sgipc_build_cp(self.ctx, _p(tet.vertexes), _p(tet.rest_vertexes), C.byref(surf), _p(body),
-                                       _p(tet.BoundaryType), float(self.params["dHat"]),
+                                       _p(tet.BoundaryType), float(self.params["dHat"] if dHat is None else dHat),
                                        float(self.params.get("ground_offset", 0.0)), cap, _p(out["pairs"]),
                                        _p(out["ccd_pairs"]), _p(out["mat_index"]), _p(out["cp_num_dev"]),
                                        out["ground_pairs"].shape[0], _p(out["ground_pairs"]), _p(out["gp_num_dev"]),

@@ -6,7 +6,8 @@
   multiset of (pair, CCD candidate) rows, every pair size's MatIndex ranks 0 .. count - 1
   once, the same counters _cpNum[5] and ground pairs; the friction arrays pair for pair.
 * Against the host generator (``sgipc.contacts``, itself pinned to the same goldens on the
-  CPU) at the bench's size (two 21^3 cubes) and on a cloth over a cube.
+  CPU) at the bench's size (two 21^3 cubes), on a cloth over a cube and on a rolled cloth over
+  a sphere.
 * Deterministic: two calls give the same arrays in the same order; the order is point-triangle
   pairs by surface point, then edge-edge pairs by edge.
 * The Newton system assembled from the GPU's pairs and friction sets equals the oracle's
@@ -89,10 +90,14 @@ def test_friction_sets_match_reference(golden):
     assert np.abs(gl - sc.fric_gd_lambda).max() <= 1e-12 * np.abs(sc.fric_gd_lambda).max()
 
 
-@pytest.fixture(scope="module", params=["two_cubes21", "cloth24_cube6"])
+@pytest.fixture(scope="module", params=["two_cubes21", "cloth24_cube6", "cloth_roll64_sphere"])
 def large(request):
-    sc = scenes.scene_two_cubes(21, seed=1) if request.param == "two_cubes21" else \
-        scenes.scene_cloth_on_cube(24, 6, seed=2)
+    if request.param == "two_cubes21":
+        sc = scenes.scene_two_cubes(21, seed=1)
+    elif request.param == "cloth24_cube6":
+        sc = scenes.scene_cloth_on_cube(24, 6, seed=2)
+    else:  # rolled cloth layers 0.4 mm apart: dense self-contact, about 50 000 pairs
+        sc = scenes.scene_cloth_on_sphere(64, 500)
     g = system.GIPC(sc, pair_capacity=max(4 * len(sc.pairs), 4096))
     yield request.param, sc, g
     g.close()

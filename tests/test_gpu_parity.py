@@ -41,7 +41,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 @pytest.fixture(scope="module", params=["c1_cube", "cube_touch", "two_cubes", "cloth_on_cube", "cube_soft",
-                                        "cubes_dirichlet"])
+                                        "cubes_dirichlet", "cloth_roll_sphere"])
 def case(request):
     if request.param == "cubes_dirichlet":
         # two 4^3 cubes with Dirichlet vertices (every ninth), soft constraints, ground and
@@ -56,6 +56,11 @@ def case(request):
         sc = scenes.scene_cube(11, touching=False, seed=0)
     elif request.param == "cube_touch":
         sc = scenes.scene_cube(6, touching=True, seed=3)
+    elif request.param == "cloth_roll_sphere":
+        # the cloth-on-sphere workload at parity size: a 32 x 32 cloth rolled into layers
+        # 0.4 mm apart over a 300-cell tet sphere resting on the ground (dense self-contact,
+        # bending hinges, membrane strain limiting)
+        sc = scenes.scene_cloth_on_sphere(32, 300)
     elif request.param == "two_cubes":
         sc = scenes.scene_two_cubes(7, seed=5)
     else:

@@ -5,8 +5,9 @@ grid barriers whose waits are bounded: past the limit a CTA raises the kernel's 
 every CTA leaves at its next barrier, and the call returns SGIPC_CUDA_ERROR with a message.
 ``sgipc_set_wait_limit(ctx, 1)`` shortens every wait to a couple of polls, so that the first
 CTA to arrive gives up before the grid has gathered; limit 0 restores the default (about
-2 s).  After such a call the context must solve normally: the same iterations and the same
-solution as before, bit for bit (the solve is deterministic).
+2 s).  After such a call the context must solve normally: with the same preconditioner the
+same iterations and the same solution, bit for bit (the persistent solve is deterministic); with
+a rebuilt one the solution to 1e-10 (the domain matrices are summed with atomics).
 """
 import ctypes
 
@@ -41,7 +42,11 @@ def _solve(g, prec):
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_pcg_barrier_wait_runs_out_and_the_context_recovers(g, prec):
     L = N.lib()
-    x0, st0 = _solve(g, prec)
+    g.computeGradientAndHessian()
+    system.MASPreconditioner(g).setPreconditioner(prec)
+    solver = system.PCGSolver(g, system.PCGSolverConfig(precision=prec))
+    x0, st0 = solver.solve(g.rhs())
+    x0 = x0.cpu().numpy()
     assert st0.status == N.OK
     b = g.rhs()
     x = torch.empty_like(b)
@@ -55,9 +60,10 @@ def test_pcg_barrier_wait_runs_out_and_the_context_recovers(g, prec):
     finally:
         N.check(L.sgipc_set_wait_limit(g.ctx, 0), g.ctx)
     torch.cuda.synchronize()  # the device is healthy: nothing is pending or faulted
-    x1, st1 = _solve(g, prec)
+    # the same preconditioner: the persistent solve is deterministic, bit for bit
+    x1, st1 = solver.solve(g.rhs())
     assert st1.status == N.OK and st1.iterations == st0.iterations
-    assert np.array_equal(x1, x0)
+    assert np.array_equal(x1.cpu().numpy(), x0)
 
 
 def test_hierarchy_barrier_wait_runs_out_and_the_context_recovers(g):
@@ -73,9 +79,10 @@ def test_hierarchy_barrier_wait_runs_out_and_the_context_recovers(g):
     finally:
         N.check(L.sgipc_set_wait_limit(g.ctx, 0), g.ctx)
     torch.cuda.synchronize()
+    # a new hierarchy and domain matrices (accumulated with atomics: equal to rounding)
     x1, st1 = _solve(g, "fp64")
     assert st1.status == N.OK and st1.iterations == st0.iterations
-    assert np.array_equal(x1, x0)
+    assert np.abs(x1 - x0).max() <= 1e-10 * np.abs(x0).max()
 
 
 def test_wait_limit_rejects_negative_values(g):
