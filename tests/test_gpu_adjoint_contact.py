@@ -16,19 +16,23 @@ vertex):
   matrix at x*: 1e-9 relative;
 * the adjoint with the exact Hessian of the energy (the Jacobian of the GPU gradient,
   applied as central differences of the gradient, solved by iterative refinement
-  preconditioned with the projected matrix to 1e-12), against central finite differences of
-  the converged step's loss (h = 1e-6, relative to each parameter): 2e-3 relative;
+  preconditioned with the projected matrix, to the 1e-5 floor the differenced products
+  leave), against central finite differences of the converged step's loss (h = 1e-6,
+  relative to each parameter): 1e-3 relative (measured: 1e-7 to 5e-5);
 * the shipped adjoint against the exact-Hessian one: the gap the PSD projection causes.
   The barrier's Gauss-Newton form (the distance Hessian term dropped), the mollifier's and
   friction's 2x2 projections and the stable Neo-Hookean projection (GIPC.cu:3106-4945,
   1439-1800; femEnergy.cu:1593-1717) make A differ from the true Hessian; on this step the
-  gradients differ by 0.3 % to 1 %.  The test bounds the gap by 3e-2 and requires it to be
+  gradients differ by 0.5 % to 1.6 %.  The test bounds the gap by 3e-2 and requires it to be
   above the finite-difference error, so it reports a real gap, not noise.
 
 Lagged friction: the friction sets (pairs, normal forces, tangent bases) are those of the
 frame start, as in the reference (buildFrictionSets once per frame, GIPC.cu:11119), so they
 do not depend on E or v0 and the adjoint differentiates the lagged step exactly; the
-finite differences above are of that lagged step.
+finite differences above are of that lagged step.  What lagging leaves out is how the
+normal forces and bases would follow the parameters: on this step (vertices resting 0.007
+d-hat above the ground, where the normal force is steep) finite differences of a step whose
+friction is re-lagged once at its own x* differ from the lagged gradient by 100 % or more.
 """
 import numpy as np
 import pytest
@@ -172,10 +176,12 @@ def test_finite_differences_and_the_projection_gap(c5):
     lam = a_inv(b)
     for _ in range(12):
         res = b - hess_vec(lam)
-        if float(res.norm() / b.norm()) < 1e-12:
+        if float(res.norm() / b.norm()) < 1e-10:
             break
         lam += a_inv(res)
-    assert float((b - hess_vec(lam)).norm() / b.norm()) < 1e-9
+    # the central-difference products carry rounding of order 1e-5 of |H lam|, which is
+    # where the refinement stops
+    assert float((b - hess_vec(lam)).norm() / b.norm()) < 1e-4
     lam_exact = lam.cpu().numpy()
     grad_at(x_star)
     b0 = oracle.assemble(st["host"])[0]
@@ -194,5 +200,5 @@ def test_finite_differences_and_the_projection_gap(c5):
             fd = (st["loss"](lp) - st["loss"](lm)).item() / (2 * h)
         fd_err = abs(fd - exact) / abs(exact)
         gap = abs(shipped - exact) / abs(exact)
-        assert fd_err < 2e-3, (kind, fd, exact)
+        assert fd_err < 1e-3, (kind, fd, exact)
         assert fd_err < gap < 3e-2, (kind, shipped, exact, fd)
