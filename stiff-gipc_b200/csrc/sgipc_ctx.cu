@@ -159,6 +159,37 @@ static SgipcStatus build_static(SgipcCtx* c, const SgipcTopology* t) {
     SG_TRY(upload(c, &c->fcol, fcol));
     SG_TRY(upload(c, &c->fup, fup));
     SG_TRY(upload(c, &c->flo, flo));
+    // column sets of the fused persistent solve: CTA b of a one-CTA-per-SM grid takes rows
+    // [128 b, 128 b + 128); its z values are prolonged once per iteration at the distinct
+    // columns of those rows
+    {
+        int nsm = 0;
+        SG_CHECK(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+        constexpr int rpc = 128;
+        if (nsm > 0 && (long long)nsm * rpc >= n) {
+            std::vector<int> cptr2(nsm + 1, 0), ccols, lcol(std::max(c->nnz_full, 1), 0), dslot(std::max(n, 1), 0);
+            int cap = 0;
+            for (int b = 0; b < nsm; b++) {
+                const int r0 = std::min(n, b * rpc), r1 = std::min(n, r0 + rpc);
+                std::vector<int> set(fcol.begin() + frow[r0], fcol.begin() + frow[r1]);
+                std::sort(set.begin(), set.end());
+                set.erase(std::unique(set.begin(), set.end()), set.end());
+                cap = std::max(cap, (int)set.size());
+                for (int e = frow[r0]; e < frow[r1]; e++)
+                    lcol[e] = (int)(std::lower_bound(set.begin(), set.end(), fcol[e]) - set.begin());
+                for (int i = r0; i < r1; i++) dslot[i] = (int)(std::lower_bound(set.begin(), set.end(), i) - set.begin());
+                ccols.insert(ccols.end(), set.begin(), set.end());
+                cptr2[b + 1] = (int)ccols.size();
+            }
+            if (ccols.empty()) ccols.push_back(0);
+            SG_TRY(upload(c, &c->cs_ptr, cptr2));
+            SG_TRY(upload(c, &c->cs_cols, ccols));
+            SG_TRY(upload(c, &c->cs_lcol, lcol));
+            SG_TRY(upload(c, &c->cs_dslot, dslot));
+            c->cs_grid = nsm;
+            c->cs_cap = cap;
+        }
+    }
     SG_TRY(dalloc(c, &c->fval64, (size_t)c->nnz_full * 9));
     SG_TRY(dalloc(c, &c->fval32, (size_t)c->nnz_full * 9));
     SG_TRY(upload(c, &c->row_ptr, row_ptr));
@@ -301,7 +332,8 @@ extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
                     c->hinges, c->hinge_adj, c->soft_idx, c->shape_grads, c->fb, c->b, c->ckey, c->ckey_s,
                     c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,
                     c->cu_ptr, c->cl_ptr, c->cl_idx, c->lcount, c->lpos, c->cub_tmp, c->dflag,
-                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32, c->run_start, c->en_part, c->en_terms, c->ccd_part, c->ccd_out, c->ccd_bad, c->en_ticket, c->ccd_ticket};
+                    c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32, c->run_start, c->en_part, c->en_terms, c->ccd_part, c->ccd_out, c->ccd_bad, c->en_ticket, c->ccd_ticket,
+                    c->cs_ptr, c->cs_cols, c->cs_lcol, c->cs_dslot};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_en) cudaFreeHost(c->h_en);

@@ -59,10 +59,12 @@ struct PcgWork {
     void* p;
     void* p2;                // second direction buffer (the SpMV forms p = z + beta p_old on the fly)
     void* Ap;
+    void* Ap2;               // second A p buffer of the fused persistent solve
+    void* w;                 // w = A z of the fused persistent solve
     PcgScalars* sc;          // [nrhs]
     double* partial;         // reduction partials [nrhs][max_blocks]
     unsigned int* ticket;    // [0..3] last-block counters; [4..5] grid barrier of the persistent solve
-    double* coop;            // persistent solve: block partials [2][nrhs][coop_cap]
+    double* coop;            // persistent solve: block partials [2][3 nrhs][coop_cap]
     int coop_cap;            // largest grid the persistent solve may use
     cudaGraphExec_t exec;    // captured iteration loop
     bool cond_graph;         // true: while-node graph (whole loop in one launch)
@@ -221,9 +223,19 @@ struct SgipcCtx {
     // launch configuration of the persistent solve per (T, M, NR) instance, computed on its
     // first use (it depends on the device and the static pattern only)
     struct CoopCfg {
-        int valid, usable, grid, ecap, kcap, dcap;
+        int valid, usable, grid, ecap, kcap, dcap, ccap, zextra;
         size_t dyn;
-    } coop_cfg[6];
+    } coop_cfg[6], fused_cfg[6];
+    // column sets of the fused persistent solve, built with the static pattern for a grid of
+    // cs_grid CTAs of 128 rows: per CTA the sorted distinct columns of its rows
+    // (cs_cols[cs_ptr[c] .. cs_ptr[c+1])), each full-pattern entry's slot among them
+    // (cs_lcol) and each row's own slot (cs_dslot); cs_cap = the largest set
+    int* cs_ptr;
+    int* cs_cols;
+    int* cs_lcol;
+    int* cs_dslot;
+    int cs_grid;
+    int cs_cap;
 
     // ---- MAS and PCG ------------------------------------------------------------------
     sgipc::MasWork mas;

@@ -617,7 +617,7 @@ int final_status(SgipcCtx* c, const PcgScalars& s) {
 
 SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
     const size_t n3 = 3 * (size_t)c->n * nrhs;
-    void** vs[] = {&w.x, &w.r, &w.r2, &w.z, &w.p, &w.p2, &w.Ap};
+    void** vs[] = {&w.x, &w.r, &w.r2, &w.z, &w.p, &w.p2, &w.Ap, &w.Ap2, &w.w};
     for (void** v : vs) SG_CHECK(c, cudaMalloc(v, elem * n3));
     SG_CHECK(c, cudaMalloc((void**)&w.sc, sizeof(PcgScalars) * nrhs));
     SG_CHECK(c, cudaMalloc((void**)&w.partial, sizeof(double) * 4 * nrhs * c->max_blocks));
@@ -626,12 +626,12 @@ SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
     SG_CHECK(c, cudaMemset(w.sc, 0, sizeof(PcgScalars) * nrhs));
     w.coop_cap = coop_max_grid(c->device);
     if (w.coop_cap < 1) w.coop_cap = 1;
-    SG_CHECK(c, cudaMalloc((void**)&w.coop, sizeof(double) * 2 * nrhs * (size_t)w.coop_cap));
+    SG_CHECK(c, cudaMalloc((void**)&w.coop, sizeof(double) * 2 * 3 * nrhs * (size_t)w.coop_cap));
     return SGIPC_OK;
 }
 
 void free_work(PcgWork& w) {
-    void* ps[] = {w.x, w.r, w.r2, w.z, w.p, w.p2, w.Ap, w.sc, w.partial, w.ticket, w.coop};
+    void* ps[] = {w.x, w.r, w.r2, w.z, w.p, w.p2, w.Ap, w.Ap2, w.w, w.sc, w.partial, w.ticket, w.coop};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (w.exec) cudaGraphExecDestroy(w.exec);

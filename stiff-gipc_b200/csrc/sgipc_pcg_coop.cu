@@ -90,7 +90,9 @@ enum PhaseTag : int {
     kPhAcc64 = 7,      // refinement: x64 += x
     kPhRes64 = 8,      // refinement: r64 = b64 - A x64
     kPhRestr64 = 9,    // refinement: restriction of r64
-    kPhProlong64 = 10  // refinement: r64 . M r64
+    kPhProlong64 = 10,  // refinement: r64 . M r64
+    kPhFusedA = 11,     // fused: z at the columns, w = A z, r.z, z.w, z.Ap_old
+    kPhFusedB = 12      // fused: p, Ap, x, r, restriction, own level-0/1 domains; r.r, p.Ap
 };
 
 __device__ __forceinline__ void tag_phase(const GridBarrier& br, unsigned int epoch, int tag) {
@@ -139,6 +141,18 @@ struct CoopArgs {
     const double* b64;
     double* r64;
     MatView<double> A64;
+    // fused iteration (k_pcg_fused): w = A z, the second Ap buffer, and per CTA the sorted
+    // distinct columns of its rows (cs_cols[cs_ptr[c] ..]), each static entry's slot among
+    // them (cs_lcol, by full-pattern index) and each row's own slot (cs_dslot); ccap bounds
+    // a CTA's count
+    T* w;
+    T* Ap2;
+    const int* cs_ptr;
+    const int* cs_cols;
+    const int* cs_lcol;
+    const int* cs_dslot;
+    int ccap;
+    int zextra;  // further z slots for the columns of resident contact entries outside the set
 };
 
 __device__ __forceinline__ void red_add_release_gpu(unsigned int* p, unsigned int v) {
@@ -187,11 +201,13 @@ __device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch, int tag)
 // Barrier + sum over CTAs: v[r] is this thread's contribution; on return out[r] holds the
 // grid total in every thread.  The partial buffer of parity epoch & 1 is rewritten two
 // barriers later at the earliest, after every CTA has read it.
+// `stride` (>= NR) is the number of values per CTA that each parity half of the buffer holds
+// (the same for every reduction of a kernel, so that the halves never overlap).
 template <int NR>
 __device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, int tag, double (&v)[NR], double* partial,
-                            double* smem, double (&out)[NR]) {
+                            double* smem, double (&out)[NR], int stride = NR) {
     __shared__ double s_tot[NR];
-    double* part = partial + (size_t)(epoch & 1) * NR * gridDim.x;
+    double* part = partial + (size_t)(epoch & 1) * stride * gridDim.x;
     block_sum<NR>(v, smem);
     if (threadIdx.x == 0)
 #pragma unroll
@@ -745,6 +761,421 @@ __device__ void phase_positions_l2(const CoopArgs<T, M, NR>& a, const double (&a
     }
 }
 
+// ---- fused iteration (three levels or more, every row resident) -----------------------------
+// One iteration in three phases and three grid barriers instead of four:
+//   A  z = M^-1 r prolonged at the columns of the CTA's rows (into shared memory), w = A z
+//      from shared memory, and the dots r.z, z.w, z.Ap_old;
+//   B  beta, alpha from those dots; p = z + beta p_old, Ap = w + beta Ap_old (A symmetric:
+//      p.Ap = z.w + 2 beta z.Ap_old + beta^2 p_old.Ap_old), x += alpha p, r -= alpha Ap,
+//      restriction to levels 0..2; r.r and p.Ap;
+//   C  the MAS domain solves (levels 0..2 over the grid, the levels above on the last CTA).
+// The prolongation needs no phase of its own, and the SpMV reads z from shared memory
+// instead of gathering z and p_old.  p.Ap enters the recurrence from the previous iteration's
+// direct dot.  (Solving each CTA's level-0/1 domains inside B, whose residuals are complete
+// in the CTA, was measured slower: B grew by 6.7 us while C stayed bound by the last CTA's
+// coarse chain.)
+constexpr int kFusedMaxCols = 1024;  // distinct columns of one CTA's rows held in shared memory
+// the column sets are built with the static pattern for CTAs of 128 rows (sgipc_ctx.cu)
+static_assert(kCoopThreads / kSpG == 128, "fused column sets assume 128 rows per CTA");
+
+// shared-memory part of the column set: [table rows (cols x SGIPC_MAX_LEVELS)] [z values]
+__host__ __device__ constexpr size_t fused_cols_bytes(int ccap, int tsize, int nr) {
+    return ccap > 0 ? (size_t)coop_pad4(ccap * SGIPC_MAX_LEVELS) * 4 + (((size_t)ccap * 3 * nr * tsize + 15) & ~(size_t)15)
+                    : 0;
+}
+
+template <class T, int NR>
+struct FusedCache {
+    const int* tab;   // [nc][SGIPC_MAX_LEVELS] cluster of each column at each level
+    T* zs;            // [nc][3][NR] z at the columns
+    const int* dsl;   // [rows] slot of each row's own column
+    int nc;           // the CTA's static columns (slots 0 .. nc-1)
+    int nz;           // slots in use: nc + the contact columns outside the static set
+};
+
+// z at vertex j: the sum over levels of Z at j's clusters (the order of phase_prolong)
+template <class T, class M, int NR>
+__device__ __forceinline__ void prolong_at(const MasView& mv, const M* Z, int j, T (&xj)[NR][3]) {
+    int gl[SGIPC_MAX_LEVELS];
+#pragma unroll
+    for (int l = 0; l < SGIPC_MAX_LEVELS; l++) gl[l] = l < mv.L ? __ldg(mv.table + (size_t)j * mv.L + l) : -1;
+    M sq[3][NR];
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int r = 0; r < NR; r++) sq[q][r] = 0;
+#pragma unroll
+    for (int l = 0; l < SGIPC_MAX_LEVELS; l++) {
+        if (gl[l] < 0) continue;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            M t[NR];
+            ldn<false, M, NR>(Z + (size_t)(3 * gl[l] + q) * NR, t);
+#pragma unroll
+            for (int r = 0; r < NR; r++) sq[q][r] += t[r];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int r = 0; r < NR; r++) xj[r][q] = (T)sq[q][r];
+}
+
+// phase A.  dots[r] += r.z, dots[NR + r] += z.w, dots[2 NR + r] += z.Ap_old (not on the first
+// iteration); z and w of the CTA's rows go to a.z and a.w.
+template <class T, class M, int NR>
+__device__ void phase_fused_spmv(const CoopArgs<T, M, NR>& a, const RowCache<T>& rc, const FusedCache<T, NR>& fc,
+                                 const T* rcur, const T* ap_old, bool first, const bool (&run)[NR],
+                                 double (&dots)[3 * NR]) {
+    const MasView& mv = a.mv;
+    constexpr int gpw = 32 / kSpG;
+    const int lane = threadIdx.x & 31, g = lane % kSpG;
+    const int i = rc.r0 + (int)(threadIdx.x >> 5) * gpw + lane / kSpG;
+    // r and Ap_old of the row, issued before the z gathers (they do not depend on them)
+    T rpre[3][NR], apre[3][NR];
+    if (i < rc.r1 && g == 0) {
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const size_t k = (size_t)(3 * i + q) * NR;
+            ldn<true, T, NR>(rcur + k, rpre[q]);
+            if (!first) ldn<true, T, NR>(ap_old + k, apre[q]);
+        }
+    }
+    // z at the CTA's columns (their cluster tables are resident)
+    for (int s = threadIdx.x; s < fc.nz; s += blockDim.x) {
+        M sq[3][NR];
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) sq[q][r] = 0;
+#pragma unroll
+        for (int l = 0; l < SGIPC_MAX_LEVELS; l++) {
+            if (l >= mv.L) break;
+            const int g = fc.tab[s * SGIPC_MAX_LEVELS + l];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                M t[NR];
+                ldn<false, M, NR>(a.Z + (size_t)(3 * g + q) * NR, t);
+#pragma unroll
+                for (int r = 0; r < NR; r++) sq[q][r] += t[r];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            T zz[NR];
+#pragma unroll
+            for (int r = 0; r < NR; r++) zz[r] = (T)sq[q][r];
+            stn<T, NR>(fc.zs + ((size_t)s * 3 + q) * NR, zz);
+        }
+    }
+    __syncthreads();
+    // w = A z over the CTA's rows: static entries from shared memory, contact entries from
+    // their z slots (or prolonged at their columns)
+    T acc[NR][3];
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r][0] = acc[r][1] = acc[r][2] = 0;
+    if (i < rc.r1) {
+        const int li = i - rc.r0;
+        const int s0 = rc.rp[li], s1 = rc.rp[li + 1];
+        for (int e = s0 + g; e < s1; e += kSpG) {
+            const T* bv = rc.val + 9 * e;
+            const T* zp = fc.zs + (size_t)rc.col[e] * 3 * NR;
+            T x3[3][NR];
+#pragma unroll
+            for (int q = 0; q < 3; q++) ldn<false, T, NR>(zp + q * NR, x3[q]);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                acc[r][0] += bv[0] * x3[0][r] + bv[1] * x3[1][r] + bv[2] * x3[2][r];
+                acc[r][1] += bv[3] * x3[0][r] + bv[4] * x3[1][r] + bv[5] * x3[2][r];
+                acc[r][2] += bv[6] * x3[0][r] + bv[7] * x3[1][r] + bv[8] * x3[2][r];
+            }
+        }
+        int u0, nu, l0, nl;
+        const int* kc;
+        const T* kv;
+        if (rc.kcol) {
+            u0 = rc.ru[li], nu = rc.ru[li + 1] - u0, l0 = rc.rl[li], nl = rc.rl[li + 1] - l0;
+            kc = rc.kcol, kv = rc.kval;
+        } else {
+            u0 = a.tp.cu_ptr[i], nu = a.tp.cu_ptr[i + 1] - u0, l0 = a.tp.cl_ptr[i], nl = a.tp.cl_ptr[i + 1] - l0;
+            kc = nullptr, kv = nullptr;
+        }
+        for (int e = g; e < nu + nl; e += kSpG) {
+            const bool up = e < nu;
+            int cj;
+            const T* src;
+            if (kc) {  // resident: a z slot (>= 0), or -(column + 1) beyond the slots
+                const int k = up ? u0 + e : l0 + (e - nu);
+                cj = kc[k];
+                src = kv + 9 * (size_t)k;
+            } else {
+                cj = -1 - (up ? __ldg(a.tp.uc_col + u0 + e) : __ldg(a.tp.cl_col + l0 + (e - nu)));
+                src = up ? a.A.uc + 9 * (size_t)(u0 + e) : a.A.cl + 9 * (size_t)(l0 + (e - nu));
+            }
+            T xb[NR][3];
+            if (cj >= 0) {
+                const T* zp = fc.zs + (size_t)cj * 3 * NR;
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    T t3[NR];
+                    ldn<false, T, NR>(zp + q * NR, t3);
+#pragma unroll
+                    for (int r = 0; r < NR; r++) xb[r][q] = t3[r];
+                }
+            } else {
+                prolong_at<T, M, NR>(mv, a.Z, -1 - cj, xb);
+            }
+            T bv[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) bv[q] = kc ? src[q] : __ldg(src + q);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                acc[r][0] += bv[0] * xb[r][0] + bv[1] * xb[r][1] + bv[2] * xb[r][2];
+                acc[r][1] += bv[3] * xb[r][0] + bv[4] * xb[r][1] + bv[5] * xb[r][2];
+                acc[r][2] += bv[6] * xb[r][0] + bv[7] * xb[r][1] + bv[8] * xb[r][2];
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int o = 1; o < kSpG; o <<= 1) acc[r][q] += __shfl_xor_sync(0xffffffffu, acc[r][q], o, kSpG);
+    if (i < rc.r1 && g == 0) {
+        const T* zp = fc.zs + (size_t)fc.dsl[i - rc.r0] * 3 * NR;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const size_t k = (size_t)(3 * i + q) * NR;
+            T zv[NR], wv[NR];
+            ldn<false, T, NR>(zp + q * NR, zv);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                wv[r] = acc[r][q];
+                if (run[r]) {
+                    dots[r] += (double)rpre[q][r] * (double)zv[r];
+                    dots[NR + r] += (double)zv[r] * (double)wv[r];
+                    if (!first) dots[2 * NR + r] += (double)zv[r] * (double)apre[q][r];
+                }
+            }
+            stn<T, NR>(a.z + k, zv);
+            stn<T, NR>(a.w + k, wv);
+        }
+    }
+}
+
+// The CTA's first level-1 bank m = blockIdx.x as the update pass reads it, kept in shared
+// memory for the solve (the hierarchy is fixed during a solve): its level-0 bank range, the
+// vertex and local level-1 parent of each position of the first kPosBanks banks of the range,
+// and the level-2 parent of each of its level-1 nodes.
+constexpr int kPosBanks = 32;
+struct PosCache {
+    int b_lo, b_hi;
+    const int* v;    // [kPosBanks * 16]
+    const int* par;  // [kPosBanks * 16] local level-1 id (up - start1), -1 without a vertex
+    const int* up1;  // [16]
+    bool valid;
+};
+
+// Phase B: the position pass of phase_positions_l2 (update mode) on the fused recurrence.
+// acc[r] += r.r, acc[NR + r] += p.Ap (owners).  A stopped right-hand side keeps x, r, p and
+// Ap (selected, never multiplied).
+template <class T, class M, int NR>
+__device__ void phase_fused_update(const CoopArgs<T, M, NR>& a, const double (&alpha)[NR], const double (&beta)[NR],
+                                   bool first, const T* p_old, T* p_new, const T* ap_old, T* ap_new, const T* r_old,
+                                   T* r_new, const bool (&run)[NR], double (&acc)[2 * NR], M (*s_l1)[3 * NR],
+                                   const PosCache& pc) {
+    const MasView& mv = a.mv;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int start1 = mv.info[1], count1 = mv.info[9];
+    const int nb1 = (count1 + 15) >> 4;
+    for (int m = blockIdx.x; m < nb1; m += gridDim.x) {  // block-uniform
+        const bool cached = pc.valid && m == (int)blockIdx.x;
+        const int b_lo = cached ? pc.b_lo : __ldg(a.l1_first + m), b_hi = cached ? pc.b_hi : __ldg(a.l1_last + m);
+        const int id_lo = 16 * m, id_hi = min(16 * m + 16, count1);
+        for (int b0 = b_lo + 2 * w; b0 <= b_hi; b0 += 2 * (kCoopThreads / 32)) {  // warp-uniform
+            const int bank = b0 + (lane >> 4);
+            const int pos = bank * 16 + (lane & 15);
+            int v, par;
+            if (cached && bank - b_lo < kPosBanks) {
+                v = bank <= b_hi ? pc.v[pos - 16 * b_lo] : -1;
+                par = bank <= b_hi ? pc.par[pos - 16 * b_lo] : -1;
+            } else {
+                v = bank <= b_hi ? __ldg(mv.part_map + pos) : -1;
+                par = v >= 0 ? __ldg(mv.up + pos) - start1 : -1;
+            }
+            int firstc = par >= 0 ? par : 0x7fffffff;
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) firstc = min(firstc, __shfl_xor_sync(0xffffffffu, firstc, o, 16));
+            const bool own = firstc >= id_lo;
+            M val[NR * 3];
+#pragma unroll
+            for (int k = 0; k < NR * 3; k++) val[k] = 0;
+            if (v >= 0) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    const size_t k = (size_t)(3 * v + q) * NR;
+                    T zv[NR], wv[NR], po[NR], ao[NR], rv[NR], xv[NR];
+                    ldn<true, T, NR>(a.z + k, zv);
+                    ldn<true, T, NR>(a.w + k, wv);
+                    ldn<true, T, NR>(r_old + k, rv);
+                    if (!first) {
+                        ldn<true, T, NR>(p_old + k, po);
+                        ldn<true, T, NR>(ap_old + k, ao);
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < NR; r++) po[r] = ao[r] = 0;
+                    }
+#pragma unroll
+                    for (int r = 0; r < NR; r++) xv[r] = 0;
+                    if (own) ldn<true, T, NR>(a.x + k, xv);
+                    T pn[NR], an[NR];
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        const T al = (T)alpha[r], be = (T)beta[r];
+                        pn[r] = po[r];
+                        an[r] = ao[r];
+                        if (run[r]) {
+                            pn[r] = first ? zv[r] : zv[r] + be * po[r];
+                            an[r] = first ? wv[r] : wv[r] + be * ao[r];
+                            rv[r] = rv[r] - al * an[r];
+                            xv[r] = xv[r] + al * pn[r];
+                            if (own) {
+                                acc[r] += (double)rv[r] * (double)rv[r];
+                                acc[NR + r] += (double)pn[r] * (double)an[r];
+                            }
+                        }
+                        val[r * 3 + q] = run[r] ? (M)rv[r] : (M)0;
+                    }
+                    if (own) {
+                        stn<T, NR>(a.x + k, xv);
+                        stn<T, NR>(r_new + k, rv);
+                        stn<T, NR>(p_new + k, pn);
+                        stn<T, NR>(ap_new + k, an);
+                    }
+                }
+            }
+            if (own && bank <= b_hi) store_levels01<M, NR>(a.R, pos, val);
+            const int gp = (par >= id_lo && par < id_hi) ? par : -1;
+            M sum[NR * 3];
+            const bool lead = bank_group_sum<M, NR>(gp, val, sum);
+            if (lead && gp >= 0) {
+#pragma unroll
+                for (int k = 0; k < NR * 3; k++) s_l1[gp - id_lo][k] = sum[k];
+                store_levels01<M, NR>(a.R, start1 + gp, sum);
+            }
+        }
+        __syncthreads();
+        if (w == 0) {
+            const int a1 = id_lo + (lane & 15);
+            const bool ok = lane < 16 && a1 < id_hi;
+            M v1[NR * 3];
+#pragma unroll
+            for (int k = 0; k < NR * 3; k++) v1[k] = ok ? s_l1[lane & 15][k] : (M)0;
+            bank_reduce_store<M, NR>(ok ? (cached ? pc.up1[lane & 15] : __ldg(mv.up + start1 + a1)) : -1, v1, a.R);
+        }
+        __syncthreads();
+    }
+}
+
+// The coarse chain in shared memory: R of levels >= 3 lives in `cb` (the CTA's staging
+// array, 160 nodes), restricted from R2 with the half-warp groups of restrict_coarse_cta (the
+// same sums), and the domains of levels >= 3 are solved from it, their inverses from `cache`
+// (ncache of them, from domain nd2 on) or global memory.  Only Z is written.  Returns false
+// (nothing done) when the levels above 2 hold more than 160 nodes.
+template <class T, class M, int NR>
+__device__ bool coarse_chain_smem(const CoopArgs<T, M, NR>& a, M* cb, const M* cache, int ncache) {
+    const int* info = a.mv.info;
+    const int L = a.mv.L;
+    const int start3 = info[3];
+    const int ntop = info[16] - start3;  // nodes of levels >= 3, padding included
+    if (ntop > 160 || ntop <= 0) return false;
+    for (int k = threadIdx.x; k < ntop * 3 * NR; k += blockDim.x) cb[k] = 0;
+    __syncthreads();
+    for (int l = 2; l + 1 < L; l++) {
+        const int count = info[8 + l], start = info[l];
+        for (int base = 0; base < count; base += blockDim.x) {
+            const int aa = base + threadIdx.x;
+            M v[NR * 3];
+            int par = -1;
+            if (aa < count) {
+                const int g = start + aa;
+                par = __ldg(a.mv.up + g);
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    M t[NR];
+                    if (l == 2) ldn<true, M, NR>(a.R + (size_t)(3 * g + q) * NR, t);
+                    else ldn<false, M, NR>(cb + (size_t)(3 * (g - start3) + q) * NR, t);
+#pragma unroll
+                    for (int r = 0; r < NR; r++) v[r * 3 + q] = t[r];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < NR * 3; k++) v[k] = 0;
+            }
+            M sum[NR * 3];
+            const bool lead = bank_group_sum<M, NR>(par, v, sum);
+            if (par >= 0 && lead) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    M o[NR];
+#pragma unroll
+                    for (int r = 0; r < NR; r++) o[r] = sum[r * 3 + q];
+                    stn<M, NR>(cb + (size_t)(3 * (par - start3) + q) * NR, o);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // Z = A_d^-1 R_d for the domains of levels >= 3, kDomPerCta per round
+    const int ld = threadIdx.x / 48, i = threadIdx.x % 48;
+    for (int d0 = a.nd2; d0 < a.ndom; d0 += kDomPerCta) {
+        const int d = d0 + ld;
+        if (ld < kDomPerCta && d < a.ndom) {
+            const int slot = d - a.nd2;
+            const bool sm = slot < ncache;
+            const M* Ad = sm ? cache + (size_t)slot * 2304 : a.inv + (size_t)d * 2304;
+            const M* Rd = cb + (size_t)(48 * d - 3 * start3) * NR;
+            M acc[NR];
+#pragma unroll
+            for (int r = 0; r < NR; r++) acc[r] = 0;
+            constexpr int kU = sizeof(M) == 4 ? (NR == 1 ? 24 : 12) : (NR == 1 ? 12 : 6);
+#pragma unroll
+            for (int j0 = 0; j0 < 48; j0 += kU) {
+                M wv[kU];
+#pragma unroll
+                for (int j = 0; j < kU; j++) wv[j] = sm ? Ad[(j0 + j) * 48 + i] : __ldg(Ad + (j0 + j) * 48 + i);
+#pragma unroll
+                for (int j = 0; j < kU; j++) {
+                    M rj[NR];
+                    ldn<false, M, NR>(Rd + (size_t)(j0 + j) * NR, rj);
+#pragma unroll
+                    for (int r = 0; r < NR; r++) acc[r] += wv[j] * rj[r];
+                }
+            }
+            stn<M, NR>(a.Z + (48 * (size_t)d + i) * NR, acc);
+        }
+    }
+    __syncthreads();  // cb is the staging array of the next phase's solves
+    return true;
+}
+
+// Phase C: the MAS domain solves, levels 0..2 over the grid while (with more levels) the
+// last CTA restricts 2 -> 3 -> ... and solves the domains above, in shared memory where the
+// levels above 2 fit (coarse_chain_smem), else as the MAS phase of k_pcg_coop.
+template <class T, class M, int NR>
+__device__ void phase_fused_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], const M* dcache, int ndc) {
+    const int L = a.mv.L, G = gridDim.x;
+    if (L > 3 && blockIdx.x == G - 1) {
+        if (!coarse_chain_smem<T, M, NR>(a, &sR[0][0], dcache, ndc)) {
+            restrict_coarse_cta<M, NR, true>(a.mv.info, a.mv.up, L, a.R, 2);
+            solve_domain_range<M, NR>(a.inv, a.R, a.Z, a.nd2, a.ndom, G - 1, 1, sR);
+        }
+    } else {
+        solve_domain_range<M, NR>(a.inv, a.R, a.Z, 0, a.nd2, 0, L > 3 ? G - 1 : G, sR, dcache, ndc);
+    }
+}
+
 // ---- refinement epilogue of the mixed solve (FP32 inner solve, one right-hand side) --------
 // x64 += x (the inner solve's correction)
 template <class T, class M, int NR>
@@ -1026,6 +1457,302 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
     }
 }
 
+
+// ---- the fused solve ------------------------------------------------------------------------
+template <int NR>
+struct FusedState {
+    double rz0[NR], rz[NR], bn2[NR], rr[NR], beta[NR], alpha[NR], pap[NR];
+    int iters[NR], status[NR];
+    bool run[NR], stop_rz[NR];
+};
+
+template <class T, class M, int NR>
+__global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a) {
+    __shared__ double smem[3 * NR * 32];
+    __shared__ __align__(16) M sR[kDomPerCta][48 * NR];
+    __shared__ __align__(16) M s_l1[16][3 * NR];
+    extern __shared__ __align__(16) unsigned char dsm[];
+    unsigned int epoch = 0;
+    if (threadIdx.x == 0) stamp(a.br, 0, 0);
+    constexpr int rpc = kCoopThreads / kSpG;
+    __shared__ RowCache<T> rcs;
+    __shared__ FusedCache<T, NR> fcs;
+    __shared__ int s_pv[kPosBanks * 16], s_ppar[kPosBanks * 16], s_pup1[16];
+    __shared__ PosCache pcs;
+    const M* dcache = nullptr;
+    int ndc = 0;
+    {
+        // the update pass's view of the first level-1 bank (PosCache)
+        {
+            const int start1 = a.mv.info[1], count1 = a.mv.info[9];
+            const int m = blockIdx.x;
+            PosCache pc{0, -1, s_pv, s_ppar, s_pup1, false};
+            if (m < ((count1 + 15) >> 4)) {
+                pc.b_lo = __ldg(a.l1_first + m);
+                pc.b_hi = __ldg(a.l1_last + m);
+                pc.valid = true;
+                const int nb = min(kPosBanks, pc.b_hi - pc.b_lo + 1);
+                for (int k = threadIdx.x; k < nb * 16; k += blockDim.x) {
+                    const int pos = 16 * pc.b_lo + k;
+                    const int v = __ldg(a.mv.part_map + pos);
+                    s_pv[k] = v;
+                    s_ppar[k] = v >= 0 ? __ldg(a.mv.up + pos) - start1 : -1;
+                }
+                if (threadIdx.x < 16) {
+                    const int a1 = 16 * m + threadIdx.x;
+                    s_pup1[threadIdx.x] = a1 < count1 ? __ldg(a.mv.up + start1 + a1) : -1;
+                }
+            }
+            if (threadIdx.x == 0) pcs = pc;
+        }
+        // rows (static entries with their column slots), contact entries, the column set
+        // (cluster tables, z slots), each row's own slot, the own domain inverses
+        int* rp = reinterpret_cast<int*>(dsm);
+        int* ccol = rp + coop_pad4(rpc + 1);
+        T* cval = reinterpret_cast<T*>(ccol + coop_pad4(a.ecap));
+        unsigned char* after_rows = dsm + coop_rows_bytes(rpc, a.ecap, sizeof(T));
+        int* ru = reinterpret_cast<int*>(after_rows);
+        int* rl = ru + coop_pad4(rpc + 1);
+        int* kcol = rl + coop_pad4(rpc + 1);
+        T* kval = reinterpret_cast<T*>(kcol + coop_pad4(a.kcap));
+        unsigned char* after_con = after_rows + coop_contact_bytes(rpc, a.kcap, sizeof(T));
+        const int zcap = a.ccap + a.zextra;
+        int* tab = reinterpret_cast<int*>(after_con);
+        T* zs = reinterpret_cast<T*>(tab + coop_pad4(zcap * SGIPC_MAX_LEVELS));
+        unsigned char* after_cols = after_con + fused_cols_bytes(zcap, sizeof(T), NR);
+        int* dsl = reinterpret_cast<int*>(after_cols);
+        M* dom = reinterpret_cast<M*>(after_cols + (size_t)coop_pad4(rpc) * 4);
+        RowCache<T> rc{rp, ccol, cval, 0, 0, nullptr, nullptr, nullptr, nullptr};
+        FusedCache<T, NR> fc{tab, zs, dsl, 0, 0};
+        __shared__ int s_extra;
+        const int r0 = blockIdx.x * rpc, r1 = min(a.tp.n, r0 + rpc);
+        if (r0 < r1) {
+            const int e0 = __ldg(a.tp.frow_ptr + r0), e1 = __ldg(a.tp.frow_ptr + r1);
+            for (int k = threadIdx.x; k <= r1 - r0; k += blockDim.x) rp[k] = __ldg(a.tp.frow_ptr + r0 + k) - e0;
+            for (int k = threadIdx.x; k < e1 - e0; k += blockDim.x) ccol[k] = __ldg(a.cs_lcol + e0 + k);
+            for (int k = threadIdx.x; k < 9 * (e1 - e0); k += blockDim.x) cval[k] = __ldg(a.A.fval + 9 * (size_t)e0 + k);
+            for (int k = threadIdx.x; k < r1 - r0; k += blockDim.x) dsl[k] = __ldg(a.cs_dslot + r0 + k);
+            rc.r0 = r0;
+            rc.r1 = r1;
+            const int u0 = __ldg(a.tp.cu_ptr + r0), u1 = __ldg(a.tp.cu_ptr + r1);
+            const int q0 = __ldg(a.tp.cl_ptr + r0), q1 = __ldg(a.tp.cl_ptr + r1);
+            const int nu = u1 - u0, nl = q1 - q0;
+            if (a.kcap > 0 && nu + nl <= a.kcap) {
+                for (int k = threadIdx.x; k <= r1 - r0; k += blockDim.x) {
+                    ru[k] = __ldg(a.tp.cu_ptr + r0 + k) - u0;
+                    rl[k] = __ldg(a.tp.cl_ptr + r0 + k) - q0 + nu;
+                }
+                for (int k = threadIdx.x; k < nu; k += blockDim.x) kcol[k] = __ldg(a.tp.uc_col + u0 + k);
+                for (int k = threadIdx.x; k < nl; k += blockDim.x) kcol[nu + k] = __ldg(a.tp.cl_col + q0 + k);
+                for (int k = threadIdx.x; k < 9 * nu; k += blockDim.x) kval[k] = __ldg(a.A.uc + 9 * (size_t)u0 + k);
+                for (int k = threadIdx.x; k < 9 * nl; k += blockDim.x)
+                    kval[9 * nu + k] = __ldg(a.A.cl + 9 * (size_t)q0 + k);
+                rc.ru = ru;
+                rc.rl = rl;
+                rc.kcol = kcol;
+                rc.kval = kval;
+            }
+            const int c0 = __ldg(a.cs_ptr + blockIdx.x);
+            fc.nc = __ldg(a.cs_ptr + blockIdx.x + 1) - c0;
+            for (int k = threadIdx.x; k < fc.nc * SGIPC_MAX_LEVELS; k += blockDim.x) {
+                const int s = k / SGIPC_MAX_LEVELS, l = k % SGIPC_MAX_LEVELS;
+                tab[k] = l < a.mv.L ? __ldg(a.mv.table + (size_t)__ldg(a.cs_cols + c0 + s) * a.mv.L + l) : -1;
+            }
+            // resident contact entries: the slot of their column in the static set, or a slot of
+            // their own (the z values, not the slot numbers, enter the products: the atomic
+            // order of the extra slots changes nothing), or -(column + 1) beyond the slots
+            fc.nz = fc.nc;
+            if (rc.kcol) {
+                int* scol = reinterpret_cast<int*>(zs);  // the sorted set, during this set-up only
+                for (int k = threadIdx.x; k < fc.nc; k += blockDim.x) scol[k] = __ldg(a.cs_cols + c0 + k);
+                if (threadIdx.x == 0) s_extra = 0;
+                __syncthreads();
+                for (int k = threadIdx.x; k < nu + nl; k += blockDim.x) {
+                    const int col = kcol[k];
+                    int lo = 0, hi = fc.nc;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (scol[mid] < col) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    int slot;
+                    if (lo < fc.nc && scol[lo] == col) {
+                        slot = lo;
+                    } else {
+                        const int x = atomicAdd(&s_extra, 1);
+                        slot = x < a.zextra ? fc.nc + x : -1 - col;
+                        if (x < a.zextra)
+                            for (int l = 0; l < SGIPC_MAX_LEVELS; l++)
+                                tab[(size_t)(fc.nc + x) * SGIPC_MAX_LEVELS + l] =
+                                    l < a.mv.L ? __ldg(a.mv.table + (size_t)col * a.mv.L + l) : -1;
+                    }
+                    kcol[k] = slot;
+                }
+                __syncthreads();
+                fc.nz = fc.nc + min(s_extra, a.zextra);
+            }
+        }
+        // the first round of the CTA's level-0..2 domains in the MAS phase (as k_pcg_coop);
+        // with more than three levels the last CTA takes the domains above level 2 instead
+        if (a.dcap > 0) {
+            const bool chain = a.mv.L > 3 && blockIdx.x == gridDim.x - 1;
+            const int d0 = chain ? a.nd2 : (int)blockIdx.x * kDomPerCta;
+            ndc = max(0, min(a.dcap, (chain ? a.ndom : a.nd2) - d0));
+            for (int k = threadIdx.x; k < ndc * 2304; k += blockDim.x) dom[k] = __ldg(a.inv + 2304 * (size_t)d0 + k);
+            dcache = dom;
+        }
+        if (threadIdx.x == 0) {
+            rcs = rc;
+            fcs = fc;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) stamp(a.br, 0, 1);
+    }
+    __shared__ FusedState<NR> S;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            S.run[r] = true;
+            S.stop_rz[r] = false;
+            S.iters[r] = 0;
+            S.status[r] = SGIPC_OK;
+            S.rz0[r] = S.rz[r] = S.rr[r] = S.bn2[r] = S.beta[r] = S.alpha[r] = S.pap[r] = 0.0;
+        }
+    double v[NR], t[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) v[r] = 0.0;
+    // ---- r = b, x = 0, R at levels 0..2, the CTA's level-0/1 domain solves; ||b||^2
+    T* rcur = a.r;
+    T* ralt = a.r2;
+    T* pcur = a.p0;
+    T* palt = a.p1;
+    T* acur = a.Ap;
+    T* aalt = a.Ap2;
+    phase_positions_l2<T, M, NR, 1>(a, S.alpha, nullptr, nullptr, rcur, S.run, v, s_l1);
+    bool ok = grid_reduce<NR>(a.br, ++epoch, kPhInit, v, a.partial, smem, t, 3 * NR);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int r = 0; r < NR; r++) S.bn2[r] = S.rr[r] = t[r];
+    if (ok) phase_fused_mas<T, M, NR>(a, sR, dcache, ndc);
+    ok = ok && grid_barrier(a.br, ++epoch, kPhMas);
+    for (int k = 1; ok; k++) {
+        // ---- A: z, w = A z, r.z, z.w, z.Ap_old
+        double d3[3 * NR], t3[3 * NR];
+#pragma unroll
+        for (int q = 0; q < 3 * NR; q++) d3[q] = 0.0;
+        __syncthreads();  // S read below is settled
+        phase_fused_spmv<T, M, NR>(a, rcs, fcs, rcur, acur, k == 1, S.run, d3);
+        if (!(ok = grid_reduce<3 * NR>(a.br, ++epoch, kPhFusedA, d3, a.partial, smem, t3, 3 * NR))) break;
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                S.stop_rz[r] = false;
+                S.alpha[r] = 0.0;
+                if (!S.run[r]) continue;
+                const double rz = t3[r], zw = t3[NR + r], zap = t3[2 * NR + r];
+                if (k == 1) {
+                    S.rz0[r] = S.rz[r] = rz;
+                    if (!(rz > 0.0) || !isfinite(rz)) {
+                        // b = 0 (or an indefinite preconditioner): nothing to iterate
+                        S.run[r] = false;
+                        if (!isfinite(rz) || rz < 0.0) S.status[r] = SGIPC_BREAKDOWN;
+                        continue;
+                    }
+                }
+                if (k >= a.max_iter) continue;  // the iteration cap: no update
+                const double beta = k == 1 ? 0.0 : rz / S.rz[r];
+                const double pAp = k == 1 ? zw : zw + 2.0 * beta * zap + beta * beta * S.pap[r];
+                S.iters[r] = k;
+                if (!(pAp > 0.0) || !isfinite(pAp) || !isfinite(rz)) {
+                    S.run[r] = false;
+                    S.status[r] = SGIPC_BREAKDOWN;
+                    continue;
+                }
+                S.beta[r] = beta;
+                S.alpha[r] = rz / pAp;
+                S.rz[r] = rz;
+                // the reference tests the r.z of the current iterate and stops after its update
+                S.stop_rz[r] = a.crit == SGIPC_CRIT_RZ && fabs(rz) <= a.tol * S.rz0[r];
+            }
+        __syncthreads();
+        bool any = false;
+#pragma unroll
+        for (int r = 0; r < NR; r++) any |= S.run[r];
+        if (!any || k >= a.max_iter) break;
+        // ---- B: p, Ap, x, r, restriction to levels 0..2; r.r, p.Ap
+        double d2[2 * NR], t2[2 * NR];
+#pragma unroll
+        for (int q = 0; q < 2 * NR; q++) d2[q] = 0.0;
+        phase_fused_update<T, M, NR>(a, S.alpha, S.beta, k == 1, pcur, palt, acur, aalt, rcur, ralt, S.run, d2, s_l1,
+                                     pcs);
+        T* tmp = rcur;
+        rcur = ralt;
+        ralt = tmp;
+        tmp = pcur;
+        pcur = palt;
+        palt = tmp;
+        tmp = acur;
+        acur = aalt;
+        aalt = tmp;
+        if (!(ok = grid_reduce<2 * NR>(a.br, ++epoch, kPhFusedB, d2, a.partial, smem, t2, 3 * NR))) break;
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                if (!S.run[r]) continue;
+                S.rr[r] = t2[r];
+                S.pap[r] = t2[NR + r];
+                if (S.stop_rz[r] || (a.crit == SGIPC_CRIT_TRUE && t2[r] <= a.tol * a.tol * S.bn2[r])) S.run[r] = false;
+            }
+        __syncthreads();
+        any = false;
+#pragma unroll
+        for (int r = 0; r < NR; r++) any |= S.run[r];
+        if (!any || k + 1 >= a.max_iter) break;  // converged, or the iteration cap
+        // ---- C: the MAS domain solves
+        phase_fused_mas<T, M, NR>(a, sR, dcache, ndc);
+        if (!(ok = grid_barrier(a.br, ++epoch, kPhMas))) break;
+    }
+    double rz_ref = 0.0, rr_ref = 0.0;
+    if constexpr (sizeof(T) == 4 && NR == 1) {
+        if (ok && a.x64) {
+            // x64 += x; r64 = b64 - A x64; r64 . r64; M r64 (FP32 MAS); r64 . M r64
+            phase_accumulate64(a);
+            ok = grid_barrier(a.br, ++epoch, kPhAcc64);
+            v[0] = 0.0;
+            if (ok) phase_residual64(a, v[0]);
+            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhRes64, v, a.partial, smem, t, 3 * NR);
+            rr_ref = t[0];
+            v[0] = 0.0;
+            if (ok) phase_positions_l2<T, M, NR, 2>(a, S.alpha, nullptr, nullptr, nullptr, S.run, v, s_l1);
+            ok = ok && grid_barrier(a.br, ++epoch, kPhRestr64);
+            if (ok) phase_fused_mas<T, M, NR>(a, sR, dcache, ndc);
+            ok = ok && grid_barrier(a.br, ++epoch, kPhMas);
+            v[0] = 0.0;
+            if (ok) phase_prolong_ref(a, v[0]);
+            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhProlong64, v, a.partial, smem, t, 3 * NR);
+            rz_ref = t[0];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            PcgScalars& sc = a.sc[r];
+            sc.rz_ref = rz_ref;
+            sc.rr_ref = rr_ref;
+            sc.iter = S.iters[r];
+            sc.rz0 = S.rz0[r];
+            sc.rz = S.rz[r];
+            sc.rz_next = S.rz[r];
+            sc.bnorm2 = S.bn2[r];
+            sc.rr = S.rr[r];
+            sc.bodies = 0;
+            sc.halt = 1;
+            sc.state = ok ? (S.run[r] ? 0 : 2) : 2;
+            sc.status = ok ? S.status[r] : SGIPC_CUDA_ERROR;
+        }
+    }
+}
+
 // ---- host launcher ----------------------------------------------------------------------------
 // Launch configuration of one instance on this context (device attributes, shared-memory
 // residency sizes, occupancy): computed once, it depends only on the device and the static
@@ -1089,6 +1816,66 @@ SgipcStatus coop_configure(SgipcCtx* c, SgipcCtx::CoopCfg& cfg) {
     return SGIPC_OK;
 }
 
+// The fused solve's configuration: one CTA per SM, every row resident (static and, when they
+// fit, contact entries), the column sets of the context (built for this grid), then as many of
+// the CTA's first round of MAS domain inverses as still fit.  usable = 0 sends the solve to
+// k_pcg_coop.
+template <class T, class M, int NR>
+SgipcStatus fused_configure(SgipcCtx* c, SgipcCtx::CoopCfg& cfg) {
+    cfg = SgipcCtx::CoopCfg{};
+    cfg.valid = 1;
+    int coop = 0, nsm = 0, per = 0, optin = 0;
+    SG_CHECK(c, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
+    SG_CHECK(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    SG_CHECK(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    constexpr int rpc = kCoopThreads / kSpG;
+    if (!coop || !c->cs_ptr || c->cs_grid != nsm || c->cs_cap > kFusedMaxCols || !c->h_frow_ptr ||
+        (long long)nsm * rpc < c->n || nsm > c->pcg64.coop_cap || nsm > c->pcg32.coop_cap)
+        return SGIPC_OK;
+    const void* fn = (const void*)k_pcg_fused<T, M, NR>;
+    cudaFuncAttributes fa;
+    SG_CHECK(c, cudaFuncGetAttributes(&fa, fn));
+    const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
+    int ecap = 0;
+    for (int b = 0; b * rpc < c->n; b++) {
+        const int r0 = b * rpc, r1 = r0 + rpc < c->n ? r0 + rpc : c->n;
+        const int e = c->h_frow_ptr[r1] - c->h_frow_ptr[r0];
+        if (e > ecap) ecap = e;
+    }
+    const int ccap = c->cs_cap;
+    const size_t fixed = coop_rows_bytes(rpc, ecap, sizeof(T)) + fused_cols_bytes(ccap, sizeof(T), NR) +
+                         (size_t)coop_pad4(rpc) * 4;
+    if ((long long)fixed > budget) return SGIPC_OK;
+    const int kcap = (long long)(fixed + coop_contact_bytes(rpc, kContactSlots, sizeof(T))) <= budget ? kContactSlots : 0;
+    // z slots for contact columns outside the static set, up to one per resident contact
+    // entry, as far as they fit
+    int zextra = 0;
+    if (kcap > 0) {
+        const long long room = budget - (long long)(fixed + coop_contact_bytes(rpc, kcap, sizeof(T)));
+        const long long per = SGIPC_MAX_LEVELS * 4 + 3LL * NR * (long long)sizeof(T);
+        zextra = room > 64 ? (int)((room - 64) / per) : 0;
+        if (zextra > kcap) zextra = kcap;
+    }
+    const size_t base = coop_rows_bytes(rpc, ecap, sizeof(T)) + fused_cols_bytes(ccap + zextra, sizeof(T), NR) +
+                        (size_t)coop_pad4(rpc) * 4 + coop_contact_bytes(rpc, kcap, sizeof(T));
+    long long left = budget - (long long)base;
+    int dcap = left > 0 ? (int)(left / (2304 * (long long)sizeof(M))) : 0;
+    if (dcap > kDomPerCta) dcap = kDomPerCta;
+    const size_t dyn = base + (size_t)dcap * 2304 * sizeof(M);
+    SG_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    SG_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_fused<T, M, NR>, kCoopThreads, dyn));
+    if (per < 1) return SGIPC_OK;
+    cfg.usable = 1;
+    cfg.grid = nsm;
+    cfg.ecap = ecap;
+    cfg.kcap = kcap;
+    cfg.dcap = dcap;
+    cfg.ccap = ccap;
+    cfg.zextra = zextra;
+    cfg.dyn = dyn;
+    return SGIPC_OK;
+}
+
 template <class T, class M, int NR>
 SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, double tol, int max_iter, int crit,
                          cudaStream_t s, bool* used, RefineArgs* ref) {
@@ -1107,9 +1894,23 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     const int L = m.levelnum;
     const int ndom = h[16] / 16;
     const int nd01 = L > 2 ? h[2] / 16 : ndom;
-    const int grid = cfg.grid, ecap = cfg.ecap, kcap = cfg.kcap, dcap = cfg.dcap;
-    const size_t dyn = cfg.dyn;
-    const void* fn = (const void*)k_pcg_coop<T, M, NR>;
+    // the fused iteration where it applies (three levels or more, every row resident);
+    // SGIPC_PCG_FUSED=0 keeps the four-phase iteration
+    const char* fz = getenv("SGIPC_PCG_FUSED");
+    SgipcCtx::CoopCfg& fcfg = c->fused_cfg[inst];
+    bool fused = false;
+    // (FP64 vectors with four right-hand sides measured slower fused: kept four-phase)
+    if (L >= 3 && !(fz && fz[0] == '0') && !(sizeof(T) == 8 && sizeof(M) == 8 && NR == 4)) {
+        if (!fcfg.valid) {
+            SgipcStatus st = fused_configure<T, M, NR>(c, fcfg);
+            if (st != SGIPC_OK) return st;
+        }
+        fused = fcfg.usable != 0;
+    }
+    const SgipcCtx::CoopCfg& use = fused ? fcfg : cfg;
+    const int grid = use.grid, ecap = use.ecap, kcap = use.kcap, dcap = use.dcap;
+    const size_t dyn = use.dyn;
+    const void* fn = fused ? (const void*)k_pcg_fused<T, M, NR> : (const void*)k_pcg_coop<T, M, NR>;
     CoopArgs<T, M, NR> a;
     a.tp = topo_of(c);
     a.A = mat_view<T>(c);
@@ -1147,6 +1948,14 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     a.max_iter = max_iter;
     a.crit = crit;
     a.tol = tol;
+    a.w = (T*)w.w;
+    a.Ap2 = (T*)w.Ap2;
+    a.cs_ptr = c->cs_ptr;
+    a.cs_cols = c->cs_cols;
+    a.cs_lcol = c->cs_lcol;
+    a.cs_dslot = c->cs_dslot;
+    a.ccap = fused ? use.ccap : 0;
+    a.zextra = fused ? use.zextra : 0;
     SG_CHECK(c, cudaMemsetAsync(w.ticket + 4, 0, 2 * sizeof(unsigned int), s));
     // level-1-aligned passes write the level-0 entries of the banks that hold vertices only:
     // the others must read as zero in every solve, whatever the right-hand-side count

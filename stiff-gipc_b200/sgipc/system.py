@@ -303,7 +303,7 @@ class GIPC:
         return float(ms.value), float(by.value)
 
     PHASES = {1: "init", 2: "mas", 3: "mas_coarse", 4: "prolong", 5: "spmv", 6: "update", 7: "acc64",
-              8: "res64", 9: "restrict64", 10: "prolong64"}
+              8: "res64", 9: "restrict64", 10: "prolong64", 11: "fused_spmv", 12: "fused_update"}
 
     def profile_pcg(self, name: str = "pcg32", max_epochs: int = 1024):
         """Barrier stamps of one persistent PCG solve (``sgipc_profile_pcg``): (stamps, phases)

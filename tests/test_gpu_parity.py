@@ -210,7 +210,8 @@ def test_batched_four_rhs(case):
 @pytest.mark.parametrize("prec", ["fp64", "mixed", "ref"])
 def test_persistent_and_graph_solves_agree(case, prec, monkeypatch):
     """The one-kernel persistent solve and the graph of per-phase kernels run the same
-    algorithm; only the summation order of the dot products differs."""
+    algorithm up to rounding: the summation order of the dot products differs, and the fused
+    persistent iteration forms A p and p.Ap by recurrences."""
     sc, g, _ = case
     mas = system.MASPreconditioner(g)
     mas.setPreconditioner(prec)
@@ -363,7 +364,31 @@ def test_phase_profile_of_the_persistent_solve(case):
     assert (stamps[:, :, 1] >= stamps[:, :, 0]).all()
     assert (stamps[:, 1:, 0] >= stamps[:, :-1, 1]).all()
     assert phases[0] == "start" and phases[1] == "init" and "?" not in phases
-    assert phases.count("spmv") == st.iterations
+    # one SpMV phase per iteration: the four-phase iteration's or the fused one's
+    assert phases.count("spmv") + phases.count("fused_spmv") == st.iterations
     mas.setPreconditioner("mixed")
     stamps4, phases4 = g.profile_pcg("pcg32x4")
-    assert phases4.count("spmv") >= 1 and (stamps4[:, :, 1] >= stamps4[:, :, 0]).all()
+    assert phases4.count("spmv") + phases4.count("fused_spmv") >= 1
+    assert (stamps4[:, :, 1] >= stamps4[:, :, 0]).all()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "ref"])
+def test_fused_and_four_phase_persistent_solves_agree(case, prec, monkeypatch):
+    """With three MAS levels or more the persistent solve runs the fused iteration (three
+    barriers: z prolonged into the SpMV, the level-0/1 domains solved in the update, p.Ap from
+    the recurrence z.w + 2 beta z.Ap_old + beta^2 p_old.Ap_old); SGIPC_PCG_FUSED=0 runs the
+    four-phase one.  Same iteration counts within one, r0.z0 to 1e-12, solutions to 1e-9
+    (FP64) / 1e-4 (FP32 vectors)."""
+    sc, g, _ = case
+    mas = system.MASPreconditioner(g)
+    mas.setPreconditioner(prec)
+    solver = system.PCGSolver(g, system.PCGSolverConfig(precision=prec))
+    xa, sa = solver.solve(g.rhs())
+    monkeypatch.setenv("SGIPC_PCG_FUSED", "0")
+    xb, sb = solver.solve(g.rhs())
+    monkeypatch.delenv("SGIPC_PCG_FUSED")
+    assert sa.status == N.OK and sb.status == N.OK
+    assert abs(sa.iterations - sb.iterations) <= 1
+    assert abs(sa.rz0 - sb.rz0) <= 1e-12 * abs(sb.rz0)
+    if sa.iterations == sb.iterations:
+        assert _rel(xa.cpu().numpy(), xb.cpu().numpy()) < (1e-9 if prec == "fp64" else 1e-4)
