@@ -54,6 +54,8 @@ def parse():
                     help="two_cubes (the headline), cube, or cloth_sphere")
     ap.add_argument("--cpu-sample", type=int, default=0, help="CPU baseline solves (0 = auto, about 10 s)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--timeline", action="store_true",
+                    help="events after the assembly, the MAS build and the solve of each step (one GPU)")
     ap.add_argument("--pcg-phases", action="store_true",
                     help="print the per-phase profile of the persistent PCG solve instead of the bench line")
     ap.add_argument("--kernel", default=None,
@@ -519,6 +521,68 @@ def run_kernel_only(args):
     return 0
 
 
+def run_timeline(args):
+    """Where one Newton system's time goes, on the caller's stream (one GPU): CUDA events at the
+    step's start, after the assembly (the right-hand side, which joins the contact and element
+    streams), after the MAS build and after the PCG solve; and the host's time inside
+    sgipc_assemble.  Medians over args.steps steps, L2 flushed before each."""
+    import torch
+
+    from sgipc import system
+
+    torch.cuda.set_device(0)
+    sc, g = make_system(args, 0)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    out = {"workload": WORKLOADS[args.workload]}
+    for prec in ("mixed", "fp64"):
+        cfg = system.PCGSolverConfig(precision=prec)
+        mas = system.MASPreconditioner(g)
+        solver = system.PCGSolver(g, cfg)
+        rows = []
+        for k in range(args.warmup + args.steps):
+            flush.zero_()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            ev[0].record(stream)
+            t0 = time.perf_counter()
+            g.computeGradientAndHessian()
+            t_host = time.perf_counter() - t0
+            ev[1].record(stream)
+            mas.setPreconditioner(prec)
+            ev[2].record(stream)
+            _, st = solver.solve(g.rhs())
+            ev[3].record(stream)
+            ev[3].synchronize()
+            if k >= args.warmup:
+                rows.append([ev[0].elapsed_time(ev[1]), ev[0].elapsed_time(ev[2]), ev[0].elapsed_time(ev[3]),
+                             1e3 * t_host, st.iterations])
+        r = np.median(np.array(rows), axis=0)
+        out[prec] = {"assembly_end_ms": r[0], "mas_end_ms": r[1], "solve_end_ms": r[2], "assemble_host_ms": r[3],
+                     "pcg_iters": int(r[4])}
+        # the same step with the stream held by a ~0.5 ms spin first, so that the host has
+        # enqueued the whole assembly before it starts: the device-side times alone
+        gpu = []
+        for k in range(args.warmup + args.steps):
+            flush.zero_()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            torch.cuda._sleep(1_000_000)
+            ev[0].record(stream)
+            g.computeGradientAndHessian()
+            ev[1].record(stream)
+            mas.setPreconditioner(prec)
+            ev[2].record(stream)
+            solver.solve(g.rhs())
+            ev[3].record(stream)
+            ev[3].synchronize()
+            if k >= args.warmup:
+                gpu.append([ev[0].elapsed_time(ev[1]), ev[0].elapsed_time(ev[2]), ev[0].elapsed_time(ev[3])])
+        r = np.median(np.array(gpu), axis=0)
+        out[prec]["enqueued_ahead"] = {"assembly_end_ms": r[0], "mas_end_ms": r[1], "solve_end_ms": r[2]}
+    g.close()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -527,6 +591,8 @@ def main():
         return run_pcg_phases(args)
     if args.kernel:
         return run_kernel_only(args)
+    if args.timeline:
+        return run_timeline(args)
     return run_ours(args)
 
 
