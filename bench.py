@@ -37,6 +37,10 @@ WORKLOADS = {
     "cloth_sphere": "256^2 cloth (130050 triangles, 195585 hinges) rolled in layers 0.4 mm apart over a tet "
                     "sphere (20000 tets, r 0.3 m) on the ground, d-hat 5e-4 m, mu 0.2; about a million contact "
                     "pairs from the GPU pair search, lagged friction from the GPU set-up" + STEP,
+    "abd_bed": "500 affine boxes (8 points, edge 0.05 m, kappa_ABD 1e8; about a fifth resting on the bed) over "
+               "a soft tet bed (100000 tets, 23409 vertices, E 1e5 Pa) on the ground, d-hat 1e-3 m, contacts from "
+               "the GPU pair search; one Newton system = FEM assembly + contact class partition + ABD body "
+               "terms + ABD block Jacobi + MAS build + the coupled FEM + ABD PCG to r.z <= 1e-4 r0.z0",
 }
 L2_FLUSH_BYTES = 256 << 20
 CPU_SOLVER = ("Eigen unavailable: the oracle's OpenMP restatement of the reference's assembly and "
@@ -51,7 +55,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=21, help="lattice vertices per cube edge (two_cubes)")
     ap.add_argument("--workload", default="two_cubes", choices=sorted(WORKLOADS),
-                    help="two_cubes (the headline), cube, or cloth_sphere")
+                    help="two_cubes (the headline), cube, cloth_sphere or abd_bed")
     ap.add_argument("--cpu-sample", type=int, default=0, help="CPU baseline solves (0 = auto, about 10 s)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--timeline", action="store_true",
@@ -138,6 +142,8 @@ def make_scene(args, host_contacts=True):
         return scenes.scene_cube(11, touching=False, seed=0)
     if args.workload == "cloth_sphere":
         return scenes.scene_cloth_on_sphere(256, 4000, contacts=host_contacts)
+    if args.workload == "abd_bed":
+        raise ValueError("the abd_bed workload runs through run_abd_bed only")
     return scenes.scene_two_cubes(args.n, seed=1)
 
 
@@ -583,6 +589,77 @@ def run_timeline(args):
     return 0
 
 
+def run_abd_bed(args):
+    """The affine-bodies-on-a-bed workload on one GPU: Newton systems per second of the coupled
+    FEM + ABD system (GlobalLinearSystem), FP64 MAS inverses vs FP32 ones (the reference's
+    shipping mix); the coupled solve has no FP32-vector mode."""
+    import torch
+
+    from sgipc import abd, scenes, system
+    from sgipc import _native as N
+
+    torch.cuda.set_device(0)
+    sc, bodies = scenes.scene_abd_on_bed(500, contacts=False)
+    g = system.GIPC(sc, device=0, pair_capacity=400_000)
+    g.buildCP(body=torch.tensor(sc.body_of_vertex, dtype=torch.int32, device="cuda"))
+    af = bodies["abd_first"]
+    g.computeGradientAndHessian()
+    part = g.contactPartition(af)
+    cap = 2 * max(part["abd_blocks"][0].numel(), part["fem_blocks"][0].numel(), 1)
+    sysm = abd.ABDSystem(bodies, max_abd_blocks=cap, max_fem_blocks=cap)
+    q = torch.tensor(bodies["q"], device="cuda")
+    qt = torch.tensor(bodies["q_tilde"], device="cuda")
+    gls = abd.GlobalLinearSystem(g, sysm)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(prec, tol=1e-4, crit=N.CRIT_RZ, ratio=0.3):
+        g.computeGradientAndHessian()
+        pt = g.contactPartition(af, cap)
+        sysm.setup_abd_system_gradient_hessian(q, qt, bodies["kappa"], bodies["dt"], point_grad=pt["point_grad"],
+                                               abd_blocks=pt["abd_blocks"], fem_blocks=pt["fem_blocks"],
+                                               fem_boundary=g.tet.BoundaryType)
+        abd.ABDPreconditioner(sysm).assemble()
+        system.MASPreconditioner(g).setPreconditioner(prec)
+        return gls.solve_linear_system(gls.right_hand_side(), tol=tol, criterion=crit, max_iter_ratio=ratio)
+
+    out = {"metric": METRIC, "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (MAS f64 / f32)",
+           "data": "synthetic (seeded lattice bed, seeded boxes)",
+           "config": {"workload": WORKLOADS["abd_bed"], "l2": "flushed (256 MiB write) between timed steps",
+                      "contact_pairs": int(g.tet.pairs.shape[0]), "abd_abd_blocks": int(part["abd_blocks"][0].numel()),
+                      "abd_fem_blocks": int(part["fem_blocks"][0].numel())}}
+    xs = {}
+    for prec in ("fp64", "ref"):
+        for _ in range(max(3, args.warmup)):
+            step(prec)
+        tot, st = 0.0, None
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            x, _, st = step(prec)
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1) / 1e3
+        xs[prec] = x.clone()
+        out[prec] = {"value": args.steps / tot, "ms_per_step": 1e3 * tot / args.steps, "pcg_iters": st.iterations,
+                     "rel_residual": st.rel_residual}
+    tight, _, st_t = step("fp64", 1e-10, N.CRIT_TRUE, 2.0)
+    out["value"] = out["ref"]["value"]
+    out["ms_per_step"] = out["ref"]["ms_per_step"]
+    out["ref_over_fp64"] = out["ref"]["value"] / out["fp64"]["value"]
+    out["accuracy"] = {"reference_solve": {"precision": "fp64", "criterion": "true residual", "tol": 1e-10,
+                                           "pcg_iters": st_t.iterations, "rel_residual": st_t.rel_residual},
+                       "dx_rel_err_ref_vs_fp64": float((xs["ref"] - xs["fp64"]).norm() / xs["fp64"].norm()),
+                       "dx_rel_err_fp64_vs_tight": float((xs["fp64"] - tight).norm() / tight.norm()),
+                       "dx_rel_err_ref_vs_tight": float((xs["ref"] - tight).norm() / tight.norm())}
+    sysm.close()
+    g.close()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -593,6 +670,8 @@ def main():
         return run_kernel_only(args)
     if args.timeline:
         return run_timeline(args)
+    if args.workload == "abd_bed":
+        return run_abd_bed(args)
     return run_ours(args)
 
 

@@ -357,6 +357,23 @@ SgipcStatus sgipc_abd_precond_build(SgipcAbdCtx* ctx, void* stream);
 /* ABDPreconditioner::apply: z_b = P_b^-1 r_b, r and z [dev double[12 * body_num]]. */
 SgipcStatus sgipc_abd_precond_apply(SgipcAbdCtx* ctx, const double* r, double* z, void* stream);
 
+/* The class partition of the contact terms (GIPC::partitionContactHessian, GIPC.cu:9932-10108,
+ * with the contact gradient of the ABD points) for a context whose vertices [abd_first, nv)
+ * are the points of affine bodies, marked Dirichlet in fem->BoundaryType so that sgipc_assemble
+ * keeps only the FEM-FEM parts of the contact terms in its matrix.  The barrier, friction and
+ * ground terms of `con` are evaluated at fem->vertexes; their blocks that touch an ABD point
+ * are written in slot order to the caller's device arrays: ABD-ABD blocks (rows, cols = ABD
+ * point ids counted from abd_first, row <= col, row-major 3x3) and ABD-FEM blocks (rows = ABD
+ * point id, cols = FEM vertex, the block in that orientation), up to cap of each, with their
+ * counts on the host; point_grad [dev double3[nv - abd_first], may be null] receives the
+ * contact gradient at the ABD points.  These are the inputs of sgipc_abd_grad_hess.
+ * Synchronises; SGIPC_CAPACITY when a count exceeds cap (the count is still returned). */
+SgipcStatus sgipc_contact_partition(SgipcCtx* ctx, const SgipcFemData* fem, const SgipcContacts* con,
+                                    const SgipcParams* prm, int32_t abd_first, int32_t cap, int32_t* abd_rows,
+                                    int32_t* abd_cols, double* abd_vals, int32_t* abd_count, int32_t* fem_rows,
+                                    int32_t* fem_cols, double* fem_vals, int32_t* fem_count, double* point_grad,
+                                    void* stream);
+
 /* ---- the global FEM + ABD system ------------------------------------------------------- */
 
 /* GlobalLinearSystem::solve_linear_system + distribute_solution (global_linear_system.cu:

@@ -407,7 +407,7 @@ struct BlockSink {
     unsigned long long* key;
     int* idx;
     double* val;
-    const int32_t* btype;
+    const int32_t* btype;  // Dirichlet flags (blocks touching a flagged vertex are zeroed); null: none
     int bits;
     int nv;
     int* flag;  // set to 1 when a pair names a vertex outside [0, nv)
@@ -443,7 +443,7 @@ __device__ __forceinline__ void emit_pair_blocks(const BlockSink& bs, int base, 
             bs.key[slot] = ((unsigned long long)rr << bs.bits) | (unsigned long long)cc;
             double H[3][3];
             fn(a, b, H);
-            bool dir = bs.btype[r] != 0 || bs.btype[c] != 0;
+            bool dir = bs.btype && (bs.btype[r] != 0 || bs.btype[c] != 0);
             double* o = bs.val + 9 * (size_t)slot;
 #pragma unroll
             for (int p = 0; p < 3; p++)
@@ -455,7 +455,7 @@ __device__ __forceinline__ void emit_pair_blocks(const BlockSink& bs, int base, 
 __device__ __forceinline__ void emit_diag_block(const BlockSink& bs, int slot, int v, const double H[3][3]) {
     bs.idx[slot] = slot;
     bs.key[slot] = ((unsigned long long)v << bs.bits) | (unsigned long long)v;
-    bool dir = bs.btype[v] != 0;
+    bool dir = bs.btype && bs.btype[v] != 0;
     double* o = bs.val + 9 * (size_t)slot;
 #pragma unroll
     for (int p = 0; p < 3; p++)
@@ -1211,8 +1211,9 @@ static int contact_slots(const SgipcContacts* k, const SgipcParams* p) {
 
 // launch the contact kernels; returns the number of contact block slots used
 static int launch_contacts(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k, const SgipcParams* p,
-                           double* grad, cudaStream_t s) {
+                           double* grad, cudaStream_t s, bool keep_dirichlet = false) {
     BlockSink bs = sink(c, f);
+    if (keep_dirichlet) bs.btype = nullptr;
     int base = 0;
     if (k) SG_COUNT(c, (k->pair_num > 0) + (k->fric_num > 0 && p->frictionRate > 0.0) + (k->ground_num > 0) +
                            (k->fric_gd_num > 0 && p->gd_frictionRate > 0.0));
@@ -1414,6 +1415,107 @@ extern "C" SgipcStatus sgipc_fem_grad_hess(SgipcCtx* c, const SgipcFemData* f, c
 // timing hook
 // ------------------------------------------------------------------------------------------
 namespace sgipc {
+// ---- class partition of the contact terms (affine-body points) ------------------------------
+// slot s of the contact blocks: fa[s] = 1 for an ABD-ABD block, ff[s] = 1 for an ABD-FEM block
+// (upper keys: r <= c, so an ABD-FEM block has r < af <= c)
+__global__ void k_part_flags(int m, const unsigned long long* __restrict__ key, int bits, int af, int* __restrict__ fa,
+                             int* __restrict__ ff) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s > m) return;
+    int a = 0, f = 0;
+    if (s < m) {
+        const unsigned long long k = key[s];
+        if (k != kBadKey) {
+            const int r = (int)(k >> bits), c = (int)(k & ((1ull << bits) - 1));
+            a = r >= af;
+            f = r < af && c >= af;
+        }
+    }
+    fa[s] = a;
+    ff[s] = f;
+}
+
+// emit the flagged blocks at their scanned positions (slot order): ABD-ABD as (point, point)
+// with point ids counted from af, ABD-FEM as (point, FEM vertex) with the block transposed to
+// that orientation
+__global__ void k_part_emit(int m, const unsigned long long* __restrict__ key, const double* __restrict__ val, int bits,
+                            int af, const int* __restrict__ oa, const int* __restrict__ of, int cap,
+                            int32_t* __restrict__ arow, int32_t* __restrict__ acol, double* __restrict__ aval,
+                            int32_t* __restrict__ frow, int32_t* __restrict__ fcol, double* __restrict__ fval) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= m) return;
+    const unsigned long long k = key[s];
+    if (k == kBadKey) return;
+    const int r = (int)(k >> bits), c = (int)(k & ((1ull << bits) - 1));
+    const double* v = val + 9 * (size_t)s;
+    if (r >= af) {
+        const int i = oa[s];
+        if (i >= cap) return;
+        arow[i] = r - af;
+        acol[i] = c - af;
+        for (int q = 0; q < 9; q++) aval[9 * (size_t)i + q] = v[q];
+    } else if (c >= af) {
+        const int i = of[s];
+        if (i >= cap) return;
+        frow[i] = c - af;
+        fcol[i] = r;
+        for (int p = 0; p < 3; p++)
+            for (int q = 0; q < 3; q++) fval[9 * (size_t)i + 3 * p + q] = v[3 * q + p];
+    }
+}
+
+__global__ void k_part_grad(int npt, int af, const double* __restrict__ g, double* __restrict__ pg) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < 3 * npt) pg[k] = g[3 * (size_t)af + k];
+}
+
+extern "C" SgipcStatus sgipc_contact_partition(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k,
+                                               const SgipcParams* p, int32_t abd_first, int32_t cap,
+                                               int32_t* abd_rows, int32_t* abd_cols, double* abd_vals,
+                                               int32_t* abd_count, int32_t* fem_rows, int32_t* fem_cols,
+                                               double* fem_vals, int32_t* fem_count, double* point_grad,
+                                               void* stream) {
+    SgipcStatus st = check_inputs(c, f, k, p);
+    if (st != SGIPC_OK) return st;
+    if (abd_first < 0 || abd_first > c->nv || cap < 0 || !abd_count || !fem_count) {
+        snprintf(c->err, sizeof(c->err), "contact_partition: abd_first %d outside [0, %d] or a missing count",
+                 abd_first, c->nv);
+        return SGIPC_BAD_INPUT;
+    }
+    if (cap > 0 && (!abd_rows || !abd_cols || !abd_vals || !fem_rows || !fem_cols || !fem_vals)) return SGIPC_BAD_INPUT;
+    cudaStream_t s = (cudaStream_t)stream;
+    SG_DEVICE(c);
+    const int npt = c->nv - abd_first;
+    SG_CHECK(c, cudaMemsetAsync(c->tmp64, 0, sizeof(double) * 3 * (size_t)c->nv, s));
+    const int m = launch_contacts(c, f, k, p, c->tmp64, s, true);
+    SG_LAUNCH_CHECK(c, "contact kernels (partition)");
+    int* fa = c->cflag;
+    int* ff = c->run_start;
+    SG_COUNT(c, 2 + (npt > 0 && point_grad ? 1 : 0));
+    k_part_flags<<<nblk(m + 1), SGIPC_BLOCK, 0, s>>>(m, c->ckey, c->key_bits, abd_first, fa, ff);
+    size_t tb = c->cub_tmp_bytes;
+    SG_CHECK(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp, tb, fa, fa, m + 1, s));
+    tb = c->cub_tmp_bytes;
+    SG_CHECK(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp, tb, ff, ff, m + 1, s));
+    if (m > 0)
+        k_part_emit<<<nblk(m), SGIPC_BLOCK, 0, s>>>(m, c->ckey, c->cval, c->key_bits, abd_first, fa, ff, cap, abd_rows,
+                                                    abd_cols, abd_vals, fem_rows, fem_cols, fem_vals);
+    if (npt > 0 && point_grad) k_part_grad<<<nblk(3LL * npt), SGIPC_BLOCK, 0, s>>>(npt, abd_first, c->tmp64, point_grad);
+    SG_LAUNCH_CHECK(c, "contact partition");
+    int cnt[2];
+    SG_CHECK(c, cudaMemcpyAsync(&cnt[0], fa + m, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaMemcpyAsync(&cnt[1], ff + m, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    *abd_count = cnt[0];
+    *fem_count = cnt[1];
+    if (cnt[0] > cap || cnt[1] > cap) {
+        snprintf(c->err, sizeof(c->err), "contact_partition: %d ABD-ABD and %d ABD-FEM blocks beyond the capacity %d",
+                 cnt[0], cnt[1], cap);
+        return SGIPC_CAPACITY;
+    }
+    return SGIPC_OK;
+}
+
 SgipcStatus assemble_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, double* bytes) {
     const SgipcFemData* f = &c->last_fem;
     const SgipcParams* p = &c->last_prm;

@@ -113,15 +113,20 @@ def lattice_tets(n: int, size: float, origin=(0.0, 0.0, 0.0)):
     Cells alternate between the two mirror-image 5-tet splits so that faces match.
     Returns (verts (n^3,3), tets (5*(n-1)^3,4)) with positively oriented tets.
     """
-    g = np.linspace(0.0, size, n)
-    ii, jj, kk = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
-    verts = np.stack([g[ii.ravel()], g[jj.ravel()], g[kk.ravel()]], 1) + np.asarray(origin)
+    return box_lattice_tets((n, n, n), size / (n - 1), origin)
+
+
+def box_lattice_tets(n, h: float, origin=(0.0, 0.0, 0.0)):
+    """Regular nx x ny x nz vertex lattice of spacing h, 5 tets per cell (the split of
+    :func:`lattice_tets`).  Returns (verts, tets) with positively oriented tets."""
+    nx, ny, nz = (int(t) for t in n)
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    verts = h * np.stack([ii.ravel(), jj.ravel(), kk.ravel()], 1).astype(np.float64) + np.asarray(origin)
 
     def vid(i, j, k):
-        return (i * n + j) * n + k
+        return (i * ny + j) * nz + k
 
-    c = np.arange(n - 1)
-    ci, cj, ck = np.meshgrid(c, c, c, indexing="ij")
+    ci, cj, ck = np.meshgrid(np.arange(nx - 1), np.arange(ny - 1), np.arange(nz - 1), indexing="ij")
     ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
     corner = {}
     for a in (0, 1):
@@ -403,7 +408,10 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
     """Concatenate tet and cloth bodies, derive ``initFEM`` data and set up one Newton iterate.
 
     Each body dict holds ``verts`` and either ``tets`` with ``E`` (a soft solid) or
-    ``tris`` (a cloth sheet), plus optional ``velocity`` (3,) and ``boundary`` flag.
+    ``tris`` (a cloth sheet), plus optional ``velocity`` (3,) and ``boundary`` flag.  A body
+    with ``affine=True`` is the point set of an affine body: its ``tris`` are its contact
+    surface only (no elements), its vertices are Dirichlet here (their motion is the body's,
+    solved in body space) with unit mass on the kept diagonal.
     ``cloth`` gives the sheet material: ``thickness``, ``E``, ``bend_E``, ``density``,
     ``strain_rate`` (StiffGIPC/gl_main.cu:578-583, 619-640).  Vertex positions of the
     current iterate are the body's positions (``verts``) plus a seeded uniform perturbation of
@@ -411,26 +419,29 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
     rest state), else ``verts``.
     """
     rng = np.random.default_rng(seed)
-    verts, cur, tets, tris, youngs, vel, btype, body_id = [], [], [], [], [], [], [], []
+    verts, cur, tets, tris, atris, youngs, vel, btype, body_id = [], [], [], [], [], [], [], [], []
     off = 0
     for b, body in enumerate(bodies):
         v = np.asarray(body["verts"], np.float64)
         cur.append(v)
         verts.append(np.asarray(body.get("rest", v), np.float64))
-        if "tets" in body:
+        if body.get("affine"):
+            atris.append(np.asarray(body["tris"], np.int64) + off)
+        elif "tets" in body:
             t = np.asarray(body["tets"], np.int64) + off
             tets.append(t)
             youngs.append(np.full(len(t), float(body["E"])))
         else:
             tris.append(np.asarray(body["tris"], np.int64) + off)
         vel.append(np.tile(np.asarray(body.get("velocity", (0.0, 0.0, 0.0)), np.float64), (len(v), 1)))
-        btype.append(np.full(len(v), int(body.get("boundary", 0)), np.int32))
+        btype.append(np.full(len(v), 1 if body.get("affine") else int(body.get("boundary", 0)), np.int32))
         body_id.append(np.full(len(v), b, np.int32))
         off += len(v)
     rest = np.concatenate(verts)
     pose = np.concatenate(cur)
     tets = np.concatenate(tets).astype(np.int32) if tets else np.zeros((0, 4), np.int32)
     tris = np.concatenate(tris).astype(np.int64) if tris else np.zeros((0, 3), np.int64)
+    atris = np.concatenate(atris).astype(np.int64) if atris else np.zeros((0, 3), np.int64)
     youngs = np.concatenate(youngs) if youngs else np.zeros(0)
     vel = np.concatenate(vel)
     btype = np.concatenate(btype)
@@ -458,11 +469,14 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
     rest, pose, vel, btype, body_id = rest[perm], pose[perm], vel[perm], btype[perm], body_id[perm]
     tets = inv[tets].astype(np.int32)
     tris = inv[tris].astype(np.int32)
+    atris = inv[atris].astype(np.int32)
 
     dm_inv, vol = tet_rest_data(rest, tets) if len(tets) else (np.zeros((0, 3, 3)), np.zeros(0))
     lr, vr = snk_rates(youngs, nu)
     masses = np.zeros(nv)
     np.add.at(masses, tets.ravel(), np.repeat(vol * density / 4.0, 4))
+    if len(atris):
+        masses[np.unique(atris)] = 1.0
     cl = _empty_cloth()
     stretch = shear = bend = srate = 0.0
     if len(tris):
@@ -486,6 +500,10 @@ def build_tet_scene(name: str, bodies: List[dict], dt: float, dhat_abs: float, d
         stris = np.concatenate([stris, tris]).astype(np.int32)
         sedges = np.unique(np.concatenate([sedges, tri_mesh_edges(tris)]), axis=0).astype(np.int32)
         sverts = np.unique(np.concatenate([sverts, tris.ravel()])).astype(np.int32)
+    if len(atris):  # affine bodies collide with their surfaces
+        stris = np.concatenate([stris, atris]).astype(np.int32)
+        sedges = np.unique(np.concatenate([sedges, tri_mesh_edges(atris)]), axis=0).astype(np.int32)
+        sverts = np.unique(np.concatenate([sverts, atris.ravel()])).astype(np.int32)
     nbr_start, nbr_list = neighbour_csr(nv, tets, tris)
     if given:
         from . import meshio
@@ -700,6 +718,87 @@ def scene_abd_boxes(nb: int = 500, seed: int = 3, edge: float = 0.05, density: f
     return dict(point_body=point_body, x_bar=x_bar, dyadic_mass=np.tile(dm, (nb, 1)),
                 volume=np.full(nb, vol_t.sum()), boundary_type=np.zeros(nb, np.int32),
                 q=q, q_tilde=q_tilde, x=x, dt=dt, kappa=kappa_abd)
+
+
+def scene_abd_on_bed(nb: int = 500, cells=(50, 8, 50), seed: int = 4, edge: float = 0.05, density: float = 1000.0,
+                     dt: float = 0.01, kappa_abd: float = 1e8, dhat_abs: float = 1e-3, resting: float = 0.3,
+                     bed_E: float = 1e5, contacts: bool = True):
+    """The affine-bodies-on-a-bed workload: nb boxes (8 points, 12 surface triangles, edge
+    0.05 m, kappa_ABD 1e8) at seeded positions over a soft tet bed (cells[0] x cells[1] x
+    cells[2] lattice cells of 5 tets over a 1 m square, 100 000 tets by default, E 1e5 Pa)
+    lying 0.5 d-hat above the ground.  A share ``resting`` of the boxes sits flat with its
+    bottom 0.5 d-hat above the bed, the others are spread, without overlap, over the metre
+    above it and fall at seeded velocities.
+
+    Returns (scene, bodies).  In the scene the bed's vertices come first and the boxes' points
+    follow from ``bodies["abd_first"]`` on, marked Dirichlet: their rows hold only the kept
+    mass diagonal, and the contact terms that touch them go to the bodies through
+    ``GIPC.contactPartition``.  ``bodies`` holds the ABDSystem inputs of
+    :func:`scene_abd_boxes` with the points in the scene's order.  With contacts=False the
+    contact arrays are left empty for the GPU pair search (body ids: the bed 0, box b b+1)."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 / cells[0]
+    base = GROUND_OFFSET + 0.5 * dhat_abs
+    bv, bt = box_lattice_tets((cells[0] + 1, cells[1] + 1, cells[2] + 1), h, (0.0, base, 0.0))
+    top = base + cells[1] * h
+    cv, ct = lattice_tets(2, edge)
+    cv = cv - cv.mean(0)
+    cs_tris, _, _ = tet_surface(ct)
+    _, vol_t = tet_rest_data(cv, ct)
+    node_m = np.zeros(8)
+    np.add.at(node_m, ct.ravel(), np.repeat(vol_t * density / 4.0, 4))
+    dm = np.concatenate([[node_m.sum()], (node_m[:, None] * cv).sum(0),
+                         np.einsum("p,pi,pj->ij", node_m, cv, cv).ravel()])
+    # box centres: resting ones on the bed, the others in the metre above, no two within
+    # edge + 2 d-hat of each other along every axis (boxes stay axis-aligned to within 1e-3)
+    gap = edge + 2.0 * dhat_abs
+    cen, rest_flag = [], []
+    tries = 0
+    while len(cen) < nb:
+        tries += 1
+        if tries > 200000:
+            raise ValueError("no room for %d boxes" % nb)
+        on = rng.uniform() < resting
+        c = np.array([rng.uniform(0.5 * edge, 1.0 - 0.5 * edge),
+                      top + 0.5 * dhat_abs + 0.5 * edge if on else rng.uniform(top + edge, top + 1.0),
+                      rng.uniform(0.5 * edge, 1.0 - 0.5 * edge)])
+        if cen:
+            d = np.abs(np.asarray(cen) - c)
+            if np.any((d < gap).all(1)):
+                continue
+        cen.append(c)
+        rest_flag.append(on)
+    cen = np.asarray(cen)
+    rest_flag = np.asarray(rest_flag)
+    A = np.tile(np.eye(3), (nb, 1, 1))
+    fly = ~rest_flag
+    A[fly] += rng.normal(scale=1e-3, size=(int(fly.sum()), 3, 3))
+    vel = np.where(rest_flag[:, None], 0.0, rng.normal(scale=0.1, size=(nb, 3)))
+    q = np.concatenate([cen, A.reshape(nb, 9)], 1)
+    q_prev = q.copy()
+    q_prev[:, :3] -= dt * vel
+    q_tilde = q_prev.copy()
+    q_tilde[:, :3] += dt * vel + dt * dt * np.asarray(GRAVITY)
+    pts = np.einsum("bij,pj->bpi", A, cv) + cen[:, None]  # (nb, 8, 3)
+    bodies_in = [dict(verts=bv, tets=bt, E=bed_E)]
+    bodies_in += [dict(verts=pts[b], tris=cs_tris, affine=True) for b in range(nb)]
+    sc = build_tet_scene("abd%d_bed%d" % (nb, len(bt)), bodies_in, dt=dt, dhat_abs=dhat_abs, density=density,
+                         nu=0.4, mu_friction=0.0, seed=seed, perturb=0.0)
+    nbed = len(bv)
+    body = sc.body_of_vertex.astype(np.int64)
+    if not (body[:nbed] == 0).all() or not (body[nbed:] > 0).all():
+        raise AssertionError("the bed's vertices must come first")
+    # each scene point: its box and its corner (matched by position; the corners are distinct)
+    pb = body[nbed:] - 1
+    x = sc.vertexes[nbed:]
+    corner = np.argmin(((pts[pb] - x[:, None, :]) ** 2).sum(2), 1)
+    bodies = dict(point_body=pb.astype(np.int32), x_bar=cv[corner], dyadic_mass=np.tile(dm, (nb, 1)),
+                  volume=np.full(nb, vol_t.sum()), boundary_type=np.zeros(nb, np.int32), q=q, q_tilde=q_tilde,
+                  x=x.copy(), dt=dt, kappa=kappa_abd, abd_first=nbed, resting=rest_flag)
+    if contacts:
+        from . import contacts as _contacts
+        _contacts.attach_contacts(sc)
+    return sc, bodies
 
 
 SCENES = {

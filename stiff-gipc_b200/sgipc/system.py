@@ -392,6 +392,35 @@ class GIPC:
         tet.fric_gd_pairs, tet.fric_gd_lambda = gpp[:ng], gl[:ng]
         return list(cp)
 
+    def contactPartition(self, abd_first: int, capacity: Optional[int] = None,
+                         tet: Optional[DeviceTetraData] = None):
+        """GIPC::partitionContactHessian (GIPC.cu:9932-10108) for a scene whose vertices
+        [abd_first, nv) are affine-body points (Dirichlet in BoundaryType): the contact blocks
+        that touch them, ABD-ABD as (point, point) and ABD-FEM as (point, FEM vertex), and the
+        contact gradient at the points (``sgipc_contact_partition``).  Returns a dict of device
+        tensors ``abd_blocks`` / ``fem_blocks`` = (rows, cols, vals (k, 3, 3)) and
+        ``point_grad`` (points, 3), the inputs of ``ABDSystem.setup_abd_system_gradient_hessian``."""
+        tet = tet or self.tet
+        dev = _dev()
+        npt = self.n - abd_first
+        cap = capacity if capacity is not None else max(1, 10 * (tet.pairs.shape[0] + tet.fric_pairs.shape[0]) +
+                                                            tet.ground_pairs.shape[0])
+        ar = torch.empty(cap, dtype=torch.int32, device=dev)
+        ac = torch.empty(cap, dtype=torch.int32, device=dev)
+        av = torch.empty((cap, 3, 3), dtype=torch.float64, device=dev)
+        fr = torch.empty(cap, dtype=torch.int32, device=dev)
+        fc = torch.empty(cap, dtype=torch.int32, device=dev)
+        fv = torch.empty((cap, 3, 3), dtype=torch.float64, device=dev)
+        pg = torch.zeros((max(npt, 1), 3), dtype=torch.float64, device=dev)
+        na, nf = C.c_int32(), C.c_int32()
+        f, k, p = tet.fem_struct_cached(), tet.contact_struct_cached(), self._params()
+        N.check(N.lib().sgipc_contact_partition(self.ctx, C.byref(f), C.byref(k), C.byref(p), abd_first, cap,
+                                                _p(ar), _p(ac), _p(av), C.byref(na), _p(fr), _p(fc), _p(fv),
+                                                C.byref(nf), _p(pg), _stream()), self.ctx)
+        a, b = na.value, nf.value
+        return {"abd_blocks": (ar[:a], ac[:a], av[:a]), "fem_blocks": (fr[:b], fc[:b], fv[:b]),
+                "point_grad": pg[:npt]}
+
     def spmv(self, x: torch.Tensor) -> torch.Tensor:
         y = torch.empty_like(x)
         N.check(N.lib().sgipc_spmv(self.ctx, _p(x), _p(y), _stream()), self.ctx)
