@@ -768,12 +768,17 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         double* r64 = c->tmp64;
         SG_CHECK(c, cudaMemsetAsync(x, 0, sizeof(double) * n3, s));
         SG_CHECK(c, cudaMemcpyAsync(r64, b, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
-        double rz0 = -1.0, rz = 0.0, bn2 = 0.0;
+        double rz0 = -1.0, rz = 0.0, bn2 = 0.0, rr = 0.0;
         int total_it = 0, ref = 0, status = SGIPC_OK;
         for (ref = 0; ref < 8; ref++) {
+            // the reduction the inner solve still has to make, on its own right-hand side (the
+            // FP64 residual): r.z by rz0 / rz; on the true residual, ||r|| to tol ||b||, aimed
+            // at half of it, so that the FP32 inner residual's drift from the FP64 one rarely
+            // costs another refinement
             double inner_tol = tol;
             if (rz0 > 0 && rz > 0) inner_tol = fmin(1.0, fmax(tol * rz0 / rz, 1e-10));
-            if (crit == SGIPC_CRIT_TRUE && bn2 > 0 && rz > 0) inner_tol = tol;
+            if (crit == SGIPC_CRIT_TRUE)
+                inner_tol = bn2 > 0 && rr > 0 ? fmin(1.0, fmax(0.5 * tol * sqrt(bn2 / rr), 1e-10)) : 0.5 * tol;
             // the persistent solve refines itself where it can (x += x32, FP64 residual, its
             // r.z and r.r); otherwise the same steps follow here
             RefineArgs rf{x, b, r64, false};
@@ -807,6 +812,7 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
                 bn2 = hs.bnorm2;
             }
             rz = c->h_pinned[0];
+            rr = c->h_pinned[1];
             if (hs.status == SGIPC_BREAKDOWN || hs.status == SGIPC_CUDA_ERROR) {
                 status = final_status(c, hs);
                 break;
