@@ -546,11 +546,10 @@ __device__ __forceinline__ void barrier_s(double I, double c, double& B, double&
     d2B = c * (2.0 * L * L + 8.0 * t * L / I + 2.0 * t * t * (1.0 - L) / (I * I));
 }
 
-__global__ void __launch_bounds__(128) k_barrier(int np, const int4* __restrict__ pairs, const double* __restrict__ x,
-                                                 const double* __restrict__ rest, double dhat, double kappa,
-                                                 double* __restrict__ fb, BlockSink bs, int base) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
+__device__ __forceinline__ void barrier_one(int p, int np, const int4* __restrict__ pairs,
+                                            const double* __restrict__ x, const double* __restrict__ rest,
+                                            double dhat, double kappa, double* __restrict__ fb, BlockSink bs,
+                                            int base) {
     int v[4], nvp;
     int kind = decode_pair(pairs[p], v, nvp);
     if (!ids_ok(bs, v, nvp)) {
@@ -629,14 +628,20 @@ __global__ void __launch_bounds__(128) k_barrier(int np, const int4* __restrict_
     });
 }
 
-// friction pairs (FrictionUtils.cuh, GIPC.cu:1439-1800 and 5087-5270), C1 static clamping
-__global__ void __launch_bounds__(128) k_friction(int np, const int4* __restrict__ pairs, const double* __restrict__ x,
-                                                  const double* __restrict__ x0, const double* __restrict__ lam,
-                                                  const double* __restrict__ coord, const double* __restrict__ basis,
-                                                  double mu, double eps2, double* __restrict__ fb, BlockSink bs,
-                                                  int base) {
+__global__ void __launch_bounds__(128) k_barrier(int np, const int4* __restrict__ pairs, const double* __restrict__ x,
+                                                 const double* __restrict__ rest, double dhat, double kappa,
+                                                 double* __restrict__ fb, BlockSink bs, int base) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np) return;
+    barrier_one(p, np, pairs, x, rest, dhat, kappa, fb, bs, base);
+}
+
+// friction pairs (FrictionUtils.cuh, GIPC.cu:1439-1800 and 5087-5270), C1 static clamping
+__device__ __forceinline__ void friction_one(int p, int np, const int4* __restrict__ pairs,
+                                             const double* __restrict__ x, const double* __restrict__ x0,
+                                             const double* __restrict__ lam, const double* __restrict__ coord,
+                                             const double* __restrict__ basis, double mu, double eps2,
+                                             double* __restrict__ fb, BlockSink bs, int base) {
     int4 e = pairs[p];
     int v[4] = {0, 0, 0, 0}, nvp = 0;
     double cf[4] = {0, 0, 0, 0};
@@ -699,11 +704,20 @@ __global__ void __launch_bounds__(128) k_friction(int np, const int4* __restrict
     });
 }
 
-// ground barrier (GIPC.cu:6463-6514), plane y = offset
-__global__ void k_ground(int ng, const uint32_t* __restrict__ gp, const double* __restrict__ x, double offset,
-                         double dhat, double kappa, double* __restrict__ fb, BlockSink bs, int base) {
+__global__ void __launch_bounds__(128) k_friction(int np, const int4* __restrict__ pairs, const double* __restrict__ x,
+                                                  const double* __restrict__ x0, const double* __restrict__ lam,
+                                                  const double* __restrict__ coord, const double* __restrict__ basis,
+                                                  double mu, double eps2, double* __restrict__ fb, BlockSink bs,
+                                                  int base) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= ng) return;
+    if (p >= np) return;
+    friction_one(p, np, pairs, x, x0, lam, coord, basis, mu, eps2, fb, bs, base);
+}
+
+// ground barrier (GIPC.cu:6463-6514), plane y = offset
+__device__ __forceinline__ void ground_one(int p, int ng, const uint32_t* __restrict__ gp,
+                                           const double* __restrict__ x, double offset, double dhat, double kappa,
+                                           double* __restrict__ fb, BlockSink bs, int base) {
     int v = gp[p];
     if (!ids_ok(bs, &v, 1)) {
         bs.idx[base + p] = base + p;
@@ -718,12 +732,12 @@ __global__ void k_ground(int ng, const uint32_t* __restrict__ gp, const double* 
     emit_diag_block(bs, base + p, v, H);
 }
 
+
 // ground friction (GIPC.cu:1357-1437, 5047-5085), normal +y
-__global__ void k_fric_ground(int ng, const uint32_t* __restrict__ gp, const double* __restrict__ x,
-                              const double* __restrict__ x0, const double* __restrict__ lam, double mu, double eps2,
-                              double* __restrict__ fb, BlockSink bs, int base) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= ng) return;
+__device__ __forceinline__ void fric_ground_one(int p, int ng, const uint32_t* __restrict__ gp,
+                                                const double* __restrict__ x, const double* __restrict__ x0,
+                                                const double* __restrict__ lam, double mu, double eps2,
+                                                double* __restrict__ fb, BlockSink bs, int base) {
     int v = gp[p];
     if (!ids_ok(bs, &v, 1)) {
         bs.idx[base + p] = base + p;
@@ -747,6 +761,46 @@ __global__ void k_fric_ground(int ng, const uint32_t* __restrict__ gp, const dou
         H[2][2] = s / eps;
     }
     emit_diag_block(bs, base + p, v, H);
+}
+
+
+// All contact terms of a call in one launch: the CTAs take the barrier pairs, then the
+// friction pairs, then the ground and the ground-friction vertices (128 threads each), so the
+// four kinds run side by side instead of one after another.
+struct ContactLaunch {
+    int np, nf, ng, ngf;           // items of each kind (0: none)
+    int cb, cf, cg;                // first CTA of friction, ground, ground friction
+    const int4* pairs;
+    const int4* fpairs;
+    const uint32_t* gpairs;
+    const uint32_t* gfpairs;
+    const double* x;
+    const double* x0;
+    const double* rest;
+    const double* flam;
+    const double* fcoord;
+    const double* fbasis;
+    const double* gflam;
+    double dhat, kappa, mu, gmu, eps2, offset;
+    int base_b, base_f, base_g, base_gf;
+};
+
+__global__ void __launch_bounds__(128) k_contacts(ContactLaunch L, double* __restrict__ fb, BlockSink bs) {
+    const int b = blockIdx.x;
+    if (b < L.cb) {
+        const int p = b * 128 + threadIdx.x;
+        if (p < L.np) barrier_one(p, L.np, L.pairs, L.x, L.rest, L.dhat, L.kappa, fb, bs, L.base_b);
+    } else if (b < L.cf) {
+        const int p = (b - L.cb) * 128 + threadIdx.x;
+        if (p < L.nf)
+            friction_one(p, L.nf, L.fpairs, L.x, L.x0, L.flam, L.fcoord, L.fbasis, L.mu, L.eps2, fb, bs, L.base_f);
+    } else if (b < L.cg) {
+        const int p = (b - L.cf) * 128 + threadIdx.x;
+        if (p < L.ng) ground_one(p, L.ng, L.gpairs, L.x, L.offset, L.dhat, L.kappa, fb, bs, L.base_g);
+    } else {
+        const int p = (b - L.cg) * 128 + threadIdx.x;
+        if (p < L.ngf) fric_ground_one(p, L.ngf, L.gfpairs, L.x, L.x0, L.gflam, L.gmu, L.eps2, fb, bs, L.base_gf);
+    }
 }
 
 // soft constraints (GIPC.cu:6363-6407)
@@ -806,24 +860,45 @@ __global__ void k_run_starts(int m, const unsigned long long* __restrict__ ks, c
 
 // ... and entry q of the transposed copy at slot lpos[u] gets entry q of the block, at its
 // transposed place 3 (q % 3) + q / 3
-__global__ void k_run_sums(int m, const int* __restrict__ nuc, const int* __restrict__ start,
-                           const int* __restrict__ is, const double* __restrict__ cval, const int* __restrict__ lpos,
-                           double* __restrict__ u64, float* __restrict__ u32, double* __restrict__ l64,
-                           float* __restrict__ l32) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int u = (int)(t / 9), q = (int)(t % 9);
-    if (u >= nuc[0]) return;
-    const int j0 = start[u], j1 = start[u + 1];
-    double acc = 0.0;
-#pragma unroll 4
-    for (int j = j0; j < j1; j++) acc += cval[9 * (size_t)is[j] + q];
-    u64[9 * (size_t)u + q] = acc;
-    u32[9 * (size_t)u + q] = (float)acc;
-    const int k = lpos[u];
-    if (k >= 0) {
-        const int qt = 3 * (q % 3) + q / 3;
-        l64[9 * (size_t)k + qt] = acc;
-        l32[9 * (size_t)k + qt] = (float)acc;
+// One warp per unique block (grid-stride over the blocks): lane l adds the run's slots l,
+// l + 32, ... in order, then a fixed xor tree adds the lanes, so the sum is the same run to
+// run; lanes 0..8 store the nine entries (upper and, transposed, lower copies).
+__global__ void __launch_bounds__(256) k_run_sums(const int* __restrict__ nuc, const int* __restrict__ start,
+                                                  const int* __restrict__ is, const double* __restrict__ cval,
+                                                  const int* __restrict__ lpos, double* __restrict__ u64,
+                                                  float* __restrict__ u32, double* __restrict__ l64,
+                                                  float* __restrict__ l32) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int nu = nuc[0];
+    for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < nu; u += nw) {
+        const int j0 = start[u], j1 = start[u + 1];
+        double acc[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++) acc[q] = 0.0;
+        for (int j = j0 + lane; j < j1; j += 32) {
+            const double* v = cval + 9 * (size_t)is[j];
+#pragma unroll
+            for (int q = 0; q < 9; q++) acc[q] += v[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        if (lane < 9) {
+            double a = acc[0];
+#pragma unroll
+            for (int q = 1; q < 9; q++)
+                if (lane == q) a = acc[q];
+            u64[9 * (size_t)u + lane] = a;
+            u32[9 * (size_t)u + lane] = (float)a;
+            const int k = lpos[u];
+            if (k >= 0) {
+                const int qt = 3 * (lane % 3) + lane / 3;
+                l64[9 * (size_t)k + qt] = a;
+                l32[9 * (size_t)k + qt] = (float)a;
+            }
+        }
     }
 }
 
@@ -1214,33 +1289,42 @@ static int launch_contacts(SgipcCtx* c, const SgipcFemData* f, const SgipcContac
                            double* grad, cudaStream_t s, bool keep_dirichlet = false) {
     BlockSink bs = sink(c, f);
     if (keep_dirichlet) bs.btype = nullptr;
-    int base = 0;
-    if (k) SG_COUNT(c, (k->pair_num > 0) + (k->fric_num > 0 && p->frictionRate > 0.0) + (k->ground_num > 0) +
-                           (k->fric_gd_num > 0 && p->gd_frictionRate > 0.0));
-    if (k && k->pair_num > 0) {
-        k_barrier<<<nblk(k->pair_num, 128), 128, 0, s>>>(k->pair_num, (const int4*)k->pairs, f->vertexes,
-                                                          f->rest_vertexes, p->dHat, p->kappa, grad, bs, base);
-        base += 10 * k->pair_num;
+    if (!k) return 0;
+    ContactLaunch L{};
+    L.np = k->pair_num > 0 ? k->pair_num : 0;
+    L.nf = k->fric_num > 0 && p->frictionRate > 0.0 ? k->fric_num : 0;
+    L.ng = k->ground_num > 0 ? k->ground_num : 0;
+    L.ngf = k->fric_gd_num > 0 && p->gd_frictionRate > 0.0 ? k->fric_gd_num : 0;
+    L.cb = nblk(L.np, 128);
+    L.cf = L.cb + nblk(L.nf, 128);
+    L.cg = L.cf + nblk(L.ng, 128);
+    const int grid = L.cg + nblk(L.ngf, 128);
+    L.pairs = (const int4*)k->pairs;
+    L.fpairs = (const int4*)k->fric_pairs;
+    L.gpairs = k->ground_pairs;
+    L.gfpairs = k->fric_gd_pairs;
+    L.x = f->vertexes;
+    L.x0 = f->o_vertexes;
+    L.rest = f->rest_vertexes;
+    L.flam = k->fric_lambda;
+    L.fcoord = k->fric_coord;
+    L.fbasis = k->fric_basis;
+    L.gflam = k->fric_gd_lambda;
+    L.dhat = p->dHat;
+    L.kappa = p->kappa;
+    L.mu = p->frictionRate;
+    L.gmu = p->gd_frictionRate;
+    L.eps2 = p->fDhat * p->dt * p->dt;
+    L.offset = p->ground_offset;
+    L.base_b = 0;
+    L.base_f = 10 * L.np;
+    L.base_g = L.base_f + 10 * L.nf;
+    L.base_gf = L.base_g + L.ng;
+    if (grid > 0) {
+        SG_COUNT(c, 1);
+        k_contacts<<<grid, 128, 0, s>>>(L, grad, bs);
     }
-    const double eps2 = p->fDhat * p->dt * p->dt;
-    if (k && k->fric_num > 0 && p->frictionRate > 0.0) {
-        k_friction<<<nblk(k->fric_num, 128), 128, 0, s>>>(k->fric_num, (const int4*)k->fric_pairs, f->vertexes,
-                                                           f->o_vertexes, k->fric_lambda, k->fric_coord, k->fric_basis,
-                                                           p->frictionRate, eps2, grad, bs, base);
-        base += 10 * k->fric_num;
-    }
-    if (k && k->ground_num > 0) {
-        k_ground<<<nblk(k->ground_num), SGIPC_BLOCK, 0, s>>>(k->ground_num, k->ground_pairs, f->vertexes,
-                                                              p->ground_offset, p->dHat, p->kappa, grad, bs, base);
-        base += k->ground_num;
-    }
-    if (k && k->fric_gd_num > 0 && p->gd_frictionRate > 0.0) {
-        k_fric_ground<<<nblk(k->fric_gd_num), SGIPC_BLOCK, 0, s>>>(k->fric_gd_num, k->fric_gd_pairs, f->vertexes,
-                                                                    f->o_vertexes, k->fric_gd_lambda,
-                                                                    p->gd_frictionRate, eps2, grad, bs, base);
-        base += k->fric_gd_num;
-    }
-    return base;
+    return L.base_gf + L.ngf;
 }
 
 static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
@@ -1272,8 +1356,8 @@ static SgipcStatus merge_contacts(SgipcCtx* c, int m, cudaStream_t s) {
                                                                    c->lcount + n + 1, c->cu_ptr, c->cl_idx);
     k_lower_rank<<<nblk(m), SGIPC_BLOCK, 0, s>>>(c->nuc, c->uc_row, c->uc_col, c->cl_ptr, c->cl_idx, c->lpos,
                                                  c->cl_col);
-    k_run_sums<<<nblk(9LL * m), SGIPC_BLOCK, 0, s>>>(m, c->nuc, c->run_start, c->cidx_s, c->cval, c->lpos, c->uc64,
-                                                     c->uc32, c->cl64, c->cl32);
+    k_run_sums<<<std::min(nblk(32LL * m), 8 * 148), SGIPC_BLOCK, 0, s>>>(c->nuc, c->run_start, c->cidx_s, c->cval,
+                                                                         c->lpos, c->uc64, c->uc32, c->cl64, c->cl32);
     SG_LAUNCH_CHECK(c, "contact merge");
     return SGIPC_OK;
 }
