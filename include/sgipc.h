@@ -44,10 +44,11 @@ typedef enum SgipcCriterion {
     SGIPC_CRIT_TRUE = 1   /* ||b - A x||_2 <= tol * ||b||_2 */
 } SgipcCriterion;
 
-/* Static topology, given once at context creation [host].  Mirrors what
- * StiffGIPC's init reads: the tet/triangle/hinge connectivity (device_TetraData,
- * StiffGIPC/device_fem_data.cuh:17-78) and the MAS neighbour CSR + part maps
- * (MASPreconditioner::initPreconditioner_Neighbor, StiffGIPC/MASPreconditioner.cu:2264). */
+/* Static topology, given once at context creation [host or dev: each array may be a host,
+ * pinned, managed or device pointer; device arrays, as device_TetraData keeps them, are read
+ * back once].  Mirrors what StiffGIPC's init reads: the tet/triangle/hinge connectivity
+ * (device_TetraData, StiffGIPC/device_fem_data.cuh:17-78) and the MAS neighbour CSR + part
+ * maps (MASPreconditioner::initPreconditioner_Neighbor, StiffGIPC/MASPreconditioner.cu:2264). */
 typedef struct SgipcTopology {
     int32_t         vertex_num;
     int32_t         tet_num;

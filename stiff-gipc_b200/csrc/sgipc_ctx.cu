@@ -209,9 +209,48 @@ static SgipcStatus build_static(SgipcCtx* c, const SgipcTopology* t) {
     return SGIPC_OK;
 }
 
-extern "C" SgipcStatus sgipc_create(const SgipcTopology* t, int device, SgipcCtx** out) {
-    if (!t || !out) return SGIPC_BAD_INPUT;
+// A host copy of a topology array the caller passed in device memory (the reference keeps
+// its connectivity in device_TetraData); host, pinned and managed arrays are read in place.
+template <class T>
+static const T* host_view(const T* p, size_t n, std::vector<T>& keep, cudaError_t& err) {
+    if (!p || n == 0) return p;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();  // an unregistered host pointer on older runtimes
+        return p;
+    }
+    if (a.type != cudaMemoryTypeDevice) return p;
+    keep.resize(n);
+    cudaError_t e = cudaMemcpy(keep.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) err = e;
+    return keep.data();
+}
+
+extern "C" SgipcStatus sgipc_create(const SgipcTopology* t_in, int device, SgipcCtx** out) {
+    if (!t_in || !out) return SGIPC_BAD_INPUT;
     *out = nullptr;
+    // the topology arrays as host arrays, wherever the caller keeps them
+    SgipcTopology th = *t_in;
+    std::vector<uint32_t> k_tets, k_tris, k_hin, k_soft, k_nstart, k_nlist;
+    std::vector<int32_t> k_hadj, k_pm, k_rm;
+    {
+        sgipc::DeviceScope scope(device);
+        if (scope.err != cudaSuccess) return SGIPC_CUDA_ERROR;
+        cudaError_t err = cudaSuccess;
+        const size_t nv = th.vertex_num > 0 ? (size_t)th.vertex_num : 0;
+        th.tetrahedras = host_view(th.tetrahedras, 4 * (size_t)std::max(th.tet_num, 0), k_tets, err);
+        th.triangles = host_view(th.triangles, 3 * (size_t)std::max(th.tri_num, 0), k_tris, err);
+        th.tri_edges = host_view(th.tri_edges, 2 * (size_t)std::max(th.tri_edge_num, 0), k_hin, err);
+        th.tri_edge_adj_vertex = host_view(th.tri_edge_adj_vertex, 2 * (size_t)std::max(th.tri_edge_num, 0), k_hadj, err);
+        th.targetIndex = host_view(th.targetIndex, (size_t)std::max(th.soft_num, 0), k_soft, err);
+        th.partId_map_real = host_view(th.partId_map_real, (size_t)std::max(th.part_map_size, 0), k_pm, err);
+        th.real_map_partId = host_view(th.real_map_partId, nv, k_rm, err);
+        th.neighborStart = host_view(th.neighborStart, nv + 1, k_nstart, err);
+        if (err == cudaSuccess && th.neighborStart && nv > 0)
+            th.neighborList = host_view(th.neighborList, (size_t)th.neighborStart[nv], k_nlist, err);
+        if (err != cudaSuccess) return SGIPC_CUDA_ERROR;
+    }
+    const SgipcTopology* t = &th;
     if (t->vertex_num <= 0 || t->tet_num < 0 || t->tri_num < 0 || t->tri_edge_num < 0 || t->soft_num < 0 ||
         t->max_pairs < 0 || t->max_ground < 0 || t->max_fric_pairs < 0 || t->max_fric_ground < 0)
         return SGIPC_BAD_INPUT;

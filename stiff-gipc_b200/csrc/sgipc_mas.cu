@@ -516,7 +516,11 @@ static int num_levels(int nodes) {
 // assembly and the host's enqueue time is on the critical path.  Barrier words live in
 // info[20] (arrivals) and info[21] (abort, set when a wait exceeds its limit).
 constexpr int kHierThreads = 256;
-constexpr int kHierMaxCtas = 32;
+constexpr int kHierMaxCtas = 296;      // the largest grid the build may take (hier_part size)
+// its grid beside the assembly (SGIPC_HIER_CTAS overrides): measured on the two-cube bench step,
+// the MAS build ends at 0.41 ms with 32 CTAs, 0.36 ms with 74 and 0.41 ms with 148 (the
+// assembly's kernels then lose their SMs)
+constexpr int kHierDefaultCtas = 74;
 constexpr long long kHierSpinLimit = 1LL << 24;
 
 struct HierArgs {
@@ -788,7 +792,11 @@ SgipcStatus mas_create(SgipcCtx* c, const SgipcTopology* t) {
         SG_CHECK(c, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
         SG_CHECK(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
         SG_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_hierarchy, kHierThreads, 0));
-        m.hier_grid = coop && per > 0 ? (nsm * per < kHierMaxCtas ? nsm * per : kHierMaxCtas) : 0;
+        // the build runs beside the assembly's kernels: a small grid leaves them the SMs
+        int want = kHierDefaultCtas;
+        const char* e = getenv("SGIPC_HIER_CTAS");
+        if (e && atoi(e) > 0) want = atoi(e) < kHierMaxCtas ? atoi(e) : kHierMaxCtas;
+        m.hier_grid = coop && per > 0 ? (nsm * per < want ? nsm * per : want) : 0;
     }
     size_t tb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tb, m.bank_cnt, m.bank_off, m.npos / 16 + 2);
