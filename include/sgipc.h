@@ -375,6 +375,31 @@ SgipcStatus sgipc_contact_partition(SgipcCtx* ctx, const SgipcFemData* fem, cons
                                     int32_t* fem_cols, double* fem_vals, int32_t* fem_count, double* point_grad,
                                     void* stream);
 
+/* ---- barrier stiffness (kappa) adaptation ----------------------------------------------- */
+
+/* GIPC::initKappa with suggestKappa and upperBoundKappa (GIPC.cu:9850-9929): with contact
+ * pairs, kappa = -(g_c . g_E) / (g_c . g_c) where g_E is the kinetic, tet elastic and soft-
+ * constraint gradient and g_c the barrier and ground gradient at kappa = 1 (both at
+ * fem->vertexes), raised to the suggested minimum minKappaCoef * meanMass / (4e-16 bbox^2
+ * H_b) and bounded by 100 times it (meanMass 0: without it).  kappa [host, in/out] keeps its
+ * value without pairs.  Uses the context's element gradient scratch: call it before
+ * sgipc_assemble, as the reference does.  Synchronises. */
+SgipcStatus sgipc_init_kappa(SgipcCtx* ctx, const SgipcFemData* fem, const SgipcContacts* con,
+                             const SgipcParams* prm, double mean_mass, double bbox_diag2, double min_kappa_coef,
+                             double* kappa, void* stream);
+/* GIPC::computeCloseGroundVal / computeSelfCloseVal (GIPC.cu:8776, 9219): records the ground
+ * vertices of con [dev] whose squared distance to the plane y = ground_offset, and the pairs
+ * whose squared distance, is below dtol (the reference's dTol = 1e-18 bbox^2), with those
+ * values, at x [dev].  counts [host int[2], may be null]: ground vertices and pairs recorded.
+ * Synchronises. */
+SgipcStatus sgipc_close_record(SgipcCtx* ctx, const double* x, const SgipcContacts* con, double dtol,
+                               double ground_offset, int32_t* counts, void* stream);
+/* GIPC::checkCloseGroundVal || checkSelfCloseVal (GIPC.cu:8794, 9230): *changed = 1 when a
+ * recorded ground vertex or pair is closer at x [dev] than when it was recorded (the caller
+ * then doubles kappa and bounds it, GIPC::postLineSearch GIPC.cu:10777-10806).  Synchronises. */
+SgipcStatus sgipc_close_check(SgipcCtx* ctx, const double* x, double ground_offset, int32_t* changed,
+                              void* stream);
+
 /* ---- the global FEM + ABD system ------------------------------------------------------- */
 
 /* GlobalLinearSystem::solve_linear_system + distribute_solution (global_linear_system.cu:

@@ -16,6 +16,8 @@
 //   * dynamic part: every contact pair writes its upper blocks under a (row,col) key; one
 //     radix sort plus a segmented sum gives the unique contact blocks, kept row-sorted
 //     together with a transposed index list so that SpMV needs no atomics.
+#include <cmath>
+
 #include <cub/cub.cuh>
 
 #include "sgipc_internal.cuh"
@@ -1597,6 +1599,186 @@ extern "C" SgipcStatus sgipc_contact_partition(SgipcCtx* c, const SgipcFemData* 
                  cnt[0], cnt[1], cap);
         return SGIPC_CAPACITY;
     }
+    return SGIPC_OK;
+}
+
+// ---- barrier stiffness adaptation (GIPC::initKappa / suggestKappa / upperBoundKappa,
+// GIPC.cu:9850-9929; the close-constraint checks of GIPC::postLineSearch, GIPC.cu:10777-10806)
+// shape_grads += the tet rows (the first 4 * nt element gradient rows) of each vertex
+__global__ void k_gather_grad_tets(int nv, int limit, const int* __restrict__ vptr, const int* __restrict__ vinc,
+                                   const double* __restrict__ egrad, double* __restrict__ out) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 3 * nv) return;
+    const int v = tid / 3, q = tid % 3;
+    double acc = 0.0;
+    for (int k = vptr[v]; k < vptr[v + 1]; k++) {
+        const int e = vinc[k];
+        if (e < limit) acc += egrad[3 * (size_t)e + q];
+    }
+    out[tid] += acc;
+}
+
+// compute_H_b (GIPC.cu, used by suggestKappa / upperBoundKappa): the barrier's second
+// derivative scale at d = 1e-16 bbox^2
+static double kappa_hb(double bbox_diag2, double dhat) {
+    const double d = 1.0e-16 * bbox_diag2, t = d - dhat;
+    return (std::log(d / dhat) * -2.0 - t * 4.0 / d) + 1.0 / (d * d) * (t * t);
+}
+
+extern "C" SgipcStatus sgipc_init_kappa(SgipcCtx* c, const SgipcFemData* f, const SgipcContacts* k,
+                                        const SgipcParams* p, double mean_mass, double bbox_diag2,
+                                        double min_kappa_coef, double* kappa, void* stream) {
+    SgipcStatus st = check_inputs(c, f, k, p);
+    if (st != SGIPC_OK) return st;
+    if (!kappa || !(bbox_diag2 > 0.0)) return SGIPC_BAD_INPUT;
+    if (!k || k->pair_num <= 0) return SGIPC_OK;  // the reference adapts only with contact pairs
+    cudaStream_t s = (cudaStream_t)stream;
+    SG_DEVICE(c);
+    const int nv = c->nv;
+    double* GE = c->tmp64;   // kinetic + tet elastic + soft-constraint gradient
+    double* gc = c->tmp64b;  // barrier + ground gradient at kappa = 1
+    SG_COUNT(c, 2 + (c->nsoft > 0));
+    k_kinetic<<<nblk(3LL * nv), SGIPC_BLOCK, 0, s>>>(nv, f->vertexes, f->xTilta, f->masses, GE, gc);
+    if ((st = launch_fem(c, f, p, s)) != SGIPC_OK) return st;
+    k_gather_grad_tets<<<nblk(3LL * nv), SGIPC_BLOCK, 0, s>>>(nv, 4 * c->nt, c->vinc_ptr, c->vinc, c->egrad, GE);
+    if (c->nsoft > 0) {
+        BlockSink bs = sink(c, f);
+        k_soft<<<nblk(c->nsoft), SGIPC_BLOCK, 0, s>>>(c->nsoft, c->soft_idx, f->vertexes, f->targetVert,
+                                                      p->motionRate * p->softRate * p->softRate, GE, bs, 0);
+    }
+    SgipcContacts only = *k;
+    only.fric_num = 0;
+    only.fric_gd_num = 0;
+    SgipcParams p1 = *p;
+    p1.kappa = 1.0;
+    p1.frictionRate = 0.0;
+    p1.gd_frictionRate = 0.0;
+    launch_contacts(c, f, &only, &p1, gc, s);
+    SG_LAUNCH_CHECK(c, "init kappa gradients");
+    if ((st = dot64(c, gc, GE, 3 * nv, c->dot_out, s)) != SGIPC_OK) return st;
+    if ((st = dot64(c, gc, gc, 3 * nv, c->dot_out + 1, s)) != SGIPC_OK) return st;
+    double h[2];
+    SG_CHECK(c, cudaMemcpyAsync(h, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    double K = *kappa;
+    double minK = -h[0] / h[1];
+    if (minK > 0.0) K = minK;
+    const double hb = kappa_hb(bbox_diag2, p->dHat);
+    // suggestKappa overwrites minKappa with its suggestion, which then bounds Kappa below
+    minK = mean_mass == 0.0 ? min_kappa_coef / (4.0e-16 * bbox_diag2 * hb)
+                            : min_kappa_coef * mean_mass / (4.0e-16 * bbox_diag2 * hb);
+    if (K < minK) K = minK;
+    double kmax = 100 * min_kappa_coef * mean_mass / (4.0e-16 * bbox_diag2 * hb);
+    if (mean_mass == 0.0) kmax = 100 * min_kappa_coef / (4.0e-16 * bbox_diag2 * hb);
+    if (K > kmax) K = kmax;
+    *kappa = K;
+    return SGIPC_OK;
+}
+
+// close constraints: ground vertices and pairs closer than dTol (squared), with their value
+__global__ void k_close_ground_record(int ng, const uint32_t* __restrict__ gp, const double* __restrict__ x,
+                                      double offset, double dtol, uint32_t* __restrict__ id,
+                                      double* __restrict__ val, unsigned int* __restrict__ cnt) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ng) return;
+    const uint32_t v = gp[p];
+    const double d = x[3 * (size_t)v + 1] - offset, d2 = d * d;
+    if (d2 < dtol) {
+        const unsigned int i = atomicAdd(cnt, 1u);
+        id[i] = v;
+        val[i] = d2;
+    }
+}
+
+__global__ void k_close_pair_record(int np, const int4* __restrict__ pairs, const double* __restrict__ x,
+                                    double dtol, int4* __restrict__ id, double* __restrict__ val,
+                                    unsigned int* __restrict__ cnt) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    int v[4], nvp;
+    const int kind = decode_pair(pairs[p], v, nvp);
+    d3 X[4], g[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) X[a] = a < nvp ? ld3(x, v[a]) : mk(0, 0, 0);
+    const double d2 = dist2_grad(kind, X, g);
+    if (d2 < dtol) {
+        const unsigned int i = atomicAdd(cnt + 1, 1u);
+        id[i] = pairs[p];
+        val[i] = d2;
+    }
+}
+
+// flag[0] = 1 when a recorded ground vertex or pair is closer now than when recorded
+__global__ void k_close_check(int ng, int np, const uint32_t* __restrict__ gid, const double* __restrict__ gval,
+                              const int4* __restrict__ pid, const double* __restrict__ pval,
+                              const double* __restrict__ x, double offset, int* __restrict__ flag) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ng) {
+        const double d = x[3 * (size_t)gid[t] + 1] - offset;
+        if (d * d < gval[t]) *flag = 1;
+    } else if (t < ng + np) {
+        int v[4], nvp;
+        const int kind = decode_pair(pid[t - ng], v, nvp);
+        d3 X[4], g[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) X[a] = a < nvp ? ld3(x, v[a]) : mk(0, 0, 0);
+        if (dist2_grad(kind, X, g) < pval[t - ng]) *flag = 1;
+    }
+}
+
+extern "C" SgipcStatus sgipc_close_record(SgipcCtx* c, const double* x, const SgipcContacts* k, double dtol,
+                                          double ground_offset, int32_t* counts, void* stream) {
+    if (!c || !x || !k || (k->pair_num > 0 && !k->pairs) || (k->ground_num > 0 && !k->ground_pairs))
+        return SGIPC_BAD_INPUT;
+    if (k->pair_num > c->max_pairs || k->ground_num > c->max_ground) return SGIPC_CAPACITY;
+    cudaStream_t s = (cudaStream_t)stream;
+    SG_DEVICE(c);
+    if (!c->close_cnt) {
+        SG_CHECK(c, cudaMalloc((void**)&c->close_gid, sizeof(uint32_t) * (size_t)std::max(c->max_ground, 1)));
+        SG_CHECK(c, cudaMalloc((void**)&c->close_gval, sizeof(double) * (size_t)std::max(c->max_ground, 1)));
+        SG_CHECK(c, cudaMalloc((void**)&c->close_pid, sizeof(int4) * (size_t)std::max(c->max_pairs, 1)));
+        SG_CHECK(c, cudaMalloc((void**)&c->close_pval, sizeof(double) * (size_t)std::max(c->max_pairs, 1)));
+        SG_CHECK(c, cudaMalloc((void**)&c->close_cnt, sizeof(unsigned int) * 4));
+    }
+    SG_CHECK(c, cudaMemsetAsync(c->close_cnt, 0, sizeof(unsigned int) * 4, s));
+    SG_COUNT(c, (k->ground_num > 0) + (k->pair_num > 0));
+    if (k->ground_num > 0)
+        k_close_ground_record<<<nblk(k->ground_num), SGIPC_BLOCK, 0, s>>>(
+            k->ground_num, k->ground_pairs, x, ground_offset, dtol, c->close_gid, c->close_gval, c->close_cnt);
+    if (k->pair_num > 0)
+        k_close_pair_record<<<nblk(k->pair_num), SGIPC_BLOCK, 0, s>>>(
+            k->pair_num, (const int4*)k->pairs, x, dtol, (int4*)c->close_pid, c->close_pval, c->close_cnt);
+    SG_LAUNCH_CHECK(c, "close constraints");
+    unsigned int h[2];
+    SG_CHECK(c, cudaMemcpyAsync(h, c->close_cnt, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    c->close_num[0] = (int)h[0];
+    c->close_num[1] = (int)h[1];
+    if (counts) {
+        counts[0] = (int32_t)h[0];
+        counts[1] = (int32_t)h[1];
+    }
+    return SGIPC_OK;
+}
+
+extern "C" SgipcStatus sgipc_close_check(SgipcCtx* c, const double* x, double ground_offset, int32_t* changed,
+                                         void* stream) {
+    if (!c || !x || !changed) return SGIPC_BAD_INPUT;
+    *changed = 0;
+    const int ng = c->close_cnt ? c->close_num[0] : 0, np = c->close_cnt ? c->close_num[1] : 0;
+    if (ng + np == 0) return SGIPC_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    SG_DEVICE(c);
+    SG_CHECK(c, cudaMemsetAsync(c->close_cnt + 2, 0, sizeof(unsigned int), s));
+    SG_COUNT(c, 1);
+    k_close_check<<<nblk(ng + np), SGIPC_BLOCK, 0, s>>>(ng, np, c->close_gid, c->close_gval, (const int4*)c->close_pid,
+                                                        c->close_pval, x, ground_offset,
+                                                        reinterpret_cast<int*>(c->close_cnt + 2));
+    SG_LAUNCH_CHECK(c, "close check");
+    unsigned int h = 0;
+    SG_CHECK(c, cudaMemcpyAsync(&h, c->close_cnt + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    SG_CHECK(c, cudaStreamSynchronize(s));
+    *changed = h != 0;
     return SGIPC_OK;
 }
 

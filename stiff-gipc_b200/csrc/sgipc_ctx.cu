@@ -229,6 +229,17 @@ static const T* host_view(const T* p, size_t n, std::vector<T>& keep, cudaError_
 extern "C" SgipcStatus sgipc_create(const SgipcTopology* t_in, int device, SgipcCtx** out) {
     if (!t_in || !out) return SGIPC_BAD_INPUT;
     *out = nullptr;
+    {
+        const SgipcTopology* t = t_in;  // counts and pointers, before any CUDA call
+        if (t->vertex_num <= 0 || t->tet_num < 0 || t->tri_num < 0 || t->tri_edge_num < 0 || t->soft_num < 0 ||
+            t->max_pairs < 0 || t->max_ground < 0 || t->max_fric_pairs < 0 || t->max_fric_ground < 0)
+            return SGIPC_BAD_INPUT;
+        if ((t->tet_num && !t->tetrahedras) || (t->tri_num && !t->triangles) ||
+            (t->tri_edge_num && (!t->tri_edges || !t->tri_edge_adj_vertex)) || !t->partId_map_real ||
+            !t->real_map_partId || !t->neighborStart || (t->soft_num && !t->targetIndex))
+            return SGIPC_BAD_INPUT;
+        if (t->part_map_size < t->vertex_num || t->part_map_size % SGIPC_BANK) return SGIPC_BAD_INPUT;
+    }
     // the topology arrays as host arrays, wherever the caller keeps them
     SgipcTopology th = *t_in;
     std::vector<uint32_t> k_tets, k_tris, k_hin, k_soft, k_nstart, k_nlist;
@@ -251,14 +262,6 @@ extern "C" SgipcStatus sgipc_create(const SgipcTopology* t_in, int device, Sgipc
         if (err != cudaSuccess) return SGIPC_CUDA_ERROR;
     }
     const SgipcTopology* t = &th;
-    if (t->vertex_num <= 0 || t->tet_num < 0 || t->tri_num < 0 || t->tri_edge_num < 0 || t->soft_num < 0 ||
-        t->max_pairs < 0 || t->max_ground < 0 || t->max_fric_pairs < 0 || t->max_fric_ground < 0)
-        return SGIPC_BAD_INPUT;
-    if ((t->tet_num && !t->tetrahedras) || (t->tri_num && !t->triangles) ||
-        (t->tri_edge_num && (!t->tri_edges || !t->tri_edge_adj_vertex)) || !t->partId_map_real ||
-        !t->real_map_partId || !t->neighborStart || (t->soft_num && !t->targetIndex))
-        return SGIPC_BAD_INPUT;
-    if (t->part_map_size < t->vertex_num || t->part_map_size % SGIPC_BANK) return SGIPC_BAD_INPUT;
     SgipcCtx* c = new SgipcCtx();
     memset(c, 0, sizeof(SgipcCtx));
     c->device = device;
@@ -372,7 +375,8 @@ extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
                     c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,
                     c->cu_ptr, c->cl_ptr, c->cl_idx, c->lcount, c->lpos, c->cub_tmp, c->dflag,
                     c->frow_ptr, c->fcol, c->fup, c->flo, c->fval64, c->fval32, c->cl_col, c->cl64, c->cl32, c->run_start, c->en_part, c->en_terms, c->ccd_part, c->ccd_out, c->ccd_bad, c->en_ticket, c->ccd_ticket,
-                    c->cs_ptr, c->cs_cols, c->cs_lcol, c->cs_dslot};
+                    c->cs_ptr, c->cs_cols, c->cs_lcol, c->cs_dslot, c->close_gid, c->close_gval, c->close_pid,
+                    c->close_pval, c->close_cnt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_en) cudaFreeHost(c->h_en);

@@ -230,6 +230,15 @@ struct SgipcCtx {
     // cs_grid CTAs of 128 rows: per CTA the sorted distinct columns of its rows
     // (cs_cols[cs_ptr[c] .. cs_ptr[c+1])), each full-pattern entry's slot among them
     // (cs_lcol) and each row's own slot (cs_dslot); cs_cap = the largest set
+    // close constraints of the barrier-stiffness update (sgipc_close_record / _check): the
+    // ground vertices and the pairs closer than dTol at the last record, with their values;
+    // close_cnt [4] device counters (ground, pairs, the check's flag), close_num their host copy
+    uint32_t* close_gid;
+    double* close_gval;
+    void* close_pid;  // int4
+    double* close_pval;
+    unsigned int* close_cnt;
+    int close_num[2];
     int* cs_ptr;
     int* cs_cols;
     int* cs_lcol;

@@ -116,6 +116,10 @@ SIGNATURES = {
     "sgipc_friction_setup": ([_vp, _vp, _vp, _i32, _vp, _i32, C.c_double, C.c_double, C.c_double, _vp, _vp, _vp,
                               _vp, _vp, _vp, _vp, _vp, _vp], _i32),
     "sgipc_profile_pcg": ([_vp, C.c_char_p, _i32, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _vp], _i32),
+    "sgipc_init_kappa": ([_vp, C.POINTER(SgipcFemData), C.POINTER(SgipcContacts), C.POINTER(SgipcParams),
+                          C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double), _vp], _i32),
+    "sgipc_close_record": ([_vp, _vp, C.POINTER(SgipcContacts), C.c_double, C.c_double, _vp, _vp], _i32),
+    "sgipc_close_check": ([_vp, _vp, C.c_double, C.POINTER(_i32), _vp], _i32),
     "sgipc_contact_partition": ([_vp, C.POINTER(SgipcFemData), C.POINTER(SgipcContacts), C.POINTER(SgipcParams),
                                  _i32, _i32, _vp, _vp, _vp, C.POINTER(_i32), _vp, _vp, _vp, C.POINTER(_i32), _vp,
                                  _vp], _i32),

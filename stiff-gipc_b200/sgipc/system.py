@@ -392,6 +392,50 @@ class GIPC:
         tet.fric_gd_pairs, tet.fric_gd_lambda = gpp[:ng], gl[:ng]
         return list(cp)
 
+    # ---- barrier stiffness ------------------------------------------------------------
+    def initKappa(self, min_kappa_coef: float = 1e11, tet: Optional[DeviceTetraData] = None) -> float:
+        """GIPC::initKappa (GIPC.cu:9887-9929, with suggestKappa and upperBoundKappa): the
+        barrier stiffness balancing the contact gradient against the kinetic, elastic and
+        soft-constraint one at the current positions (``sgipc_init_kappa``); it becomes
+        ``params["kappa"]`` and is returned.  Unchanged without contact pairs."""
+        tet = tet or self.tet
+        f, k, p = tet.fem_struct_cached(), tet.contact_struct_cached(), self._params()
+        kap = C.c_double(float(self.params["kappa"]))
+        N.check(N.lib().sgipc_init_kappa(self.ctx, C.byref(f), C.byref(k), C.byref(p),
+                                         float(self.params.get("meanMass", 0.0)), float(self.params["bboxDiag2"]),
+                                         float(min_kappa_coef), C.byref(kap), _stream()), self.ctx)
+        self.params["kappa"] = kap.value
+        return kap.value
+
+    def closeRecord(self, tet: Optional[DeviceTetraData] = None):
+        """computeCloseGroundVal + computeSelfCloseVal (GIPC.cu:8776, 9219) with the
+        reference's dTol = 1e-18 bbox^2: (ground vertices, pairs) recorded."""
+        tet = tet or self.tet
+        k = tet.contact_struct_cached()
+        cnt = (C.c_int32 * 2)()
+        N.check(N.lib().sgipc_close_record(self.ctx, _p(tet.vertexes), C.byref(k),
+                                           1e-18 * float(self.params["bboxDiag2"]),
+                                           float(self.params.get("ground_offset", 0.0)), cnt, _stream()), self.ctx)
+        return int(cnt[0]), int(cnt[1])
+
+    def postLineSearch(self, min_kappa_coef: float = 1e11, tet: Optional[DeviceTetraData] = None) -> float:
+        """GIPC::postLineSearch (GIPC.cu:10777-10806) after a line search to tet.vertexes: with
+        kappa 0, initKappa; otherwise kappa doubles (within its upper bound) when a recorded
+        close ground vertex or pair came closer, and the close sets are recorded anew."""
+        tet = tet or self.tet
+        if float(self.params["kappa"]) == 0.0:
+            return self.initKappa(min_kappa_coef, tet)
+        changed = C.c_int32()
+        N.check(N.lib().sgipc_close_check(self.ctx, _p(tet.vertexes), float(self.params.get("ground_offset", 0.0)),
+                                          C.byref(changed), _stream()), self.ctx)
+        if changed.value:
+            from .scenes import suggest_kappa
+            kmax = 100.0 * suggest_kappa(float(self.params["bboxDiag2"]), float(self.params["dHat"]),
+                                         float(self.params.get("meanMass", 0.0)), min_kappa_coef)
+            self.params["kappa"] = min(2.0 * float(self.params["kappa"]), kmax)
+        self.closeRecord(tet)
+        return float(self.params["kappa"])
+
     def contactPartition(self, abd_first: int, capacity: Optional[int] = None,
                          tet: Optional[DeviceTetraData] = None):
         """GIPC::partitionContactHessian (GIPC.cu:9932-10108) for a scene whose vertices
