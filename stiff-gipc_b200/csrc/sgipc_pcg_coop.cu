@@ -24,7 +24,7 @@
 // barrier every CTA adds all partials in the same fixed order, so all CTAs take identical
 // decisions from identical numbers (partials are double-buffered by epoch parity).  Values
 // written by one CTA and read by another inside the kernel are loaded through L2
-// (ld.global.cg) or, after the barrier's gpu-scope fence, through L1.  Waits are bounded:
+// (ld.global.cg) or, after the barrier's acquire, through L1.  Waits are bounded:
 // past the limit a CTA raises the abort word, every CTA leaves, and the solve reports
 // SGIPC_CUDA_ERROR.
 #include <cstdlib>
@@ -54,6 +54,26 @@ __host__ __device__ constexpr size_t coop_contact_bytes(int rows, int kcap, int 
                     : 0;
 }
 constexpr int kContactSlots = 768;  // contact entries per CTA held in shared memory
+
+// dst[k] = src[k] for k < n by the whole CTA, eight loads in flight per thread (a plain
+// strided loop waits out one L2 round trip per element a thread copies)
+template <class T>
+__device__ __forceinline__ void smem_fill(T* dst, const T* __restrict__ src, int n) {
+    constexpr int kU = 8;
+    for (int k0 = threadIdx.x; k0 < n; k0 += kU * (int)blockDim.x) {
+        T v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int k = k0 + u * (int)blockDim.x;
+            if (k < n) v[u] = __ldg(src + k);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int k = k0 + u * (int)blockDim.x;
+            if (k < n) dst[k] = v[u];
+        }
+    }
+}
 
 struct GridBarrier {
     unsigned int* count;  // arrivals since launch (zeroed before the launch)
@@ -117,7 +137,7 @@ struct CoopArgs {
     T* p1;
     T* Ap;
     PcgScalars* sc;
-    double* partial;   // [2][NR][gridDim.x]
+    double* partial;   // [2][stride][gridDim.x] (stride: NR values, five NR in the fused solve)
     GridBarrier br;
     int nv;
     int nd01;          // domains of levels 0 and 1
@@ -188,9 +208,11 @@ __device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch, int tag)
             }
             if (k > 256) __nanosleep(32);
         }
-        // gpu-scope fence after the acquire: the SM's L1 holds no line older than the
-        // barrier, so the CTA may read other CTAs' writes with ordinary (L1-cached) loads
-        __threadfence();
+        // No fence here: the acquire load that saw the count orders every later access of
+        // this thread after the other CTAs' released writes, and the __syncthreads below
+        // extends that order to the CTA's other threads (the memory model's causality
+        // order is transitive through CTA barriers), so their ordinary loads, L1-cached
+        // ones included, see those writes.  (A fence here measured 0.9 us per iteration.)
         stamp(br, epoch, 1);
         s_ok = ok;
     }
@@ -985,6 +1007,9 @@ __device__ void phase_fused_update(const CoopArgs<T, M, NR>& a, const double (&a
                                    bool first, const T* p_old, T* p_new, const T* ap_old, T* ap_new, const T* r_old,
                                    T* r_new, const bool (&run)[NR], double (&acc)[2 * NR], M (*s_l1)[3 * NR],
                                    const PosCache& pc) {
+    // components of a vertex loaded together: all three with one right-hand side (with four,
+    // the 72 values spill and the batched solve measured slower)
+    constexpr int kQ = NR == 1 ? 3 : 1;
     const MasView& mv = a.mv;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int start1 = mv.info[1], count1 = mv.info[9];
@@ -1012,46 +1037,57 @@ __device__ void phase_fused_update(const CoopArgs<T, M, NR>& a, const double (&a
 #pragma unroll
             for (int k = 0; k < NR * 3; k++) val[k] = 0;
             if (v >= 0) {
+                // the loads of kQ components go out together, ahead of their stores: the
+                // compiler cannot move a load above a store to another array (it may alias),
+                // so component by component would cost one L2 round trip each
 #pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    const size_t k = (size_t)(3 * v + q) * NR;
-                    T zv[NR], wv[NR], po[NR], ao[NR], rv[NR], xv[NR];
-                    ldn<true, T, NR>(a.z + k, zv);
-                    ldn<true, T, NR>(a.w + k, wv);
-                    ldn<true, T, NR>(r_old + k, rv);
-                    if (!first) {
-                        ldn<true, T, NR>(p_old + k, po);
-                        ldn<true, T, NR>(ap_old + k, ao);
-                    } else {
+                for (int q0 = 0; q0 < 3; q0 += kQ) {
+                    T zv[kQ][NR], wv[kQ][NR], po[kQ][NR], ao[kQ][NR], rv[kQ][NR], xv[kQ][NR];
 #pragma unroll
-                        for (int r = 0; r < NR; r++) po[r] = ao[r] = 0;
-                    }
+                    for (int j = 0; j < kQ; j++) {
+                        const size_t k = (size_t)(3 * v + q0 + j) * NR;
+                        ldn<true, T, NR>(a.z + k, zv[j]);
+                        ldn<true, T, NR>(a.w + k, wv[j]);
+                        ldn<true, T, NR>(r_old + k, rv[j]);
+                        if (!first) {
+                            ldn<true, T, NR>(p_old + k, po[j]);
+                            ldn<true, T, NR>(ap_old + k, ao[j]);
+                        } else {
 #pragma unroll
-                    for (int r = 0; r < NR; r++) xv[r] = 0;
-                    if (own) ldn<true, T, NR>(a.x + k, xv);
-                    T pn[NR], an[NR];
-#pragma unroll
-                    for (int r = 0; r < NR; r++) {
-                        const T al = (T)alpha[r], be = (T)beta[r];
-                        pn[r] = po[r];
-                        an[r] = ao[r];
-                        if (run[r]) {
-                            pn[r] = first ? zv[r] : zv[r] + be * po[r];
-                            an[r] = first ? wv[r] : wv[r] + be * ao[r];
-                            rv[r] = rv[r] - al * an[r];
-                            xv[r] = xv[r] + al * pn[r];
-                            if (own) {
-                                acc[r] += (double)rv[r] * (double)rv[r];
-                                acc[NR + r] += (double)pn[r] * (double)an[r];
-                            }
+                            for (int r = 0; r < NR; r++) po[j][r] = ao[j][r] = 0;
                         }
-                        val[r * 3 + q] = run[r] ? (M)rv[r] : (M)0;
+#pragma unroll
+                        for (int r = 0; r < NR; r++) xv[j][r] = 0;
+                        if (own) ldn<true, T, NR>(a.x + k, xv[j]);
                     }
-                    if (own) {
-                        stn<T, NR>(a.x + k, xv);
-                        stn<T, NR>(r_new + k, rv);
-                        stn<T, NR>(p_new + k, pn);
-                        stn<T, NR>(ap_new + k, an);
+#pragma unroll
+                    for (int j = 0; j < kQ; j++) {
+                        const int q = q0 + j;
+                        const size_t k = (size_t)(3 * v + q) * NR;
+                        T pn[NR], an[NR];
+#pragma unroll
+                        for (int r = 0; r < NR; r++) {
+                            const T al = (T)alpha[r], be = (T)beta[r];
+                            pn[r] = po[j][r];
+                            an[r] = ao[j][r];
+                            if (run[r]) {
+                                pn[r] = first ? zv[j][r] : zv[j][r] + be * po[j][r];
+                                an[r] = first ? wv[j][r] : wv[j][r] + be * ao[j][r];
+                                rv[j][r] = rv[j][r] - al * an[r];
+                                xv[j][r] = xv[j][r] + al * pn[r];
+                                if (own) {
+                                    acc[r] += (double)rv[j][r] * (double)rv[j][r];
+                                    acc[NR + r] += (double)pn[r] * (double)an[r];
+                                }
+                            }
+                            val[r * 3 + q] = run[r] ? (M)rv[j][r] : (M)0;
+                        }
+                        if (own) {
+                            stn<T, NR>(a.x + k, xv[j]);
+                            stn<T, NR>(r_new + k, rv[j]);
+                            stn<T, NR>(p_new + k, pn);
+                            stn<T, NR>(ap_new + k, an);
+                        }
                     }
                 }
             }
@@ -1263,8 +1299,8 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
             if (r0 < r1) {
                 const int e0 = __ldg(a.tp.frow_ptr + r0), e1 = __ldg(a.tp.frow_ptr + r1);
                 for (int k = threadIdx.x; k <= r1 - r0; k += blockDim.x) rp[k] = __ldg(a.tp.frow_ptr + r0 + k) - e0;
-                for (int k = threadIdx.x; k < e1 - e0; k += blockDim.x) ccol[k] = __ldg(a.tp.fcol + e0 + k);
-                for (int k = threadIdx.x; k < 9 * (e1 - e0); k += blockDim.x) cval[k] = __ldg(a.A.fval + 9 * (size_t)e0 + k);
+                smem_fill(ccol, a.tp.fcol + e0, e1 - e0);
+                smem_fill(cval, a.A.fval + 9 * (size_t)e0, 9 * (e1 - e0));
                 rc = RowCache<T>{rp, ccol, cval, r0, r1, nullptr, nullptr, nullptr, nullptr};
                 // the rows' contact entries, when they fit the kcap slots
                 int* ru = reinterpret_cast<int*>(dsm + coop_rows_bytes(rpc, a.ecap, sizeof(T)));
@@ -1279,11 +1315,10 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
                         ru[k] = __ldg(a.tp.cu_ptr + r0 + k) - u0;
                         rl[k] = __ldg(a.tp.cl_ptr + r0 + k) - q0 + nu;
                     }
-                    for (int k = threadIdx.x; k < nu; k += blockDim.x) kcol[k] = __ldg(a.tp.uc_col + u0 + k);
-                    for (int k = threadIdx.x; k < nl; k += blockDim.x) kcol[nu + k] = __ldg(a.tp.cl_col + q0 + k);
-                    for (int k = threadIdx.x; k < 9 * nu; k += blockDim.x) kval[k] = __ldg(a.A.uc + 9 * (size_t)u0 + k);
-                    for (int k = threadIdx.x; k < 9 * nl; k += blockDim.x)
-                        kval[9 * nu + k] = __ldg(a.A.cl + 9 * (size_t)q0 + k);
+                    smem_fill(kcol, a.tp.uc_col + u0, nu);
+                    smem_fill(kcol + nu, a.tp.cl_col + q0, nl);
+                    smem_fill(kval, a.A.uc + 9 * (size_t)u0, 9 * nu);
+                    smem_fill(kval + 9 * nu, a.A.cl + 9 * (size_t)q0, 9 * nl);
                     rc.ru = ru;
                     rc.rl = rl;
                     rc.kcol = kcol;
@@ -1294,7 +1329,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
         if (a.dcap > 0) {
             const int d0 = blockIdx.x * kDomPerCta;
             ndc = max(0, min(a.dcap, a.nd01 - d0));
-            for (int k = threadIdx.x; k < ndc * 2304; k += blockDim.x) dom[k] = __ldg(a.inv + 2304 * (size_t)d0 + k);
+            smem_fill(dom, a.inv + 2304 * (size_t)d0, ndc * 2304);
             dcache = dom;
         }
         if (threadIdx.x == 0) rcs = rc;
@@ -1464,7 +1499,12 @@ struct FusedState {
     double rz0[NR], rz[NR], bn2[NR], rr[NR], beta[NR], alpha[NR], pap[NR];
     int iters[NR], status[NR];
     bool run[NR], stop_rz[NR];
+    bool ran_b[NR];  // updated by the last phase B, whose r.r and p.Ap are not applied yet
 };
+// values per CTA in each parity half of the partial buffer: phase A's three dots and the
+// previous phase B's two
+template <int NR>
+constexpr int kFusedStride = 5 * NR;
 
 template <class T, class M, int NR>
 __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a) {
@@ -1529,8 +1569,8 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
         if (r0 < r1) {
             const int e0 = __ldg(a.tp.frow_ptr + r0), e1 = __ldg(a.tp.frow_ptr + r1);
             for (int k = threadIdx.x; k <= r1 - r0; k += blockDim.x) rp[k] = __ldg(a.tp.frow_ptr + r0 + k) - e0;
-            for (int k = threadIdx.x; k < e1 - e0; k += blockDim.x) ccol[k] = __ldg(a.cs_lcol + e0 + k);
-            for (int k = threadIdx.x; k < 9 * (e1 - e0); k += blockDim.x) cval[k] = __ldg(a.A.fval + 9 * (size_t)e0 + k);
+            smem_fill(ccol, a.cs_lcol + e0, e1 - e0);
+            smem_fill(cval, a.A.fval + 9 * (size_t)e0, 9 * (e1 - e0));
             for (int k = threadIdx.x; k < r1 - r0; k += blockDim.x) dsl[k] = __ldg(a.cs_dslot + r0 + k);
             rc.r0 = r0;
             rc.r1 = r1;
@@ -1542,11 +1582,10 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
                     ru[k] = __ldg(a.tp.cu_ptr + r0 + k) - u0;
                     rl[k] = __ldg(a.tp.cl_ptr + r0 + k) - q0 + nu;
                 }
-                for (int k = threadIdx.x; k < nu; k += blockDim.x) kcol[k] = __ldg(a.tp.uc_col + u0 + k);
-                for (int k = threadIdx.x; k < nl; k += blockDim.x) kcol[nu + k] = __ldg(a.tp.cl_col + q0 + k);
-                for (int k = threadIdx.x; k < 9 * nu; k += blockDim.x) kval[k] = __ldg(a.A.uc + 9 * (size_t)u0 + k);
-                for (int k = threadIdx.x; k < 9 * nl; k += blockDim.x)
-                    kval[9 * nu + k] = __ldg(a.A.cl + 9 * (size_t)q0 + k);
+                smem_fill(kcol, a.tp.uc_col + u0, nu);
+                smem_fill(kcol + nu, a.tp.cl_col + q0, nl);
+                smem_fill(kval, a.A.uc + 9 * (size_t)u0, 9 * nu);
+                smem_fill(kval + 9 * nu, a.A.cl + 9 * (size_t)q0, 9 * nl);
                 rc.ru = ru;
                 rc.rl = rl;
                 rc.kcol = kcol;
@@ -1554,9 +1593,24 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
             }
             const int c0 = __ldg(a.cs_ptr + blockIdx.x);
             fc.nc = __ldg(a.cs_ptr + blockIdx.x + 1) - c0;
-            for (int k = threadIdx.x; k < fc.nc * SGIPC_MAX_LEVELS; k += blockDim.x) {
-                const int s = k / SGIPC_MAX_LEVELS, l = k % SGIPC_MAX_LEVELS;
-                tab[k] = l < a.mv.L ? __ldg(a.mv.table + (size_t)__ldg(a.cs_cols + c0 + s) * a.mv.L + l) : -1;
+            // (a gather through the column list: four elements per thread in flight)
+            for (int k0 = threadIdx.x; k0 < fc.nc * SGIPC_MAX_LEVELS; k0 += 4 * (int)blockDim.x) {
+                int col[4], tv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int k = k0 + u * (int)blockDim.x;
+                    col[u] = k < fc.nc * SGIPC_MAX_LEVELS ? __ldg(a.cs_cols + c0 + k / SGIPC_MAX_LEVELS) : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int k = k0 + u * (int)blockDim.x, l = k % SGIPC_MAX_LEVELS;
+                    tv[u] = col[u] >= 0 && l < a.mv.L ? __ldg(a.mv.table + (size_t)col[u] * a.mv.L + l) : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int k = k0 + u * (int)blockDim.x;
+                    if (k < fc.nc * SGIPC_MAX_LEVELS) tab[k] = tv[u];
+                }
             }
             // resident contact entries: the slot of their column in the static set, or a slot of
             // their own (the z values, not the slot numbers, enter the products: the atomic
@@ -1598,7 +1652,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
             const bool chain = a.mv.L > 3 && blockIdx.x == gridDim.x - 1;
             const int d0 = chain ? a.nd2 : (int)blockIdx.x * kDomPerCta;
             ndc = max(0, min(a.dcap, (chain ? a.ndom : a.nd2) - d0));
-            for (int k = threadIdx.x; k < ndc * 2304; k += blockDim.x) dom[k] = __ldg(a.inv + 2304 * (size_t)d0 + k);
+            smem_fill(dom, a.inv + 2304 * (size_t)d0, ndc * 2304);
             dcache = dom;
         }
         if (threadIdx.x == 0) {
@@ -1616,6 +1670,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
             S.stop_rz[r] = false;
             S.iters[r] = 0;
             S.status[r] = SGIPC_OK;
+            S.ran_b[r] = false;
             S.rz0[r] = S.rz[r] = S.rr[r] = S.bn2[r] = S.beta[r] = S.alpha[r] = S.pap[r] = 0.0;
         }
     double v[NR], t[NR];
@@ -1629,27 +1684,44 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
     T* acur = a.Ap;
     T* aalt = a.Ap2;
     phase_positions_l2<T, M, NR, 1>(a, S.alpha, nullptr, nullptr, rcur, S.run, v, s_l1);
-    bool ok = grid_reduce<NR>(a.br, ++epoch, kPhInit, v, a.partial, smem, t, 3 * NR);
+    bool ok = grid_reduce<NR>(a.br, ++epoch, kPhInit, v, a.partial, smem, t, kFusedStride<NR>);
     if (threadIdx.x == 0)
 #pragma unroll
         for (int r = 0; r < NR; r++) S.bn2[r] = S.rr[r] = t[r];
     if (ok) phase_fused_mas<T, M, NR>(a, sR, dcache, ndc);
     ok = ok && grid_barrier(a.br, ++epoch, kPhMas);
+    // phase B's r.r and p.Ap travel with the next phase A's dots (one reduction per
+    // iteration): the true-residual test of an update is taken one phase C + A later, and
+    // an update after which the solve ends (the r.z test, the cap) reduces them alone
+    double dB[2 * NR];
+#pragma unroll
+    for (int q = 0; q < 2 * NR; q++) dB[q] = 0.0;
     for (int k = 1; ok; k++) {
-        // ---- A: z, w = A z, r.z, z.w, z.Ap_old
-        double d3[3 * NR], t3[3 * NR];
+        // ---- A: z, w = A z, r.z, z.w, z.Ap_old (+ the previous B's r.r, p.Ap)
+        double d3[3 * NR], d5[5 * NR], t5[5 * NR];
 #pragma unroll
         for (int q = 0; q < 3 * NR; q++) d3[q] = 0.0;
         __syncthreads();  // S read below is settled
         phase_fused_spmv<T, M, NR>(a, rcs, fcs, rcur, acur, k == 1, S.run, d3);
-        if (!(ok = grid_reduce<3 * NR>(a.br, ++epoch, kPhFusedA, d3, a.partial, smem, t3, 3 * NR))) break;
+#pragma unroll
+        for (int q = 0; q < 3 * NR; q++) d5[q] = d3[q];
+#pragma unroll
+        for (int q = 0; q < 2 * NR; q++) d5[3 * NR + q] = dB[q];
+        if (!(ok = grid_reduce<5 * NR>(a.br, ++epoch, kPhFusedA, d5, a.partial, smem, t5, kFusedStride<NR>))) break;
         if (threadIdx.x == 0)
 #pragma unroll
             for (int r = 0; r < NR; r++) {
+                // the previous update's r.r and p.Ap; the true-residual test of that update
+                if (S.ran_b[r]) {
+                    S.ran_b[r] = false;
+                    S.rr[r] = t5[3 * NR + r];
+                    S.pap[r] = t5[4 * NR + r];
+                    if (S.run[r] && a.crit == SGIPC_CRIT_TRUE && S.rr[r] <= a.tol * a.tol * S.bn2[r]) S.run[r] = false;
+                }
                 S.stop_rz[r] = false;
                 S.alpha[r] = 0.0;
                 if (!S.run[r]) continue;
-                const double rz = t3[r], zw = t3[NR + r], zap = t3[2 * NR + r];
+                const double rz = t5[r], zw = t5[NR + r], zap = t5[2 * NR + r];
                 if (k == 1) {
                     S.rz0[r] = S.rz[r] = rz;
                     if (!(rz > 0.0) || !isfinite(rz)) {
@@ -1680,10 +1752,9 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
         for (int r = 0; r < NR; r++) any |= S.run[r];
         if (!any || k >= a.max_iter) break;
         // ---- B: p, Ap, x, r, restriction to levels 0..2; r.r, p.Ap
-        double d2[2 * NR], t2[2 * NR];
 #pragma unroll
-        for (int q = 0; q < 2 * NR; q++) d2[q] = 0.0;
-        phase_fused_update<T, M, NR>(a, S.alpha, S.beta, k == 1, pcur, palt, acur, aalt, rcur, ralt, S.run, d2, s_l1,
+        for (int q = 0; q < 2 * NR; q++) dB[q] = 0.0;
+        phase_fused_update<T, M, NR>(a, S.alpha, S.beta, k == 1, pcur, palt, acur, aalt, rcur, ralt, S.run, dB, s_l1,
                                      pcs);
         T* tmp = rcur;
         rcur = ralt;
@@ -1694,21 +1765,36 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
         tmp = acur;
         acur = aalt;
         aalt = tmp;
-        if (!(ok = grid_reduce<2 * NR>(a.br, ++epoch, kPhFusedB, d2, a.partial, smem, t2, 3 * NR))) break;
+        __syncthreads();  // every thread has read S.run for this update
         if (threadIdx.x == 0)
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                if (!S.run[r]) continue;
-                S.rr[r] = t2[r];
-                S.pap[r] = t2[NR + r];
-                if (S.stop_rz[r] || (a.crit == SGIPC_CRIT_TRUE && t2[r] <= a.tol * a.tol * S.bn2[r])) S.run[r] = false;
+                S.ran_b[r] = S.run[r];
+                if (S.stop_rz[r]) S.run[r] = false;  // the r.z test: this update was the last
             }
         __syncthreads();
         any = false;
 #pragma unroll
         for (int r = 0; r < NR; r++) any |= S.run[r];
-        if (!any || k + 1 >= a.max_iter) break;  // converged, or the iteration cap
-        // ---- C: the MAS domain solves
+        if (!any || k + 1 >= a.max_iter) {
+            // the solve ends with this update: its r.r (and the true-residual test) alone
+            double t2[2 * NR];
+            if (!(ok = grid_reduce<2 * NR>(a.br, ++epoch, kPhFusedB, dB, a.partial, smem, t2, kFusedStride<NR>)))
+                break;
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    if (!S.ran_b[r]) continue;
+                    S.ran_b[r] = false;
+                    S.rr[r] = t2[r];
+                    S.pap[r] = t2[NR + r];
+                    if (S.run[r] && a.crit == SGIPC_CRIT_TRUE && S.rr[r] <= a.tol * a.tol * S.bn2[r]) S.run[r] = false;
+                }
+            __syncthreads();
+            break;
+        }
+        // ---- C: the MAS domain solves (B's stores reach them through this barrier)
+        if (!(ok = grid_barrier(a.br, ++epoch, kPhFusedB))) break;
         phase_fused_mas<T, M, NR>(a, sR, dcache, ndc);
         if (!(ok = grid_barrier(a.br, ++epoch, kPhMas))) break;
     }
@@ -1720,7 +1806,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
             ok = grid_barrier(a.br, ++epoch, kPhAcc64);
             v[0] = 0.0;
             if (ok) phase_residual64(a, v[0]);
-            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhRes64, v, a.partial, smem, t, 3 * NR);
+            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhRes64, v, a.partial, smem, t, kFusedStride<NR>);
             rr_ref = t[0];
             v[0] = 0.0;
             if (ok) phase_positions_l2<T, M, NR, 2>(a, S.alpha, nullptr, nullptr, nullptr, S.run, v, s_l1);
@@ -1729,7 +1815,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
             ok = ok && grid_barrier(a.br, ++epoch, kPhMas);
             v[0] = 0.0;
             if (ok) phase_prolong_ref(a, v[0]);
-            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhProlong64, v, a.partial, smem, t, 3 * NR);
+            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhProlong64, v, a.partial, smem, t, kFusedStride<NR>);
             rz_ref = t[0];
         }
     }
