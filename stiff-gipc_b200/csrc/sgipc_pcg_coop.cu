@@ -225,9 +225,10 @@ __device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch, int tag)
 // barriers later at the earliest, after every CTA has read it.
 // `stride` (>= NR) is the number of values per CTA that each parity half of the buffer holds
 // (the same for every reduction of a kernel, so that the halves never overlap).
-template <int NR>
+template <int NR, int S>
 __device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, int tag, double (&v)[NR], double* partial,
-                            double* smem, double (&out)[NR], int stride = NR) {
+                            double (&smem)[S], double (&out)[NR], int stride = NR) {
+    static_assert(S >= NR * 32, "block_sum needs 32 doubles of shared memory per value");
     __shared__ double s_tot[NR];
     double* part = partial + (size_t)(epoch & 1) * stride * gridDim.x;
     block_sum<NR>(v, smem);
@@ -1508,7 +1509,7 @@ constexpr int kFusedStride = 5 * NR;
 
 template <class T, class M, int NR>
 __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a) {
-    __shared__ double smem[3 * NR * 32];
+    __shared__ double smem[kFusedStride<NR> * 32];  // block_sum of up to five values per right-hand side
     __shared__ __align__(16) M sR[kDomPerCta][48 * NR];
     __shared__ __align__(16) M s_l1[16][3 * NR];
     extern __shared__ __align__(16) unsigned char dsm[];
