@@ -64,7 +64,7 @@ struct PcgWork {
     PcgScalars* sc;          // [nrhs]
     double* partial;         // reduction partials [nrhs][max_blocks]
     unsigned int* ticket;    // [0..3] last-block counters; [4..5] grid barrier of the persistent solve
-    double* coop;            // persistent solve: block partials [2][5 nrhs][coop_cap]
+    double* coop;            // persistent solve: block partials [2][3 nrhs][coop_cap]
     int coop_cap;            // largest grid the persistent solve may use
     cudaGraphExec_t exec;    // captured iteration loop
     bool cond_graph;         // true: while-node graph (whole loop in one launch)

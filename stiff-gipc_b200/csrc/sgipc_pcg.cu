@@ -626,9 +626,9 @@ SgipcStatus alloc_work(SgipcCtx* c, PcgWork& w, size_t elem, int nrhs) {
     SG_CHECK(c, cudaMemset(w.sc, 0, sizeof(PcgScalars) * nrhs));
     w.coop_cap = coop_max_grid(c->device);
     if (w.coop_cap < 1) w.coop_cap = 1;
-    // grid-reduction partials: two parity halves of up to five values per right-hand side
+    // grid-reduction partials: two parity halves of up to three values per right-hand side
     // and CTA (the fused solve's phase-A reduction)
-    SG_CHECK(c, cudaMalloc((void**)&w.coop, sizeof(double) * 2 * 5 * nrhs * (size_t)w.coop_cap));
+    SG_CHECK(c, cudaMalloc((void**)&w.coop, sizeof(double) * 2 * 3 * nrhs * (size_t)w.coop_cap));
     return SGIPC_OK;
 }
 
