@@ -220,6 +220,8 @@ __device__ bool grid_barrier(const GridBarrier& br, unsigned int epoch, int tag)
     return s_ok != 0;
 }
 
+constexpr int kReduceLoads = 10;  // partial loads per lane issued together: grids up to 320 CTAs
+
 // Barrier + sum over CTAs: v[r] is this thread's contribution; on return out[r] holds the
 // grid total in every thread.  The partial buffer of parity epoch & 1 is rewritten two
 // barriers later at the earliest, after every CTA has read it.
@@ -236,21 +238,27 @@ __device__ bool grid_reduce(const GridBarrier& br, unsigned int epoch, int tag, 
 #pragma unroll
         for (int r = 0; r < NR; r++) part[r * gridDim.x + blockIdx.x] = v[r];
     const bool ok = grid_barrier(br, epoch, tag);
-    if (threadIdx.x < 32) {
-        // warp 0 adds the partials (fixed lane assignment and shuffle tree: the same total
-        // in every CTA)
-        double acc[NR];
+    // warp r adds the partials of value r: lane l takes CTAs l, l + 32, ... in that order
+    // (all its loads issued together, and all warps side by side: one L2 round trip), then a
+    // fixed xor tree, so every CTA computes the same total
+    static_assert(NR <= kCoopThreads / 32, "one warp per reduced value");
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w < NR) {
+        const int G = gridDim.x;
+        const double* pr = part + (size_t)w * G;
+        double t[kReduceLoads];
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
-            acc[r] = 0.0;
-#pragma unroll 4
-            for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) acc[r] += __ldcg(part + r * gridDim.x + k);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+        for (int j = 0; j < kReduceLoads; j++) {
+            const int k = lane + 32 * j;
+            t[j] = k < G ? __ldcg(pr + k) : 0.0;
         }
-        if (threadIdx.x == 0)
+        double acc = 0.0;
 #pragma unroll
-            for (int r = 0; r < NR; r++) s_tot[r] = acc[r];
+        for (int j = 0; j < kReduceLoads; j++) acc += t[j];
+        for (int k = lane + 32 * kReduceLoads; k < G; k += 32) acc += __ldcg(pr + k);  // grids beyond 320 CTAs
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) s_tot[w] = acc;
     }
     __syncthreads();
 #pragma unroll

@@ -55,12 +55,15 @@ __device__ __forceinline__ void block_sum(double (&v)[NR], double* smem /*[NR*32
 #pragma unroll
         for (int r = 0; r < NR; r++) smem[r * 32 + w] = v[r];
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (w == 0) {
+        // the warps' sums by warp 0: lane k takes warp k's, then a fixed xor tree (all NR
+        // values side by side; a serial loop in one thread waited out each load in turn)
         const int nw = (blockDim.x + 31) >> 5;
 #pragma unroll
         for (int r = 0; r < NR; r++) {
-            double s = 0;
-            for (int k = 0; k < nw; k++) s += smem[r * 32 + k];
+            double s = lane < nw ? smem[r * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             v[r] = s;
         }
     }
