@@ -1216,18 +1216,28 @@ __global__ void __launch_bounds__(SGIPC_BLOCK) k_energy(EnergyArgs a, EnergyOffs
         last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!last || threadIdx.x >= 32) return;
+    if (!last) return;
     __threadfence();
-    double total = 0.0;
-    for (int q = 0; q < 9; q++) {
+    // the terms' partials side by side: warp w adds terms w and w + 8 (lane l takes partials
+    // l, l + 32, ... of a term, four loads in flight, then a fixed xor tree); thread 0 adds
+    // the terms in order
+    __shared__ double st[9];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = w; q < 9; q += (int)(blockDim.x >> 5)) {
         double sum = 0.0;
-        for (int i = o.off[q] + (int)threadIdx.x; i < o.off[q + 1]; i += 32) sum += __ldcg(part + i);
+#pragma unroll 4
+        for (int i = o.off[q] + lane; i < o.off[q + 1]; i += 32) sum += __ldcg(part + i);
 #pragma unroll
         for (int k = 16; k > 0; k >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, k);
-        if (threadIdx.x == 0) terms[q] = sum;
-        total += sum;
+        if (lane == 0) st[q] = sum;
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
+        double total = 0.0;
+        for (int q = 0; q < 9; q++) {
+            terms[q] = st[q];
+            total += st[q];
+        }
         terms[9] = total;
         *ticket = 0u;
     }

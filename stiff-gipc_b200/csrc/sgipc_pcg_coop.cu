@@ -1259,13 +1259,24 @@ __device__ void phase_prolong_ref(const CoopArgs<T, M, NR>& a, double& rz) {
     const MasView& mv = a.mv;
     for (int v = spread_warp() * 32 + (int)(threadIdx.x & 31); v < a.nv; v += gridDim.x * blockDim.x) {
         const int* tv = mv.table + (size_t)v * mv.L;
+        // the vertex's clusters first, then all their Z values (two round trips, not two per
+        // level); the sums in level order
+        int gl[SGIPC_MAX_LEVELS];
+#pragma unroll
+        for (int l = 0; l < SGIPC_MAX_LEVELS; l++) gl[l] = l < mv.L ? __ldg(tv + l) : -1;
+        M zl[SGIPC_MAX_LEVELS][3];
+#pragma unroll
+        for (int l = 0; l < SGIPC_MAX_LEVELS; l++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) zl[l][q] = gl[l] >= 0 ? a.Z[3 * (size_t)gl[l] + q] : (M)0;
         M s0 = 0, s1 = 0, s2 = 0;
-        for (int l = 0; l < mv.L; l++) {
-            const int gl = __ldg(tv + l);
-            s0 += a.Z[3 * (size_t)gl];
-            s1 += a.Z[3 * (size_t)gl + 1];
-            s2 += a.Z[3 * (size_t)gl + 2];
-        }
+#pragma unroll
+        for (int l = 0; l < SGIPC_MAX_LEVELS; l++)
+            if (gl[l] >= 0) {
+                s0 += zl[l][0];
+                s1 += zl[l][1];
+                s2 += zl[l][2];
+            }
         const size_t k = 3 * (size_t)v;
         rz += __ldcg(a.r64 + k) * (double)(T)s0 + __ldcg(a.r64 + k + 1) * (double)(T)s1 +
               __ldcg(a.r64 + k + 2) * (double)(T)s2;
