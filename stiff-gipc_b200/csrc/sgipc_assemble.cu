@@ -357,9 +357,24 @@ __global__ void k_gather_blocks(int nnz, const int* __restrict__ cptr, const int
     if (tid >= 9LL * nnz) return;
     int s = (int)(tid / 9), q = (int)(tid % 9);
     int r = slot_row[s], c = col[s];
+    const int k0 = cptr[s], k1 = cptr[s + 1];
+    // the contributions four at a time, their index and value loads issued together (one by
+    // one, each waited out two L2 round trips), added in list order as before; the boundary
+    // test is applied after the loads
     double acc = 0.0;
-    if (btype[r] == 0 && btype[c] == 0)
-        for (int k = cptr[s]; k < cptr[s + 1]; k++) acc += eblk[9 * (size_t)contrib[k] + q];
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {
+        int ix[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) ix[u] = contrib[k + u];
+        double e[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) e[u] = eblk[9 * (size_t)ix[u] + q];
+#pragma unroll
+        for (int u = 0; u < 4; u++) acc += e[u];
+    }
+    for (; k < k1; k++) acc += eblk[9 * (size_t)contrib[k] + q];
+    if (btype[r] != 0 || btype[c] != 0) acc = 0.0;
     if (r == c && (q == 0 || q == 4 || q == 8)) acc += mass[r];
     o.v64[tid] = acc;
     o.v32[tid] = (float)acc;
@@ -390,8 +405,20 @@ __global__ void k_gather_grad(int nv, const int* __restrict__ vptr, const int* _
     int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= 3 * nv) return;
     int v = tid / 3, q = tid % 3;
+    const int k0 = vptr[v], k1 = vptr[v + 1];
     double acc = 0.0;
-    for (int k = vptr[v]; k < vptr[v + 1]; k++) acc += egrad[3 * (size_t)vinc[k] + q];
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {  // four incident elements in flight, added in list order
+        int ix[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) ix[u] = vinc[k + u];
+        double e[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) e[u] = egrad[3 * (size_t)ix[u] + q];
+#pragma unroll
+        for (int u = 0; u < 4; u++) acc += e[u];
+    }
+    for (; k < k1; k++) acc += egrad[3 * (size_t)vinc[k] + q];
     shape_grads[tid] += acc;
 }
 
@@ -836,18 +863,17 @@ __global__ void k_run_starts(int m, const unsigned long long* __restrict__ ks, c
                              int* __restrict__ nuc, int* __restrict__ lcount) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > m) return;
-    if (i == m) {
-        const int nu = rid[m];
-        nuc[0] = nu;
-        // end of the last run: the first unused-slot key (sorted last) or m
-        int lo = 0, hi = m;
-        while (lo < hi) {
-            int mid = (lo + hi) >> 1;
-            if (ks[mid] != kBadKey) lo = mid + 1; else hi = mid;
+    // end of the last run: the first unused-slot key (sorted last), or m; written by the
+    // thread at that boundary (a binary search by one thread took ~19 round trips)
+    {
+        const bool here = i == m ? (m == 0 || ks[m - 1] != kBadKey) : (ks[i] == kBadKey && (i == 0 || ks[i - 1] != kBadKey));
+        if (here) {
+            const int nu = rid[m];
+            nuc[0] = nu;
+            start[nu] = i;
         }
-        start[nu] = lo;
-        return;
     }
+    if (i == m) return;
     const unsigned long long k = ks[i];
     if (k == kBadKey || (i > 0 && ks[i - 1] == k)) return;
     const int u = rid[i];
@@ -913,9 +939,25 @@ __global__ void k_lower_place(int m, int n, const int* __restrict__ nuc, const i
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int nu = nuc[0];
     if (t <= n) {
+        // first block with row >= t: an 8-way search, seven probes in flight per step (five
+        // round trips for 30 000 blocks instead of fifteen)
         int lo = 0, hi = nu;
+        while (hi - lo > 8) {
+            const int step = (hi - lo + 7) >> 3;
+            int below = 0;  // probes lo + step .. lo + 7 step with row < t
+#pragma unroll
+            for (int j = 1; j < 8; j++) {
+                const int p = lo + j * step;
+                below += (p < hi && uc_row[p] < t) ? 1 : 0;
+            }
+            // the answer lies in (lo + below * step, lo + (below + 1) * step]
+            const int nlo = lo + below * step, nhi = min(hi, lo + (below + 1) * step);
+            lo = below > 0 ? nlo + 1 : lo;
+            hi = nhi;
+            if (below > 0 && lo > hi) lo = hi;
+        }
         while (lo < hi) {
-            int mid = (lo + hi) >> 1;
+            const int mid = (lo + hi) >> 1;
             if (uc_row[mid] < t) lo = mid + 1; else hi = mid;
         }
         cu_ptr[t] = lo;
@@ -941,7 +983,15 @@ __global__ void k_lower_rank(const int* __restrict__ nuc, const int* __restrict_
     }
     const int k0 = cl_ptr[col], k1 = cl_ptr[col + 1];
     int rank = 0;
-    for (int k = k0; k < k1; k++) rank += __ldg(uc_row + __ldg(cl_idx + k)) < row;
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {  // four list entries in flight
+        int ix[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) ix[u] = __ldg(cl_idx + k + u);
+#pragma unroll
+        for (int u = 0; u < 4; u++) rank += __ldg(uc_row + ix[u]) < row;
+    }
+    for (; k < k1; k++) rank += __ldg(uc_row + __ldg(cl_idx + k)) < row;
     lpos[u] = k0 + rank;
     cl_col[k0 + rank] = row;
 }

@@ -184,11 +184,21 @@ __device__ __forceinline__ void scatter_block_warp(double* dom, const int* __res
     for (int q = 0; q < 9; q++) V[q] = valid ? B[q] : 0.0;
     unsigned carriers = __ballot_sync(full, valid);  // lanes holding a partial sum
     const unsigned long long diag = r == c ? 1ull : 0ull;
-    for (int l = l_first; l < L; l++) {
+    // the clusters of r and c at every level, loaded together up front (one round trip)
+    int tr[SGIPC_MAX_LEVELS], tc[SGIPC_MAX_LEVELS];
+#pragma unroll
+    for (int l = 0; l < SGIPC_MAX_LEVELS; l++) {
+        const bool in = valid && l >= l_first && l < L;
+        tr[l] = in ? table[(size_t)r * L + l] : -1;
+        tc[l] = in ? table[(size_t)c * L + l] : -1;
+    }
+#pragma unroll
+    for (int l = 0; l < SGIPC_MAX_LEVELS; l++) {
+        if (l < l_first || l >= L) continue;  // warp-uniform
         int ga = -1, gb = -1;
         if (valid) {
-            ga = table[(size_t)r * L + l];
-            gb = table[(size_t)c * L + l];
+            ga = tr[l];
+            gb = tc[l];
         }
         // target (ga, gb) and whether the block is a diagonal one
         const unsigned long long key =
