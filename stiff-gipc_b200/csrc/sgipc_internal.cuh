@@ -35,7 +35,7 @@ struct PcgScalars {
     int32_t first;    // 1 until the first SpMV (p = z, no beta)
     int32_t pcur;     // which of the two p buffers holds the current direction
     int32_t halt;     // [rhs 0 only] set once the loop must stop; later bodies return at once
-    int32_t pad;
+    int32_t input_flag;  // persistent solve: the assembly's bad-input flag, copied at its end
     double rz_ref;    // refinement epilogue: r64 . M r64 and r64 . r64 of the FP64 residual
     double rr_ref;
 };
@@ -48,6 +48,7 @@ struct RefineArgs {
     const double* b64;
     double* r64;
     bool done;
+    bool assign;  // first refinement: x64 = x (x64 is not read before)
 };
 
 // One precision's PCG workspace (T = double or float) for up to `nrhs` right-hand sides.
@@ -66,6 +67,7 @@ struct PcgWork {
     unsigned int* ticket;    // [0..3] last-block counters; [4..5] grid barrier of the persistent solve
     double* coop;            // persistent solve: block partials [2][3 nrhs][coop_cap]
     int coop_cap;            // largest grid the persistent solve may use
+    bool last_coop;          // the latest solve ran as the persistent kernel (its scalars carry input_flag)
     cudaGraphExec_t exec;    // captured iteration loop
     bool cond_graph;         // true: while-node graph (whole loop in one launch)
     long long captured_key;  // precision/rhs tag and domain count the graph was captured for

@@ -444,9 +444,10 @@ __global__ void k_axpby_res(int n, const double* __restrict__ b, const double* _
     if (k < n) r[k] = b[k] - Ax[k];
 }
 
-__global__ void k_add_f32(int n, const float* __restrict__ d, double* __restrict__ x) {
+// x += d, or x = d (assign: the first refinement, x not read)
+__global__ void k_add_f32(int n, const float* __restrict__ d, double* __restrict__ x, int assign) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) x[k] += (double)d[k];
+    if (k < n) x[k] = (assign ? 0.0 : x[k]) + (double)d[k];
 }
 
 // rhs-major [nrhs][n3] <-> interleaved [n3][nrhs]
@@ -580,6 +581,7 @@ SgipcStatus run_pcg(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b, doub
     bool coop = false;
     if (ref) ref->done = false;
     SgipcStatus st = run_pcg_coop<T, M, NR>(c, w, fp32_mas, b, tol, max_iter, crit, s, &coop, ref);
+    w.last_coop = coop;
     if (st != SGIPC_OK || coop) return st;
     const int k3grid = domain_grid(c);
     st = get_loop_graph<T, M, NR>(c, w, inv, R, Z, k3grid, tag);
@@ -756,8 +758,11 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         SG_CHECK(c, cudaMemcpyAsync(x, c->pcg64.x, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
         PcgScalars hs;
         SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg64.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
-        SG_CHECK(c, cudaMemcpyAsync(input_flag(c), c->dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        // the persistent solve copies the bad-input flag into its scalars: one read-back
+        if (!c->pcg64.last_coop)
+            SG_CHECK(c, cudaMemcpyAsync(input_flag(c), c->dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
         SG_CHECK(c, cudaStreamSynchronize(s));
+        if (c->pcg64.last_coop) *input_flag(c) = hs.input_flag;
         if (*input_flag(c)) return input_error(c, s);
         SG_COUNT(c, 4LL * hs.bodies);
         out.iterations = hs.iter;
@@ -767,9 +772,9 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
         out.status = final_status(c, hs);
     } else {
         // mixed: FP32 MAS-PCG inner solves on the FP32 matrix copy, FP64 residual refinement
+        // the first inner solve takes b itself and sets x = its correction (nothing to zero or
+        // copy first); later ones take the FP64 residual r64 and add to x
         double* r64 = c->tmp64;
-        SG_CHECK(c, cudaMemsetAsync(x, 0, sizeof(double) * n3, s));
-        SG_CHECK(c, cudaMemcpyAsync(r64, b, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
         double rz0 = -1.0, rz = 0.0, bn2 = 0.0, rr = 0.0;
         int total_it = 0, ref = 0, status = SGIPC_OK;
         for (ref = 0; ref < 8; ref++) {
@@ -783,13 +788,14 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
                 inner_tol = bn2 > 0 && rr > 0 ? fmin(1.0, fmax(0.5 * tol * sqrt(bn2 / rr), 1e-10)) : 0.5 * tol;
             // the persistent solve refines itself where it can (x += x32, FP64 residual, its
             // r.z and r.r); otherwise the same steps follow here
-            RefineArgs rf{x, b, r64, false};
-            st = run_pcg<float, float, 1>(c, c->pcg32, 1, r64, inner_tol, max_iter, (int)crit, s, 20, &rf);
+            RefineArgs rf{x, b, r64, false, ref == 0};
+            st = run_pcg<float, float, 1>(c, c->pcg32, 1, ref == 0 ? b : r64, inner_tol, max_iter, (int)crit, s, 20,
+                                          &rf);
             if (st != SGIPC_OK) return st;
             PcgScalars hs;
             if (!rf.done) {
                 SG_COUNT(c, 2);
-                k_add_f32<<<nblk(n3), 256, 0, s>>>(n3, (const float*)c->pcg32.x, x);
+                k_add_f32<<<nblk(n3), 256, 0, s>>>(n3, (const float*)c->pcg32.x, x, ref == 0 ? 1 : 0);
                 // r = b - A x in FP64
                 if ((st = spmv_t<double>(c, x, c->tmp64b, s)) != SGIPC_OK) return st;
                 k_axpby_res<<<nblk(n3), 256, 0, s>>>(n3, b, c->tmp64b, r64);
@@ -800,8 +806,10 @@ static SgipcStatus solve_one(SgipcCtx* c, SgipcPrecision prec, SgipcCriterion cr
                 SG_CHECK(c, cudaMemcpyAsync(c->h_pinned, c->dot_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
             }
             SG_CHECK(c, cudaMemcpyAsync(&hs, c->pcg32.sc, sizeof(hs), cudaMemcpyDeviceToHost, s));
-            SG_CHECK(c, cudaMemcpyAsync(input_flag(c), c->dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
+            if (!c->pcg32.last_coop)
+                SG_CHECK(c, cudaMemcpyAsync(input_flag(c), c->dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
             SG_CHECK(c, cudaStreamSynchronize(s));
+            if (c->pcg32.last_coop) *input_flag(c) = hs.input_flag;
             if (*input_flag(c)) return input_error(c, s);
             if (rf.done) {
                 c->h_pinned[0] = hs.rz_ref;

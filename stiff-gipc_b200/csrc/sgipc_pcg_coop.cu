@@ -107,7 +107,7 @@ enum PhaseTag : int {
     kPhProlong = 4,    // z = sum of the levels' Z, r.z
     kPhSpmv = 5,       // p = z + beta p, Ap, p.Ap
     kPhUpdate = 6,     // x, r, restriction, r.r
-    kPhAcc64 = 7,      // refinement: x64 += x
+    kPhAcc64 = 7,      // refinement: x64 += x (no longer a phase of its own: kept for the tag numbering)
     kPhRes64 = 8,      // refinement: r64 = b64 - A x64
     kPhRestr64 = 9,    // refinement: restriction of r64
     kPhProlong64 = 10,  // refinement: r64 . M r64
@@ -157,6 +157,8 @@ struct CoopArgs {
     const int* l1_first;
     const int* l1_last;
     // refinement epilogue (FP32 inner solve, one right-hand side; x64 == nullptr: none)
+    int x64_assign;  // x64 = x instead of x64 += x (the first refinement)
+    const int* input_flag;  // copied into the scalars at the end (one read-back for both)
     double* x64;
     const double* b64;
     double* r64;
@@ -1222,21 +1224,37 @@ __device__ void phase_fused_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], c
 }
 
 // ---- refinement epilogue of the mixed solve (FP32 inner solve, one right-hand side) --------
+// The refined iterate x64 + x at column j, formed where the residual reads it (x64 is updated
+// only after every CTA has read it; on the first refinement x64 is not read)
+template <class T>
+struct RefineOperand {
+    const double* x64;
+    const T* x;
+    int assign;
+    __device__ __forceinline__ void load(int j, double (&xj)[1][3]) const {
+        double xa[3], xb[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            xa[q] = assign ? 0.0 : __ldcg(x64 + 3 * (size_t)j + q);
+            xb[q] = (double)__ldcg(x + 3 * (size_t)j + q);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++) xj[0][q] = xa[q] + xb[q];
+    }
+};
+
 // x64 += x (the inner solve's correction)
 template <class T, class M, int NR>
 __device__ void phase_accumulate64(const CoopArgs<T, M, NR>& a) {
     const int n3 = 3 * a.tp.n;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x)
-        a.x64[k] += (double)__ldcg(a.x + k);
+        a.x64[k] = (a.x64_assign ? 0.0 : a.x64[k]) + (double)__ldcg(a.x + k);
 }
 
 // r64 = b64 - A x64 with the FP64 matrix, r64 . r64
 template <class T, class M, int NR>
 __device__ void phase_residual64(const CoopArgs<T, M, NR>& a, double& rr) {
-    Operand<double, 1, true> op;  // x64 was written by every CTA: read through L2
-    op.a = a.x64;
-    op.b = nullptr;
-    op.beta[0] = 0.0;
+    RefineOperand<T> op{a.x64, a.x, a.x64_assign};
     constexpr int gpw = 32 / kSpG;
     const int lane = threadIdx.x & 31, n = a.tp.n;
     for (int i0 = grid_warp() * gpw; i0 < n; i0 += grid_warps() * gpw) {  // warp-uniform bound
@@ -1474,13 +1492,13 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
     double rz_ref = 0.0, rr_ref = 0.0;
     if constexpr (sizeof(T) == 4 && NR == 1) {
         if (ok && a.x64 && a.l2mode) {
-            // x64 += x; r64 = b64 - A x64; r64 . r64; M r64 (FP32 MAS); r64 . M r64
-            phase_accumulate64(a);
-            ok = grid_barrier(a.br, ++epoch, kPhAcc64);
+            // r64 = b64 - A (x64 + x); r64 . r64; x64 += x (after every CTA has read it);
+            // M r64 (FP32 MAS); r64 . M r64
             v[0] = 0.0;
-            if (ok) phase_residual64(a, v[0]);
-            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhRes64, v, a.partial, smem, t);
+            phase_residual64(a, v[0]);
+            ok = grid_reduce<NR>(a.br, ++epoch, kPhRes64, v, a.partial, smem, t);
             rr_ref = t[0];
+            if (ok) phase_accumulate64(a);
             v[0] = 0.0;
             if (ok) phase_positions_l2<T, M, NR, 2>(a, S.alpha, nullptr, nullptr, nullptr, S.run, v, s_l1);
             ok = ok && grid_barrier(a.br, ++epoch, kPhRestr64);
@@ -1505,6 +1523,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_coop(CoopArgs<T, M, NR> a)
             sc.rr = S.rr[r];
             sc.bodies = 0;
             sc.halt = 1;
+            sc.input_flag = a.input_flag ? *(volatile const int*)a.input_flag : 0;
             // state 0 = still running when the iteration cap was reached
             sc.state = ok ? (S.run[r] ? 0 : 2) : 2;
             sc.status = ok ? S.status[r] : SGIPC_CUDA_ERROR;
@@ -1789,13 +1808,13 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
     double rz_ref = 0.0, rr_ref = 0.0;
     if constexpr (sizeof(T) == 4 && NR == 1) {
         if (ok && a.x64) {
-            // x64 += x; r64 = b64 - A x64; r64 . r64; M r64 (FP32 MAS); r64 . M r64
-            phase_accumulate64(a);
-            ok = grid_barrier(a.br, ++epoch, kPhAcc64);
+            // r64 = b64 - A (x64 + x); r64 . r64; x64 += x (after every CTA has read it);
+            // M r64 (FP32 MAS); r64 . M r64
             v[0] = 0.0;
-            if (ok) phase_residual64(a, v[0]);
-            ok = ok && grid_reduce<NR>(a.br, ++epoch, kPhRes64, v, a.partial, smem, t, kFusedStride<NR>);
+            phase_residual64(a, v[0]);
+            ok = grid_reduce<NR>(a.br, ++epoch, kPhRes64, v, a.partial, smem, t, kFusedStride<NR>);
             rr_ref = t[0];
+            if (ok) phase_accumulate64(a);
             v[0] = 0.0;
             if (ok) phase_positions_l2<T, M, NR, 2>(a, S.alpha, nullptr, nullptr, nullptr, S.run, v, s_l1);
             ok = ok && grid_barrier(a.br, ++epoch, kPhRestr64);
@@ -1821,6 +1840,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
             sc.rr = S.rr[r];
             sc.bodies = 0;
             sc.halt = 1;
+            sc.input_flag = a.input_flag ? *(volatile const int*)a.input_flag : 0;
             sc.state = ok ? (S.run[r] ? 0 : 2) : 2;
             sc.status = ok ? S.status[r] : SGIPC_CUDA_ERROR;
         }
@@ -2015,6 +2035,8 @@ SgipcStatus run_pcg_coop(SgipcCtx* c, PcgWork& w, int fp32_mas, const double* b,
     a.l1_last = m.l1_last;
     const bool refine = ref && sizeof(T) == 4 && NR == 1 && a.l2mode;
     a.x64 = refine ? ref->x64 : nullptr;
+    a.x64_assign = refine && ref->assign ? 1 : 0;
+    a.input_flag = c->dflag;
     a.b64 = refine ? ref->b64 : nullptr;
     a.r64 = refine ? ref->r64 : nullptr;
     a.A64 = mat_view<double>(c);
