@@ -561,12 +561,15 @@ __device__ bool hier_barrier(int* info, unsigned int& epoch, long long limit) {
     if (threadIdx.x == 0) {
         unsigned int* cnt = reinterpret_cast<unsigned int*>(info + 20);
         volatile unsigned int* abort = reinterpret_cast<volatile unsigned int*>(info + 21);
-        __threadfence();
-        atomicAdd(cnt, 1u);
+        // release add / acquire poll (the CTA barriers around them carry the order to the
+        // CTA's other threads), as the persistent PCG's barrier: no separate fences
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(cnt), "r"(1u) : "memory");
         const unsigned int target = epoch * gridDim.x;
         int ok = 1;
         for (long long k = 0;; k++) {
-            if ((int)(*reinterpret_cast<volatile unsigned int*>(cnt) - target) >= 0) break;
+            unsigned int seen;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(cnt) : "memory");
+            if ((int)(seen - target) >= 0) break;
             if (*abort) {
                 ok = 0;
                 break;
@@ -578,7 +581,6 @@ __device__ bool hier_barrier(int* info, unsigned int& epoch, long long limit) {
             }
             if (k > 64) __nanosleep(64);
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
