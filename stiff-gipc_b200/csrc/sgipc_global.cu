@@ -18,9 +18,13 @@
 // B200 layout: the FEM rows run the FEM context's SpMV and MAS unchanged; the body rows
 // (a few thousand block rows at the C4 size) are one thread per block row over the row-
 // sorted merged blocks and a column-sorted index of their transposes, so every output is
-// summed in a fixed order (no atomics).  The loop is host-driven with device dot products
-// (two scalar reads per iteration, as the reference's): the coupled system is the
-// secondary path next to the persistent FEM solve.
+// summed in a fixed order (no atomics).  The loop's scalars (alpha, beta, the stop tests) live on
+// the device: small kernels compute them from the dot products and the vector kernels read
+// them, so the host reads the state back once per iteration, after the update and its stop
+// tests (the reference reads two scalars back per iteration).  Enqueuing several iterations per
+// read-back (the kernels after a stop return at once) measured slower on the affine-body bed:
+// its solves take about six iterations, and the preconditioner and SpMV of the iterations past
+// the stop cost more than the read-backs saved.
 #include <cub/cub.cuh>
 
 #include "sgipc_abd_ctx.cuh"
@@ -117,17 +121,71 @@ __global__ void k_g_fem_coupling(int nfem, int off, const int* __restrict__ cptr
     for (int q = 0; q < 3; q++) y[3 * (size_t)c + q] += acc[q];
 }
 
-__global__ void k_g_update(long long n, double alpha, const double* __restrict__ p, const double* __restrict__ Ap,
-                           double* __restrict__ x, double* __restrict__ r) {
+// Device state of the loop (PCGSolver::pcg's scalars).  halt: 0 running, 1 stopped (converged
+// or broken down), 2 stopped at the iteration cap.
+struct GState {
+    double rz0, rz, bn2, alpha, beta;
+    int iters, halt, status, stop;
+};
+// dot-product slots: d[0] p.Ap, d[1] r.r, d[2] r.z (new), d[3] r0.z0, d[4] b.b, d[5] residual^2;
+// the state from d + kStateOff
+constexpr int kStateOff = 16;
+
+__global__ void k_g_start(GState* st, const double* __restrict__ d) {
+    const double rz0 = d[3];
+    const bool run = rz0 > 0.0 && isfinite(rz0);
+    st->rz0 = st->rz = rz0;
+    st->bn2 = d[4];
+    st->alpha = st->beta = 0.0;
+    st->iters = 0;
+    st->stop = 0;
+    st->halt = run ? 0 : 1;
+    st->status = (!run && (!isfinite(rz0) || rz0 < 0.0)) ? SGIPC_BREAKDOWN : SGIPC_OK;
+}
+
+// alpha = r.z / p.Ap of iteration k; the r.z test of the current iterate (the reference stops
+// after this iteration's update)
+__global__ void k_g_alpha(GState* st, const double* __restrict__ d, int k, int crit, double tol) {
+    if (st->halt) return;
+    const double pAp = d[0];
+    st->iters = k;
+    if (!(pAp > 0.0) || !isfinite(pAp)) {
+        st->status = SGIPC_BREAKDOWN;
+        st->halt = 1;
+        return;
+    }
+    st->alpha = st->rz / pAp;
+    st->stop = crit == SGIPC_CRIT_RZ && fabs(st->rz) <= tol * st->rz0;
+}
+
+// after the update: the true-residual test, or the r.z one decided before it; the cap
+__global__ void k_g_after(GState* st, const double* __restrict__ d, int k, int crit, double tol, int max_iter) {
+    if (st->halt) return;
+    const bool stop = crit == SGIPC_CRIT_TRUE ? d[1] <= tol * tol * st->bn2 : st->stop != 0;
+    if (stop) st->halt = 1;
+    else if (k + 1 >= max_iter) st->halt = 2;
+}
+
+__global__ void k_g_beta(GState* st, const double* __restrict__ d) {
+    if (st->halt) return;
+    const double rz_new = d[2];
+    st->beta = rz_new / st->rz;
+    st->rz = rz_new;
+}
+
+__global__ void k_g_update(long long n, const GState* __restrict__ st, const double* __restrict__ p,
+                           const double* __restrict__ Ap, double* __restrict__ x, double* __restrict__ r) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || st->halt) return;
+    const double alpha = st->alpha;
     x[i] += alpha * p[i];
     r[i] -= alpha * Ap[i];
 }
 
-__global__ void k_g_direction(long long n, double beta, const double* __restrict__ z, double* __restrict__ p) {
+__global__ void k_g_direction(long long n, const GState* __restrict__ st, const double* __restrict__ z,
+                              double* __restrict__ p) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = z[i] + beta * p[i];
+    if (i < n && !st->halt) p[i] = z[i] + st->beta * p[i];
 }
 
 __global__ void k_g_residual(long long n, const double* __restrict__ b, double* __restrict__ y) {
@@ -186,13 +244,9 @@ SgipcStatus g_precond(const Global& g, const double* r, double* z) {
     return mas_apply_t<double>(g.f, r + 3 * (size_t)g.nb, z + 3 * (size_t)g.nb, g.fp32_mas, g.s);
 }
 
-SgipcStatus g_dot(const Global& g, const double* u, const double* v, double* out) {
-    SgipcStatus st = dot64(g.f, u, v, (int)g.N, g.a->g_dot, g.s);
-    if (st != SGIPC_OK) return st;
-    SG_CHECK(g.f, cudaMemcpyAsync(g.f->h_pinned, g.a->g_dot, sizeof(double), cudaMemcpyDeviceToHost, g.s));
-    SG_CHECK(g.f, cudaStreamSynchronize(g.s));
-    *out = g.f->h_pinned[0];
-    return SGIPC_OK;
+// u . v into the device slot d[slot] (no read-back)
+SgipcStatus g_dot(const Global& g, const double* u, const double* v, int slot) {
+    return dot64(g.f, u, v, (int)g.N, g.a->g_dot + slot, g.s);
 }
 
 }  // namespace
@@ -236,7 +290,7 @@ extern "C" SgipcStatus sgipc_global_pcg_solve(SgipcCtx* f, SgipcAbdCtx* a, Sgipc
         a->g_cap_ptr = ncols + 1;
     }
     if (a->g_cap_vec < (size_t)g.N) {
-        if ((st = grow(f, &a->g_vec, 4 * (size_t)g.N)) || (st = grow(f, &a->g_dot, 8))) return st;
+        if ((st = grow(f, &a->g_vec, 4 * (size_t)g.N)) || (st = grow(f, &a->g_dot, 32))) return st;
         a->g_cap_vec = (size_t)g.N;
     }
     SG_COUNT(f, 3);
@@ -254,60 +308,50 @@ extern "C" SgipcStatus sgipc_global_pcg_solve(SgipcCtx* f, SgipcAbdCtx* a, Sgipc
     double* p = z + g.N;
     double* Ap = p + g.N;
     const int gb = nblk(g.N);
+    double* d = a->g_dot;
+    GState* gst = reinterpret_cast<GState*>(d + kStateOff);
     SG_CHECK(f, cudaMemsetAsync(x, 0, sizeof(double) * g.N, g.s));
     SG_CHECK(f, cudaMemcpyAsync(r, b, sizeof(double) * g.N, cudaMemcpyDeviceToDevice, g.s));
     if ((st = g_precond(g, r, z))) return st;
-    double rz0 = 0, bn2 = 0;
-    if ((st = g_dot(g, r, z, &rz0))) return st;
-    if ((st = g_dot(g, b, b, &bn2))) return st;
+    if ((st = g_dot(g, r, z, 3)) || (st = g_dot(g, b, b, 4))) return st;
     SG_CHECK(f, cudaMemcpyAsync(p, z, sizeof(double) * g.N, cudaMemcpyDeviceToDevice, g.s));
-    double rz = rz0;
-    int iters = 0, status = SGIPC_OK;
-    bool running = rz0 > 0.0 && std::isfinite(rz0);
-    if (!running && (!std::isfinite(rz0) || rz0 < 0.0)) status = SGIPC_BREAKDOWN;
-    for (int k = 1; running && k < max_iter; k++) {
-        if ((st = g_spmv(g, p, Ap))) return st;
-        double pAp = 0;
-        if ((st = g_dot(g, p, Ap, &pAp))) return st;
-        iters = k;
-        if (!(pAp > 0.0) || !std::isfinite(pAp)) {
-            status = SGIPC_BREAKDOWN;
-            running = false;
-            break;
-        }
-        const double alpha = rz / pAp;
-        // the reference tests the r.z of the current iterate and stops after its update
-        bool stop = crit == SGIPC_CRIT_RZ && std::fabs(rz) <= tol * rz0;
+    SG_COUNT(f, 1);
+    k_g_start<<<1, 1, 0, g.s>>>(gst, d);
+    GState hs{};
+    SG_CHECK(f, cudaMemcpyAsync(&hs, gst, sizeof(hs), cudaMemcpyDeviceToHost, g.s));
+    SG_CHECK(f, cudaStreamSynchronize(g.s));
+    for (int k = 1; !hs.halt && k < max_iter; k++) {
+        if ((st = g_spmv(g, p, Ap)) || (st = g_dot(g, p, Ap, 0))) return st;
+        SG_COUNT(f, 2);
+        k_g_alpha<<<1, 1, 0, g.s>>>(gst, d, k, (int)crit, tol);
+        k_g_update<<<gb, SGIPC_BLOCK, 0, g.s>>>(g.N, gst, p, Ap, x, r);
+        if (crit == SGIPC_CRIT_TRUE && (st = g_dot(g, r, r, 1))) return st;
         SG_COUNT(f, 1);
-        k_g_update<<<gb, SGIPC_BLOCK, 0, g.s>>>(g.N, alpha, p, Ap, x, r);
-        if (crit == SGIPC_CRIT_TRUE) {
-            double rr = 0;
-            if ((st = g_dot(g, r, r, &rr))) return st;
-            stop = rr <= tol * tol * bn2;
-        }
-        if (stop) {
-            running = false;
-            break;
-        }
-        if (k + 1 >= max_iter) break;
-        if ((st = g_precond(g, r, z))) return st;
-        double rz_new = 0;
-        if ((st = g_dot(g, r, z, &rz_new))) return st;
-        const double beta = rz_new / rz;
-        rz = rz_new;
-        SG_COUNT(f, 1);
-        k_g_direction<<<gb, SGIPC_BLOCK, 0, g.s>>>(g.N, beta, z, p);
+        k_g_after<<<1, 1, 0, g.s>>>(gst, d, k, (int)crit, tol, max_iter);
+        SG_LAUNCH_CHECK(f, "global pcg");
+        // the one read-back of the iteration: stopped (converged, broken down, at the cap)?
+        SG_CHECK(f, cudaMemcpyAsync(&hs, gst, sizeof(hs), cudaMemcpyDeviceToHost, g.s));
+        SG_CHECK(f, cudaStreamSynchronize(g.s));
+        if (hs.halt) break;
+        if ((st = g_precond(g, r, z)) || (st = g_dot(g, r, z, 2))) return st;
+        SG_COUNT(f, 2);
+        k_g_beta<<<1, 1, 0, g.s>>>(gst, d);
+        k_g_direction<<<gb, SGIPC_BLOCK, 0, g.s>>>(g.N, gst, z, p);
     }
-    if (running && status == SGIPC_OK) status = SGIPC_NOT_CONVERGED;  // the iteration cap
-    SG_LAUNCH_CHECK(f, "global pcg");
+    int status = hs.status;
+    // still running at the cap: not converged
+    if (status == SGIPC_OK && hs.halt != 1) status = SGIPC_NOT_CONVERGED;
     // ---- true residual, distribute_solution
-    double rel = 0;
     if ((st = g_spmv(g, x, Ap))) return st;
     SG_COUNT(f, 1);
     k_g_residual<<<gb, SGIPC_BLOCK, 0, g.s>>>(g.N, b, Ap);
-    double res2 = 0;
-    if ((st = g_dot(g, Ap, Ap, &res2))) return st;
-    rel = bn2 > 0 ? std::sqrt(res2 / bn2) : std::sqrt(res2);
+    if ((st = g_dot(g, Ap, Ap, 5))) return st;
+    SG_CHECK(f, cudaMemcpyAsync(f->h_pinned, d + 5, sizeof(double), cudaMemcpyDeviceToHost, g.s));
+    SG_CHECK(f, cudaStreamSynchronize(g.s));
+    const double res2 = f->h_pinned[0], bn2 = hs.bn2;
+    const double rel = bn2 > 0 ? std::sqrt(res2 / bn2) : std::sqrt(res2);
+    const double rz0 = hs.rz0, rz = hs.rz;
+    const int iters = hs.iters;
     if (abd_point_dx && a->P > 0) {
         SG_COUNT(f, 1);
         k_g_point_dx<<<nblk(a->P), SGIPC_BLOCK, 0, g.s>>>(a->P, a->point_body, a->x_bar, x, abd_point_dx);
