@@ -110,3 +110,23 @@ def test_global_solve_needs_both_preconditioners(coupled):
         assert e.value.status == N.NOT_READY
     finally:
         sysm.close()
+
+
+def test_global_solve_stops_at_cap_and_on_zero_rhs(coupled):
+    """The loop's state lives on the device: at the iteration cap the solve reports
+    NOT_CONVERGED after max_iter - 1 updates, at the iterate of the oracle's loop with the same
+    cap (1e-9); a zero right-hand side stops before the first update (status OK, x = 0)."""
+    sc, bodies, A, (frow, fcol, fval), c, g, sysm = coupled
+    system.MASPreconditioner(g).setPreconditioner("fp64")
+    om = oracle.Mas(sc, frow, fcol, fval)
+    gls = abd.GlobalLinearSystem(g, sysm)
+    b = np.random.default_rng(13).normal(size=A.shape[0])
+    cap = 4
+    x, _, st = gls.solve_linear_system(torch.tensor(b, device="cuda"), tol=1e-14, max_iter_ratio=(cap + 0.5) / gls.dof)
+    ox, oit, orz0, _ = oracle.global_pcg(A, NB, om, b, 1e-14, max_iter=cap)
+    assert st.status == N.NOT_CONVERGED
+    assert st.iterations == cap - 1 and oit == cap  # the oracle counts as or_pcg does
+    assert _rel(x.cpu().numpy(), ox) < 1e-9
+    z, _, st0 = gls.solve_linear_system(torch.zeros(A.shape[0], dtype=torch.float64, device="cuda"))
+    assert st0.status == N.OK and st0.iterations == 0
+    assert float(z.abs().max()) == 0.0
