@@ -131,7 +131,9 @@ __global__ void __launch_bounds__(128) k_snk(int nt, const uint32_t* __restrict_
     const int pa[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
     const int pb[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
     const int ax_i[3] = {1, 0, 0}, ax_j[3] = {2, 2, 1};
-#pragma unroll 1
+    // (unrolled: the vertex pair of each block is then a compile-time index into d, which a
+    // rolled loop kept in local memory; 168 registers, measured 4 % faster than rolled)
+#pragma unroll
     for (int k = 0; k < 10; k++) {
         const int a = pa[k], b = pb[k];
         double K[3][3];
