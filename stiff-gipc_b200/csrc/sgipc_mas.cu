@@ -603,7 +603,10 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
         if (h.L == 1) info[16] = h.npos;
     }
     for (int v = tid; v < max(h.nv, h.npos); v += nth) {
-        if (v < h.npos) h.up[v] = -1;  // padding positions have no parent
+        if (v < h.npos) {
+            h.up[v] = -1;     // padding positions have no parent
+            h.mask[v] = 0u;   // level 0's connection masks start empty
+        }
         if (v < h.nv) {
             const int p = h.real_map[v];
             h.node[v] = p;
@@ -614,8 +617,7 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
     for (int l = 0; l + 1 < h.L; l++) {
         const int count = info[8 + l], start = info[l];
         const int nbank = (count + 15) >> 4;
-        for (int k = tid; k < count; k += nth) h.mask[k] = 0u;
-        if (!hier_barrier(info, epoch, h.spin_limit)) return;
+        // (the masks of this level were zeroed by the previous phase)
         // edge masks (one lane per neighbour slot) and contact-pair masks, warp-aggregated
         for (int k0 = gw * 32; k0 < h.nnbr; k0 += nw * 32) {
             const int k = k0 + lane;
@@ -677,6 +679,9 @@ __global__ void __launch_bounds__(kHierThreads) k_hierarchy(HierArgs h) {
             h.up[start + a] = start_next + nn;  // every vertex of node a writes the same parent
             if (l + 2 == h.L) h.up[start_next + nn] = -1;
         }
+        // the next level's masks start empty (nothing reads the masks in this phase)
+        if (l + 2 < h.L)
+            for (int k = tid; k < h.bank_off[nbank]; k += nth) h.mask[k] = 0u;
         if (!hier_barrier(info, epoch, h.spin_limit)) return;
     }
     if (h.L >= 3) {
