@@ -412,7 +412,7 @@ SgipcStatus sgipc_close_check(SgipcCtx* ctx, const double* x, double ground_offs
  * b, x [dev double[12 * body_num + 3 n]]; abd_point_dx [dev double3[point_num], may be
  * null] receives J(x_bar) dq of every ABD point.  max_iter <= 0: 0.3 x DOFs.  Returns
  * SGIPC_NOT_READY unless both systems are assembled and both preconditioners built.
- * Synchronises (two scalar reads per iteration). */
+ * Synchronises (one read-back of the loop's device-side state per iteration). */
 SgipcStatus sgipc_global_pcg_solve(SgipcCtx* fem, SgipcAbdCtx* abd, SgipcCriterion crit, double tol,
                                    int32_t max_iter, const double* b, double* x, double* abd_point_dx,
                                    SgipcSolveStats* stats, void* stream);
