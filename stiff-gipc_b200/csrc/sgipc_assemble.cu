@@ -343,8 +343,7 @@ __global__ void k_hinge_quad(int nh, const uint32_t* __restrict__ edges, const i
 // static gathers
 // ------------------------------------------------------------------------------------------
 struct StaticOut {
-    double* v64;       // upper slots
-    float* v32;
+    double* v64;       // upper slots (the MAS scatter and the BCOO export read these)
     const int* fup;    // full-pattern index of each upper slot
     const int* flo;    // full-pattern index of its transpose (-1 on the diagonal)
     double* f64;       // full symmetric copy
@@ -379,7 +378,6 @@ __global__ void k_gather_blocks(int nnz, const int* __restrict__ cptr, const int
     if (btype[r] != 0 || btype[c] != 0) acc = 0.0;
     if (r == c && (q == 0 || q == 4 || q == 8)) acc += mass[r];
     o.v64[tid] = acc;
-    o.v32[tid] = (float)acc;
     const size_t fu = 9 * (size_t)o.fup[s] + q;
     o.f64[fu] = acc;
     o.f32[fu] = (float)acc;
@@ -394,7 +392,6 @@ __global__ void k_gather_blocks(int nnz, const int* __restrict__ cptr, const int
 static StaticOut static_out(SgipcCtx* c) {
     StaticOut o;
     o.v64 = c->val64;
-    o.v32 = c->val32;
     o.fup = c->fup;
     o.flo = c->flo;
     o.f64 = c->fval64;
@@ -1864,7 +1861,10 @@ SgipcStatus assemble_time_hook(SgipcCtx* c, const char* name, cudaStream_t s, do
         k_gather_blocks<<<nblk(9LL * c->nnz), SGIPC_BLOCK, 0, s>>>(c->nnz, c->contrib_ptr, c->contrib, c->eblk,
                                                                     c->slot_row, c->col, f->BoundaryType, f->masses,
                                                                     static_out(c));
-        *bytes = (double)c->n_eblk * (72 + 4) + (double)c->nnz * (72 + 36 + 8 + 4);
+        // element blocks and their indices in; per upper slot its indices, flags and the FP64
+        // upper value out, the full-pattern FP64 + FP32 copy, and the transposed copy off the
+        // diagonal
+        *bytes = (double)c->n_eblk * (72 + 4) + (double)c->nnz * (28 + 72 + 108) + (double)(c->nnz - c->n) * 108;
     } else if (!strcmp(name, "barrier")) {
         if (!k || k->pair_num <= 0) return SGIPC_BAD_INPUT;
         SG_COUNT(c, 1);

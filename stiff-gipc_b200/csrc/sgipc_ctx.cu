@@ -203,7 +203,6 @@ static SgipcStatus build_static(SgipcCtx* c, const SgipcTopology* t) {
     SG_TRY(upload(c, &c->vinc_ptr, vptr));
     SG_TRY(upload(c, &c->vinc, vinc));
     SG_TRY(dalloc(c, &c->val64, (size_t)nnz * 9));
-    SG_TRY(dalloc(c, &c->val32, (size_t)nnz * 9));
     SG_TRY(dalloc(c, &c->eblk, (size_t)c->n_eblk * 9));
     SG_TRY(dalloc(c, &c->egrad, (size_t)c->n_egrad * 3));
     return SGIPC_OK;
@@ -369,7 +368,7 @@ extern "C" SgipcStatus sgipc_destroy(SgipcCtx* c) {
     broad_destroy(c);
     pcg_destroy(c);
     mas_destroy(c);
-    void* ptrs[] = {c->row_ptr, c->col, c->slot_row, c->diag_slot, c->low_ptr, c->low_slot, c->val64, c->val32,
+    void* ptrs[] = {c->row_ptr, c->col, c->slot_row, c->diag_slot, c->low_ptr, c->low_slot, c->val64,
                     c->eblk, c->contrib_ptr, c->contrib, c->egrad, c->vinc_ptr, c->vinc, c->tets, c->tris,
                     c->hinges, c->hinge_adj, c->soft_idx, c->shape_grads, c->fb, c->b, c->ckey, c->ckey_s,
                     c->cidx, c->cidx_s, c->cval, c->cflag, c->nuc, c->uc_row, c->uc_col, c->uc64, c->uc32,

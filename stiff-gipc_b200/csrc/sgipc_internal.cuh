@@ -140,7 +140,6 @@ struct SgipcCtx {
     int* low_ptr;             // [n+1] lower (transposed) entries per row
     int* low_slot;            // [nnz - n]
     double* val64;            // [nnz*9]
-    float* val32;             // [nnz*9]
     // full symmetric copy of the static blocks (both triangles) for the SpMV
     int nnz_full;             // 2*nnz - n
     int* frow_ptr;            // [n+1]
