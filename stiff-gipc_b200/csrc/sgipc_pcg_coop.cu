@@ -1129,16 +1129,17 @@ __device__ void phase_fused_update(const CoopArgs<T, M, NR>& a, const double (&a
 // array, 160 nodes), restricted from R2 with the half-warp groups of restrict_coarse_cta (the
 // same sums), and the domains of levels >= 3 are solved from it, their inverses from `cache`
 // (ncache of them, from domain nd2 on) or global memory.  Only Z is written.  Returns false
-// (nothing done) when the levels above 2 hold more than 160 nodes.
+// (nothing done) when the levels above 2 hold more than 160 nodes.  `cb` was zeroed once at
+// the start of the solve: every node with children is overwritten by each call, and the
+// padding nodes stay zero.  upc: the parents of the nodes from level 2 on (up[info[2] + k]),
+// kept in shared memory for the solve, or nullptr (read from global memory).
 template <class T, class M, int NR>
-__device__ bool coarse_chain_smem(const CoopArgs<T, M, NR>& a, M* cb, const M* cache, int ncache) {
+__device__ bool coarse_chain_smem(const CoopArgs<T, M, NR>& a, M* cb, const M* cache, int ncache, const int* upc) {
     const int* info = a.mv.info;
     const int L = a.mv.L;
-    const int start3 = info[3];
+    const int start3 = info[3], start2 = info[2];
     const int ntop = info[16] - start3;  // nodes of levels >= 3, padding included
     if (ntop > 160 || ntop <= 0) return false;
-    for (int k = threadIdx.x; k < ntop * 3 * NR; k += blockDim.x) cb[k] = 0;
-    __syncthreads();
     for (int l = 2; l + 1 < L; l++) {
         const int count = info[8 + l], start = info[l];
         for (int base = 0; base < count; base += blockDim.x) {
@@ -1147,7 +1148,7 @@ __device__ bool coarse_chain_smem(const CoopArgs<T, M, NR>& a, M* cb, const M* c
             int par = -1;
             if (aa < count) {
                 const int g = start + aa;
-                par = __ldg(a.mv.up + g);
+                par = upc ? upc[g - start2] : __ldg(a.mv.up + g);
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
                     M t[NR];
@@ -1211,10 +1212,11 @@ __device__ bool coarse_chain_smem(const CoopArgs<T, M, NR>& a, M* cb, const M* c
 // last CTA restricts 2 -> 3 -> ... and solves the domains above, in shared memory where the
 // levels above 2 fit (coarse_chain_smem), else as the MAS phase of k_pcg_coop.
 template <class T, class M, int NR>
-__device__ void phase_fused_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], const M* dcache, int ndc) {
+__device__ void phase_fused_mas(const CoopArgs<T, M, NR>& a, M (*sR)[48 * NR], const M* dcache, int ndc,
+                                const int* upc) {
     const int L = a.mv.L, G = gridDim.x;
     if (L > 3 && blockIdx.x == G - 1) {
-        if (!coarse_chain_smem<T, M, NR>(a, &sR[0][0], dcache, ndc)) {
+        if (!coarse_chain_smem<T, M, NR>(a, &sR[0][0], dcache, ndc, upc)) {
             restrict_coarse_cta<M, NR, true>(a.mv.info, a.mv.up, L, a.R, 2);
             solve_domain_range<M, NR>(a.inv, a.R, a.Z, a.nd2, a.ndom, G - 1, 1, sR);
         }
@@ -1558,6 +1560,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
     __shared__ FusedCache<T, NR> fcs;
     __shared__ int s_pv[kPosBanks * 16], s_ppar[kPosBanks * 16], s_pup1[16];
     __shared__ PosCache pcs;
+    __shared__ const int* s_chain_up;
     const M* dcache = nullptr;
     int ndc = 0;
     {
@@ -1694,6 +1697,21 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
             smem_fill(dom, a.inv + 2304 * (size_t)d0, ndc * 2304);
             dcache = dom;
         }
+        // the coarse chain's CTA: its staging array zeroed once (the chain overwrites every node
+        // with children and leaves the padding nodes at zero), and the parents of the nodes
+        // from level 2 on cached in the update pass's position arrays, which this CTA does not
+        // use when it holds no level-1 bank
+        if (a.mv.L > 3 && blockIdx.x == gridDim.x - 1) {
+            for (int k = threadIdx.x; k < kDomPerCta * 48 * NR; k += blockDim.x) (&sR[0][0])[k] = 0;
+            const int nup = a.mv.info[16] - a.mv.info[2];
+            const bool no_bank = (int)blockIdx.x >= ((a.mv.info[9] + 15) >> 4);  // s_pv unused
+            const bool room = no_bank && nup > 0 && nup <= kPosBanks * 16;
+            if (room)
+                for (int k = threadIdx.x; k < nup; k += blockDim.x) s_pv[k] = __ldg(a.mv.up + a.mv.info[2] + k);
+            if (threadIdx.x == 0) s_chain_up = room ? s_pv : nullptr;
+        } else if (threadIdx.x == 0) {
+            s_chain_up = nullptr;
+        }
         if (threadIdx.x == 0) {
             rcs = rc;
             fcs = fc;
@@ -1726,7 +1744,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
     if (threadIdx.x == 0)
 #pragma unroll
         for (int r = 0; r < NR; r++) S.bn2[r] = S.rr[r] = t[r];
-    if (ok) phase_fused_mas<T, M, NR>(a, sR, dcache, ndc);
+    if (ok) phase_fused_mas<T, M, NR>(a, sR, dcache, ndc, s_chain_up);
     ok = ok && grid_barrier(a.br, ++epoch, kPhMas);
     for (int k = 1; ok; k++) {
         // ---- A: z, w = A z, r.z, z.w, z.Ap_old
@@ -1802,7 +1820,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
         for (int r = 0; r < NR; r++) any |= S.run[r];
         if (!any || k + 1 >= a.max_iter) break;  // converged, or the iteration cap
         // ---- C: the MAS domain solves
-        phase_fused_mas<T, M, NR>(a, sR, dcache, ndc);
+        phase_fused_mas<T, M, NR>(a, sR, dcache, ndc, s_chain_up);
         if (!(ok = grid_barrier(a.br, ++epoch, kPhMas))) break;
     }
     double rz_ref = 0.0, rr_ref = 0.0;
@@ -1818,7 +1836,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_pcg_fused(CoopArgs<T, M, NR> a
             v[0] = 0.0;
             if (ok) phase_positions_l2<T, M, NR, 2>(a, S.alpha, nullptr, nullptr, nullptr, S.run, v, s_l1);
             ok = ok && grid_barrier(a.br, ++epoch, kPhRestr64);
-            if (ok) phase_fused_mas<T, M, NR>(a, sR, dcache, ndc);
+            if (ok) phase_fused_mas<T, M, NR>(a, sR, dcache, ndc, s_chain_up);
             ok = ok && grid_barrier(a.br, ++epoch, kPhMas);
             v[0] = 0.0;
             if (ok) phase_prolong_ref(a, v[0]);
